@@ -1,0 +1,880 @@
+// fmg_oracle.cpp -- CPU restatement of Femlisp's multigrid solve path.
+//
+// TEST INFRASTRUCTURE ONLY (the checker of the GPU path; see fmg_oracle.h for
+// the list of reference files restated and for the canonical arithmetic).
+// Build with -ffp-contract=off: every fused multiply-add is an explicit fma().
+//
+// Structured restatement: Femlisp keys matrix blocks by mesh cells in hash
+// tables (sparse-matrix.lisp:703-840).  On a uniformly refined n-cube the
+// key <-> index map is fixed (lexicographic node numbering, x fastest), and a
+// level matrix is stored by stencil slot: slot s holds A(i, i+off_s) for every
+// node i, with zeros where the reference has no block (outside the grid,
+// eliminated Dirichlet columns, structurally absent Q2 couplings).
+#include "fmg_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------- reductions
+constexpr int DR_LANES = 256, DR_VEC = 2, DR_CHUNK = 4096, DR_M = DR_CHUNK / (DR_LANES * DR_VEC);
+
+// 256 lane sums -> one value: halving 16,8,4,2,1 inside each 32-lane group,
+// then halving 4,2,1 over the 8 group sums (the order of a warp butterfly
+// followed by a butterfly over the warp sums).
+double dr_fold256(double* v) {
+  double g[8];
+  for (int w = 0; w < 8; ++w) {
+    double a[32];
+    for (int l = 0; l < 32; ++l) a[l] = v[32 * w + l];
+    for (int half = 16; half >= 1; half >>= 1)
+      for (int l = 0; l < half; ++l) a[l] = a[l] + a[l + half];
+    g[w] = a[0];
+  }
+  for (int half = 4; half >= 1; half >>= 1)
+    for (int l = 0; l < half; ++l) g[l] = g[l] + g[l + half];
+  return g[0];
+}
+
+double dr_chunk(const double* x, const double* y, long n, long c) {
+  double lane[DR_LANES];
+  long base = c * DR_CHUNK;
+  for (int t = 0; t < DR_LANES; ++t) {
+    double acc = 0.0;
+    for (int m = 0; m < DR_M; ++m)
+      for (int u = 0; u < DR_VEC; ++u) {
+        long i = base + DR_VEC * t + (long)DR_LANES * DR_VEC * m + u;
+        if (i < n) acc = std::fma(x[i], y[i], acc);
+      }
+    lane[t] = acc;
+  }
+  return dr_fold256(lane);
+}
+
+double dr_final(const double* part, long P) {
+  double lane[DR_LANES];
+  for (int t = 0; t < DR_LANES; ++t) {
+    double acc = 0.0;
+    for (long k = t; k < P; k += DR_LANES) acc = acc + part[k];
+    lane[t] = acc;
+  }
+  return dr_fold256(lane);
+}
+
+double dr_dot(const double* x, const double* y, long n, bool par) {
+  long P = (n + DR_CHUNK - 1) / DR_CHUNK;
+  if (P == 0) return 0.0;
+  std::vector<double> part(P);
+  if (par) {
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < P; ++c) part[c] = dr_chunk(x, y, n, c);
+  } else {
+    for (long c = 0; c < P; ++c) part[c] = dr_chunk(x, y, n, c);
+  }
+  return dr_final(part.data(), P);
+}
+
+// ---------------------------------------------------------------- FE tables
+// Gauss rule with order+1 points per direction on [0,1]
+// (fe.lisp:235-244, quadrature.lisp:202-215): xi = (1 - t)/2 for the
+// Gauss-Legendre nodes t in ascending order, weight = w_GL / 2.
+struct Rule1D {
+  int np = 0;
+  double xi[3], w[3];
+};
+
+Rule1D gauss1d(int order) {
+  Rule1D r;
+  if (order == 1) {
+    double t = std::sqrt(1.0 / 3.0);
+    double ts[2] = {-t, t};
+    r.np = 2;
+    for (int k = 0; k < 2; ++k) { r.xi[k] = 0.5 * (1.0 - ts[k]); r.w[k] = 0.5; }
+  } else {
+    double t = std::sqrt(0.6);
+    double ts[3] = {-t, 0.0, t};
+    double wg[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    r.np = 3;
+    for (int k = 0; k < 3; ++k) { r.xi[k] = 0.5 * (1.0 - ts[k]); r.w[k] = 0.5 * wg[k]; }
+  }
+  return r;
+}
+
+// 1D Lagrange basis with uniform nodes 0, 1/p, .., 1 (lagrange.lisp:41-51)
+double lag1d(int order, int a, double s) {
+  if (order == 1) return a == 0 ? 1.0 - s : s;
+  if (a == 0) return 2.0 * (s - 0.5) * (s - 1.0);
+  if (a == 1) return 4.0 * s * (1.0 - s);
+  return 2.0 * s * (s - 0.5);
+}
+double dlag1d(int order, int a, double s) {
+  if (order == 1) return a == 0 ? -1.0 : 1.0;
+  if (a == 0) return 4.0 * s - 3.0;
+  if (a == 1) return 4.0 - 8.0 * s;
+  return 4.0 * s - 1.0;
+}
+
+struct Tables {
+  int dim = 0, order = 0, nl = 0, nq = 0;
+  Rule1D r;
+  std::vector<double> C;     // [q][a][b]: (W_q vol) * grad phi_a . grad phi_b
+  std::vector<double> Kbar;  // [a][b]: sum_q C
+  std::vector<double> Phi;   // [q][a]: (W_q vol) * phi_a
+};
+
+Tables make_tables(int dim, int order, double h) {
+  Tables T;
+  T.dim = dim; T.order = order;
+  T.r = gauss1d(order);
+  int p1 = order + 1;
+  T.nl = 1; T.nq = 1;
+  for (int k = 0; k < dim; ++k) { T.nl *= p1; T.nq *= T.r.np; }
+  double vol = 1.0;
+  for (int k = 0; k < dim; ++k) vol = vol * h;
+  double invh = 1.0 / h;
+  T.C.assign((size_t)T.nq * T.nl * T.nl, 0.0);
+  T.Kbar.assign((size_t)T.nl * T.nl, 0.0);
+  T.Phi.assign((size_t)T.nq * T.nl, 0.0);
+  for (int q = 0; q < T.nq; ++q) {
+    int qi[3] = {q % T.r.np, (q / T.r.np) % T.r.np, q / (T.r.np * T.r.np)};
+    double W = 1.0;
+    for (int k = 0; k < dim; ++k) W = W * T.r.w[qi[k]];
+    double Wv = W * vol;
+    std::vector<double> G((size_t)T.nl * 3, 0.0), phi(T.nl);
+    for (int a = 0; a < T.nl; ++a) {
+      int ai[3] = {a % p1, (a / p1) % p1, a / (p1 * p1)};
+      double v = 1.0;
+      for (int k = 0; k < dim; ++k) v = v * lag1d(order, ai[k], T.r.xi[qi[k]]);
+      phi[a] = v;
+      for (int kd = 0; kd < dim; ++kd) {
+        double g = 1.0;
+        for (int k = 0; k < dim; ++k)
+          g = g * (k == kd ? dlag1d(order, ai[k], T.r.xi[qi[k]]) : lag1d(order, ai[k], T.r.xi[qi[k]]));
+        G[a * 3 + kd] = g * invh;
+      }
+    }
+    for (int a = 0; a < T.nl; ++a) {
+      T.Phi[(size_t)q * T.nl + a] = Wv * phi[a];
+      for (int b = 0; b < T.nl; ++b) {
+        double g = G[a * 3] * G[b * 3];
+        for (int kd = 1; kd < dim; ++kd) g = std::fma(G[a * 3 + kd], G[b * 3 + kd], g);
+        T.C[((size_t)q * T.nl + a) * T.nl + b] = Wv * g;
+      }
+    }
+  }
+  for (int q = 0; q < T.nq; ++q)
+    for (int ab = 0; ab < T.nl * T.nl; ++ab) T.Kbar[ab] = T.Kbar[ab] + T.C[(size_t)q * T.nl * T.nl + ab];
+  return T;
+}
+
+// ---------------------------------------------------------------- hierarchy
+struct Level {
+  long n = 0, M = 0, N = 0;
+  double h = 0;
+  std::vector<double> A;        // [slot][node][nc][nc]
+  std::vector<double> omega;    // optional per-node damping (size N)
+};
+
+struct Hier {
+  int dim, order, nc, n0, top, base, dmask;
+  int span;                     // stencil half width (= order)
+  int nslots;
+  int kkind = ORA_K_CONST;
+  double kconst = 1.0;
+  std::vector<double> kcell;    // top-level cells
+  int fkind = ORA_F_CONST;
+  double fconst = 1.0;
+  std::vector<double> fip;      // top-level cells x nq
+  std::vector<Level> lev;
+  std::vector<double> rhs;
+  std::vector<double> ainv;     // base-level inverse, row-major
+  long nbase = 0;
+  bool assembled = false;
+
+  // V-cycle state (multigrid.lisp:101-116)
+  std::vector<double*> sol, rhsv, res;
+  std::vector<int> rp;
+  std::vector<std::vector<double>> store;
+  int cur = 0;
+};
+
+inline void coords(const Hier& H, long M, long i, long c[3]) {
+  c[0] = i % M; c[1] = H.dim > 1 ? (i / M) % M : 0; c[2] = H.dim > 2 ? i / (M * M) : 0;
+}
+
+inline bool is_dirichlet(const Hier& H, long M, const long c[3]) {
+  for (int k = 0; k < H.dim; ++k) {
+    if (c[k] == 0 && (H.dmask >> (2 * k) & 1)) return true;
+    if (c[k] == M - 1 && (H.dmask >> (2 * k + 1) & 1)) return true;
+  }
+  return false;
+}
+
+inline int slot_of(const Hier& H, const long o[3]) {
+  int w = 2 * H.span + 1, s = 0, mul = 1;
+  for (int k = 0; k < H.dim; ++k) { s += (int)(o[k] + H.span) * mul; mul *= w; }
+  return s;
+}
+
+inline void slot_offset(const Hier& H, int s, long o[3]) {
+  int w = 2 * H.span + 1;
+  o[0] = o[1] = o[2] = 0;
+  for (int k = 0; k < H.dim; ++k) { o[k] = s % w - H.span; s /= w; }
+}
+
+long vec_len(const Hier& H, int l) { return H.lev[l].N * H.nc; }
+
+// coefficient at Gauss point q of cell c on level l (re-discretisation:
+// coarse levels evaluate the coefficient at their own integration points,
+// ellsys-fe.lisp:102-121, pde-problem.lisp:212-247)
+double k_at(const Hier& H, int l, const Tables& T, const long cc[3], int q) {
+  if (H.kkind == ORA_K_CONST) return H.kconst;
+  long nt = H.lev[H.top].n;
+  double r = std::ldexp(1.0, H.top - l);
+  int np = T.r.np;
+  int qi[3] = {q % np, (q / np) % np, q / (np * np)};
+  long f[3] = {0, 0, 0};
+  for (int k = 0; k < H.dim; ++k) f[k] = (long)std::floor(((double)cc[k] + T.r.xi[qi[k]]) * r);
+  long idx = f[0] + nt * (f[1] + nt * f[2]);
+  return H.kcell[idx];
+}
+
+int assemble_level(Hier& H, int l) {
+  Level& L = H.lev[l];
+  Tables T = make_tables(H.dim, H.order, L.h);
+  const int p = H.order, p1 = p + 1, nl = T.nl, nq = T.nq, nc = H.nc;
+  if (nc != 1) return -2;  // vector-valued assembly: elasticity path not in this oracle build
+  L.A.assign((size_t)H.nslots * L.N, 0.0);
+  const bool top = (l == H.top);
+  const bool cellconst = (H.kkind == ORA_K_CONST) || top;
+  if (top) H.rhs.assign(L.N, 0.0);
+  const long n = L.n, M = L.M;
+  const int center = [&] { long z[3] = {0, 0, 0}; return slot_of(H, z); }();
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < L.N; ++i) {
+    long ci[3];
+    coords(H, M, i, ci);
+    if (is_dirichlet(H, M, ci)) {
+      L.A[(size_t)center * L.N + i] = 1.0;
+      continue;
+    }
+    // adjacent cells per direction, ascending
+    // cells c with p*c <= i <= p*c + p, clipped to the grid
+    long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int k = 0; k < H.dim; ++k) {
+      lo[k] = ci[k] >= p ? (ci[k] - 1) / p : 0;
+      hi[k] = std::min(n - 1, ci[k] / p);
+    }
+    double acc_b = 0.0;
+    for (long cz = lo[2]; cz <= hi[2]; ++cz)
+      for (long cy = lo[1]; cy <= hi[1]; ++cy)
+        for (long cx = lo[0]; cx <= hi[0]; ++cx) {
+          long cc[3] = {cx, cy, cz};
+          long cidx = cx + n * (cy + n * cz);
+          int ai[3] = {0, 0, 0};
+          for (int k = 0; k < H.dim; ++k) ai[k] = (int)(ci[k] - p * cc[k]);
+          int a = ai[0] + p1 * (ai[1] + p1 * ai[2]);
+          double kc = 0.0;
+          double kq[27];
+          if (cellconst) kc = (H.kkind == ORA_K_CONST) ? H.kconst : H.kcell[cidx];
+          else
+            for (int q = 0; q < nq; ++q) kq[q] = k_at(H, l, T, cc, q);
+          for (int b = 0; b < nl; ++b) {
+            int bi[3] = {b % p1, (b / p1) % p1, b / (p1 * p1)};
+            long cj[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+            for (int k = 0; k < H.dim; ++k) { cj[k] = p * cc[k] + bi[k]; o[k] = cj[k] - ci[k]; }
+            if (is_dirichlet(H, M, cj)) continue;  // S*A*S: constrained column removed
+            double v;
+            if (cellconst) v = kc * T.Kbar[(size_t)a * nl + b];
+            else {
+              v = 0.0;
+              for (int q = 0; q < nq; ++q) v = std::fma(kq[q], T.C[((size_t)q * nl + a) * nl + b], v);
+            }
+            int s = slot_of(H, o);
+            double& dst = L.A[(size_t)s * L.N + i];
+            dst = dst + v;
+          }
+          if (top) {
+            double bl = 0.0;
+            for (int q = 0; q < nq; ++q) {
+              double f = (H.fkind == ORA_F_CONST) ? H.fconst : H.fip[(size_t)cidx * nq + q];
+              bl = std::fma(f, T.Phi[(size_t)q * nl + a], bl);
+            }
+            acc_b = acc_b + bl;
+          }
+        }
+    if (top) H.rhs[i] = acc_b;
+  }
+  return 0;
+}
+
+// dense LU with partial pivoting and explicit inverse of the base level
+// (replaces the sparse LDU of sparselu.lisp:61-216; both are exact solves)
+void build_coarse_inverse(Hier& H) {
+  Level& L = H.lev[H.base];
+  long n = L.N;  // nc == 1
+  H.nbase = n;
+  std::vector<double> A((size_t)n * n, 0.0);
+  for (long i = 0; i < n; ++i)
+    for (int s = 0; s < H.nslots; ++s) {
+      long o[3];
+      slot_offset(H, s, o);
+      long ci[3];
+      coords(H, L.M, i, ci);
+      long cj[3] = {ci[0] + o[0], ci[1] + o[1], ci[2] + o[2]};
+      bool in = true;
+      for (int k = 0; k < H.dim; ++k) if (cj[k] < 0 || cj[k] >= L.M) in = false;
+      if (!in) continue;
+      long j = cj[0] + L.M * (cj[1] + L.M * cj[2]);
+      A[(size_t)i * n + j] = L.A[(size_t)s * L.N + i];
+    }
+  std::vector<long> piv(n);
+  for (long k = 0; k < n; ++k) {
+    long pk = k;
+    double mx = std::fabs(A[(size_t)k * n + k]);
+    for (long i = k + 1; i < n; ++i) {
+      double v = std::fabs(A[(size_t)i * n + k]);
+      if (v > mx) { mx = v; pk = i; }
+    }
+    piv[k] = pk;
+    if (pk != k)
+      for (long j = 0; j < n; ++j) std::swap(A[(size_t)k * n + j], A[(size_t)pk * n + j]);
+    double d = A[(size_t)k * n + k];
+    for (long i = k + 1; i < n; ++i) A[(size_t)i * n + k] = A[(size_t)i * n + k] / d;
+    for (long i = k + 1; i < n; ++i) {
+      double lik = A[(size_t)i * n + k];
+      for (long j = k + 1; j < n; ++j) A[(size_t)i * n + j] = std::fma(-lik, A[(size_t)k * n + j], A[(size_t)i * n + j]);
+    }
+  }
+  H.ainv.assign((size_t)n * n, 0.0);
+  std::vector<double> b(n);
+  for (long col = 0; col < n; ++col) {
+    std::fill(b.begin(), b.end(), 0.0);
+    b[col] = 1.0;
+    for (long k = 0; k < n; ++k) if (piv[k] != k) std::swap(b[k], b[piv[k]]);
+    for (long k = 0; k < n; ++k)
+      for (long i = k + 1; i < n; ++i) b[i] = std::fma(-A[(size_t)i * n + k], b[k], b[i]);
+    for (long k = n - 1; k >= 0; --k) {
+      b[k] = b[k] / A[(size_t)k * n + k];
+      for (long i = 0; i < k; ++i) b[i] = std::fma(-A[(size_t)i * n + k], b[k], b[i]);
+    }
+    for (long i = 0; i < n; ++i) H.ainv[(size_t)i * n + col] = b[i];
+  }
+}
+
+// ---------------------------------------------------------------- kernels
+inline double row_sum(const Hier& H, const Level& L, long i, const double* x) {
+  long ci[3];
+  coords(H, L.M, i, ci);
+  double acc = 0.0;
+  for (int s = 0; s < H.nslots; ++s) {
+    long o[3];
+    slot_offset(H, s, o);
+    bool in = true;
+    long cj[3];
+    for (int k = 0; k < 3; ++k) {
+      cj[k] = ci[k] + o[k];
+      if (k < H.dim && (cj[k] < 0 || cj[k] >= L.M)) in = false;
+    }
+    if (!in) continue;
+    long j = cj[0] + L.M * (cj[1] + L.M * cj[2]);
+    acc = std::fma(L.A[(size_t)s * L.N + i], x[j], acc);
+  }
+  return acc;
+}
+
+// gemm! 1.0 A x 0.0 y (sparse-matrix.lisp:392-405)
+void matvec(const Hier& H, int l, const double* x, double* y) {
+  const Level& L = H.lev[l];
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < L.N; ++i) y[i] = row_sum(H, L, i, x);
+}
+
+// compute-residual r := b - A x (linit.lisp:73-80); b may alias r
+void residual(const Hier& H, int l, const double* x, const double* b, double* r) {
+  const Level& L = H.lev[l];
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < L.N; ++i) {
+    double s = row_sum(H, L, i, x);
+    r[i] = b[i] - s;
+  }
+}
+
+inline double diag(const Hier& H, const Level& L, long i) {
+  long z[3] = {0, 0, 0};
+  return L.A[(size_t)slot_of(H, z) * L.N + i];
+}
+
+// <jacobi> on a sparse matrix (linit.lisp:220-250): r_k := A_kk^-1 r_k
+// (gesv! overwrites the residual block), x_k += damp * r_k
+void jacobi(const Hier& H, int l, double damp, double* x, double* r) {
+  const Level& L = H.lev[l];
+  const double* w = L.omega.empty() ? nullptr : L.omega.data();
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < L.N; ++i) {
+    double t = r[i] / diag(H, L, i);
+    r[i] = t;
+    x[i] = std::fma(w ? w[i] : damp, t, x[i]);
+  }
+}
+
+int colour_of(const Hier& H, const long c[3]) {
+  int p1 = H.order + 1, col = 0, mul = 1;
+  for (int k = 0; k < H.dim; ++k) { col += (int)(c[k] % p1) * mul; mul *= p1; }
+  return col;
+}
+
+// <sor> on a sparse matrix (linit.lisp:288-323), rows ordered by colour
+// class (the :compare slot, linit.lisp:260-263,293-295).  Rows of one colour
+// do not couple, so the order inside a colour does not matter.
+void sor(const Hier& H, int l, double omega, double* x, const double* b, double* r) {
+  const Level& L = H.lev[l];
+  int ncol = 1;
+  for (int k = 0; k < H.dim; ++k) ncol *= H.order + 1;
+  const double* w = L.omega.empty() ? nullptr : L.omega.data();
+  for (int col = 0; col < ncol; ++col) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < L.N; ++i) {
+      long ci[3];
+      coords(H, L.M, i, ci);
+      if (colour_of(H, ci) != col) continue;
+      double s = row_sum(H, L, i, x);
+      double ri = b[i] - s;
+      double t = ri / diag(H, L, i);
+      r[i] = t;
+      x[i] = std::fma(w ? w[i] : omega, t, x[i]);
+    }
+  }
+}
+
+// 1D interpolation stencils (fetransfer.lisp:73-195 evaluated for uniform
+// Lagrange Q1/Q2): coarse node J <-> fine node 2J.
+int restrict_stencil1d(int order, long J, long* off, double* w) {
+  if (order == 1) { off[0] = -1; off[1] = 0; off[2] = 1; w[0] = 0.5; w[1] = 1.0; w[2] = 0.5; return 3; }
+  if (J % 2 == 0) {
+    long o[5] = {-3, -1, 0, 1, 3};
+    double ww[5] = {-0.125, 0.375, 1.0, 0.375, -0.125};
+    for (int k = 0; k < 5; ++k) { off[k] = o[k]; w[k] = ww[k]; }
+    return 5;
+  }
+  off[0] = -1; off[1] = 0; off[2] = 1; w[0] = 0.75; w[1] = 1.0; w[2] = 0.75;
+  return 3;
+}
+
+// coarse nodes contributing to fine node I (ascending J)
+int prolong_stencil1d(int order, long I, long* J, double* w) {
+  if (I % 2 == 0) { J[0] = I / 2; w[0] = 1.0; return 1; }
+  if (order == 1) { J[0] = (I - 1) / 2; J[1] = (I + 1) / 2; w[0] = 0.5; w[1] = 0.5; return 2; }
+  long c = I / 4;
+  double s = (double)(I - 4 * c) / 4.0;
+  J[0] = 2 * c; J[1] = 2 * c + 1; J[2] = 2 * c + 2;
+  w[0] = 2.0 * (s - 0.5) * (s - 1.0);
+  w[1] = 4.0 * s * (1.0 - s);
+  w[2] = 2.0 * s * (s - 0.5);
+  return 3;
+}
+
+// res_{l-1} := I^T res_l (multigrid.lisp:202-212, gemm! ... :tn) with the
+// constrained interpolation (constraints.lisp:58-72)
+void restrict_(const Hier& H, int lf, const double* rf, double* rc) {
+  const Level& F = H.lev[lf];
+  const Level& C = H.lev[lf - 1];
+#pragma omp parallel for schedule(static)
+  for (long J = 0; J < C.N; ++J) {
+    long cJ[3];
+    coords(H, C.M, J, cJ);
+    if (is_dirichlet(H, C.M, cJ)) { rc[J] = 0.0; continue; }
+    long off[3][5] = {{0}, {0}, {0}};
+    double w[3][5] = {{1.0}, {1.0}, {1.0}};
+    int cnt[3] = {1, 1, 1};
+    for (int k = 0; k < H.dim; ++k) cnt[k] = restrict_stencil1d(H.order, cJ[k], off[k], w[k]);
+    double acc = 0.0;
+    for (int z = 0; z < cnt[2]; ++z)
+      for (int y = 0; y < cnt[1]; ++y)
+        for (int x = 0; x < cnt[0]; ++x) {
+          long fi[3] = {2 * cJ[0] + off[0][x], 2 * cJ[1] + off[1][y], 2 * cJ[2] + off[2][z]};
+          bool in = true;
+          for (int k = 0; k < H.dim; ++k) if (fi[k] < 0 || fi[k] >= F.M) in = false;
+          if (!in) continue;
+          if (is_dirichlet(H, F.M, fi)) continue;
+          double ww = w[0][x];
+          if (H.dim > 1) ww = ww * w[1][y];
+          if (H.dim > 2) ww = ww * w[2][z];
+          long i = fi[0] + F.M * (fi[1] + F.M * fi[2]);
+          acc = std::fma(ww, rf[i], acc);
+        }
+    rc[J] = acc;
+  }
+}
+
+// sol_{l+1} += I sol_l (multigrid.lisp:237-239, gemm! ... :nn)
+void prolongate(const Hier& H, int lc, const double* xc, double* xf, bool constrained) {
+  const Level& C = H.lev[lc];
+  const Level& F = H.lev[lc + 1];
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < F.N; ++i) {
+    long fi[3];
+    coords(H, F.M, i, fi);
+    if (constrained && is_dirichlet(H, F.M, fi)) continue;
+    long J[3][3] = {{0}, {0}, {0}};
+    double w[3][3] = {{1.0}, {1.0}, {1.0}};
+    int cnt[3] = {1, 1, 1};
+    for (int k = 0; k < H.dim; ++k) cnt[k] = prolong_stencil1d(H.order, fi[k], J[k], w[k]);
+    double acc = 0.0;
+    for (int z = 0; z < cnt[2]; ++z)
+      for (int y = 0; y < cnt[1]; ++y)
+        for (int x = 0; x < cnt[0]; ++x) {
+          long cj[3] = {J[0][x], J[1][y], J[2][z]};
+          if (constrained && is_dirichlet(H, C.M, cj)) continue;
+          double ww = w[0][x];
+          if (H.dim > 1) ww = ww * w[1][y];
+          if (H.dim > 2) ww = ww * w[2][z];
+          long j = cj[0] + C.M * (cj[1] + C.M * cj[2]);
+          acc = std::fma(ww, xc[j], acc);
+        }
+    xf[i] = xf[i] + acc;
+  }
+}
+
+// <lu> coarse-grid iterator (linit.lisp:137-162): r := A^-1 r; x += damp r
+void coarse_solve(const Hier& H, double damp, double* x, double* r) {
+  long n = H.nbase;
+  std::vector<double> t(n);
+  for (long i = 0; i < n; ++i) {
+    double acc = 0.0;
+    for (long j = 0; j < n; ++j) acc = std::fma(H.ainv[(size_t)i * n + j], r[j], acc);
+    t[i] = acc;
+  }
+  for (long i = 0; i < n; ++i) { r[i] = t[i]; x[i] = std::fma(damp, t[i], x[i]); }
+}
+
+// ---------------------------------------------------------------- multigrid
+// One smoother step (the base iterator) and its flags (linit.lisp:220-323):
+// <jacobi> residual-before t, <sor> residual-before nil; both residual-after nil.
+bool smoother_residual_before(const ora_solve_cfg& c) { return c.smoother == ORA_JACOBI; }
+
+void smoother_step(Hier& H, const ora_solve_cfg& c, int l, double* x, double* b, double* r) {
+  if (c.smoother == ORA_JACOBI) jacobi(H, l, c.damp, x, r);
+  else sor(H, l, c.damp, x, b, r);
+}
+
+// product-iterator (linit.lisp:94-120): after every step the residual is
+// recomputed when residual-before and not residual-after
+void smoother_product(Hier& H, const ora_solve_cfg& c, int l, int steps, double* x, double* b,
+                      double* r) {
+  if (steps == 1) { smoother_step(H, c, l, x, b, r); return; }
+  for (int s = 0; s < steps; ++s) {
+    smoother_step(H, c, l, x, b, r);
+    if (smoother_residual_before(c)) residual(H, l, x, b, r);
+  }
+}
+
+void ensure_mg_residual(Hier& H) {  // multigrid.lisp:173-177
+  int l = H.cur;
+  if (!H.rp[l]) {
+    residual(H, l, H.sol[l], H.rhsv[l], H.res[l]);
+    H.rp[l] = 1;
+  }
+}
+
+void smooth(Hier& H, const ora_solve_cfg& c, int steps) {  // multigrid.lisp:179-189
+  if (steps <= 0) return;
+  if (smoother_residual_before(c)) ensure_mg_residual(H);
+  int l = H.cur;
+  smoother_product(H, c, l, steps, H.sol[l], H.rhsv[l], H.res[l]);
+  H.rp[l] = 0;
+}
+
+void mg_restrict(Hier& H) {  // multigrid.lisp:202-224
+  int l = H.cur;
+  ensure_mg_residual(H);
+  restrict_(H, l, H.res[l], H.res[l - 1]);
+  H.cur = l - 1;
+  H.rp[l - 1] = 0;
+  long n = vec_len(H, l - 1);
+  std::fill(H.sol[l - 1], H.sol[l - 1] + n, 0.0);
+  std::copy(H.res[l - 1], H.res[l - 1] + n, H.rhsv[l - 1]);
+  H.rp[l - 1] = 1;
+}
+
+void mg_prolongate(Hier& H) {  // multigrid.lisp:237-252
+  int l = H.cur;
+  prolongate(H, l, H.sol[l], H.sol[l + 1], true);
+  H.cur = l + 1;
+  H.rp[l + 1] = 0;
+}
+
+void lmgc(Hier& H, const ora_solve_cfg& c) {  // multigrid.lisp:254-288
+  int l = H.cur;
+  if (l == H.base) {
+    coarse_solve(H, c.coarse_damp, H.sol[l], H.res[l]);
+    H.rp[l] = 0;
+    return;
+  }
+  if (c.combination == 0) {
+    smooth(H, c, c.pre_steps);
+    mg_restrict(H);
+  } else {  // :additive -- smoothing on level l after the restriction
+    mg_restrict(H);
+    H.cur += 1;
+    smooth(H, c, c.pre_steps);
+    H.cur -= 1;
+  }
+  int g = c.gamma == 0 ? 0 : (H.cur == H.base ? 1 : c.gamma);
+  for (int i = g; i >= 1; --i) {
+    lmgc(H, c);
+    if (i != 1) ensure_mg_residual(H);
+  }
+  if (c.combination == 0) {
+    mg_prolongate(H);
+    smooth(H, c, c.post_steps);
+  } else {
+    H.cur += 1;
+    smooth(H, c, c.post_steps);
+    H.cur -= 1;
+    mg_prolongate(H);
+  }
+}
+
+// the multigrid iterator's iterate function (multigrid.lisp:366-386): the
+// top-level sol/rhs/res are the caller's vectors, with no copy
+void mg_iterate(Hier& H, const ora_solve_cfg& c, double* x, double* b, double* r) {
+  int top = H.top;
+  H.sol[top] = x; H.rhsv[top] = b; H.res[top] = r;
+  H.rp[top] = 1;
+  H.cur = top;
+  lmgc(H, c);
+}
+
+void ensure_state(Hier& H) {
+  int nl = H.top + 1;
+  if ((int)H.sol.size() == nl) return;
+  H.sol.assign(nl, nullptr); H.rhsv.assign(nl, nullptr); H.res.assign(nl, nullptr);
+  H.rp.assign(nl, 0);
+  H.store.assign(3 * nl, {});
+  for (int l = H.base; l < H.top; ++l) {
+    long n = vec_len(H, l);
+    H.store[3 * l].assign(n, 0.0); H.store[3 * l + 1].assign(n, 0.0); H.store[3 * l + 2].assign(n, 0.0);
+    H.sol[l] = H.store[3 * l].data(); H.rhsv[l] = H.store[3 * l + 1].data(); H.res[l] = H.store[3 * l + 2].data();
+  }
+}
+
+}  // namespace
+
+// ==================================================================== C API
+extern "C" {
+
+void* ora_create(int dim, int order, int ncomp, int n0, int top_level, int base_level,
+                 int dirichlet_mask) {
+  if (dim < 1 || dim > 3 || order < 1 || order > 2 || ncomp < 1 || n0 < 1 || base_level < 0 ||
+      base_level > top_level || top_level > 12)
+    return nullptr;
+  Hier* H = new Hier();
+  H->dim = dim; H->order = order; H->nc = ncomp; H->n0 = n0;
+  H->top = top_level; H->base = base_level; H->dmask = dirichlet_mask;
+  H->span = order;
+  H->nslots = 1;
+  for (int k = 0; k < dim; ++k) H->nslots *= 2 * order + 1;
+  H->lev.resize(top_level + 1);
+  for (int l = 0; l <= top_level; ++l) {
+    Level& L = H->lev[l];
+    L.n = (long)n0 << l;
+    L.M = order * L.n + 1;
+    L.N = 1;
+    for (int k = 0; k < dim; ++k) L.N *= L.M;
+    L.h = 1.0 / (double)L.n;
+  }
+  return H;
+}
+
+void ora_destroy(void* h) { delete (Hier*)h; }
+
+int ora_set_coefficient(void* h, int kind, const double* vals, long n) {
+  Hier& H = *(Hier*)h;
+  long nt = H.lev[H.top].n, ncell = 1;
+  for (int k = 0; k < H.dim; ++k) ncell *= nt;
+  Tables T = make_tables(H.dim, H.order, 1.0);
+  switch (kind) {
+    case ORA_K_CONST: if (n != 1) return -1; H.kkind = kind; H.kconst = vals[0]; break;
+    case ORA_K_CELL: if (n != ncell) return -1; H.kkind = kind; H.kcell.assign(vals, vals + n); break;
+    case ORA_F_CONST: if (n != 1) return -1; H.fkind = kind; H.fconst = vals[0]; break;
+    case ORA_F_IP: if (n != ncell * T.nq) return -1; H.fkind = kind; H.fip.assign(vals, vals + n); break;
+    default: return -1;
+  }
+  H.assembled = false;
+  return 0;
+}
+
+int ora_assemble(void* h) {
+  Hier& H = *(Hier*)h;
+  for (int l = H.top; l >= H.base; --l) {
+    int rc = assemble_level(H, l);
+    if (rc) return rc;
+  }
+  build_coarse_inverse(H);
+  H.assembled = true;
+  ensure_state(H);
+  return 0;
+}
+
+int ora_set_node_damping(void* h, int level, const double* w, long n) {
+  Hier& H = *(Hier*)h;
+  if (level < 0 || level > H.top || n != H.lev[level].N) return -1;
+  if (w) H.lev[level].omega.assign(w, w + n); else H.lev[level].omega.clear();
+  return 0;
+}
+
+long ora_nnodes(void* h, int level) { return ((Hier*)h)->lev[level].N; }
+int ora_nslots(void* h) { return ((Hier*)h)->nslots; }
+
+int ora_get_matrix(void* h, int level, double* out) {
+  Hier& H = *(Hier*)h;
+  if (!H.assembled || level < H.base || level > H.top) return -1;
+  std::copy(H.lev[level].A.begin(), H.lev[level].A.end(), out);
+  return 0;
+}
+
+int ora_get_rhs(void* h, double* out) {
+  Hier& H = *(Hier*)h;
+  if (!H.assembled) return -1;
+  std::copy(H.rhs.begin(), H.rhs.end(), out);
+  return 0;
+}
+
+int ora_get_coarse_inverse(void* h, double* out) {
+  Hier& H = *(Hier*)h;
+  if (!H.assembled) return -1;
+  std::copy(H.ainv.begin(), H.ainv.end(), out);
+  return 0;
+}
+
+int ora_matvec(void* h, int level, const double* x, double* y) { matvec(*(Hier*)h, level, x, y); return 0; }
+int ora_residual(void* h, int level, const double* x, const double* b, double* r) {
+  residual(*(Hier*)h, level, x, b, r);
+  return 0;
+}
+int ora_restrict(void* h, int fine_level, const double* rf, double* rc) {
+  restrict_(*(Hier*)h, fine_level, rf, rc);
+  return 0;
+}
+int ora_prolongate(void* h, int coarse_level, const double* xc, double* xf, int constrained) {
+  prolongate(*(Hier*)h, coarse_level, xc, xf, constrained != 0);
+  return 0;
+}
+// projection (injection) of fine nodal values onto the coarse nodes
+int ora_inject(void* h, int coarse_level, const double* xf, double* xc) {
+  Hier& H = *(Hier*)h;
+  const Level& C = H.lev[coarse_level];
+  const Level& F = H.lev[coarse_level + 1];
+  for (long J = 0; J < C.N; ++J) {
+    long c[3];
+    coords(H, C.M, J, c);
+    xc[J] = xf[2 * c[0] + F.M * (2 * c[1] + F.M * 2 * c[2])];
+  }
+  return 0;
+}
+int ora_jacobi(void* h, int level, double damp, double* x, double* r) {
+  jacobi(*(Hier*)h, level, damp, x, r);
+  return 0;
+}
+int ora_sor(void* h, int level, double omega, double* x, const double* b, double* r) {
+  sor(*(Hier*)h, level, omega, x, b, r);
+  return 0;
+}
+int ora_coarse_solve(void* h, double damp, double* x, double* r) {
+  coarse_solve(*(Hier*)h, damp, x, r);
+  return 0;
+}
+double ora_dot(const double* x, const double* y, long n) { return dr_dot(x, y, n, false); }
+double ora_dot_par(const double* x, const double* y, long n) { return dr_dot(x, y, n, true); }
+
+int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* r) {
+  Hier& H = *(Hier*)h;
+  if (!H.assembled) return -1;
+  mg_iterate(H, *cfg, x, b, r);
+  return 0;
+}
+
+// <linear-solver> loop (iterate.lisp:239-250, solve.lisp:139-155,
+// linsolve.lisp:58-73) around <cg> (krylow.lisp:72-132) or the bare
+// multigrid iterator
+int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hist_len, int* nsteps) {
+  Hier& H = *(Hier*)h;
+  if (!H.assembled) return -1;
+  const ora_solve_cfg& c = *cfg;
+  const int top = H.top;
+  const long n = vec_len(H, top);
+  std::vector<double> r(n, 0.0), p(n, 0.0), a(n, 0.0), w(n, 0.0), w2(n, 0.0), q(n, 0.0);
+  std::vector<double> bcopy(H.rhs);  // the problem's rhs is never written
+  bool rp = false, initialized = false;
+  double defnorm = 0.0, initial = -1.0, alpha = 0.0;
+  const bool par = true;
+  auto precond = [&](double* sol, double* rr) {
+    // (copy! r w) then (iterate sol w w) -- or a separate residual vector
+    std::copy(rr, rr + n, w.begin());
+    if (c.compat_alias) mg_iterate(H, c, sol, w.data(), w.data());
+    else {
+      std::copy(rr, rr + n, w2.begin());
+      mg_iterate(H, c, sol, w.data(), w2.data());
+    }
+  };
+  for (int step = 0;; ++step) {
+    if (!rp) { residual(H, top, x, bcopy.data(), r.data()); rp = true; }
+    defnorm = std::sqrt(dr_dot(r.data(), r.data(), n, par));
+    if (initial < 0) initial = defnorm;
+    double reduction = (initial == 0.0) ? 0.0 : defnorm / initial;
+    if (step < hist_len) hist[step] = defnorm;
+    *nsteps = step;
+    if ((c.rtol > 0 && reduction < c.rtol) || (c.atol > 0 && defnorm < c.atol)) return 0;
+    if (step > c.maxsteps) return 1;
+    if (c.method == ORA_METHOD_MG) {
+      mg_iterate(H, c, x, bcopy.data(), r.data());
+      rp = false;
+      continue;
+    }
+    // <cg>
+    if (!initialized) {  // restart (krylow.lisp:88-96)
+      if (c.method == ORA_METHOD_CG_MG) precond(p.data(), r.data());
+      else std::copy(r.begin(), r.end(), p.begin());
+      alpha = dr_dot(p.data(), r.data(), n, par);
+      initialized = true;
+    }
+    if (alpha != 0.0) {  // krylow.lisp:106-127
+      matvec(H, top, p.data(), a.data());
+      double beta = dr_dot(a.data(), p.data(), n, par);
+      double lam = alpha / beta;
+      for (long i = 0; i < n; ++i) x[i] = std::fma(lam, p[i], x[i]);
+      for (long i = 0; i < n; ++i) r[i] = std::fma(-lam, a[i], r[i]);
+      if (c.method == ORA_METHOD_CG_MG) {
+        std::fill(q.begin(), q.end(), 0.0);
+        precond(q.data(), r.data());
+      } else {
+        std::copy(r.begin(), r.end(), q.begin());
+      }
+      double new_alpha = dr_dot(q.data(), r.data(), n, par);
+      double s = new_alpha / alpha;
+      for (long i = 0; i < n; ++i) p[i] = s * p[i];
+      for (long i = 0; i < n; ++i) p[i] = p[i] + q[i];
+      alpha = new_alpha;
+    }
+    rp = true;
+  }
+}
+
+int ora_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,273 @@
+"""ctypes wrapper of the CPU oracle (oracle/libfmg_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker of the GPU path.  Only tests/,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import
+this module; the product package never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libfmg_oracle.so")
+
+K_CONST, K_CELL, F_CONST, F_IP, LAMBDA_MU_CELL = 0, 1, 2, 3, 4
+JACOBI, SOR = 0, 1
+METHOD_MG, METHOD_CG_MG, METHOD_CG = 0, 1, 2
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class SolveCfg(ctypes.Structure):
+    _fields_ = [
+        ("method", ctypes.c_int),
+        ("smoother", ctypes.c_int),
+        ("damp", ctypes.c_double),
+        ("pre_steps", ctypes.c_int),
+        ("post_steps", ctypes.c_int),
+        ("gamma", ctypes.c_int),
+        ("compat_alias", ctypes.c_int),
+        ("coarse_damp", ctypes.c_double),
+        ("rtol", ctypes.c_double),
+        ("atol", ctypes.c_double),
+        ("maxsteps", ctypes.c_int),
+        ("combination", ctypes.c_int),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.ora_create.restype = ctypes.c_void_p
+        L.ora_create.argtypes = [ctypes.c_int] * 7
+        L.ora_destroy.argtypes = [ctypes.c_void_p]
+        L.ora_set_coefficient.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_long]
+        L.ora_assemble.argtypes = [ctypes.c_void_p]
+        L.ora_set_node_damping.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_long]
+        L.ora_nnodes.restype = ctypes.c_long
+        L.ora_nnodes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ora_nslots.argtypes = [ctypes.c_void_p]
+        for name in ("ora_get_matrix",):
+            getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.ora_get_rhs.argtypes = [ctypes.c_void_p, _dp]
+        L.ora_get_coarse_inverse.argtypes = [ctypes.c_void_p, _dp]
+        L.ora_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.ora_residual.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+        L.ora_restrict.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.ora_prolongate.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.ora_inject.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.ora_jacobi.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp]
+        L.ora_sor.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.ora_coarse_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp, _dp]
+        L.ora_dot.restype = ctypes.c_double
+        L.ora_dot.argtypes = [_dp, _dp, ctypes.c_long]
+        L.ora_dot_par.restype = ctypes.c_double
+        L.ora_dot_par.argtypes = [_dp, _dp, ctypes.c_long]
+        L.ora_vcycle.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveCfg), _dp, _dp, _dp]
+        L.ora_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveCfg), _dp, _dp, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_int)]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+@dataclass
+class SolveResult:
+    x: np.ndarray
+    history: np.ndarray
+    steps: int
+    status: int
+
+    @property
+    def reduction(self) -> float:
+        return float(self.history[-1] / self.history[0]) if self.history[0] != 0 else 0.0
+
+    @property
+    def convergence_rate(self) -> float:
+        """reduction^(1/steps) as in solve.lisp:157-164."""
+        return self.reduction ** (1.0 / self.steps) if self.steps > 0 else float("nan")
+
+
+MULTIPLICATIVE, ADDITIVE = 0, 1
+
+
+def solve_cfg(method=METHOD_CG_MG, smoother=JACOBI, damp=0.6, pre=1, post=1, gamma=1,
+              compat=True, coarse_damp=1.0, rtol=1e-10, atol=0.0, maxsteps=200,
+              combination=MULTIPLICATIVE) -> SolveCfg:
+    return SolveCfg(method, smoother, damp, pre, post, gamma, 1 if compat else 0, coarse_damp,
+                    rtol, atol, maxsteps, combination)
+
+
+class Oracle:
+    """A structured level hierarchy of Femlisp's uniformly refined n-cube
+    (meshgen.lisp:180-183) with Lagrange Q1/Q2 (lagrange.lisp:176-202)."""
+
+    def __init__(self, dim, order, level, base_level=0, ncomp=1, n0=1, dirichlet_mask=None):
+        self.dim, self.order, self.top, self.base = dim, order, level, base_level
+        if dirichlet_mask is None:
+            dirichlet_mask = (1 << (2 * dim)) - 1
+        self.h = lib().ora_create(dim, order, ncomp, n0, level, base_level, dirichlet_mask)
+        if not self.h:
+            raise ValueError("invalid oracle hierarchy")
+        self.n_cells = n0 << level
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ora_destroy(self.h)
+            self.h = None
+
+    def set_coefficient(self, kind, vals):
+        v = np.ascontiguousarray(np.atleast_1d(np.asarray(vals, dtype=np.float64)).ravel())
+        rc = lib().ora_set_coefficient(self.h, kind, _p(v), v.size)
+        if rc:
+            raise ValueError(f"ora_set_coefficient rc={rc}")
+
+    def assemble(self):
+        rc = lib().ora_assemble(self.h)
+        if rc:
+            raise RuntimeError(f"ora_assemble rc={rc}")
+        return self
+
+    def nnodes(self, level=None):
+        return lib().ora_nnodes(self.h, self.top if level is None else level)
+
+    @property
+    def nslots(self):
+        return lib().ora_nslots(self.h)
+
+    def matrix(self, level=None):
+        level = self.top if level is None else level
+        out = np.zeros(self.nslots * self.nnodes(level))
+        assert lib().ora_get_matrix(self.h, level, _p(out)) == 0
+        return out.reshape(self.nslots, -1)
+
+    def rhs(self):
+        out = np.zeros(self.nnodes())
+        assert lib().ora_get_rhs(self.h, _p(out)) == 0
+        return out
+
+    def coarse_inverse(self):
+        n = self.nnodes(self.base)
+        out = np.zeros(n * n)
+        assert lib().ora_get_coarse_inverse(self.h, _p(out)) == 0
+        return out.reshape(n, n)
+
+    def set_node_damping(self, level, w):
+        if w is None:
+            lib().ora_set_node_damping(self.h, level, None, self.nnodes(level))
+            return
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        assert lib().ora_set_node_damping(self.h, level, _p(w), w.size) == 0
+
+    def matvec(self, x, level=None):
+        level = self.top if level is None else level
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        lib().ora_matvec(self.h, level, _p(x), _p(y))
+        return y
+
+    def residual(self, x, b, level=None):
+        level = self.top if level is None else level
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        r = np.zeros_like(x)
+        lib().ora_residual(self.h, level, _p(x), _p(b), _p(r))
+        return r
+
+    def restrict(self, rf, fine_level):
+        rf = np.ascontiguousarray(rf, dtype=np.float64)
+        rc = np.zeros(self.nnodes(fine_level - 1))
+        lib().ora_restrict(self.h, fine_level, _p(rf), _p(rc))
+        return rc
+
+    def prolongate(self, xc, xf, coarse_level, constrained=True):
+        xc = np.ascontiguousarray(xc, dtype=np.float64)
+        xf = np.array(xf, dtype=np.float64, copy=True)
+        lib().ora_prolongate(self.h, coarse_level, _p(xc), _p(xf), 1 if constrained else 0)
+        return xf
+
+    def inject(self, xf, coarse_level):
+        xf = np.ascontiguousarray(xf, dtype=np.float64)
+        xc = np.zeros(self.nnodes(coarse_level))
+        lib().ora_inject(self.h, coarse_level, _p(xf), _p(xc))
+        return xc
+
+    def jacobi(self, x, r, damp, level=None):
+        level = self.top if level is None else level
+        x = np.array(x, dtype=np.float64, copy=True)
+        r = np.array(r, dtype=np.float64, copy=True)
+        lib().ora_jacobi(self.h, level, damp, _p(x), _p(r))
+        return x, r
+
+    def sor(self, x, b, r, omega, level=None):
+        level = self.top if level is None else level
+        x = np.array(x, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        r = np.array(r, dtype=np.float64, copy=True)
+        lib().ora_sor(self.h, level, omega, _p(x), _p(b), _p(r))
+        return x, r
+
+    def coarse_solve(self, x, r, damp=1.0):
+        x = np.array(x, dtype=np.float64, copy=True)
+        r = np.array(r, dtype=np.float64, copy=True)
+        lib().ora_coarse_solve(self.h, damp, _p(x), _p(r))
+        return x, r
+
+    def vcycle(self, cfg: SolveCfg, x, b, r=None):
+        """One multigrid iterator application; r=None aliases r to b."""
+        x = np.array(x, dtype=np.float64, copy=True)
+        b = np.array(b, dtype=np.float64, copy=True)
+        if r is None:
+            lib().ora_vcycle(self.h, ctypes.byref(cfg), _p(x), _p(b), _p(b))
+            return x, b, b
+        r = np.array(r, dtype=np.float64, copy=True)
+        lib().ora_vcycle(self.h, ctypes.byref(cfg), _p(x), _p(b), _p(r))
+        return x, b, r
+
+    def solve(self, cfg: SolveCfg, x0=None) -> SolveResult:
+        n = self.nnodes()
+        x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        hist = np.zeros(cfg.maxsteps + 2)
+        steps = ctypes.c_int(0)
+        st = lib().ora_solve(self.h, ctypes.byref(cfg), _p(x), _p(hist), hist.size,
+                             ctypes.byref(steps))
+        if st < 0:
+            raise RuntimeError(f"ora_solve rc={st}")
+        return SolveResult(x, hist[: steps.value + 1].copy(), steps.value, st)
+
+
+def dot(x, y) -> float:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    return lib().ora_dot(_p(x), _p(y), x.size)
+
+
+def dot_par(x, y) -> float:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    return lib().ora_dot_par(_p(x), _p(y), x.size)
+
+
+def num_threads() -> int:
+    return lib().ora_num_threads()

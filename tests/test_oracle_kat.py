@@ -1,0 +1,125 @@
+"""The oracle against the reference's own known answers.
+
+Femlisp ships no golden vectors; its numerics are pinned by these asserts:
+  * mg-cdr.lisp:85-87       V-cycle convergence rate "should be 0.39407..."
+  * ellsys-fe.lisp:249-256  1D Q1 level-2 nodal value at x=1/2 is exactly 0.125
+  * sparseas.lisp:401-448   interpolation reproduces quadratics, P*I = Id (Q2)
+  * fetransfer.lisp:331-340 local imatrix entry counts (28 for 2-comp Q2, 2 for Q1)
+  * mg-cdr.lisp:100-109     convergence-rate bounds (2D Q1 Gauss-Seidel < 0.18)
+"""
+import numpy as np
+import pytest
+
+
+def test_v_cycle_convergence_rate_1d(oracle_mod):
+    # (test-v-cycle-convergence 1 1 3 :base-level 2 :steps 10 :cr-max 0.3941
+    #   :smoother (make-instance '<jacobi> :damp 0.5))   mg-cdr.lisp:85-87
+    O = oracle_mod
+    o = O.Oracle(1, 1, 3, base_level=2).assemble()
+    cfg = O.solve_cfg(method=O.METHOD_MG, smoother=O.JACOBI, damp=0.5, pre=1, post=0,
+                      rtol=0.0, atol=1e-12, maxsteps=10)
+    r = o.solve(cfg)
+    assert r.steps == 11
+    assert r.convergence_rate < 0.3941
+    assert abs(r.convergence_rate - 0.39407) < 1e-5
+
+
+def test_exact_nodal_value_1d(oracle_mod):
+    # ellsys-fe-tests: (fe-value (gesv matrix rhs) #(0.5)) == 0.125 exactly
+    O = oracle_mod
+    o = O.Oracle(1, 1, 2, base_level=2).assemble()  # top == base: one exact LU solve
+    r = o.solve(O.solve_cfg(method=O.METHOD_MG, rtol=1e-14, maxsteps=3))
+    assert r.x[2] == 0.125
+    # and by CG with an exact-enough preconditioned iteration
+    o2 = O.Oracle(1, 1, 2, base_level=0).assemble()
+    r2 = o2.solve(O.solve_cfg(method=O.METHOD_CG_MG, compat=False, rtol=1e-15, maxsteps=50))
+    assert abs(r2.x[2] - 0.125) < 1e-15
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_projection_times_interpolation_is_identity(oracle_mod, order):
+    O = oracle_mod
+    for dim in (1, 2):
+        o = O.Oracle(dim, order, 2, base_level=0, dirichlet_mask=0).assemble()
+        nc, nf = o.nnodes(1), o.nnodes(2)
+        for j in range(nc):
+            e = np.zeros(nc)
+            e[j] = 1.0
+            xf = o.prolongate(e, np.zeros(nf), coarse_level=1, constrained=False)
+            assert np.array_equal(o.inject(xf, coarse_level=1), e)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_interpolation_reproduces_quadratics(oracle_mod, dim):
+    O = oracle_mod
+    o = O.Oracle(dim, 2, 2, base_level=0, dirichlet_mask=0).assemble()
+
+    def nodal(level):
+        M = 2 * (1 << level) + 1
+        g = np.linspace(0.0, 1.0, M)
+        axes = np.meshgrid(*([g] * dim), indexing="ij")[::-1]  # x fastest
+        x = axes[0]
+        f = x * (1.0 - x)
+        for a in axes[1:]:
+            f = f + 0.5 * a * a
+        return f.ravel()
+
+    zf = o.prolongate(nodal(1), np.zeros(o.nnodes(2)), coarse_level=1, constrained=False)
+    assert np.max(np.abs(zf - nodal(2))) < 1e-10
+
+
+def _local_imatrix_blocks(O, order):
+    """Nonzero (fine interior DoF, coarse subcell) blocks of the 1D local
+    interpolation matrix of one refined interval."""
+    o = O.Oracle(1, order, 1, base_level=0, dirichlet_mask=0).assemble()
+    nc, nf = o.nnodes(0), o.nnodes(1)
+    cols = []
+    for j in range(nc):
+        e = np.zeros(nc)
+        e[j] = 1.0
+        cols.append(o.prolongate(e, np.zeros(nf), coarse_level=0, constrained=False))
+    I = np.array(cols).T                      # nf x nc
+    fine_inner = range(1, nf - 1)             # DoFs of the inner children
+    blocks = sum(1 for i in fine_inner for j in range(nc) if abs(I[i, j]) > 1e-10)
+    return blocks
+
+
+def test_local_imatrix_entry_counts(oracle_mod):
+    O = oracle_mod
+    assert _local_imatrix_blocks(O, 1) == 2          # (fe 1): 2 blocks
+    ncomp = 2
+    assert _local_imatrix_blocks(O, 2) * ncomp * ncomp == 28   # (fe 2 2): 28 entries
+
+
+def test_gauss_seidel_rate_bound_2d(oracle_mod):
+    # (test-v-cycle-convergence 2 1 3 :smoother *gauss-seidel* :cr-max 0.18)
+    O = oracle_mod
+    o = O.Oracle(2, 1, 3, base_level=1).assemble()
+    cfg = O.solve_cfg(method=O.METHOD_MG, smoother=O.SOR, damp=1.0, pre=1, post=0,
+                      rtol=0.0, atol=1e-12, maxsteps=20)
+    r = o.solve(cfg)
+    assert r.convergence_rate < 0.18
+
+
+def test_additive_alias_is_harmless(oracle_mod):
+    # Femlisp preconditions <cg> with the additive cycle and no post-smoothing
+    # (multigrid-demos.lisp:208-214, model-problem.lisp:134-141): the
+    # rhs/residual alias of krylow.lisp:120 is never read after it is written.
+    O = oracle_mod
+    o = O.Oracle(2, 1, 5, base_level=1).assemble()
+    h = []
+    for compat in (True, False):
+        cfg = O.solve_cfg(method=O.METHOD_CG_MG, damp=1.0, pre=1, post=0,
+                          combination=O.ADDITIVE, compat=compat, rtol=1e-10)
+        h.append(o.solve(cfg).history)
+    assert np.array_equal(h[0], h[1])
+
+
+def test_dot_chunked_equals_parallel(oracle_mod):
+    O = oracle_mod
+    rng = np.random.default_rng(1)
+    for n in (1, 7, 4096, 4097, 100_000, 1_234_567):
+        x, y = rng.standard_normal(n), rng.standard_normal(n)
+        d = O.dot(x, y)
+        assert d == O.dot_par(x, y)
+        assert abs(d - float(np.dot(x, y))) <= 1e-12 * np.sqrt(n) * np.linalg.norm(x) * np.linalg.norm(y)
