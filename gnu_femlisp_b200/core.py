@@ -1,0 +1,216 @@
+"""Device handles: context, level hierarchy (grid) and level vectors.
+
+Thin, checked wrappers of the C-ABI: every non-zero status becomes an
+:class:`FmgError` carrying the library's message.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+from ._capi import FmgError
+
+
+class Context:
+    """One CUDA device and the stream all work is queued on
+    (``fmg_init``)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = C.load()
+        h = ctypes.c_void_p()
+        rc = self._lib.fmg_init(device, ctypes.byref(h))
+        if rc != C.FMG_OK:
+            raise FmgError(rc, f"fmg_init(device={device}) failed (no CUDA device?)")
+        self.h = h
+        self.device = device
+
+    def check(self, rc: int, what: str = ""):
+        if rc != C.FMG_OK:
+            buf = ctypes.create_string_buffer(512)
+            self._lib.fmg_last_error(self.h, buf, 512)
+            raise FmgError(rc, f"{what}: {buf.value.decode(errors='replace')}")
+
+    def synchronize(self):
+        self.check(self._lib.fmg_synchronize(self.h), "synchronize")
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self.check(self._lib.fmg_get_stream(self.h, ctypes.byref(s)), "get_stream")
+        return s.value or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fmg_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Grid:
+    """A level hierarchy of the uniformly refined unit n-cube with a Lagrange
+    Q1/Q2 space (``fmg_grid_create``); levels base_level..level."""
+
+    def __init__(self, ctx: Context, dim: int, order: int, level: int, base_level: int = 0,
+                 n0: int = 1, ncomp: int = 1, dirichlet_mask: int | None = None):
+        self.ctx, self.dim, self.order, self.top, self.base = ctx, dim, order, level, base_level
+        if dirichlet_mask is None:
+            dirichlet_mask = (1 << (2 * dim)) - 1
+        h = ctypes.c_void_p()
+        ctx.check(ctx._lib.fmg_grid_create(ctx.h, dim, order, ncomp, n0, level, base_level,
+                                           dirichlet_mask, ctypes.byref(h)), "grid_create")
+        self.h = h
+        self.n_cells = n0 << level
+        self.assembled = False
+
+    @property
+    def _lib(self):
+        return self.ctx._lib
+
+    def nnodes(self, level: int | None = None) -> int:
+        return int(self._lib.fmg_grid_nnodes(self.h, self.top if level is None else level))
+
+    @property
+    def nslots(self) -> int:
+        return int(self._lib.fmg_grid_nslots(self.h))
+
+    def set_coefficient(self, kind: int, values):
+        v = np.ascontiguousarray(np.atleast_1d(np.asarray(values, dtype=np.float64)).ravel())
+        self.ctx.check(self._lib.fmg_set_coefficient(self.h, kind, C.dptr(v), v.size), "set_coefficient")
+        self.assembled = False
+
+    def assemble(self) -> "Grid":
+        self.ctx.check(self._lib.fmg_assemble(self.h), "assemble")
+        self.assembled = True
+        return self
+
+    def matrix(self, level: int | None = None) -> np.ndarray:
+        level = self.top if level is None else level
+        out = np.zeros(self.nslots * self.nnodes(level))
+        self.ctx.check(self._lib.fmg_get_matrix(self.h, level, C.dptr(out)), "get_matrix")
+        return out.reshape(self.nslots, -1)
+
+    def rhs(self) -> np.ndarray:
+        out = np.zeros(self.nnodes())
+        self.ctx.check(self._lib.fmg_get_rhs(self.h, C.dptr(out)), "get_rhs")
+        return out
+
+    def set_node_damping(self, level: int, w):
+        if w is None:
+            self.ctx.check(self._lib.fmg_set_node_damping(self.h, level, None, 0), "set_node_damping")
+            return
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        self.ctx.check(self._lib.fmg_set_node_damping(self.h, level, C.dptr(w), w.size),
+                       "set_node_damping")
+
+    def vector(self, level: int | None = None, values=None) -> "Vector":
+        v = Vector(self, self.top if level is None else level)
+        if values is not None:
+            v.set(values)
+        return v
+
+    # operators of one level ---------------------------------------------
+    def matvec(self, x: "Vector", y: "Vector"):
+        self.ctx.check(self._lib.fmg_matvec(self.h, x.level, x.h, y.h), "matvec")
+
+    def residual(self, x: "Vector", b: "Vector", r: "Vector"):
+        self.ctx.check(self._lib.fmg_residual(self.h, x.level, x.h, b.h, r.h), "residual")
+
+    def restrict(self, rf: "Vector", rc: "Vector"):
+        self.ctx.check(self._lib.fmg_restrict(self.h, rf.level, rf.h, rc.h), "restrict")
+
+    def prolongate(self, xc: "Vector", xf: "Vector"):
+        self.ctx.check(self._lib.fmg_prolongate(self.h, xc.level, xc.h, xf.h), "prolongate")
+
+    def jacobi(self, x: "Vector", r: "Vector", damp: float):
+        self.ctx.check(self._lib.fmg_jacobi(self.h, x.level, damp, x.h, r.h), "jacobi")
+
+    def sor(self, x: "Vector", b: "Vector", r: "Vector", omega: float):
+        self.ctx.check(self._lib.fmg_sor(self.h, x.level, omega, x.h, b.h, r.h), "sor")
+
+    def coarse_solve(self, x: "Vector", r: "Vector", damp: float = 1.0):
+        self.ctx.check(self._lib.fmg_coarse_solve(self.h, damp, x.h, r.h), "coarse_solve")
+
+    def vcycle(self, cfg: C.SolveCfg, x: "Vector", b: "Vector", r: "Vector"):
+        self.ctx.check(self._lib.fmg_vcycle(self.h, ctypes.byref(cfg), x.h, b.h, r.h), "vcycle")
+
+    def solve(self, cfg: C.SolveCfg, x: "Vector"):
+        hist = np.zeros(cfg.maxsteps + 2)
+        ns, st = ctypes.c_int(0), ctypes.c_int(0)
+        self.ctx.check(self._lib.fmg_solve(self.h, ctypes.byref(cfg), x.h, C.dptr(hist), hist.size,
+                                           ctypes.byref(ns), ctypes.byref(st)), "solve")
+        return hist[: ns.value + 1].copy(), ns.value, st.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fmg_grid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Vector:
+    """A device vector of one level (``fmg_vec_create``)."""
+
+    def __init__(self, grid: Grid, level: int):
+        self.grid, self.level = grid, level
+        self.n = grid.nnodes(level)
+        h = ctypes.c_void_p()
+        grid.ctx.check(grid._lib.fmg_vec_create(grid.h, level, ctypes.byref(h)), "vec_create")
+        self.h = h
+
+    @property
+    def _lib(self):
+        return self.grid._lib
+
+    def set(self, values):
+        v = np.ascontiguousarray(np.asarray(values, dtype=np.float64).ravel())
+        self.grid.ctx.check(self._lib.fmg_vec_set(self.h, C.dptr(v), v.size), "vec_set")
+        return self
+
+    def get(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        self.grid.ctx.check(self._lib.fmg_vec_get(self.h, C.dptr(out), self.n), "vec_get")
+        return out
+
+    def fill(self, value: float = 0.0):
+        self.grid.ctx.check(self._lib.fmg_vec_fill(self.h, value), "fill")
+        return self
+
+    def copy_to(self, y: "Vector"):
+        self.grid.ctx.check(self._lib.fmg_copy(self.h, y.h), "copy")
+
+    def axpy(self, alpha: float, x: "Vector"):
+        """self := self + alpha x"""
+        self.grid.ctx.check(self._lib.fmg_axpy(alpha, x.h, self.h), "axpy")
+
+    def dot(self, y: "Vector") -> float:
+        out = ctypes.c_double()
+        self.grid.ctx.check(self._lib.fmg_dot(self.h, y.h, ctypes.byref(out)), "dot")
+        return out.value
+
+    def l2_norm(self) -> float:
+        out = ctypes.c_double()
+        self.grid.ctx.check(self._lib.fmg_l2_norm(self.h, ctypes.byref(out)), "l2_norm")
+        return out.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fmg_vec_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,894 @@
+// fmgpu.cu -- host runtime of libfmgpu.so: handles, assembly driver, the
+// multigrid iterator and the <linear-solver>/<cg> loop, and the C-ABI.
+//
+// The multigrid iterator replays Femlisp's bookkeeping exactly
+// (multigrid.lisp:173-393, linit.lisp:73-323): per level a residual-p flag
+// decides when compute-residual runs, the product-iterator recomputes the
+// residual after each Jacobi step, restrict zeroes the coarse solution and
+// copies the restricted residual into the coarse rhs, and the top level uses
+// the caller's vectors without copying -- so passing the same vector as rhs
+// and residual reproduces the alias of the <cg> preconditioner call.
+// Kernel fusion is applied only where it leaves every observable value
+// unchanged: compute-residual is fused into the Jacobi step that consumes it,
+// and the residual writes of a smoother are skipped when nothing can read them
+// before they are recomputed (distinct rhs and residual vectors).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <utility>
+
+#include "fmgpu_kernels.cuh"
+
+using namespace fmg;
+
+struct fmg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  double* host_scal = nullptr;  // pinned copy of a grid's scalar slots
+  std::string err;
+};
+
+namespace {
+
+struct Lvl {
+  long long n = 0, M = 0, N = 0, Np = 0;
+  double h = 0;
+  double* A = nullptr;
+  double* omega = nullptr;
+  double* sol[2] = {nullptr, nullptr};
+  double* rhs = nullptr;
+  double* res = nullptr;
+  double* Kbar = nullptr;
+  double* Ctab = nullptr;
+  double* Phi = nullptr;
+};
+
+}  // namespace
+
+struct fmg_grid {
+  fmg_ctx* ctx = nullptr;
+  int dim = 0, order = 0, nc = 1, n0 = 1, top = 0, base = 0, dmask = 0;
+  int nslots = 0, center = 0, nl = 0, nq = 0, np = 0;
+  std::vector<Lvl> lev;
+  int kkind = FMG_K_CONST;
+  double kconst = 1.0;
+  std::vector<double> kcell_h;
+  int fkind = FMG_F_CONST;
+  double fconst = 1.0;
+  std::vector<double> fip_h;
+  double xi_h[3] = {0, 0, 0};
+  double* xi_d = nullptr;
+  double* kcell_d = nullptr;
+  double* fip_d = nullptr;
+  double* rhs = nullptr;       // assembled top-level rhs
+  double* ainvT = nullptr;     // base-level inverse, transposed
+  int nbase = 0;
+  double* scal = nullptr;      // S_COUNT scalar slots
+  double* part = nullptr;      // reduction partials
+  unsigned* counter = nullptr;
+  // top-level work vectors of the solvers
+  double *p = nullptr, *a = nullptr, *w = nullptr, *w2 = nullptr, *q = nullptr, *r = nullptr,
+         *xs = nullptr, *xs2 = nullptr;
+  bool assembled = false;
+  bool assembled_once = false;
+  double* kq = nullptr;        // Gauss-point coefficient samples of a coarse level
+  double *lu = nullptr, *lux = nullptr;  // coarse LU factors and inverse workspace
+  int* piv = nullptr;
+  // multigrid state (multigrid.lisp:101-116)
+  std::vector<double*> solp, sparep, rhsp, resp;
+  std::vector<int> rp;
+  int cur = 0;
+  std::vector<void*> allocs;
+};
+
+struct fmg_vec {
+  fmg_grid* g = nullptr;
+  int level = 0;
+  long long n = 0;
+  double* d = nullptr;
+};
+
+// ------------------------------------------------------------------ errors
+namespace {
+
+int set_err(fmg_ctx* c, int code, const char* fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+int cuda_err(fmg_ctx* c, cudaError_t e, const char* what) {
+  return set_err(c, FMG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define FMG_CK(ctx, call)                                   \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_err((ctx), e_, #call); \
+  } while (0)
+
+int launched(fmg_ctx* c, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(c, e, what);
+  return FMG_OK;
+}
+
+long long pad64(long long n) { return (n + 63) / 64 * 64; }
+
+int dalloc(fmg_grid* g, double** p, long long n) {
+  void* q = nullptr;
+  size_t bytes = (size_t)(n > 0 ? n : 1) * sizeof(double);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(g->ctx, FMG_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  e = cudaMemsetAsync(q, 0, bytes, g->ctx->stream);
+  if (e != cudaSuccess) return cuda_err(g->ctx, e, "cudaMemsetAsync");
+  g->allocs.push_back(q);
+  *p = (double*)q;
+  return FMG_OK;
+}
+
+void dfree(fmg_grid* g, void* p) {
+  if (!p) return;
+  for (auto it = g->allocs.begin(); it != g->allocs.end(); ++it)
+    if (*it == p) { g->allocs.erase(it); break; }
+  cudaFree(p);
+}
+
+// ------------------------------------------------------------ FE tables
+// Gauss rule with order+1 points per direction on [0,1] (fe.lisp:235-244,
+// quadrature.lisp:202-215): xi = (1 - t)/2 for the Gauss-Legendre nodes t in
+// ascending order, weights w_GL/2.
+void gauss1d(int order, int* np, double* xi, double* w) {
+  if (order == 1) {
+    const double t = std::sqrt(1.0 / 3.0);
+    const double ts[2] = {-t, t};
+    *np = 2;
+    for (int k = 0; k < 2; ++k) { xi[k] = 0.5 * (1.0 - ts[k]); w[k] = 0.5; }
+  } else {
+    const double t = std::sqrt(0.6);
+    const double ts[3] = {-t, 0.0, t};
+    const double wg[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    *np = 3;
+    for (int k = 0; k < 3; ++k) { xi[k] = 0.5 * (1.0 - ts[k]); w[k] = 0.5 * wg[k]; }
+  }
+}
+
+// 1D Lagrange basis on the uniform nodes 0, 1/p, .., 1 (lagrange.lisp:41-51)
+double lag(int order, int a, double s) {
+  if (order == 1) return a == 0 ? 1.0 - s : s;
+  if (a == 0) return 2.0 * (s - 0.5) * (s - 1.0);
+  if (a == 1) return 4.0 * s * (1.0 - s);
+  return 2.0 * s * (s - 0.5);
+}
+double dlag(int order, int a, double s) {
+  if (order == 1) return a == 0 ? -1.0 : 1.0;
+  if (a == 0) return 4.0 * s - 3.0;
+  if (a == 1) return 4.0 - 8.0 * s;
+  return 4.0 * s - 1.0;
+}
+
+// Element tables of one level (cell width h): the integration weight at q is
+// W_q h^d (fe-cell-geometry, fe.lisp:502-535) and the physical gradient is the
+// reference gradient times 1/h; C[q][a][b] = W_q h^d grad phi_a . grad phi_b,
+// Kbar = sum_q C[q], Phi[q][a] = W_q h^d phi_a (ellsys-fe.lisp:120-127,183-190).
+void make_tables(int dim, int order, double h, std::vector<double>& C, std::vector<double>& Kbar,
+                 std::vector<double>& Phi, int* nl_out, int* nq_out) {
+  int np;
+  double xi[3], w[3];
+  gauss1d(order, &np, xi, w);
+  const int p1 = order + 1;
+  int nl = 1, nq = 1;
+  for (int k = 0; k < dim; ++k) { nl *= p1; nq *= np; }
+  double vol = 1.0;
+  for (int k = 0; k < dim; ++k) vol = vol * h;
+  const double invh = 1.0 / h;
+  C.assign((size_t)nq * nl * nl, 0.0);
+  Kbar.assign((size_t)nl * nl, 0.0);
+  Phi.assign((size_t)nq * nl, 0.0);
+  std::vector<double> G((size_t)nl * 3), phi(nl);
+  for (int q = 0; q < nq; ++q) {
+    const int qi[3] = {q % np, (q / np) % np, q / (np * np)};
+    double W = 1.0;
+    for (int k = 0; k < dim; ++k) W = W * w[qi[k]];
+    const double Wv = W * vol;
+    for (int a = 0; a < nl; ++a) {
+      const int ai[3] = {a % p1, (a / p1) % p1, a / (p1 * p1)};
+      double v = 1.0;
+      for (int k = 0; k < dim; ++k) v = v * lag(order, ai[k], xi[qi[k]]);
+      phi[a] = v;
+      for (int kd = 0; kd < dim; ++kd) {
+        double gg = 1.0;
+        for (int k = 0; k < dim; ++k)
+          gg = gg * (k == kd ? dlag(order, ai[k], xi[qi[k]]) : lag(order, ai[k], xi[qi[k]]));
+        G[a * 3 + kd] = gg * invh;
+      }
+    }
+    for (int a = 0; a < nl; ++a) {
+      Phi[(size_t)q * nl + a] = Wv * phi[a];
+      for (int b = 0; b < nl; ++b) {
+        double gg = G[a * 3] * G[b * 3];
+        for (int kd = 1; kd < dim; ++kd) gg = std::fma(G[a * 3 + kd], G[b * 3 + kd], gg);
+        C[((size_t)q * nl + a) * nl + b] = Wv * gg;
+      }
+    }
+  }
+  for (int q = 0; q < nq; ++q)
+    for (int ab = 0; ab < nl * nl; ++ab) Kbar[ab] = Kbar[ab] + C[(size_t)q * nl * nl + ab];
+  *nl_out = nl;
+  *nq_out = nq;
+}
+
+int upload(fmg_grid* g, double** dst, const std::vector<double>& v) {
+  int rc = dalloc(g, dst, (long long)v.size());
+  if (rc) return rc;
+  FMG_CK(g->ctx, cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 g->ctx->stream));
+  return FMG_OK;
+}
+
+LevelView view(const fmg_grid* g, int l) {
+  const Lvl& L = g->lev[l];
+  LevelView v;
+  v.A = L.A; v.N = L.N; v.Np = L.Np; v.M = L.M;
+  v.dim = g->dim; v.order = g->order; v.dmask = g->dmask; v.center = g->center;
+  v.omega = L.omega;
+  return v;
+}
+
+Reduce reducer(fmg_grid* g, int epi, int slot) {
+  Reduce R;
+  R.part = g->part; R.counter = g->counter; R.scal = g->scal; R.epi = epi; R.slot = slot;
+  return R;
+}
+
+// ------------------------------------------------------- multigrid iterator
+struct MG {
+  fmg_grid* g;
+  const fmg_solve_cfg& c;
+  bool literal;          // keep every residual write (fmg_vcycle on user vectors)
+  cudaStream_t st;
+
+  bool alias(int l) const { return g->rhsp[l] == g->resp[l]; }
+
+  void residual(int l) {
+    launch_spmv(view(g, l), g->solp[l], g->rhsp[l], g->resp[l], nullptr, nullptr, st);
+  }
+  void ensure_res() {  // ensure-mg-residual (multigrid.lisp:173-177)
+    const int l = g->cur;
+    if (!g->rp[l]) { residual(l); g->rp[l] = 1; }
+  }
+  // one <jacobi> step; with need_res the preceding compute-residual is fused in
+  void jacobi_step(int l, bool need_res) {
+    const bool write_r = literal || alias(l);
+    if (need_res) {
+      launch_jacobi_res(view(g, l), c.damp, g->solp[l], g->rhsp[l], g->sparep[l], g->resp[l], write_r,
+                        nullptr, nullptr, st);
+      std::swap(g->solp[l], g->sparep[l]);
+    } else {
+      launch_jacobi(view(g, l), c.damp, g->solp[l], g->resp[l], write_r, st);
+    }
+  }
+  void smooth(int steps) {  // smooth (multigrid.lisp:179-189) + product-iterator (linit.lisp:94-120)
+    if (steps <= 0) return;
+    const int l = g->cur;
+    if (c.smoother == FMG_JACOBI) {
+      bool need = !g->rp[l];  // residual-before: ensure-mg-residual
+      for (int s = 0; s < steps; ++s) {
+        jacobi_step(l, need);
+        need = true;          // the product-iterator recomputes after every step
+      }
+      if (steps > 1 && (literal || alias(l))) residual(l);
+    } else {
+      for (int s = 0; s < steps; ++s) launch_sor(view(g, l), c.damp, g->solp[l], g->rhsp[l], g->resp[l], st);
+    }
+    g->rp[l] = 0;
+  }
+  void restrict_() {  // restrict + :after methods (multigrid.lisp:202-224)
+    const int l = g->cur;
+    ensure_res();
+    launch_restrict(view(g, l), view(g, l - 1), g->resp[l], g->resp[l - 1], g->rhsp[l - 1], g->solp[l - 1], st);
+    g->cur = l - 1;
+    g->rp[l - 1] = 1;
+  }
+  void prolongate() {  // multigrid.lisp:237-252
+    const int l = g->cur;
+    launch_prolong(view(g, l), view(g, l + 1), g->solp[l], g->solp[l + 1], st);
+    g->cur = l + 1;
+    g->rp[l + 1] = 0;
+  }
+  void lmgc() {  // multigrid.lisp:254-288
+    const int l = g->cur;
+    if (l == g->base) {
+      launch_coarse_solve(g->ainvT, g->nbase, c.coarse_damp, g->solp[l], g->resp[l], st);
+      g->rp[l] = 0;
+      return;
+    }
+    if (c.combination == FMG_MULTIPLICATIVE) {
+      smooth(c.pre_steps);
+      restrict_();
+    } else {
+      restrict_();
+      g->cur += 1;
+      smooth(c.pre_steps);
+      g->cur -= 1;
+    }
+    const int gam = c.gamma == 0 ? 0 : (g->cur == g->base ? 1 : c.gamma);
+    for (int i = gam; i >= 1; --i) {
+      lmgc();
+      if (i != 1) ensure_res();
+    }
+    if (c.combination == FMG_MULTIPLICATIVE) {
+      prolongate();
+      smooth(c.post_steps);
+    } else {
+      g->cur += 1;
+      smooth(c.post_steps);
+      g->cur -= 1;
+      prolongate();
+    }
+  }
+  // the iterate closure of the multigrid iterator (multigrid.lisp:366-386);
+  // *x may be swapped with *spare (ping-pong of fused Jacobi steps)
+  void iterate(double** x, double** spare, double* b, double* r) {
+    const int top = g->top;
+    g->solp[top] = *x; g->sparep[top] = *spare;
+    g->rhsp[top] = b; g->resp[top] = r;
+    g->rp[top] = 1;
+    g->cur = top;
+    lmgc();
+    *x = g->solp[top];
+    *spare = g->sparep[top];
+  }
+};
+
+int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
+  if (!c) return set_err(g->ctx, FMG_ERR_ARG, "null configuration");
+  if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR)
+    return set_err(g->ctx, FMG_ERR_ARG, "unknown smoother %d", c->smoother);
+  if (c->pre_steps < 0 || c->post_steps < 0 || c->gamma < 0 || c->gamma > 4)
+    return set_err(g->ctx, FMG_ERR_ARG, "bad cycle parameters");
+  if (c->combination != FMG_MULTIPLICATIVE && c->combination != FMG_ADDITIVE)
+    return set_err(g->ctx, FMG_ERR_ARG, "bad combination");
+  if (c->method < FMG_METHOD_MG || c->method > FMG_METHOD_CG)
+    return set_err(g->ctx, FMG_ERR_ARG, "bad method");
+  return FMG_OK;
+}
+
+int vec_check(const fmg_vec* v, const fmg_grid* g, int level) {
+  if (!v || v->g != g || v->level != level) return FMG_ERR_ARG;
+  return FMG_OK;
+}
+
+// copies the grid scalars to the host and waits
+int read_scalars(fmg_grid* g) {
+  fmg_ctx* c = g->ctx;
+  FMG_CK(c, cudaMemcpyAsync(c->host_scal, g->scal, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
+  return FMG_OK;
+}
+
+}  // namespace
+
+// =================================================================== C-ABI
+extern "C" {
+
+int fmg_init(int device, fmg_ctx** out) {
+  if (!out) return FMG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || device < 0 || device >= ndev) return FMG_ERR_CUDA;
+  fmg_ctx* c = new (std::nothrow) fmg_ctx();
+  if (!c) return FMG_ERR_NOMEM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost((void**)&c->host_scal, S_COUNT * sizeof(double)) != cudaSuccess) {
+    delete c;
+    return FMG_ERR_CUDA;
+  }
+  *out = c;
+  return FMG_OK;
+}
+
+int fmg_finalize(fmg_ctx* c) {
+  if (!c) return FMG_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  cudaFreeHost(c->host_scal);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return FMG_OK;
+}
+
+int fmg_last_error(fmg_ctx* c, char* buf, int len) {
+  if (!c || !buf || len <= 0) return FMG_ERR_ARG;
+  snprintf(buf, (size_t)len, "%s", c->err.c_str());
+  return FMG_OK;
+}
+
+int fmg_synchronize(fmg_ctx* c) {
+  if (!c) return FMG_ERR_ARG;
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
+  return FMG_OK;
+}
+
+int fmg_launch_count(long long* out) {
+  if (!out) return FMG_ERR_ARG;
+  *out = g_launches.load(std::memory_order_relaxed);
+  return FMG_OK;
+}
+
+int fmg_get_stream(fmg_ctx* c, void** stream) {
+  if (!c || !stream) return FMG_ERR_ARG;
+  *stream = (void*)c->stream;
+  return FMG_OK;
+}
+
+int fmg_grid_create(fmg_ctx* c, int dim, int order, int ncomp, int n0, int top_level, int base_level,
+                    int dirichlet_mask, fmg_grid** out) {
+  if (!c || !out) return FMG_ERR_ARG;
+  *out = nullptr;
+  if (dim < 1 || dim > 3 || order < 1 || order > 2 || n0 < 1 || base_level < 0 || base_level > top_level ||
+      top_level >= kMaxLevels)
+    return set_err(c, FMG_ERR_ARG, "unsupported grid (dim %d order %d levels %d..%d)", dim, order, base_level,
+                   top_level);
+  if (ncomp != 1) return set_err(c, FMG_ERR_UNSUPPORTED, "ncomp %d: only scalar problems are built", ncomp);
+  fmg_grid* g = new (std::nothrow) fmg_grid();
+  if (!g) return FMG_ERR_NOMEM;
+  g->ctx = c;
+  g->dim = dim; g->order = order; g->nc = ncomp; g->n0 = n0;
+  g->top = top_level; g->base = base_level; g->dmask = dirichlet_mask;
+  int w = 2 * order + 1;
+  g->nslots = 1;
+  for (int k = 0; k < dim; ++k) g->nslots *= w;
+  g->center = (g->nslots - 1) / 2;
+  g->lev.resize(top_level + 1);
+  for (int l = 0; l <= top_level; ++l) {
+    Lvl& L = g->lev[l];
+    L.n = (long long)n0 << l;
+    L.M = order * L.n + 1;
+    L.N = 1;
+    for (int k = 0; k < dim; ++k) L.N *= L.M;
+    L.Np = pad64(L.N);
+    L.h = 1.0 / (double)L.n;
+  }
+  double wq[3];
+  gauss1d(order, &g->np, g->xi_h, wq);
+  g->nl = 1; g->nq = 1;
+  for (int k = 0; k < dim; ++k) { g->nl *= order + 1; g->nq *= g->np; }
+  *out = g;
+  return FMG_OK;
+}
+
+int fmg_grid_destroy(fmg_grid* g) {
+  if (!g) return FMG_ERR_ARG;
+  cudaStreamSynchronize(g->ctx->stream);
+  for (void* p : g->allocs) cudaFree(p);
+  delete g;
+  return FMG_OK;
+}
+
+long fmg_grid_nnodes(const fmg_grid* g, int level) {
+  if (!g || level < 0 || level > g->top) return -1;
+  return (long)g->lev[level].N;
+}
+
+int fmg_grid_nslots(const fmg_grid* g) { return g ? g->nslots : -1; }
+
+int fmg_set_coefficient(fmg_grid* g, int kind, const double* host, long n) {
+  if (!g || !host) return FMG_ERR_ARG;
+  long long ncell = 1;
+  for (int k = 0; k < g->dim; ++k) ncell *= g->lev[g->top].n;
+  switch (kind) {
+    case FMG_K_CONST:
+      if (n != 1) return set_err(g->ctx, FMG_ERR_ARG, "K_CONST wants 1 value");
+      g->kkind = kind; g->kconst = host[0]; break;
+    case FMG_K_CELL:
+      if (n != ncell) return set_err(g->ctx, FMG_ERR_ARG, "K_CELL wants %lld values, got %ld", ncell, n);
+      g->kkind = kind; g->kcell_h.assign(host, host + n); break;
+    case FMG_F_CONST:
+      if (n != 1) return set_err(g->ctx, FMG_ERR_ARG, "F_CONST wants 1 value");
+      g->fkind = kind; g->fconst = host[0]; break;
+    case FMG_F_IP:
+      if (n != ncell * g->nq) return set_err(g->ctx, FMG_ERR_ARG, "F_IP wants %lld values", ncell * g->nq);
+      g->fkind = kind; g->fip_h.assign(host, host + n); break;
+    default: return set_err(g->ctx, FMG_ERR_ARG, "unknown coefficient kind %d", kind);
+  }
+  g->assembled = false;
+  return FMG_OK;
+}
+
+// device buffers of a hierarchy, allocated by the first assembly and reused
+// by later ones (only the coefficient data change between assemblies)
+static int ensure_buffers(fmg_grid* g) {
+  if (g->assembled_once) return FMG_OK;
+  int rc;
+  const Lvl& T = g->lev[g->top];
+  long long ncell_top = 1, ncell_kq = 0;
+  for (int k = 0; k < g->dim; ++k) ncell_top *= T.n;
+  if (g->top > g->base) ncell_kq = ncell_top >> g->dim;  // largest coarse level
+  std::vector<double> xiv(g->xi_h, g->xi_h + g->np);
+  if ((rc = upload(g, &g->xi_d, xiv))) return rc;
+  if ((rc = dalloc(g, &g->rhs, T.Np))) return rc;
+  if ((rc = dalloc(g, &g->kq, ncell_kq * g->nq))) return rc;
+  for (int l = g->top; l >= g->base; --l) {
+    Lvl& L = g->lev[l];
+    std::vector<double> C, Kbar, Phi;
+    int nl, nq;
+    make_tables(g->dim, g->order, L.h, C, Kbar, Phi, &nl, &nq);
+    if ((rc = upload(g, &L.Kbar, Kbar)) || (rc = upload(g, &L.Ctab, C)) || (rc = upload(g, &L.Phi, Phi)))
+      return rc;
+    if ((rc = dalloc(g, &L.A, (long long)g->nslots * L.Np))) return rc;
+  }
+  const Lvl& B = g->lev[g->base];
+  if (B.N > 1024)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "base level has %lld nodes; the dense coarse solve takes <= 1024",
+                   B.N);
+  g->nbase = (int)B.N;
+  const long long nn = (long long)B.N * B.N;
+  if ((rc = dalloc(g, &g->lu, nn)) || (rc = dalloc(g, &g->lux, nn)) || (rc = dalloc(g, &g->ainvT, nn)) ||
+      (rc = dalloc(g, (double**)&g->piv, B.N)))
+    return rc;
+  for (int l = g->base; l < g->top; ++l) {
+    Lvl& L = g->lev[l];
+    if ((rc = dalloc(g, &L.sol[0], L.Np)) || (rc = dalloc(g, &L.sol[1], L.Np)) || (rc = dalloc(g, &L.rhs, L.Np)) ||
+        (rc = dalloc(g, &L.res, L.Np)))
+      return rc;
+  }
+  if ((rc = dalloc(g, &g->scal, S_COUNT))) return rc;
+  if ((rc = dalloc(g, &g->part, nchunks(T.Np) + 1))) return rc;
+  if ((rc = dalloc(g, (double**)&g->counter, 1))) return rc;
+  double** tv[] = {&g->p, &g->a, &g->w, &g->w2, &g->q, &g->r, &g->xs, &g->xs2};
+  for (double** v : tv)
+    if ((rc = dalloc(g, v, T.Np))) return rc;
+  g->assembled_once = true;
+  return FMG_OK;
+}
+
+int fmg_assemble(fmg_grid* g) {
+  if (!g) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  int rc;
+  FMG_CK(c, cudaSetDevice(c->device));
+  g->assembled = false;
+  if ((rc = ensure_buffers(g))) return rc;
+  // coefficient inputs (host -> device)
+  long long ncell_top = 1;
+  for (int k = 0; k < g->dim; ++k) ncell_top *= g->lev[g->top].n;
+  if (g->kkind == FMG_K_CELL) {
+    if (!g->kcell_d && (rc = dalloc(g, &g->kcell_d, ncell_top))) return rc;
+    FMG_CK(c, cudaMemcpyAsync(g->kcell_d, g->kcell_h.data(), ncell_top * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  if (g->fkind == FMG_F_IP) {
+    if (!g->fip_d && (rc = dalloc(g, &g->fip_d, ncell_top * g->nq))) return rc;
+    FMG_CK(c, cudaMemcpyAsync(g->fip_d, g->fip_h.data(), ncell_top * g->nq * sizeof(double),
+                              cudaMemcpyHostToDevice, st));
+  }
+  const long long n_top = g->lev[g->top].n;
+  for (int l = g->top; l >= g->base; --l) {
+    Lvl& L = g->lev[l];
+    long long ncells = 1;
+    for (int k = 0; k < g->dim; ++k) ncells *= L.n;
+    const bool sample = (l < g->top && g->kkind == FMG_K_CELL);
+    if (sample) {
+      launch_sample_kq(g->dim, ncells, L.n, n_top, std::ldexp(1.0, g->top - l), g->np, g->xi_d, g->kcell_d, g->kq,
+                       st);
+      if ((rc = launched(c, "sample_kq"))) return rc;
+    }
+    AsmArgs a;
+    a.N = L.N; a.Np = L.Np; a.M = L.M; a.n = L.n;
+    a.dmask = g->dmask; a.nl = g->nl; a.nq = g->nq;
+    a.A = L.A;
+    a.rhs = (l == g->top) ? g->rhs : nullptr;
+    a.Kbar = L.Kbar; a.Ctab = L.Ctab; a.Phi = L.Phi;
+    a.kcell = (l == g->top && g->kkind == FMG_K_CELL) ? g->kcell_d : nullptr;
+    a.kq = sample ? g->kq : nullptr;
+    a.fip = g->fkind == FMG_F_IP ? g->fip_d : nullptr;
+    a.kconst = g->kconst; a.fconst = g->fconst;
+    launch_assemble(g->dim, g->order, a, st);
+    if ((rc = launched(c, "assemble"))) return rc;
+  }
+  // dense LU of the base level and its explicit inverse
+  const Lvl& B = g->lev[g->base];
+  FMG_CK(c, cudaMemsetAsync(g->lu, 0, (size_t)B.N * B.N * sizeof(double), st));
+  launch_densify(view(g, g->base), g->lu, st);
+  launch_lu(g->lu, (int)B.N, g->piv, g->lux, g->ainvT, st);
+  if ((rc = launched(c, "coarse LU"))) return rc;
+  // multigrid state
+  const int nlev = g->top + 1;
+  g->solp.assign(nlev, nullptr); g->sparep.assign(nlev, nullptr);
+  g->rhsp.assign(nlev, nullptr); g->resp.assign(nlev, nullptr);
+  g->rp.assign(nlev, 0);
+  for (int l = g->base; l < g->top; ++l) {
+    g->solp[l] = g->lev[l].sol[0]; g->sparep[l] = g->lev[l].sol[1];
+    g->rhsp[l] = g->lev[l].rhs; g->resp[l] = g->lev[l].res;
+  }
+  FMG_CK(c, cudaStreamSynchronize(st));
+  g->assembled = true;
+  return FMG_OK;
+}
+
+int fmg_get_matrix(fmg_grid* g, int level, double* host) {
+  if (!g || !host) return FMG_ERR_ARG;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  if (level < g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d out of range", level);
+  const Lvl& L = g->lev[level];
+  FMG_CK(g->ctx, cudaMemcpy2DAsync(host, L.N * sizeof(double), L.A, L.Np * sizeof(double), L.N * sizeof(double),
+                                   g->nslots, cudaMemcpyDeviceToHost, g->ctx->stream));
+  FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+  return FMG_OK;
+}
+
+int fmg_get_rhs(fmg_grid* g, double* host) {
+  if (!g || !host) return FMG_ERR_ARG;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  const Lvl& T = g->lev[g->top];
+  FMG_CK(g->ctx, cudaMemcpyAsync(host, g->rhs, T.N * sizeof(double), cudaMemcpyDeviceToHost, g->ctx->stream));
+  FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+  return FMG_OK;
+}
+
+int fmg_set_node_damping(fmg_grid* g, int level, const double* host, long n) {
+  if (!g) return FMG_ERR_ARG;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  if (level <= g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d has no smoother", level);
+  Lvl& L = g->lev[level];
+  if (!host) {
+    if (L.omega) { cudaStreamSynchronize(g->ctx->stream); dfree(g, L.omega); }
+    L.omega = nullptr;
+    return FMG_OK;
+  }
+  if (n != L.N) return set_err(g->ctx, FMG_ERR_ARG, "damping wants %lld values", L.N);
+  int rc;
+  if (!L.omega && (rc = dalloc(g, &L.omega, L.Np))) return rc;
+  FMG_CK(g->ctx, cudaMemcpyAsync(L.omega, host, L.N * sizeof(double), cudaMemcpyHostToDevice, g->ctx->stream));
+  return FMG_OK;
+}
+
+int fmg_vec_create(fmg_grid* g, int level, fmg_vec** out) {
+  if (!g || !out || level < 0 || level > g->top) return FMG_ERR_ARG;
+  fmg_vec* v = new (std::nothrow) fmg_vec();
+  if (!v) return FMG_ERR_NOMEM;
+  v->g = g; v->level = level; v->n = g->lev[level].N;
+  const long long np = pad64(v->n);
+  cudaError_t e = cudaMalloc((void**)&v->d, np * sizeof(double));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete v;
+    return set_err(g->ctx, FMG_ERR_NOMEM, "vector allocation failed");
+  }
+  FMG_CK(g->ctx, cudaMemsetAsync(v->d, 0, np * sizeof(double), g->ctx->stream));
+  *out = v;
+  return FMG_OK;
+}
+
+int fmg_vec_destroy(fmg_vec* v) {
+  if (!v) return FMG_ERR_ARG;
+  cudaStreamSynchronize(v->g->ctx->stream);
+  cudaFree(v->d);
+  delete v;
+  return FMG_OK;
+}
+
+int fmg_vec_set(fmg_vec* v, const double* host, long n) {
+  if (!v || !host || n != v->n) return FMG_ERR_ARG;
+  FMG_CK(v->g->ctx, cudaMemcpyAsync(v->d, host, n * sizeof(double), cudaMemcpyHostToDevice, v->g->ctx->stream));
+  FMG_CK(v->g->ctx, cudaStreamSynchronize(v->g->ctx->stream));
+  return FMG_OK;
+}
+
+int fmg_vec_get(const fmg_vec* v, double* host, long n) {
+  if (!v || !host || n != v->n) return FMG_ERR_ARG;
+  FMG_CK(v->g->ctx, cudaMemcpyAsync(host, v->d, n * sizeof(double), cudaMemcpyDeviceToHost, v->g->ctx->stream));
+  FMG_CK(v->g->ctx, cudaStreamSynchronize(v->g->ctx->stream));
+  return FMG_OK;
+}
+
+int fmg_vec_fill(fmg_vec* v, double value) {
+  if (!v) return FMG_ERR_ARG;
+  launch_fill(v->d, v->n, value, v->g->ctx->stream);
+  return launched(v->g->ctx, "fill");
+}
+
+int fmg_copy(const fmg_vec* x, fmg_vec* y) {
+  if (!x || !y || x->n != y->n) return FMG_ERR_ARG;
+  launch_copy(x->d, y->d, x->n, x->g->ctx->stream);
+  return launched(x->g->ctx, "copy");
+}
+
+int fmg_axpy(double alpha, const fmg_vec* x, fmg_vec* y) {
+  if (!x || !y || x->n != y->n) return FMG_ERR_ARG;
+  launch_axpy(alpha, nullptr, -1, x->d, y->d, x->n, x->g->ctx->stream);
+  return launched(x->g->ctx, "axpy");
+}
+
+int fmg_dot(const fmg_vec* x, const fmg_vec* y, double* out) {
+  if (!x || !y || !out || x->n != y->n) return FMG_ERR_ARG;
+  fmg_grid* g = x->g;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  launch_dot(x->d, y->d, x->n, reducer(g, EPI_STORE, S_DOT), g->ctx->stream);
+  int rc = launched(g->ctx, "dot");
+  if (rc) return rc;
+  if ((rc = read_scalars(g))) return rc;
+  *out = g->ctx->host_scal[S_DOT];
+  return FMG_OK;
+}
+
+int fmg_l2_norm(const fmg_vec* x, double* out) {
+  int rc = fmg_dot(x, x, out);
+  if (rc) return rc;
+  *out = std::sqrt(*out);
+  return FMG_OK;
+}
+
+int fmg_matvec(fmg_grid* g, int level, const fmg_vec* x, fmg_vec* y) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (vec_check(x, g, level) || vec_check(y, g, level) || x == y) return FMG_ERR_ARG;
+  launch_spmv(view(g, level), x->d, nullptr, y->d, nullptr, nullptr, g->ctx->stream);
+  return launched(g->ctx, "matvec");
+}
+
+int fmg_residual(fmg_grid* g, int level, const fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level) || x == r) return FMG_ERR_ARG;
+  launch_spmv(view(g, level), x->d, b->d, r->d, nullptr, nullptr, g->ctx->stream);
+  return launched(g->ctx, "residual");
+}
+
+int fmg_restrict(fmg_grid* g, int fine_level, const fmg_vec* rf, fmg_vec* rc) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (fine_level <= g->base || vec_check(rf, g, fine_level) || vec_check(rc, g, fine_level - 1)) return FMG_ERR_ARG;
+  const Lvl& C = g->lev[fine_level - 1];
+  // the coarse rhs/sol side outputs of the fused kernel go to level scratch
+  launch_restrict(view(g, fine_level), view(g, fine_level - 1), rf->d, rc->d, C.rhs, C.sol[1], g->ctx->stream);
+  return launched(g->ctx, "restrict");
+}
+
+int fmg_prolongate(fmg_grid* g, int coarse_level, const fmg_vec* xc, fmg_vec* xf) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (coarse_level < g->base || coarse_level >= g->top || vec_check(xc, g, coarse_level) ||
+      vec_check(xf, g, coarse_level + 1))
+    return FMG_ERR_ARG;
+  launch_prolong(view(g, coarse_level), view(g, coarse_level + 1), xc->d, xf->d, g->ctx->stream);
+  return launched(g->ctx, "prolongate");
+}
+
+int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (vec_check(x, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
+  launch_jacobi(view(g, level), damp, x->d, r->d, true, g->ctx->stream);
+  return launched(g->ctx, "jacobi");
+}
+
+int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
+  launch_sor(view(g, level), omega, x->d, b->d, r->d, g->ctx->stream);
+  return launched(g->ctx, "sor");
+}
+
+int fmg_coarse_solve(fmg_grid* g, double damp, fmg_vec* x, fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (vec_check(x, g, g->base) || vec_check(r, g, g->base)) return FMG_ERR_ARG;
+  launch_coarse_solve(g->ainvT, g->nbase, damp, x->d, r->d, g->ctx->stream);
+  return launched(g->ctx, "coarse solve");
+}
+
+int fmg_vcycle(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  int rc = check_cfg(g, cfg);
+  if (rc) return rc;
+  if (vec_check(x, g, g->top) || vec_check(b, g, g->top) || vec_check(r, g, g->top) || x == b || x == r)
+    return FMG_ERR_ARG;
+  MG mg{g, *cfg, true, g->ctx->stream};
+  double* xp = x->d;
+  double* sp = g->xs;
+  mg.iterate(&xp, &sp, b->d, r->d);
+  if (xp != x->d) launch_copy(xp, x->d, x->n, g->ctx->stream);
+  return launched(g->ctx, "vcycle");
+}
+
+int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, int hist_len, int* nsteps,
+              int* status) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  int rc = check_cfg(g, cfg);
+  if (rc) return rc;
+  if (vec_check(xv, g, g->top) || !nsteps || !status) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const fmg_solve_cfg& cf = *cfg;
+  const LevelView T = view(g, g->top);
+  const long long n = T.N;
+  const double* b = g->rhs;
+  double* x = xv->d;
+  double* xspare = g->xs2;
+  MG mg{g, cf, false, st};
+  double defnorm = 0.0, initial = -1.0, alpha = 0.0;
+  bool rp = false, initialized = false;
+  *status = 1;
+  // CG vectors start at zero (make-domain-vector-for)
+  launch_fill(g->p, n, 0.0, st);
+  for (int step = 0;; ++step) {
+    if (!rp) {  // intermediate :before -> ensure-residual (problem.lisp:109-116)
+      launch_spmv(T, x, b, g->r, nullptr, nullptr, st);
+      launch_dot(g->r, g->r, n, reducer(g, EPI_STORE, S_RR), st);
+      if ((rc = launched(c, "residual"))) return rc;
+      rp = true;
+    }
+    if ((rc = read_scalars(g))) return rc;
+    defnorm = std::sqrt(c->host_scal[S_RR]);
+    if (initialized) alpha = c->host_scal[S_ALPHA];
+    if (!std::isfinite(defnorm)) {
+      *nsteps = step;
+      return set_err(c, FMG_ERR_NUMERIC, "defnorm is %g at step %d", defnorm, step);
+    }
+    if (initial < 0) initial = defnorm;
+    const double reduction = initial == 0.0 ? 0.0 : defnorm / initial;
+    if (hist && step < hist_len) hist[step] = defnorm;
+    *nsteps = step;
+    if ((cf.rtol > 0 && reduction < cf.rtol) || (cf.atol > 0 && defnorm < cf.atol)) { *status = 0; break; }
+    if (step > cf.maxsteps) { *status = 1; break; }
+    if (cf.method == FMG_METHOD_MG) {
+      mg.iterate(&x, &xspare, const_cast<double*>(b), g->r);
+      rp = false;
+      continue;
+    }
+    // <cg> (krylow.lisp:72-132)
+    if (!initialized) {  // restart: w := r; M(p <- w, w); alpha = (p, r)
+      if (cf.method == FMG_METHOD_CG_MG) {
+        if (cf.compat_alias) {
+          launch_copy(g->r, g->w, n, st);
+          mg.iterate(&g->p, &g->xs, g->w, g->w);
+        } else {
+          launch_copy(g->r, g->w2, n, st);
+          mg.iterate(&g->p, &g->xs, g->r, g->w2);
+        }
+      } else {
+        launch_copy(g->r, g->p, n, st);
+      }
+      launch_dot(g->p, g->r, n, reducer(g, EPI_STORE, S_ALPHA), st);
+      if ((rc = launched(c, "restart"))) return rc;
+      if ((rc = read_scalars(g))) return rc;
+      alpha = c->host_scal[S_ALPHA];
+      initialized = true;
+    }
+    if (alpha != 0.0) {  // krylow.lisp:106-127
+      const bool pre = cf.method == FMG_METHOD_CG_MG;
+      const Reduce Rl = reducer(g, EPI_CG_LAMBDA, 0);
+      launch_spmv(T, g->p, nullptr, g->a, g->p, &Rl, st);  // a = A p; beta = (a,p); lam = alpha/beta
+      const Reduce Rr = reducer(g, EPI_STORE, S_RR);
+      // x += lam p; r -= lam a; (r,r) for the next :defnorm; w := r; q := 0
+      if (pre && cf.compat_alias)
+        launch_cg_update(g->scal, x, g->p, g->r, g->a, g->w, nullptr, g->q, n, Rr, st);
+      else if (pre)
+        launch_cg_update(g->scal, x, g->p, g->r, g->a, nullptr, g->w2, g->q, n, Rr, st);
+      else
+        launch_cg_update(g->scal, x, g->p, g->r, g->a, g->q, nullptr, nullptr, n, Rr, st);  // q := (copy r)
+      if (pre) {
+        if (cf.compat_alias) mg.iterate(&g->q, &g->xs, g->w, g->w);
+        else mg.iterate(&g->q, &g->xs, g->r, g->w2);
+      }
+      launch_dot(g->q, g->r, n, reducer(g, EPI_CG_ALPHA, 0), st);  // new alpha, ratio
+      launch_p_update(g->scal, g->p, g->q, n, st);                     // p := ratio p + q
+      if ((rc = launched(c, "cg step"))) return rc;
+    }
+    rp = true;  // residual-after t
+  }
+  if (x != xv->d) launch_copy(x, xv->d, n, st);
+  FMG_CK(c, cudaStreamSynchronize(st));
+  return launched(c, "solve");
+}
+
+}  // extern "C"

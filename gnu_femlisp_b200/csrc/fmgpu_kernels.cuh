@@ -1,0 +1,55 @@
+// fmgpu_kernels.cuh -- launch interface of the FP64 kernels.
+#pragma once
+
+#include "fmgpu_internal.cuh"
+
+namespace fmg {
+
+// what a kernel needs to know about one level
+struct LevelView {
+  const double* A;      // [slot][Np]
+  long long N, Np, M;   // nodes, padded stride, nodes per direction
+  int dim, order, dmask, center;
+  const double* omega;  // per-node damping or nullptr
+};
+
+// arguments of the assembly kernel of one level
+struct AsmArgs {
+  long long N, Np, M, n;        // nodes, padded stride, nodes/direction, cells/direction
+  int dmask, nl, nq;
+  double* A;                    // out: [slot][Np]
+  double* rhs;                  // out (top level only) or nullptr
+  const double* Kbar;           // [a][b]: sum over Gauss points
+  const double* Ctab;           // [q][a][b]
+  const double* Phi;            // [q][a]
+  const double* kcell;          // top level: k per cell, or nullptr
+  const double* kq;             // coarse level: k per cell and Gauss point, or nullptr
+  const double* fip;            // source per cell and Gauss point, or nullptr
+  double kconst, fconst;
+};
+
+void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
+                 const Reduce* R, cudaStream_t st);
+void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st);
+void launch_jacobi_res(const LevelView& L, double damp, const double* x, const double* b, double* xout,
+                       double* r, bool write_r, const double* dv, const Reduce* R, cudaStream_t st);
+void launch_sor(const LevelView& L, double omega, double* x, const double* b, double* r, cudaStream_t st);
+void launch_restrict(const LevelView& F, const LevelView& C, const double* rf, double* rc, double* rhsc,
+                     double* solc, cudaStream_t st);
+void launch_prolong(const LevelView& C, const LevelView& F, const double* xc, double* xf, cudaStream_t st);
+void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st);
+void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t st);
+void launch_fill(double* x, long long n, double v, cudaStream_t st);
+void launch_copy(const double* x, double* y, long long n, cudaStream_t st);
+void launch_axpy(double alpha, const double* sc, int aslot, const double* x, double* y, long long n,
+                 cudaStream_t st);
+void launch_dot(const double* x, const double* y, long long n, const Reduce& R, cudaStream_t st);
+void launch_cg_update(const double* sc, double* x, const double* p, double* r, const double* a, double* w,
+                      double* w2, double* q, long long n, const Reduce& R, cudaStream_t st);
+void launch_p_update(const double* sc, double* p, const double* q, long long n, cudaStream_t st);
+void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_top, double ratio, int np,
+                      const double* xi, const double* kcell, double* kq, cudaStream_t st);
+void launch_assemble(int dim, int order, const AsmArgs& a, cudaStream_t st);
+void launch_densify(const LevelView& L, double* Dm, cudaStream_t st);
+
+}  // namespace fmg

@@ -1,0 +1,705 @@
+// kernels_fp64.cu -- the FP64 kernels of the multigrid solve path (sm_100a).
+//
+// Layout in HBM: a level matrix is stored by stencil slot (structure of
+// arrays): A[s * Np + i] = A(i, i + off_s), Np = node count rounded up to a
+// multiple of 64 so that every slot array starts on a 512-byte boundary.
+// Column indices are implicit (off_s = ox + M oy + M^2 oz), so the matvec
+// streams only matrix values: 128-bit loads of two consecutive rows per
+// thread, coalesced across the warp.  Entries outside the grid, in eliminated
+// Dirichlet columns and structurally absent Q2 couplings are stored as zeros,
+// which lets neighbour indices be clamped to the vector instead of tested.
+#include "fmgpu_kernels.cuh"
+
+namespace fmg {
+
+std::atomic<long long> g_launches{0};
+
+template <int D, int P>
+struct St {
+  static constexpr int W = 2 * P + 1;
+  static constexpr int NS = D == 1 ? W : (D == 2 ? W * W : W * W * W);
+  static constexpr int CENTER = (NS - 1) / 2;
+};
+
+template <int D, int P>
+__device__ __forceinline__ long long slot_off(int s, long long M) {
+  constexpr int W = 2 * P + 1;
+  long long o = (long long)(s % W - P);
+  if (D > 1) o += M * (long long)((s / W) % W - P);
+  if (D > 2) o += M * M * (long long)((s / (W * W)) % W - P);
+  return o;
+}
+
+__device__ __forceinline__ void node_coords(long long i, long long M, int dim, long long c[3]) {
+  c[0] = i % M;
+  c[1] = dim > 1 ? (i / M) % M : 0;
+  c[2] = dim > 2 ? i / (M * M) : 0;
+}
+
+__device__ __forceinline__ bool node_dirichlet(const long long c[3], long long M, int dim, int dmask) {
+  for (int k = 0; k < dim; ++k) {
+    if (c[k] == 0 && ((dmask >> (2 * k)) & 1)) return true;
+    if (c[k] == M - 1 && ((dmask >> (2 * k + 1)) & 1)) return true;
+  }
+  return false;
+}
+
+// ----------------------------------------------------------------- matvec
+// y = A x (RES = false) or r = b - A x (RES = true, b may alias r); with DOT
+// the chunk reduction of (y, dv) is fused in (DR4096 order).
+template <int D, int P, bool RES, bool DOT>
+__global__ void __launch_bounds__(kBlock)
+k_spmv(const double* __restrict__ A, long long N, long long Np, long long M,
+       const double* __restrict__ x, const double* b, double* y, const double* __restrict__ dv,
+       Reduce R) {
+  constexpr int NS = St<D, P>::NS;
+  __shared__ double smem[8];
+  const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 1
+  for (int m = 0; m < kPairsPerThread; ++m) {
+    const long long i0 = base + 512LL * m;
+    if (i0 >= N) break;
+    const bool two = i0 + 1 < N;
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const long long o = slot_off<D, P>(s, M);
+      const double2 a = __ldg(reinterpret_cast<const double2*>(A + (long long)s * Np + i0));
+      const double x0 = __ldg(x + clampi(i0 + o, N));
+      const double x1 = __ldg(x + clampi(i0 + 1 + o, N));
+      s0 = fma(a.x, x0, s0);
+      s1 = fma(a.y, x1, s1);
+    }
+    double y0 = s0, y1 = s1;
+    if (RES) {
+      y0 = b[i0] - s0;
+      if (two) y1 = b[i0 + 1] - s1;
+    }
+    y[i0] = y0;
+    if (two) y[i0 + 1] = y1;
+    if (DOT) {
+      acc = fma(y0, dv[i0], acc);
+      if (two) acc = fma(y1, dv[i0 + 1], acc);
+    }
+  }
+  if (DOT) dr_finish(acc, R, smem);
+}
+
+// ------------------------------------------------------------- smoothers
+// <jacobi> step with an up-to-date residual: t = r/d, x += w t, r := t
+__global__ void __launch_bounds__(kBlock)
+k_jacobi(const double* __restrict__ Dg, long long N, double damp, const double* __restrict__ omega,
+         double* x, double* r, int write_r) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double t = r[i] / Dg[i];
+  if (write_r) r[i] = t;
+  const double w = omega ? omega[i] : damp;
+  x[i] = fma(w, t, x[i]);
+}
+
+// compute-residual fused with the following <jacobi> step:
+// t = (b - A x)/d, xout = x + w t, r := t; optional fused (xout, dv) reduction
+template <int D, int P, bool DOT>
+__global__ void __launch_bounds__(kBlock)
+k_jacobi_res(const double* __restrict__ A, long long N, long long Np, long long M, double damp,
+             const double* __restrict__ omega, const double* __restrict__ x, const double* b,
+             double* __restrict__ xout, double* r, int write_r, const double* __restrict__ dv,
+             Reduce R) {
+  constexpr int NS = St<D, P>::NS;
+  constexpr int C = St<D, P>::CENTER;
+  __shared__ double smem[8];
+  const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 1
+  for (int m = 0; m < kPairsPerThread; ++m) {
+    const long long i0 = base + 512LL * m;
+    if (i0 >= N) break;
+    const bool two = i0 + 1 < N;
+    double s0 = 0.0, s1 = 0.0, d0 = 1.0, d1 = 1.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const long long o = slot_off<D, P>(s, M);
+      const double2 a = __ldg(reinterpret_cast<const double2*>(A + (long long)s * Np + i0));
+      if (s == C) { d0 = a.x; d1 = a.y; }
+      const double x0 = __ldg(x + clampi(i0 + o, N));
+      const double x1 = __ldg(x + clampi(i0 + 1 + o, N));
+      s0 = fma(a.x, x0, s0);
+      s1 = fma(a.y, x1, s1);
+    }
+    {
+      const double t = (b[i0] - s0) / d0;
+      if (write_r) r[i0] = t;
+      const double xn = fma(omega ? omega[i0] : damp, t, x[i0]);
+      xout[i0] = xn;
+      if (DOT) acc = fma(xn, dv[i0], acc);
+    }
+    if (two) {
+      const double t = (b[i0 + 1] - s1) / d1;
+      if (write_r) r[i0 + 1] = t;
+      const double xn = fma(omega ? omega[i0 + 1] : damp, t, x[i0 + 1]);
+      xout[i0 + 1] = xn;
+      if (DOT) acc = fma(xn, dv[i0 + 1], acc);
+    }
+  }
+  if (DOT) dr_finish(acc, R, smem);
+}
+
+// one colour of the multicolour <sor> sweep: rows with (i_k mod (P+1)) = col_k
+template <int D, int P>
+__global__ void __launch_bounds__(kBlock)
+k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long M, int colour,
+             double omega_s, const double* __restrict__ omega, double* x, const double* b, double* r) {
+  constexpr int NS = St<D, P>::NS;
+  constexpr int C = St<D, P>::CENTER;
+  constexpr int Q = P + 1;
+  const int cx = colour % Q, cy = (colour / Q) % Q, cz = colour / (Q * Q);
+  const long long nx = (M - cx + Q - 1) / Q;
+  const long long ny = D > 1 ? (M - cy + Q - 1) / Q : 1;
+  const long long nz = D > 2 ? (M - cz + Q - 1) / Q : 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * ny * nz) return;
+  const long long jx = t % nx, jy = (t / nx) % ny, jz = t / (nx * ny);
+  const long long i = (cx + Q * jx) + M * ((D > 1 ? cy + Q * jy : 0) + M * (D > 2 ? cz + Q * jz : 0));
+  double s = 0.0, d = 1.0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const long long o = slot_off<D, P>(k, M);
+    const double a = A[(long long)k * Np + i];
+    if (k == C) d = a;
+    s = fma(a, x[clampi(i + o, N)], s);
+  }
+  const double tt = (b[i] - s) / d;
+  r[i] = tt;
+  x[i] = fma(omega ? omega[i] : omega_s, tt, x[i]);
+}
+
+// -------------------------------------------------------------- transfers
+template <int P>
+__device__ __forceinline__ int restrict_1d(long long J, long long* off, double* w) {
+  if (P == 1) { off[0] = -1; off[1] = 0; off[2] = 1; w[0] = 0.5; w[1] = 1.0; w[2] = 0.5; return 3; }
+  if ((J & 1) == 0) {
+    off[0] = -3; off[1] = -1; off[2] = 0; off[3] = 1; off[4] = 3;
+    w[0] = -0.125; w[1] = 0.375; w[2] = 1.0; w[3] = 0.375; w[4] = -0.125;
+    return 5;
+  }
+  off[0] = -1; off[1] = 0; off[2] = 1; w[0] = 0.75; w[1] = 1.0; w[2] = 0.75;
+  return 3;
+}
+
+template <int P>
+__device__ __forceinline__ int prolong_1d(long long I, long long* J, double* w) {
+  if ((I & 1) == 0) { J[0] = I / 2; w[0] = 1.0; return 1; }
+  if (P == 1) { J[0] = (I - 1) / 2; J[1] = (I + 1) / 2; w[0] = 0.5; w[1] = 0.5; return 2; }
+  const long long c = I / 4;
+  const double s = (double)(I - 4 * c) / 4.0;
+  J[0] = 2 * c; J[1] = 2 * c + 1; J[2] = 2 * c + 2;
+  w[0] = 2.0 * (s - 0.5) * (s - 1.0);
+  w[1] = 4.0 * s * (1.0 - s);
+  w[2] = 2.0 * s * (s - 0.5);
+  return 3;
+}
+
+// rc := I^T rf (constrained), rhs_c := rc, sol_c := 0 (restrict + its :after
+// methods for the correction scheme, multigrid.lisp:202-224)
+template <int D, int P>
+__global__ void __launch_bounds__(kBlock)
+k_restrict(long long NC, long long MC, long long MF, int dmask, const double* __restrict__ rf,
+           double* __restrict__ rc, double* __restrict__ rhsc, double* __restrict__ solc) {
+  const long long J = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= NC) return;
+  long long cJ[3];
+  node_coords(J, MC, D, cJ);
+  double acc = 0.0;
+  if (!node_dirichlet(cJ, MC, D, dmask)) {
+    long long off[3][5] = {{0}, {0}, {0}};
+    double w[3][5] = {{1.0}, {1.0}, {1.0}};
+    int cnt[3] = {1, 1, 1};
+    for (int k = 0; k < D; ++k) cnt[k] = restrict_1d<P>(cJ[k], off[k], w[k]);
+    for (int z = 0; z < cnt[2]; ++z)
+      for (int y = 0; y < cnt[1]; ++y)
+        for (int xx = 0; xx < cnt[0]; ++xx) {
+          long long fi[3] = {2 * cJ[0] + off[0][xx], 2 * cJ[1] + off[1][y], 2 * cJ[2] + off[2][z]};
+          bool in = true;
+          for (int k = 0; k < D; ++k) if (fi[k] < 0 || fi[k] >= MF) in = false;
+          if (!in || node_dirichlet(fi, MF, D, dmask)) continue;
+          double ww = w[0][xx];
+          if (D > 1) ww = ww * w[1][y];
+          if (D > 2) ww = ww * w[2][z];
+          acc = fma(ww, rf[fi[0] + MF * (fi[1] + MF * fi[2])], acc);
+        }
+  }
+  rc[J] = acc;
+  rhsc[J] = acc;
+  solc[J] = 0.0;
+}
+
+// xf := xf + I xc (constrained) (prolongate, multigrid.lisp:237-239)
+template <int D, int P>
+__global__ void __launch_bounds__(kBlock)
+k_prolong(long long NF, long long MF, long long MC, int dmask, const double* __restrict__ xc,
+          double* __restrict__ xf) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NF) return;
+  long long fi[3];
+  node_coords(i, MF, D, fi);
+  if (node_dirichlet(fi, MF, D, dmask)) return;
+  long long J[3][3] = {{0}, {0}, {0}};
+  double w[3][3] = {{1.0}, {1.0}, {1.0}};
+  int cnt[3] = {1, 1, 1};
+  for (int k = 0; k < D; ++k) cnt[k] = prolong_1d<P>(fi[k], J[k], w[k]);
+  double acc = 0.0;
+  for (int z = 0; z < cnt[2]; ++z)
+    for (int y = 0; y < cnt[1]; ++y)
+      for (int xx = 0; xx < cnt[0]; ++xx) {
+        const long long cj[3] = {J[0][xx], J[1][y], J[2][z]};
+        if (node_dirichlet(cj, MC, D, dmask)) continue;
+        double ww = w[0][xx];
+        if (D > 1) ww = ww * w[1][y];
+        if (D > 2) ww = ww * w[2][z];
+        acc = fma(ww, xc[cj[0] + MC * (cj[1] + MC * cj[2])], acc);
+      }
+  xf[i] = xf[i] + acc;
+}
+
+// -------------------------------------------------------------- coarse LU
+// Single-block dense LU with partial pivoting, row-major, in place.
+__global__ void __launch_bounds__(1024) k_lu_factor(double* A, int n, int* piv) {
+  __shared__ double bv[32];
+  __shared__ int bi[32];
+  __shared__ int pk_s;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int k = 0; k < n; ++k) {
+    double best = -1.0;
+    int besti = n;
+    for (int i = k + tid; i < n; i += nt) {
+      const double v = fabs(A[(long long)i * n + k]);
+      if (v > best || (v == best && i < besti)) { best = v; besti = i; }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+      if (ov > best || (ov == best && oi < besti)) { best = ov; besti = oi; }
+    }
+    if ((tid & 31) == 0) { bv[tid >> 5] = best; bi[tid >> 5] = besti; }
+    __syncthreads();
+    if (tid == 0) {
+      double b = bv[0];
+      int ib = bi[0];
+      for (int w = 1; w < (nt + 31) / 32; ++w)
+        if (bv[w] > b || (bv[w] == b && bi[w] < ib)) { b = bv[w]; ib = bi[w]; }
+      pk_s = ib;
+      piv[k] = ib;
+    }
+    __syncthreads();
+    const int pk = pk_s;
+    if (pk != k)
+      for (int j = tid; j < n; j += nt) {
+        const double t = A[(long long)k * n + j];
+        A[(long long)k * n + j] = A[(long long)pk * n + j];
+        A[(long long)pk * n + j] = t;
+      }
+    __syncthreads();
+    const double d = A[(long long)k * n + k];
+    for (int i = k + 1 + tid; i < n; i += nt) A[(long long)i * n + k] = A[(long long)i * n + k] / d;
+    __syncthreads();
+    const int m = n - k - 1;
+    for (long long idx = tid; idx < (long long)m * m; idx += nt) {
+      const int i = k + 1 + (int)(idx / m), j = k + 1 + (int)(idx % m);
+      A[(long long)i * n + j] = fma(-A[(long long)i * n + k], A[(long long)k * n + j], A[(long long)i * n + j]);
+    }
+    __syncthreads();
+  }
+}
+
+// Column j of A^-1 per thread, from the LU factors; X row-major (j fastest).
+__global__ void k_lu_inverse(const double* __restrict__ LU, const int* __restrict__ piv, int n, double* X) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int i = 0; i < n; ++i) X[(long long)i * n + j] = (i == j) ? 1.0 : 0.0;
+  for (int k = 0; k < n; ++k) {
+    const int p = piv[k];
+    if (p != k) {
+      const double t = X[(long long)k * n + j];
+      X[(long long)k * n + j] = X[(long long)p * n + j];
+      X[(long long)p * n + j] = t;
+    }
+  }
+  for (int k = 0; k < n; ++k) {
+    const double bk = X[(long long)k * n + j];
+    for (int i = k + 1; i < n; ++i) X[(long long)i * n + j] = fma(-LU[(long long)i * n + k], bk, X[(long long)i * n + j]);
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const double bk = X[(long long)k * n + j] / LU[(long long)k * n + k];
+    X[(long long)k * n + j] = bk;
+    for (int i = 0; i < k; ++i) X[(long long)i * n + j] = fma(-LU[(long long)i * n + k], bk, X[(long long)i * n + j]);
+  }
+}
+
+__global__ void k_transpose(const double* __restrict__ X, int n, double* __restrict__ XT) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const long long i = t / n, j = t % n;
+  XT[j * n + i] = X[i * n + j];
+}
+
+// <lu> coarse-grid iterator: r := A^-1 r, x := x + damp r (one block, n <= 1024)
+__global__ void __launch_bounds__(1024)
+k_coarse_solve(const double* __restrict__ AinvT, int n, double damp, double* x, double* r) {
+  __shared__ double rs[1024];
+  const int i = threadIdx.x;
+  if (i < n) rs[i] = r[i];
+  __syncthreads();
+  if (i >= n) return;
+  double acc = 0.0;
+  for (int j = 0; j < n; ++j) acc = fma(AinvT[(long long)j * n + i], rs[j], acc);
+  r[i] = acc;
+  x[i] = fma(damp, acc, x[i]);
+}
+
+// ------------------------------------------------------------ vector ops
+__global__ void k_fill(double* x, long long n, double v) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = v;
+}
+
+__global__ void k_copy(const double* __restrict__ x, double* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = x[i];
+}
+
+// axpy!: y := y + alpha x (alpha from a device slot when aslot >= 0)
+__global__ void k_axpy(double alpha, const double* __restrict__ sc, int aslot, const double* __restrict__ x,
+                       double* y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = aslot >= 0 ? sc[aslot] : alpha;
+  y[i] = fma(a, x[i], y[i]);
+}
+
+// DR4096 dot product (x, y)
+__global__ void __launch_bounds__(kBlock)
+k_dot(const double* __restrict__ x, const double* __restrict__ y, long long n, Reduce R) {
+  __shared__ double smem[8];
+  const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
+  double acc = 0.0;
+#pragma unroll
+  for (int m = 0; m < kPairsPerThread; ++m) {
+    const long long i0 = base + 512LL * m;
+    if (i0 < n) acc = fma(x[i0], y[i0], acc);
+    if (i0 + 1 < n) acc = fma(x[i0 + 1], y[i0 + 1], acc);
+  }
+  dr_finish(acc, R, smem);
+}
+
+// CG update (krylow.lisp:117-121): x += lam p; r -= lam a; fused (r,r);
+// then w := r and (optionally) w2 := r, q := 0 for the preconditioner call
+__global__ void __launch_bounds__(kBlock)
+k_cg_update(const double* __restrict__ sc, double* __restrict__ x, const double* __restrict__ p,
+            double* __restrict__ r, const double* __restrict__ a, double* __restrict__ w,
+            double* __restrict__ w2, double* __restrict__ q, long long n, Reduce R) {
+  __shared__ double smem[8];
+  const double lam = sc[S_LAM], nlam = sc[S_NEGLAM];
+  const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 2
+  for (int m = 0; m < kPairsPerThread; ++m) {
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const long long i = base + 512LL * m + u;
+      if (i < n) {
+        x[i] = fma(lam, p[i], x[i]);
+        const double rn = fma(nlam, a[i], r[i]);
+        r[i] = rn;
+        acc = fma(rn, rn, acc);
+        if (w) w[i] = rn;
+        if (w2) w2[i] = rn;
+        if (q) q[i] = 0.0;
+      }
+    }
+  }
+  dr_finish(acc, R, smem);
+}
+
+// p := (new_alpha/alpha) p (scal!), then p := p + q (m+!)
+__global__ void k_p_update(const double* __restrict__ sc, double* __restrict__ p, const double* __restrict__ q,
+                           long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double t = sc[S_RATIO] * p[i];
+  p[i] = t + q[i];
+}
+
+// -------------------------------------------------------------- assembly
+// Gauss-point samples of a cell-wise coefficient for a coarse level:
+// kq[c * nq + q] = kcell[top cell containing the q-th Gauss point of c]
+template <int D>
+__global__ void k_sample_kq(long long ncells_l, long long n_l, long long n_top, double ratio, int np,
+                            const double* __restrict__ xi, const double* __restrict__ kcell,
+                            double* __restrict__ kq) {
+  int nq = 1;
+  for (int k = 0; k < D; ++k) nq *= np;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncells_l * nq) return;
+  const long long c = t / nq;
+  const int q = (int)(t % nq);
+  const long long cc[3] = {c % n_l, D > 1 ? (c / n_l) % n_l : 0, D > 2 ? c / (n_l * n_l) : 0};
+  const int qi[3] = {q % np, (q / np) % np, q / (np * np)};
+  long long f[3] = {0, 0, 0};
+  for (int k = 0; k < D; ++k) f[k] = (long long)floor(((double)cc[k] + xi[qi[k]]) * ratio);
+  kq[t] = kcell[f[0] + n_top * (f[1] + n_top * f[2])];
+}
+
+// Stiffness entries by gather: for node i and slot s with neighbour j, the
+// sum over the cells containing both nodes, in increasing cell index, of the
+// local matrix entry (assemble-interior + global-local-matrix-operation,
+// fedisc.lisp:73-206, sparseif.lisp:308-385).  Dirichlet rows become identity
+// rows and Dirichlet columns are dropped (S A S + P).  On the top level the
+// right-hand side is gathered the same way.
+template <int D, int P>
+__global__ void __launch_bounds__(kBlock)
+k_assemble(AsmArgs g) {
+  constexpr int NS = St<D, P>::NS;
+  constexpr int C = St<D, P>::CENTER;
+  constexpr int W = 2 * P + 1;
+  constexpr int P1 = P + 1;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  long long ci[3];
+  node_coords(i, g.M, D, ci);
+  if (node_dirichlet(ci, g.M, D, g.dmask)) {
+    for (int s = 0; s < NS; ++s) g.A[(long long)s * g.Np + i] = (s == C) ? 1.0 : 0.0;
+    if (g.rhs) g.rhs[i] = 0.0;
+    return;
+  }
+  const int nl = g.nl, nq = g.nq;
+  for (int s = 0; s < NS; ++s) {
+    long long o[3] = {s % W - P, D > 1 ? (s / W) % W - P : 0, D > 2 ? (s / (W * W)) % W - P : 0};
+    long long cj[3], lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) cj[k] = ci[k] + o[k];
+    for (int k = 0; k < D; ++k) {
+      if (cj[k] < 0 || cj[k] >= g.M) ok = false;
+      const long long mx = ci[k] > cj[k] ? ci[k] : cj[k];
+      const long long mn = ci[k] < cj[k] ? ci[k] : cj[k];
+      lo[k] = mx >= P ? (mx - 1) / P : 0;
+      hi[k] = mn / P;
+      if (hi[k] > g.n - 1) hi[k] = g.n - 1;
+    }
+    double v = 0.0;
+    if (ok && !node_dirichlet(cj, g.M, D, g.dmask)) {
+      for (long long cz = lo[2]; cz <= hi[2]; ++cz)
+        for (long long cy = lo[1]; cy <= hi[1]; ++cy)
+          for (long long cx = lo[0]; cx <= hi[0]; ++cx) {
+            const long long cc[3] = {cx, cy, cz};
+            const long long cidx = cx + g.n * (cy + g.n * cz);
+            int a = 0, b = 0, mul = 1;
+            for (int k = 0; k < D; ++k) {
+              a += (int)(ci[k] - P * cc[k]) * mul;
+              b += (int)(cj[k] - P * cc[k]) * mul;
+              mul *= P1;
+            }
+            double e;
+            if (g.kq == nullptr) {
+              const double kc = g.kcell ? g.kcell[cidx] : g.kconst;
+              e = kc * g.Kbar[a * nl + b];
+            } else {
+              e = 0.0;
+              for (int q = 0; q < nq; ++q)
+                e = fma(g.kq[cidx * nq + q], g.Ctab[((long long)q * nl + a) * nl + b], e);
+            }
+            v = v + e;
+          }
+    }
+    g.A[(long long)s * g.Np + i] = v;
+  }
+  if (g.rhs) {
+    long long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int k = 0; k < D; ++k) {
+      lo[k] = ci[k] >= P ? (ci[k] - 1) / P : 0;
+      hi[k] = ci[k] / P;
+      if (hi[k] > g.n - 1) hi[k] = g.n - 1;
+    }
+    double acc = 0.0;
+    for (long long cz = lo[2]; cz <= hi[2]; ++cz)
+      for (long long cy = lo[1]; cy <= hi[1]; ++cy)
+        for (long long cx = lo[0]; cx <= hi[0]; ++cx) {
+          const long long cc[3] = {cx, cy, cz};
+          const long long cidx = cx + g.n * (cy + g.n * cz);
+          int a = 0, mul = 1;
+          for (int k = 0; k < D; ++k) { a += (int)(ci[k] - P * cc[k]) * mul; mul *= P1; }
+          double bl = 0.0;
+          for (int q = 0; q < nq; ++q) {
+            const double f = g.fip ? g.fip[cidx * nq + q] : g.fconst;
+            bl = fma(f, g.Phi[q * nl + a], bl);
+          }
+          acc = acc + bl;
+        }
+    g.rhs[i] = acc;
+  }
+}
+
+// ---------------------------------------------------------- dispatchers
+#define FMG_DISPATCH(D_, P_, ...)                                             \
+  do {                                                                        \
+    if ((D_) == 1 && (P_) == 1) { constexpr int D = 1, P = 1; __VA_ARGS__; }  \
+    else if ((D_) == 2 && (P_) == 1) { constexpr int D = 2, P = 1; __VA_ARGS__; } \
+    else if ((D_) == 3 && (P_) == 1) { constexpr int D = 3, P = 1; __VA_ARGS__; } \
+    else if ((D_) == 1 && (P_) == 2) { constexpr int D = 1, P = 2; __VA_ARGS__; } \
+    else if ((D_) == 2 && (P_) == 2) { constexpr int D = 2, P = 2; __VA_ARGS__; } \
+    else { constexpr int D = 3, P = 2; __VA_ARGS__; }                         \
+  } while (0)
+
+static inline unsigned grid1(long long n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
+
+void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
+                 const Reduce* R, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const unsigned g = nchunks(L.N);
+  Reduce r0 = R ? *R : Reduce{};
+  FMG_DISPATCH(L.dim, L.order, {
+    if (b && dv) k_spmv<D, P, true, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+    else if (b) k_spmv<D, P, true, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+    else if (dv) k_spmv<D, P, false, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+    else k_spmv<D, P, false, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+  });
+}
+
+void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const double* Dg = L.A + (long long)L.center * L.Np;
+  k_jacobi<<<grid1(L.N), kBlock, 0, st>>>(Dg, L.N, damp, L.omega, x, r, write_r ? 1 : 0);
+}
+
+void launch_jacobi_res(const LevelView& L, double damp, const double* x, const double* b, double* xout,
+                       double* r, bool write_r, const double* dv, const Reduce* R, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const unsigned g = nchunks(L.N);
+  Reduce r0 = R ? *R : Reduce{};
+  FMG_DISPATCH(L.dim, L.order, {
+    if (dv) k_jacobi_res<D, P, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+                                                             write_r ? 1 : 0, dv, r0);
+    else k_jacobi_res<D, P, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+                                                         write_r ? 1 : 0, dv, r0);
+  });
+}
+
+void launch_sor(const LevelView& L, double omega, double* x, const double* b, double* r, cudaStream_t st) {
+  int Q = L.order + 1, ncol = 1;
+  for (int k = 0; k < L.dim; ++k) ncol *= Q;
+  g_launches.fetch_add(ncol, std::memory_order_relaxed);
+  for (int col = 0; col < ncol; ++col) {
+    const int cx = col % Q, cy = (col / Q) % Q, cz = col / (Q * Q);
+    long long cnt = (L.M - cx + Q - 1) / Q;
+    if (L.dim > 1) cnt *= (L.M - cy + Q - 1) / Q;
+    if (L.dim > 2) cnt *= (L.M - cz + Q - 1) / Q;
+    FMG_DISPATCH(L.dim, L.order, {
+      k_sor_colour<D, P><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, L.omega, x, b, r);
+    });
+  }
+}
+
+void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, double* rc, double* rhsc,
+                     double* solc, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  FMG_DISPATCH(F.dim, F.order, {
+    k_restrict<D, P><<<grid1(Cl.N), kBlock, 0, st>>>(Cl.N, Cl.M, F.M, F.dmask, rf, rc, rhsc, solc);
+  });
+}
+
+void launch_prolong(const LevelView& Cl, const LevelView& F, const double* xc, double* xf, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  FMG_DISPATCH(F.dim, F.order, {
+    k_prolong<D, P><<<grid1(F.N), kBlock, 0, st>>>(F.N, F.M, Cl.M, F.dmask, xc, xf);
+  });
+}
+
+void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_coarse_solve<<<1, 1024, 0, st>>>(AinvT, n, damp, x, r);
+}
+
+void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t st) {
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  k_lu_factor<<<1, 1024, 0, st>>>(A, n, piv);
+  k_lu_inverse<<<grid1(n, 64), 64, 0, st>>>(A, piv, n, X);
+  k_transpose<<<grid1((long long)n * n), kBlock, 0, st>>>(X, n, XT);
+}
+
+void launch_fill(double* x, long long n, double v, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (n > 0) k_fill<<<grid1(n), kBlock, 0, st>>>(x, n, v);
+}
+void launch_copy(const double* x, double* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (n > 0) k_copy<<<grid1(n), kBlock, 0, st>>>(x, y, n);
+}
+void launch_axpy(double alpha, const double* sc, int aslot, const double* x, double* y, long long n,
+                 cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (n > 0) k_axpy<<<grid1(n), kBlock, 0, st>>>(alpha, sc, aslot, x, y, n);
+}
+void launch_dot(const double* x, const double* y, long long n, const Reduce& R, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_dot<<<nchunks(n), kBlock, 0, st>>>(x, y, n, R);
+}
+void launch_cg_update(const double* sc, double* x, const double* p, double* r, const double* a, double* w,
+                      double* w2, double* q, long long n, const Reduce& R, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_cg_update<<<nchunks(n), kBlock, 0, st>>>(sc, x, p, r, a, w, w2, q, n, R);
+}
+void launch_p_update(const double* sc, double* p, const double* q, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_p_update<<<grid1(n), kBlock, 0, st>>>(sc, p, q, n);
+}
+
+void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_top, double ratio, int np,
+                      const double* xi, const double* kcell, double* kq, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  long long nq = 1;
+  for (int k = 0; k < dim; ++k) nq *= np;
+  const unsigned g = grid1(ncells_l * nq);
+  if (dim == 1) k_sample_kq<1><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
+  else if (dim == 2) k_sample_kq<2><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
+  else k_sample_kq<3><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
+}
+
+void launch_assemble(int dim, int order, const AsmArgs& a, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  FMG_DISPATCH(dim, order, { k_assemble<D, P><<<grid1(a.N), kBlock, 0, st>>>(a); });
+}
+
+}  // namespace fmg
+
+namespace fmg {
+
+// dense row-major copy of a (small) level matrix, for the coarse LU
+template <int D, int P>
+__global__ void k_densify(const double* __restrict__ A, long long N, long long Np, long long M,
+                          double* __restrict__ Dm) {
+  constexpr int NS = St<D, P>::NS;
+  constexpr int W = 2 * P + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N * NS) return;
+  const long long i = t / NS;
+  const int s = (int)(t % NS);
+  long long ci[3];
+  node_coords(i, M, D, ci);
+  const long long o[3] = {s % W - P, D > 1 ? (s / W) % W - P : 0, D > 2 ? (s / (W * W)) % W - P : 0};
+  long long cj[3];
+  for (int k = 0; k < 3; ++k) cj[k] = ci[k] + o[k];
+  for (int k = 0; k < D; ++k) if (cj[k] < 0 || cj[k] >= M) return;
+  const long long j = cj[0] + M * (cj[1] + M * cj[2]);
+  Dm[i * N + j] = A[(long long)s * Np + i];
+}
+
+void launch_densify(const LevelView& L, double* Dm, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  FMG_DISPATCH(L.dim, L.order, {
+    constexpr int NS = St<D, P>::NS;
+    k_densify<D, P><<<grid1(L.N * NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);
+  });
+}
+
+}  // namespace fmg

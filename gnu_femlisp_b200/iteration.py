@@ -1,0 +1,308 @@
+"""Host-side mirror of Femlisp's problem, discretization and iteration API
+for the multigrid solve path, running on the B200 through libfmgpu.
+
+The names and meanings follow the reference so that code written against
+Femlisp reads the same here:
+
+  cdr_model_problem                 src/problem/cdr.lisp:153-204
+  uniformly_refined_hierarchical_mesh  src/mesh/meshgen.lisp:180-183
+  lagrange_fe                       src/discretization/lagrange.lisp:176-202
+  discretize_globally               src/discretization/fedisc.lisp:307-316
+  Jacobi, SOR, GaussSeidel, LU      src/iteration/linit.lisp:132-385
+  geometric_cs / GeometricCS        src/iteration/geomg.lisp:148-155,
+                                    multigrid.lisp:55-70
+  CG                                src/iteration/krylow.lisp:67-132
+  LinearSolver, solve               src/iteration/linsolve.lisp:40-73,
+                                    solve.lisp:113-164, iterate.lisp:105-250
+
+Success/failure conditions are given as Femlisp forms, e.g.
+``"(or (< :defnorm 1.0e-12) (> :step 10))"``.  Coefficients are sampled on
+the host (a Lisp coefficient closure cannot run on the device): diffusion
+as a constant or one value per top-level cell, source as a constant or its
+values at the Gauss points of every top-level cell.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Any, Callable
+
+import numpy as np
+
+from . import _capi as C
+from .core import Context, Grid, Vector
+
+# ------------------------------------------------------------------ problem
+
+
+@dataclass
+class CdrProblem:
+    """-div(k grad u) = f on the unit dim-cube with Dirichlet data 0 on the
+    faces in ``dirichlet_mask`` (cdr-model-problem defaults: k = 1, f = 1,
+    u = 0 on the whole boundary)."""
+    dim: int
+    diffusion: Any = 1.0           # float, or array of per-cell values, or callable(x) -> k
+    source: Any = 1.0              # float, or callable(x) -> f evaluated at Gauss points
+    dirichlet_mask: int | None = None
+
+
+def cdr_model_problem(dim: int, diffusion=None, source=None, dirichlet_mask=None) -> CdrProblem:
+    return CdrProblem(dim, 1.0 if diffusion is None else diffusion, 1.0 if source is None else source,
+                      dirichlet_mask)
+
+
+@dataclass
+class Mesh:
+    """Uniformly refined hierarchical mesh of the unit n-cube: level l has
+    n0 * 2^l cells per direction."""
+    dim: int
+    level: int
+    n0: int = 1
+
+
+def uniformly_refined_hierarchical_mesh(dim: int, level: int, n0: int = 1) -> Mesh:
+    return Mesh(dim, level, n0)
+
+
+@dataclass
+class LagrangeFE:
+    order: int
+    nr_comps: int = 1
+
+
+def lagrange_fe(order: int, nr_comps: int = 1) -> LagrangeFE:
+    return LagrangeFE(order, nr_comps)
+
+
+def gauss_points_1d(order: int) -> np.ndarray:
+    """Gauss points on [0,1] in the order of the quadrature rule
+    (quadrature.lisp:202-215): (1 - t)/2 for ascending Legendre roots t."""
+    if order == 1:
+        t = math.sqrt(1.0 / 3.0)
+        ts = [-t, t]
+    else:
+        t = math.sqrt(0.6)
+        ts = [-t, 0.0, t]
+    return np.array([0.5 * (1.0 - v) for v in ts])
+
+
+def sample_at_gauss_points(f: Callable[[np.ndarray], np.ndarray], dim: int, order: int,
+                           n_cells: int) -> np.ndarray:
+    """Values of f at the Gauss points of every cell, layout [cell][q] with
+    cells and points numbered x fastest; f maps points [..., dim] to values."""
+    xi = gauss_points_1d(order)
+    npt = len(xi)
+    h = 1.0 / n_cells
+    c = np.arange(n_cells ** dim)[:, None]
+    q = np.arange(npt ** dim)[None, :]
+    pts = [((c // n_cells ** k) % n_cells + xi[(q // npt ** k) % npt]) * h for k in range(dim)]
+    return np.ascontiguousarray(f(np.stack(pts, axis=-1))).reshape(-1)
+
+
+def cell_centres(dim: int, n_cells: int) -> np.ndarray:
+    """Cell midpoints [cell, dim], cells numbered x fastest."""
+    c = np.arange(n_cells ** dim)
+    return np.stack([((c // n_cells ** k) % n_cells + 0.5) / n_cells for k in range(dim)], axis=-1)
+
+
+class DiscreteSystem:
+    """The assembled system A x = b of discretize_globally.  The level
+    hierarchy is assembled on the device lazily, once per coarse level a
+    solver asks for (the reference assembles coarse levels when the
+    multigrid iterator is made, geomg.lisp:109-142)."""
+
+    def __init__(self, problem: CdrProblem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
+        if fe.nr_comps != 1:
+            raise NotImplementedError("vector-valued problems are not built yet")
+        self.problem, self.mesh, self.fe = problem, mesh, fe
+        self.ctx = ctx or Context()
+        self._grids: dict[int, Grid] = {}
+
+    def grid(self, base_level: int = 0) -> Grid:
+        if base_level not in self._grids:
+            p, m = self.problem, self.mesh
+            g = Grid(self.ctx, p.dim, self.fe.order, m.level, base_level=base_level, n0=m.n0,
+                     dirichlet_mask=p.dirichlet_mask)
+            ncell = g.n_cells
+            k = p.diffusion
+            if callable(k):
+                g.set_coefficient(C.FMG_K_CELL, np.ascontiguousarray(k(cell_centres(p.dim, ncell))).ravel())
+            elif np.ndim(k) == 0:
+                g.set_coefficient(C.FMG_K_CONST, [float(k)])
+            else:
+                g.set_coefficient(C.FMG_K_CELL, np.asarray(k, dtype=np.float64).ravel())
+            f = p.source
+            if callable(f):
+                g.set_coefficient(C.FMG_F_IP, sample_at_gauss_points(f, p.dim, self.fe.order, ncell))
+            else:
+                g.set_coefficient(C.FMG_F_CONST, [float(f)])
+            self._grids[base_level] = g.assemble()
+        return self._grids[base_level]
+
+
+def discretize_globally(problem: CdrProblem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
+    """Returns (A, b) like Femlisp; here A is the DiscreteSystem and b its
+    assembled right-hand side on the host."""
+    sysm = DiscreteSystem(problem, mesh, fe, ctx)
+    return sysm, sysm.grid(0).rhs()
+
+
+# ---------------------------------------------------------------- iterations
+
+
+@dataclass
+class Jacobi:
+    damp: float = 1.0
+
+
+@dataclass
+class SOR:
+    omega: float = 1.0
+
+
+class GaussSeidel(SOR):
+    def __init__(self):
+        super().__init__(1.0)
+
+
+@dataclass
+class LU:
+    damp: float = 1.0
+
+
+@dataclass
+class GeometricCS:
+    smoother: Any = None
+    pre_steps: int = 1
+    post_steps: int = 1
+    gamma: int = 1
+    base_level: int = 0
+    coarse_grid_iteration: Any = None
+    combination: str = "multiplicative"
+
+
+def geometric_cs(**kw) -> GeometricCS:
+    return GeometricCS(**kw)
+
+
+@dataclass
+class CG:
+    preconditioner: Any = None
+    # True: call the preconditioner as (iterate q w w), rhs and residual
+    # aliased exactly as krylow.lisp:120 does; False: a separate residual.
+    compat_alias: bool = False
+
+
+# ------------------------------------------------------------ solver forms
+
+def _parse_form(text: str):
+    toks = text.replace("(", " ( ").replace(")", " ) ").split()
+
+    def rd(i):
+        if toks[i] == "(":
+            out, i = [], i + 1
+            while toks[i] != ")":
+                e, i = rd(i)
+                out.append(e)
+            return out, i + 1
+        t = toks[i]
+        try:
+            return float(t), i + 1
+        except ValueError:
+            return t.lower(), i + 1
+
+    form, _ = rd(0)
+    return form
+
+
+def _conditions(form) -> dict:
+    """Flatten (or (< :defnorm a) (< :reduction b) (> :step n)) into bounds."""
+    out: dict = {}
+    if isinstance(form, str):
+        form = _parse_form(form)
+    if not form:
+        return out
+    if form[0] == "or":
+        for f in form[1:]:
+            out.update(_conditions(f))
+        return out
+    op, key, val = form
+    if op == "<" and key == ":defnorm":
+        out["atol"] = val
+    elif op == "<" and key == ":reduction":
+        out["rtol"] = val
+    elif op in (">", ">=") and key == ":step":
+        out["maxsteps"] = int(val) if op == ">" else int(val) - 1
+    else:
+        raise ValueError(f"unsupported condition {form}")
+    return out
+
+
+@dataclass
+class LinearSolver:
+    iteration: Any
+    success_if: str = "(< :reduction 1.0e-10)"
+    failure_if: str = "(> :step 100)"
+    output: bool = False
+
+
+@dataclass
+class SolveReport:
+    status: str
+    steps: int
+    history: np.ndarray
+    convergence_rate: float
+    extra: dict = field(default_factory=dict)
+
+
+def make_cfg(iteration, success_if: str, failure_if: str) -> tuple[C.SolveCfg, int, bool]:
+    cs = iteration.preconditioner if isinstance(iteration, CG) else iteration
+    cfg = C.SolveCfg()
+    if isinstance(iteration, CG):
+        cfg.method = C.FMG_METHOD_CG_MG if cs is not None else C.FMG_METHOD_CG
+        cfg.compat_alias = 1 if iteration.compat_alias else 0
+    else:
+        cfg.method = C.FMG_METHOD_MG
+    base = 0
+    if cs is not None:
+        sm = cs.smoother or GaussSeidel()
+        if isinstance(sm, Jacobi):
+            cfg.smoother, cfg.damp = C.FMG_JACOBI, sm.damp
+        elif isinstance(sm, SOR):
+            cfg.smoother, cfg.damp = C.FMG_SOR, sm.omega
+        else:
+            raise NotImplementedError(f"smoother {sm!r}")
+        cfg.pre_steps, cfg.post_steps, cfg.gamma = cs.pre_steps, cs.post_steps, cs.gamma
+        cfg.combination = C.FMG_ADDITIVE if cs.combination == "additive" else C.FMG_MULTIPLICATIVE
+        cgi = cs.coarse_grid_iteration or LU()
+        if not isinstance(cgi, LU):
+            raise NotImplementedError("only the <lu> coarse-grid iteration is built")
+        cfg.coarse_damp = cgi.damp
+        base = cs.base_level
+    succ, fail = _conditions(success_if), _conditions(failure_if)
+    cfg.rtol = succ.get("rtol", 0.0)
+    cfg.atol = succ.get("atol", 0.0)
+    step_success = "maxsteps" in succ
+    cfg.maxsteps = succ.get("maxsteps", fail.get("maxsteps", 100))
+    return cfg, base, step_success
+
+
+def solve(blackboard: dict) -> dict:
+    """(solve (blackboard :matrix A :rhs b :solver solver)) -- returns the
+    blackboard with :solution, :report and :history filled in."""
+    A: DiscreteSystem = blackboard["matrix"]
+    solver: LinearSolver = blackboard["solver"]
+    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if)
+    g = A.grid(base)
+    x = g.vector()
+    if "solution" in blackboard and blackboard["solution"] is not None:
+        x.set(blackboard["solution"])
+    hist, steps, status = g.solve(cfg, x)
+    st = "success" if (status == 0 or step_success) else "failure"
+    red = hist[-1] / hist[0] if hist[0] != 0 else 0.0
+    rate = red ** (1.0 / steps) if steps > 0 else float("nan")
+    out = dict(blackboard)
+    out["solution"] = x.get()
+    out["history"] = hist
+    out["report"] = SolveReport(st, steps, hist, rate)
+    return out

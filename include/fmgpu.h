@@ -1,0 +1,177 @@
+/*
+ * fmgpu.h -- C-ABI of libfmgpu.so, the B200 (sm_100a) multigrid solve path
+ * behind Femlisp's Lisp-level iteration API.
+ *
+ * Style follows Femlisp's foreign interface (interface/superlu.c:51-88,
+ * interface/umfpack.c:44-77, bound by src/alien/superlu.lisp:57-75 through
+ * fl.port:def-function, src/basic/port.lisp:442-547): plain C functions of
+ * ints, longs, doubles and pointers that return an int status
+ * (0 = FMG_OK, negative = error).  Handles are opaque.  Host arrays passed in
+ * are read or written during the call only and never retained.  A context
+ * serialises all its work on one CUDA stream and must be used from one host
+ * thread at a time.  Device faults are returned as status codes, never as
+ * aborts; fmg_last_error() gives the message of the last failure.
+ *
+ * Grids are Femlisp's uniformly refined hierarchical meshes of the unit
+ * n-cube (src/mesh/meshgen.lisp:180-183: level l has n0*2^l cells per
+ * direction) with a Lagrange Q1/Q2 ansatz space (lagrange.lisp:176-202).
+ * Nodes are numbered lexicographically, x fastest; a level matrix is stored by
+ * stencil slot (slot s = sum_k (o_k + order) (2 order + 1)^k for the node
+ * offset o), the structured form of Femlisp's key-indexed <sparse-matrix>
+ * (src/matlisp/sparse-matrix.lisp:49,703-840).
+ */
+#ifndef FMGPU_H
+#define FMGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define FMG_OK 0
+#define FMG_ERR_ARG (-1)        /* invalid argument or size */
+#define FMG_ERR_CUDA (-2)       /* CUDA runtime error (message in fmg_last_error) */
+#define FMG_ERR_STATE (-3)      /* call out of order (e.g. solve before assemble) */
+#define FMG_ERR_NOMEM (-4)      /* device allocation failed */
+#define FMG_ERR_NUMERIC (-5)    /* NaN/Inf met in a residual norm */
+#define FMG_ERR_UNSUPPORTED (-6)
+#define FMG_ERR_IO (-7)         /* bad or corrupted file */
+
+/* ------------------------------------------------------ coefficient kinds */
+#define FMG_K_CONST 0           /* scalar diffusion k, n = 1 (default 1.0) */
+#define FMG_K_CELL 1            /* k per top-level cell, n = cells; coarse levels
+                                   sample it at their own Gauss points */
+#define FMG_F_CONST 2           /* constant source, n = 1 (default 1.0) */
+#define FMG_F_IP 3              /* source at the Gauss points of every top-level
+                                   cell, n = cells * (order+1)^dim */
+
+/* ------------------------------------------------------------ iteration */
+#define FMG_JACOBI 0            /* <jacobi> :damp (linit.lisp:220-250) */
+#define FMG_SOR 1               /* <sor> :omega, colour ordering (linit.lisp:288-323) */
+
+#define FMG_METHOD_MG 0         /* <linear-solver> :iteration <geometric-cs> */
+#define FMG_METHOD_CG_MG 1      /* <cg> :preconditioner <geometric-cs> */
+#define FMG_METHOD_CG 2         /* <cg> without preconditioner */
+
+#define FMG_MULTIPLICATIVE 0    /* :combination (multigrid.lisp:67-70) */
+#define FMG_ADDITIVE 1
+
+typedef struct fmg_ctx fmg_ctx;
+typedef struct fmg_grid fmg_grid;
+typedef struct fmg_vec fmg_vec;
+
+/* Solver configuration: the initargs of <geometric-cs> (multigrid.lisp:55-70,
+   geomg.lisp:148-155), <cg> (krylow.lisp:67-70) and the success/failure
+   forms of <linear-solver> (iterate.lisp:105-123). */
+typedef struct {
+  int method;          /* FMG_METHOD_* */
+  int smoother;        /* FMG_JACOBI or FMG_SOR */
+  double damp;         /* :damp of <jacobi>, :omega of <sor> */
+  int pre_steps, post_steps, gamma;
+  int compat_alias;    /* 1: the preconditioner is called as (iterate q w w),
+                          rhs and residual aliased (krylow.lisp:120) */
+  double coarse_damp;  /* :damp of the <lu> coarse-grid iteration (1.0) */
+  double rtol;         /* success if :reduction < rtol (<= 0: off) */
+  double atol;         /* success if :defnorm < atol (<= 0: off) */
+  int maxsteps;        /* failure if :step > maxsteps */
+  int combination;     /* FMG_MULTIPLICATIVE or FMG_ADDITIVE */
+} fmg_solve_cfg;
+
+/* ------------------------------------------------------------- context */
+/* Opens device `device` (load-foreign-library, port.lisp:360-379, plus the
+   state the Lisp side keeps).  */
+int fmg_init(int device, fmg_ctx** ctx);
+int fmg_finalize(fmg_ctx* ctx);
+/* Copies the message of the last failure (NUL-terminated) into buf. */
+int fmg_last_error(fmg_ctx* ctx, char* buf, int len);
+int fmg_synchronize(fmg_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all work of ctx is queued on. */
+int fmg_get_stream(fmg_ctx* ctx, void** stream);
+/* Number of kernels this library has launched in this process (diagnostics;
+   no counterpart in the reference). */
+int fmg_launch_count(long long* out);
+
+/* ---------------------------------------------------------------- grids */
+/* A level hierarchy base_level..top_level of the uniformly refined unit
+   n-cube (uniformly-refined-hierarchical-mesh, meshgen.lisp:180-183) with
+   Lagrange order `order` (lagrange-fe, lagrange.lisp:176-202) and `ncomp`
+   components.  dirichlet_mask bit 2k / 2k+1 marks the face x_k = 0 / 1 as
+   essential boundary (the :external-boundary constraint coefficient,
+   cdr.lisp:184-185). */
+int fmg_grid_create(fmg_ctx* ctx, int dim, int order, int ncomp, int n0, int top_level,
+                    int base_level, int dirichlet_mask, fmg_grid** grid);
+int fmg_grid_destroy(fmg_grid* grid);
+long fmg_grid_nnodes(const fmg_grid* grid, int level);
+int fmg_grid_nslots(const fmg_grid* grid);
+
+/* Coefficients of the cdr model problem (cdr-model-problem, cdr.lisp:153-204):
+   diffusion k and source f, sampled by the host (Lisp coefficient closures
+   cannot run on the device). */
+int fmg_set_coefficient(fmg_grid* grid, int kind, const double* host, long n);
+
+/* Cell-wise Lagrange stiffness assembly of every level, with the Dirichlet
+   rows turned into identity rows, and the dense LU of the base level:
+   assemble-interior (fedisc.lisp:108-206) for the top level (:surface) and
+   for each coarse level (:refined, geomg.lisp:109-142), eliminate-constraints
+   + m+! P (constraints.lisp:323-411, fedisc.lisp:244-253, geomg.lisp:128-137),
+   and getrf! of the <lu> coarse-grid iteration (linit.lisp:137-151). */
+int fmg_assemble(fmg_grid* grid);
+/* Level matrix to the host, layout [slot][node] (debug / parity). */
+int fmg_get_matrix(fmg_grid* grid, int level, double* host);
+/* Top-level right-hand side (the assembled rhs of discretize-globally,
+   fedisc.lisp:307-316). */
+int fmg_get_rhs(fmg_grid* grid, double* host);
+/* Per-node Jacobi/SOR damping on a level (NULL resets to the scalar :damp). */
+int fmg_set_node_damping(fmg_grid* grid, int level, const double* host, long n);
+
+/* -------------------------------------------------------------- vectors */
+/* A device vector on a level (make-domain-vector-for, sparse-vector.lisp:53-58). */
+int fmg_vec_create(fmg_grid* grid, int level, fmg_vec** vec);
+int fmg_vec_destroy(fmg_vec* vec);
+int fmg_vec_set(fmg_vec* vec, const double* host, long n);
+int fmg_vec_get(const fmg_vec* vec, double* host, long n);
+/* fill! / x<-0 (vector.lisp:224) */
+int fmg_vec_fill(fmg_vec* vec, double value);
+/* copy! (vector.lisp:304-312, sparse-vector.lisp:248-258) */
+int fmg_copy(const fmg_vec* x, fmg_vec* y);
+/* axpy! y := y + alpha x (vector.lisp:321-326) */
+int fmg_axpy(double alpha, const fmg_vec* x, fmg_vec* y);
+/* dot (sparse-vector.lisp:260-264), deterministic chunked reduction */
+int fmg_dot(const fmg_vec* x, const fmg_vec* y, double* out);
+/* l2-norm (vector.lisp:328-331) */
+int fmg_l2_norm(const fmg_vec* x, double* out);
+
+/* ------------------------------------------------------------ operators */
+/* gemm! 1.0 A x 0.0 y on level `level` (sparse-matrix.lisp:392-405) */
+int fmg_matvec(fmg_grid* grid, int level, const fmg_vec* x, fmg_vec* y);
+/* compute-residual r := b - A x (linit.lisp:73-80); b may be r */
+int fmg_residual(fmg_grid* grid, int level, const fmg_vec* x, const fmg_vec* b, fmg_vec* r);
+/* restrict: rc := I^T rf with the constrained interpolation
+   (multigrid.lisp:202-212, constraints.lisp:58-72) */
+int fmg_restrict(fmg_grid* grid, int fine_level, const fmg_vec* rf, fmg_vec* rc);
+/* prolongate: xf := xf + I xc (multigrid.lisp:237-239) */
+int fmg_prolongate(fmg_grid* grid, int coarse_level, const fmg_vec* xc, fmg_vec* xf);
+/* one <jacobi> step: r := D^-1 r, x := x + damp r (linit.lisp:220-250) */
+int fmg_jacobi(fmg_grid* grid, int level, double damp, fmg_vec* x, fmg_vec* r);
+/* one multicolour <sor> sweep (linit.lisp:288-323); b may be r */
+int fmg_sor(fmg_grid* grid, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r);
+/* the <lu> coarse-grid iteration on the base level: r := A^-1 r,
+   x := x + damp r (linit.lisp:156-161) */
+int fmg_coarse_solve(fmg_grid* grid, double damp, fmg_vec* x, fmg_vec* r);
+
+/* ------------------------------------------------------------- solvers */
+/* One application of the <geometric-cs> iterator (multigrid.lisp:366-386) on
+   the top level.  Passing the same vector as b and r reproduces the alias of
+   the <cg> preconditioner call (krylow.lisp:120). */
+int fmg_vcycle(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fmg_vec* r);
+/* The <linear-solver> loop (iterate.lisp:239-250, solve.lisp:139-164,
+   linsolve.lisp:58-73) on the assembled top-level system, starting from x.
+   hist receives :defnorm per step (hist_len >= maxsteps + 2), *nsteps the
+   last step index, *status 0 = success, 1 = failure (maxsteps). */
+int fmg_solve(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, double* hist, int hist_len,
+              int* nsteps, int* status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMGPU_H */
