@@ -87,6 +87,7 @@ SIGNATURES = {
     "fmg_vcycle": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _vp, _vp]),
     "fmg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "fmg_dot_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_long, _vp]),
 }
 
 _lib = None

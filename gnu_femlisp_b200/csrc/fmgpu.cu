@@ -892,3 +892,13 @@ int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, 
 }
 
 }  // extern "C"
+
+// context accessors for the allocation-free entry point (fmgpu_noalloc.cu)
+namespace fmg {
+int ctx_device(const fmg_ctx* c) { return c->device; }
+cudaStream_t ctx_stream(const fmg_ctx* c) { return c->stream; }
+int ctx_error(fmg_ctx* c, int code, const char* msg) {
+  c->err = msg;
+  return code;
+}
+}  // namespace fmg

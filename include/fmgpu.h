@@ -171,6 +171,21 @@ int fmg_vcycle(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b,
 int fmg_solve(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, double* hist, int hist_len,
               int* nsteps, int* status);
 
+/* ------------------------------------------------- allocation-free variant */
+/* No counterpart in the reference.  The dot product of fmg_dot for callers
+   that cannot allocate device memory: hosts whose device memory is already
+   owned by their own pool allocator, and latency-critical loops that must not
+   take the implicit device synchronisation of cudaMalloc/cudaFree.  x, y
+   (n doubles) and out (1 double) are device pointers supplied by the caller;
+   the result is written to *out on the context's stream (no host sync).  The
+   reduction scratch is a fixed ~256 KB array inside the library, held by every
+   GPU that loads it until exit.  n <= FMG_NOALLOC_MAX_N, else FMG_ERR_ARG.
+   The first call on a device looks up the scratch address and should come
+   before any stream capture.  All calls share the scratch: calls that overlap
+   on the GPU race. */
+#define FMG_NOALLOC_MAX_N 134217728L
+int fmg_dot_noalloc(fmg_ctx* ctx, const double* x, const double* y, long n, double* out);
+
 #ifdef __cplusplus
 }
 #endif
