@@ -293,6 +293,9 @@ def run_mine(args, world, rank, local):
     t_mv, _ = timed(mv, args.matvec_reps)
     nnz = (3 * wl.n_cells + 1) ** 3
     alg_bytes = 8 * nnz + 16 * n
+    # DRAM traffic of one launch: 233.7 B per row, from the ncu capture at
+    # 129^3 (profiles/k_spmv_q1_3d_fp64_128cube.md), scaled by rows
+    traffic = 233.7 * n
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / t_mv / 1e9
 
@@ -310,7 +313,7 @@ def run_mine(args, world, rank, local):
         "mdof_per_s_per_vcycle": n / t_cycle / 1e6,
         "vcycle_ms": t_cycle * 1e3,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": traffic,
                      "kernel": "k_spmv<3,1> (top-level FP64 matvec)", "peak_kind": peak_kind,
                      "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
         "e2e": {"value": world * n / t_e2e_max / 1e6, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",

@@ -1,0 +1,142 @@
+;;; -*- mode: lisp; -*-
+;;;
+;;; fmgpu.lisp -- Femlisp binding of libfmgpu.so (the B200 multigrid solve
+;;; path).  Written for Femlisp's fl.port foreign-function layer
+;;; (src/basic/port.lisp:360-547) in the style of src/alien/superlu.lisp:57-75.
+;;;
+;;; Not exercised here: no Common Lisp implementation is available where this
+;;; library is built and tested.  The C side is tested through the same C-ABI
+;;; from Python (tests/).
+;;;
+;;; Load with (fl.port:load-foreign-library "libfmgpu.so") after adding the
+;;; library path to fl.start's foreign-library configuration
+;;; (src/config/femlisp-config.lisp:65-93).
+
+(defpackage "FL.FMGPU"
+  (:use "COMMON-LISP" "FL.MATLISP" "FL.ITERATION")
+  (:export "<GPU-LINEAR-SOLVER>" "GPU-SOLVE" "GPU-CONTEXT"))
+
+(in-package "FL.FMGPU")
+
+;;;; constants of include/fmgpu.h
+
+(defconstant +fmg-ok+ 0)
+(defconstant +fmg-k-const+ 0)
+(defconstant +fmg-k-cell+ 1)
+(defconstant +fmg-f-const+ 2)
+(defconstant +fmg-f-ip+ 3)
+(defconstant +fmg-jacobi+ 0)
+(defconstant +fmg-sor+ 1)
+(defconstant +fmg-method-mg+ 0)
+(defconstant +fmg-method-cg-mg+ 1)
+(defconstant +fmg-multiplicative+ 0)
+(defconstant +fmg-additive+ 1)
+
+;;;; foreign functions (handles are passed as (* :char) pointers)
+
+(fl.port:def-function ("fmg_init" fmg-init)
+    ((device :int) (ctx (* (* :char))))
+  :returning :int)
+
+(fl.port:def-function ("fmg_finalize" fmg-finalize)
+    ((ctx (* :char)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_grid_create" fmg-grid-create)
+    ((ctx (* :char)) (dim :int) (order :int) (ncomp :int) (n0 :int)
+     (top-level :int) (base-level :int) (dirichlet-mask :int)
+     (grid (* (* :char))))
+  :returning :int)
+
+(fl.port:def-function ("fmg_set_coefficient" fmg-set-coefficient)
+    ((grid (* :char)) (kind :int) (values (* :double)) (n :long))
+  :returning :int)
+
+(fl.port:def-function ("fmg_assemble" fmg-assemble)
+    ((grid (* :char)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_vec_create" fmg-vec-create)
+    ((grid (* :char)) (level :int) (vec (* (* :char))))
+  :returning :int)
+
+(fl.port:def-function ("fmg_vec_get" fmg-vec-get)
+    ((vec (* :char)) (host (* :double)) (n :long))
+  :returning :int)
+
+;;; fmg_solve takes a pointer to an fmg_solve_cfg struct; it is passed as a
+;;; byte vector laid out like the C struct (see %cfg-bytes).
+(fl.port:def-function ("fmg_solve" fmg-solve)
+    ((grid (* :char)) (cfg (* :char)) (x (* :char))
+     (hist (* :double)) (hist-len :int) (nsteps (* :int)) (status (* :int)))
+  :returning :int)
+
+(defun check (status what)
+  (unless (= status +fmg-ok+)
+    (error "libfmgpu: ~A failed with status ~D" what status)))
+
+;;;; a solver class usable on a Femlisp blackboard
+
+(defclass <gpu-linear-solver> (<linear-solver>)
+  ((smoother :initarg :smoother :initform :jacobi)
+   (damp :initarg :damp :initform 0.6d0)
+   (pre-steps :initarg :pre-steps :initform 1)
+   (post-steps :initarg :post-steps :initform 1)
+   (base-level :initarg :base-level :initform 0)
+   (reduction :initarg :reduction :initform 1d-10)
+   (maxsteps :initarg :maxsteps :initform 200))
+  (:documentation "<cg> preconditioned by <geometric-cs>, run by libfmgpu on
+the GPU.  The problem must be a cdr problem on a uniformly refined unit
+n-cube with Lagrange Q1/Q2; the coefficients are sampled on the host."))
+
+(defvar *gpu-context* nil)
+
+(defun gpu-context ()
+  (or *gpu-context*
+      (let ((ctx (make-array 1 :element-type '(unsigned-byte 64))))
+        (check (fl.port:foreign-call #'fmg-init 0 ctx) "fmg_init")
+        (setq *gpu-context* (aref ctx 0)))))
+
+(defun %cfg-bytes (method smoother damp pre post rtol maxsteps)
+  "fmg_solve_cfg laid out as the C struct (64 bytes with x86-64 alignment)."
+  (let ((v (make-array 64 :element-type '(unsigned-byte 8) :initial-element 0)))
+    (flet ((int! (off x) (setf (fl.port:sap-ref-32 v off) x))
+           (dbl! (off x) (setf (fl.port:sap-ref-double v off) x)))
+      (int! 0 method) (int! 4 smoother) (dbl! 8 damp)
+      (int! 16 pre) (int! 20 post) (int! 24 1) (int! 28 0)
+      (dbl! 32 1d0) (dbl! 40 rtol) (dbl! 48 0d0) (int! 56 maxsteps)
+      (int! 60 +fmg-multiplicative+))
+    v))
+
+(defun gpu-solve (solver dim order level kcell &key (source 1d0))
+  "Assemble and solve on the GPU; returns the nodal solution (lexicographic,
+x fastest) and the :defnorm history."
+  (with-slots (smoother damp pre-steps post-steps base-level reduction maxsteps) solver
+    (let ((grid (make-array 1 :element-type '(unsigned-byte 64)))
+          (x (make-array 1 :element-type '(unsigned-byte 64)))
+          (hist (make-array (+ maxsteps 2) :element-type 'double-float))
+          (nsteps (make-array 1 :element-type '(signed-byte 32)))
+          (status (make-array 1 :element-type '(signed-byte 32))))
+      (check (fl.port:foreign-call #'fmg-grid-create (gpu-context) dim order 1 1 level
+                                   base-level (1- (expt 2 (* 2 dim))) grid)
+             "fmg_grid_create")
+      (if kcell
+          (check (fl.port:foreign-call #'fmg-set-coefficient (aref grid 0) +fmg-k-cell+
+                                       kcell (length kcell))
+                 "fmg_set_coefficient")
+          nil)
+      (let ((f (make-array 1 :element-type 'double-float :initial-element source)))
+        (check (fl.port:foreign-call #'fmg-set-coefficient (aref grid 0) +fmg-f-const+ f 1)
+               "fmg_set_coefficient"))
+      (check (fl.port:foreign-call #'fmg-assemble (aref grid 0)) "fmg_assemble")
+      (check (fl.port:foreign-call #'fmg-vec-create (aref grid 0) level x) "fmg_vec_create")
+      (check (fl.port:foreign-call
+              #'fmg-solve (aref grid 0)
+              (%cfg-bytes +fmg-method-cg-mg+ (if (eq smoother :sor) +fmg-sor+ +fmg-jacobi+)
+                          damp pre-steps post-steps reduction maxsteps)
+              (aref x 0) hist (length hist) nsteps status)
+             "fmg_solve")
+      (let* ((n (expt (1+ (* order (expt 2 level))) dim))
+             (sol (make-array n :element-type 'double-float)))
+        (check (fl.port:foreign-call #'fmg-vec-get (aref x 0) sol n) "fmg_vec_get")
+        (values sol (subseq hist 0 (1+ (aref nsteps 0))))))))
