@@ -4,7 +4,7 @@ Conjugate gradients preconditioned by a geometric correction-scheme V-cycle
 with damped-Jacobi / multicolour-SOR smoothing on Lagrange Q1/Q2 level
 matrices, all on one GPU behind the C-ABI in ``include/fmgpu.h``.
 """
-from ._capi import FmgError, SolveCfg  # noqa: F401
+from ._capi import FmgError, MixedCfg, SolveCfg  # noqa: F401
 from .core import Context, Grid, Vector  # noqa: F401
 from .iteration import (CG, LU, SOR, CdrProblem, GaussSeidel, GeometricCS, Jacobi,  # noqa: F401
                         LagrangeFE, LinearSolver, Mesh, cdr_model_problem, discretize_globally,
@@ -12,7 +12,7 @@ from .iteration import (CG, LU, SOR, CdrProblem, GaussSeidel, GeometricCS, Jacob
                         uniformly_refined_hierarchical_mesh)
 
 __all__ = [
-    "FmgError", "SolveCfg", "Context", "Grid", "Vector", "CG", "LU", "SOR", "GaussSeidel",
+    "FmgError", "MixedCfg", "SolveCfg", "Context", "Grid", "Vector", "CG", "LU", "SOR", "GaussSeidel",
     "GeometricCS", "Jacobi", "CdrProblem", "LagrangeFE", "LinearSolver", "Mesh",
     "cdr_model_problem", "discretize_globally", "geometric_cs", "lagrange_fe",
     "sample_at_gauss_points", "solve", "uniformly_refined_hierarchical_mesh",

@@ -51,6 +51,16 @@ class SolveCfg(ctypes.Structure):
     ]
 
 
+class MixedCfg(ctypes.Structure):
+    """fmg_mixed_cfg: inner tolerance and limits of the mixed-precision solve."""
+    _fields_ = [
+        ("inner_rtol", ctypes.c_double),
+        ("max_inner", ctypes.c_int),
+        ("max_outer", ctypes.c_int),
+        ("matrix_free", ctypes.c_int),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "fmg_init": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -88,6 +98,9 @@ SIGNATURES = {
     "fmg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "fmg_dot_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_long, _vp]),
+    "fmg_solve_mixed": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), ctypes.POINTER(MixedCfg), _vp, _dp,
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
 }
 
 _lib = None

@@ -9,8 +9,22 @@ import ctypes
 
 import numpy as np
 
+import atexit
+
 from . import _capi as C
 from ._capi import FmgError
+
+# At interpreter exit handles may be collected in any order; the process is
+# ending and the driver reclaims device memory, so destructors do nothing.
+_EXITING = False
+
+
+def _mark_exit():
+    global _EXITING
+    _EXITING = True
+
+
+atexit.register(_mark_exit)
 
 
 class Context:
@@ -47,6 +61,8 @@ class Context:
             self.h = None
 
     def __del__(self):
+        if _EXITING:
+            return
         try:
             self.close()
         except Exception:
@@ -147,12 +163,28 @@ class Grid:
                                            ctypes.byref(ns), ctypes.byref(st)), "solve")
         return hist[: ns.value + 1].copy(), ns.value, st.value
 
+    def solve_mixed(self, cfg: C.SolveCfg, x: "Vector", inner_rtol: float = 1e-5, max_inner: int = 200,
+                    max_outer: int = 20, matrix_free: bool = True):
+        """FP64 flexible CG preconditioned by the FP32/BF16 V-cycle; returns
+        (defnorm history: true FP64 residuals at the start and at every
+        restart, recursive residuals in between; restarts; CG iterations;
+        status)."""
+        mc = C.MixedCfg(inner_rtol, max_inner, max_outer, 1 if matrix_free else 0)
+        hist = np.zeros(cfg.maxsteps + max_outer + 4)
+        no, ni, st = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        self.ctx.check(self._lib.fmg_solve_mixed(self.h, ctypes.byref(cfg), ctypes.byref(mc), x.h, C.dptr(hist),
+                                                 hist.size, ctypes.byref(no), ctypes.byref(ni), ctypes.byref(st)),
+                       "solve_mixed")
+        return hist[: no.value + ni.value + 1].copy(), no.value, ni.value, st.value
+
     def close(self):
         if getattr(self, "h", None):
             self._lib.fmg_grid_destroy(self.h)
             self.h = None
 
     def __del__(self):
+        if _EXITING:
+            return
         try:
             self.close()
         except Exception:
@@ -210,6 +242,8 @@ class Vector:
             self.h = None
 
     def __del__(self):
+        if _EXITING:
+            return
         try:
             self.close()
         except Exception:

@@ -17,9 +17,11 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <algorithm>
 #include <utility>
 
 #include "fmgpu_kernels.cuh"
+#include "fmgpu_mixed.cuh"
 
 using namespace fmg;
 
@@ -28,6 +30,8 @@ struct fmg_ctx {
   cudaStream_t stream = nullptr;
   double* host_scal = nullptr;  // pinned copy of a grid's scalar slots
   std::string err;
+  int grids = 0;                // live grids: the context outlives them
+  bool closed = false;          // fmg_finalize called while grids were alive
 };
 
 namespace {
@@ -73,6 +77,8 @@ struct fmg_grid {
          *xs = nullptr, *xs2 = nullptr;
   bool assembled = false;
   bool assembled_once = false;
+  long long epoch = 0;         // incremented by every assembly
+  struct MixedState* mx = nullptr;
   double* kq = nullptr;        // Gauss-point coefficient samples of a coarse level
   double *lu = nullptr, *lux = nullptr;  // coarse LU factors and inverse workspace
   int* piv = nullptr;
@@ -81,6 +87,8 @@ struct fmg_grid {
   std::vector<int> rp;
   int cur = 0;
   std::vector<void*> allocs;
+  int vecs = 0;                // live vectors: the grid outlives them
+  bool destroyed = false;      // fmg_grid_destroy called while vectors were alive
 };
 
 struct fmg_vec {
@@ -88,6 +96,21 @@ struct fmg_vec {
   int level = 0;
   long long n = 0;
   double* d = nullptr;
+};
+
+// device data of the mixed-precision solve, built from an assembly
+struct MixedState {
+  long long epoch = -1;             // assembly it was converted from
+  bool mf = false;                  // top level applied matrix-free
+  std::vector<Lev32> lv;            // per level (FP32 matrices)
+  std::vector<float*> A32, om32, x0, x1;
+  std::vector<__nv_bfloat16*> bc, rc;  // coarse rhs and residual (BF16)
+  float* k32 = nullptr;             // top-level cell coefficients (FP32)
+  float *rtop = nullptr, *r = nullptr, *q = nullptr, *qs = nullptr;  // FP32 top-level vectors
+  double* sc = nullptr;
+  double* part = nullptr;
+  unsigned* counter = nullptr;
+  double* host = nullptr;           // pinned copy of sc
 };
 
 // ------------------------------------------------------------------ errors
@@ -402,12 +425,19 @@ int fmg_init(int device, fmg_ctx** out) {
   return FMG_OK;
 }
 
-int fmg_finalize(fmg_ctx* c) {
-  if (!c) return FMG_ERR_ARG;
+static void ctx_release(fmg_ctx* c) {
   cudaStreamSynchronize(c->stream);
   cudaFreeHost(c->host_scal);
   cudaStreamDestroy(c->stream);
   delete c;
+}
+
+// Releases the context; if grids of it are still alive the release happens
+// when the last of them is destroyed.
+int fmg_finalize(fmg_ctx* c) {
+  if (!c || c->closed) return FMG_ERR_ARG;
+  c->closed = true;
+  if (c->grids == 0) ctx_release(c);
   return FMG_OK;
 }
 
@@ -447,6 +477,7 @@ int fmg_grid_create(fmg_ctx* c, int dim, int order, int ncomp, int n0, int top_l
   fmg_grid* g = new (std::nothrow) fmg_grid();
   if (!g) return FMG_ERR_NOMEM;
   g->ctx = c;
+  c->grids += 1;
   g->dim = dim; g->order = order; g->nc = ncomp; g->n0 = n0;
   g->top = top_level; g->base = base_level; g->dmask = dirichlet_mask;
   int w = 2 * order + 1;
@@ -471,11 +502,23 @@ int fmg_grid_create(fmg_ctx* c, int dim, int order, int ncomp, int n0, int top_l
   return FMG_OK;
 }
 
-int fmg_grid_destroy(fmg_grid* g) {
-  if (!g) return FMG_ERR_ARG;
-  cudaStreamSynchronize(g->ctx->stream);
+static void grid_release(fmg_grid* g) {
+  fmg_ctx* c = g->ctx;
+  cudaStreamSynchronize(c->stream);
   for (void* p : g->allocs) cudaFree(p);
+  if (g->mx && g->mx->host) cudaFreeHost(g->mx->host);
+  delete g->mx;
   delete g;
+  c->grids -= 1;
+  if (c->closed && c->grids == 0) ctx_release(c);
+}
+
+// Releases the grid; if vectors of it are still alive the release happens
+// when the last of them is destroyed.
+int fmg_grid_destroy(fmg_grid* g) {
+  if (!g || g->destroyed) return FMG_ERR_ARG;
+  g->destroyed = true;
+  if (g->vecs == 0) grid_release(g);
   return FMG_OK;
 }
 
@@ -617,6 +660,7 @@ int fmg_assemble(fmg_grid* g) {
   }
   FMG_CK(c, cudaStreamSynchronize(st));
   g->assembled = true;
+  g->epoch += 1;
   return FMG_OK;
 }
 
@@ -662,11 +706,13 @@ int fmg_vec_create(fmg_grid* g, int level, fmg_vec** out) {
   fmg_vec* v = new (std::nothrow) fmg_vec();
   if (!v) return FMG_ERR_NOMEM;
   v->g = g; v->level = level; v->n = g->lev[level].N;
+  g->vecs += 1;
   const long long np = pad64(v->n);
   cudaError_t e = cudaMalloc((void**)&v->d, np * sizeof(double));
   if (e != cudaSuccess) {
     cudaGetLastError();
     delete v;
+    g->vecs -= 1;
     return set_err(g->ctx, FMG_ERR_NOMEM, "vector allocation failed");
   }
   FMG_CK(g->ctx, cudaMemsetAsync(v->d, 0, np * sizeof(double), g->ctx->stream));
@@ -676,9 +722,12 @@ int fmg_vec_create(fmg_grid* g, int level, fmg_vec** out) {
 
 int fmg_vec_destroy(fmg_vec* v) {
   if (!v) return FMG_ERR_ARG;
-  cudaStreamSynchronize(v->g->ctx->stream);
+  fmg_grid* g = v->g;
+  cudaStreamSynchronize(g->ctx->stream);
   cudaFree(v->d);
   delete v;
+  g->vecs -= 1;
+  if (g->destroyed && g->vecs == 0) grid_release(g);
   return FMG_OK;
 }
 
@@ -902,3 +951,252 @@ int ctx_error(fmg_ctx* c, int code, const char* msg) {
   return code;
 }
 }  // namespace fmg
+
+// ============================================================ mixed solve
+// FP64 iterative refinement around an FP32 flexible CG whose preconditioner is
+// one V-cycle in FP32 (smoothing, restriction, prolongation), with BF16
+// coarse right-hand sides and residuals and the coarsest dense solve in FP64.
+// The outer residual r = b - A x and the update x += e use the assembled FP64
+// top-level matrix, so the reported :defnorm is the true FP64 residual.
+namespace {
+
+int mx_alloc_f(fmg_grid* g, float** p, long long n) { return dalloc(g, (double**)p, (n + 1) / 2); }
+
+int mixed_prepare(fmg_grid* g, bool want_mf) {
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  int rc;
+  if (!g->mx) g->mx = new MixedState();
+  MixedState& X = *g->mx;
+  const int nl = g->top + 1;
+  const bool mf = want_mf && g->dim == 3 && g->order == 1 && g->nc == 1;
+  if (X.lv.empty()) {  // first use: allocate
+    X.lv.assign(nl, Lev32{});
+    X.A32.assign(nl, nullptr); X.om32.assign(nl, nullptr);
+    X.x0.assign(nl, nullptr); X.x1.assign(nl, nullptr);
+    X.bc.assign(nl, nullptr); X.rc.assign(nl, nullptr);
+    for (int l = g->base; l <= g->top; ++l) {
+      const Lvl& L = g->lev[l];
+      if ((rc = mx_alloc_f(g, &X.A32[l], (long long)g->nslots * L.Np)) || (rc = mx_alloc_f(g, &X.x0[l], L.Np)) ||
+          (rc = mx_alloc_f(g, &X.x1[l], L.Np)) || (rc = mx_alloc_f(g, &X.om32[l], L.Np)))
+        return rc;
+      if ((rc = dalloc(g, (double**)&X.bc[l], (L.Np + 3) / 4)) || (rc = dalloc(g, (double**)&X.rc[l], (L.Np + 3) / 4)))
+        return rc;
+    }
+    const Lvl& T = g->lev[g->top];
+    long long ncell = 1;
+    for (int k = 0; k < g->dim; ++k) ncell *= T.n;
+    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs};
+    for (float** v : tv)
+      if ((rc = mx_alloc_f(g, v, T.Np))) return rc;
+    if ((rc = mx_alloc_f(g, &X.k32, ncell))) return rc;
+    const long long nparts = std::max({(long long)nchunks(T.Np), mx_top_blocks((int)T.M), T.Np / kBlock + 1}) + 1;
+    if ((rc = dalloc(g, &X.sc, M_COUNT)) || (rc = dalloc(g, &X.part, 2 * nparts)) ||
+        (rc = dalloc(g, (double**)&X.counter, 1)))
+      return rc;
+    if (!X.host) FMG_CK(c, cudaMallocHost((void**)&X.host, M_COUNT * sizeof(double)));
+  }
+  if (X.epoch != g->epoch) {  // convert the current assembly
+    for (int l = g->base; l <= g->top; ++l) {
+      const Lvl& L = g->lev[l];
+      mx_f64_to_f32(L.A, X.A32[l], (long long)g->nslots * L.Np, st);
+    }
+    if (g->kkind == FMG_K_CELL) {
+      long long ncell = 1;
+      for (int k = 0; k < g->dim; ++k) ncell *= g->lev[g->top].n;
+      mx_f64_to_f32(g->kcell_d, X.k32, ncell, st);
+    }
+    X.epoch = g->epoch;
+  }
+  for (int l = g->base; l <= g->top; ++l) {  // per-node damping may change between solves
+    const Lvl& L = g->lev[l];
+    if (L.omega) mx_f64_to_f32(L.omega, X.om32[l], L.N, st);
+    Lev32& V = X.lv[l];
+    V.A = X.A32[l]; V.om = L.omega ? X.om32[l] : nullptr;
+    V.N = L.N; V.Np = L.Np; V.M = L.M; V.dim = g->dim; V.order = g->order; V.dmask = g->dmask;
+  }
+  X.mf = mf;
+  return launched(c, "mixed prepare");
+}
+
+struct MixedMG {
+  fmg_grid* g;
+  MixedState& X;
+  const fmg_solve_cfg& c;
+  cudaStream_t st;
+
+  bool top_mf() const { return X.mf && g->kkind == FMG_K_CELL; }
+  MFArgs mf_args() const {
+    const Lvl& T = g->lev[g->top];
+    MFArgs a;
+    a.k = X.k32;
+    a.omega = X.lv[g->top].om;
+    a.N = T.N; a.M = (int)T.M; a.n = (int)T.n; a.dmask = g->dmask;
+    a.hs = (float)(T.h / 12.0);
+    a.w = (float)c.damp;
+    return a;
+  }
+  // one FP32 operator application on level l (modes of k_mf_q1 / k_st32)
+  void apply(int l, int mode, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16, const double* v,
+             const double* v2, const Reduce2* R) {
+    Lev32 L = X.lv[l];
+    L.w = (float)c.damp;
+    if (l == g->top && top_mf() && !b_bf16 && !y_bf16)
+      mx_top_apply(mode, mf_args(), x, (const float*)b, (float*)y, v, v2, R, st);
+    else
+      mx_level_apply(mode, L, x, b, b_bf16, y, y_bf16, v, v2, R, st);
+  }
+  // V-cycle on level l from x = 0 for rhs b (FP32 on the top level, BF16
+  // below); the result is left in X.x0[l] (top: *xq); with R the last top-level
+  // smoothing step also reduces (x, v) and (x, v2)
+  void vcycle(int l, const void* b, float** xq, float** xs, const double* v, const double* v2, const Reduce2* R) {
+    const bool top = (l == g->top);
+    const bool bbf = !top;
+    float*& x = top ? *xq : X.x0[l];
+    float*& xn = top ? *xs : X.x1[l];
+    if (l == g->base) {
+      mx_coarse(g->ainvT, g->nbase, (const __nv_bfloat16*)b, x, st);
+      return;
+    }
+    if (c.pre_steps >= 1) {  // pre-smoothing from x = 0
+      apply(l, 3, nullptr, b, bbf, x, false, nullptr, nullptr, nullptr);
+      for (int s = 1; s < c.pre_steps; ++s) {
+        apply(l, 2, x, b, bbf, xn, false, nullptr, nullptr, nullptr);
+        std::swap(x, xn);
+      }
+    } else {
+      launch_fill((double*)x, (X.lv[l].Np + 1) / 2, 0.0, st);
+    }
+    void* r = top ? (void*)X.rtop : (void*)X.rc[l];  // residual and restriction
+    apply(l, 1, x, b, bbf, r, !top, nullptr, nullptr, nullptr);
+    mx_restrict(X.lv[l], X.lv[l - 1], r, !top, X.bc[l - 1], X.x0[l - 1], st);
+    vcycle(l - 1, X.bc[l - 1], nullptr, nullptr, nullptr, nullptr, nullptr);
+    mx_prolong(X.lv[l - 1], X.lv[l], X.x0[l - 1], x, st);
+    for (int s = 0; s < c.post_steps; ++s) {
+      const bool last = top && R && s == c.post_steps - 1;
+      apply(l, 2, x, b, bbf, xn, false, last ? v : nullptr, last ? v2 : nullptr, last ? R : nullptr);
+      std::swap(x, xn);
+    }
+  }
+  // FP64 a = A p with (a, p) -> lam = rho / (a, p)
+  void matvec64(const double* p, double* a, const Reduce2& Rl) {
+    const LevelView T = view(g, g->top);
+    if (top_mf()) {
+      const Lvl& L = g->lev[g->top];
+      MFArgs64 m;
+      m.k = g->kcell_d; m.omega = nullptr; m.N = L.N; m.M = (int)L.M; m.n = (int)L.n; m.dmask = g->dmask;
+      m.hs = L.h / 12.0; m.w = c.damp;
+      mx_top_apply64(m, p, a, p, &Rl, st);
+    } else {
+      launch_spmv(T, p, nullptr, a, nullptr, nullptr, st);
+      mx_dot2_64(a, p, nullptr, T.N, Rl, st);
+    }
+  }
+};
+
+Reduce2 red2(MixedState& X, int epi, int s0, int s1) {
+  Reduce2 R;
+  R.part = X.part; R.counter = X.counter; R.scal = X.sc; R.epi = epi; R.slot0 = s0; R.slot1 = s1;
+  return R;
+}
+
+int mx_read(fmg_grid* g) {
+  MixedState& X = *g->mx;
+  FMG_CK(g->ctx, cudaMemcpyAsync(X.host, X.sc, M_COUNT * sizeof(double), cudaMemcpyDeviceToHost, g->ctx->stream));
+  FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+  return FMG_OK;
+}
+
+int mx_set_scalar(fmg_grid* g, int slot, double v) {
+  MixedState& X = *g->mx;
+  X.host[slot] = v;
+  FMG_CK(g->ctx, cudaMemcpyAsync(X.sc + slot, X.host + slot, sizeof(double), cudaMemcpyHostToDevice, g->ctx->stream));
+  return FMG_OK;
+}
+
+}  // namespace
+
+// Flexible CG in FP64 (recursive FP64 residual, FP64 solution update, FP64
+// operator) preconditioned by one FP32/BF16 V-cycle per step.  The FP32
+// residual handed to the V-cycle is scaled to unit norm by the previous
+// step's residual norm; the preconditioned vector is scaled back in FP64.
+// When the recursive residual meets the tolerance the true residual is
+// recomputed with the assembled FP64 matrix and reported; if it does not meet
+// the tolerance, CG restarts from it.
+extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* xv,
+                               double* hist, int hist_len, int* nouter, int* ninner, int* status) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  int rc = check_cfg(g, cfg);
+  if (rc) return rc;
+  if (!mcfg || vec_check(xv, g, g->top) || !nouter || !ninner || !status) return FMG_ERR_ARG;
+  if (cfg->smoother != FMG_JACOBI || cfg->combination != FMG_MULTIPLICATIVE || cfg->gamma != 1 ||
+      g->base >= g->top || cfg->post_steps < 1)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
+                   "mixed solve: Jacobi V(pre,post>=1) cycles with gamma 1 and at least two levels");
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  if ((rc = mixed_prepare(g, mcfg->matrix_free != 0))) return rc;
+  MixedState& X = *g->mx;
+  MixedMG mg{g, X, *cfg, st};
+  const LevelView T = view(g, g->top);
+  const long long n = T.N;
+  double* x = xv->d;
+  const double* b = g->rhs;
+  double *r = g->r, *p = g->p, *a = g->a;
+  *status = 1;
+  *nouter = 0;
+  *ninner = 0;
+  const int max_restart = mcfg->max_outer > 0 ? mcfg->max_outer : 20;
+  double initial = -1.0;
+  int step = 0, iters = 0;  // history slots, CG iterations
+  for (int restart = 0; restart <= max_restart; ++restart) {
+    // true FP64 residual with the assembled matrix
+    launch_spmv(T, x, b, r, nullptr, nullptr, st);
+    launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
+    if ((rc = read_scalars(g))) return rc;
+    const double dn = std::sqrt(c->host_scal[S_RR]);
+    if (!std::isfinite(dn)) return set_err(c, FMG_ERR_NUMERIC, "defnorm is %g", dn);
+    if (initial < 0) initial = dn;
+    if (hist && step < hist_len) hist[step] = dn;
+    *nouter = restart;
+    *ninner = iters;
+    if ((cfg->rtol > 0 && (initial == 0.0 || dn / initial < cfg->rtol)) || (cfg->atol > 0 && dn < cfg->atol)) {
+      *status = 0;
+      break;
+    }
+    if (restart == max_restart || iters > cfg->maxsteps) break;
+    // start: r32 = r / |r|, z = M r, p = z
+    if ((rc = mx_set_scalar(g, M_SCALE, dn > 0 ? 1.0 / dn : 1.0))) return rc;
+    if ((rc = mx_set_scalar(g, M_SUSED, dn > 0 ? 1.0 / dn : 1.0))) return rc;
+    mx_scale_to32(r, X.sc, M_SCALE, X.r, T.Np, st);
+    {
+      const Reduce2 Rr = red2(X, EPI2_RHO, 0, 0);
+      mg.vcycle(g->top, X.r, &X.q, &X.qs, r, nullptr, &Rr);
+      mx_fcg64_p(X.sc, p, X.q, n, true, st);
+    }
+    bool converged = false;
+    while (iters <= cfg->maxsteps) {
+      mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
+      mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
+      if ((rc = launched(c, "mixed step"))) return rc;
+      if ((rc = mx_read(g))) return rc;
+      ++step;
+      ++iters;
+      const double rn = std::sqrt(X.host[M_RR]);
+      if (!std::isfinite(rn)) return set_err(c, FMG_ERR_NUMERIC, "residual is %g at step %d", rn, step);
+      if (hist && step < hist_len) hist[step] = rn;
+      if ((cfg->rtol > 0 && rn / initial < cfg->rtol) || (cfg->atol > 0 && rn < cfg->atol)) { converged = true; break; }
+      const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
+      mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
+      mx_fcg64_p(X.sc, p, X.q, n, false, st);
+    }
+    if (!converged && iters > cfg->maxsteps) {
+      *ninner = iters;
+      break;
+    }
+    ++step;  // the true-residual check occupies one history slot
+  }
+  FMG_CK(c, cudaStreamSynchronize(st));
+  return launched(c, "solve_mixed");
+}
+

@@ -53,11 +53,12 @@ __device__ __forceinline__ long long clampi(long long j, long long N) {
 }
 
 // Warp butterfly then butterfly over the 8 warp sums; the result is valid in
-// thread 0.  smem must hold 8 doubles.
+// thread 0.  smem must hold 8 doubles.  Blocks of 256 threads, 1D or (32, 8).
 __device__ __forceinline__ double dr_fold256(double v, double* smem) {
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;  // blocks of 256 threads, 1D or 2D
+  const int warp = tid >> 5, lane = tid & 31;
   __syncthreads();  // smem may still be read by a previous fold
   if (lane == 0) smem[warp] = v;
   __syncthreads();

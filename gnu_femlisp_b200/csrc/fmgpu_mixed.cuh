@@ -1,0 +1,64 @@
+// fmgpu_mixed.cuh -- launch interface of the mixed-precision kernels.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "fmgpu_internal.cuh"
+
+namespace fmg {
+
+// scalar slots of the mixed solve (FP64)
+enum MScal { M_ALPHA = 0, M_PA, M_LAM, M_BETA, M_QA, M_RR, M_SCALE, M_SUSED, M_TMP, M_COUNT = 16 };
+enum Epi2 { EPI2_STORE = 0, EPI2_LAMBDA = 1, EPI2_FCG = 2, EPI2_RHO = 3, EPI2_UPDATE = 4 };
+
+struct Reduce2 {
+  double* part;        // 2 partials per chunk
+  unsigned* counter;
+  double* scal;
+  int epi, slot0, slot1;
+};
+
+// matrix-free 3D Q1 top level
+template <typename T>
+struct MFArgsT {
+  const T* k;          // coefficient per cell (n^3)
+  const T* omega;      // per-node damping or nullptr
+  long long N;
+  int M, n, dmask;
+  T hs;                // h / 12
+  T w;                 // scalar damping
+};
+typedef MFArgsT<float> MFArgs;
+typedef MFArgsT<double> MFArgs64;
+
+// one level with an FP32 copy of its assembled matrix
+struct Lev32 {
+  const float* A;      // [slot][Np]
+  const float* om;     // per-node damping or nullptr
+  long long N, Np, M;
+  int dim, order, dmask;
+  float w;
+};
+
+void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,
+                  const double* v2, const Reduce2* R, cudaStream_t st);
+// FP64 y = A x on the top level with (y, v) reduced (epilogue of R)
+void mx_top_apply64(const MFArgs64& g, const double* x, double* y, const double* v, const Reduce2* R,
+                    cudaStream_t st);
+long long mx_top_blocks(int M);  // blocks of the matrix-free kernel (reduction partials)
+void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
+                    const double* v, const double* v2, const Reduce2* R, cudaStream_t st);
+void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, __nv_bfloat16* bc, float* xc,
+                 cudaStream_t st);
+void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cudaStream_t st);
+void mx_coarse(const double* AinvT, int n, const __nv_bfloat16* b, float* x, cudaStream_t st);
+void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st);
+// FP64 flexible CG: x += lam p, r -= lam a, (r,r), r32 = r * scale (np = padded length)
+void mx_fcg64_update(double* sc, double* x, const double* p, double* r, const double* a, float* r32, long long np,
+                     const Reduce2& R, cudaStream_t st);
+// p = q / s + beta p
+void mx_fcg64_p(const double* sc, double* p, const float* q, long long n, bool first, cudaStream_t st);
+void mx_scale_to32(const double* r, const double* sc, int slot, float* r32, long long n, cudaStream_t st);
+void mx_dot2_64(const double* x, const double* y, const double* y2, long long n, const Reduce2& R, cudaStream_t st);
+
+}  // namespace fmg

@@ -201,18 +201,27 @@ __device__ __forceinline__ int prolong_1d(long long I, long long* J, double* w) 
   return 3;
 }
 
+// Launch shape of the transfer kernels: blocks (32, 8) over x and y, one z
+// plane per blockIdx.z, 32-bit node coordinates (levels have < 2^31 nodes).
+__device__ __forceinline__ bool face_dir(int c, int M, int k, int dmask) {
+  return (c == 0 && ((dmask >> (2 * k)) & 1)) || (c == M - 1 && ((dmask >> (2 * k + 1)) & 1));
+}
+
 // rc := I^T rf (constrained), rhs_c := rc, sol_c := 0 (restrict + its :after
 // methods for the correction scheme, multigrid.lisp:202-224)
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
-k_restrict(long long NC, long long MC, long long MF, int dmask, const double* __restrict__ rf,
-           double* __restrict__ rc, double* __restrict__ rhsc, double* __restrict__ solc) {
-  const long long J = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (J >= NC) return;
-  long long cJ[3];
-  node_coords(J, MC, D, cJ);
+k_restrict(int MC, int MF, int dmask, const double* __restrict__ rf, double* __restrict__ rc,
+           double* __restrict__ rhsc, double* __restrict__ solc) {
+  if (D == 1 && threadIdx.y != 0) return;
+  const int cJ[3] = {(int)(blockIdx.x * 32 + threadIdx.x), D > 1 ? (int)(blockIdx.y * 8 + threadIdx.y) : 0,
+                     D > 2 ? (int)blockIdx.z : 0};
+  if (cJ[0] >= MC || cJ[1] >= MC) return;
+  const long long J = cJ[0] + (long long)MC * (cJ[1] + (long long)MC * cJ[2]);
+  bool dj = false;
+  for (int k = 0; k < D; ++k) dj = dj || face_dir(cJ[k], MC, k, dmask);
   double acc = 0.0;
-  if (!node_dirichlet(cJ, MC, D, dmask)) {
+  if (!dj) {
     long long off[3][5] = {{0}, {0}, {0}};
     double w[3][5] = {{1.0}, {1.0}, {1.0}};
     int cnt[3] = {1, 1, 1};
@@ -220,14 +229,14 @@ k_restrict(long long NC, long long MC, long long MF, int dmask, const double* __
     for (int z = 0; z < cnt[2]; ++z)
       for (int y = 0; y < cnt[1]; ++y)
         for (int xx = 0; xx < cnt[0]; ++xx) {
-          long long fi[3] = {2 * cJ[0] + off[0][xx], 2 * cJ[1] + off[1][y], 2 * cJ[2] + off[2][z]};
-          bool in = true;
-          for (int k = 0; k < D; ++k) if (fi[k] < 0 || fi[k] >= MF) in = false;
-          if (!in || node_dirichlet(fi, MF, D, dmask)) continue;
+          const int fi[3] = {2 * cJ[0] + (int)off[0][xx], 2 * cJ[1] + (int)off[1][y], 2 * cJ[2] + (int)off[2][z]};
+          bool skip = false;
+          for (int k = 0; k < D; ++k) skip = skip || fi[k] < 0 || fi[k] >= MF || face_dir(fi[k], MF, k, dmask);
+          if (skip) continue;
           double ww = w[0][xx];
           if (D > 1) ww = ww * w[1][y];
           if (D > 2) ww = ww * w[2][z];
-          acc = fma(ww, rf[fi[0] + MF * (fi[1] + MF * fi[2])], acc);
+          acc = fma(ww, rf[fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2])], acc);
         }
   }
   rc[J] = acc;
@@ -238,13 +247,14 @@ k_restrict(long long NC, long long MC, long long MF, int dmask, const double* __
 // xf := xf + I xc (constrained) (prolongate, multigrid.lisp:237-239)
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
-k_prolong(long long NF, long long MF, long long MC, int dmask, const double* __restrict__ xc,
-          double* __restrict__ xf) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= NF) return;
-  long long fi[3];
-  node_coords(i, MF, D, fi);
-  if (node_dirichlet(fi, MF, D, dmask)) return;
+k_prolong(int MF, int MC, int dmask, const double* __restrict__ xc, double* __restrict__ xf) {
+  if (D == 1 && threadIdx.y != 0) return;
+  const int fi[3] = {(int)(blockIdx.x * 32 + threadIdx.x), D > 1 ? (int)(blockIdx.y * 8 + threadIdx.y) : 0,
+                     D > 2 ? (int)blockIdx.z : 0};
+  if (fi[0] >= MF || fi[1] >= MF) return;
+  for (int k = 0; k < D; ++k)
+    if (face_dir(fi[k], MF, k, dmask)) return;
+  const long long i = fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2]);
   long long J[3][3] = {{0}, {0}, {0}};
   double w[3][3] = {{1.0}, {1.0}, {1.0}};
   int cnt[3] = {1, 1, 1};
@@ -253,12 +263,14 @@ k_prolong(long long NF, long long MF, long long MC, int dmask, const double* __r
   for (int z = 0; z < cnt[2]; ++z)
     for (int y = 0; y < cnt[1]; ++y)
       for (int xx = 0; xx < cnt[0]; ++xx) {
-        const long long cj[3] = {J[0][xx], J[1][y], J[2][z]};
-        if (node_dirichlet(cj, MC, D, dmask)) continue;
+        const int cj[3] = {(int)J[0][xx], (int)J[1][y], (int)J[2][z]};
+        bool dj = false;
+        for (int k = 0; k < D; ++k) dj = dj || face_dir(cj[k], MC, k, dmask);
+        if (dj) continue;
         double ww = w[0][xx];
         if (D > 1) ww = ww * w[1][y];
         if (D > 2) ww = ww * w[2][z];
-        acc = fma(ww, xc[cj[0] + MC * (cj[1] + MC * cj[2])], acc);
+        acc = fma(ww, xc[cj[0] + (long long)MC * (cj[1] + (long long)MC * cj[2])], acc);
       }
   xf[i] = xf[i] + acc;
 }
@@ -600,18 +612,22 @@ void launch_sor(const LevelView& L, double omega, double* x, const double* b, do
   }
 }
 
+static inline dim3 xfer_grid(long long M, int dim) {
+  return dim3((unsigned)((M + 31) / 32), (unsigned)(dim > 1 ? (M + 7) / 8 : 1), (unsigned)(dim > 2 ? M : 1));
+}
+
 void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, double* rc, double* rhsc,
                      double* solc, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   FMG_DISPATCH(F.dim, F.order, {
-    k_restrict<D, P><<<grid1(Cl.N), kBlock, 0, st>>>(Cl.N, Cl.M, F.M, F.dmask, rf, rc, rhsc, solc);
+    k_restrict<D, P><<<xfer_grid(Cl.M, D), dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc);
   });
 }
 
 void launch_prolong(const LevelView& Cl, const LevelView& F, const double* xc, double* xf, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   FMG_DISPATCH(F.dim, F.order, {
-    k_prolong<D, P><<<grid1(F.N), kBlock, 0, st>>>(F.N, F.M, Cl.M, F.dmask, xc, xf);
+    k_prolong<D, P><<<xfer_grid(F.M, D), dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf);
   });
 }
 

@@ -81,6 +81,8 @@ typedef struct {
 /* Opens device `device` (load-foreign-library, port.lisp:360-379, plus the
    state the Lisp side keeps).  */
 int fmg_init(int device, fmg_ctx** ctx);
+/* Grids keep their context alive and vectors their grid: destroying a handle
+   that still has dependants defers its release to the last dependant. */
 int fmg_finalize(fmg_ctx* ctx);
 /* Copies the message of the last failure (NUL-terminated) into buf. */
 int fmg_last_error(fmg_ctx* ctx, char* buf, int len);
@@ -170,6 +172,29 @@ int fmg_vcycle(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b,
    last step index, *status 0 = success, 1 = failure (maxsteps). */
 int fmg_solve(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, double* hist, int hist_len,
               int* nsteps, int* status);
+
+/* ------------------------------------------------------ mixed precision */
+/* No counterpart in the reference.  Mixed-precision variant of fmg_solve for
+   <cg> + <geometric-cs> with Jacobi smoothing: flexible CG in FP64 (FP64
+   operator, recursive FP64 residual, FP64 solution update) preconditioned by
+   one V-cycle per step that smooths, restricts and prolongates in FP32 with
+   BF16 coarse right-hand sides and residuals, the coarsest dense solve staying
+   in FP64.  When the recursive residual meets the tolerance the true residual
+   is recomputed with the assembled FP64 matrix, and CG restarts from it if it
+   does not.  With matrix_free set, a 3D Q1 problem with a cell-wise
+   coefficient applies its top-level operator (FP64 and FP32) from the cell
+   coefficients instead of the stored matrix.  hist receives the true residual
+   at the start and at every restart check and the recursive residual after
+   each CG iteration; *nouter counts restart checks, *ninner CG iterations. */
+typedef struct {
+  double inner_rtol;   /* reserved, 0 */
+  int max_inner;       /* reserved, 0 */
+  int max_outer;       /* restart checks allowed (default 20) */
+  int matrix_free;     /* 1: matrix-free top level where available */
+} fmg_mixed_cfg;
+
+int fmg_solve_mixed(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* x,
+                    double* hist, int hist_len, int* nouter, int* ninner, int* status);
 
 /* ------------------------------------------------- allocation-free variant */
 /* No counterpart in the reference.  The dot product of fmg_dot for callers
