@@ -141,47 +141,24 @@ k_mf_q1(MFArgsT<T> g, const T* __restrict__ x, const T* __restrict__ b, T* __res
   if (iy < M) {
     const long long MM = (long long)M * M;
     auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-    // validity of node positions x-1 .. x+NX, rows y-1 .. y+1; cells x-1 .. x+NX-1, rows y-1, y
-    bool vx[NX + 2], vy[3], cxv[NX + 1], cyv[2];
-    int jxc[NX + 2], cxc[NX + 1];
-#pragma unroll
-    for (int j = 0; j < NX + 2; ++j) {
-      const int jx = ix0 - 1 + j;
-      vx[j] = jx >= 0 && jx < M && !dirf(jx, 1, 2);
-      jxc[j] = min(max(jx, 0), M - 1);
-    }
-#pragma unroll
-    for (int j = 0; j < NX + 1; ++j) {
-      const int cx = ix0 - 1 + j;
-      cxv[j] = cx >= 0 && cx < n;
-      cxc[j] = min(max(cx, 0), n - 1);
-    }
-    int jyc[3], cyc[2];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const int jy = iy - 1 + j;
-      vy[j] = jy >= 0 && jy < M && !dirf(jy, 4, 8);
-      jyc[j] = min(max(jy, 0), M - 1);
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int cy = iy - 1 + j;
-      cyv[j] = cy >= 0 && cy < n;
-      cyc[j] = min(max(cy, 0), n - 1);
-    }
     T W[3][3][NX + 2];   // [plane][row][x]
     T K[2][2][NX + 1];   // [cell plane][cell row][cell x]
+    // boundary columns: clamped addresses, validity recomputed per load
+    // (inside the grid, off the Dirichlet faces; cells inside the grid)
     auto ldplane = [&](int jz, T (*dst)[NX + 2]) {
       const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
       const long long zb = (long long)min(max(jz, 0), M - 1) * MM;
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
-        const T* row = x + zb + (long long)jyc[r] * M;
-        const bool vr = vz && vy[r];
+        const int jy = iy - 1 + r;
+        const bool vr = vz && jy >= 0 && jy < M && !dirf(jy, 4, 8);
+        const T* row = x + zb + (long long)min(max(jy, 0), M - 1) * M;
 #pragma unroll
         for (int j = 0; j < NX + 2; ++j) {
-          const T xv = __ldg(row + jxc[j]);
-          dst[r][j] = (vr && vx[j]) ? xv : T(0);
+          const int jx = ix0 - 1 + j;
+          const bool ok = vr && jx >= 0 && jx < M && !dirf(jx, 1, 2);
+          const T xv = __ldg(row + min(max(jx, 0), M - 1));
+          dst[r][j] = ok ? xv : T(0);
         }
       }
     };
@@ -190,25 +167,71 @@ k_mf_q1(MFArgsT<T> g, const T* __restrict__ x, const T* __restrict__ b, T* __res
       const long long zb = (long long)min(max(cz, 0), n - 1) * n * n;
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
-        const T* row = g.k + zb + (long long)cyc[r] * n;
-        const bool vr = vz && cyv[r];
+        const int cy = iy - 1 + r;
+        const bool vr = vz && cy >= 0 && cy < n;
+        const T* row = g.k + zb + (long long)min(max(cy, 0), n - 1) * n;
 #pragma unroll
         for (int j = 0; j < NX + 1; ++j) {
-          const T kv = __ldg(row + cxc[j]);
-          dst[r][j] = (vr && cxv[j]) ? kv : T(0);
+          const int cx = ix0 - 1 + j;
+          const T kv = __ldg(row + min(max(cx, 0), n - 1));
+          dst[r][j] = (vr && cx >= 0 && cx < n) ? kv : T(0);
         }
       }
     };
-    if (MODE != 3) { ldplane(z0 - 1, W[0]); ldplane(z0, W[1]); }
-    ldcells(z0 - 1, K[0]);
+    // interior columns (every x and y neighbour position in 1 .. M-2) load
+    // without clamps or masks; a plane is then valid or zero as a whole
+    const bool fast = ix0 >= 2 && ix0 + NX <= M - 2 && iy >= 2 && iy <= M - 3;
+    const T* xcol = x + (long long)(iy - 1) * M + (ix0 - 1);
+    const T* kcol = g.k + (long long)(iy - 1) * n + (ix0 - 1);
+    auto ldplane_fast = [&](int jz, T (*dst)[NX + 2]) {
+      const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
+      if (vz) {
+        const T* p0 = xcol + (long long)jz * MM;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int j = 0; j < NX + 2; ++j) dst[r][j] = __ldg(p0 + r * M + j);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int j = 0; j < NX + 2; ++j) dst[r][j] = T(0);
+      }
+    };
+    auto ldcells_fast = [&](int cz, T (*dst)[NX + 1]) {
+      if (cz >= 0 && cz < n) {
+        const T* p0 = kcol + (long long)cz * n * n;
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+          for (int j = 0; j < NX + 1; ++j) dst[r][j] = __ldg(p0 + r * n + j);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+          for (int j = 0; j < NX + 1; ++j) dst[r][j] = T(0);
+      }
+    };
+    if (fast) {
+      if (MODE != 3) { ldplane_fast(z0 - 1, W[0]); ldplane_fast(z0, W[1]); }
+      ldcells_fast(z0 - 1, K[0]);
+    } else {
+      if (MODE != 3) { ldplane(z0 - 1, W[0]); ldplane(z0, W[1]); }
+      ldcells(z0 - 1, K[0]);
+    }
     const bool diry = dirf(iy, 4, 8);
     const T hs = g.hs;
 #pragma unroll 1
     for (int kz = 0; kz < ZS; ++kz) {
       const int iz = z0 + kz;
       if (iz < M) {
-        if (MODE != 3) ldplane(iz + 1, W[2]);
-        ldcells(iz, K[1]);
+        if (fast) {
+          if (MODE != 3) ldplane_fast(iz + 1, W[2]);
+          ldcells_fast(iz, K[1]);
+        } else {
+          if (MODE != 3) ldplane(iz + 1, W[2]);
+          ldcells(iz, K[1]);
+        }
         const bool dirz = dirf(iz, 16, 32);
         const long long rowi = (long long)iz * MM + (long long)iy * M;
 #pragma unroll
