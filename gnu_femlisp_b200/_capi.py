@@ -23,6 +23,7 @@ _ERRNAMES = {-1: "FMG_ERR_ARG", -2: "FMG_ERR_CUDA", -3: "FMG_ERR_STATE", -4: "FM
              -5: "FMG_ERR_NUMERIC", -6: "FMG_ERR_UNSUPPORTED", -7: "FMG_ERR_IO"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
 
 
@@ -101,6 +102,22 @@ SIGNATURES = {
     "fmg_solve_mixed": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), ctypes.POINTER(MixedCfg), _vp, _dp,
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),
+    "fmg_net_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(_vp)]),
+    "fmg_net_destroy": (ctypes.c_int, [_vp]),
+    "fmg_net_nparams": (ctypes.c_long, [_vp]),
+    "fmg_net_get_params": (ctypes.c_int, [_vp, _fp, ctypes.c_long]),
+    "fmg_net_set_params": (ctypes.c_int, [_vp, _fp, ctypes.c_long]),
+    "fmg_net_get_grads": (ctypes.c_int, [_vp, _fp, ctypes.c_long]),
+    "fmg_net_zero_grads": (ctypes.c_int, [_vp]),
+    "fmg_net_adam": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+    "fmg_net_save": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+    "fmg_net_load": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]),
+    "fmg_net_damping": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _dp]),
+    "fmg_net_apply": (ctypes.c_int, [_vp, _vp]),
+    "fmg_net_backward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _dp]),
+    "fmg_learn_loss": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, _dp]),
+    "fmg_learn_step": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(SolveCfg), ctypes.c_int, ctypes.c_ulonglong,
+                                      ctypes.c_int, _dp]),
 }
 
 _lib = None
@@ -134,3 +151,9 @@ def dptr(a):
     import numpy as np
     assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(_dp)
+
+
+def fptr(a):
+    import numpy as np
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_fp)

@@ -21,6 +21,7 @@
 #include <utility>
 
 #include "fmgpu_kernels.cuh"
+#include "fmgpu_learn.cuh"
 #include "fmgpu_mixed.cuh"
 
 using namespace fmg;
@@ -30,7 +31,7 @@ struct fmg_ctx {
   cudaStream_t stream = nullptr;
   double* host_scal = nullptr;  // pinned copy of a grid's scalar slots
   std::string err;
-  int grids = 0;                // live grids: the context outlives them
+  int grids = 0;                // live grids and nets: the context outlives them
   bool closed = false;          // fmg_finalize called while grids were alive
 };
 
@@ -86,6 +87,8 @@ struct fmg_grid {
   std::vector<double*> solp, sparep, rhsp, resp;
   std::vector<int> rp;
   int cur = 0;
+  double* lt[10] = {};         // top-level vectors of the damping-network training loss
+  bool learned = false;        // per-node damping installed by a damping network
   std::vector<void*> allocs;
   int vecs = 0;                // live vectors: the grid outlives them
   bool destroyed = false;      // fmg_grid_destroy called while vectors were alive
@@ -1200,3 +1203,468 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   return launched(c, "solve_mixed");
 }
 
+
+// ========================================================= learned damping
+// The damping network predicts per-node Jacobi damping for every level above
+// the base from the coefficient field; the values become the level's node
+// damping (the same storage fmg_set_node_damping writes), used by the FP64
+// and the mixed-precision cycles alike.  Training minimises the A-norm error
+// contraction of one V-cycle,
+//   L = |e3|_A^2 / |e0|_A^2,  e1 = S e0,  e2 = C e1,  e3 = S e2,
+//   S = I - diag(w) D^-1 A (one damped Jacobi sweep),
+//   C = I - P M R A (coarse-grid correction, M the V-cycle of the level below),
+// on errors e0 that the multigrid itself produces (random vectors after 0..k
+// plain cycles of A e = 0).  With M symmetric (Jacobi pre- and post-smoothing
+// with equal damping, exact coarsest solve) and R = P^T the gradient is
+//   g3 = 2 A e3 / |e0|_A^2
+//   dL/dw += -g3 .* (D^-1 A e2)
+//   g2 = g3 - A D^-1 (w .* g3)          (S^T g3)
+//   g1 = g2 - A P M R g2                (C^T g2)
+//   dL/dw += -g1 .* (D^-1 A e0)
+namespace {
+
+constexpr int S_LOSS = 10, S_E0 = 11, S_E3 = 12;  // grid scalar slots used by the training loss
+
+unsigned long long splitmix(unsigned long long& s) {
+  unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// He-uniform weights, zero hidden biases, output bias giving omega = 0.6
+void net_init_params(std::vector<float>& p, const NetLayout& L, float omin, float omax, unsigned long long seed) {
+  p.assign((size_t)L.n, 0.f);
+  unsigned long long s = seed ^ 0x5DEECE66Dull;
+  auto uni = [&](float a) { return a * (float)((double)(splitmix(s) >> 11) * (2.0 / 9007199254740992.0) - 1.0); };
+  const int nin = 2 << L.dim;  // features actually present in the 16 input channels
+  const float a1 = std::sqrt(6.f / (float)(L.taps * nin)), a2 = std::sqrt(6.f / (float)(L.taps * kNetHid));
+  for (long long i = 0; i < (long long)L.taps * kNetHid * kNetIn; ++i) p[L.w1 + i] = uni(a1);
+  for (long long i = 0; i < (long long)L.taps * kNetHid * kNetHid; ++i) p[L.w2 + i] = uni(a2);
+  for (long long i = 0; i < (long long)L.taps * kNetHid; ++i) p[L.w3 + i] = 0.1f * uni(a2);
+  const double f = (0.6 - omin) / (omax - omin);
+  p[L.b3] = (float)std::log(f / (1.0 - f));
+}
+
+int net_upload(fmg_net* net, const float* host) {
+  fmg_ctx* c = net->ctx;
+  FMG_CK(c, cudaMemcpyAsync(net->P, host, (size_t)net->lay.n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
+  net->weights_stale = true;
+  return FMG_OK;
+}
+
+void net_release(fmg_net* net) {
+  fmg_ctx* c = net->ctx;
+  cudaStreamSynchronize(c->stream);
+  net_free_all(net);
+  delete net;
+  c->grids -= 1;
+  if (c->closed && c->grids == 0) ctx_release(c);
+}
+
+int net_grid_check(fmg_net* net, fmg_grid* g) {
+  if (!net || !g) return FMG_ERR_ARG;
+  if (g->ctx != net->ctx) return set_err(g->ctx, FMG_ERR_ARG, "net and grid belong to different contexts");
+  if (g->dim != net->dim) return set_err(g->ctx, FMG_ERR_ARG, "net is %dD, grid %dD", net->dim, g->dim);
+  if (g->order != 1 || g->nc != 1)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "damping network: scalar Q1 levels only");
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  return FMG_OK;
+}
+
+// features + forward pass on level l; writes the level's node damping
+int net_level_forward(fmg_net* net, fmg_grid* g, int l) {
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  int rc;
+  Lvl& L = g->lev[l];
+  const Lvl& T = g->lev[g->top];
+  if ((rc = net_reserve(net, act_geom(g->dim, (int)T.M, 1)))) return set_err(c, rc, "damping network: no memory");
+  if (!L.omega && (rc = dalloc(g, &L.omega, L.Np))) return rc;
+  long long ncell_top = 1;
+  for (int k = 0; k < g->dim; ++k) ncell_top *= T.n;
+  const bool kc = g->kkind == FMG_K_CELL;
+  if (kc) launch_logmean(g->kcell_d, ncell_top, net->stat + 8, net->stat, st);
+  else launch_set_scalar(net->stat, std::log(g->kconst), st);
+  const ActGeom ag = act_geom(g->dim, (int)L.M, 1);
+  launch_features(ag, (int)L.n, T.n, std::ldexp(1.0, g->top - l), g->np, g->xi_d, kc ? g->kcell_d : nullptr,
+                  g->kconst, net->stat, net->X0, st);
+  if ((rc = net_forward(net, ag, L.omega, st))) return set_err(c, rc, "damping network forward failed");
+  return launched(c, "damping network forward");
+}
+
+int net_finish(fmg_net* net) {
+  const char* msg = nullptr;
+  int rc = net_check_error(net, net->ctx->stream, &msg);
+  if (rc) return set_err(net->ctx, rc, "%s", msg);
+  return FMG_OK;
+}
+
+int learn_vectors(fmg_grid* g) {
+  if (g->lt[0]) return FMG_OK;
+  int rc;
+  for (double*& v : g->lt)
+    if ((rc = dalloc(g, &v, g->lev[g->top].Np))) return rc;
+  return FMG_OK;
+}
+
+// M R y on the level below the top (result in that level's solution vector)
+void coarse_apply(fmg_grid* g, const fmg_solve_cfg& cf, const double* y, cudaStream_t st) {
+  const int t = g->top;
+  launch_restrict(view(g, t), view(g, t - 1), y, g->resp[t - 1], g->rhsp[t - 1], g->solp[t - 1], st);
+  g->cur = t - 1;
+  g->rp[t - 1] = 1;
+  MG mg{g, cf, false, st};
+  mg.lmgc();
+  g->cur = t;
+}
+
+// loss of one error sample and its gradient with respect to the top-level
+// damping w (device); scal[S_LOSS] (+)= L * weight, gw (+)= weight * dL/dw
+void learn_loss_grad(fmg_grid* g, const fmg_solve_cfg& cf, const double* e0, const double* w, double* gw,
+                     double weight, bool first, cudaStream_t st) {
+  const LevelView T = view(g, g->top);
+  const long long n = T.N, Np = T.Np;
+  const double* A = T.A;
+  const int ce = g->center;
+  double *u = g->lt[0], *v0 = g->lt[1], *e1 = g->lt[2], *e2 = g->lt[3], *v2 = g->lt[4], *e3 = g->lt[5],
+         *g3 = g->lt[6], *t = g->lt[7], *g2 = g->lt[8], *q = g->lt[9];
+  launch_spmv(T, e0, nullptr, u, nullptr, nullptr, st);                     // u = A e0
+  launch_dot(e0, u, n, reducer(g, EPI_STORE, S_E0), st);                    // |e0|_A^2
+  launch_dinv(A, ce, Np, u, v0, n, st);                                     // v0 = D^-1 A e0
+  launch_sub_wv(e0, w, v0, e1, n, st);                                      // e1 = S e0
+  launch_spmv(T, e1, nullptr, u, nullptr, nullptr, st);                     // u = A e1
+  coarse_apply(g, cf, u, st);
+  launch_fill(q, n, 0.0, st);
+  launch_prolong(view(g, g->top - 1), T, g->solp[g->top - 1], q, st);      // q = P M R A e1
+  launch_sub_wv(e1, nullptr, q, e2, n, st);                                 // e2 = C e1
+  launch_spmv(T, e2, nullptr, u, nullptr, nullptr, st);
+  launch_dinv(A, ce, Np, u, v2, n, st);                                     // v2 = D^-1 A e2
+  launch_sub_wv(e2, w, v2, e3, n, st);                                      // e3 = S e2
+  launch_spmv(T, e3, nullptr, u, nullptr, nullptr, st);                     // u = A e3
+  launch_dot(e3, u, n, reducer(g, EPI_STORE, S_E3), st);
+  launch_ratio_acc(g->scal, S_LOSS, S_E3, S_E0, weight, first, st);
+  launch_scale_by(u, 2.0 * weight, g->scal, S_E0, g3, n, st);               // g3
+  launch_gomega(g3, v2, gw, !first, n, st);                                 // post-smoother term
+  launch_wg_dinv(A, ce, Np, w, g3, t, n, st);                               // t = w g3 / d
+  launch_spmv(T, t, g3, g2, nullptr, nullptr, st);                          // g2 = g3 - A t
+  coarse_apply(g, cf, g2, st);
+  launch_fill(q, n, 0.0, st);
+  launch_prolong(view(g, g->top - 1), T, g->solp[g->top - 1], q, st);      // q = P M R g2
+  launch_spmv(T, q, g2, t, nullptr, nullptr, st);                           // g1 = g2 - A q
+  launch_gomega(t, v0, gw, true, n, st);                                    // pre-smoother term
+}
+
+int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
+  int rc = check_cfg(g, cf);
+  if (rc) return rc;
+  if (cf->smoother != FMG_JACOBI || cf->combination != FMG_MULTIPLICATIVE || cf->pre_steps != 1 ||
+      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training loss: Jacobi V(1,1) with at least two levels");
+  return FMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmg_net_create(fmg_ctx* c, int dim, unsigned long long seed, fmg_net** out) {
+  if (!c || !out || c->closed) return FMG_ERR_ARG;
+  *out = nullptr;
+  if (dim != 2 && dim != 3) return set_err(c, FMG_ERR_UNSUPPORTED, "damping network: dim %d (2 or 3)", dim);
+  FMG_CK(c, cudaSetDevice(c->device));
+  fmg_net* net = new (std::nothrow) fmg_net();
+  if (!net) return FMG_ERR_NOMEM;
+  net->ctx = c;
+  net->dim = dim;
+  net->lay = net_layout(dim);
+  net->seed = seed;
+  net->omega_min = 0.1f;
+  net->omega_max = 1.3f;
+  c->grids += 1;
+  const NetLayout& L = net->lay;
+  const size_t T = (size_t)L.taps, nb = sizeof(__nv_bfloat16);
+  int rc = FMG_OK;
+  if ((rc = net_alloc(net, (void**)&net->P, L.n * sizeof(float))) ||
+      (rc = net_alloc(net, (void**)&net->G, L.n * sizeof(float))) ||
+      (rc = net_alloc(net, (void**)&net->Mo, L.n * sizeof(float))) ||
+      (rc = net_alloc(net, (void**)&net->Vo, L.n * sizeof(float))) ||
+      (rc = net_alloc(net, (void**)&net->wf1, T * kNetHid * kNetIn * nb)) ||
+      (rc = net_alloc(net, (void**)&net->wf2, T * kNetHid * kNetHid * nb)) ||
+      (rc = net_alloc(net, (void**)&net->wf3, T * kNetOut * kNetHid * nb)) ||
+      (rc = net_alloc(net, (void**)&net->wb2, T * kNetHid * kNetHid * nb)) ||
+      (rc = net_alloc(net, (void**)&net->wb3, T * kNetHid * kNetOut * nb)) ||
+      (rc = net_alloc(net, (void**)&net->stat, 512 * sizeof(double))) ||
+      (rc = net_alloc(net, (void**)&net->err, sizeof(unsigned)))) {
+    net_release(net);
+    return set_err(c, rc, "damping network: device allocation failed");
+  }
+  std::vector<float> p;
+  net_init_params(p, L, net->omega_min, net->omega_max, seed);
+  if ((rc = net_upload(net, p.data()))) {
+    net_release(net);
+    return rc;
+  }
+  *out = net;
+  return FMG_OK;
+}
+
+int fmg_net_destroy(fmg_net* net) {
+  if (!net) return FMG_ERR_ARG;
+  net_release(net);
+  return FMG_OK;
+}
+
+long fmg_net_nparams(const fmg_net* net) { return net ? (long)net->lay.n : -1; }
+
+int fmg_net_get_params(fmg_net* net, float* host, long n) {
+  if (!net || !host || n != (long)net->lay.n) return FMG_ERR_ARG;
+  fmg_ctx* c = net->ctx;
+  FMG_CK(c, cudaMemcpyAsync(host, net->P, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
+  return FMG_OK;
+}
+
+int fmg_net_set_params(fmg_net* net, const float* host, long n) {
+  if (!net || !host || n != (long)net->lay.n) return FMG_ERR_ARG;
+  for (long i = 0; i < n; ++i)
+    if (!std::isfinite(host[i])) return set_err(net->ctx, FMG_ERR_NUMERIC, "parameter %ld is not finite", i);
+  return net_upload(net, host);
+}
+
+int fmg_net_get_grads(fmg_net* net, float* host, long n) {
+  if (!net || !host || n != (long)net->lay.n) return FMG_ERR_ARG;
+  fmg_ctx* c = net->ctx;
+  FMG_CK(c, cudaMemcpyAsync(host, net->G, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
+  return FMG_OK;
+}
+
+int fmg_net_zero_grads(fmg_net* net) {
+  if (!net) return FMG_ERR_ARG;
+  FMG_CK(net->ctx, cudaMemsetAsync(net->G, 0, (size_t)net->lay.n * sizeof(float), net->ctx->stream));
+  return FMG_OK;
+}
+
+int fmg_net_adam(fmg_net* net, double lr, double beta1, double beta2, double eps) {
+  if (!net || !(lr > 0) || !(beta1 >= 0 && beta1 < 1) || !(beta2 >= 0 && beta2 < 1) || !(eps > 0)) return FMG_ERR_ARG;
+  launch_adam(net, (float)lr, (float)beta1, (float)beta2, (float)eps, net->ctx->stream);
+  return launched(net->ctx, "adam");
+}
+
+int fmg_net_damping(fmg_net* net, fmg_grid* g, int level, double* host_omega) {
+  int rc = net_grid_check(net, g);
+  if (rc) return rc;
+  if (level <= g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d has no smoother", level);
+  if ((rc = net_level_forward(net, g, level))) return rc;
+  if ((rc = net_finish(net))) return rc;
+  const Lvl& L = g->lev[level];
+  if (host_omega) {
+    FMG_CK(g->ctx, cudaMemcpyAsync(host_omega, L.omega, L.N * sizeof(double), cudaMemcpyDeviceToHost, g->ctx->stream));
+    FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+  }
+  return FMG_OK;
+}
+
+int fmg_net_apply(fmg_net* net, fmg_grid* g) {
+  int rc = net_grid_check(net, g);
+  if (rc) return rc;
+  for (int l = g->top; l > g->base; --l)
+    if ((rc = net_level_forward(net, g, l))) return rc;
+  if ((rc = net_finish(net))) return rc;
+  g->learned = true;
+  return FMG_OK;
+}
+
+int fmg_net_backward(fmg_net* net, fmg_grid* g, int level, const double* host_gomega) {
+  int rc = net_grid_check(net, g);
+  if (rc) return rc;
+  if (!host_gomega || level <= g->base || level > g->top) return FMG_ERR_ARG;
+  const Lvl& L = g->lev[level];
+  const ActGeom ag = act_geom(g->dim, (int)L.M, 1);
+  if (!net->have_forward || net->geom.Mx != ag.Mx || net->geom.Mz != ag.Mz || !L.omega)
+    return set_err(g->ctx, FMG_ERR_STATE, "backward needs the forward pass of this level (fmg_net_damping)");
+  if ((rc = learn_vectors(g))) return rc;
+  FMG_CK(g->ctx, cudaMemcpyAsync(g->lt[0], host_gomega, L.N * sizeof(double), cudaMemcpyHostToDevice, g->ctx->stream));
+  if ((rc = net_backward(net, g->lt[0], L.omega, g->ctx->stream))) return set_err(g->ctx, rc, "backward failed");
+  if ((rc = launched(g->ctx, "damping network backward"))) return rc;
+  return net_finish(net);
+}
+
+int fmg_learn_loss(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* e0, double* loss, double* host_gomega) {
+  if (!g || !loss) return FMG_ERR_ARG;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  int rc = learn_cfg_check(g, cfg);
+  if (rc) return rc;
+  if (vec_check(e0, g, g->top)) return FMG_ERR_ARG;
+  if ((rc = learn_vectors(g))) return rc;
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const Lvl& T = g->lev[g->top];
+  // gradient into xs2, damping from the level (or the scalar damping in xs)
+  const double* w = T.omega;
+  if (!w) {
+    launch_fill(g->xs, T.N, cfg->damp, st);
+    w = g->xs;
+  }
+  learn_loss_grad(g, *cfg, e0->d, w, g->xs2, 1.0, true, st);
+  if ((rc = launched(c, "learn loss"))) return rc;
+  if ((rc = read_scalars(g))) return rc;
+  *loss = c->host_scal[S_LOSS];
+  if (host_gomega) {
+    FMG_CK(c, cudaMemcpyAsync(host_gomega, g->xs2, T.N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FMG_CK(c, cudaStreamSynchronize(st));
+  }
+  return FMG_OK;
+}
+
+// One training step on one grid: forward pass on every level (the coarse
+// levels' damping is used by the cycle but not differentiated), nsamples
+// error samples made by the multigrid (sample s: a random vector after
+// s mod (max_cycles + 1) plain V-cycles of A e = 0), the mean loss and its
+// gradient, and the backward pass; gradients are added to the net's
+// accumulator (fmg_net_adam applies and clears them).
+int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsamples, unsigned long long seed,
+                   int max_cycles, double* loss) {
+  int rc = net_grid_check(net, g);
+  if (rc) return rc;
+  if ((rc = learn_cfg_check(g, cfg))) return rc;
+  if (nsamples < 1 || max_cycles < 0 || !loss) return FMG_ERR_ARG;
+  if ((rc = learn_vectors(g))) return rc;
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  for (int l = g->base + 1; l < g->top; ++l)
+    if ((rc = net_level_forward(net, g, l))) return rc;
+  if ((rc = net_level_forward(net, g, g->top))) return rc;  // last: its activations feed the backward pass
+  Lvl& T = g->lev[g->top];
+  const long long n = T.N;
+  double* gw = g->xs2;
+  double* e = g->xs;
+  double* spare = g->w2;
+  for (int s = 0; s < nsamples; ++s) {
+    launch_rand_fill(e, g->dim, T.M, g->dmask, seed * 1000003ull + (unsigned long long)s, st);
+    const int ncyc = s % (max_cycles + 1);
+    if (ncyc > 0) {  // plain cycles: hide the learned damping
+      std::vector<double*> saved(g->lev.size());
+      for (size_t l = 0; l < g->lev.size(); ++l) { saved[l] = g->lev[l].omega; g->lev[l].omega = nullptr; }
+      MG mg{g, *cfg, false, st};
+      launch_fill(g->q, n, 0.0, st);  // b = 0
+      for (int k = 0; k < ncyc; ++k) {
+        launch_spmv(view(g, g->top), e, g->q, g->r, nullptr, nullptr, st);  // r = 0 - A e
+        mg.iterate(&e, &spare, g->q, g->r);
+      }
+      for (size_t l = 0; l < g->lev.size(); ++l) g->lev[l].omega = saved[l];
+    }
+    learn_loss_grad(g, *cfg, e, T.omega, gw, 1.0 / nsamples, s == 0, st);
+  }
+  if ((rc = launched(c, "learn step"))) return rc;
+  if ((rc = net_backward(net, gw, T.omega, st))) return set_err(c, rc, "backward failed");
+  if ((rc = launched(c, "learn backward"))) return rc;
+  if ((rc = read_scalars(g))) return rc;
+  *loss = c->host_scal[S_LOSS];
+  if ((rc = net_finish(net))) return rc;
+  if (!std::isfinite(*loss)) return set_err(c, FMG_ERR_NUMERIC, "training loss is %g", *loss);
+  return FMG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ weight files
+// Layout (little endian): "FMGDNET1", u32 version (1), u32 dim, u64 nparams,
+// f32 omega_min, f32 omega_max, u64 seed, u64 optimiser steps, f32 params[],
+// then the FNV-1a 64 hash of every preceding byte.
+namespace {
+
+constexpr char kNetMagic[8] = {'F', 'M', 'G', 'D', 'N', 'E', 'T', '1'};
+
+uint64_t fnv1a(const unsigned char* p, size_t n) {
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = 0; i < n; ++i) { h ^= p[i]; h *= 1099511628211ull; }
+  return h;
+}
+
+template <typename T>
+void put(std::vector<unsigned char>& b, const T& v) {
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+  b.insert(b.end(), p, p + sizeof(T));
+}
+
+template <typename T>
+T get(const unsigned char* p) {
+  T v;
+  std::memcpy(&v, p, sizeof(T));
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmg_net_save(fmg_net* net, const char* path) {
+  if (!net || !path) return FMG_ERR_ARG;
+  std::vector<float> p((size_t)net->lay.n);
+  int rc = fmg_net_get_params(net, p.data(), (long)p.size());
+  if (rc) return rc;
+  std::vector<unsigned char> b(kNetMagic, kNetMagic + 8);
+  put<uint32_t>(b, 1u);
+  put<uint32_t>(b, (uint32_t)net->dim);
+  put<uint64_t>(b, (uint64_t)net->lay.n);
+  put<float>(b, net->omega_min);
+  put<float>(b, net->omega_max);
+  put<uint64_t>(b, (uint64_t)net->seed);
+  put<uint64_t>(b, (uint64_t)net->adam_t);
+  const unsigned char* pp = reinterpret_cast<const unsigned char*>(p.data());
+  b.insert(b.end(), pp, pp + p.size() * sizeof(float));
+  put<uint64_t>(b, fnv1a(b.data(), b.size()));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_err(net->ctx, FMG_ERR_IO, "cannot write %s", path);
+  const size_t w = std::fwrite(b.data(), 1, b.size(), f);
+  const int cl = std::fclose(f);
+  if (w != b.size() || cl != 0) return set_err(net->ctx, FMG_ERR_IO, "short write to %s", path);
+  return FMG_OK;
+}
+
+int fmg_net_load(fmg_ctx* c, const char* path, fmg_net** out) {
+  if (!c || !path || !out) return FMG_ERR_ARG;
+  *out = nullptr;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_err(c, FMG_ERR_IO, "cannot read %s", path);
+  std::vector<unsigned char> b;
+  unsigned char buf[65536];
+  size_t k;
+  while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) {
+    b.insert(b.end(), buf, buf + k);
+    if (b.size() > ((size_t)64 << 20)) break;
+  }
+  std::fclose(f);
+  const size_t head = 8 + 4 + 4 + 8 + 4 + 4 + 8 + 8;
+  if (b.size() < head + 8 || std::memcmp(b.data(), kNetMagic, 8) != 0)
+    return set_err(c, FMG_ERR_IO, "%s: not a damping-network file", path);
+  if (get<uint64_t>(b.data() + b.size() - 8) != fnv1a(b.data(), b.size() - 8))
+    return set_err(c, FMG_ERR_IO, "%s: checksum mismatch (corrupted file)", path);
+  const uint32_t ver = get<uint32_t>(b.data() + 8), dim = get<uint32_t>(b.data() + 12);
+  const uint64_t n = get<uint64_t>(b.data() + 16);
+  if (ver != 1 || (dim != 2 && dim != 3) || n != (uint64_t)net_layout((int)dim).n ||
+      b.size() != head + n * sizeof(float) + 8)
+    return set_err(c, FMG_ERR_IO, "%s: unsupported version, dimension or size", path);
+  const float omin = get<float>(b.data() + 24), omax = get<float>(b.data() + 28);
+  if (!(omin > 0.f) || !(omax > omin) || !(omax < 2.f))
+    return set_err(c, FMG_ERR_IO, "%s: bad damping range", path);
+  fmg_net* net = nullptr;
+  int rc = fmg_net_create(c, (int)dim, get<uint64_t>(b.data() + 32), &net);
+  if (rc) return rc;
+  net->omega_min = omin;
+  net->omega_max = omax;
+  net->adam_t = (long long)get<uint64_t>(b.data() + 40);
+  std::vector<float> p((size_t)n);
+  std::memcpy(p.data(), b.data() + head, n * sizeof(float));
+  if ((rc = fmg_net_set_params(net, p.data(), (long)n))) {
+    fmg_net_destroy(net);
+    return rc == FMG_ERR_NUMERIC ? set_err(c, FMG_ERR_IO, "%s: parameters are not finite", path) : rc;
+  }
+  *out = net;
+  return FMG_OK;
+}
+
+}  // extern "C"

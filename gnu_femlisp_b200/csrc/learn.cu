@@ -1,0 +1,870 @@
+// learn.cu -- kernels and handle of the damping network (the learned part of
+// the smoother: per-node Jacobi damping predicted from the coefficient field).
+//
+// Every convolution of the net -- the three forward layers and the two
+// data-gradient layers of the backward pass -- is one implicit GEMM on the
+// 5th-generation tensor cores.  A CTA owns 8 x 16 output nodes of one plane
+// (the 128 rows of one tcgen05.mma), stages the (8+2) x (16+2) x 3 halo of
+// its input activations in shared memory in the no-swizzle K-major layout,
+// and for each of the 3^D taps issues MMAs whose A operand is that halo
+// shifted by the tap -- a different start address of the same shared memory,
+// no copy -- against the tap's weights, accumulating the 128 x Cout tile in
+// tensor memory.  The CTA is persistent: it stages the weights once and walks
+// its tiles; two CTAs share an SM so one stages while the other multiplies.
+//
+// The weight gradients are tensor-core GEMMs as well: for each tap,
+// dW[co][ci] = sum over nodes of G[node][co] X[node + tap][ci], the node
+// dimension being K.  The staged gradient tile and the staged input halo are
+// read MN-major (their 8 channels are the contiguous 16 bytes), M = 64 with
+// the gradient channels zero-padded, 8 taps accumulating side by side in
+// tensor memory across all tiles of a CTA; per-CTA partials are then summed
+// in a fixed order.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "fmgpu_learn.cuh"
+#include "umma.cuh"
+
+namespace fmg {
+
+NetLayout net_layout(int dim) {
+  NetLayout L;
+  L.dim = dim;
+  L.taps = dim == 3 ? 27 : 9;
+  long long o = 0;
+  L.w1 = o; o += (long long)L.taps * kNetHid * kNetIn;
+  L.b1 = o; o += kNetHid;
+  L.w2 = o; o += (long long)L.taps * kNetHid * kNetHid;
+  L.b2 = o; o += kNetHid;
+  L.w3 = o; o += (long long)L.taps * kNetHid;
+  L.b3 = o; o += 1;
+  L.n = o;
+  return L;
+}
+
+ActGeom act_geom(int D, int M, int planes) {
+  ActGeom g;
+  g.D = D;
+  g.Mx = M; g.My = M; g.Mz = D == 3 ? M : planes;
+  g.Px = M + 2; g.Py = M + 2; g.Pz = D == 3 ? M + 2 : planes;
+  return g;
+}
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int kThreads = 128;                  // 4 warps: one per tensor-memory lane quadrant
+constexpr int TX = 8, TY = 16;                 // output tile (x fastest): 128 MMA rows
+constexpr int HX = TX + 2, HY = TY + 2;        // halo tile
+constexpr int kRowB = 16;                      // one 8-channel chunk of one node
+constexpr int kHyB = HX * kRowB;               // 160: halo y-row stride
+constexpr int kPlaneB = HY * kHyB;             // 2880: halo plane stride
+
+template <int D>
+struct Tp {
+  static constexpr int TAPS = D == 3 ? 27 : 9;
+  static constexpr int ZH = D == 3 ? 3 : 1;    // halo planes
+  static constexpr int CHB = ZH * kPlaneB;     // bytes of one 8-channel chunk of the halo
+  static constexpr int ROWS = HX * HY * ZH;    // halo nodes
+};
+
+struct TileGeo {
+  int Mx, My, Mz, Px, Py, Pz, ntx, nty;
+  long long ntiles;
+};
+
+TileGeo tile_geo(const ActGeom& g) {
+  TileGeo t;
+  t.Mx = g.Mx; t.My = g.My; t.Mz = g.Mz; t.Px = g.Px; t.Py = g.Py; t.Pz = g.Pz;
+  t.ntx = (g.Mx + TX - 1) / TX;
+  t.nty = (g.My + TY - 1) / TY;
+  t.ntiles = (long long)t.ntx * t.nty * g.Mz;
+  return t;
+}
+
+__device__ __forceinline__ void tile_xyz(const TileGeo& t, long long id, int& tx, int& ty, int& tz) {
+  tx = (int)(id % t.ntx);
+  const long long r = id / t.ntx;
+  ty = (int)(r % t.nty);
+  tz = (int)(r / t.nty);
+}
+
+// tap = (dx+1) + 3 (dy+1) [+ 9 (dz+1)]: byte offset of the shifted window in the halo
+template <int D>
+__device__ __forceinline__ uint32_t tap_off(int tap) {
+  const int dx = tap % 3, dy = (tap / 3) % 3, dz = D == 3 ? tap / 9 : 0;
+  return (uint32_t)(dz * kPlaneB + dy * kHyB + dx * kRowB);
+}
+
+// padded index of interior node (ix, iy) of plane tz
+template <int D>
+__device__ __forceinline__ long long pad_index(const TileGeo& t, int ix, int iy, int tz) {
+  const int pz = D == 3 ? tz + 1 : tz;
+  return ((long long)pz * t.Py + iy + 1) * t.Px + ix + 1;
+}
+
+// halo of input activations [npad][C] -> shared memory, chunk c of halo node
+// r = hx + HX (hy + HY hz) at byte c*CHB + 16 r (zeros outside the array)
+template <int D, int C>
+__device__ __forceinline__ void stage_halo(uint8_t* hs, const bf16* __restrict__ in, const TileGeo& t, int tx,
+                                           int ty, int tz) {
+  constexpr int ROWS = Tp<D>::ROWS, CHB = Tp<D>::CHB;
+  for (int idx = threadIdx.x; idx < (C / 8) * ROWS; idx += kThreads) {
+    const int c = idx / ROWS, r = idx - c * ROWS;
+    const int hx = r % HX, hy = (r / HX) % HY, hz = r / (HX * HY);
+    const int px = tx * TX + hx, py = ty * TY + hy, pz = tz + hz;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (px < t.Px && py < t.Py && pz < t.Pz)
+      v = __ldg(reinterpret_cast<const uint4*>(in + (((long long)pz * t.Py + py) * t.Px + px) * C) + c);
+    *reinterpret_cast<uint4*>(hs + c * CHB + r * kRowB) = v;
+  }
+}
+
+// weights [taps][COUT][CIN] -> per tap a K-major COUT x CIN tile
+template <int TAPS, int CIN, int COUT>
+__device__ __forceinline__ void stage_weights(uint8_t* ws, const bf16* __restrict__ w) {
+  constexpr int CH = CIN / 8;
+  for (int idx = threadIdx.x; idx < TAPS * COUT * CH; idx += kThreads) {
+    const int c = idx % CH, co = (idx / CH) % COUT, tap = idx / (CH * COUT);
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + ((long long)tap * COUT + co) * CIN) + c);
+    *reinterpret_cast<uint4*>(ws + tap * (COUT * CIN * 2) + umma::kmajor_offset(co, c * 8, CIN)) = v;
+  }
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+enum ConvEpi { EPI_RELU = 0, EPI_OMEGA = 1, EPI_MASK = 2 };
+
+struct ConvArgs {
+  TileGeo t;
+  const bf16* in;     // [npad][CIN]
+  const bf16* w;      // [taps][COUT][CIN]
+  const float* bias;  // EPI_RELU: COUT values; EPI_OMEGA: 1
+  const bf16* mask;   // EPI_MASK: activation [npad][COUT] whose relu is differentiated
+  bf16* out;          // [npad][COUT]
+  double* omega;      // EPI_OMEGA: level order
+  float omin, omax;
+  unsigned* err;
+};
+
+template <int D, int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
+  constexpr int TAPS = Tp<D>::TAPS, CHB = Tp<D>::CHB;
+  constexpr int WTAP = COUT * CIN * 2;
+  constexpr uint32_t IDESC = umma::idesc_bf16(128, COUT, false, false);
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* ws = smem;
+  uint8_t* hs = smem + TAPS * WTAP;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  stage_weights<TAPS, CIN, COUT>(ws, a.w);
+  if (warp == 0) umma::tmem_alloc(&tslot, 32);
+  if (tid == 0) umma::mbar_init(&bar);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tslot;
+  const uint32_t hb = umma::smem_u32(hs), wb = umma::smem_u32(ws);
+  uint32_t phase = 0;
+  bool failed = false;
+  for (long long id = blockIdx.x; id < a.t.ntiles; id += gridDim.x) {
+    int tx, ty, tz;
+    tile_xyz(a.t, id, tx, ty, tz);
+    stage_halo<D, CIN>(hs, a.in, a.t, tx, ty, tz);
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after();
+      uint32_t acc = 0;
+      for (int tap = 0; tap < TAPS; ++tap) {
+        const uint32_t aoff = tap_off<D>(tap);
+#pragma unroll
+        for (int kh = 0; kh < CIN / 16; ++kh) {
+          // A: rows = 8 x-nodes (16 B apart) x 16 y-rows (kHyB apart), K chunks CHB apart
+          const uint64_t ad = umma::make_desc(hb + aoff + 2 * kh * CHB, CHB, kHyB);
+          // B: the tap's COUT x CIN weights, K chunks 128 B apart, 8-row groups (CIN/8)*128 apart
+          const uint64_t bd = umma::make_desc(wb + tap * WTAP + kh * 256, 128, (CIN / 8) * 128);
+          umma::mma_bf16(tmem, ad, bd, IDESC, acc);
+          acc = 1;
+        }
+      }
+      umma::mma_commit(&bar);
+    }
+    const bool ok = umma::mbar_wait(&bar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    umma::fence_after();
+    float v[COUT];
+    umma::tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16), v);
+    const int r = warp * 32 + lane, ix = tx * TX + (r & 7), iy = ty * TY + (r >> 3);
+    if (ix < a.t.Mx && iy < a.t.My) {
+      const long long p = pad_index<D>(a.t, ix, iy, tz);
+      if constexpr (EPI == EPI_RELU) {
+        uint32_t pk[COUT / 2];
+#pragma unroll
+        for (int c = 0; c < COUT; c += 2)
+          pk[c / 2] = pack2(fmaxf(v[c] + __ldg(a.bias + c), 0.f), fmaxf(v[c + 1] + __ldg(a.bias + c + 1), 0.f));
+        uint4* o = reinterpret_cast<uint4*>(a.out + p * COUT);
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q) o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+      } else if constexpr (EPI == EPI_OMEGA) {
+        const float z = v[0] + __ldg(a.bias);
+        const float s = 1.f / (1.f + __expf(-z));
+        const long long i = ((long long)tz * a.t.My + iy) * a.t.Mx + ix;
+        a.omega[i] = (double)(a.omin + (a.omax - a.omin) * s);
+      } else {  // EPI_MASK
+        const uint4* m = reinterpret_cast<const uint4*>(a.mask + p * COUT);
+        uint4* o = reinterpret_cast<uint4*>(a.out + p * COUT);
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q) {
+          uint4 mm = __ldg(m + q);
+          const bf16* mh = reinterpret_cast<const bf16*>(&mm);
+          uint32_t pk[4];
+#pragma unroll
+          for (int e = 0; e < 8; e += 2) {
+            const float g0 = __bfloat162float(mh[e]) > 0.f ? v[8 * q + e] : 0.f;
+            const float g1 = __bfloat162float(mh[e + 1]) > 0.f ? v[8 * q + e + 1] : 0.f;
+            pk[e / 2] = pack2(g0, g1);
+          }
+          o[q] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+      }
+    }
+    umma::fence_before();  // the loads above precede the next tile's MMAs (barrier at the loop top)
+  }
+  if (failed) {
+    if (tid == 0) atomicOr(a.err, 1u);
+    umma::mbar_wait(&bar, phase ^ 1u);  // bounded: let the tile's MMAs drain before freeing
+  }
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after();
+    umma::tmem_dealloc(tmem, 32);
+  }
+}
+
+struct WgradArgs {
+  TileGeo t;
+  const bf16* g;   // [npad][CG] gradient at the layer's output
+  const bf16* x;   // [npad][CX] the layer's input
+  float* part;     // [gridDim.x][TAPS][CG][CX]
+  unsigned* err;
+};
+
+constexpr int kWgTaps = 8;  // taps per CTA: one block of tensor-memory columns each
+
+template <int D, int CG, int CX>
+__global__ void __launch_bounds__(kThreads) k_wgrad(WgradArgs a) {
+  constexpr int TAPS = Tp<D>::TAPS, CHB = Tp<D>::CHB;
+  constexpr int GCH = TY * 128;  // one 8-channel chunk of the gradient tile (16 y-rows of 8 nodes)
+  constexpr uint32_t IDESC = umma::idesc_bf16(64, CX, true, true);
+  constexpr uint32_t TCOLS = kWgTaps * CX;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* gs = smem;            // 8 chunks (M = 64); chunks >= CG/8 stay zero
+  uint8_t* hs = smem + 8 * GCH;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tap0 = blockIdx.y * kWgTaps;
+  const int nt = min(kWgTaps, TAPS - tap0);
+
+  for (int i = tid; i < (8 - CG / 8) * GCH / 16; i += kThreads)
+    reinterpret_cast<uint4*>(gs + (CG / 8) * GCH)[i] = make_uint4(0u, 0u, 0u, 0u);
+  if (warp == 0) umma::tmem_alloc(&tslot, TCOLS);
+  if (tid == 0) umma::mbar_init(&bar);
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tslot;
+  const uint32_t gb = umma::smem_u32(gs), hb = umma::smem_u32(hs);
+  uint32_t phase = 0;
+  bool failed = false, any = false;
+  for (long long id = blockIdx.x; id < a.t.ntiles; id += gridDim.x) {
+    int tx, ty, tz;
+    tile_xyz(a.t, id, tx, ty, tz);
+    for (int idx = tid; idx < (CG / 8) * 128; idx += kThreads) {
+      const int c = idx >> 7, r = idx & 127, x = r & 7, y = r >> 3;
+      const int ix = tx * TX + x, iy = ty * TY + y;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (ix < a.t.Mx && iy < a.t.My)
+        v = __ldg(reinterpret_cast<const uint4*>(a.g + pad_index<D>(a.t, ix, iy, tz) * CG) + c);
+      *reinterpret_cast<uint4*>(gs + c * GCH + y * 128 + x * 16) = v;
+    }
+    stage_halo<D, CX>(hs, a.x, a.t, tx, ty, tz);
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after();
+      for (int j = 0; j < nt; ++j) {
+        const uint32_t boff = tap_off<D>(tap0 + j);
+#pragma unroll
+        for (int kk = 0; kk < TY / 2; ++kk) {  // K = 16 nodes: y-rows 2kk, 2kk+1
+          // A = G^T (M = channels, MN-major): K groups (y-rows) 128 B apart, channel chunks GCH apart
+          const uint64_t ad = umma::make_desc(gb + kk * 256, 128, GCH);
+          // B = shifted halo (N = channels, MN-major): K groups kHyB apart, channel chunks CHB apart
+          const uint64_t bd = umma::make_desc(hb + boff + 2 * kk * kHyB, kHyB, CHB);
+          umma::mma_bf16(tmem + j * CX, ad, bd, IDESC, (any || kk > 0) ? 1u : 0u);
+        }
+      }
+      umma::mma_commit(&bar);
+    }
+    const bool ok = umma::mbar_wait(&bar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    any = true;
+  }
+  if (failed) {
+    if (tid == 0) atomicOr(a.err, 1u);
+    umma::mbar_wait(&bar, phase ^ 1u);
+  } else {
+    umma::fence_after();
+    float* dst = a.part + (long long)blockIdx.x * TAPS * CG * CX;
+    if (warp < 2) {  // M = 64: row m lives in lane (m % 16) + 32 (m / 16)
+      const int m = warp * 16 + lane;
+      for (int j = 0; j < nt; ++j) {
+        float v[CX];
+        umma::tmem_ld<CX>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * CX), v);
+        if (lane < 16 && m < CG) {
+          float* o = dst + ((long long)(tap0 + j) * CG + m) * CX;
+#pragma unroll
+          for (int c = 0; c < CX; ++c) o[c] = any ? v[c] : 0.f;
+        }
+      }
+    }
+  }
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after();
+    umma::tmem_dealloc(tmem, TCOLS);
+  }
+}
+
+// out[tap][co][ci] += sum over s of part[s][tap][co][ci], co < nco, fixed order
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int S, int taps, int CG, int CX, int nco,
+                               float* __restrict__ out) {
+  const long long n = (long long)taps * nco * CX;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int ci = (int)(k % CX);
+    const long long r = k / CX;
+    const int co = (int)(r % nco), tap = (int)(r / nco);
+    float s = 0.f;
+    for (int q = 0; q < S; ++q) s += part[(((long long)q * taps + tap) * CG + co) * CX + ci];
+    out[k] += s;
+  }
+}
+
+// zero the ghost layer of an activation buffer laid out for t (buffers are
+// shared between levels, so the ghost nodes of a smaller level may hold data)
+template <int D>
+__global__ void k_zero_ghosts(TileGeo t, int chunks, uint4* __restrict__ buf) {
+  const long long npad = (long long)t.Px * t.Py * t.Pz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npad; p += (long long)gridDim.x * blockDim.x) {
+    const int px = (int)(p % t.Px), py = (int)((p / t.Px) % t.Py), pz = (int)(p / ((long long)t.Px * t.Py));
+    const bool ghost = px == 0 || px == t.Px - 1 || py == 0 || py == t.Py - 1 ||
+                       (D == 3 && (pz == 0 || pz == t.Pz - 1));
+    if (!ghost) continue;
+    for (int c = 0; c < chunks; ++c) buf[p * chunks + c] = make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
+template <int D>
+void zero_ghosts(const TileGeo& t, int C, bf16* buf, cudaStream_t st) {
+  const long long npad = (long long)t.Px * t.Py * t.Pz;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_zero_ghosts<D><<<(unsigned)std::min<long long>((npad + 255) / 256, 4096), 256, 0, st>>>(
+      t, C / 8, reinterpret_cast<uint4*>(buf));
+}
+
+// per-block channel sums of [npad][C] -> part[block][C]
+template <int C>
+__global__ void __launch_bounds__(256) k_colsum(const bf16* __restrict__ g, long long npad, float* __restrict__ part) {
+  constexpr int J = 256 / C;
+  __shared__ float s[256];
+  const int c = threadIdx.x % C, j = threadIdx.x / C;
+  float acc = 0.f;
+  for (long long p = (long long)blockIdx.x * J + j; p < npad; p += (long long)gridDim.x * J)
+    acc += __bfloat162float(g[p * C + c]);
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  if (j == 0) {
+    float t = 0.f;
+    for (int q = 0; q < J; ++q) t += s[q * C + c];
+    part[(long long)blockIdx.x * C + c] = t;
+  }
+}
+
+__global__ void k_colsum_final(const float* __restrict__ part, int nb, int C, int nout, float* __restrict__ out) {
+  const int c = threadIdx.x;
+  if (c >= nout) return;
+  float t = 0.f;
+  for (int b = 0; b < nb; ++b) t += part[(long long)b * C + c];
+  out[c] += t;
+}
+
+// dZ (16 channels, channel 0 used) from dL/domega: dL/dz = g (w - wmin)(wmax - w)/(wmax - wmin)
+template <int D>
+__global__ void k_dz(TileGeo t, const double* __restrict__ gw, const double* __restrict__ w, float omin, float omax,
+                     bf16* __restrict__ dz) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)t.Mx * t.My * t.Mz) return;
+  const int ix = (int)(i % t.Mx), iy = (int)((i / t.Mx) % t.My), iz = (int)(i / ((long long)t.Mx * t.My));
+  const double om = w[i];
+  const float d = (float)(gw[i] * (om - omin) * (omax - om) / (double)(omax - omin));
+  uint4* o = reinterpret_cast<uint4*>(dz + pad_index<D>(t, ix, iy, iz) * kNetOut);
+  o[0] = make_uint4(pack2(d, 0.f), 0u, 0u, 0u);
+  o[1] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// FP32 parameters -> BF16 forward weights and flipped/transposed backward weights
+__global__ void k_net_weights(const float* __restrict__ P, NetLayout L, bf16* wf1, bf16* wf2, bf16* wf3, bf16* wb2,
+                              bf16* wb3) {
+  const long long T = L.taps;
+  const long long n1 = T * kNetHid * kNetIn, n2 = T * kNetHid * kNetHid, n3 = T * kNetOut * kNetHid;
+  const long long nb2 = n2, nb3 = T * kNetHid * kNetOut;
+  const long long tot = n1 + n2 + n3 + nb2 + nb3;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
+    long long q = k;
+    if (q < n1) { wf1[q] = __float2bfloat16_rn(P[L.w1 + q]); continue; }
+    q -= n1;
+    if (q < n2) { wf2[q] = __float2bfloat16_rn(P[L.w2 + q]); continue; }
+    q -= n2;
+    if (q < n3) {  // [tap][co 16][ci 32]
+      const int ci = (int)(q % kNetHid), co = (int)((q / kNetHid) % kNetOut), tap = (int)(q / (kNetHid * kNetOut));
+      wf3[q] = __float2bfloat16_rn(co == 0 ? P[L.w3 + (long long)tap * kNetHid + ci] : 0.f);
+      continue;
+    }
+    q -= n3;
+    if (q < nb2) {  // [tap][o = ci of W2][i = co of W2] = W2[flip][co][ci]
+      const int i = (int)(q % kNetHid), o = (int)((q / kNetHid) % kNetHid), tap = (int)(q / (kNetHid * kNetHid));
+      const long long ft = T - 1 - tap;
+      wb2[q] = __float2bfloat16_rn(P[L.w2 + (ft * kNetHid + i) * kNetHid + o]);
+      continue;
+    }
+    q -= nb2;
+    {  // [tap][o = ci of W3 (32)][i (16)]: i = 0 carries W3[flip][ci]
+      const int i = (int)(q % kNetOut), o = (int)((q / kNetOut) % kNetHid), tap = (int)(q / (kNetOut * kNetHid));
+      const long long ft = T - 1 - tap;
+      wb3[q] = __float2bfloat16_rn(i == 0 ? P[L.w3 + ft * kNetHid + o] : 0.f);
+    }
+  }
+}
+
+__global__ void k_adam(float* __restrict__ P, float* __restrict__ G, float* __restrict__ Mo, float* __restrict__ Vo,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = G[i];
+  const float m = b1 * Mo[i] + (1.f - b1) * g;
+  const float v = b2 * Vo[i] + (1.f - b2) * g * g;
+  Mo[i] = m;
+  Vo[i] = v;
+  P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+  G[i] = 0.f;
+}
+
+// deterministic sum of log k over n values: per-block partials then one block
+__global__ void __launch_bounds__(kBlock) k_logsum(const double* __restrict__ k, long long n, double* __restrict__ part) {
+  __shared__ double sm[8];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * kBlock + threadIdx.x; i < n; i += (long long)gridDim.x * kBlock)
+    acc += log(k[i]);
+  const double s = dr_fold256(acc, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kBlock) k_logmean_final(const double* __restrict__ part, int nb, long long n,
+                                                          double* __restrict__ out) {
+  __shared__ double sm[8];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nb; b += kBlock) acc += part[b];
+  const double s = dr_fold256(acc, sm);
+  if (threadIdx.x == 0) *out = s / (double)n;
+}
+
+__global__ void k_set_scalar(double* p, double v) { *p = v; }
+
+__global__ void k_ratio_acc(double* scal, int dst, int num, int den, double factor, int first) {
+  const double r = factor * scal[num] / scal[den];
+  scal[dst] = first ? r : scal[dst] + r;
+}
+
+// node features of one Q1 level
+template <int D>
+__global__ void k_features(TileGeo t, int n_l, long long n_top, double ratio, int np, const double* __restrict__ xi,
+                           const double* __restrict__ kcell, double kconst, const double* __restrict__ mean,
+                           bf16* __restrict__ X0) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)t.Mx * t.My * t.Mz) return;
+  const int ix = (int)(i % t.Mx), iy = (int)((i / t.Mx) % t.My), iz = (int)(i / ((long long)t.Mx * t.My));
+  const int node[3] = {ix, iy, iz};
+  constexpr int NC = 1 << D;
+  float f[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) f[c] = 0.f;
+  const double mu = *mean;
+  for (int c = 0; c < NC; ++c) {
+    int cc[3] = {0, 0, 0};
+    bool in = true;
+    for (int k = 0; k < D; ++k) {
+      cc[k] = node[k] - 1 + ((c >> k) & 1);
+      in = in && cc[k] >= 0 && cc[k] < n_l;
+    }
+    if (!in) continue;
+    double lk;
+    if (kcell) {
+      int nq = 1;
+      for (int k = 0; k < D; ++k) nq *= np;
+      double s = 0.0;
+      for (int q = 0; q < nq; ++q) {
+        const int qi[3] = {q % np, (q / np) % np, q / (np * np)};
+        long long fi[3] = {0, 0, 0};
+        for (int k = 0; k < D; ++k) fi[k] = (long long)floor(((double)cc[k] + xi[qi[k]]) * ratio);
+        s += log(kcell[fi[0] + n_top * (fi[1] + n_top * fi[2])]);
+      }
+      lk = s / nq;
+    } else {
+      lk = log(kconst);
+    }
+    f[c] = (float)fmin(fmax((lk - mu) * 0.5, -8.0), 8.0);
+    f[NC + c] = 1.f;
+  }
+  uint4* o = reinterpret_cast<uint4*>(X0 + pad_index<D>(t, ix, iy, iz) * kNetIn);
+  o[0] = make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
+  o[1] = make_uint4(pack2(f[8], f[9]), pack2(f[10], f[11]), pack2(f[12], f[13]), pack2(f[14], f[15]));
+}
+
+// ----------------------------------------------------- FP64 loss helpers
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed) {
+  long long N = M;
+  for (int k = 1; k < D; ++k) N *= M;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const long long c[3] = {i % M, D > 1 ? (i / M) % M : 0, D > 2 ? i / (M * M) : 0};
+  bool dir = false;
+  for (int k = 0; k < D; ++k) {
+    if (c[k] == 0 && ((dmask >> (2 * k)) & 1)) dir = true;
+    if (c[k] == M - 1 && ((dmask >> (2 * k + 1)) & 1)) dir = true;
+  }
+  const unsigned long long h = mix64(seed * 0x100000001B3ull ^ (unsigned long long)i);
+  e[i] = dir ? 0.0 : (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+__global__ void k_dinv(const double* __restrict__ A, long long Np, const double* __restrict__ u, double* __restrict__ v,
+                       long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = u[i] / A[i];
+}
+
+__global__ void k_sub_wv(const double* __restrict__ x, const double* __restrict__ w, const double* __restrict__ v,
+                         double* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = x[i] - (w ? w[i] * v[i] : v[i]);
+}
+
+__global__ void k_gomega(const double* __restrict__ g, const double* __restrict__ v, double* __restrict__ gw,
+                         int accumulate, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) gw[i] = (accumulate ? gw[i] : 0.0) - g[i] * v[i];
+}
+
+__global__ void k_wg_dinv(const double* __restrict__ A, const double* __restrict__ w, const double* __restrict__ g,
+                          double* __restrict__ t, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) t[i] = w[i] * g[i] / A[i];
+}
+
+__global__ void k_scale_by(const double* __restrict__ x, double s, const double* __restrict__ scal, int slot,
+                           double* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = s * x[i] / scal[slot];
+}
+
+inline unsigned blocks_for(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int D, int CIN, int COUT, int EPI>
+void conv(const ConvArgs& a, cudaStream_t st) {
+  constexpr size_t smem = (size_t)Tp<D>::TAPS * COUT * CIN * 2 + (size_t)(CIN / 8) * Tp<D>::CHB;
+  static bool init = false;
+  if (!init) {
+    cudaFuncSetAttribute(k_conv<D, CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    init = true;
+  }
+  const long long grid = std::min<long long>(a.t.ntiles, 2LL * sm_count());
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_conv<D, CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a);
+}
+
+template <int D, int CG, int CX>
+int wgrad(fmg_net* net, const TileGeo& t, const bf16* g, const bf16* x, long long w_off, int nco, cudaStream_t st) {
+  constexpr int TAPS = Tp<D>::TAPS;
+  constexpr size_t smem = (size_t)8 * TY * 128 + (size_t)(CX / 8) * Tp<D>::CHB;
+  static bool init = false;
+  if (!init) {
+    cudaFuncSetAttribute(k_wgrad<D, CG, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    init = true;
+  }
+  const int groups = (TAPS + kWgTaps - 1) / kWgTaps;
+  const long long S = std::max<long long>(1, std::min<long long>(t.ntiles, (2LL * sm_count()) / groups));
+  const long long need = std::max<long long>(S * TAPS * CG * CX, 256LL * kNetHid);  // colsum partials too
+  if (need > net->part_cap) {
+    if (net->part) { cudaStreamSynchronize(st); cudaFree(net->part); net->part = nullptr; net->part_cap = 0; }
+    if (cudaMalloc(&net->part, (size_t)need * sizeof(float)) != cudaSuccess) { cudaGetLastError(); return FMG_ERR_NOMEM; }
+    net->part_cap = need;
+  }
+  WgradArgs a;
+  a.t = t; a.g = g; a.x = x; a.part = net->part; a.err = net->err;
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  k_wgrad<D, CG, CX><<<dim3((unsigned)S, (unsigned)groups), kThreads, smem, st>>>(a);
+  const long long nout = (long long)TAPS * nco * CX;
+  k_wgrad_reduce<<<blocks_for(nout), 256, 0, st>>>(net->part, (int)S, TAPS, CG, CX, nco, net->G + w_off);
+  return FMG_OK;
+}
+
+template <int C>
+void colsum(fmg_net* net, const bf16* g, long long npad, long long b_off, int nout, cudaStream_t st) {
+  const int nb = 256;
+  // the partials use the head of the weight-gradient scratch (reserved by wgrad first)
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  k_colsum<C><<<nb, 256, 0, st>>>(g, npad, net->part);
+  k_colsum_final<<<1, 32, 0, st>>>(net->part, nb, C, nout, net->G + b_off);
+}
+
+template <int D>
+int forward_d(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st) {
+  const TileGeo t = tile_geo(g);
+  const NetLayout& L = net->lay;
+  zero_ghosts<D>(t, kNetIn, net->X0, st);
+  zero_ghosts<D>(t, kNetHid, net->H1, st);
+  zero_ghosts<D>(t, kNetHid, net->H2, st);
+  ConvArgs a{};
+  a.t = t; a.err = net->err; a.omin = net->omega_min; a.omax = net->omega_max;
+  a.in = net->X0; a.w = net->wf1; a.bias = net->P + L.b1; a.out = net->H1;
+  conv<D, kNetIn, kNetHid, EPI_RELU>(a, st);
+  a.in = net->H1; a.w = net->wf2; a.bias = net->P + L.b2; a.out = net->H2;
+  conv<D, kNetHid, kNetHid, EPI_RELU>(a, st);
+  if (omega) {
+    a.in = net->H2; a.w = net->wf3; a.bias = net->P + L.b3; a.out = nullptr; a.omega = omega;
+    conv<D, kNetHid, kNetOut, EPI_OMEGA>(a, st);
+  }
+  return FMG_OK;
+}
+
+template <int D>
+int backward_d(fmg_net* net, const double* gomega, const double* omega, cudaStream_t st) {
+  const ActGeom& g = net->geom;
+  const TileGeo t = tile_geo(g);
+  const NetLayout& L = net->lay;
+  const long long npad = g.npad();
+  int rc;
+  zero_ghosts<D>(t, kNetOut, net->dZ, st);
+  zero_ghosts<D>(t, kNetHid, net->dP2, st);
+  zero_ghosts<D>(t, kNetHid, net->dP1, st);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_dz<D><<<blocks_for(g.nodes()), 256, 0, st>>>(t, gomega, omega, net->omega_min, net->omega_max, net->dZ);
+  // layer 3: dW3 = sum dZ (x) H2_shift, db3 = sum dZ
+  if ((rc = wgrad<D, kNetOut, kNetHid>(net, t, net->dZ, net->H2, L.w3, 1, st))) return rc;
+  colsum<kNetOut>(net, net->dZ, npad, L.b3, 1, st);
+  ConvArgs a{};
+  a.t = t; a.err = net->err;
+  a.in = net->dZ; a.w = net->wb3; a.mask = net->H2; a.out = net->dP2;
+  conv<D, kNetOut, kNetHid, EPI_MASK>(a, st);
+  // layer 2
+  if ((rc = wgrad<D, kNetHid, kNetHid>(net, t, net->dP2, net->H1, L.w2, kNetHid, st))) return rc;
+  colsum<kNetHid>(net, net->dP2, npad, L.b2, kNetHid, st);
+  a.in = net->dP2; a.w = net->wb2; a.mask = net->H1; a.out = net->dP1;
+  conv<D, kNetHid, kNetHid, EPI_MASK>(a, st);
+  // layer 1
+  if ((rc = wgrad<D, kNetHid, kNetIn>(net, t, net->dP1, net->X0, L.w1, kNetHid, st))) return rc;
+  colsum<kNetHid>(net, net->dP1, npad, L.b1, kNetHid, st);
+  return FMG_OK;
+}
+
+}  // namespace
+
+int net_alloc(fmg_net* net, void** p, size_t bytes) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, bytes ? bytes : 16) != cudaSuccess) {
+    cudaGetLastError();
+    return FMG_ERR_NOMEM;
+  }
+  if (cudaMemset(q, 0, bytes ? bytes : 16) != cudaSuccess) {
+    cudaFree(q);
+    return FMG_ERR_CUDA;
+  }
+  net->allocs.push_back(q);
+  *p = q;
+  return FMG_OK;
+}
+
+static void net_free(fmg_net* net, void* p) {
+  if (!p) return;
+  for (auto it = net->allocs.begin(); it != net->allocs.end(); ++it)
+    if (*it == p) { net->allocs.erase(it); break; }
+  cudaFree(p);
+}
+
+void net_free_all(fmg_net* net) {
+  for (void* p : net->allocs) cudaFree(p);
+  net->allocs.clear();
+  if (net->part) cudaFree(net->part);
+  net->part = nullptr;
+  net->part_cap = 0;
+}
+
+int net_reserve(fmg_net* net, const ActGeom& g) {
+  const long long need = g.npad();
+  if (need <= net->cap) {
+    return FMG_OK;
+  }
+  bf16** bufs[] = {&net->X0, &net->H1, &net->H2, &net->dZ, &net->dP2, &net->dP1};
+  const int ch[] = {kNetIn, kNetHid, kNetHid, kNetOut, kNetHid, kNetHid};
+  cudaDeviceSynchronize();
+  for (int b = 0; b < 6; ++b) {
+    net_free(net, *bufs[b]);
+    *bufs[b] = nullptr;
+  }
+  net->cap = 0;
+  for (int b = 0; b < 6; ++b) {
+    int rc = net_alloc(net, (void**)bufs[b], (size_t)need * ch[b] * sizeof(bf16));
+    if (rc) return rc;
+  }
+  net->cap = need;
+  return FMG_OK;
+}
+
+void net_refresh_weights(fmg_net* net, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_net_weights<<<256, 256, 0, st>>>(net->P, net->lay, net->wf1, net->wf2, net->wf3, net->wb2, net->wb3);
+  net->weights_stale = false;
+}
+
+void launch_logmean(const double* k, long long n, double* scratch, double* out, cudaStream_t st) {
+  const int nb = 256;
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  k_logsum<<<nb, kBlock, 0, st>>>(k, n, scratch);
+  k_logmean_final<<<1, kBlock, 0, st>>>(scratch, nb, n, out);
+}
+
+void launch_features(const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
+                     const double* kcell, double kconst, const double* mean, bf16* X0, cudaStream_t st) {
+  const TileGeo t = tile_geo(g);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (g.D == 3)
+    k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, n_top, ratio, np, xi, kcell, kconst, mean, X0);
+  else
+    k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, n_top, ratio, np, xi, kcell, kconst, mean, X0);
+}
+
+int net_forward(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st) {
+  if (net->weights_stale) net_refresh_weights(net, st);
+  int rc = g.D == 3 ? forward_d<3>(net, g, omega, st) : forward_d<2>(net, g, omega, st);
+  if (rc) return rc;
+  net->geom = g;
+  net->have_forward = true;
+  return FMG_OK;
+}
+
+int net_backward(fmg_net* net, const double* gomega, const double* omega, cudaStream_t st) {
+  if (!net->have_forward) return FMG_ERR_STATE;
+  if (net->weights_stale) net_refresh_weights(net, st);
+  return net->geom.D == 3 ? backward_d<3>(net, gomega, omega, st) : backward_d<2>(net, gomega, omega, st);
+}
+
+void launch_adam(fmg_net* net, float lr, float b1, float b2, float eps, cudaStream_t st) {
+  net->adam_t += 1;
+  const float c1 = 1.f - powf(b1, (float)net->adam_t), c2 = 1.f - powf(b2, (float)net->adam_t);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_adam<<<blocks_for(net->lay.n), 256, 0, st>>>(net->P, net->G, net->Mo, net->Vo, net->lay.n, lr, b1, b2, eps, c1, c2);
+  net->weights_stale = true;
+}
+
+int net_check_error(fmg_net* net, cudaStream_t st, const char** msg) {
+  unsigned h = 0;
+  if (cudaMemcpyAsync(&h, net->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    *msg = "CUDA error in the damping network";
+    return FMG_ERR_CUDA;
+  }
+  if (h) {
+    cudaMemsetAsync(net->err, 0, sizeof(unsigned), st);
+    *msg = "a tensor-core wait of the damping network timed out";
+    return FMG_ERR_CUDA;
+  }
+  return FMG_OK;
+}
+
+void launch_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed, cudaStream_t st) {
+  long long N = M;
+  for (int k = 1; k < D; ++k) N *= M;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_rand_fill<<<blocks_for(N), 256, 0, st>>>(e, D, M, dmask, seed);
+}
+
+void launch_dinv(const double* A, int center, long long Np, const double* u, double* v, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_dinv<<<blocks_for(n), 256, 0, st>>>(A + (long long)center * Np, Np, u, v, n);
+}
+
+void launch_sub_wv(const double* x, const double* w, const double* v, double* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_sub_wv<<<blocks_for(n), 256, 0, st>>>(x, w, v, y, n);
+}
+
+void launch_gomega(const double* g, const double* v, double* gw, bool accumulate, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_gomega<<<blocks_for(n), 256, 0, st>>>(g, v, gw, accumulate ? 1 : 0, n);
+}
+
+void launch_wg_dinv(const double* A, int center, long long Np, const double* w, const double* g, double* t,
+                    long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_wg_dinv<<<blocks_for(n), 256, 0, st>>>(A + (long long)center * Np, w, g, t, n);
+}
+
+void launch_scale_by(const double* x, double s, const double* scal, int slot, double* y, long long n,
+                     cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_scale_by<<<blocks_for(n), 256, 0, st>>>(x, s, scal, slot, y, n);
+}
+
+void launch_ratio_acc(double* scal, int dst, int num, int den, double factor, bool first, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_ratio_acc<<<1, 1, 0, st>>>(scal, dst, num, den, factor, first ? 1 : 0);
+}
+
+void launch_set_scalar(double* p, double v, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_set_scalar<<<1, 1, 0, st>>>(p, v);
+}
+
+}  // namespace fmg

@@ -196,6 +196,53 @@ typedef struct {
 int fmg_solve_mixed(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* x,
                     double* hist, int hist_len, int* nouter, int* ninner, int* status);
 
+/* ------------------------------------------------------ damping network */
+/* No counterpart in the reference: the learned part of the smoother.  A
+   3-layer 3^d convolution net on the node grid of a level (16 input channels:
+   per adjacent cell the centred log coefficient and a presence bit; 32 hidden
+   channels; BF16 weights and activations, FP32 accumulation on the tensor
+   cores) predicts each node's Jacobi damping in [omega_min, omega_max]
+   (0.1, 1.3).  The prediction becomes the level's node damping, i.e. it
+   replaces the scalar damp of <jacobi> (linit.lisp:220-250) node by node in
+   the FP64 and the mixed-precision cycles.  Scalar Q1 grids, d = 2 or 3. */
+typedef struct fmg_net fmg_net;
+
+/* parameters: He-uniform weights from seed, output bias for omega = 0.6 */
+int fmg_net_create(fmg_ctx* ctx, int dim, unsigned long long seed, fmg_net** out);
+int fmg_net_destroy(fmg_net* net);
+/* flat FP32 parameter vector: W1[taps][32][16], b1[32], W2[taps][32][32],
+   b2[32], W3[taps][32], b3[1]; tap = (dx+1) + 3(dy+1) + 9(dz+1) */
+long fmg_net_nparams(const fmg_net* net);
+int fmg_net_get_params(fmg_net* net, float* host, long n);
+int fmg_net_set_params(fmg_net* net, const float* host, long n);
+/* accumulated gradient of the training loss (same layout) */
+int fmg_net_get_grads(fmg_net* net, float* host, long n);
+int fmg_net_zero_grads(fmg_net* net);
+/* one Adam step with the accumulated gradients, which are then cleared */
+int fmg_net_adam(fmg_net* net, double lr, double beta1, double beta2, double eps);
+/* versioned weight file with a checksum; a damaged file fails with FMG_ERR_IO */
+int fmg_net_save(fmg_net* net, const char* path);
+int fmg_net_load(fmg_ctx* ctx, const char* path, fmg_net** out);
+/* forward pass on one level (base < level <= top): installs the node damping
+   of that level and copies it to omega (N values) when omega is not NULL */
+int fmg_net_damping(fmg_net* net, fmg_grid* grid, int level, double* omega);
+/* forward pass on every level above the base (installs the damping) */
+int fmg_net_apply(fmg_net* net, fmg_grid* grid);
+/* backward pass from dL/domega (N host values) of the level of the last
+   fmg_net_damping call; gradients are added to the accumulator */
+int fmg_net_backward(fmg_net* net, fmg_grid* grid, int level, const double* gomega);
+/* Training loss of one error sample e0 on the top level: the A-norm error
+   contraction |S C S e0|_A^2 / |e0|_A^2 of one V(1,1) cycle with the level's
+   current node damping (S the damped Jacobi sweep, C the coarse-grid
+   correction of the cycle below), and its gradient with respect to that
+   damping (N values, when gomega is not NULL).  FP64. */
+int fmg_learn_loss(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_vec* e0, double* loss, double* gomega);
+/* One training step: forward on all levels, nsamples errors generated by the
+   multigrid (sample s: random, then s mod (max_cycles+1) plain V-cycles of
+   A e = 0), mean loss -> *loss, backward into the gradient accumulator. */
+int fmg_learn_step(fmg_net* net, fmg_grid* grid, const fmg_solve_cfg* cfg, int nsamples,
+                   unsigned long long seed, int max_cycles, double* loss);
+
 /* ------------------------------------------------- allocation-free variant */
 /* No counterpart in the reference.  The dot product of fmg_dot for callers
    that cannot allocate device memory: hosts whose device memory is already
