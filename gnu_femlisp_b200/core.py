@@ -177,6 +177,20 @@ class Grid:
                        "solve_mixed")
         return hist[: no.value + ni.value + 1].copy(), no.value, ni.value, st.value
 
+    def learned_judge(self, cfg: C.SolveCfg):
+        """Plain cycle vs the installed node damping (``fmg_learned_judge``);
+        returns (accepted, rho_plain, rho_learned)."""
+        rp, rl, ok = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self.ctx.check(self._lib.fmg_learned_judge(self.h, ctypes.byref(cfg), ctypes.byref(rp), ctypes.byref(rl),
+                                                   ctypes.byref(ok)), "learned_judge")
+        return bool(ok.value), rp.value, rl.value
+
+    def learned_status(self) -> dict:
+        a, rp, rl, rv = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self.ctx.check(self._lib.fmg_learned_status(self.h, ctypes.byref(a), ctypes.byref(rp), ctypes.byref(rl),
+                                                    ctypes.byref(rv)), "learned_status")
+        return {"active": bool(a.value), "rho_plain": rp.value, "rho_learned": rl.value, "reverts": rv.value}
+
     def close(self):
         if getattr(self, "h", None):
             self._lib.fmg_grid_destroy(self.h)

@@ -89,6 +89,9 @@ struct fmg_grid {
   int cur = 0;
   double* lt[10] = {};         // top-level vectors of the damping-network training loss
   bool learned = false;        // per-node damping installed by a damping network
+  double rho_plain = 0.0;      // judge: slow-mode contraction of the plain cycle (0: not measured)
+  double rho_learned = 0.0;    //        and of the learned cycle
+  int reverts = 0;             // mixed solves whose runtime judge fell back to the plain cycle
   std::vector<void*> allocs;
   int vecs = 0;                // live vectors: the grid outlives them
   bool destroyed = false;      // fmg_grid_destroy called while vectors were alive
@@ -692,6 +695,7 @@ int fmg_set_node_damping(fmg_grid* g, int level, const double* host, long n) {
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   if (level <= g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d has no smoother", level);
   Lvl& L = g->lev[level];
+  g->learned = false;  // damping set by hand: no judge
   if (!host) {
     if (L.omega) { cudaStreamSynchronize(g->ctx->stream); dfree(g, L.omega); }
     L.omega = nullptr;
@@ -1150,6 +1154,8 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   *nouter = 0;
   *ninner = 0;
   const int max_restart = mcfg->max_outer > 0 ? mcfg->max_outer : 20;
+  bool judge_active = g->learned;
+  int slow = 0;
   double initial = -1.0;
   int step = 0, iters = 0;  // history slots, CG iterations
   for (int restart = 0; restart <= max_restart; ++restart) {
@@ -1178,6 +1184,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       mx_fcg64_p(X.sc, p, X.q, n, true, st);
     }
     bool converged = false;
+    double rn_prev = dn;
     while (iters <= cfg->maxsteps) {
       mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
       mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
@@ -1188,6 +1195,18 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       const double rn = std::sqrt(X.host[M_RR]);
       if (!std::isfinite(rn)) return set_err(c, FMG_ERR_NUMERIC, "residual is %g at step %d", rn, step);
       if (hist && step < hist_len) hist[step] = rn;
+      if (judge_active) {  // the plain <geometric-cs> judges every learned cycle
+        const double rho = rn / rn_prev;
+        // without a setup verdict, a cycle that removes less than 10% is slower than any working plain cycle
+        const double bound = g->rho_plain > 0 ? g->rho_plain : 0.9;
+        slow = rho > bound ? slow + 1 : 0;
+        if (rho > 1.5 || slow >= 2) {
+          for (auto& V : X.lv) V.om = nullptr;  // plain damping for the rest of the solve
+          judge_active = false;
+          g->reverts += 1;
+        }
+      }
+      rn_prev = rn;
       if ((cfg->rtol > 0 && rn / initial < cfg->rtol) || (cfg->atol > 0 && rn < cfg->atol)) { converged = true; break; }
       const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
       mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
@@ -1213,8 +1232,8 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
 //   L = |e3|_A^2 / |e0|_A^2,  e1 = S e0,  e2 = C e1,  e3 = S e2,
 //   S = I - diag(w) D^-1 A (one damped Jacobi sweep),
 //   C = I - P M R A (coarse-grid correction, M the V-cycle of the level below),
-// on errors e0 that the multigrid itself produces (random vectors after 0..k
-// plain cycles of A e = 0).  With M symmetric (Jacobi pre- and post-smoothing
+// on errors e0 that the multigrid itself produces (random vectors after k
+// cycles of A e = 0 with the current damping).  With M symmetric (Jacobi pre- and post-smoothing
 // with equal damping, exact coarsest solve) and R = P^T the gradient is
 //   g3 = 2 A e3 / |e0|_A^2
 //   dL/dw += -g3 .* (D^-1 A e2)
@@ -1521,10 +1540,14 @@ int fmg_learn_loss(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* e0, dou
 
 // One training step on one grid: forward pass on every level (the coarse
 // levels' damping is used by the cycle but not differentiated), nsamples
-// error samples made by the multigrid (sample s: a random vector after
-// s mod (max_cycles + 1) plain V-cycles of A e = 0), the mean loss and its
+// error samples made by the multigrid itself (a random vector after
+// max_cycles V-cycles of A e = 0 with the current damping: power iterations
+// that turn toward the slowest modes of the cycle), the mean loss and its
 // gradient, and the backward pass; gradients are added to the net's
-// accumulator (fmg_net_adam applies and clears them).
+// accumulator (fmg_net_adam applies and clears them).  For CG the rate is set
+// by the largest eigenvalue mu of the cycle's error propagator E (symmetric
+// and positive semidefinite in the A inner product); on its eigenvector the
+// loss is mu^2 and the gradient that of mu^2.
 int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsamples, unsigned long long seed,
                    int max_cycles, double* loss) {
   int rc = net_grid_check(net, g);
@@ -1544,17 +1567,13 @@ int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsam
   double* spare = g->w2;
   for (int s = 0; s < nsamples; ++s) {
     launch_rand_fill(e, g->dim, T.M, g->dmask, seed * 1000003ull + (unsigned long long)s, st);
-    const int ncyc = s % (max_cycles + 1);
-    if (ncyc > 0) {  // plain cycles: hide the learned damping
-      std::vector<double*> saved(g->lev.size());
-      for (size_t l = 0; l < g->lev.size(); ++l) { saved[l] = g->lev[l].omega; g->lev[l].omega = nullptr; }
+    if (max_cycles > 0) {  // power iterations of the current (learned) cycle: A e = 0
       MG mg{g, *cfg, false, st};
       launch_fill(g->q, n, 0.0, st);  // b = 0
-      for (int k = 0; k < ncyc; ++k) {
+      for (int k = 0; k < max_cycles; ++k) {
         launch_spmv(view(g, g->top), e, g->q, g->r, nullptr, nullptr, st);  // r = 0 - A e
         mg.iterate(&e, &spare, g->q, g->r);
       }
-      for (size_t l = 0; l < g->lev.size(); ++l) g->lev[l].omega = saved[l];
     }
     learn_loss_grad(g, *cfg, e, T.omega, gw, 1.0 / nsamples, s == 0, st);
   }
@@ -1565,6 +1584,93 @@ int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsam
   *loss = c->host_scal[S_LOSS];
   if ((rc = net_finish(net))) return rc;
   if (!std::isfinite(*loss)) return set_err(c, FMG_ERR_NUMERIC, "training loss is %g", *loss);
+  return FMG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ the judge
+namespace {
+
+// A-norm contraction |e_k|_A / |e_{k-1}|_A of the FP64 cycle with the damping
+// currently installed, after k cycles of A e = 0 from a seeded random vector
+int cycle_contraction(fmg_grid* g, const fmg_solve_cfg& cf, int k, unsigned long long seed, double* rho) {
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const Lvl& T = g->lev[g->top];
+  const long long n = T.N;
+  double* e = g->xs;
+  double* spare = g->w2;
+  launch_rand_fill(e, g->dim, T.M, g->dmask, seed, st);
+  launch_fill(g->q, n, 0.0, st);
+  MG mg{g, cf, false, st};
+  for (int it = 0; it < k; ++it) {
+    if (it == k - 1) {
+      launch_spmv(view(g, g->top), e, nullptr, g->a, nullptr, nullptr, st);
+      launch_dot(e, g->a, n, reducer(g, EPI_STORE, S_E0), st);
+    }
+    launch_spmv(view(g, g->top), e, g->q, g->r, nullptr, nullptr, st);
+    mg.iterate(&e, &spare, g->q, g->r);
+  }
+  launch_spmv(view(g, g->top), e, nullptr, g->a, nullptr, nullptr, st);
+  launch_dot(e, g->a, n, reducer(g, EPI_STORE, S_E3), st);
+  int rc;
+  if ((rc = launched(c, "judge"))) return rc;
+  if ((rc = read_scalars(g))) return rc;
+  const double e0 = c->host_scal[S_E0], e1 = c->host_scal[S_E3];
+  *rho = (e0 > 0 && std::isfinite(e1)) ? std::sqrt(e1 / e0) : INFINITY;
+  return FMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The plain <geometric-cs> (scalar :damp) judges the learned damping: both
+// cycles run 4 times on A e = 0 from the same random vector and the learned
+// damping stays installed only if its last-cycle A-norm contraction is no
+// worse than the plain cycle's; otherwise it is removed (the fallback).
+int fmg_learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned, int* accepted) {
+  if (!g || !accepted) return FMG_ERR_ARG;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  int rc = check_cfg(g, cfg);
+  if (rc) return rc;
+  if (cfg->smoother != FMG_JACOBI || g->top <= g->base)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: Jacobi cycles with at least two levels");
+  bool any = false;
+  for (int l = g->base + 1; l <= g->top; ++l) any = any || g->lev[l].omega;
+  if (!any) return set_err(g->ctx, FMG_ERR_STATE, "no node damping installed");
+  const int k = 4;
+  const unsigned long long seed = 0x4A554447ull;
+  std::vector<double*> saved(g->lev.size());
+  for (size_t l = 0; l < g->lev.size(); ++l) { saved[l] = g->lev[l].omega; g->lev[l].omega = nullptr; }
+  double rp = 0, rl = 0;
+  rc = cycle_contraction(g, *cfg, k, seed, &rp);
+  for (size_t l = 0; l < g->lev.size(); ++l) g->lev[l].omega = saved[l];
+  if (rc || (rc = cycle_contraction(g, *cfg, k, seed, &rl))) return rc;
+  g->rho_plain = rp;
+  g->rho_learned = rl;
+  const bool ok = rl <= rp;
+  if (!ok) {  // fall back to the plain cycle
+    cudaStreamSynchronize(g->ctx->stream);
+    for (int l = g->base + 1; l <= g->top; ++l) {
+      dfree(g, g->lev[l].omega);
+      g->lev[l].omega = nullptr;
+    }
+  }
+  g->learned = ok;
+  if (rho_plain) *rho_plain = rp;
+  if (rho_learned) *rho_learned = rl;
+  *accepted = ok ? 1 : 0;
+  return FMG_OK;
+}
+
+int fmg_learned_status(const fmg_grid* g, int* active, double* rho_plain, double* rho_learned, int* reverts) {
+  if (!g) return FMG_ERR_ARG;
+  if (active) *active = g->learned ? 1 : 0;
+  if (rho_plain) *rho_plain = g->rho_plain;
+  if (rho_learned) *rho_learned = g->rho_learned;
+  if (reverts) *reverts = g->reverts;
   return FMG_OK;
 }
 

@@ -163,7 +163,7 @@ class TrainSpec:
     steps: int = 600
     lr: float = 2e-3
     nsamples: int = 4
-    max_cycles: int = 2
+    max_cycles: int = 4
     damp: float = 0.6
 
 
@@ -186,30 +186,36 @@ def training_grids(ctx: Context, spec: TrainSpec):
 
 
 def train(net: DampingNet, grids, cfg: C.SolveCfg, steps: int, lr: float, nsamples: int = 4,
-          max_cycles: int = 2, seed: int = 0, log=None):
-    """Adam on the mean V-cycle loss, cycling through the training grids;
-    returns the loss history."""
+          max_cycles: int = 4, seed: int = 0, lr_end: float | None = None, log=None):
+    """Adam on the mean V-cycle loss, cycling through the training grids, the
+    learning rate decaying from lr to lr_end (cosine); returns the loss history."""
+    lr_end = lr / 10 if lr_end is None else lr_end
     hist = []
     for it in range(steps):
         g = grids[it % len(grids)]
         loss = net.step(g, cfg, nsamples, seed * 1000003 + it, max_cycles)
-        net.adam(lr)
+        rate = lr_end + 0.5 * (lr - lr_end) * (1 + np.cos(np.pi * it / max(1, steps - 1)))
+        net.adam(rate)
         hist.append(loss)
         if log and (it % max(1, steps // 20) == 0 or it == steps - 1):
-            log(f"step {it:5d} loss {loss:.5f}")
+            log(f"step {it:5d} loss {loss:.5f} lr {rate:.2e}")
     return np.array(hist)
 
 
-def mean_loss(grids, cfg: C.SolveCfg, nsamples: int = 4, seed: int = 7) -> float:
-    """Mean V-cycle loss of random errors with the damping currently installed."""
+def mean_loss(grids, cfg: C.SolveCfg, nsamples: int = 4, seed: int = 7, cycles: int = 0) -> float:
+    """Mean V-cycle loss, with the damping currently installed, of random
+    errors after `cycles` cycles of A e = 0 (the same cycle)."""
     tot = 0.0
     for g in grids:
-        e = g.vector()
+        e, z, r = g.vector(), g.vector(), g.vector()
         for s in range(nsamples):
             rng = np.random.default_rng(seed * 7919 + s)
             v = rng.uniform(-1, 1, g.nnodes())
             v[_dirichlet_mask(g)] = 0.0
             e.set(v)
+            for _ in range(cycles):
+                g.residual(e, z, r)
+                g.vcycle(cfg, e, z, r)
             tot += learn_loss(g, cfg, e, want_grad=False)[0]
     return tot / (len(grids) * nsamples)
 

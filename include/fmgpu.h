@@ -238,10 +238,25 @@ int fmg_net_backward(fmg_net* net, fmg_grid* grid, int level, const double* gome
    damping (N values, when gomega is not NULL).  FP64. */
 int fmg_learn_loss(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_vec* e0, double* loss, double* gomega);
 /* One training step: forward on all levels, nsamples errors generated by the
-   multigrid (sample s: random, then s mod (max_cycles+1) plain V-cycles of
-   A e = 0), mean loss -> *loss, backward into the gradient accumulator. */
+   multigrid (random, then max_cycles V-cycles of A e = 0 with the current
+   damping), mean loss -> *loss, backward into the gradient accumulator. */
 int fmg_learn_step(fmg_net* net, fmg_grid* grid, const fmg_solve_cfg* cfg, int nsamples,
                    unsigned long long seed, int max_cycles, double* loss);
+
+/* The judge (no counterpart in the reference): the plain <geometric-cs>
+   cycle (scalar cfg->damp) and the cycle with the installed node damping each
+   run 4 times on A e = 0 from the same random vector; the node damping stays
+   only if its last-cycle A-norm contraction rho_learned <= rho_plain, else it
+   is removed and the plain cycle is used (*accepted = 0).  fmg_solve_mixed
+   then judges every learned cycle as well: after two consecutive CG steps
+   that reduce the residual by less than rho_plain (0.9 when the judge has not
+   run), or one that grows it by more than 1.5x, it drops the node damping for
+   the rest of the solve. */
+int fmg_learned_judge(fmg_grid* grid, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned,
+                      int* accepted);
+/* active: learned damping installed and accepted; reverts: mixed solves whose
+   runtime judge fell back to the plain cycle */
+int fmg_learned_status(const fmg_grid* grid, int* active, double* rho_plain, double* rho_learned, int* reverts);
 
 /* ------------------------------------------------- allocation-free variant */
 /* No counterpart in the reference.  The dot product of fmg_dot for callers
