@@ -6,11 +6,13 @@ multigrid, and the throughput of one V-cycle.
 
 One step = one solve from the device-resident assembled hierarchy (x = 0 to
 ||r||/||r0|| < 1e-10 in the FP64 residual) with the mixed-precision path (FP32
-V-cycle with BF16 coarse residuals inside FP64 iterative refinement).
+V-cycle with BF16 coarse residuals inside FP64 iterative refinement) and the
+per-node damping of the damping network (gnu_femlisp_b200/weights).
 value = top-level DoF / time-to-solution (MDoF/s, whole job: summed over
-replicas); the plain FP64 path is timed beside it.  e2e = the mixed solve
-through the C-ABI from host buffers: coefficient upload, assembly of all
-levels, solve and the solution copied back, every step.
+replicas); the plain FP64 path and the mixed path without the network are
+timed beside it.  e2e = the same solve through the C-ABI from pinned host
+buffers: coefficient upload, assembly of all levels, damping network and
+judge, solve and the solution copied back, every step (wall clock).
 
 --impl reference times the CPU restatement of the reference algorithm
 (oracle/, C++ with OpenMP) on the same workload.
@@ -31,6 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time to 1e-10 rel. residual + MDoF/s per V-cycle: mixed/learned vs FP64 GMG"
+WEIGHTS = os.path.join(ROOT, "gnu_femlisp_b200", "weights", "damping3d.fmgnet")
 HBM_FALLBACK_GBS = 6650.0
 
 
@@ -43,6 +46,7 @@ def parse_args():
     ap.add_argument("--level", type=int, default=8, help="top level (256^3 cells = 8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--matvec-reps", type=int, default=20)
+    ap.add_argument("--no-learned", action="store_true", help="mixed precision without the damping network")
     return ap.parse_args()
 
 
@@ -190,7 +194,9 @@ def run_reference(args, world, rank):
         if it >= args.warmup:
             times.append(dt / max(r.steps, 1))
     per_step = float(np.mean(times))
-    full_steps = int(os.environ.get("FMG_C3_STEPS", "0")) or 35
+    # the plain FP64 GPU path runs this algorithm with bitwise the oracle's
+    # arithmetic and takes 17 CG steps on this workload
+    full_steps = int(os.environ.get("FMG_C3_STEPS", "0")) or 17
     t_solve = per_step * full_steps + t_asm
     val = n / t_solve / 1e6
     line = {
@@ -214,6 +220,7 @@ def run_mine(args, world, rank, local):
 
     import gnu_femlisp_b200 as G
     from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.learn import DampingNet
     C = G._capi
     torch.cuda.set_device(local)
     wl = problems.c3(seed=0, level=args.level)
@@ -225,37 +232,38 @@ def run_mine(args, world, rank, local):
     x_host = torch.empty(n, dtype=torch.float64).pin_memory()  # pinned host output
     k_np, x_np = k_host.numpy(), x_host.numpy()
     cfg = plain_cfg(G)
-    x = g.vector()
+    net = None if args.no_learned else DampingNet.load(ctx, WEIGHTS)
+    x, xm = g.vector(), g.vector()
+    judge = {}
 
-    mcfg_kw = dict(inner_rtol=1e-5, matrix_free=True)
-    xm = g.vector()
+    def clear_damping():
+        for lev in range(g.base + 1, g.top + 1):
+            g.set_node_damping(lev, None)
 
-    def e2e_step():
+    def install_learned():
+        net.apply(g)
+        ok, rp, rl = g.learned_judge(cfg)
+        judge.update(accepted=ok, rho_plain=rp, rho_learned=rl)
+
+    def setup():
         g.set_coefficient(C.FMG_K_CELL, k_np)
         g.assemble()
-        hist, nouter, ninner, status = g.solve_mixed(cfg, xm, **mcfg_kw)
-        x_np[:] = xm.get()
-        return nouter
+        if net is not None:
+            install_learned()
 
-    def dev_step():
+    def plain_step():
         x.fill(0.0)
         return g.solve(cfg, x)
 
     def mixed_step():
         xm.fill(0.0)
-        return g.solve_mixed(cfg, xm, **mcfg_kw)
+        return g.solve_mixed(cfg, xm, matrix_free=True)
 
-    # warm-up (first call assembles)
-    e2e_step()
-    for _ in range(max(args.warmup - 1, 0)):
-        dev_step()
-        mixed_step()
-    hist, steps, status = dev_step()
-    if status != 0:
-        raise RuntimeError(f"plain solve did not converge: {steps} steps")
-    mhist, nouter, ninner, mstatus = mixed_step()
-    if mstatus != 0:
-        raise RuntimeError(f"mixed solve did not converge: {nouter} outer steps")
+    def e2e_step():
+        setup()
+        out = mixed_step()
+        xm.get(out=x_np)
+        return out
 
     def timed(fn, reps):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -271,35 +279,70 @@ def run_mine(args, world, rank, local):
         ctx.synchronize()
         return ev0.elapsed_time(ev1) / 1e3 / reps, out
 
+    def wall(fn, reps):
+        barrier(world)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        out = None
+        for _ in range(reps):
+            out = fn()
+        ctx.synchronize()
+        return (time.perf_counter() - t0) / reps, out
+
+    # ---- plain FP64 path (scalar damping 0.6): the baseline of the speed-up
+    g.set_coefficient(C.FMG_K_CELL, k_np)
+    g.assemble()
+    clear_damping()
+    for _ in range(max(args.warmup, 1)):
+        plain_step()
     clocks = ClockSampler(local)
-    launches0 = ctypes_count(C)
     clocks.start()
-    t_mixed, _ = timed(mixed_step, args.steps)
-    launches = (ctypes_count(C) - launches0) // max(args.steps, 1)
-    t_plain, _ = timed(dev_step, args.steps)
-    clk = clocks.stop()
-    t_mixed_max = allreduce_max(t_mixed, world)
-    t_plain_max = allreduce_max(t_plain, world)
-
-    t_e2e, _ = timed(e2e_step, max(1, min(args.steps, 2)))
-    t_e2e_max = allreduce_max(t_e2e, world)
-
-    # error of the mixed solution against FP64 solutions: the plain path at the
-    # same tolerance and a tight (1e-13) FP64 solve
+    t_plain, (hist, steps, status) = timed(plain_step, args.steps)
+    if status != 0:
+        raise RuntimeError(f"plain solve did not converge: {steps} steps")
     x_plain = x.get()
-    xm.fill(0.0)
-    g.solve_mixed(cfg, xm, **mcfg_kw)
-    x_mixed = xm.get()
+    # ---- mixed precision without the learned damping
+    for _ in range(max(args.warmup, 1)):
+        mixed_step()
+    t_mixed_plain, (mh, no_p, ni_p, st_p) = timed(mixed_step, args.steps)
+    # ---- mixed precision + learned damping: the headline
+    t_setup = None
+    if net is not None:
+        t_setup, _ = wall(install_learned, 3)
+    for _ in range(max(args.warmup, 1)):
+        mixed_step()
+    launches0 = ctypes_count(C)
+    t_head, (mhist, nouter, ninner, mstatus) = timed(mixed_step, args.steps)
+    launches = (ctypes_count(C) - launches0) // max(args.steps, 1)
+    clk = clocks.stop()
+    if mstatus != 0:
+        raise RuntimeError(f"mixed solve did not converge: {nouter} outer steps")
+    status_learned = g.learned_status()
+    t_head_max = allreduce_max(t_head, world)
+    t_plain_max = allreduce_max(t_plain, world)
+    t_mp_max = allreduce_max(t_mixed_plain, world)
+
+    # error of the headline solution against FP64 solutions: the plain path at
+    # the same tolerance and a tight (1e-13) FP64 solve
+    x_head = xm.get()
     tight = plain_cfg(G)
     tight.rtol = 1e-13
     x.fill(0.0)
     g.solve(tight, x)
     x_tight = x.get()
-    err_plain = float(np.linalg.norm(x_mixed - x_plain) / np.linalg.norm(x_plain))
-    err_tight = float(np.linalg.norm(x_mixed - x_tight) / np.linalg.norm(x_tight))
+    err_plain = float(np.linalg.norm(x_head - x_plain) / np.linalg.norm(x_plain))
+    err_tight = float(np.linalg.norm(x_head - x_tight) / np.linalg.norm(x_tight))
     err_plain_tight = float(np.linalg.norm(x_plain - x_tight) / np.linalg.norm(x_tight))
 
-    # one V-cycle (the preconditioner application) on the top level
+    # ---- end to end through the C-ABI from pinned host buffers: coefficient
+    # upload, assembly of all levels, learned damping + judge, mixed solve,
+    # solution download
+    e2e_step()
+    t_e2e, _ = wall(e2e_step, max(1, min(args.steps, 3)))
+    t_e2e_max = allreduce_max(t_e2e, world)
+
+    # ---- one plain FP64 V-cycle (the preconditioner application) on the top level
+    clear_damping()
     mg = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, 0.0, 0.0, 1, C.FMG_MULTIPLICATIVE)
     B = g.vector(values=g.rhs())
     R = g.vector()
@@ -311,7 +354,7 @@ def run_mine(args, world, rank, local):
         vcyc()
     t_cycle, _ = timed(vcyc, 10)
 
-    # dominant kernel: the FP64 stencil matvec of the top level, timed alone
+    # ---- dominant kernel of the plain path: the FP64 stencil matvec of the top level
     P = g.vector(values=np.random.default_rng(1).standard_normal(n))
     Y = g.vector()
 
@@ -328,44 +371,58 @@ def run_mine(args, world, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / t_mv / 1e9
 
-    value = world * n / t_mixed_max / 1e6
+    value = world * n / t_head_max / 1e6
     line = {
         "metric": METRIC, "value": value, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mixed_max * 1e3,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_head_max * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 outer residual/update + f32 V-cycle + bf16 coarse residuals", "data": "synthetic",
         "config": {"workload": wl.name, "nodes": n,
-                   "path": "mixed: FP64 iterative refinement around FP32 flexible CG, V(1,1) Jacobi(0.6) "
-                           "in FP32 (matrix-free top level), BF16 coarse rhs/residuals, FP64 dense LU on 5^3",
+                   "path": ("mixed+learned: FP64 flexible CG (true FP64 residual restarts) preconditioned by "
+                            "an FP32 V(1,1) Jacobi cycle (matrix-free top level) with per-node damping from "
+                            "the damping network, BF16 coarse rhs/residuals, FP64 dense LU on 5^3"
+                            if net is not None else
+                            "mixed: FP64 flexible CG preconditioned by an FP32 V(1,1) Jacobi(0.6) cycle"),
                    "outer_steps": int(nouter), "inner_iterations": int(ninner),
                    "parallelism": "replicas" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (3.9 GB FP64 matrix, 67 MB FP32 coefficients)"},
-        "time_to_solution_s": t_mixed_max,
+                   "l2": "inputs larger than L2 (3.9 GB FP64 matrix, 134 MB FP64 coefficients)"},
+        "time_to_solution_s": t_head_max,
         "plain_fp64": {"time_to_solution_s": t_plain_max, "mdof_per_s": world * n / t_plain_max / 1e6,
                        "cg_steps": int(steps), "solver": "CG + V(1,1) Jacobi(0.6) on assembled FP64 levels"},
-        "speedup_vs_plain_fp64": t_plain_max / t_mixed_max,
+        "mixed_without_learned": {"time_to_solution_s": t_mp_max, "inner_iterations": int(ni_p),
+                                  "speedup_vs_plain_fp64": t_plain_max / t_mp_max},
+        "speedup_vs_plain_fp64": t_plain_max / t_head_max,
         "error_vs_fp64": {"vs_plain_same_tol": err_plain, "vs_fp64_1e-13": err_tight,
                           "plain_vs_fp64_1e-13": err_plain_tight},
         "mdof_per_s_per_vcycle": n / t_cycle / 1e6,
         "vcycle_ms": t_cycle * 1e3,
-        "mixed_ms_per_inner_iteration": t_mixed_max * 1e3 / max(int(ninner), 1),
+        "ms_per_inner_iteration": t_head_max * 1e3 / max(int(ninner), 1),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": "k_spmv<3,1> (top-level FP64 matvec, outer residual)", "peak_kind": peak_kind,
                      "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
         "e2e": {"value": world * n / t_e2e_max / 1e6, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
                 "h2d_bytes_per_step": int(k_np.nbytes), "d2h_bytes_per_step": int(x_np.nbytes),
-                "includes": "coefficient upload + assembly of all levels + mixed solve + solution download"},
+                "time_s": t_e2e_max,
+                "includes": ("coefficient upload + assembly of all levels + damping network on all levels + "
+                             "judge + mixed solve + solution download (wall clock)")},
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if net is not None:
+        line["learned"] = {"weights": os.path.relpath(WEIGHTS, ROOT), "setup_s": t_setup,
+                           "judge": judge, "status": status_learned,
+                           "setup": "damping network on levels 3..8 (tcgen05 convolutions) + plain-cycle judge"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, int(steps))
         line["cpu_baseline"]["note"] = ("plain FP64 algorithm (the reference's), CG step count of the "
                                         "GPU plain solve")
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del P, Y, B, R, X, x, xm, g
+    del P, Y, B, R, X, x, xm
+    if net is not None:
+        net.close()
+    g.close()
     ctx.close()
 
 

@@ -224,8 +224,10 @@ class Vector:
         self.grid.ctx.check(self._lib.fmg_vec_set(self.h, C.dptr(v), v.size), "vec_set")
         return self
 
-    def get(self) -> np.ndarray:
-        out = np.zeros(self.n)
+    def get(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy to the host (into `out`, e.g. a pinned buffer, when given)."""
+        if out is None:
+            out = np.zeros(self.n)
         self.grid.ctx.check(self._lib.fmg_vec_get(self.h, C.dptr(out), self.n), "vec_get")
         return out
 

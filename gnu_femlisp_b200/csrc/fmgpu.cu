@@ -59,10 +59,8 @@ struct fmg_grid {
   std::vector<Lvl> lev;
   int kkind = FMG_K_CONST;
   double kconst = 1.0;
-  std::vector<double> kcell_h;
   int fkind = FMG_F_CONST;
   double fconst = 1.0;
-  std::vector<double> fip_h;
   double xi_h[3] = {0, 0, 0};
   double* xi_d = nullptr;
   double* kcell_d = nullptr;
@@ -543,15 +541,28 @@ int fmg_set_coefficient(fmg_grid* g, int kind, const double* host, long n) {
     case FMG_K_CONST:
       if (n != 1) return set_err(g->ctx, FMG_ERR_ARG, "K_CONST wants 1 value");
       g->kkind = kind; g->kconst = host[0]; break;
-    case FMG_K_CELL:
+    case FMG_K_CELL: {  // straight to the device (read during the call only)
       if (n != ncell) return set_err(g->ctx, FMG_ERR_ARG, "K_CELL wants %lld values, got %ld", ncell, n);
-      g->kkind = kind; g->kcell_h.assign(host, host + n); break;
+      int rc;
+      if (!g->kcell_d && (rc = dalloc(g, &g->kcell_d, ncell))) return rc;
+      FMG_CK(g->ctx, cudaMemcpyAsync(g->kcell_d, host, ncell * sizeof(double), cudaMemcpyHostToDevice, g->ctx->stream));
+      FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+      g->kkind = kind;
+      break;
+    }
     case FMG_F_CONST:
       if (n != 1) return set_err(g->ctx, FMG_ERR_ARG, "F_CONST wants 1 value");
       g->fkind = kind; g->fconst = host[0]; break;
-    case FMG_F_IP:
+    case FMG_F_IP: {
       if (n != ncell * g->nq) return set_err(g->ctx, FMG_ERR_ARG, "F_IP wants %lld values", ncell * g->nq);
-      g->fkind = kind; g->fip_h.assign(host, host + n); break;
+      int rc;
+      if (!g->fip_d && (rc = dalloc(g, &g->fip_d, ncell * g->nq))) return rc;
+      FMG_CK(g->ctx, cudaMemcpyAsync(g->fip_d, host, ncell * g->nq * sizeof(double), cudaMemcpyHostToDevice,
+                                     g->ctx->stream));
+      FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+      g->fkind = kind;
+      break;
+    }
     default: return set_err(g->ctx, FMG_ERR_ARG, "unknown coefficient kind %d", kind);
   }
   g->assembled = false;
@@ -613,18 +624,6 @@ int fmg_assemble(fmg_grid* g) {
   FMG_CK(c, cudaSetDevice(c->device));
   g->assembled = false;
   if ((rc = ensure_buffers(g))) return rc;
-  // coefficient inputs (host -> device)
-  long long ncell_top = 1;
-  for (int k = 0; k < g->dim; ++k) ncell_top *= g->lev[g->top].n;
-  if (g->kkind == FMG_K_CELL) {
-    if (!g->kcell_d && (rc = dalloc(g, &g->kcell_d, ncell_top))) return rc;
-    FMG_CK(c, cudaMemcpyAsync(g->kcell_d, g->kcell_h.data(), ncell_top * sizeof(double), cudaMemcpyHostToDevice, st));
-  }
-  if (g->fkind == FMG_F_IP) {
-    if (!g->fip_d && (rc = dalloc(g, &g->fip_d, ncell_top * g->nq))) return rc;
-    FMG_CK(c, cudaMemcpyAsync(g->fip_d, g->fip_h.data(), ncell_top * g->nq * sizeof(double),
-                              cudaMemcpyHostToDevice, st));
-  }
   const long long n_top = g->lev[g->top].n;
   for (int l = g->top; l >= g->base; --l) {
     Lvl& L = g->lev[l];
@@ -1155,7 +1154,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   *ninner = 0;
   const int max_restart = mcfg->max_outer > 0 ? mcfg->max_outer : 20;
   bool judge_active = g->learned;
-  int slow = 0;
+  double win[3] = {0.0, 0.0, 0.0};
   double initial = -1.0;
   int step = 0, iters = 0;  // history slots, CG iterations
   for (int restart = 0; restart <= max_restart; ++restart) {
@@ -1185,6 +1184,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     }
     bool converged = false;
     double rn_prev = dn;
+    const int it0 = iters;
     while (iters <= cfg->maxsteps) {
       mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
       mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
@@ -1195,15 +1195,22 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       const double rn = std::sqrt(X.host[M_RR]);
       if (!std::isfinite(rn)) return set_err(c, FMG_ERR_NUMERIC, "residual is %g at step %d", rn, step);
       if (hist && step < hist_len) hist[step] = rn;
-      if (judge_active) {  // the plain <geometric-cs> judges every learned cycle
+      if (judge_active) {  // the plain <geometric-cs> judges the learned cycles
+        // CG preconditioned by a cycle converges at least as fast as that
+        // cycle iterated alone; single CG steps fluctuate, so the learned
+        // cycles are judged by the mean reduction of the last 3 steps against
+        // the plain cycle's contraction (0.9 without a setup verdict); the
+        // first step of a CG run may grow the residual and is not judged
         const double rho = rn / rn_prev;
-        // without a setup verdict, a cycle that removes less than 10% is slower than any working plain cycle
-        const double bound = g->rho_plain > 0 ? g->rho_plain : 0.9;
-        slow = rho > bound ? slow + 1 : 0;
-        if (rho > 1.5 || slow >= 2) {
-          for (auto& V : X.lv) V.om = nullptr;  // plain damping for the rest of the solve
-          judge_active = false;
-          g->reverts += 1;
+        if (iters - it0 >= 2) {
+          win[(iters - it0) % 3] = rho;
+          const double bound = g->rho_plain > 0 ? g->rho_plain : 0.9;
+          const bool slow = iters - it0 >= 4 && std::cbrt(win[0] * win[1] * win[2]) > bound;
+          if (rho > 1.5 || slow) {
+            for (auto& V : X.lv) V.om = nullptr;  // plain damping for the rest of the solve
+            judge_active = false;
+            g->reverts += 1;
+          }
         }
       }
       rn_prev = rn;

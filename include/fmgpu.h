@@ -248,10 +248,10 @@ int fmg_learn_step(fmg_net* net, fmg_grid* grid, const fmg_solve_cfg* cfg, int n
    run 4 times on A e = 0 from the same random vector; the node damping stays
    only if its last-cycle A-norm contraction rho_learned <= rho_plain, else it
    is removed and the plain cycle is used (*accepted = 0).  fmg_solve_mixed
-   then judges every learned cycle as well: after two consecutive CG steps
-   that reduce the residual by less than rho_plain (0.9 when the judge has not
-   run), or one that grows it by more than 1.5x, it drops the node damping for
-   the rest of the solve. */
+   then judges the learned cycles as they run: when the mean residual
+   reduction of the last 3 CG steps is worse than rho_plain (0.9 when the judge
+   has not run), or one step after the first of a CG run grows the residual by
+   more than 1.5x, it drops the node damping for the rest of the solve. */
 int fmg_learned_judge(fmg_grid* grid, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned,
                       int* accepted);
 /* active: learned damping installed and accepted; reverts: mixed solves whose

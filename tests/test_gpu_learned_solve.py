@@ -94,18 +94,26 @@ def test_judge_rejects_a_divergent_net(G, ctx):
 
 
 def test_runtime_judge_reverts_to_the_plain_cycle(G, ctx):
+    from gnu_femlisp_b200.learn import DampingNet
     g = _grid(G, ctx, 5, 5)
     cfg = _cfg(G)
     x0 = g.vector()
     _, _, ni_plain, st = g.solve_mixed(cfg, x0)
     assert st == 0
+    # the setup judge measures the plain cycle's contraction (with the trained net)
+    good = DampingNet.load(ctx, WEIGHTS)
+    good.apply(g)
+    ok, rho_p, _ = g.learned_judge(cfg)
+    assert ok
+    # then a divergent damping is installed behind the judge's back
     net = _divergent_net(G, ctx)
-    net.apply(g)  # installed without the setup judge
+    net.apply(g)
     before = g.learned_status()["reverts"]
     x = g.vector()
     hist, _, ni, st = g.solve_mixed(cfg, x)
-    assert st == 0 and hist[-1] / hist[0] < 1e-10
-    assert g.learned_status()["reverts"] == before + 1
-    assert ni <= ni_plain + 6, (ni_plain, ni)
+    rates = (hist[1:] / hist[:-1]).round(3).tolist()
+    assert st == 0 and hist[-1] / hist[0] < 1e-10, rates
+    assert g.learned_status()["reverts"] == before + 1, (rho_p, rates)
+    assert ni <= ni_plain + 6, (ni_plain, ni, rates)
     b = x0.get()
     assert np.linalg.norm(x.get() - b) / np.linalg.norm(b) < 1e-8
