@@ -115,6 +115,17 @@ struct MixedState {
   double* part = nullptr;
   unsigned* counter = nullptr;
   double* host = nullptr;           // pinned copy of sc
+  // CUDA graphs of one flexible-CG step, keyed by every pointer and value the
+  // captured kernels bake in (the V-cycle's ping-pong buffers alternate)
+  struct StepGraph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+    float *q = nullptr, *qs = nullptr;
+    std::vector<float*> x0, x1;
+  };
+  std::vector<StepGraph> graphs;
+  bool graphs_off = false;          // a capture failed: launch eagerly from then on
 };
 
 // ------------------------------------------------------------------ errors
@@ -511,6 +522,8 @@ static void grid_release(fmg_grid* g) {
   cudaStreamSynchronize(c->stream);
   for (void* p : g->allocs) cudaFree(p);
   if (g->mx && g->mx->host) cudaFreeHost(g->mx->host);
+  if (g->mx)
+    for (auto& e : g->mx->graphs) cudaGraphExecDestroy(e.exec);
   delete g->mx;
   delete g;
   c->grids -= 1;
@@ -1120,6 +1133,77 @@ int mx_set_scalar(fmg_grid* g, int slot, double v) {
   return FMG_OK;
 }
 
+// key of one CG step: the vectors it reads and writes, the level buffers in
+// their current ping-pong state, the node damping in use and the cycle's
+// scalar parameters
+std::vector<uint64_t> step_key(const fmg_grid* g, const MixedState& X, const fmg_solve_cfg& c, const double* x) {
+  std::vector<uint64_t> k;
+  auto P = [&](const void* v) { k.push_back((uint64_t)(uintptr_t)v); };
+  P(x); P(X.q); P(X.qs); P(X.r); P(X.rtop);
+  for (size_t l = 0; l < X.lv.size(); ++l) { P(X.x0[l]); P(X.x1[l]); P(X.lv[l].om); }
+  uint64_t d;
+  std::memcpy(&d, &c.damp, sizeof d);
+  k.push_back(d);
+  k.push_back((uint64_t)c.pre_steps << 32 | (uint32_t)c.post_steps);
+  k.push_back((uint64_t)(X.mf ? 1 : 0) << 8 | (uint64_t)g->kkind);
+  return k;
+}
+
+// Runs one CG step through a cached CUDA graph (captured on first use): the
+// ~30 launches of a step then cost one graph launch.  body() must queue the
+// whole step, the scalar copy to the host included, and nothing that waits.
+template <class Body>
+int run_step_graph(fmg_grid* g, const fmg_solve_cfg& c, const double* x, Body body) {
+  MixedState& X = *g->mx;
+  fmg_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  if (X.graphs_off) {
+    body();
+    return launched(ctx, "mixed step");
+  }
+  const std::vector<uint64_t> key = step_key(g, X, c, x);
+  MixedState::StepGraph* e = nullptr;
+  for (auto& ge : X.graphs)
+    if (ge.key == key) e = &ge;
+  if (!e) {
+    const float *q0 = X.q, *qs0 = X.qs;
+    const std::vector<float*> x00 = X.x0, x10 = X.x1;
+    const long long l0 = g_launches.load(std::memory_order_relaxed);
+    cudaGraph_t gr = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      body();
+      ok = cudaStreamEndCapture(st, &gr) == cudaSuccess && gr;
+      ok = ok && cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess;
+      if (gr) cudaGraphDestroy(gr);
+    }
+    const long long nl = g_launches.load(std::memory_order_relaxed) - l0;
+    g_launches.fetch_sub(nl, std::memory_order_relaxed);  // queued in the graph, not launched yet
+    if (!ok) {  // run this step eagerly from the state before the capture
+      cudaGetLastError();
+      X.q = const_cast<float*>(q0); X.qs = const_cast<float*>(qs0);
+      X.x0 = x00; X.x1 = x10;
+      X.graphs_off = true;
+      body();
+      return launched(ctx, "mixed step");
+    }
+    if (X.graphs.size() >= 4) {
+      cudaGraphExecDestroy(X.graphs.front().exec);
+      X.graphs.erase(X.graphs.begin());
+    }
+    MixedState::StepGraph ng;
+    ng.key = key; ng.exec = ex; ng.launches = nl;
+    ng.q = X.q; ng.qs = X.qs; ng.x0 = X.x0; ng.x1 = X.x1;  // state after the step
+    X.graphs.push_back(std::move(ng));
+    e = &X.graphs.back();
+  }
+  FMG_CK(ctx, cudaGraphLaunch(e->exec, st));
+  g_launches.fetch_add(e->launches, std::memory_order_relaxed);
+  X.q = e->q; X.qs = e->qs; X.x0 = e->x0; X.x1 = e->x1;
+  return FMG_OK;
+}
+
 }  // namespace
 
 // Flexible CG in FP64 (recursive FP64 residual, FP64 solution update, FP64
@@ -1185,11 +1269,26 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     bool converged = false;
     double rn_prev = dn;
     const int it0 = iters;
-    while (iters <= cfg->maxsteps) {
+    // one CG step after the first: z = M r with (z, r) and (z, a), p = z/s + beta p,
+    // a = A p with (a, p), x += lam p, r -= lam a with (r, r), scalars to the host
+    auto step_body = [&]() {
+      const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
+      mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
+      mx_fcg64_p(X.sc, p, X.q, n, false, st);
       mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
       mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
-      if ((rc = launched(c, "mixed step"))) return rc;
-      if ((rc = mx_read(g))) return rc;
+      cudaMemcpyAsync(X.host, X.sc, M_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st);
+    };
+    while (iters <= cfg->maxsteps) {
+      if (iters == it0) {
+        mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
+        mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
+        if ((rc = launched(c, "mixed step"))) return rc;
+        if ((rc = mx_read(g))) return rc;
+      } else {
+        if ((rc = run_step_graph(g, *cfg, x, step_body))) return rc;
+        FMG_CK(c, cudaStreamSynchronize(st));
+      }
       ++step;
       ++iters;
       const double rn = std::sqrt(X.host[M_RR]);
@@ -1215,9 +1314,6 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       }
       rn_prev = rn;
       if ((cfg->rtol > 0 && rn / initial < cfg->rtol) || (cfg->atol > 0 && rn < cfg->atol)) { converged = true; break; }
-      const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
-      mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
-      mx_fcg64_p(X.sc, p, X.q, n, false, st);
     }
     if (!converged && iters > cfg->maxsteps) {
       *ninner = iters;
