@@ -111,6 +111,7 @@ struct MixedState {
   std::vector<__nv_bfloat16*> bc, rc;  // coarse rhs and residual (BF16)
   float* k32 = nullptr;             // top-level cell coefficients (FP32)
   float *rtop = nullptr, *r = nullptr, *q = nullptr, *qs = nullptr;  // FP32 top-level vectors
+  float* p32 = nullptr;             // FP32 search direction of the flexible CG
   double* sc = nullptr;
   double* part = nullptr;
   unsigned* counter = nullptr;
@@ -1005,7 +1006,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     const Lvl& T = g->lev[g->top];
     long long ncell = 1;
     for (int k = 0; k < g->dim; ++k) ncell *= T.n;
-    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs};
+    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32};
     for (float** v : tv)
       if ((rc = mx_alloc_f(g, v, T.Np))) return rc;
     if ((rc = mx_alloc_f(g, &X.k32, ncell))) return rc;
@@ -1097,8 +1098,8 @@ struct MixedMG {
       std::swap(x, xn);
     }
   }
-  // FP64 a = A p with (a, p) -> lam = rho / (a, p)
-  void matvec64(const double* p, double* a, const Reduce2& Rl) {
+  // FP64 a = A p for the FP32 search direction p, with (a, p) -> lam = rho / (a, p)
+  void matvec64(const float* p, double* a, const Reduce2& Rl) {
     const LevelView T = view(g, g->top);
     if (top_mf()) {
       const Lvl& L = g->lev[g->top];
@@ -1106,11 +1107,13 @@ struct MixedMG {
       m.k = g->kcell_d; m.omega = nullptr; m.N = L.N; m.M = (int)L.M; m.n = (int)L.n; m.dmask = g->dmask;
       m.hs = L.h / 12.0; m.w = c.damp;
       mx_top_apply64(m, p, a, p, &Rl, st);
-    } else {
-      launch_spmv(T, p, nullptr, a, nullptr, nullptr, st);
+    } else {  // stored FP64 matrix: widen p first
+      mx_f32_to_f64(p, g->xs2, T.N, st);
+      launch_spmv(T, g->xs2, nullptr, a, nullptr, nullptr, st);
       mx_dot2_64(a, p, nullptr, T.N, Rl, st);
     }
   }
+
 };
 
 Reduce2 red2(MixedState& X, int epi, int s0, int s1) {
@@ -1232,7 +1235,8 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   const long long n = T.N;
   double* x = xv->d;
   const double* b = g->rhs;
-  double *r = g->r, *p = g->p, *a = g->a;
+  double *r = g->r, *a = g->a;
+  float* p = X.p32;
   *status = 1;
   *nouter = 0;
   *ninner = 0;

@@ -42,8 +42,8 @@ struct Lev32 {
 
 void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,
                   const double* v2, const Reduce2* R, cudaStream_t st);
-// FP64 y = A x on the top level with (y, v) reduced (epilogue of R)
-void mx_top_apply64(const MFArgs64& g, const double* x, double* y, const double* v, const Reduce2* R,
+// FP64 y = A x on the top level for an FP32 x, with (y, v) reduced (epilogue of R)
+void mx_top_apply64(const MFArgs64& g, const float* x, double* y, const float* v, const Reduce2* R,
                     cudaStream_t st);
 long long mx_top_blocks(int M);  // blocks of the matrix-free kernel (reduction partials)
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
@@ -54,11 +54,12 @@ void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cuda
 void mx_coarse(const double* AinvT, int n, const __nv_bfloat16* b, float* x, cudaStream_t st);
 void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st);
 // FP64 flexible CG: x += lam p, r -= lam a, (r,r), r32 = r * scale (np = padded length)
-void mx_fcg64_update(double* sc, double* x, const double* p, double* r, const double* a, float* r32, long long np,
+void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
                      const Reduce2& R, cudaStream_t st);
-// p = q / s + beta p
-void mx_fcg64_p(const double* sc, double* p, const float* q, long long n, bool first, cudaStream_t st);
+// p = q / s + beta p (FP32 search direction)
+void mx_fcg64_p(const double* sc, float* p, const float* q, long long n, bool first, cudaStream_t st);
+void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st);
 void mx_scale_to32(const double* r, const double* sc, int slot, float* r32, long long n, cudaStream_t st);
-void mx_dot2_64(const double* x, const double* y, const double* y2, long long n, const Reduce2& R, cudaStream_t st);
+void mx_dot2_64(const double* x, const float* y, const double* y2, long long n, const Reduce2& R, cudaStream_t st);
 
 }  // namespace fmg

@@ -288,6 +288,334 @@ k_mf_q1(MFArgsT<T> g, const T* __restrict__ x, const T* __restrict__ b, T* __res
   if (RED) dr_finish2_grid(acc0, acc1, R, smem);
 }
 
+// 2.5D-blocked version of the same operator: a CTA owns a 32 x 8 column of
+// nodes and marches z through ZS planes, one node per thread per plane.  The
+// (32+2) x (8+2) halo of each x plane and the 33 x 9 cells of each cell plane
+// are staged in two-slot shared-memory rings; each thread keeps the 3 x 3
+// neighbourhood of three x planes and the 2 x 2 cells of two cell planes in
+// registers, so a plane is read from HBM once (coalesced rows) and from
+// shared memory 9 + 4 times per node.  The next planes are loaded into
+// registers while the current one is computed.  Values at Dirichlet nodes and
+// outside the grid are staged as zero (eliminated columns), cells outside as
+// zero coefficient.  Per cell the arithmetic is that of k_mf_q1, in the same
+// order.
+constexpr int kMX = 32, kMY = 8;                   // nodes of a CTA plane
+constexpr int kHX = kMX + 2, kHY = kMY + 2;        // node halo
+constexpr int kCX = kMX + 1, kCY = kMY + 1;        // cell tile
+constexpr int kNH = kHX * kHY, kNC = kCX * kCY;    // 340, 297
+constexpr int kMFThreads = kMX * kMY;              // 256
+
+template <typename T, typename TV, int ZS, int MODE, bool RED>
+__global__ void __launch_bounds__(kMFThreads)
+k_mf2(MFArgsT<T> g, const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
+      const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
+  __shared__ T xs[2][kNH];
+  __shared__ T ks[2][kNC];
+  __shared__ double smem[8];
+  const int tid = threadIdx.x, lx = tid & (kMX - 1), ly = tid / kMX;
+  const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, z0 = blockIdx.z * ZS;
+  const int M = g.M, n = g.n, dm = g.dmask;
+  const long long MM = (long long)M * M, nn = (long long)n * n;
+  const int ix = x0 + lx, iy = y0 + ly;
+  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+  // halo entries e = tid, tid + 256 of a node plane / cell plane
+  int hoff[2], coff[2];
+  bool hok[2], cok[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * kMFThreads;
+    const int jx = x0 - 1 + e % kHX, jy = y0 - 1 + e / kHX;
+    hok[q] = e < kNH && jx >= 0 && jx < M && jy >= 0 && jy < M && !dirf(jx, 1, 2) && !dirf(jy, 4, 8);
+    hoff[q] = hok[q] ? jy * M + jx : 0;
+    const int cx = x0 - 1 + e % kCX, cy = y0 - 1 + e / kCX;
+    cok[q] = e < kNC && cx >= 0 && cx < n && cy >= 0 && cy < n;
+    coff[q] = cok[q] ? cy * n + cx : 0;
+  }
+  auto ldx = [&](int jz, T* r) {
+    const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
+    const T* pl = x + (long long)(vz ? jz : 0) * MM;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) r[q] = (vz && hok[q]) ? __ldg(pl + hoff[q]) : T(0);
+  };
+  auto ldk = [&](int cz, T* r) {
+    const bool vz = cz >= 0 && cz < n;
+    const T* pl = g.k + (long long)(vz ? cz : 0) * nn;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) r[q] = (vz && cok[q]) ? __ldg(pl + coff[q]) : T(0);
+  };
+  auto stx = [&](int slot, const T* r) {
+    xs[slot][tid] = r[0];
+    if (tid + kMFThreads < kNH) xs[slot][tid + kMFThreads] = r[1];
+  };
+  auto stk = [&](int slot, const T* r) {
+    ks[slot][tid] = r[0];
+    if (tid + kMFThreads < kNC) ks[slot][tid + kMFThreads] = r[1];
+  };
+  auto rdx = [&](int slot, T (*P)[3]) {
+#pragma unroll
+    for (int ry = 0; ry < 3; ++ry)
+#pragma unroll
+      for (int rx = 0; rx < 3; ++rx) P[ry][rx] = xs[slot][(ly + ry) * kHX + lx + rx];
+  };
+  auto rdk = [&](int slot, T (*K)[2]) {
+#pragma unroll
+    for (int by = 0; by < 2; ++by)
+#pragma unroll
+      for (int bx = 0; bx < 2; ++bx) K[by][bx] = ks[slot][(ly + by) * kCX + lx + bx];
+  };
+  T P[3][3][3];  // [plane z-1, z, z+1][row][col]
+  T K[2][2][2];  // [cell plane z-1, z][row][col]
+  T rx_[2], rk_[2];
+  // prologue: x planes z0-1, z0 and cell plane z0-1 into registers; x plane
+  // z0+1 and cell plane z0 into the rings
+  if (MODE != 3) {
+    ldx(z0 - 1, rx_); stx(0, rx_);
+    ldx(z0, rx_); stx(1, rx_);
+  }
+  ldk(z0 - 1, rk_); stk(0, rk_);
+  __syncthreads();
+  if (MODE != 3) { rdx(0, P[0]); rdx(1, P[1]); }
+  rdk(0, K[0]);
+  __syncthreads();
+  if (MODE != 3) { ldx(z0 + 1, rx_); stx(0, rx_); }
+  ldk(z0, rk_); stk(1, rk_);
+  __syncthreads();
+  int sx = 0, sk = 1;  // ring slots of x plane z+1 and cell plane z
+  double acc0 = 0.0, acc1 = 0.0;
+  const bool own = ix < M && iy < M;
+  const bool diry = dirf(iy, 4, 8), dirx = dirf(ix, 1, 2);
+  const T hs = g.hs;
+  const int zend = min(z0 + ZS, M);
+  // per-node operands of plane iz, loaded one plane ahead
+  const long long col = (long long)iy * M + ix;
+  T bq = T(0), oq = T(0);
+  TV vq = TV(0), v2q = TV(0);
+  auto ldnode = [&](int jz, T& bb, T& oo, TV& vv, TV& vv2) {
+    if (own && jz < zend) {
+      const long long i = (long long)jz * MM + col;
+      if (MODE != 0) bb = __ldg(b + i);
+      if ((MODE == 2 || MODE == 3) && g.omega) oo = __ldg(g.omega + i);
+      if (RED) {
+        vv = __ldg(v + i);
+        if (v2) vv2 = __ldg(v2 + i);
+      }
+    }
+  };
+  ldnode(z0, bq, oq, vq, v2q);
+#pragma unroll 1
+  for (int iz = z0; iz < zend; ++iz) {
+    // prefetch x plane iz+2, cell plane iz+1 and the node operands of iz+1
+    if (MODE != 3) ldx(iz + 2, rx_);
+    ldk(iz + 1, rk_);
+    T bn = T(0), on = T(0);
+    TV vn = TV(0), v2n = TV(0);
+    ldnode(iz + 1, bn, on, vn, v2n);
+    if (MODE != 3) rdx(sx, P[2]);
+    rdk(sk, K[1]);
+    if (own) {
+      const long long i = (long long)iz * MM + col;
+      const bool dir = diry || dirx || dirf(iz, 16, 32);
+      T ax = T(0), d = T(1), xc = T(0);
+      if (dir) {
+        if (MODE != 3) { xc = x[i]; ax = xc; }
+      } else {
+        T ksum = T(0), sacc = T(0);
+        xc = MODE != 3 ? P[1][1][1] : T(0);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
+          const T kc = K[cz][cy][cx];
+          ksum += kc;
+          if (MODE != 3) {
+            const int px = 1 + (2 * cx - 1), py = 1 + (2 * cy - 1), pz = 1 + (2 * cz - 1);
+            const T e = T(4) * xc - P[1][py][px] - P[pz][1][px] - P[pz][py][1] - P[pz][py][px];
+            sacc = fma(kc, e, sacc);
+          }
+        }
+        d = T(4) * hs * ksum;
+        ax = hs * sacc;
+      }
+      T out;
+      if (MODE == 0) out = ax;
+      else if (MODE == 1) out = bq - ax;
+      else if (MODE == 2) out = fma(g.omega ? oq : g.w, (bq - ax) / d, xc);
+      else out = (g.omega ? oq : g.w) * (bq / d);
+      y[i] = out;
+      if (RED) {
+        acc0 = fma((double)out, (double)vq, acc0);
+        if (v2) acc1 = fma((double)out, (double)v2q, acc1);
+      }
+    }
+    bq = bn; oq = on; vq = vn; v2q = v2n;
+    __syncthreads();  // ring slots sx, sk read by every thread
+    if (MODE != 3) stx(sx ^ 1, rx_);
+    stk(sk ^ 1, rk_);
+    __syncthreads();
+    sx ^= 1;
+    sk ^= 1;
+    if (MODE != 3) {
+#pragma unroll
+      for (int ry = 0; ry < 3; ++ry)
+#pragma unroll
+        for (int rx = 0; rx < 3; ++rx) { P[0][ry][rx] = P[1][ry][rx]; P[1][ry][rx] = P[2][ry][rx]; }
+    }
+#pragma unroll
+    for (int by = 0; by < 2; ++by)
+#pragma unroll
+      for (int bx = 0; bx < 2; ++bx) K[0][by][bx] = K[1][by][bx];
+  }
+  if (RED) dr_finish2_grid(acc0, acc1, R, smem);
+}
+
+// Pipelined version: the same 32 x 8 x ZS blocking, but every operand of a
+// plane -- the node halo of x, the cell tile of k and the per-node b, omega,
+// v, v2 -- is copied into a 5-stage shared-memory ring by cp.async (4/8-byte
+// copies; masked entries are zero-filled), two stages ahead of the plane being
+// computed, so each SM keeps tens of KB of loads in flight.  Stage s holds x
+// plane s+1, cell plane s and the node operands of plane s; plane iz reads the
+// x planes of stages iz-2 .. iz and the cell planes of stages iz-1, iz.
+constexpr int kStages = 5;
+
+__device__ __forceinline__ void cpa(void* dst, const void* src, bool ok, int bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(ok ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T, typename TV, typename TX, int ZS, int MODE, bool RED>
+__global__ void __launch_bounds__(kMFThreads)
+k_mf3(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
+      const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
+  constexpr bool HX = MODE != 3;                   // x stencil
+  constexpr bool HB = MODE != 0;                   // right-hand side
+  constexpr bool HO = MODE == 2 || MODE == 3;      // damping
+  __shared__ TX xs[kStages][HX ? kNH : 1];
+  __shared__ T ks[kStages][kNC];
+  __shared__ T bs[kStages][HB ? kMFThreads : 1];
+  __shared__ T os[kStages][HO ? kMFThreads : 1];
+  __shared__ TV vs[kStages][RED ? kMFThreads : 1];
+  __shared__ TV v2s[kStages][RED ? kMFThreads : 1];
+  __shared__ double smem[8];
+  const int tid = threadIdx.x, lx = tid & (kMX - 1), ly = tid / kMX;
+  const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, z0 = blockIdx.z * ZS;
+  const int M = g.M, n = g.n, dm = g.dmask;
+  const long long MM = (long long)M * M, nn = (long long)n * n;
+  const int ix = x0 + lx, iy = y0 + ly;
+  const bool own = ix < M && iy < M;
+  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+  int hoff[2], coff[2];
+  bool hok[2], cok[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * kMFThreads;
+    const int jx = x0 - 1 + e % kHX, jy = y0 - 1 + e / kHX;
+    hok[q] = e < kNH && jx >= 0 && jx < M && jy >= 0 && jy < M && !dirf(jx, 1, 2) && !dirf(jy, 4, 8);
+    hoff[q] = hok[q] ? jy * M + jx : 0;
+    const int cx = x0 - 1 + e % kCX, cy = y0 - 1 + e / kCX;
+    cok[q] = e < kNC && cx >= 0 && cx < n && cy >= 0 && cy < n;
+    coff[q] = cok[q] ? cy * n + cx : 0;
+  }
+  const long long col = own ? (long long)iy * M + ix : 0;
+  const bool omv = g.omega != nullptr;
+  const int zend = min(z0 + ZS, M);
+  auto slot = [&](int st) { return (st - z0 + 2 * kStages) % kStages; };
+  // queue stage st (always one commit group, possibly empty)
+  auto issue = [&](int st) {
+    const int sl = slot(st);
+    if (HX) {
+      const int jz = st + 1;
+      const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
+      const TX* pl = x + (long long)(vz ? jz : 0) * MM;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int e = tid + q * kMFThreads;
+        if (e < kNH) cpa(&xs[sl][e], pl + hoff[q], vz && hok[q], (int)sizeof(TX));
+      }
+    }
+    {
+      const bool vz = st >= 0 && st < n;
+      const T* pl = g.k + (long long)(vz ? st : 0) * nn;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int e = tid + q * kMFThreads;
+        if (e < kNC) cpa(&ks[sl][e], pl + coff[q], vz && cok[q], (int)sizeof(T));
+      }
+    }
+    const bool nz = own && st >= z0 && st < zend;
+    const long long i = (long long)(nz ? st : 0) * MM + col;
+    if (HB) cpa(&bs[sl][tid], b + i, nz, (int)sizeof(T));
+    if (HO && omv) cpa(&os[sl][tid], g.omega + i, nz, (int)sizeof(T));
+    if (RED) {
+      cpa(&vs[sl][tid], v + i, nz, (int)sizeof(TV));
+      if (v2) cpa(&v2s[sl][tid], v2 + i, nz, (int)sizeof(TV));
+    }
+    cpa_commit();
+  };
+  for (int st = z0 - 2; st <= z0 + 1; ++st) issue(st);
+  double acc0 = 0.0, acc1 = 0.0;
+  const bool diry = dirf(iy, 4, 8), dirx = dirf(ix, 1, 2);
+  const T hs = g.hs;
+#pragma unroll 1
+  for (int iz = z0; iz < zend; ++iz) {
+    issue(iz + 2);
+    cpa_wait<2>();  // stages up to iz have landed (this thread's copies)
+    __syncthreads();  // ... and every other thread's
+    if (own) {
+      const long long i = (long long)iz * MM + col;
+      const int sc = slot(iz);
+      const bool dir = diry || dirx || dirf(iz, 16, 32);
+      T ax = T(0), d = T(1), xc = T(0);
+      if (dir) {
+        if (HX) { xc = (T)x[i]; ax = xc; }
+      } else {
+        const TX* X0 = HX ? xs[slot(iz - 2)] : nullptr;  // x plane iz-1
+        const TX* X1 = HX ? xs[slot(iz - 1)] : nullptr;  // x plane iz
+        const TX* X2 = HX ? xs[sc] : nullptr;            // x plane iz+1
+        const T* K0 = ks[slot(iz - 1)];                 // cell plane iz-1
+        const T* K1 = ks[sc];                           // cell plane iz
+        T ksum = T(0), sacc = T(0);
+        const int h = (ly + 1) * kHX + lx + 1;          // centre in the halo
+        xc = HX ? (T)X1[h] : T(0);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
+          const T kc = (cz ? K1 : K0)[(ly + cy) * kCX + lx + cx];
+          ksum += kc;
+          if (HX) {
+            const int sx = 2 * cx - 1, sy = 2 * cy - 1;
+            const TX* Xz = cz ? X2 : X0;
+            const T e = T(4) * xc - (T)X1[h + sy * kHX + sx] - (T)Xz[h + sx] - (T)Xz[h + sy * kHX] -
+                        (T)Xz[h + sy * kHX + sx];
+            sacc = fma(kc, e, sacc);
+          }
+        }
+        d = T(4) * hs * ksum;
+        ax = hs * sacc;
+      }
+      T out;
+      const T bq = HB ? bs[sc][tid] : T(0);
+      const T oq = (HO && omv) ? os[sc][tid] : g.w;
+      if (MODE == 0) out = ax;
+      else if (MODE == 1) out = bq - ax;
+      else if (MODE == 2) out = fma(oq, (bq - ax) / d, xc);
+      else out = oq * (bq / d);
+      y[i] = out;
+      if (RED) {
+        acc0 = fma((double)out, (double)vs[sc][tid], acc0);
+        if (v2) acc1 = fma((double)out, (double)v2s[sc][tid], acc1);
+      }
+    }
+    __syncthreads();  // the slot of stage iz-2 is refilled by the next issue
+  }
+  cpa_wait<0>();
+  if (RED) dr_finish2_grid(acc0, acc1, R, smem);
+}
+
 // ------------------------------------------------------ stored FP32 levels
 template <int D, int P>
 struct St32 {
@@ -477,6 +805,58 @@ k_prolong_q1(int MF, int MC, int dmask, const float* __restrict__ xc, float* __r
   xf[i] += acc;
 }
 
+// 3D Q1 prolongation by coarse node: thread (I, J, K) updates the fine nodes
+// (2I+a, 2J+b, 2K+c), a, b, c in {0, 1}, from the 8 coarse values at
+// I..I+1, J..J+1, K..K+1, loaded once; each fine node is summed with the
+// weights and in the order of k_prolong_q1 (coarse Dirichlet values read as
+// zero, which is what a zero weight gives there).
+__global__ void __launch_bounds__(kBlock)
+k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __restrict__ xf) {
+  const int I = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, K = blockIdx.z;
+  if (I >= MC || J >= MC) return;
+  const long long MC2 = (long long)MC * MC, MF2 = (long long)MF * MF;
+  float v[2][2][2];
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const int ci = I + dx, cj = J + dy, ck = K + dz;
+        const bool ok = ci < MC && cj < MC && ck < MC && !fdir(ci, MC, 0, dmask) && !fdir(cj, MC, 1, dmask) &&
+                        !fdir(ck, MC, 2, dmask);
+        v[dz][dy][dx] = ok ? __ldg(xc + ck * MC2 + (long long)cj * MC + ci) : 0.f;
+      }
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int fz = 2 * K + c;
+    if (fz >= MF || fdir(fz, MF, 2, dmask)) continue;
+    const float wz0 = c ? .5f : 1.f, wz1 = c ? .5f : 0.f;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int fy = 2 * J + b;
+      if (fy >= MF || fdir(fy, MF, 1, dmask)) continue;
+      const float wy0 = b ? .5f : 1.f, wy1 = b ? .5f : 0.f;
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int fx = 2 * I + a;
+        if (fx >= MF || fdir(fx, MF, 0, dmask)) continue;
+        const float wx0 = a ? .5f : 1.f, wx1 = a ? .5f : 0.f;
+        float acc = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int bx = q & 1, by = (q >> 1) & 1, bz = q >> 2;
+          const float ww = (bx ? wx1 : wx0) * (by ? wy1 : wy0) * (bz ? wz1 : wz0);
+          // even fine index: the second coarse node is the first one, weight 0
+          acc = fmaf(ww, v[c ? bz : 0][b ? by : 0][a ? bx : 0], acc);
+        }
+        float* o = xf + fz * MF2 + (long long)fy * MF + fx;
+        *o += acc;
+      }
+    }
+  }
+}
+
 // Q2 (and any order): generic stencil with runtime lengths
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
@@ -556,14 +936,15 @@ __global__ void k_scale_out(const float* __restrict__ e32, const double* __restr
 // FP64 flexible-CG update: x += lam p; r -= lam a; (r, r); and the FP32
 // copy of the new residual scaled by the current scale slot
 __global__ void __launch_bounds__(kBlock)
-k_fcg64_update(double* sc, double* __restrict__ x, const double* __restrict__ p, double* __restrict__ r,
+k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, double* __restrict__ r,
                const double* __restrict__ a, float* __restrict__ r32, long long n, Reduce2 R) {
   __shared__ double smem[8];
   const double lam = sc[M_LAM], s = sc[M_SCALE];
   double acc = 0.0;
   const long long i0 = ((long long)blockIdx.x * kBlock + threadIdx.x) * 2;
   if (i0 < n) {  // n is the padded length (even); padding entries are zero
-    const double2 pv = *reinterpret_cast<const double2*>(p + i0);
+    const float2 pf = *reinterpret_cast<const float2*>(p + i0);
+    const double2 pv = make_double2((double)pf.x, (double)pf.y);
     const double2 av = *reinterpret_cast<const double2*>(a + i0);
     double2 xv = *reinterpret_cast<double2*>(x + i0);
     double2 rv = *reinterpret_cast<double2*>(r + i0);
@@ -578,13 +959,20 @@ k_fcg64_update(double* sc, double* __restrict__ x, const double* __restrict__ p,
   dr_finish2(acc, 0.0, R, smem);
 }
 
-// p = q / s + beta p  (first: p = q / s), s the scale of the FP32 residual
-__global__ void k_fcg64_p(const double* __restrict__ sc, double* __restrict__ p, const float* __restrict__ q,
+// p = q / s + beta p  (first: p = q / s), s the scale of the FP32 residual,
+// computed in FP64 and stored in FP32: the search direction only has to be
+// the same vector in a = A p and in x += lam p, which it is
+__global__ void k_fcg64_p(const double* __restrict__ sc, float* __restrict__ p, const float* __restrict__ q,
                           long long n, int first) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double z = (double)q[i] / sc[M_SUSED];
-  p[i] = first ? z : fma(sc[M_BETA], p[i], z);
+  p[i] = (float)(first ? z : fma(sc[M_BETA], (double)p[i], z));
+}
+
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
 }
 
 // r32 = r * sc[slot]
@@ -596,13 +984,13 @@ __global__ void k_scale_to32(const double* __restrict__ r, const double* __restr
 
 // two FP64 dot products (x, y) and (x, y2) with the epilogue of R
 __global__ void __launch_bounds__(kBlock)
-k_dot2_64(const double* __restrict__ xv, const double* __restrict__ yv, const double* __restrict__ y2,
+k_dot2_64(const double* __restrict__ xv, const float* __restrict__ yv, const double* __restrict__ y2,
           long long n, Reduce2 R) {
   __shared__ double smem[8];
   const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
   double a0 = 0.0, a1 = 0.0;
   if (i < n) {
-    a0 = xv[i] * yv[i];
+    a0 = xv[i] * (double)yv[i];
     if (y2) a1 = xv[i] * y2[i];
   }
   dr_finish2(a0, a1, R, smem);
@@ -621,51 +1009,51 @@ k_dot2_64(const double* __restrict__ xv, const double* __restrict__ yv, const do
 
 static inline unsigned g1(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
-constexpr int kNX32 = 4, kNX64 = 1, kZS = 8;
+constexpr int kZS2 = 32;  // planes per CTA of k_mf2
 
-template <typename T, typename TV, int NX>
-static unsigned mf_blocks_x(int M) {
-  const long long cols = (long long)((M + NX - 1) / NX) * M;
-  return (unsigned)((cols + kBlock - 1) / kBlock);
+static dim3 mf2_grid(int M) {
+  return dim3((unsigned)((M + kMX - 1) / kMX), (unsigned)((M + kMY - 1) / kMY), (unsigned)((M + kZS2 - 1) / kZS2));
 }
 
-template <typename T, typename TV, int NX>
-static void mf_launch(int mode, const MFArgsT<T>& g, const T* x, const T* b, T* y, const TV* v, const TV* v2,
+template <typename T, typename TV, typename TX>
+static void mf_launch(int mode, const MFArgsT<T>& g, const TX* x, const T* b, T* y, const TV* v, const TV* v2,
                       const Reduce2* R, cudaStream_t st) {
-  const dim3 grid(mf_blocks_x<T, TV, NX>(g.M), (g.M + kZS - 1) / kZS);
+  const dim3 grid = mf2_grid(g.M);
   Reduce2 r0 = R ? *R : Reduce2{};
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  if (R) {
+  if constexpr (sizeof(T) == 8) {  // the FP64 operator is only applied (mode 0)
+    if (R) k_mf3<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+    else k_mf3<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+  } else if (R) {
     switch (mode) {
-      case 0: k_mf_q1<T, TV, NX, kZS, 0, true><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 1: k_mf_q1<T, TV, NX, kZS, 1, true><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 2: k_mf_q1<T, TV, NX, kZS, 2, true><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      default: k_mf_q1<T, TV, NX, kZS, 3, true><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0);
+      case 0: k_mf3<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 1: k_mf3<T, TV, TX, kZS2, 1, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 2: k_mf3<T, TV, TX, kZS2, 2, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      default: k_mf3<T, TV, TX, kZS2, 3, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
     }
   } else {
     switch (mode) {
-      case 0: k_mf_q1<T, TV, NX, kZS, 0, false><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 1: k_mf_q1<T, TV, NX, kZS, 1, false><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 2: k_mf_q1<T, TV, NX, kZS, 2, false><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      default: k_mf_q1<T, TV, NX, kZS, 3, false><<<grid, kBlock, 0, st>>>(g, x, b, y, v, v2, r0);
+      case 0: k_mf3<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 1: k_mf3<T, TV, TX, kZS2, 1, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 2: k_mf3<T, TV, TX, kZS2, 2, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      default: k_mf3<T, TV, TX, kZS2, 3, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
     }
   }
 }
 
 void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,
                   const double* v2, const Reduce2* R, cudaStream_t st) {
-  mf_launch<float, double, kNX32>(mode, g, x, b, y, v, v2, R, st);
+  mf_launch<float, double, float>(mode, g, x, b, y, v, v2, R, st);
 }
 
-void mx_top_apply64(const MFArgs64& g, const double* x, double* y, const double* v, const Reduce2* R,
+void mx_top_apply64(const MFArgs64& g, const float* x, double* y, const float* v, const Reduce2* R,
                     cudaStream_t st) {
-  mf_launch<double, double, kNX64>(0, g, x, nullptr, y, v, nullptr, R, st);
+  mf_launch<double, float, float>(0, g, x, nullptr, y, v, nullptr, R, st);
 }
 
 long long mx_top_blocks(int M) {
-  const long long a = (long long)mf_blocks_x<float, double, kNX32>(M) * ((M + kZS - 1) / kZS);
-  const long long b = (long long)mf_blocks_x<double, double, kNX64>(M) * ((M + kZS - 1) / kZS);
-  return a > b ? a : b;
+  const dim3 gr = mf2_grid(M);
+  return (long long)gr.x * gr.y * gr.z;
 }
 
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
@@ -728,7 +1116,9 @@ void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cuda
   g_launches.fetch_add(1, std::memory_order_relaxed);
   const dim3 gr = xgrid(F.M, F.dim), bl(32, 8);
   if (F.order == 1) {
-    if (F.dim == 3) k_prolong_q1<3><<<gr, bl, 0, st>>>((int)F.M, (int)C.M, F.dmask, xc, xf);
+    if (F.dim == 3)
+      k_prolong_q1c<<<dim3((unsigned)((C.M + 31) / 32), (unsigned)((C.M + 7) / 8), (unsigned)C.M), bl, 0, st>>>(
+          (int)F.M, (int)C.M, F.dmask, xc, xf);
     else if (F.dim == 2) k_prolong_q1<2><<<gr, bl, 0, st>>>((int)F.M, (int)C.M, F.dmask, xc, xf);
     else k_prolong_q1<1><<<gr, bl, 0, st>>>((int)F.M, (int)C.M, F.dmask, xc, xf);
     return;
@@ -746,13 +1136,18 @@ void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st) {
   k_f64_to_f32<<<g1(n), kBlock, 0, st>>>(a, b, n);
 }
 
-void mx_fcg64_update(double* sc, double* x, const double* p, double* r, const double* a, float* r32, long long np,
+void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
                      const Reduce2& R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_fcg64_update<<<g1(np / 2), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
 }
 
-void mx_fcg64_p(const double* sc, double* p, const float* q, long long n, bool first, cudaStream_t st) {
+void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_f32_to_f64<<<g1(n), kBlock, 0, st>>>(a, b, n);
+}
+
+void mx_fcg64_p(const double* sc, float* p, const float* q, long long n, bool first, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_fcg64_p<<<g1(n), kBlock, 0, st>>>(sc, p, q, n, first ? 1 : 0);
 }
@@ -762,7 +1157,7 @@ void mx_scale_to32(const double* r, const double* sc, int slot, float* r32, long
   k_scale_to32<<<g1(n), kBlock, 0, st>>>(r, sc, slot, r32, n);
 }
 
-void mx_dot2_64(const double* x, const double* y, const double* y2, long long n, const Reduce2& R, cudaStream_t st) {
+void mx_dot2_64(const double* x, const float* y, const double* y2, long long n, const Reduce2& R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_dot2_64<<<g1(n), kBlock, 0, st>>>(x, y, y2, n, R);
 }
