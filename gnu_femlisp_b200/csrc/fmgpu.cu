@@ -1264,6 +1264,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     // start: r32 = r / |r|, z = M r, p = z
     if ((rc = mx_set_scalar(g, M_SCALE, dn > 0 ? 1.0 / dn : 1.0))) return rc;
     if ((rc = mx_set_scalar(g, M_SUSED, dn > 0 ? 1.0 / dn : 1.0))) return rc;
+    if ((rc = mx_set_scalar(g, M_SINV, dn > 0 ? dn : 1.0))) return rc;
     mx_scale_to32(r, X.sc, M_SCALE, X.r, T.Np, st);
     {
       const Reduce2 Rr = red2(X, EPI2_RHO, 0, 0);

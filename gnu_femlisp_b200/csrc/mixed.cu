@@ -49,6 +49,7 @@ __device__ __forceinline__ void epi2_apply(const Reduce2& R, double t0, double t
     case EPI2_UPDATE: {  // (r, r); the scale of the next FP32 residual
       sc[M_RR] = t0;
       sc[M_SUSED] = sc[M_SCALE];
+      sc[M_SINV] = 1.0 / sc[M_SCALE];
       sc[M_SCALE] = t0 > 0.0 ? 1.0 / sqrt(t0) : 1.0;
       break;
     }
@@ -118,362 +119,24 @@ __device__ __forceinline__ void dr_finish2_grid(double v0, double v1, const Redu
   }
 }
 
-// Register-blocked stencil: a thread owns NX consecutive nodes along x of
-// one (y, z-segment) column block and marches z over ZS planes, keeping the
-// x values of three planes (rows y-1, y, y+1, positions x-1 .. x+NX) and the
-// coefficients of two cell planes (rows y-1, y, cells x-1 .. x+NX-1) in
-// registers.  Each new plane costs 3 (NX+2) loads of x and 2 (NX+1) loads of
-// k, shared by NX nodes; validity is separable per direction (inside the grid
-// and off the Dirichlet faces), so eliminated columns read as zero.
-// mode 0: y = A x; 1: y = b - A x; 2: y = x + w (b - A x)/d; 3: y = w b / d
-// (x = 0).  With RED, (y, v) and (y, v2) are accumulated in FP64.
-template <typename T, typename TV, int NX, int ZS, int MODE, bool RED>
-__global__ void __launch_bounds__(kBlock, 2)
-k_mf_q1(MFArgsT<T> g, const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
-        const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
-  __shared__ double smem[8];
-  const int M = g.M, n = g.n, dm = g.dmask;
-  const int ngx = (M + NX - 1) / NX;
-  const long long t = (long long)blockIdx.x * kBlock + threadIdx.x;
-  const int xg = (int)(t % ngx), iy = (int)(t / ngx);
-  const int ix0 = xg * NX, z0 = blockIdx.y * ZS;
-  double acc0 = 0.0, acc1 = 0.0;
-  if (iy < M) {
-    const long long MM = (long long)M * M;
-    auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-    T W[3][3][NX + 2];   // [plane][row][x]
-    T K[2][2][NX + 1];   // [cell plane][cell row][cell x]
-    // boundary columns: clamped addresses, validity recomputed per load
-    // (inside the grid, off the Dirichlet faces; cells inside the grid)
-    auto ldplane = [&](int jz, T (*dst)[NX + 2]) {
-      const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
-      const long long zb = (long long)min(max(jz, 0), M - 1) * MM;
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        const int jy = iy - 1 + r;
-        const bool vr = vz && jy >= 0 && jy < M && !dirf(jy, 4, 8);
-        const T* row = x + zb + (long long)min(max(jy, 0), M - 1) * M;
-#pragma unroll
-        for (int j = 0; j < NX + 2; ++j) {
-          const int jx = ix0 - 1 + j;
-          const bool ok = vr && jx >= 0 && jx < M && !dirf(jx, 1, 2);
-          const T xv = __ldg(row + min(max(jx, 0), M - 1));
-          dst[r][j] = ok ? xv : T(0);
-        }
-      }
-    };
-    auto ldcells = [&](int cz, T (*dst)[NX + 1]) {
-      const bool vz = cz >= 0 && cz < n;
-      const long long zb = (long long)min(max(cz, 0), n - 1) * n * n;
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int cy = iy - 1 + r;
-        const bool vr = vz && cy >= 0 && cy < n;
-        const T* row = g.k + zb + (long long)min(max(cy, 0), n - 1) * n;
-#pragma unroll
-        for (int j = 0; j < NX + 1; ++j) {
-          const int cx = ix0 - 1 + j;
-          const T kv = __ldg(row + min(max(cx, 0), n - 1));
-          dst[r][j] = (vr && cx >= 0 && cx < n) ? kv : T(0);
-        }
-      }
-    };
-    // interior columns (every x and y neighbour position in 1 .. M-2) load
-    // without clamps or masks; a plane is then valid or zero as a whole
-    const bool fast = ix0 >= 2 && ix0 + NX <= M - 2 && iy >= 2 && iy <= M - 3;
-    const T* xcol = x + (long long)(iy - 1) * M + (ix0 - 1);
-    const T* kcol = g.k + (long long)(iy - 1) * n + (ix0 - 1);
-    auto ldplane_fast = [&](int jz, T (*dst)[NX + 2]) {
-      const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
-      if (vz) {
-        const T* p0 = xcol + (long long)jz * MM;
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-          for (int j = 0; j < NX + 2; ++j) dst[r][j] = __ldg(p0 + r * M + j);
-      } else {
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-          for (int j = 0; j < NX + 2; ++j) dst[r][j] = T(0);
-      }
-    };
-    auto ldcells_fast = [&](int cz, T (*dst)[NX + 1]) {
-      if (cz >= 0 && cz < n) {
-        const T* p0 = kcol + (long long)cz * n * n;
-#pragma unroll
-        for (int r = 0; r < 2; ++r)
-#pragma unroll
-          for (int j = 0; j < NX + 1; ++j) dst[r][j] = __ldg(p0 + r * n + j);
-      } else {
-#pragma unroll
-        for (int r = 0; r < 2; ++r)
-#pragma unroll
-          for (int j = 0; j < NX + 1; ++j) dst[r][j] = T(0);
-      }
-    };
-    if (fast) {
-      if (MODE != 3) { ldplane_fast(z0 - 1, W[0]); ldplane_fast(z0, W[1]); }
-      ldcells_fast(z0 - 1, K[0]);
-    } else {
-      if (MODE != 3) { ldplane(z0 - 1, W[0]); ldplane(z0, W[1]); }
-      ldcells(z0 - 1, K[0]);
-    }
-    const bool diry = dirf(iy, 4, 8);
-    const T hs = g.hs;
-#pragma unroll 1
-    for (int kz = 0; kz < ZS; ++kz) {
-      const int iz = z0 + kz;
-      if (iz < M) {
-        if (fast) {
-          if (MODE != 3) ldplane_fast(iz + 1, W[2]);
-          ldcells_fast(iz, K[1]);
-        } else {
-          if (MODE != 3) ldplane(iz + 1, W[2]);
-          ldcells(iz, K[1]);
-        }
-        const bool dirz = dirf(iz, 16, 32);
-        const long long rowi = (long long)iz * MM + (long long)iy * M;
-#pragma unroll
-        for (int j = 0; j < NX; ++j) {
-          const int ix = ix0 + j;
-          if (ix < M) {
-            const long long i = rowi + ix;
-            const bool dir = diry || dirz || dirf(ix, 1, 2);
-            T ax = T(0), d = T(1), xc = T(0);
-            if (dir) {
-              if (MODE != 3) { xc = x[i]; ax = xc; }
-            } else {
-              T ks = T(0), sacc = T(0);
-              xc = MODE != 3 ? W[1][1][j + 1] : T(0);
-#pragma unroll
-              for (int c = 0; c < 8; ++c) {
-                const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
-                const T kc = K[cz][cy][j + cx];
-                ks += kc;
-                if (MODE != 3) {
-                  const int px = j + 1 + (2 * cx - 1), py = 1 + (2 * cy - 1), pz = 1 + (2 * cz - 1);
-                  const T e = T(4) * xc - W[1][py][px] - W[pz][1][px] - W[pz][py][j + 1] - W[pz][py][px];
-                  sacc = fma(kc, e, sacc);
-                }
-              }
-              d = T(4) * hs * ks;
-              ax = hs * sacc;
-            }
-            T out;
-            if (MODE == 0) out = ax;
-            else if (MODE == 1) out = b[i] - ax;
-            else if (MODE == 2) out = fma(g.omega ? g.omega[i] : g.w, (b[i] - ax) / d, xc);
-            else out = (g.omega ? g.omega[i] : g.w) * (b[i] / d);
-            y[i] = out;
-            if (RED) {
-              acc0 = fma((double)out, (double)v[i], acc0);
-              if (v2) acc1 = fma((double)out, (double)v2[i], acc1);
-            }
-          }
-        }
-        if (MODE != 3) {
-#pragma unroll
-          for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int j = 0; j < NX + 2; ++j) { W[0][r][j] = W[1][r][j]; W[1][r][j] = W[2][r][j]; }
-        }
-#pragma unroll
-        for (int r = 0; r < 2; ++r)
-#pragma unroll
-          for (int j = 0; j < NX + 1; ++j) K[0][r][j] = K[1][r][j];
-      }
-    }
-  }
-  if (RED) dr_finish2_grid(acc0, acc1, R, smem);
-}
-
-// 2.5D-blocked version of the same operator: a CTA owns a 32 x 8 column of
-// nodes and marches z through ZS planes, one node per thread per plane.  The
-// (32+2) x (8+2) halo of each x plane and the 33 x 9 cells of each cell plane
-// are staged in two-slot shared-memory rings; each thread keeps the 3 x 3
-// neighbourhood of three x planes and the 2 x 2 cells of two cell planes in
-// registers, so a plane is read from HBM once (coalesced rows) and from
-// shared memory 9 + 4 times per node.  The next planes are loaded into
-// registers while the current one is computed.  Values at Dirichlet nodes and
-// outside the grid are staged as zero (eliminated columns), cells outside as
-// zero coefficient.  Per cell the arithmetic is that of k_mf_q1, in the same
-// order.
-constexpr int kMX = 32, kMY = 8;                   // nodes of a CTA plane
-constexpr int kHX = kMX + 2, kHY = kMY + 2;        // node halo
-constexpr int kCX = kMX + 1, kCY = kMY + 1;        // cell tile
-constexpr int kNH = kHX * kHY, kNC = kCX * kCY;    // 340, 297
-constexpr int kMFThreads = kMX * kMY;              // 256
-
-template <typename T, typename TV, int ZS, int MODE, bool RED>
-__global__ void __launch_bounds__(kMFThreads)
-k_mf2(MFArgsT<T> g, const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
-      const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
-  __shared__ T xs[2][kNH];
-  __shared__ T ks[2][kNC];
-  __shared__ double smem[8];
-  const int tid = threadIdx.x, lx = tid & (kMX - 1), ly = tid / kMX;
-  const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, z0 = blockIdx.z * ZS;
-  const int M = g.M, n = g.n, dm = g.dmask;
-  const long long MM = (long long)M * M, nn = (long long)n * n;
-  const int ix = x0 + lx, iy = y0 + ly;
-  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-  // halo entries e = tid, tid + 256 of a node plane / cell plane
-  int hoff[2], coff[2];
-  bool hok[2], cok[2];
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const int e = tid + q * kMFThreads;
-    const int jx = x0 - 1 + e % kHX, jy = y0 - 1 + e / kHX;
-    hok[q] = e < kNH && jx >= 0 && jx < M && jy >= 0 && jy < M && !dirf(jx, 1, 2) && !dirf(jy, 4, 8);
-    hoff[q] = hok[q] ? jy * M + jx : 0;
-    const int cx = x0 - 1 + e % kCX, cy = y0 - 1 + e / kCX;
-    cok[q] = e < kNC && cx >= 0 && cx < n && cy >= 0 && cy < n;
-    coff[q] = cok[q] ? cy * n + cx : 0;
-  }
-  auto ldx = [&](int jz, T* r) {
-    const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
-    const T* pl = x + (long long)(vz ? jz : 0) * MM;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) r[q] = (vz && hok[q]) ? __ldg(pl + hoff[q]) : T(0);
-  };
-  auto ldk = [&](int cz, T* r) {
-    const bool vz = cz >= 0 && cz < n;
-    const T* pl = g.k + (long long)(vz ? cz : 0) * nn;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) r[q] = (vz && cok[q]) ? __ldg(pl + coff[q]) : T(0);
-  };
-  auto stx = [&](int slot, const T* r) {
-    xs[slot][tid] = r[0];
-    if (tid + kMFThreads < kNH) xs[slot][tid + kMFThreads] = r[1];
-  };
-  auto stk = [&](int slot, const T* r) {
-    ks[slot][tid] = r[0];
-    if (tid + kMFThreads < kNC) ks[slot][tid + kMFThreads] = r[1];
-  };
-  auto rdx = [&](int slot, T (*P)[3]) {
-#pragma unroll
-    for (int ry = 0; ry < 3; ++ry)
-#pragma unroll
-      for (int rx = 0; rx < 3; ++rx) P[ry][rx] = xs[slot][(ly + ry) * kHX + lx + rx];
-  };
-  auto rdk = [&](int slot, T (*K)[2]) {
-#pragma unroll
-    for (int by = 0; by < 2; ++by)
-#pragma unroll
-      for (int bx = 0; bx < 2; ++bx) K[by][bx] = ks[slot][(ly + by) * kCX + lx + bx];
-  };
-  T P[3][3][3];  // [plane z-1, z, z+1][row][col]
-  T K[2][2][2];  // [cell plane z-1, z][row][col]
-  T rx_[2], rk_[2];
-  // prologue: x planes z0-1, z0 and cell plane z0-1 into registers; x plane
-  // z0+1 and cell plane z0 into the rings
-  if (MODE != 3) {
-    ldx(z0 - 1, rx_); stx(0, rx_);
-    ldx(z0, rx_); stx(1, rx_);
-  }
-  ldk(z0 - 1, rk_); stk(0, rk_);
-  __syncthreads();
-  if (MODE != 3) { rdx(0, P[0]); rdx(1, P[1]); }
-  rdk(0, K[0]);
-  __syncthreads();
-  if (MODE != 3) { ldx(z0 + 1, rx_); stx(0, rx_); }
-  ldk(z0, rk_); stk(1, rk_);
-  __syncthreads();
-  int sx = 0, sk = 1;  // ring slots of x plane z+1 and cell plane z
-  double acc0 = 0.0, acc1 = 0.0;
-  const bool own = ix < M && iy < M;
-  const bool diry = dirf(iy, 4, 8), dirx = dirf(ix, 1, 2);
-  const T hs = g.hs;
-  const int zend = min(z0 + ZS, M);
-  // per-node operands of plane iz, loaded one plane ahead
-  const long long col = (long long)iy * M + ix;
-  T bq = T(0), oq = T(0);
-  TV vq = TV(0), v2q = TV(0);
-  auto ldnode = [&](int jz, T& bb, T& oo, TV& vv, TV& vv2) {
-    if (own && jz < zend) {
-      const long long i = (long long)jz * MM + col;
-      if (MODE != 0) bb = __ldg(b + i);
-      if ((MODE == 2 || MODE == 3) && g.omega) oo = __ldg(g.omega + i);
-      if (RED) {
-        vv = __ldg(v + i);
-        if (v2) vv2 = __ldg(v2 + i);
-      }
-    }
-  };
-  ldnode(z0, bq, oq, vq, v2q);
-#pragma unroll 1
-  for (int iz = z0; iz < zend; ++iz) {
-    // prefetch x plane iz+2, cell plane iz+1 and the node operands of iz+1
-    if (MODE != 3) ldx(iz + 2, rx_);
-    ldk(iz + 1, rk_);
-    T bn = T(0), on = T(0);
-    TV vn = TV(0), v2n = TV(0);
-    ldnode(iz + 1, bn, on, vn, v2n);
-    if (MODE != 3) rdx(sx, P[2]);
-    rdk(sk, K[1]);
-    if (own) {
-      const long long i = (long long)iz * MM + col;
-      const bool dir = diry || dirx || dirf(iz, 16, 32);
-      T ax = T(0), d = T(1), xc = T(0);
-      if (dir) {
-        if (MODE != 3) { xc = x[i]; ax = xc; }
-      } else {
-        T ksum = T(0), sacc = T(0);
-        xc = MODE != 3 ? P[1][1][1] : T(0);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
-          const T kc = K[cz][cy][cx];
-          ksum += kc;
-          if (MODE != 3) {
-            const int px = 1 + (2 * cx - 1), py = 1 + (2 * cy - 1), pz = 1 + (2 * cz - 1);
-            const T e = T(4) * xc - P[1][py][px] - P[pz][1][px] - P[pz][py][1] - P[pz][py][px];
-            sacc = fma(kc, e, sacc);
-          }
-        }
-        d = T(4) * hs * ksum;
-        ax = hs * sacc;
-      }
-      T out;
-      if (MODE == 0) out = ax;
-      else if (MODE == 1) out = bq - ax;
-      else if (MODE == 2) out = fma(g.omega ? oq : g.w, (bq - ax) / d, xc);
-      else out = (g.omega ? oq : g.w) * (bq / d);
-      y[i] = out;
-      if (RED) {
-        acc0 = fma((double)out, (double)vq, acc0);
-        if (v2) acc1 = fma((double)out, (double)v2q, acc1);
-      }
-    }
-    bq = bn; oq = on; vq = vn; v2q = v2n;
-    __syncthreads();  // ring slots sx, sk read by every thread
-    if (MODE != 3) stx(sx ^ 1, rx_);
-    stk(sk ^ 1, rk_);
-    __syncthreads();
-    sx ^= 1;
-    sk ^= 1;
-    if (MODE != 3) {
-#pragma unroll
-      for (int ry = 0; ry < 3; ++ry)
-#pragma unroll
-        for (int rx = 0; rx < 3; ++rx) { P[0][ry][rx] = P[1][ry][rx]; P[1][ry][rx] = P[2][ry][rx]; }
-    }
-#pragma unroll
-    for (int by = 0; by < 2; ++by)
-#pragma unroll
-      for (int bx = 0; bx < 2; ++bx) K[0][by][bx] = K[1][by][bx];
-  }
-  if (RED) dr_finish2_grid(acc0, acc1, R, smem);
-}
-
-// Pipelined version: the same 32 x 8 x ZS blocking, but every operand of a
-// plane -- the node halo of x, the cell tile of k and the per-node b, omega,
-// v, v2 -- is copied into a 5-stage shared-memory ring by cp.async (4/8-byte
-// copies; masked entries are zero-filled), two stages ahead of the plane being
-// computed, so each SM keeps tens of KB of loads in flight.  Stage s holds x
-// plane s+1, cell plane s and the node operands of plane s; plane iz reads the
-// x planes of stages iz-2 .. iz and the cell planes of stages iz-1, iz.
+// Matrix-free top-level operator, 2.5D blocking: a CTA owns a 32 x 16 column
+// of nodes (256 threads, thread (lx, ly) computes the y-adjacent nodes 2ly and
+// 2ly+1) and marches z through ZS planes.  The (32+2) x (16+2) halo of each x
+// plane and the 33 x 17 cells of each cell plane are copied into a 5-stage
+// shared-memory ring by cp.async (4/8-byte copies, masked entries zero-filled:
+// Dirichlet nodes and nodes outside the grid read as zero -- eliminated
+// columns -- and cells outside the grid as zero coefficient), two stages ahead
+// of the plane being computed.  Stage s holds x plane s+1 and cell plane s;
+// plane iz reads the x planes of stages iz-2 .. iz and the cell planes of
+// stages iz-1, iz.  The per-node operands (b, omega, v, v2) are register-
+// prefetched one plane ahead, and ring slots advance by increments.  The row
+// is evaluated in factored form: 4 K x_i minus, over the 12 face diagonals,
+// the sum of the two cells sharing each times its value, minus, over the 8
+// body diagonals, the one cell times its value (axis neighbours have weight
+// zero in the Q1 stiffness).
+constexpr int kMX = 32;                            // nodes along x of a CTA
+constexpr int kHX = kMX + 2, kCX = kMX + 1;        // halo / cell tile along x
+constexpr int kMFThreads = 256;
 constexpr int kStages = 5;
 
 __device__ __forceinline__ void cpa(void* dst, const void* src, bool ok, int bytes) {
@@ -487,130 +150,160 @@ __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_gro
 template <int N>
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+constexpr int kMY4 = 16;
+constexpr int kHY4 = kMY4 + 2, kCY4 = kMY4 + 1;
+constexpr int kNH4 = kHX * kHY4, kNC4 = kCX * kCY4;  // 612, 561
+
 template <typename T, typename TV, typename TX, int ZS, int MODE, bool RED>
 __global__ void __launch_bounds__(kMFThreads)
-k_mf3(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
+k_mf4(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
       const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
-  constexpr bool HX = MODE != 3;                   // x stencil
-  constexpr bool HB = MODE != 0;                   // right-hand side
-  constexpr bool HO = MODE == 2 || MODE == 3;      // damping
-  __shared__ TX xs[kStages][HX ? kNH : 1];
-  __shared__ T ks[kStages][kNC];
-  __shared__ T bs[kStages][HB ? kMFThreads : 1];
-  __shared__ T os[kStages][HO ? kMFThreads : 1];
-  __shared__ TV vs[kStages][RED ? kMFThreads : 1];
-  __shared__ TV v2s[kStages][RED ? kMFThreads : 1];
+  constexpr bool HX = MODE != 3;
+  constexpr bool HB = MODE != 0;
+  constexpr bool HO = MODE == 2 || MODE == 3;
+  __shared__ TX xs[kStages][HX ? kNH4 : 1];
+  __shared__ T ks[kStages][kNC4];
   __shared__ double smem[8];
   const int tid = threadIdx.x, lx = tid & (kMX - 1), ly = tid / kMX;
-  const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, z0 = blockIdx.z * ZS;
+  const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY4, z0 = blockIdx.z * ZS;
   const int M = g.M, n = g.n, dm = g.dmask;
   const long long MM = (long long)M * M, nn = (long long)n * n;
-  const int ix = x0 + lx, iy = y0 + ly;
-  const bool own = ix < M && iy < M;
+  const int ix = x0 + lx, iy0 = y0 + 2 * ly;
   auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-  int hoff[2], coff[2];
-  bool hok[2], cok[2];
+  int hoff[3], coff[3];
+  bool hok[3], cok[3];
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < 3; ++q) {
     const int e = tid + q * kMFThreads;
     const int jx = x0 - 1 + e % kHX, jy = y0 - 1 + e / kHX;
-    hok[q] = e < kNH && jx >= 0 && jx < M && jy >= 0 && jy < M && !dirf(jx, 1, 2) && !dirf(jy, 4, 8);
+    hok[q] = e < kNH4 && jx >= 0 && jx < M && jy >= 0 && jy < M && !dirf(jx, 1, 2) && !dirf(jy, 4, 8);
     hoff[q] = hok[q] ? jy * M + jx : 0;
     const int cx = x0 - 1 + e % kCX, cy = y0 - 1 + e / kCX;
-    cok[q] = e < kNC && cx >= 0 && cx < n && cy >= 0 && cy < n;
+    cok[q] = e < kNC4 && cx >= 0 && cx < n && cy >= 0 && cy < n;
     coff[q] = cok[q] ? cy * n + cx : 0;
   }
-  const long long col = own ? (long long)iy * M + ix : 0;
+  const bool own0 = ix < M && iy0 < M, own1 = ix < M && iy0 + 1 < M;
+  const long long col0 = own0 ? (long long)iy0 * M + ix : 0;
+  const long long col1 = own1 ? (long long)(iy0 + 1) * M + ix : 0;
   const bool omv = g.omega != nullptr;
   const int zend = min(z0 + ZS, M);
-  auto slot = [&](int st) { return (st - z0 + 2 * kStages) % kStages; };
-  // queue stage st (always one commit group, possibly empty)
-  auto issue = [&](int st) {
-    const int sl = slot(st);
+  auto issue = [&](int st, int sl) {  // x plane st+1 and cell plane st into slot sl
     if (HX) {
       const int jz = st + 1;
       const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
       const TX* pl = x + (long long)(vz ? jz : 0) * MM;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < 3; ++q) {
         const int e = tid + q * kMFThreads;
-        if (e < kNH) cpa(&xs[sl][e], pl + hoff[q], vz && hok[q], (int)sizeof(TX));
+        if (e < kNH4) cpa(&xs[sl][e], pl + hoff[q], vz && hok[q], (int)sizeof(TX));
       }
     }
-    {
-      const bool vz = st >= 0 && st < n;
-      const T* pl = g.k + (long long)(vz ? st : 0) * nn;
+    const bool vz = st >= 0 && st < n;
+    const T* pl = g.k + (long long)(vz ? st : 0) * nn;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int e = tid + q * kMFThreads;
-        if (e < kNC) cpa(&ks[sl][e], pl + coff[q], vz && cok[q], (int)sizeof(T));
-      }
-    }
-    const bool nz = own && st >= z0 && st < zend;
-    const long long i = (long long)(nz ? st : 0) * MM + col;
-    if (HB) cpa(&bs[sl][tid], b + i, nz, (int)sizeof(T));
-    if (HO && omv) cpa(&os[sl][tid], g.omega + i, nz, (int)sizeof(T));
-    if (RED) {
-      cpa(&vs[sl][tid], v + i, nz, (int)sizeof(TV));
-      if (v2) cpa(&v2s[sl][tid], v2 + i, nz, (int)sizeof(TV));
+    for (int q = 0; q < 3; ++q) {
+      const int e = tid + q * kMFThreads;
+      if (e < kNC4) cpa(&ks[sl][e], pl + coff[q], vz && cok[q], (int)sizeof(T));
     }
     cpa_commit();
   };
-  for (int st = z0 - 2; st <= z0 + 1; ++st) issue(st);
+  struct Ops { T b[2], o[2]; TV v[2], v2[2]; };
+  auto ldops = [&](int jz, Ops& o) {  // per-node operands of a plane (two nodes)
+    const bool in = jz < zend;
+    const long long zb = (long long)jz * MM;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const bool ok = in && (r ? own1 : own0);
+      const long long i = zb + (r ? col1 : col0);
+      o.b[r] = (HB && ok) ? __ldg(b + i) : T(0);
+      o.o[r] = (HO && omv && ok) ? __ldg(g.omega + i) : g.w;
+      o.v[r] = (RED && ok) ? __ldg(v + i) : TV(0);
+      o.v2[r] = (RED && ok && v2) ? __ldg(v2 + i) : TV(0);
+    }
+  };
+  issue(z0 - 2, 0);
+  issue(z0 - 1, 1);
+  issue(z0, 2);
+  issue(z0 + 1, 3);
+  int s2 = 0, s1 = 1, s0 = 2, si = 4;  // slots of stages iz-2, iz-1, iz and of the next issue
+  Ops cur, nxt;
+  ldops(z0, cur);
   double acc0 = 0.0, acc1 = 0.0;
-  const bool diry = dirf(iy, 4, 8), dirx = dirf(ix, 1, 2);
+  const bool dirx = dirf(ix, 1, 2);
   const T hs = g.hs;
 #pragma unroll 1
   for (int iz = z0; iz < zend; ++iz) {
-    issue(iz + 2);
-    cpa_wait<2>();  // stages up to iz have landed (this thread's copies)
-    __syncthreads();  // ... and every other thread's
-    if (own) {
-      const long long i = (long long)iz * MM + col;
-      const int sc = slot(iz);
-      const bool dir = diry || dirx || dirf(iz, 16, 32);
+    issue(iz + 2, si);
+    ldops(iz + 1, nxt);
+    cpa_wait<2>();
+    __syncthreads();
+    const bool dirz = dirf(iz, 16, 32);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (!(r ? own1 : own0)) continue;
+      const int iy = iy0 + r;
+      const long long i = (long long)iz * MM + (r ? col1 : col0);
+      const bool dir = dirz || dirx || dirf(iy, 4, 8);
       T ax = T(0), d = T(1), xc = T(0);
       if (dir) {
         if (HX) { xc = (T)x[i]; ax = xc; }
       } else {
-        const TX* X0 = HX ? xs[slot(iz - 2)] : nullptr;  // x plane iz-1
-        const TX* X1 = HX ? xs[slot(iz - 1)] : nullptr;  // x plane iz
-        const TX* X2 = HX ? xs[sc] : nullptr;            // x plane iz+1
-        const T* K0 = ks[slot(iz - 1)];                 // cell plane iz-1
-        const T* K1 = ks[sc];                           // cell plane iz
-        T ksum = T(0), sacc = T(0);
-        const int h = (ly + 1) * kHX + lx + 1;          // centre in the halo
-        xc = HX ? (T)X1[h] : T(0);
+        T k[2][2][2];  // k[cz][cy][cx]: cz 0 cell plane iz-1 (slot s1), 1 cell plane iz (slot s0)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
-          const T kc = (cz ? K1 : K0)[(ly + cy) * kCX + lx + cx];
-          ksum += kc;
-          if (HX) {
-            const int sx = 2 * cx - 1, sy = 2 * cy - 1;
-            const TX* Xz = cz ? X2 : X0;
-            const T e = T(4) * xc - (T)X1[h + sy * kHX + sx] - (T)Xz[h + sx] - (T)Xz[h + sy * kHX] -
-                        (T)Xz[h + sy * kHX + sx];
-            sacc = fma(kc, e, sacc);
+        for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+          for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+            for (int cx = 0; cx < 2; ++cx) k[cz][cy][cx] = ks[cz ? s0 : s1][(2 * ly + r + cy) * kCX + lx + cx];
+        const T wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
+                            {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
+        const T ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
+        T sacc = T(0);
+        if (HX) {
+          const int h = (2 * ly + r + 1) * kHX + lx + 1;
+          const TX* X1 = xs[s1];  // x plane iz
+          xc = (T)X1[h];
+#pragma unroll
+          for (int sy = 0; sy < 2; ++sy)
+#pragma unroll
+            for (int sx = 0; sx < 2; ++sx) sacc = fma(wc[sy][sx], (T)X1[h + (2 * sy - 1) * kHX + 2 * sx - 1], sacc);
+#pragma unroll
+          for (int cz = 0; cz < 2; ++cz) {
+            const TX* Xz = xs[cz ? s0 : s2];  // x plane iz+1 / iz-1
+#pragma unroll
+            for (int sx = 0; sx < 2; ++sx)   // face diagonals (sx, 0, sz): cells (sx, *, sz)
+              sacc = fma(k[cz][0][sx] + k[cz][1][sx], (T)Xz[h + 2 * sx - 1], sacc);
+#pragma unroll
+            for (int sy = 0; sy < 2; ++sy)   // face diagonals (0, sy, sz): cells (*, sy, sz)
+              sacc = fma(k[cz][sy][0] + k[cz][sy][1], (T)Xz[h + (2 * sy - 1) * kHX], sacc);
+#pragma unroll
+            for (int sy = 0; sy < 2; ++sy)
+#pragma unroll
+              for (int sx = 0; sx < 2; ++sx)  // body diagonals
+                sacc = fma(k[cz][sy][sx], (T)Xz[h + (2 * sy - 1) * kHX + 2 * sx - 1], sacc);
           }
+          sacc = fma(T(4) * ksum, xc, -sacc);
         }
         d = T(4) * hs * ksum;
         ax = hs * sacc;
       }
       T out;
-      const T bq = HB ? bs[sc][tid] : T(0);
-      const T oq = (HO && omv) ? os[sc][tid] : g.w;
       if (MODE == 0) out = ax;
-      else if (MODE == 1) out = bq - ax;
-      else if (MODE == 2) out = fma(oq, (bq - ax) / d, xc);
-      else out = oq * (bq / d);
+      else if (MODE == 1) out = cur.b[r] - ax;
+      else if (MODE == 2) out = fma(cur.o[r], (cur.b[r] - ax) / d, xc);
+      else out = cur.o[r] * (cur.b[r] / d);
       y[i] = out;
       if (RED) {
-        acc0 = fma((double)out, (double)vs[sc][tid], acc0);
-        if (v2) acc1 = fma((double)out, (double)v2s[sc][tid], acc1);
+        acc0 = fma((double)out, (double)cur.v[r], acc0);
+        if (v2) acc1 = fma((double)out, (double)cur.v2[r], acc1);
       }
     }
-    __syncthreads();  // the slot of stage iz-2 is refilled by the next issue
+    cur = nxt;
+    __syncthreads();  // slot s2 is refilled by the next issue
+    si = s2;
+    s2 = s1;
+    s1 = s0;
+    s0 = s0 + 1 == kStages ? 0 : s0 + 1;
   }
   cpa_wait<0>();
   if (RED) dr_finish2_grid(acc0, acc1, R, smem);
@@ -964,10 +657,24 @@ k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, 
 // the same vector in a = A p and in x += lam p, which it is
 __global__ void k_fcg64_p(const double* __restrict__ sc, float* __restrict__ p, const float* __restrict__ q,
                           long long n, int first) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double z = (double)q[i] / sc[M_SUSED];
-  p[i] = (float)(first ? z : fma(sc[M_BETA], (double)p[i], z));
+  const long long i0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  const double inv = sc[M_SINV], beta = sc[M_BETA];  // 1 / scale of the FP32 residual
+  if (i0 + 4 <= n && (((uintptr_t)(p + i0) | (uintptr_t)(q + i0)) & 15) == 0) {
+    const float4 qv = *reinterpret_cast<const float4*>(q + i0);
+    float4 pv = *reinterpret_cast<float4*>(p + i0);
+    const double z0 = (double)qv.x * inv, z1 = (double)qv.y * inv, z2 = (double)qv.z * inv, z3 = (double)qv.w * inv;
+    pv.x = (float)(first ? z0 : fma(beta, (double)pv.x, z0));
+    pv.y = (float)(first ? z1 : fma(beta, (double)pv.y, z1));
+    pv.z = (float)(first ? z2 : fma(beta, (double)pv.z, z2));
+    pv.w = (float)(first ? z3 : fma(beta, (double)pv.w, z3));
+    *reinterpret_cast<float4*>(p + i0) = pv;
+  } else {
+    for (long long i = i0; i < n && i < i0 + 4; ++i) {
+      const double z = (double)q[i] * inv;
+      p[i] = (float)(first ? z : fma(beta, (double)p[i], z));
+    }
+  }
 }
 
 __global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, long long n) {
@@ -1012,7 +719,7 @@ static inline unsigned g1(long long n) { return (unsigned)((n + kBlock - 1) / kB
 constexpr int kZS2 = 32;  // planes per CTA of k_mf2
 
 static dim3 mf2_grid(int M) {
-  return dim3((unsigned)((M + kMX - 1) / kMX), (unsigned)((M + kMY - 1) / kMY), (unsigned)((M + kZS2 - 1) / kZS2));
+  return dim3((unsigned)((M + kMX - 1) / kMX), (unsigned)((M + kMY4 - 1) / kMY4), (unsigned)((M + kZS2 - 1) / kZS2));
 }
 
 template <typename T, typename TV, typename TX>
@@ -1022,21 +729,21 @@ static void mf_launch(int mode, const MFArgsT<T>& g, const TX* x, const T* b, T*
   Reduce2 r0 = R ? *R : Reduce2{};
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if constexpr (sizeof(T) == 8) {  // the FP64 operator is only applied (mode 0)
-    if (R) k_mf3<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
-    else k_mf3<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+    if (R) k_mf4<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+    else k_mf4<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
   } else if (R) {
     switch (mode) {
-      case 0: k_mf3<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 1: k_mf3<T, TV, TX, kZS2, 1, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 2: k_mf3<T, TV, TX, kZS2, 2, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      default: k_mf3<T, TV, TX, kZS2, 3, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+      case 0: k_mf4<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 1: k_mf4<T, TV, TX, kZS2, 1, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 2: k_mf4<T, TV, TX, kZS2, 2, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      default: k_mf4<T, TV, TX, kZS2, 3, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
     }
   } else {
     switch (mode) {
-      case 0: k_mf3<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 1: k_mf3<T, TV, TX, kZS2, 1, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 2: k_mf3<T, TV, TX, kZS2, 2, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      default: k_mf3<T, TV, TX, kZS2, 3, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+      case 0: k_mf4<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 1: k_mf4<T, TV, TX, kZS2, 1, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      case 2: k_mf4<T, TV, TX, kZS2, 2, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
+      default: k_mf4<T, TV, TX, kZS2, 3, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
     }
   }
 }
@@ -1149,7 +856,7 @@ void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st) {
 
 void mx_fcg64_p(const double* sc, float* p, const float* q, long long n, bool first, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_fcg64_p<<<g1(n), kBlock, 0, st>>>(sc, p, q, n, first ? 1 : 0);
+  k_fcg64_p<<<g1((n + 3) / 4), kBlock, 0, st>>>(sc, p, q, n, first ? 1 : 0);
 }
 
 void mx_scale_to32(const double* r, const double* sc, int slot, float* r32, long long n, cudaStream_t st) {
