@@ -47,6 +47,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--matvec-reps", type=int, default=20)
     ap.add_argument("--no-learned", action="store_true", help="mixed precision without the damping network")
+    ap.add_argument("--profile", choices=["solve", "net"], default=None,
+                    help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
+                         "the launch count, one more solve; net: the damping network on every level, 8 times)")
     return ap.parse_args()
 
 
@@ -426,6 +429,42 @@ def run_mine(args, world, rank, local):
     ctx.close()
 
 
+def run_profile(args):
+    """Workloads for ncu captures (profiles/ names the commands)."""
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.learn import DampingNet
+    C = G._capi
+    wl = problems.c3(seed=0, level=args.level)
+    ctx = G.Context(0)
+    g = G.Grid(ctx, 3, 1, wl.level, base_level=wl.base_level)
+    g.set_coefficient(C.FMG_K_CELL, wl.kcell)
+    g.assemble()
+    cfg = plain_cfg(G)
+    net = DampingNet.load(ctx, WEIGHTS)
+    if args.profile == "net":
+        for _ in range(8):
+            net.apply(g)
+        ctx.synchronize()
+        print("launches", ctypes_count(C), flush=True)
+    else:
+        net.apply(g)
+        g.learned_judge(cfg)
+        x = g.vector()
+        for _ in range(2):
+            x.fill(0.0)
+            g.solve_mixed(cfg, x)
+        ctx.synchronize()
+        print("launches_before_last", ctypes_count(C), flush=True)
+        x.fill(0.0)
+        _, _, ninner, _ = g.solve_mixed(cfg, x)
+        ctx.synchronize()
+        print("launches_after", ctypes_count(C), "inner_iterations", ninner, flush=True)
+    net.close()
+    g.close()
+    ctx.close()
+
+
 def ctypes_count(C) -> int:
     import ctypes
     v = ctypes.c_longlong(0)
@@ -437,7 +476,10 @@ def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.profile:
+            if rank == 0:
+                run_profile(args)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_mine(args, world, rank, local)
