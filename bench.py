@@ -47,6 +47,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--matvec-reps", type=int, default=20)
     ap.add_argument("--no-learned", action="store_true", help="mixed precision without the damping network")
+    ap.add_argument("--config", choices=["c3", "c4"], default="c3",
+                    help="c4: the learned smoother on 128^2 block fields, 256 held-out seeds, its own JSON line")
+    ap.add_argument("--c4-fields", type=int, default=256)
     ap.add_argument("--profile", choices=["solve", "net"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
                          "the launch count, one more solve; net: the damping network on every level, 8 times)")
@@ -429,6 +432,52 @@ def run_mine(args, world, rank, local):
     ctx.close()
 
 
+WEIGHTS2D = os.path.join(ROOT, "gnu_femlisp_b200", "weights", "damping2d.fmgnet")
+
+
+def run_c4(args):
+    """The learned smoother on the block-field set: 2D Q1, 128^2 cells, k
+    piecewise constant on 8 x 8 blocks with log10 k ~ U[-3, 3]; for each of
+    the held-out seeds 1,000,000 .. the plain V(1,1) Jacobi(0.6) cycle and the
+    learned damping (network on every level, then the judge), as the
+    iteration (GMG) and as the CG preconditioner, from x = 0 to 1e-10."""
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import learn
+    C = G._capi
+    ctx = G.Context(0)
+    net = learn.DampingNet.load(ctx, WEIGHTS2D)
+    seeds = range(1000000, 1000000 + args.c4_fields)
+    out = {}
+    for method, name, maxsteps in ((C.FMG_METHOD_MG, "gmg", 400), (C.FMG_METHOD_CG_MG, "cg_gmg", 200)):
+        cfg = G.SolveCfg(method, C.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, 1e-10, 0.0, maxsteps, C.FMG_MULTIPLICATIVE)
+        rows = learn.evaluate_on_fields(net, ctx, learn.block_field, seeds, cfg, 2, 7, 2, top_only=False)
+        ps = np.array([r["plain_steps"] for r in rows], float)
+        ls = np.array([r["learned_steps"] for r in rows], float)
+        pt = np.array([r["plain_s"] for r in rows])
+        lt = np.array([r["learned_s"] for r in rows])
+        out[name] = {
+            "plain": {"cycles_mean": ps.mean(), "cycles_median": float(np.median(ps)),
+                      "failed": int(sum(r["plain_status"] for r in rows)), "ms_mean": 1e3 * pt.mean()},
+            "learned": {"cycles_mean": ls.mean(), "cycles_median": float(np.median(ls)),
+                        "failed": int(sum(r["learned_status"] for r in rows)), "ms_mean": 1e3 * lt.mean(),
+                        "setup_ms_mean": 1e3 * float(np.mean([r["setup_s"] for r in rows]))},
+            "judge_accepted": float(np.mean([r["accepted"] for r in rows])),
+            "fields_learned_fewer_cycles": int(np.sum(ls < ps)), "fields_learned_more_cycles": int(np.sum(ls > ps)),
+        }
+    line = {"metric": "C4 learned smoother: cycles and time to 1e-10, learned damping vs plain w=0.6 GMG",
+            "value": out["cg_gmg"]["plain"]["cycles_mean"] / out["cg_gmg"]["learned"]["cycles_mean"],
+            "unit": "plain / learned mean CG+GMG cycles", "higher_is_better": True, "n_gpus": 1,
+            "data": "synthetic", "dtype": "f64",
+            "config": {"workload": "2D Q1 128^2 cells, 8x8 blocks, log10 k ~ U[-3,3]",
+                       "fields": f"held-out seeds 1000000..{1000000 + args.c4_fields - 1}",
+                       "weights": os.path.relpath(WEIGHTS2D, ROOT),
+                       "solve": "one field at a time (fmg_solve), base level 2"},
+            "results": out}
+    print(json.dumps(line), flush=True)
+    net.close()
+    ctx.close()
+
+
 def run_profile(args):
     """Workloads for ncu captures (profiles/ names the commands)."""
     import gnu_femlisp_b200 as G
@@ -479,6 +528,9 @@ def main():
         if args.profile:
             if rank == 0:
                 run_profile(args)
+        elif args.config == "c4":
+            if rank == 0:
+                run_c4(args)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

@@ -110,6 +110,12 @@ void launch_wg_dinv(const double* A, int center, long long Np, const double* w, 
 // scal[dst] (+)= factor * scal[num] / scal[den]
 void launch_ratio_acc(double* scal, int dst, int num, int den, double factor, bool first, cudaStream_t st);
 void launch_set_scalar(double* p, double v, cudaStream_t st);
+// y = x + w .* v (y may be x); acc += a .* b; y += w .* x / diag(A); y += x
+void launch_xpwv(const double* x, const double* w, const double* v, double* y, long long n, cudaStream_t st);
+void launch_acc_prod(double* acc, const double* a, const double* b, long long n, cudaStream_t st);
+void launch_wg_dinv_acc(const double* A, int center, long long Np, const double* w, const double* x, double* y,
+                        long long n, cudaStream_t st);
+void launch_add(const double* x, double* y, long long n, cudaStream_t st);
 // y = s * x / scal[slot]
 void launch_scale_by(const double* x, double s, const double* scal, int slot, double* y, long long n,
                      cudaStream_t st);

@@ -598,6 +598,32 @@ __global__ void k_scale_by(const double* __restrict__ x, double s, const double*
   if (i < n) y[i] = s * x[i] / scal[slot];
 }
 
+// y = x + w .* v  (y may be x)
+__global__ void k_xpwv(const double* x, const double* __restrict__ w, const double* __restrict__ v, double* y,
+                       long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = x[i] + w[i] * v[i];
+}
+
+// acc += a .* b
+__global__ void k_acc_prod(double* __restrict__ acc, const double* __restrict__ a, const double* __restrict__ b,
+                           long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc[i] += a[i] * b[i];
+}
+
+// y += w .* x / diag(A)
+__global__ void k_wg_dinv_acc(const double* __restrict__ A, const double* __restrict__ w, const double* __restrict__ x,
+                              double* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += w[i] * x[i] / A[i];
+}
+
+__global__ void k_add(const double* __restrict__ x, double* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
 inline unsigned blocks_for(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
 int sm_count() {
@@ -860,6 +886,27 @@ void launch_scale_by(const double* x, double s, const double* scal, int slot, do
 void launch_ratio_acc(double* scal, int dst, int num, int den, double factor, bool first, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_ratio_acc<<<1, 1, 0, st>>>(scal, dst, num, den, factor, first ? 1 : 0);
+}
+
+void launch_xpwv(const double* x, const double* w, const double* v, double* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_xpwv<<<blocks_for(n), 256, 0, st>>>(x, w, v, y, n);
+}
+
+void launch_acc_prod(double* acc, const double* a, const double* b, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_acc_prod<<<blocks_for(n), 256, 0, st>>>(acc, a, b, n);
+}
+
+void launch_wg_dinv_acc(const double* A, int center, long long Np, const double* w, const double* x, double* y,
+                        long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_wg_dinv_acc<<<blocks_for(n), 256, 0, st>>>(A + (long long)center * Np, w, x, y, n);
+}
+
+void launch_add(const double* x, double* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_add<<<blocks_for(n), 256, 0, st>>>(x, y, n);
 }
 
 void launch_set_scalar(double* p, double v, cudaStream_t st) {

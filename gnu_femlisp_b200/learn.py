@@ -88,6 +88,13 @@ class DampingNet:
         """Forward pass on every level above the base (installs the damping)."""
         self.ctx.check(self._lib.fmg_net_apply(self.h, grid.h), "net_apply")
 
+    def apply_top(self, grid: Grid):
+        """Forward pass on the top level only (the levels below keep the
+        scalar damping) -- the setting the network is trained in."""
+        for lev in range(grid.base + 1, grid.top):
+            grid.set_node_damping(lev, None)
+        self.damping(grid, grid.top)
+
     def backward(self, grid: Grid, level: int, gomega):
         g = np.ascontiguousarray(gomega, dtype=np.float64)
         self.ctx.check(self._lib.fmg_net_backward(self.h, grid.h, level, C.dptr(g)), "net_backward")
@@ -121,6 +128,17 @@ def learn_loss(grid: Grid, cfg: C.SolveCfg, e0: Vector, want_grad: bool = True):
     g = np.zeros(grid.nnodes()) if want_grad else None
     grid.ctx.check(grid._lib.fmg_learn_loss(grid.h, ctypes.byref(cfg), e0.h, ctypes.byref(loss),
                                             C.dptr(g) if want_grad else None), "learn_loss")
+    return loss.value, g
+
+
+def learn_loss_levels(grid: Grid, cfg: C.SolveCfg, e0: Vector, level: int, want_grad: bool = True):
+    """The same loss with the damping of every level differentiated through
+    the whole cycle; returns (loss, dL/domega of `level`)
+    (``fmg_learn_loss_levels``)."""
+    loss = ctypes.c_double()
+    g = np.zeros(grid.nnodes(level)) if want_grad else None
+    grid.ctx.check(grid._lib.fmg_learn_loss_levels(grid.h, ctypes.byref(cfg), e0.h, level, ctypes.byref(loss),
+                                                   C.dptr(g) if want_grad else None), "learn_loss_levels")
     return loss.value, g
 
 
@@ -227,3 +245,75 @@ def _dirichlet_mask(g: Grid) -> np.ndarray:
     for k in range(g.dim):
         bnd |= (idx[k] == 0) | (idx[k] == m - 1)
     return bnd
+
+
+# -------------------------------------------- the batched 2D block-field set
+def block_field(seed: int, n: int = 128, blocks: int = 8, lo: float = -3.0, hi: float = 3.0) -> np.ndarray:
+    """Diffusion per cell of an n x n grid, piecewise constant on a
+    blocks x blocks partition with log10 k ~ U[lo, hi] per block (seeded)."""
+    from .problems import block_log10_field
+    return 10.0 ** block_log10_field(n, blocks, seed, lo, hi)
+
+
+def train_on_fields(net: DampingNet, ctx: Context, field_of, seeds, cfg: C.SolveCfg, dim: int, level: int,
+                    base: int, pool: int = 8, lr: float = 2e-3, lr_end: float | None = None, nsamples: int = 4,
+                    max_cycles: int = 4, log=None):
+    """One Adam step per field: field_of(seed) gives the cell coefficients;
+    a pool of grids is re-assembled with each new field, so every step trains
+    on a field not seen before.  Returns the loss history."""
+    seeds = list(seeds)
+    steps = len(seeds)
+    lr_end = lr / 10 if lr_end is None else lr_end
+    grids = [Grid(ctx, dim, 1, level, base) for _ in range(pool)]
+    hist = []
+    for it, sd in enumerate(seeds):
+        g = grids[it % pool]
+        g.set_coefficient(C.FMG_K_CELL, field_of(sd))
+        g.assemble()
+        loss = net.step(g, cfg, nsamples, 7919 * sd + 1, max_cycles)
+        rate = lr_end + 0.5 * (lr - lr_end) * (1 + np.cos(np.pi * it / max(1, steps - 1)))
+        net.adam(rate)
+        hist.append(loss)
+        if log and (it % max(1, steps // 20) == 0 or it == steps - 1):
+            log(f"step {it:6d} field {sd} loss {loss:.5f} mean(last 200) {np.mean(hist[-200:]):.5f}")
+    for g in grids:
+        g.close()
+    return np.array(hist)
+
+
+def evaluate_on_fields(net: DampingNet, ctx: Context, field_of, seeds, cfg: C.SolveCfg, dim: int, level: int,
+                       base: int, top_only: bool = True):
+    """Per field: steps and solve time of the plain cycle (scalar damping) and
+    of the learned damping (network on every level, then the judge), from x = 0
+    to cfg's tolerance with fmg_solve.  Times are wall clock of the solve call
+    (it synchronises), without the setup; the learned setup is timed apart."""
+    import time
+    g = Grid(ctx, dim, 1, level, base)
+    x = g.vector()
+    rows = []
+    for sd in seeds:
+        g.set_coefficient(C.FMG_K_CELL, field_of(sd))
+        g.assemble()
+        for lev in range(g.base + 1, g.top + 1):
+            g.set_node_damping(lev, None)
+        x.fill(0.0)
+        t0 = time.perf_counter()
+        hp, sp, stp = g.solve(cfg, x)
+        tp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        if top_only:
+            net.apply_top(g)
+        else:
+            net.apply(g)
+        ok, rp, rl = g.learned_judge(cfg)
+        ts = time.perf_counter() - t0
+        x.fill(0.0)
+        t0 = time.perf_counter()
+        hl, sl, stl = g.solve(cfg, x)
+        tl = time.perf_counter() - t0
+        rows.append(dict(seed=sd, plain_steps=sp, plain_status=stp, plain_s=tp, learned_steps=sl,
+                         learned_status=stl, learned_s=tl, setup_s=ts, accepted=ok, rho_plain=rp,
+                         rho_learned=rl))
+    x.close()
+    g.close()
+    return rows

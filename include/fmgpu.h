@@ -237,21 +237,35 @@ int fmg_net_backward(fmg_net* net, fmg_grid* grid, int level, const double* gome
    correction of the cycle below), and its gradient with respect to that
    damping (N values, when gomega is not NULL).  FP64. */
 int fmg_learn_loss(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_vec* e0, double* loss, double* gomega);
-/* One training step: forward on all levels, nsamples errors generated by the
+/* The loss of fmg_learn_loss with the node damping of every level (levels
+   without node damping use cfg->damp), differentiated through the whole
+   V-cycle: dL/domega of `level` (N of that level values) when gomega is not
+   NULL.  FP64. */
+int fmg_learn_loss_levels(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_vec* e0, int level, double* loss,
+                          double* gomega);
+/* One training step: forward on every level above the base (the net's
+   damping everywhere, as at inference), nsamples errors generated by the
    multigrid (random, then max_cycles V-cycles of A e = 0 with the current
-   damping), mean loss -> *loss, backward into the gradient accumulator. */
+   damping), mean loss -> *loss, and its gradient with respect to the damping
+   of every level (through the whole cycle) back through the net of each
+   level into the gradient accumulator. */
 int fmg_learn_step(fmg_net* net, fmg_grid* grid, const fmg_solve_cfg* cfg, int nsamples,
                    unsigned long long seed, int max_cycles, double* loss);
 
 /* The judge (no counterpart in the reference): the plain <geometric-cs>
-   cycle (scalar cfg->damp) and the cycle with the installed node damping each
-   run 4 times on A e = 0 from the same random vector; the node damping stays
-   only if its last-cycle A-norm contraction rho_learned <= rho_plain, else it
-   is removed and the plain cycle is used (*accepted = 0).  fmg_solve_mixed
-   then judges the learned cycles as they run: when the mean residual
-   reduction of the last 3 CG steps is worse than rho_plain (0.9 when the judge
-   has not run), or one step after the first of a CG run grows the residual by
-   more than 1.5x, it drops the node damping for the rest of the solve. */
+   cycle (scalar cfg->damp) judges the cycle with the installed node damping
+   the way it will be used.  cfg->method CG+MG: 6 CG steps with each on the
+   same manufactured problem (random x*, b = A x*, x0 = 0), rho = per-step
+   A-norm error contraction (what CG minimises).  MG: each cycle 8 times on
+   A e = 0 from the same random vector, rho = the last cycle's A-norm
+   contraction.  The node damping stays only if rho_learned <= 0.98
+   rho_plain, else it is removed and the plain cycle is used (*accepted = 0).
+   During solves: fmg_solve's MG iteration drops the node damping when the
+   mean residual reduction of the last 3 cycles is worse than rho_plain (0.9
+   when the judge has not run) or a cycle grows the residual 1.5x; in CG runs
+   (fmg_solve CG+MG, fmg_solve_mixed), whose residual norms need not fall
+   monotonically, only divergence (100x the run's initial residual) drops it,
+   and CG restarts from the current residual with the plain cycle. */
 int fmg_learned_judge(fmg_grid* grid, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned,
                       int* accepted);
 /* active: learned damping installed and accepted; reverts: mixed solves whose

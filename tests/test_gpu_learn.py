@@ -107,6 +107,38 @@ def test_loss_gradient_matches_finite_differences(G, ctx):
     assert abs(fd - grad @ d) <= 1e-6 * max(1.0, abs(fd)), (fd, grad @ d)
 
 
+def test_all_level_gradient_matches_finite_differences(G, ctx):
+    # dL/domega of a coarse level and of the top level through the whole
+    # V-cycle, against central differences; the loss equals fmg_learn_loss's
+    from gnu_femlisp_b200.learn import learn_loss, learn_loss_levels
+    g, _ = _grid(G, ctx, 3, 4, 1, seed=14)
+    cfg = _cfg(G)
+    rng = np.random.default_rng(3)
+    ws = {}
+    for lev in range(g.base + 1, g.top + 1):
+        ws[lev] = rng.uniform(0.4, 1.0, g.nnodes(lev))
+        g.set_node_damping(lev, ws[lev])
+    n = g.nnodes()
+    e0 = rng.uniform(-1, 1, n)
+    m = (1 << 4) + 1
+    idx = np.indices((m, m, m)).reshape(3, -1)
+    e0[((idx == 0) | (idx == m - 1)).any(0)] = 0.0
+    ev = g.vector(values=e0)
+    L_old, _ = learn_loss(g, cfg, ev, want_grad=False)
+    for lev in (g.top - 1, g.top):
+        L0, grad = learn_loss_levels(g, cfg, ev, lev)
+        assert abs(L0 - L_old) <= 1e-12 * L_old, (L0, L_old)
+        d = rng.standard_normal(ws[lev].size)
+        eps = 1e-5
+        g.set_node_damping(lev, ws[lev] + eps * d)
+        Lp, _ = learn_loss_levels(g, cfg, ev, lev, want_grad=False)
+        g.set_node_damping(lev, ws[lev] - eps * d)
+        Lm, _ = learn_loss_levels(g, cfg, ev, lev, want_grad=False)
+        g.set_node_damping(lev, ws[lev])
+        fd = (Lp - Lm) / (2 * eps)
+        assert abs(fd - grad @ d) <= 1e-6 * max(1e-3, abs(fd)), (lev, fd, grad @ d)
+
+
 def test_training_lowers_the_loss(G, ctx):
     from gnu_femlisp_b200.learn import DampingNet, TrainSpec, mean_loss, train, training_grids
     spec = TrainSpec(dim=3, level=4, base=1, count=3)
