@@ -248,8 +248,8 @@ def run_mine(args, world, rank, local):
 
     def install_learned():
         net.apply(g)
-        ok, rp, rl = g.learned_judge(cfg)
-        judge.update(accepted=ok, rho_plain=rp, rho_learned=rl)
+        ok, rp, rl = g.learned_judge_mixed(cfg)
+        judge.update(accepted=ok, rho_plain=rp, rho_learned=rl, probe="6 mixed flexible-CG steps")
 
     def setup():
         g.set_coefficient(C.FMG_K_CELL, k_np)
@@ -498,7 +498,7 @@ def run_profile(args):
         print("launches", ctypes_count(C), flush=True)
     else:
         net.apply(g)
-        g.learned_judge(cfg)
+        g.learned_judge_mixed(cfg)
         x = g.vector()
         for _ in range(2):
             x.fill(0.0)

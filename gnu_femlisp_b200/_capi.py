@@ -117,6 +117,8 @@ SIGNATURES = {
     "fmg_net_backward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _dp]),
     "fmg_learn_loss": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, _dp]),
     "fmg_learned_judge": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
+    "fmg_learned_judge_mixed": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), ctypes.POINTER(MixedCfg), _dp, _dp,
+                                               ctypes.POINTER(ctypes.c_int)]),
     "fmg_learned_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
     "fmg_learn_loss_levels": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, ctypes.c_int, _dp, _dp]),
     "fmg_learn_step": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(SolveCfg), ctypes.c_int, ctypes.c_ulonglong,

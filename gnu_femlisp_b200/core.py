@@ -185,6 +185,16 @@ class Grid:
                                                    ctypes.byref(ok)), "learned_judge")
         return bool(ok.value), rp.value, rl.value
 
+    def learned_judge_mixed(self, cfg: C.SolveCfg, matrix_free: bool = True):
+        """``fmg_learned_judge_mixed``: the judge's CG probe run with the
+        mixed-precision cycle of ``solve_mixed``; returns (accepted,
+        rho_plain, rho_learned)."""
+        mc = C.MixedCfg(0.0, 0, 1, 1 if matrix_free else 0)
+        rp, rl, ok = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self.ctx.check(self._lib.fmg_learned_judge_mixed(self.h, ctypes.byref(cfg), ctypes.byref(mc), ctypes.byref(rp),
+                                                         ctypes.byref(rl), ctypes.byref(ok)), "learned_judge_mixed")
+        return bool(ok.value), rp.value, rl.value
+
     def learned_status(self) -> dict:
         a, rp, rl, rv = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         self.ctx.check(self._lib.fmg_learned_status(self.h, ctypes.byref(a), ctypes.byref(rp), ctypes.byref(rl),

@@ -48,6 +48,7 @@ struct Lvl {
   double* Kbar = nullptr;
   double* Ctab = nullptr;
   double* Phi = nullptr;
+  std::vector<double> Kbar_h, Ctab_h;  // host copies of the element tables
 };
 
 }  // namespace
@@ -604,6 +605,8 @@ static int ensure_buffers(fmg_grid* g) {
     make_tables(g->dim, g->order, L.h, C, Kbar, Phi, &nl, &nq);
     if ((rc = upload(g, &L.Kbar, Kbar)) || (rc = upload(g, &L.Ctab, C)) || (rc = upload(g, &L.Phi, Phi)))
       return rc;
+    L.Kbar_h = Kbar;
+    L.Ctab_h = C;
     if ((rc = dalloc(g, &L.A, (long long)g->nslots * L.Np))) return rc;
   }
   const Lvl& B = g->lev[g->base];
@@ -660,7 +663,7 @@ int fmg_assemble(fmg_grid* g) {
     a.kq = sample ? g->kq : nullptr;
     a.fip = g->fkind == FMG_F_IP ? g->fip_d : nullptr;
     a.kconst = g->kconst; a.fconst = g->fconst;
-    launch_assemble(g->dim, g->order, a, st);
+    launch_assemble(g->dim, g->order, a, L.Kbar_h.data(), L.Ctab_h.data(), st);
     if ((rc = launched(c, "assemble"))) return rc;
   }
   // dense LU of the base level and its explicit inverse
@@ -1421,8 +1424,10 @@ int net_grid_check(fmg_net* net, fmg_grid* g) {
   return FMG_OK;
 }
 
-// features + forward pass on level l; writes the level's node damping
-int net_level_forward(fmg_net* net, fmg_grid* g, int l) {
+// features + forward pass on level l; writes the level's node damping.
+// with_mean: first (re)compute the mean log k over the top level's cells,
+// which every level's features are centred by
+int net_level_forward(fmg_net* net, fmg_grid* g, int l, bool with_mean) {
   fmg_ctx* c = g->ctx;
   cudaStream_t st = c->stream;
   int rc;
@@ -1433,11 +1438,14 @@ int net_level_forward(fmg_net* net, fmg_grid* g, int l) {
   long long ncell_top = 1;
   for (int k = 0; k < g->dim; ++k) ncell_top *= T.n;
   const bool kc = g->kkind == FMG_K_CELL;
-  if (kc) launch_logmean(g->kcell_d, ncell_top, net->stat + 8, net->stat, st);
-  else launch_set_scalar(net->stat, std::log(g->kconst), st);
+  if (with_mean) {
+    if (kc) launch_logmean(g->kcell_d, ncell_top, net->stat + 8, net->stat, st);
+    else launch_set_scalar(net->stat, std::log(g->kconst), st);
+  }
   const ActGeom ag = act_geom(g->dim, (int)L.M, 1);
-  launch_features(ag, (int)L.n, T.n, std::ldexp(1.0, g->top - l), g->np, g->xi_d, kc ? g->kcell_d : nullptr,
-                  g->kconst, net->stat, net->X0, st);
+  if ((rc = launch_features(net, ag, (int)L.n, T.n, std::ldexp(1.0, g->top - l), g->np, g->xi_d,
+                            kc ? g->kcell_d : nullptr, g->kconst, net->stat, st)))
+    return set_err(c, rc, "damping network: no memory");
   if ((rc = net_forward(net, ag, L.omega, st))) return set_err(c, rc, "damping network forward failed");
   return launched(c, "damping network forward");
 }
@@ -1704,7 +1712,7 @@ int fmg_net_damping(fmg_net* net, fmg_grid* g, int level, double* host_omega) {
   int rc = net_grid_check(net, g);
   if (rc) return rc;
   if (level <= g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d has no smoother", level);
-  if ((rc = net_level_forward(net, g, level))) return rc;
+  if ((rc = net_level_forward(net, g, level, true))) return rc;
   if ((rc = net_finish(net))) return rc;
   const Lvl& L = g->lev[level];
   if (host_omega) {
@@ -1718,7 +1726,7 @@ int fmg_net_apply(fmg_net* net, fmg_grid* g) {
   int rc = net_grid_check(net, g);
   if (rc) return rc;
   for (int l = g->top; l > g->base; --l)
-    if ((rc = net_level_forward(net, g, l))) return rc;
+    if ((rc = net_level_forward(net, g, l, l == g->top))) return rc;
   if ((rc = net_finish(net))) return rc;
   g->learned = true;
   return FMG_OK;
@@ -1812,7 +1820,7 @@ int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsam
   fmg_ctx* c = g->ctx;
   cudaStream_t st = c->stream;
   for (int l = g->base + 1; l <= g->top; ++l) {
-    if ((rc = net_level_forward(net, g, l))) return rc;
+    if ((rc = net_level_forward(net, g, l, l == g->base + 1))) return rc;
     launch_fill(g->lvv[l][LV_WBAR], g->lev[l].N, 0.0, st);
   }
   Lvl& T = g->lev[g->top];
@@ -1834,7 +1842,7 @@ int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsam
   if ((rc = launched(c, "learn step"))) return rc;
   // backward through the net of every level (its forward pass recomputed)
   for (int l = g->base + 1; l <= g->top; ++l) {
-    if ((rc = net_level_forward(net, g, l))) return rc;
+    if ((rc = net_level_forward(net, g, l, false))) return rc;
     if ((rc = net_backward(net, g->lvv[l][LV_WBAR], g->lev[l].omega, st))) return set_err(c, rc, "backward failed");
   }
   if ((rc = launched(c, "learn backward"))) return rc;
@@ -1892,7 +1900,9 @@ namespace {
 // x* random (Dirichlet nodes zero), b = A x*, x0 = 0; CG minimises the A-norm
 // error, so (|x* - x_k|_A / |x*|_A)^(1/k) ranks preconditioners for CG where
 // residual norms (not monotone under strong coefficient jumps) do not
-int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, int k, unsigned long long seed, double* rho) {
+// (mc non-null: the steps are those of fmg_solve_mixed with the mixed cycle)
+int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int k, unsigned long long seed,
+             double* rho) {
   fmg_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   const Lvl& T = g->lev[g->top];
@@ -1916,8 +1926,14 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, int k, unsigned long long see
   const bool learned = g->learned;
   g->rhs = b;
   g->learned = false;
-  int ns = 0, status = 0;
-  int rc = fmg_solve(g, &c, &x, nullptr, 0, &ns, &status);
+  int ns = 0, status = 0, nouter = 0, rc;
+  if (mc) {
+    fmg_mixed_cfg m = *mc;
+    m.max_outer = 1;
+    rc = fmg_solve_mixed(g, &c, &m, &x, nullptr, 0, &nouter, &ns, &status);
+  } else {
+    rc = fmg_solve(g, &c, &x, nullptr, 0, &ns, &status);
+  }
   g->rhs = rhs;
   g->learned = learned;
   if (rc) return rc;
@@ -1933,7 +1949,7 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, int k, unsigned long long see
 
 }  // namespace
 
-extern "C" {
+namespace {
 
 // The plain <geometric-cs> (scalar :damp) judges the learned damping the way
 // the cycle will be used.  As a CG preconditioner (cfg->method CG+MG): 6 CG
@@ -1943,22 +1959,26 @@ extern "C" {
 // compared.  The learned damping stays installed only if its figure is at
 // least 2 % below the plain cycle's; otherwise it is removed (the fallback).
 // The plain cycle's figure is also the bound of the judge inside fmg_solve's
-// MG iteration.
+// MG iteration.  mc non-null: the CG steps are fmg_solve_mixed's (the FP32 /
+// BF16 cycle with the same damping) -- the cycle the mixed solve will use,
+// at a third of the FP64 cycle's cost.
 constexpr double kJudgeMargin = 0.98;
-int fmg_learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned, int* accepted) {
+int learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mc, double* rho_plain,
+                  double* rho_learned, int* accepted) {
   if (!g || !accepted) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (cfg->smoother != FMG_JACOBI || g->top <= g->base)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: Jacobi cycles with at least two levels");
+  const bool cg = cfg->method == FMG_METHOD_CG_MG;
+  if (mc && !cg) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed judge: the CG+MG method only");
   bool any = false;
   for (int l = g->base + 1; l <= g->top; ++l) any = any || g->lev[l].omega;
   if (!any) return set_err(g->ctx, FMG_ERR_STATE, "no node damping installed");
   if ((rc = learn_vectors(g))) return rc;
-  const bool cg = cfg->method == FMG_METHOD_CG_MG;
   auto figure = [&](double* rho) {
-    return cg ? cg_probe(g, *cfg, 6, 0x4A554447ull, rho) : cycle_contraction(g, *cfg, 8, 0x4A554447ull, rho);
+    return cg ? cg_probe(g, *cfg, mc, 6, 0x4A554447ull, rho) : cycle_contraction(g, *cfg, 8, 0x4A554447ull, rho);
   };
   std::vector<double*> saved(g->lev.size());
   for (size_t l = 0; l < g->lev.size(); ++l) { saved[l] = g->lev[l].omega; g->lev[l].omega = nullptr; }
@@ -1981,6 +2001,20 @@ int fmg_learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, double* rho_plain, 
   if (rho_learned) *rho_learned = rl;
   *accepted = ok ? 1 : 0;
   return FMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmg_learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned, int* accepted) {
+  return learned_judge(g, cfg, nullptr, rho_plain, rho_learned, accepted);
+}
+
+int fmg_learned_judge_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, double* rho_plain,
+                            double* rho_learned, int* accepted) {
+  if (!mcfg) return FMG_ERR_ARG;
+  return learned_judge(g, cfg, mcfg, rho_plain, rho_learned, accepted);
 }
 
 int fmg_learned_status(const fmg_grid* g, int* active, double* rho_plain, double* rho_learned, int* reverts) {

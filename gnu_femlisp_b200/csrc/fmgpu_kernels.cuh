@@ -49,7 +49,9 @@ void launch_cg_update(const double* sc, double* x, const double* p, double* r, c
 void launch_p_update(const double* sc, double* p, const double* q, long long n, cudaStream_t st);
 void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_top, double ratio, int np,
                       const double* xi, const double* kcell, double* kq, cudaStream_t st);
-void launch_assemble(int dim, int order, const AsmArgs& a, cudaStream_t st);
+// kbar_h / ctab_h: host copies of a.Kbar / a.Ctab (null: the generic kernel)
+void launch_assemble(int dim, int order, const AsmArgs& a, const double* kbar_h, const double* ctab_h,
+                     cudaStream_t st);
 void launch_densify(const LevelView& L, double* Dm, cudaStream_t st);
 
 }  // namespace fmg

@@ -68,6 +68,8 @@ struct fmg_net {
   float* part = nullptr;       // weight-gradient partials
   long long part_cap = 0;
   double* stat = nullptr;      // [0] mean log k, scratch partials after it
+  double* lk = nullptr;        // cell log-coefficients of the level being featurised
+  long long lk_cap = 0;
   unsigned* err = nullptr;     // device error word (bounded waits that ran out)
   std::vector<void*> allocs;
 };
@@ -86,8 +88,9 @@ void launch_logmean(const double* k, long long n, double* scratch, double* out, 
 // the top level (n_top cells per direction) sampled at np Gauss points xi
 // per direction of each level cell (ratio = n_top / n_l); kconst used when
 // kcell is null
-void launch_features(const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
-                     const double* kcell, double kconst, const double* mean, __nv_bfloat16* X0, cudaStream_t st);
+// (written to net->X0; the level's cell log-coefficients go to net->lk first)
+int launch_features(fmg_net* net, const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
+                    const double* kcell, double kconst, const double* mean, cudaStream_t st);
 // the three forward convolutions; omega (level order, FP64) written when non-null
 int net_forward(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st);
 // backward from dL/domega (level order) through the net of the last forward

@@ -8,6 +8,7 @@
 // thread, coalesced across the warp.  Entries outside the grid, in eliminated
 // Dirichlet columns and structurally absent Q2 couplings are stored as zeros,
 // which lets neighbour indices be clamped to the vector instead of tested.
+#include <cstring>
 #include "fmgpu_kernels.cuh"
 
 namespace fmg {
@@ -325,6 +326,94 @@ __global__ void __launch_bounds__(1024) k_lu_factor(double* A, int n, int* piv) 
   }
 }
 
+// k_lu_factor on a shared-memory copy of A (n x n doubles fit in one CTA's
+// shared memory): the same operations in the same order, so the factors and
+// pivots are bitwise equal, at shared-memory instead of global latency.
+__global__ void __launch_bounds__(1024) k_lu_factor_smem(double* A, int n, int* piv) {
+  extern __shared__ double S[];
+  __shared__ double bv[32];
+  __shared__ int bi[32];
+  __shared__ int pk_s;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int idx = tid; idx < n * n; idx += nt) S[idx] = A[idx];
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    double best = -1.0;
+    int besti = n;
+    for (int i = k + tid; i < n; i += nt) {
+      const double v = fabs(S[i * n + k]);
+      if (v > best || (v == best && i < besti)) { best = v; besti = i; }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+      if (ov > best || (ov == best && oi < besti)) { best = ov; besti = oi; }
+    }
+    if ((tid & 31) == 0) { bv[tid >> 5] = best; bi[tid >> 5] = besti; }
+    __syncthreads();
+    if (tid == 0) {
+      double b = bv[0];
+      int ib = bi[0];
+      for (int w = 1; w < (nt + 31) / 32; ++w)
+        if (bv[w] > b || (bv[w] == b && bi[w] < ib)) { b = bv[w]; ib = bi[w]; }
+      pk_s = ib;
+      piv[k] = ib;
+    }
+    __syncthreads();
+    const int pk = pk_s;
+    if (pk != k)
+      for (int j = tid; j < n; j += nt) {
+        const double t = S[k * n + j];
+        S[k * n + j] = S[pk * n + j];
+        S[pk * n + j] = t;
+      }
+    __syncthreads();
+    const double d = S[k * n + k];
+    for (int i = k + 1 + tid; i < n; i += nt) S[i * n + k] = S[i * n + k] / d;
+    __syncthreads();
+    const int m = n - k - 1;
+    for (int idx = tid; idx < m * m; idx += nt) {
+      const int i = k + 1 + idx / m, j = k + 1 + idx % m;
+      S[i * n + j] = fma(-S[i * n + k], S[k * n + j], S[i * n + j]);
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < n * n; idx += nt) A[idx] = S[idx];
+}
+
+// k_lu_inverse with the factors and a block of 32 columns of X in shared
+// memory: thread = column, the same operations in the same order.
+__global__ void __launch_bounds__(32) k_lu_inverse_smem(const double* __restrict__ LU, const int* __restrict__ piv,
+                                                        int n, double* X) {
+  extern __shared__ double S[];
+  double* L = S;           // n x n
+  double* Xs = S + n * n;  // n x 32
+  const int lane = threadIdx.x, j = blockIdx.x * 32 + lane;
+  for (int idx = lane; idx < n * n; idx += 32) L[idx] = LU[idx];
+  __syncwarp();
+  if (j < n) {
+    for (int i = 0; i < n; ++i) Xs[i * 32 + lane] = (i == j) ? 1.0 : 0.0;
+    for (int k = 0; k < n; ++k) {
+      const int p = piv[k];
+      if (p != k) {
+        const double t = Xs[k * 32 + lane];
+        Xs[k * 32 + lane] = Xs[p * 32 + lane];
+        Xs[p * 32 + lane] = t;
+      }
+    }
+    for (int k = 0; k < n; ++k) {
+      const double bk = Xs[k * 32 + lane];
+      for (int i = k + 1; i < n; ++i) Xs[i * 32 + lane] = fma(-L[i * n + k], bk, Xs[i * 32 + lane]);
+    }
+    for (int k = n - 1; k >= 0; --k) {
+      const double bk = Xs[k * 32 + lane] / L[k * n + k];
+      Xs[k * 32 + lane] = bk;
+      for (int i = 0; i < k; ++i) Xs[i * 32 + lane] = fma(-L[i * n + k], bk, Xs[i * 32 + lane]);
+    }
+    for (int i = 0; i < n; ++i) X[(long long)i * n + j] = Xs[i * 32 + lane];
+  }
+}
+
 // Column j of A^-1 per thread, from the LU factors; X row-major (j fastest).
 __global__ void k_lu_inverse(const double* __restrict__ LU, const int* __restrict__ piv, int n, double* X) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -552,6 +641,95 @@ k_assemble(AsmArgs g) {
   }
 }
 
+// k_assemble for 3D Q1 with the cell loops unrolled at compile time.  Node i
+// is corner a = (1-bx) + 2 (1-by) + 4 (1-bz) of its adjacent cell ci - 1 + b
+// (b = bx + 2 by + 4 bz), and neighbour j = i + o is corner a + ox + 2 oy +
+// 4 oz of that cell when every 1 - b_k + o_k is 0 or 1.  The cells are walked
+// in increasing b -- increasing cell index, the order k_assemble sums in --
+// each adding its contribution to the 8 slots it touches, and every entry is
+// formed with the same operations (e = k Kbar[a][b'], or e = sum_q fma(kq,
+// Ctab, e); v = v + e), so the two kernels agree bit for bit.  The element
+// tables travel as a kernel parameter (constant bank): operands of the FMAs
+// without loads.  KQ: a coarse level's coefficient samples at the 8 Gauss
+// points of each cell.
+struct Q1Tab {
+  double K[64];   // Kbar[a][b]
+  double C[512];  // Ctab[q][a][b]
+};
+
+template <bool KQ>
+__global__ void __launch_bounds__(kBlock)
+k_assemble_q1_3d(AsmArgs g, const __grid_constant__ Q1Tab tab) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  const int M = (int)g.M, n = (int)g.n;
+  const int ix = (int)(i % M), iy = (int)((i / M) % M), iz = (int)(i / ((long long)M * M));
+  const long long ci[3] = {ix, iy, iz};
+  if (node_dirichlet(ci, g.M, 3, g.dmask)) {
+#pragma unroll
+    for (int s = 0; s < 27; ++s) g.A[(long long)s * g.Np + i] = (s == 13) ? 1.0 : 0.0;
+    if (g.rhs) g.rhs[i] = 0.0;
+    return;
+  }
+  double v[27];
+#pragma unroll
+  for (int s = 0; s < 27; ++s) v[s] = 0.0;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const int cx = ix - 1 + (b & 1), cy = iy - 1 + ((b >> 1) & 1), cz = iz - 1 + (b >> 2);
+    if (cx < 0 || cx >= n || cy < 0 || cy >= n || cz < 0 || cz >= n) continue;
+    const long long cidx = cx + (long long)n * (cy + (long long)n * cz);
+    const int ax = 1 - (b & 1), ay = 1 - ((b >> 1) & 1), az = 1 - (b >> 2);
+    const int a = ax + 2 * ay + 4 * az;
+    double kq[KQ ? 8 : 1];
+    if (KQ) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) kq[q] = __ldg(g.kq + cidx * 8 + q);
+    } else {
+      kq[0] = g.kcell ? __ldg(g.kcell + cidx) : g.kconst;
+    }
+#pragma unroll
+    for (int bb = 0; bb < 8; ++bb) {  // neighbour corner: slot o = corner bb - corner a
+      const int ox = (bb & 1) - ax, oy = ((bb >> 1) & 1) - ay, oz = (bb >> 2) - az;
+      const int s = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1);
+      double e;
+      if (KQ) {
+        e = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) e = fma(kq[q], tab.C[(q * 8 + a) * 8 + bb], e);
+      } else {
+        e = kq[0] * tab.K[a * 8 + bb];
+      }
+      v[s] = v[s] + e;
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < 27; ++s) {
+    const int ox = s % 3 - 1, oy = (s / 3) % 3 - 1, oz = s / 9 - 1;
+    const long long cj[3] = {ix + ox, iy + oy, iz + oz};
+    const bool ok = cj[0] >= 0 && cj[0] < g.M && cj[1] >= 0 && cj[1] < g.M && cj[2] >= 0 && cj[2] < g.M &&
+                    !node_dirichlet(cj, g.M, 3, g.dmask);
+    g.A[(long long)s * g.Np + i] = ok ? v[s] : 0.0;
+  }
+  if (g.rhs) {
+    double acc = 0.0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int cx = ix - 1 + (b & 1), cy = iy - 1 + ((b >> 1) & 1), cz = iz - 1 + (b >> 2);
+      if (cx < 0 || cx >= n || cy < 0 || cy >= n || cz < 0 || cz >= n) continue;
+      const long long cidx = cx + (long long)n * (cy + (long long)n * cz);
+      const int a = (1 - (b & 1)) + 2 * (1 - ((b >> 1) & 1)) + 4 * (1 - (b >> 2));
+      double bl = 0.0;
+      for (int q = 0; q < g.nq; ++q) {
+        const double f = g.fip ? g.fip[cidx * g.nq + q] : g.fconst;
+        bl = fma(f, g.Phi[q * g.nl + a], bl);
+      }
+      acc = acc + bl;
+    }
+    g.rhs[i] = acc;
+  }
+}
+
 // ---------------------------------------------------------- dispatchers
 #define FMG_DISPATCH(D_, P_, ...)                                             \
   do {                                                                        \
@@ -638,8 +816,21 @@ void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, dou
 
 void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t st) {
   g_launches.fetch_add(3, std::memory_order_relaxed);
-  k_lu_factor<<<1, 1024, 0, st>>>(A, n, piv);
-  k_lu_inverse<<<grid1(n, 64), 64, 0, st>>>(A, piv, n, X);
+  const size_t f_smem = (size_t)n * n * sizeof(double), i_smem = f_smem + (size_t)n * 32 * sizeof(double);
+  constexpr size_t kMaxSmem = 200 * 1024;
+  if (i_smem <= kMaxSmem) {  // the factors fit in shared memory (n <= 144)
+    static bool init = false;
+    if (!init) {
+      cudaFuncSetAttribute(k_lu_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+      cudaFuncSetAttribute(k_lu_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+      init = true;
+    }
+    k_lu_factor_smem<<<1, 1024, f_smem, st>>>(A, n, piv);
+    k_lu_inverse_smem<<<grid1(n, 32), 32, i_smem, st>>>(A, piv, n, X);
+  } else {
+    k_lu_factor<<<1, 1024, 0, st>>>(A, n, piv);
+    k_lu_inverse<<<grid1(n, 64), 64, 0, st>>>(A, piv, n, X);
+  }
   k_transpose<<<grid1((long long)n * n), kBlock, 0, st>>>(X, n, XT);
 }
 
@@ -681,8 +872,17 @@ void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_to
   else k_sample_kq<3><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
 }
 
-void launch_assemble(int dim, int order, const AsmArgs& a, cudaStream_t st) {
+void launch_assemble(int dim, int order, const AsmArgs& a, const double* kbar_h, const double* ctab_h,
+                     cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (dim == 3 && order == 1 && a.nl == 8 && a.nq == 8 && kbar_h && ctab_h && a.M < (1 << 20)) {
+    Q1Tab tab;
+    std::memcpy(tab.K, kbar_h, sizeof tab.K);
+    std::memcpy(tab.C, ctab_h, sizeof tab.C);
+    if (a.kq) k_assemble_q1_3d<true><<<grid1(a.N), kBlock, 0, st>>>(a, tab);
+    else k_assemble_q1_3d<false><<<grid1(a.N), kBlock, 0, st>>>(a, tab);
+    return;
+  }
   FMG_DISPATCH(dim, order, { k_assemble<D, P><<<grid1(a.N), kBlock, 0, st>>>(a); });
 }
 

@@ -106,8 +106,21 @@ __device__ __forceinline__ long long pad_index(const TileGeo& t, int ix, int iy,
   return ((long long)pz * t.Py + iy + 1) * t.Px + ix + 1;
 }
 
+// 16-byte asynchronous copy global -> shared, zero-filled when !ok
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool ok) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(ok ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // halo of input activations [npad][C] -> shared memory, chunk c of halo node
-// r = hx + HX (hy + HY hz) at byte c*CHB + 16 r (zeros outside the array)
+// r = hx + HX (hy + HY hz) at byte c*CHB + 16 r (zeros outside the array);
+// asynchronous copies, so all of a thread's copies are in flight at once
+// (the caller waits with cp_wait_all before the barrier)
 template <int D, int C>
 __device__ __forceinline__ void stage_halo(uint8_t* hs, const bf16* __restrict__ in, const TileGeo& t, int tx,
                                            int ty, int tz) {
@@ -116,21 +129,20 @@ __device__ __forceinline__ void stage_halo(uint8_t* hs, const bf16* __restrict__
     const int c = idx / ROWS, r = idx - c * ROWS;
     const int hx = r % HX, hy = (r / HX) % HY, hz = r / (HX * HY);
     const int px = tx * TX + hx, py = ty * TY + hy, pz = tz + hz;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (px < t.Px && py < t.Py && pz < t.Pz)
-      v = __ldg(reinterpret_cast<const uint4*>(in + (((long long)pz * t.Py + py) * t.Px + px) * C) + c);
-    *reinterpret_cast<uint4*>(hs + c * CHB + r * kRowB) = v;
+    const bool ok = px < t.Px && py < t.Py && pz < t.Pz;
+    const long long node = ok ? ((long long)pz * t.Py + py) * t.Px + px : 0;
+    cp16(hs + c * CHB + r * kRowB, reinterpret_cast<const uint4*>(in + node * C) + c, ok);
   }
 }
 
-// weights [taps][COUT][CIN] -> per tap a K-major COUT x CIN tile
+// weights [taps][COUT][CIN] -> per tap a K-major COUT x CIN tile (asynchronous)
 template <int TAPS, int CIN, int COUT>
 __device__ __forceinline__ void stage_weights(uint8_t* ws, const bf16* __restrict__ w) {
   constexpr int CH = CIN / 8;
   for (int idx = threadIdx.x; idx < TAPS * COUT * CH; idx += kThreads) {
     const int c = idx % CH, co = (idx / CH) % COUT, tap = idx / (CH * COUT);
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + ((long long)tap * COUT + co) * CIN) + c);
-    *reinterpret_cast<uint4*>(ws + tap * (COUT * CIN * 2) + umma::kmajor_offset(co, c * 8, CIN)) = v;
+    cp16(ws + tap * (COUT * CIN * 2) + umma::kmajor_offset(co, c * 8, CIN),
+         reinterpret_cast<const uint4*>(w + ((long long)tap * COUT + co) * CIN) + c, true);
   }
 }
 
@@ -153,6 +165,44 @@ struct ConvArgs {
   unsigned* err;
 };
 
+// epilogue of output node (ix, iy) of plane tz: v = its COUT accumulators
+template <int D, int COUT, int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, const float* v, int ix, int iy, int tz) {
+  if (ix < a.t.Mx && iy < a.t.My) {
+    const long long p = pad_index<D>(a.t, ix, iy, tz);
+    if constexpr (EPI == EPI_RELU) {
+      uint32_t pk[COUT / 2];
+#pragma unroll
+      for (int c = 0; c < COUT; c += 2)
+        pk[c / 2] = pack2(fmaxf(v[c] + __ldg(a.bias + c), 0.f), fmaxf(v[c + 1] + __ldg(a.bias + c + 1), 0.f));
+      uint4* o = reinterpret_cast<uint4*>(a.out + p * COUT);
+#pragma unroll
+      for (int q = 0; q < COUT / 8; ++q) o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+    } else if constexpr (EPI == EPI_OMEGA) {
+      const float z = v[0] + __ldg(a.bias);
+      const float s = 1.f / (1.f + __expf(-z));
+      const long long i = ((long long)tz * a.t.My + iy) * a.t.Mx + ix;
+      a.omega[i] = (double)(a.omin + (a.omax - a.omin) * s);
+    } else {  // EPI_MASK
+      const uint4* m = reinterpret_cast<const uint4*>(a.mask + p * COUT);
+      uint4* o = reinterpret_cast<uint4*>(a.out + p * COUT);
+#pragma unroll
+      for (int q = 0; q < COUT / 8; ++q) {
+        uint4 mm = __ldg(m + q);
+        const bf16* mh = reinterpret_cast<const bf16*>(&mm);
+        uint32_t pk[4];
+#pragma unroll
+        for (int e = 0; e < 8; e += 2) {
+          const float g0 = __bfloat162float(mh[e]) > 0.f ? v[8 * q + e] : 0.f;
+          const float g1 = __bfloat162float(mh[e + 1]) > 0.f ? v[8 * q + e + 1] : 0.f;
+          pk[e / 2] = pack2(g0, g1);
+        }
+        o[q] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      }
+    }
+  }
+}
+
 template <int D, int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
   constexpr int TAPS = Tp<D>::TAPS, CHB = Tp<D>::CHB;
@@ -166,6 +216,7 @@ __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   stage_weights<TAPS, CIN, COUT>(ws, a.w);
+  cp_wait_all();
   if (warp == 0) umma::tmem_alloc(&tslot, 32);
   if (tid == 0) umma::mbar_init(&bar);
   umma::fence_before();
@@ -179,6 +230,7 @@ __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
     int tx, ty, tz;
     tile_xyz(a.t, id, tx, ty, tz);
     stage_halo<D, CIN>(hs, a.in, a.t, tx, ty, tz);
+    cp_wait_all();
     umma::fence_async_smem();
     umma::fence_before();
     __syncthreads();
@@ -205,40 +257,8 @@ __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
     umma::fence_after();
     float v[COUT];
     umma::tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16), v);
-    const int r = warp * 32 + lane, ix = tx * TX + (r & 7), iy = ty * TY + (r >> 3);
-    if (ix < a.t.Mx && iy < a.t.My) {
-      const long long p = pad_index<D>(a.t, ix, iy, tz);
-      if constexpr (EPI == EPI_RELU) {
-        uint32_t pk[COUT / 2];
-#pragma unroll
-        for (int c = 0; c < COUT; c += 2)
-          pk[c / 2] = pack2(fmaxf(v[c] + __ldg(a.bias + c), 0.f), fmaxf(v[c + 1] + __ldg(a.bias + c + 1), 0.f));
-        uint4* o = reinterpret_cast<uint4*>(a.out + p * COUT);
-#pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
-      } else if constexpr (EPI == EPI_OMEGA) {
-        const float z = v[0] + __ldg(a.bias);
-        const float s = 1.f / (1.f + __expf(-z));
-        const long long i = ((long long)tz * a.t.My + iy) * a.t.Mx + ix;
-        a.omega[i] = (double)(a.omin + (a.omax - a.omin) * s);
-      } else {  // EPI_MASK
-        const uint4* m = reinterpret_cast<const uint4*>(a.mask + p * COUT);
-        uint4* o = reinterpret_cast<uint4*>(a.out + p * COUT);
-#pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) {
-          uint4 mm = __ldg(m + q);
-          const bf16* mh = reinterpret_cast<const bf16*>(&mm);
-          uint32_t pk[4];
-#pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            const float g0 = __bfloat162float(mh[e]) > 0.f ? v[8 * q + e] : 0.f;
-            const float g1 = __bfloat162float(mh[e + 1]) > 0.f ? v[8 * q + e + 1] : 0.f;
-            pk[e / 2] = pack2(g0, g1);
-          }
-          o[q] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-        }
-      }
-    }
+    const int r = warp * 32 + lane;
+    conv_epilogue<D, COUT, EPI>(a, v, tx * TX + (r & 7), ty * TY + (r >> 3), tz);
     umma::fence_before();  // the loads above precede the next tile's MMAs (barrier at the loop top)
   }
   if (failed) {
@@ -250,6 +270,184 @@ __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
   if (warp == 0) {
     umma::fence_after();
     umma::tmem_dealloc(tmem, 32);
+  }
+}
+
+// ---- 3D convolution marching along z
+// A CTA owns the 8 x 16 column (tx, ty) over kSeg output planes z0 .. z0+S-1
+// and walks the input planes P = z0 .. z0+S+1 (padded plane numbers) once
+// each.  Input plane P feeds output planes P, P-1, P-2 through the weight
+// slices dz = 0, 1, 2, so one MMA per (xy tap, K step) multiplies the plane's
+// shifted halo (A, M = 128 nodes) by the three slices side by side (B, N =
+// 3 COUT rows) into three accumulators: output z's COUT columns sit at
+// col(z) = COUT (kSeg - 1 - (z - z0)), descending in z, so the slices dz of
+// plane P land at col(P - dz) = col(P) + dz COUT, one contiguous N range.
+// Slices whose output plane lies outside the segment are dropped from the
+// ends of that range.  An output plane's first product (plane P = z, dz = 0,
+// first tap) is issued on its own with accumulate off.
+//   Per input plane the A tile is read 9 (CIN / 16) + 1 times instead of
+// 27 (CIN / 16) times, which is what bounds the single-plane form (an
+// M = 128, N = COUT MMA reads 4 KB of A from shared memory per K step).
+// Pipeline: the halo planes sit in a ring of kRing slots; plane P + 2 is
+// loaded (cp.async) while plane P is multiplied, and output plane P - 3 is
+// read out of tensor memory and stored while the MMAs of plane P run (two
+// mbarriers, one per plane parity, each with at most one commit pending).
+constexpr int kSeg = 8;    // output planes per work item
+constexpr int kRing = 4;   // halo plane slots
+
+template <int CIN, int COUT>
+struct Z3 {
+  static constexpr int CHB = kRing * kPlaneB;      // one 8-channel chunk of the ring
+  static constexpr int RING = (CIN / 8) * CHB;
+  static constexpr int WTAP = 3 * COUT * CIN * 2;  // one xy tap: the dz = 0, 1, 2 slices, K-major
+  static constexpr int WBYTES = 9 * WTAP;
+  static constexpr int SMEM = WBYTES + RING;
+  static constexpr uint32_t TCOLS = kSeg * COUT;   // 128 or 256 tensor-memory columns
+};
+
+// weights [27 taps][COUT][CIN] (tap = dx + 3 dy + 9 dz) -> per xy tap t a
+// K-major (3 COUT) x CIN tile whose row dz COUT + co holds tap t + 9 dz
+template <int CIN, int COUT>
+__device__ __forceinline__ void stage_weights_z3(uint8_t* ws, const bf16* __restrict__ w) {
+  constexpr int CH = CIN / 8, R = 3 * COUT;
+  for (int idx = threadIdx.x; idx < 9 * R * CH; idx += kThreads) {
+    const int c = idx % CH, row = (idx / CH) % R, t = idx / (CH * R);
+    const int dz = row / COUT, co = row - dz * COUT;
+    cp16(ws + t * Z3<CIN, COUT>::WTAP + umma::kmajor_offset(row, c * 8, CIN),
+         reinterpret_cast<const uint4*>(w + ((long long)(t + 9 * dz) * COUT + co) * CIN) + c, true);
+  }
+}
+
+// padded input plane P of column (tx, ty) -> ring slot P % kRing; chunk c of
+// halo node (hx, hy) at byte c CHB + slot kPlaneB + hy kHyB + 16 hx
+template <int CIN>
+__device__ __forceinline__ void stage_plane_z3(uint8_t* hs, const bf16* __restrict__ in, const TileGeo& t, int tx,
+                                               int ty, int P) {
+  constexpr int ROWS = HX * HY, CHB = kRing * kPlaneB;
+  uint8_t* base = hs + (P % kRing) * kPlaneB;
+  for (int idx = threadIdx.x; idx < (CIN / 8) * ROWS; idx += kThreads) {
+    const int c = idx / ROWS, r = idx - c * ROWS;
+    const int hx = r % HX, hy = r / HX;
+    const int px = tx * TX + hx, py = ty * TY + hy;
+    const bool ok = px < t.Px && py < t.Py && P < t.Pz;
+    const long long node = ok ? ((long long)P * t.Py + py) * t.Px + px : 0;
+    cp16(base + c * CHB + r * kRowB, reinterpret_cast<const uint4*>(in + node * CIN) + c, ok);
+  }
+}
+
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
+
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a) {
+  using Z = Z3<CIN, COUT>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* ws = smem;
+  uint8_t* hs = smem + Z::WBYTES;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TileGeo& t = a.t;
+  const int nseg = (t.Mz + kSeg - 1) / kSeg;
+  const long long items = (long long)t.ntx * t.nty * nseg;
+
+  stage_weights_z3<CIN, COUT>(ws, a.w);
+  cp_commit();
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (warp == 0) umma::tmem_alloc(&tslot, Z::TCOLS);
+  if (tid == 0) { umma::mbar_init(&bar[0]); umma::mbar_init(&bar[1]); }
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tslot;
+  const uint32_t hb = umma::smem_u32(hs), wb = umma::smem_u32(ws);
+  uint32_t phase = 0u;  // bit i: parity of bar[i]'s next phase
+  uint32_t pend = 0u;   // bit i: a commit on bar[i] not yet waited for
+  bool failed = false;
+  auto wait_plane = [&](int i) {  // all threads: the MMAs committed to bar[i] are done
+    const bool ok = !__syncthreads_or(!umma::mbar_wait(&bar[i], (phase >> i) & 1u));
+    if (ok) { phase ^= 1u << i; pend &= ~(1u << i); }
+    return ok;
+  };
+  auto epilogue = [&](int z0, int z, int tx, int ty) {
+    umma::fence_after();
+    float v[COUT];
+    umma::tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(COUT * (kSeg - 1 - (z - z0))), v);
+    const int r = warp * 32 + lane;
+    conv_epilogue<3, COUT, EPI>(a, v, tx * TX + (r & 7), ty * TY + (r >> 3), z);
+  };
+  for (long long id = blockIdx.x; id < items && !failed; id += gridDim.x) {
+    const int tx = (int)(id % t.ntx);
+    const long long rest = id / t.ntx;
+    const int ty = (int)(rest % t.nty), z0 = (int)(rest / t.nty) * kSeg;
+    const int S = min(kSeg, t.Mz - z0);
+    const int nplanes = S + 2;  // padded input planes z0 .. z0+S+1
+    stage_plane_z3<CIN>(hs, a.in, t, tx, ty, z0);
+    cp_commit();
+    stage_plane_z3<CIN>(hs, a.in, t, tx, ty, z0 + 1);
+    cp_commit();
+    for (int k = 0; k < nplanes; ++k) {
+      const int P = z0 + k;
+      // the slot of plane P + 2 was last read by the MMAs of plane P - 2, waited for at step k - 1
+      if (k + 2 < nplanes) stage_plane_z3<CIN>(hs, a.in, t, tx, ty, P + 2);
+      cp_commit();
+      cp_wait_2();  // plane P has landed (this thread's copies)
+      umma::fence_async_smem();
+      umma::fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        umma::fence_after();
+        const int dlo = max(0, P - (z0 + S - 1)), dhi = min(2, P - z0);
+        const uint32_t dcol = tmem + (uint32_t)(COUT * (kSeg - 1 - (P - dlo - z0)));
+        const uint32_t aslot = hb + (uint32_t)((P % kRing) * kPlaneB);
+        const uint32_t idesc = umma::idesc_bf16(128, (dhi - dlo + 1) * COUT, false, false);
+        const uint32_t brow = (uint32_t)(dlo * (COUT / 8) * (CIN / 8) * 128);  // row dlo COUT of the B tile
+        bool first = dlo == 0;  // this plane opens output plane P
+        for (int tap = 0; tap < 9; ++tap) {
+          const uint32_t aoff = (uint32_t)((tap / 3) * kHyB + (tap % 3) * kRowB);
+#pragma unroll
+          for (int kh = 0; kh < CIN / 16; ++kh) {
+            // A: 8 x-nodes 16 B apart x 16 y-rows kHyB apart, K chunks CHB apart
+            const uint64_t ad = umma::make_desc(aslot + aoff + 2 * kh * Z::CHB, Z::CHB, kHyB);
+            const uint32_t wt = wb + tap * Z::WTAP + kh * 256;
+            if (first) {
+              // output P alone (slice dz = 0, N = COUT) with accumulate off, then the other slices
+              umma::mma_bf16(dcol, ad, umma::make_desc(wt, 128, (CIN / 8) * 128),
+                             umma::idesc_bf16(128, COUT, false, false), 0u);
+              if (dhi > 0)
+                umma::mma_bf16(dcol + COUT, ad, umma::make_desc(wt + (COUT / 8) * (CIN / 8) * 128, 128, (CIN / 8) * 128),
+                               umma::idesc_bf16(128, dhi * COUT, false, false), 1u);
+              first = false;
+            } else {
+              umma::mma_bf16(dcol, ad, umma::make_desc(wt + brow, 128, (CIN / 8) * 128), idesc, 1u);
+            }
+          }
+        }
+        umma::mma_commit(&bar[k & 1]);
+      }
+      pend |= 1u << (k & 1);
+      if (k >= 1) {
+        if (!wait_plane((k - 1) & 1)) { failed = true; break; }
+        if (k >= 3) epilogue(z0, P - 3, tx, ty);
+        umma::fence_before();
+      }
+    }
+    if (failed) break;
+    if (!wait_plane((nplanes - 1) & 1)) { failed = true; break; }
+    epilogue(z0, z0 + S - 1, tx, ty);
+    umma::fence_before();  // the loads above precede the next item's MMAs (barrier before them)
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (failed) {
+    if (tid == 0) atomicOr(a.err, 1u);
+    for (int i = 0; i < 2; ++i)
+      if ((pend >> i) & 1u) umma::mbar_wait(&bar[i], (phase >> i) & 1u);  // bounded: let issued MMAs drain
+  }
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after();
+    umma::tmem_dealloc(tmem, Z::TCOLS);
   }
 }
 
@@ -295,12 +493,12 @@ __global__ void __launch_bounds__(kThreads) k_wgrad(WgradArgs a) {
     for (int idx = tid; idx < (CG / 8) * 128; idx += kThreads) {
       const int c = idx >> 7, r = idx & 127, x = r & 7, y = r >> 3;
       const int ix = tx * TX + x, iy = ty * TY + y;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (ix < a.t.Mx && iy < a.t.My)
-        v = __ldg(reinterpret_cast<const uint4*>(a.g + pad_index<D>(a.t, ix, iy, tz) * CG) + c);
-      *reinterpret_cast<uint4*>(gs + c * GCH + y * 128 + x * 16) = v;
+      const bool ok = ix < a.t.Mx && iy < a.t.My;
+      const long long p = ok ? pad_index<D>(a.t, ix, iy, tz) : 0;
+      cp16(gs + c * GCH + y * 128 + x * 16, reinterpret_cast<const uint4*>(a.g + p * CG) + c, ok);
     }
     stage_halo<D, CX>(hs, a.x, a.t, tx, ty, tz);
+    cp_wait_all();
     umma::fence_async_smem();
     umma::fence_before();
     __syncthreads();
@@ -369,21 +567,39 @@ __global__ void k_wgrad_reduce(const float* __restrict__ part, int S, int taps, 
 // shared between levels, so the ghost nodes of a smaller level may hold data)
 template <int D>
 __global__ void k_zero_ghosts(TileGeo t, int chunks, uint4* __restrict__ buf) {
-  const long long npad = (long long)t.Px * t.Py * t.Pz;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npad; p += (long long)gridDim.x * blockDim.x) {
-    const int px = (int)(p % t.Px), py = (int)((p / t.Px) % t.Py), pz = (int)(p / ((long long)t.Px * t.Py));
-    const bool ghost = px == 0 || px == t.Px - 1 || py == 0 || py == t.Py - 1 ||
-                       (D == 3 && (pz == 0 || pz == t.Pz - 1));
-    if (!ghost) continue;
-    for (int c = 0; c < chunks; ++c) buf[p * chunks + c] = make_uint4(0u, 0u, 0u, 0u);
+  // ghost nodes only: the two z faces (3D), then the ring of every other plane
+  const long long face = (long long)t.Px * t.Py;
+  const long long g1 = D == 3 ? 2 * face : 0;
+  const int ring = 2 * t.Px + 2 * (t.Py - 2);
+  const long long nghost = g1 + (long long)(D == 3 ? t.Pz - 2 : t.Pz) * ring;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nghost * chunks;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long node = g / chunks;
+    const int c = (int)(g - node * chunks);
+    long long p;
+    if (node < g1) {
+      p = (node >= face ? (long long)(t.Pz - 1) * face : 0) + node % face;
+    } else {
+      const long long r0 = node - g1;
+      const long long pz = r0 / ring + (D == 3 ? 1 : 0);
+      const int r = (int)(r0 % ring);
+      int x, y;
+      if (r < t.Px) { x = r; y = 0; }
+      else if (r < 2 * t.Px) { x = r - t.Px; y = t.Py - 1; }
+      else { const int r2 = r - 2 * t.Px; y = 1 + (r2 >> 1); x = (r2 & 1) ? t.Px - 1 : 0; }
+      p = pz * face + (long long)y * t.Px + x;
+    }
+    buf[p * chunks + c] = make_uint4(0u, 0u, 0u, 0u);
   }
 }
 
 template <int D>
 void zero_ghosts(const TileGeo& t, int C, bf16* buf, cudaStream_t st) {
-  const long long npad = (long long)t.Px * t.Py * t.Pz;
+  const long long face = (long long)t.Px * t.Py;
+  const long long n = ((D == 3 ? 2 * face : 0) + (long long)(D == 3 ? t.Pz - 2 : t.Pz) * (2 * t.Px + 2 * (t.Py - 2))) *
+                      (C / 8);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_zero_ghosts<D><<<(unsigned)std::min<long long>((npad + 255) / 256, 4096), 256, 0, st>>>(
+  k_zero_ghosts<D><<<(unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 8192)), 256, 0, st>>>(
       t, C / 8, reinterpret_cast<uint4*>(buf));
 }
 
@@ -500,20 +716,61 @@ __global__ void k_ratio_acc(double* scal, int dst, int num, int den, double fact
   scal[dst] = first ? r : scal[dst] + r;
 }
 
-// node features of one Q1 level
+// log-coefficient of every cell of one Q1 level: the mean of log k over the
+// cell's np^D Gauss points xi, k being the top level's cell coefficient
+// (ratio = n_top / n_l fine cells per level cell and direction).  Consecutive
+// points in one fine cell reuse its logarithm (the same value the sum would
+// add again), so the top level costs one log per cell.
 template <int D>
-__global__ void k_features(TileGeo t, int n_l, long long n_top, double ratio, int np, const double* __restrict__ xi,
-                           const double* __restrict__ kcell, double kconst, const double* __restrict__ mean,
-                           bf16* __restrict__ X0) {
+__global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, const double* __restrict__ xi,
+                            const double* __restrict__ kcell, double* __restrict__ lk) {
+  long long nc = n_l;
+  for (int k = 1; k < D; ++k) nc *= n_l;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const unsigned cu = (unsigned)c, nu = (unsigned)n_l;  // nc < 2^32 (checked by the launcher)
+  const int cc[3] = {(int)(cu % nu), (int)((cu / nu) % nu), D == 3 ? (int)(cu / (nu * nu)) : 0};
+  int nq = 1;
+  for (int k = 0; k < D; ++k) nq *= np;
+  if (ratio == 1.0) {  // every Gauss point lies in the cell itself (0 < xi < 1)
+    const double l1 = log(kcell[c]);
+    double s1 = 0.0;
+    for (int q = 0; q < nq; ++q) s1 += l1;
+    lk[c] = s1 / nq;
+    return;
+  }
+  double s = 0.0, lv = 0.0;
+  long long last = -1;
+  for (int q = 0; q < nq; ++q) {
+    const int qi[3] = {q % np, (q / np) % np, q / (np * np)};
+    long long fi[3] = {0, 0, 0};
+    for (int k = 0; k < D; ++k) fi[k] = (long long)floor(((double)cc[k] + xi[qi[k]]) * ratio);
+    const long long idx = fi[0] + n_top * (fi[1] + n_top * fi[2]);
+    if (idx != last) {
+      lv = log(kcell[idx]);
+      last = idx;
+    }
+    s += lv;
+  }
+  lk[c] = s / nq;
+}
+
+// node features of one Q1 level from the level's cell log-coefficients lk
+// (null: the constant log kconst)
+template <int D>
+__global__ void k_features(TileGeo t, int n_l, const double* __restrict__ lkc, double kconst,
+                           const double* __restrict__ mean, bf16* __restrict__ X0) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)t.Mx * t.My * t.Mz) return;
-  const int ix = (int)(i % t.Mx), iy = (int)((i / t.Mx) % t.My), iz = (int)(i / ((long long)t.Mx * t.My));
+  const unsigned iu = (unsigned)i, mx = (unsigned)t.Mx, my = (unsigned)t.My;  // < 2^32 nodes (launcher)
+  const int ix = (int)(iu % mx), iy = (int)((iu / mx) % my), iz = (int)(iu / (mx * my));
   const int node[3] = {ix, iy, iz};
   constexpr int NC = 1 << D;
   float f[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) f[c] = 0.f;
   const double mu = *mean;
+#pragma unroll
   for (int c = 0; c < NC; ++c) {
     int cc[3] = {0, 0, 0};
     bool in = true;
@@ -522,21 +779,7 @@ __global__ void k_features(TileGeo t, int n_l, long long n_top, double ratio, in
       in = in && cc[k] >= 0 && cc[k] < n_l;
     }
     if (!in) continue;
-    double lk;
-    if (kcell) {
-      int nq = 1;
-      for (int k = 0; k < D; ++k) nq *= np;
-      double s = 0.0;
-      for (int q = 0; q < nq; ++q) {
-        const int qi[3] = {q % np, (q / np) % np, q / (np * np)};
-        long long fi[3] = {0, 0, 0};
-        for (int k = 0; k < D; ++k) fi[k] = (long long)floor(((double)cc[k] + xi[qi[k]]) * ratio);
-        s += log(kcell[fi[0] + n_top * (fi[1] + n_top * fi[2])]);
-      }
-      lk = s / nq;
-    } else {
-      lk = log(kconst);
-    }
+    const double lk = lkc ? __ldg(lkc + cc[0] + (long long)n_l * (cc[1] + (long long)n_l * cc[2])) : log(kconst);
     f[c] = (float)fmin(fmax((lk - mu) * 0.5, -8.0), 8.0);
     f[NC + c] = 1.f;
   }
@@ -639,15 +882,28 @@ int sm_count() {
 
 template <int D, int CIN, int COUT, int EPI>
 void conv(const ConvArgs& a, cudaStream_t st) {
-  constexpr size_t smem = (size_t)Tp<D>::TAPS * COUT * CIN * 2 + (size_t)(CIN / 8) * Tp<D>::CHB;
-  static bool init = false;
-  if (!init) {
-    cudaFuncSetAttribute(k_conv<D, CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    init = true;
+  if constexpr (D == 3) {
+    constexpr size_t smem = Z3<CIN, COUT>::SMEM;
+    static bool init3 = false;
+    if (!init3) {
+      cudaFuncSetAttribute(k_conv3z<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      init3 = true;
+    }
+    const long long items = (long long)a.t.ntx * a.t.nty * ((a.t.Mz + kSeg - 1) / kSeg);
+    const long long grid = std::min<long long>(items, 2LL * sm_count());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_conv3z<CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a);
+  } else {
+    constexpr size_t smem = (size_t)Tp<D>::TAPS * COUT * CIN * 2 + (size_t)(CIN / 8) * Tp<D>::CHB;
+    static bool init = false;
+    if (!init) {
+      cudaFuncSetAttribute(k_conv<D, CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      init = true;
+    }
+    const long long grid = std::min<long long>(a.t.ntiles, 2LL * sm_count());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_conv<D, CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a);
   }
-  const long long grid = std::min<long long>(a.t.ntiles, 2LL * sm_count());
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_conv<D, CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a);
 }
 
 template <int D, int CG, int CX>
@@ -801,14 +1057,30 @@ void launch_logmean(const double* k, long long n, double* scratch, double* out, 
   k_logmean_final<<<1, kBlock, 0, st>>>(scratch, nb, n, out);
 }
 
-void launch_features(const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
-                     const double* kcell, double kconst, const double* mean, bf16* X0, cudaStream_t st) {
+int launch_features(fmg_net* net, const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
+                    const double* kcell, double kconst, const double* mean, cudaStream_t st) {
   const TileGeo t = tile_geo(g);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  if (g.D == 3)
-    k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, n_top, ratio, np, xi, kcell, kconst, mean, X0);
-  else
-    k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, n_top, ratio, np, xi, kcell, kconst, mean, X0);
+  long long ncell = n_l;
+  for (int k = 1; k < g.D; ++k) ncell *= n_l;
+  if (kcell && ncell > net->lk_cap) {
+    cudaStreamSynchronize(st);
+    net_free(net, net->lk);
+    net->lk = nullptr;
+    net->lk_cap = 0;
+    if (int rc = net_alloc(net, (void**)&net->lk, (size_t)ncell * sizeof(double))) return rc;
+    net->lk_cap = ncell;
+  }
+  const double* lk = kcell ? net->lk : nullptr;
+  if (ncell >= (1LL << 32) || g.nodes() >= (1LL << 32)) return FMG_ERR_UNSUPPORTED;
+  g_launches.fetch_add(kcell ? 2 : 1, std::memory_order_relaxed);
+  if (g.D == 3) {
+    if (kcell) k_cell_logk<3><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, net->lk);
+    k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, lk, kconst, mean, net->X0);
+  } else {
+    if (kcell) k_cell_logk<2><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, net->lk);
+    k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, lk, kconst, mean, net->X0);
+  }
+  return FMG_OK;
 }
 
 int net_forward(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st) {

@@ -113,7 +113,7 @@ class DampingNet:
             self.h = None
 
     def __del__(self):
-        if _core._EXITING:
+        if _core is None or _core._EXITING:
             return
         try:
             self.close()

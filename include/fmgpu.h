@@ -268,6 +268,14 @@ int fmg_learn_step(fmg_net* net, fmg_grid* grid, const fmg_solve_cfg* cfg, int n
    and CG restarts from the current residual with the plain cycle. */
 int fmg_learned_judge(fmg_grid* grid, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned,
                       int* accepted);
+/* fmg_learned_judge for the mixed-precision solve: the CG probe takes its 6
+   steps with fmg_solve_mixed (the FP32/BF16 cycle, with and without the node
+   damping) instead of fmg_solve, so the damping is judged with the cycle that
+   fmg_solve_mixed runs, at about a third of the FP64 probe's cost.
+   cfg->method must be FMG_METHOD_CG_MG; mcfg as for fmg_solve_mixed
+   (max_outer is ignored). */
+int fmg_learned_judge_mixed(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg,
+                            double* rho_plain, double* rho_learned, int* accepted);
 /* active: learned damping installed and accepted; reverts: mixed solves whose
    runtime judge fell back to the plain cycle */
 int fmg_learned_status(const fmg_grid* grid, int* active, double* rho_plain, double* rho_learned, int* reverts);

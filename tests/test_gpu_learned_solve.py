@@ -155,3 +155,33 @@ def test_2d_net_gains_on_held_out_block_fields(G, ctx):
     assert all(r["plain_status"] == 0 and r["learned_status"] == 0 for r in rows)
     assert lrn.mean() <= 0.85 * plain.mean(), (plain, lrn)
     assert np.all(lrn <= plain + 1), (plain, lrn)
+
+
+def test_mixed_judge_agrees_with_the_fp64_judge(G, ctx):
+    # the judge's CG probe run with the mixed cycle: same verdicts, contraction
+    # figures close to the FP64 cycle's (the FP32/BF16 cycle is a slightly
+    # different preconditioner), and the divergent damping is still rejected
+    from gnu_femlisp_b200.learn import DampingNet
+    g = _grid(G, ctx, 6, 0)
+    cfg = _cfg(G)
+    net = DampingNet.load(ctx, WEIGHTS)
+    net.apply(g)
+    ok64, rp64, rl64 = g.learned_judge(cfg)
+    net.apply(g)
+    ok, rp, rl = g.learned_judge_mixed(cfg)
+    assert ok64 and ok and rl < 0.98 * rp, (rp, rl)
+    assert abs(rp - rp64) < 0.1 * rp64 and abs(rl - rl64) < 0.1 * rl64, (rp64, rl64, rp, rl)
+    assert g.learned_status()["active"]
+    x = g.vector()
+    hist, _, _, st = g.solve_mixed(cfg, x)
+    assert st == 0 and hist[-1] / hist[0] < 1e-10
+    bad = _divergent_net(G, ctx)
+    bad.apply(g)
+    ok, rp2, rl2 = g.learned_judge_mixed(cfg)
+    assert not ok and rl2 > rp2 and not g.learned_status()["active"], (rp2, rl2)
+    assert abs(rp2 - rp) < 1e-9 * rp  # the plain probe is deterministic
+    C = G._capi
+    mg = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 10, C.FMG_MULTIPLICATIVE)
+    bad.apply(g)
+    with pytest.raises(G.FmgError):
+        g.learned_judge_mixed(mg)
