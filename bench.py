@@ -47,8 +47,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--matvec-reps", type=int, default=20)
     ap.add_argument("--no-learned", action="store_true", help="mixed precision without the damping network")
-    ap.add_argument("--config", choices=["c3", "c4"], default="c3",
-                    help="c4: the learned smoother on 128^2 block fields, 256 held-out seeds, its own JSON line")
+    ap.add_argument("--config", choices=["c2", "c3", "c4"], default="c3",
+                    help=("c2: plain FP64 Q2 SOR multigrid on 64^3 cells vs the oracle; c4: the learned "
+                          "smoother on 128^2 block fields, 256 held-out seeds; each its own JSON line"))
     ap.add_argument("--c4-fields", type=int, default=256)
     ap.add_argument("--profile", choices=["solve", "net"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
@@ -521,6 +522,114 @@ def ctypes_count(C) -> int:
     return v.value
 
 
+def run_c2(args):
+    """3D Poisson, f = sin(pi x) sin(pi y) sin(pi z), Q2 on 64^3 cells
+    (2,146,689 nodes), the multigrid iteration with V(2,2) multicolour
+    SOR(1.2), base level 2 (4^3 cells, dense LU), from x = 0 to 1e-10: the
+    plain FP64 GPU path, with the oracle (C++ restatement, all host threads)
+    timed on a bounded sample of the same solve beside it."""
+    import torch
+
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.iteration import sample_at_gauss_points
+    from oracle import oracle as O
+    C = G._capi
+    wl = problems.c2()
+    n = wl.nodes
+    fip = sample_at_gauss_points(wl.source, 3, 2, wl.n_cells)
+    ctx = G.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    g = G.Grid(ctx, 3, 2, wl.level, base_level=wl.base_level)
+    g.set_coefficient(C.FMG_F_IP, fip)
+    cfg = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_SOR, wl.damp, wl.pre, wl.post, 1, 0, 1.0, wl.rtol, 0.0, 200,
+                     C.FMG_MULTIPLICATIVE)
+
+    def timed(fn, reps):
+        ctx.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        out = None
+        for _ in range(reps):
+            out = fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        ctx.synchronize()
+        return ev0.elapsed_time(ev1) / 1e3 / reps, out
+
+    for _ in range(2):
+        g.assemble()
+    t_asm, _ = timed(lambda: g.assemble(), 3)
+    x = g.vector()
+
+    def solve():
+        x.fill(0.0)
+        return g.solve(cfg, x)
+    for _ in range(max(args.warmup, 1)):
+        solve()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_solve, (hist, cycles, status) = timed(solve, args.steps)
+    B = g.vector(values=g.rhs())
+    R, X = g.vector(), g.vector()
+    one = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_SOR, wl.damp, wl.pre, wl.post, 1, 0, 1.0, 0.0, 0.0, 1,
+                     C.FMG_MULTIPLICATIVE)
+    for _ in range(3):
+        g.vcycle(one, X, B, R)
+    t_cycle, _ = timed(lambda: g.vcycle(one, X, B, R), 10)
+    P = g.vector(values=np.random.default_rng(1).standard_normal(n))
+    Y = g.vector()
+    for _ in range(3):
+        g.matvec(P, Y)
+    t_mv, _ = timed(lambda: g.matvec(P, Y), args.matvec_reps)
+    clk = clocks.stop()
+    if status != 0:
+        raise RuntimeError(f"C2 solve did not converge in {cycles} cycles")
+    nnz = (8 * wl.n_cells + 1) ** 3
+    alg_bytes = 8 * nnz + 16 * n
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / t_mv / 1e9
+    # CPU: the same algorithm restated in C++ (bitwise the GPU path's
+    # arithmetic), assembly plus a bounded number of cycles, extrapolated by
+    # the GPU's cycle count
+    cpu = None
+    if not args.no_cpu_baseline:
+        O.build()
+        o = O.Oracle(3, 2, wl.level, base_level=wl.base_level)
+        o.set_coefficient(O.F_IP, fip)
+        t0 = time.perf_counter()
+        o.assemble()
+        t_asm_cpu = time.perf_counter() - t0
+        sample = 2
+        ocfg = O.solve_cfg(method=O.METHOD_MG, smoother=O.SOR, damp=wl.damp, pre=wl.pre, post=wl.post,
+                           compat=False, rtol=wl.rtol, maxsteps=sample)
+        t0 = time.perf_counter()
+        r = o.solve(ocfg)
+        per_cycle = (time.perf_counter() - t0) / max(r.steps, 1)
+        t_cpu = per_cycle * cycles
+        cpu = {"value": n / t_cpu / 1e6, "unit": "MDoF/s to 1e-10 (N / time-to-solution)",
+               "cores": O.num_threads(), "kind": "port",
+               "sample": (f"oracle C++ restatement, {O.num_threads()} OpenMP threads: assembly "
+                          f"({t_asm_cpu:.1f} s) + {r.steps} cycles ({per_cycle:.2f} s/cycle) x {cycles} cycles"),
+               "assembly_s": t_asm_cpu, "time_to_solution_est_s": t_cpu}
+    line = {"metric": "C2 time to 1e-10 (plain FP64 GPU multigrid, Q2 SOR V(2,2))",
+            "value": n / t_solve / 1e6, "unit": "MDoF/s to 1e-10 (N / time-to-solution)", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_solve * 1e3, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "nodes": n, "nnz": nnz,
+                       "solver": "MG iteration, V(2,2) multicolour SOR(1.2), base level 2 dense LU",
+                       "l2": "inputs larger than L2 (2.2 GB level-6 matrix)"},
+            "time_to_solution_s": t_solve, "cycles": int(cycles), "assembly_s": t_asm,
+            "vcycle_ms": t_cycle * 1e3, "mdof_per_s_per_vcycle": n / t_cycle / 1e6,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_spmv<3,2> (top-level FP64 Q2 matvec)", "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
+            "cpu_baseline": cpu, "clocks": clk,
+            "history_tail": [float(v) for v in hist[-3:]]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
@@ -531,6 +640,9 @@ def main():
         elif args.config == "c4":
             if rank == 0:
                 run_c4(args)
+        elif args.config == "c2":
+            if rank == 0:
+                run_c2(args)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
