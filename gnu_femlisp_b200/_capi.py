@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libfmgpu.so")
 HEADER = os.path.join(os.path.dirname(_HERE), "include", "fmgpu.h")
 
 FMG_OK = 0
-FMG_K_CONST, FMG_K_CELL, FMG_F_CONST, FMG_F_IP = 0, 1, 2, 3
+FMG_K_CONST, FMG_K_CELL, FMG_F_CONST, FMG_F_IP, FMG_LAMBDA_MU_CELL, FMG_F_VEC = 0, 1, 2, 3, 4, 5
 FMG_JACOBI, FMG_SOR = 0, 1
 FMG_METHOD_MG, FMG_METHOD_CG_MG, FMG_METHOD_CG = 0, 1, 2
 FMG_MULTIPLICATIVE, FMG_ADDITIVE = 0, 1

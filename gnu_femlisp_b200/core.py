@@ -76,6 +76,7 @@ class Grid:
     def __init__(self, ctx: Context, dim: int, order: int, level: int, base_level: int = 0,
                  n0: int = 1, ncomp: int = 1, dirichlet_mask: int | None = None):
         self.ctx, self.dim, self.order, self.top, self.base = ctx, dim, order, level, base_level
+        self.nc = ncomp
         if dirichlet_mask is None:
             dirichlet_mask = (1 << (2 * dim)) - 1
         h = ctypes.c_void_p()
@@ -108,12 +109,12 @@ class Grid:
 
     def matrix(self, level: int | None = None) -> np.ndarray:
         level = self.top if level is None else level
-        out = np.zeros(self.nslots * self.nnodes(level))
+        out = np.zeros(self.nslots * self.nc * self.nc * self.nnodes(level))
         self.ctx.check(self._lib.fmg_get_matrix(self.h, level, C.dptr(out)), "get_matrix")
-        return out.reshape(self.nslots, -1)
+        return out.reshape(self.nslots * self.nc * self.nc, -1)
 
     def rhs(self) -> np.ndarray:
-        out = np.zeros(self.nnodes())
+        out = np.zeros(self.nnodes() * self.nc)
         self.ctx.check(self._lib.fmg_get_rhs(self.h, C.dptr(out)), "get_rhs")
         return out
 
@@ -220,7 +221,7 @@ class Vector:
 
     def __init__(self, grid: Grid, level: int):
         self.grid, self.level = grid, level
-        self.n = grid.nnodes(level)
+        self.n = grid.nnodes(level) * grid.nc
         h = ctypes.c_void_p()
         grid.ctx.check(grid._lib.fmg_vec_create(grid.h, level, ctypes.byref(h)), "vec_create")
         self.h = h

@@ -62,6 +62,7 @@ struct fmg_grid {
   double kconst = 1.0;
   int fkind = FMG_F_CONST;
   double fconst = 1.0;
+  double fvec[3] = {0.0, 0.0, 0.0};  // FMG_F_VEC
   double xi_h[3] = {0, 0, 0};
   double* xi_d = nullptr;
   double* kcell_d = nullptr;
@@ -270,6 +271,55 @@ void make_tables(int dim, int order, double h, std::vector<double>& C, std::vect
   *nq_out = nq;
 }
 
+// Elastic tables of one level, lambda = mu = E (isotropic-elasticity-tensor,
+// elasticity.lisp:71-88, in the A-term of ellsys-fe.lisp:120-127), per unit E:
+//   Etab[q][a][b][k][l] = W_q h^d (G_ak G_bl + G_al G_bk + d_kl G_a . G_b),
+// t = fma(G_al, G_bk, G_ak G_bl), t = t + G_a . G_b on the diagonal, the dot
+// as an fma chain over the directions; Ebar = sum_q Etab[q].
+void make_elastic_tables(int dim, int order, double h, std::vector<double>& E, std::vector<double>& Ebar) {
+  int np;
+  double xi[3], w[3];
+  gauss1d(order, &np, xi, w);
+  const int p1 = order + 1;
+  int nl = 1, nq = 1;
+  for (int k = 0; k < dim; ++k) { nl *= p1; nq *= np; }
+  double vol = 1.0;
+  for (int k = 0; k < dim; ++k) vol = vol * h;
+  const double invh = 1.0 / h;
+  const size_t per_q = (size_t)nl * nl * dim * dim;
+  E.assign(per_q * nq, 0.0);
+  Ebar.assign(per_q, 0.0);
+  std::vector<double> G((size_t)nl * 3);
+  for (int q = 0; q < nq; ++q) {
+    const int qi[3] = {q % np, (q / np) % np, q / (np * np)};
+    double W = 1.0;
+    for (int k = 0; k < dim; ++k) W = W * w[qi[k]];
+    const double Wv = W * vol;
+    for (int a = 0; a < nl; ++a) {
+      const int ai[3] = {a % p1, (a / p1) % p1, a / (p1 * p1)};
+      for (int kd = 0; kd < dim; ++kd) {
+        double gg = 1.0;
+        for (int k = 0; k < dim; ++k)
+          gg = gg * (k == kd ? dlag(order, ai[k], xi[qi[k]]) : lag(order, ai[k], xi[qi[k]]));
+        G[a * 3 + kd] = gg * invh;
+      }
+    }
+    for (int a = 0; a < nl; ++a)
+      for (int b = 0; b < nl; ++b) {
+        double gg = G[a * 3] * G[b * 3];
+        for (int kd = 1; kd < dim; ++kd) gg = std::fma(G[a * 3 + kd], G[b * 3 + kd], gg);
+        for (int k = 0; k < dim; ++k)
+          for (int l = 0; l < dim; ++l) {
+            double t = std::fma(G[a * 3 + l], G[b * 3 + k], G[a * 3 + k] * G[b * 3 + l]);
+            if (k == l) t = t + gg;
+            E[(size_t)q * per_q + (((size_t)a * nl + b) * dim + k) * dim + l] = Wv * t;
+          }
+      }
+  }
+  for (int q = 0; q < nq; ++q)
+    for (size_t e = 0; e < per_q; ++e) Ebar[e] = Ebar[e] + E[(size_t)q * per_q + e];
+}
+
 int upload(fmg_grid* g, double** dst, const std::vector<double>& v) {
   int rc = dalloc(g, dst, (long long)v.size());
   if (rc) return rc;
@@ -284,6 +334,7 @@ LevelView view(const fmg_grid* g, int l) {
   v.A = L.A; v.N = L.N; v.Np = L.Np; v.M = L.M;
   v.dim = g->dim; v.order = g->order; v.dmask = g->dmask; v.center = g->center;
   v.omega = L.omega;
+  v.nc = g->nc;
   return v;
 }
 
@@ -395,6 +446,8 @@ struct MG {
 
 int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (!c) return set_err(g->ctx, FMG_ERR_ARG, "null configuration");
+  if (g->nc != 1 && c->smoother != FMG_JACOBI)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "3-component grids: the (block) Jacobi smoother only");
   if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR)
     return set_err(g->ctx, FMG_ERR_ARG, "unknown smoother %d", c->smoother);
   if (c->pre_steps < 0 || c->post_steps < 0 || c->gamma < 0 || c->gamma > 4)
@@ -491,7 +544,8 @@ int fmg_grid_create(fmg_ctx* c, int dim, int order, int ncomp, int n0, int top_l
       top_level >= kMaxLevels)
     return set_err(c, FMG_ERR_ARG, "unsupported grid (dim %d order %d levels %d..%d)", dim, order, base_level,
                    top_level);
-  if (ncomp != 1) return set_err(c, FMG_ERR_UNSUPPORTED, "ncomp %d: only scalar problems are built", ncomp);
+  if (ncomp != 1 && !(ncomp == 3 && dim == 3))
+    return set_err(c, FMG_ERR_UNSUPPORTED, "ncomp %d: scalar problems and 3D elasticity (3) are built", ncomp);
   fmg_grid* g = new (std::nothrow) fmg_grid();
   if (!g) return FMG_ERR_NOMEM;
   g->ctx = c;
@@ -569,7 +623,23 @@ int fmg_set_coefficient(fmg_grid* g, int kind, const double* host, long n) {
     case FMG_F_CONST:
       if (n != 1) return set_err(g->ctx, FMG_ERR_ARG, "F_CONST wants 1 value");
       g->fkind = kind; g->fconst = host[0]; break;
+    case FMG_LAMBDA_MU_CELL: {  // elasticity: lambda = mu = E per top-level cell
+      if (g->nc != 3) return set_err(g->ctx, FMG_ERR_ARG, "LAMBDA_MU_CELL is for 3-component grids");
+      if (n != ncell) return set_err(g->ctx, FMG_ERR_ARG, "LAMBDA_MU_CELL wants %lld values, got %ld", ncell, n);
+      int rc;
+      if (!g->kcell_d && (rc = dalloc(g, &g->kcell_d, ncell))) return rc;
+      FMG_CK(g->ctx, cudaMemcpyAsync(g->kcell_d, host, ncell * sizeof(double), cudaMemcpyHostToDevice, g->ctx->stream));
+      FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+      g->kkind = FMG_K_CELL;
+      break;
+    }
+    case FMG_F_VEC:
+      if (g->nc != 3 || n != 3) return set_err(g->ctx, FMG_ERR_ARG, "F_VEC wants 3 values on a 3-component grid");
+      g->fkind = kind;
+      for (int k = 0; k < 3; ++k) g->fvec[k] = host[k];
+      break;
     case FMG_F_IP: {
+      if (g->nc != 1) return set_err(g->ctx, FMG_ERR_ARG, "F_IP is for scalar grids");
       if (n != ncell * g->nq) return set_err(g->ctx, FMG_ERR_ARG, "F_IP wants %lld values", ncell * g->nq);
       int rc;
       if (!g->fip_d && (rc = dalloc(g, &g->fip_d, ncell * g->nq))) return rc;
@@ -596,40 +666,44 @@ static int ensure_buffers(fmg_grid* g) {
   if (g->top > g->base) ncell_kq = ncell_top >> g->dim;  // largest coarse level
   std::vector<double> xiv(g->xi_h, g->xi_h + g->np);
   if ((rc = upload(g, &g->xi_d, xiv))) return rc;
-  if ((rc = dalloc(g, &g->rhs, T.Np))) return rc;
+  const int nc = g->nc;
+  if ((rc = dalloc(g, &g->rhs, T.Np * nc))) return rc;
   if ((rc = dalloc(g, &g->kq, ncell_kq * g->nq))) return rc;
   for (int l = g->top; l >= g->base; --l) {
     Lvl& L = g->lev[l];
     std::vector<double> C, Kbar, Phi;
     int nl, nq;
     make_tables(g->dim, g->order, L.h, C, Kbar, Phi, &nl, &nq);
+    if (nc == 3) make_elastic_tables(g->dim, g->order, L.h, C, Kbar);  // Kbar := Ebar, C := Etab
     if ((rc = upload(g, &L.Kbar, Kbar)) || (rc = upload(g, &L.Ctab, C)) || (rc = upload(g, &L.Phi, Phi)))
       return rc;
     L.Kbar_h = Kbar;
     L.Ctab_h = C;
-    if ((rc = dalloc(g, &L.A, (long long)g->nslots * L.Np))) return rc;
+    if ((rc = dalloc(g, &L.A, (long long)g->nslots * nc * nc * L.Np))) return rc;
   }
   const Lvl& B = g->lev[g->base];
-  if (B.N > 1024)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "base level has %lld nodes; the dense coarse solve takes <= 1024",
-                   B.N);
-  g->nbase = (int)B.N;
-  const long long nn = (long long)B.N * B.N;
+  const long long nb = B.N * nc;
+  if ((nc == 1 && nb > 1024) || nb > 2048)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
+                   "base level has %lld unknowns; the dense coarse solve takes <= %d", nb, nc == 1 ? 1024 : 2048);
+  g->nbase = (int)nb;
+  const long long nn = nb * nb;
   if ((rc = dalloc(g, &g->lu, nn)) || (rc = dalloc(g, &g->lux, nn)) || (rc = dalloc(g, &g->ainvT, nn)) ||
-      (rc = dalloc(g, (double**)&g->piv, B.N)))
+      (rc = dalloc(g, (double**)&g->piv, nb)))
     return rc;
   for (int l = g->base; l < g->top; ++l) {
     Lvl& L = g->lev[l];
-    if ((rc = dalloc(g, &L.sol[0], L.Np)) || (rc = dalloc(g, &L.sol[1], L.Np)) || (rc = dalloc(g, &L.rhs, L.Np)) ||
-        (rc = dalloc(g, &L.res, L.Np)))
+    const long long nv = L.Np * nc;
+    if ((rc = dalloc(g, &L.sol[0], nv)) || (rc = dalloc(g, &L.sol[1], nv)) || (rc = dalloc(g, &L.rhs, nv)) ||
+        (rc = dalloc(g, &L.res, nv)))
       return rc;
   }
   if ((rc = dalloc(g, &g->scal, S_COUNT))) return rc;
-  if ((rc = dalloc(g, &g->part, nchunks(T.Np) + 1))) return rc;
+  if ((rc = dalloc(g, &g->part, nchunks(T.Np * nc) + 1))) return rc;
   if ((rc = dalloc(g, (double**)&g->counter, 1))) return rc;
   double** tv[] = {&g->p, &g->a, &g->w, &g->w2, &g->q, &g->r, &g->xs, &g->xs2};
   for (double** v : tv)
-    if ((rc = dalloc(g, v, T.Np))) return rc;
+    if ((rc = dalloc(g, v, T.Np * nc))) return rc;
   g->assembled_once = true;
   return FMG_OK;
 }
@@ -663,14 +737,18 @@ int fmg_assemble(fmg_grid* g) {
     a.kq = sample ? g->kq : nullptr;
     a.fip = g->fkind == FMG_F_IP ? g->fip_d : nullptr;
     a.kconst = g->kconst; a.fconst = g->fconst;
+    a.nc = g->nc;
+    a.fvec_on = g->fkind == FMG_F_VEC ? 1 : 0;
+    for (int k = 0; k < 3; ++k) a.fvec[k] = g->fvec[k];
     launch_assemble(g->dim, g->order, a, L.Kbar_h.data(), L.Ctab_h.data(), st);
     if ((rc = launched(c, "assemble"))) return rc;
   }
   // dense LU of the base level and its explicit inverse
   const Lvl& B = g->lev[g->base];
-  FMG_CK(c, cudaMemsetAsync(g->lu, 0, (size_t)B.N * B.N * sizeof(double), st));
+  const long long nb = B.N * g->nc;
+  FMG_CK(c, cudaMemsetAsync(g->lu, 0, (size_t)nb * nb * sizeof(double), st));
   launch_densify(view(g, g->base), g->lu, st);
-  launch_lu(g->lu, (int)B.N, g->piv, g->lux, g->ainvT, st);
+  launch_lu(g->lu, (int)nb, g->piv, g->lux, g->ainvT, st);
   if ((rc = launched(c, "coarse LU"))) return rc;
   // multigrid state
   const int nlev = g->top + 1;
@@ -693,7 +771,7 @@ int fmg_get_matrix(fmg_grid* g, int level, double* host) {
   if (level < g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d out of range", level);
   const Lvl& L = g->lev[level];
   FMG_CK(g->ctx, cudaMemcpy2DAsync(host, L.N * sizeof(double), L.A, L.Np * sizeof(double), L.N * sizeof(double),
-                                   g->nslots, cudaMemcpyDeviceToHost, g->ctx->stream));
+                                   (size_t)g->nslots * g->nc * g->nc, cudaMemcpyDeviceToHost, g->ctx->stream));
   FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
   return FMG_OK;
 }
@@ -702,7 +780,8 @@ int fmg_get_rhs(fmg_grid* g, double* host) {
   if (!g || !host) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   const Lvl& T = g->lev[g->top];
-  FMG_CK(g->ctx, cudaMemcpyAsync(host, g->rhs, T.N * sizeof(double), cudaMemcpyDeviceToHost, g->ctx->stream));
+  FMG_CK(g->ctx, cudaMemcpyAsync(host, g->rhs, T.N * g->nc * sizeof(double), cudaMemcpyDeviceToHost,
+                                 g->ctx->stream));
   FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
   return FMG_OK;
 }
@@ -729,7 +808,7 @@ int fmg_vec_create(fmg_grid* g, int level, fmg_vec** out) {
   if (!g || !out || level < 0 || level > g->top) return FMG_ERR_ARG;
   fmg_vec* v = new (std::nothrow) fmg_vec();
   if (!v) return FMG_ERR_NOMEM;
-  v->g = g; v->level = level; v->n = g->lev[level].N;
+  v->g = g; v->level = level; v->n = g->lev[level].N * g->nc;
   g->vecs += 1;
   const long long np = pad64(v->n);
   cudaError_t e = cudaMalloc((void**)&v->d, np * sizeof(double));
@@ -883,7 +962,7 @@ int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, 
   cudaStream_t st = c->stream;
   const fmg_solve_cfg& cf = *cfg;
   const LevelView T = view(g, g->top);
-  const long long n = T.N;
+  const long long n = T.N * g->nc;
   const double* b = g->rhs;
   double* x = xv->d;
   double* xspare = g->xs2;
@@ -1255,6 +1334,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (!mcfg || vec_check(xv, g, g->top) || !nouter || !ninner || !status) return FMG_ERR_ARG;
+  if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed solve: scalar grids only");
   if (cfg->smoother != FMG_JACOBI || cfg->combination != FMG_MULTIPLICATIVE || cfg->gamma != 1 ||
       g->base >= g->top || cfg->post_steps < 1)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
@@ -1615,8 +1695,8 @@ int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
   int rc = check_cfg(g, cf);
   if (rc) return rc;
   if (cf->smoother != FMG_JACOBI || cf->combination != FMG_MULTIPLICATIVE || cf->pre_steps != 1 ||
-      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training loss: Jacobi V(1,1) with at least two levels");
+      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base || g->nc != 1)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training loss: scalar Jacobi V(1,1) with at least two levels");
   return FMG_OK;
 }
 
@@ -1969,8 +2049,8 @@ int learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mc
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
-  if (cfg->smoother != FMG_JACOBI || g->top <= g->base)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: Jacobi cycles with at least two levels");
+  if (cfg->smoother != FMG_JACOBI || g->top <= g->base || g->nc != 1)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: scalar Jacobi cycles with at least two levels");
   const bool cg = cfg->method == FMG_METHOD_CG_MG;
   if (mc && !cg) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed judge: the CG+MG method only");
   bool any = false;

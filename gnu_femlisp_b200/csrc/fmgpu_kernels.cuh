@@ -7,16 +7,18 @@ namespace fmg {
 
 // what a kernel needs to know about one level
 struct LevelView {
-  const double* A;      // [slot][Np]
+  const double* A;      // [slot][Np], or [slot][k][l][Np] for nc = 3
   long long N, Np, M;   // nodes, padded stride, nodes per direction
   int dim, order, dmask, center;
   const double* omega;  // per-node damping or nullptr
+  int nc = 1;           // components per node (1, or 3 for elasticity)
 };
 
 // arguments of the assembly kernel of one level
 struct AsmArgs {
   long long N, Np, M, n;        // nodes, padded stride, nodes/direction, cells/direction
   int dmask, nl, nq;
+  int nc = 1;                   // components (3: elasticity, Kbar/Ctab = Ebar/Etab)
   double* A;                    // out: [slot][Np]
   double* rhs;                  // out (top level only) or nullptr
   const double* Kbar;           // [a][b]: sum over Gauss points
@@ -26,6 +28,8 @@ struct AsmArgs {
   const double* kq;             // coarse level: k per cell and Gauss point, or nullptr
   const double* fip;            // source per cell and Gauss point, or nullptr
   double kconst, fconst;
+  double fvec[3] = {0.0, 0.0, 0.0};  // nc = 3: constant force per component
+  int fvec_on = 0;
 };
 
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,

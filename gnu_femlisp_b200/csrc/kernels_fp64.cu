@@ -459,6 +459,21 @@ k_coarse_solve(const double* __restrict__ AinvT, int n, double damp, double* x, 
   x[i] = fma(damp, acc, x[i]);
 }
 
+// the same for n > 1024 unknowns (block bases of the vector form): one CTA,
+// rows strided over its threads, the residual staged in shared memory
+__global__ void __launch_bounds__(1024)
+k_coarse_solve_big(const double* __restrict__ AinvT, int n, double damp, double* x, double* r) {
+  extern __shared__ double rsb[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) rsb[i] = r[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double acc = 0.0;
+    for (int j = 0; j < n; ++j) acc = fma(AinvT[(long long)j * n + i], rsb[j], acc);
+    r[i] = acc;
+    x[i] = fma(damp, acc, x[i]);
+  }
+}
+
 // ------------------------------------------------------------ vector ops
 __global__ void k_fill(double* x, long long n, double v) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -730,6 +745,320 @@ k_assemble_q1_3d(AsmArgs g, const __grid_constant__ Q1Tab tab) {
   }
 }
 
+// ====================================================== vector form (nc = 3)
+// Elasticity with 3 x 3 nodal blocks: vectors [node][3], level matrices
+// [slot][k][l][Np] (block row component k, column component l).  Every
+// kernel follows the scalar one with the component loops innermost, in the
+// order the oracle uses.
+
+// t := B^-1 r for one diagonal block: LU with partial pivoting (the first
+// largest |entry| of the column, LAPACK dgetrf semantics) and substitution
+// -- the gesv! of <jacobi> on a 3 x 3 block (linit.lisp:234)
+__device__ __forceinline__ void block_solve3(const double* B, const double* r, double* t) {
+  double M[3][3], b[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    b[k] = r[k];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) M[k][m] = B[k * 3 + m];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    int pr = c;
+    double mx = fabs(M[c][c]);
+#pragma unroll
+    for (int rr = c + 1; rr < 3; ++rr)
+      if (fabs(M[rr][c]) > mx) { mx = fabs(M[rr][c]); pr = rr; }
+    if (pr != c) {
+#pragma unroll
+      for (int rr = c + 1; rr < 3; ++rr)
+        if (rr == pr) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) { const double tt = M[c][m]; M[c][m] = M[rr][m]; M[rr][m] = tt; }
+          const double tb = b[c]; b[c] = b[rr]; b[rr] = tb;
+        }
+    }
+#pragma unroll
+    for (int rr = c + 1; rr < 3; ++rr) {
+      const double f = M[rr][c] / M[c][c];
+#pragma unroll
+      for (int m = c + 1; m < 3; ++m) M[rr][m] = fma(-f, M[c][m], M[rr][m]);
+      b[rr] = fma(-f, b[c], b[rr]);
+    }
+  }
+#pragma unroll
+  for (int c = 2; c >= 0; --c) {
+    double sacc = b[c];
+#pragma unroll
+    for (int m = c + 1; m < 3; ++m) sacc = fma(-M[c][m], t[m], sacc);
+    t[c] = sacc / M[c][c];
+  }
+}
+
+// the three block-row sums of node i: slots ascending, columns ascending
+template <int P>
+__device__ __forceinline__ void row_sums3(const double* __restrict__ A, long long N, long long Np, long long M,
+                                          const double* __restrict__ x, long long i, double* s, double* dblk) {
+  constexpr int NS = St<3, P>::NS;
+  constexpr int C = St<3, P>::CENTER;
+  s[0] = s[1] = s[2] = 0.0;
+#pragma unroll 5
+  for (int sl = 0; sl < NS; ++sl) {
+    const long long j = clampi(i + slot_off<3, P>(sl, M), N);
+    const double xj[3] = {__ldg(x + 3 * j), __ldg(x + 3 * j + 1), __ldg(x + 3 * j + 2)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const double a = __ldg(A + ((long long)(sl * 3 + k) * 3 + m) * Np + i);
+        if (dblk && sl == C) dblk[k * 3 + m] = a;
+        s[k] = fma(a, xj[m], s[k]);
+      }
+  }
+}
+
+// y = A x or r = b - A x (b may alias r)
+template <int P, bool RES>
+__global__ void __launch_bounds__(kBlock)
+k_spmv3(const double* __restrict__ A, long long N, long long Np, long long M, const double* __restrict__ x,
+        const double* b, double* y) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s[3];
+  row_sums3<P>(A, N, Np, M, x, i, s, nullptr);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) y[3 * i + k] = RES ? b[3 * i + k] - s[k] : s[k];
+}
+
+// <jacobi> on 3 x 3 blocks with an up-to-date residual: t = B^-1 r_i, x_i += w t, r_i := t
+__global__ void __launch_bounds__(kBlock)
+k_jacobi3(const double* __restrict__ A, long long N, long long Np, int center, double damp,
+          const double* __restrict__ omega, double* x, double* r, int write_r) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double B[9], t[3];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) B[e] = A[((long long)center * 9 + e) * Np + i];
+  const double rr[3] = {r[3 * i], r[3 * i + 1], r[3 * i + 2]};
+  block_solve3(B, rr, t);
+  const double w = omega ? omega[i] : damp;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (write_r) r[3 * i + k] = t[k];
+    x[3 * i + k] = fma(w, t[k], x[3 * i + k]);
+  }
+}
+
+// compute-residual fused with the following block <jacobi> step:
+// r_i = b_i - (A x)_i, t = B^-1 r_i, xout_i = x_i + w t, r_i := t
+template <int P>
+__global__ void __launch_bounds__(kBlock)
+k_jacobi_res3(const double* __restrict__ A, long long N, long long Np, long long M, double damp,
+              const double* __restrict__ omega, const double* __restrict__ x, const double* b,
+              double* __restrict__ xout, double* r, int write_r) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s[3], B[9], t[3];
+  row_sums3<P>(A, N, Np, M, x, i, s, B);
+  const double rr[3] = {b[3 * i] - s[0], b[3 * i + 1] - s[1], b[3 * i + 2] - s[2]};
+  block_solve3(B, rr, t);
+  const double w = omega ? omega[i] : damp;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (write_r) r[3 * i + k] = t[k];
+    xout[3 * i + k] = fma(w, t[k], x[3 * i + k]);
+  }
+}
+
+// rc := I^T rf per component (constrained), rhs_c := rc, sol_c := 0
+template <int P>
+__global__ void __launch_bounds__(kBlock)
+k_restrict3(int MC, int MF, int dmask, const double* __restrict__ rf, double* __restrict__ rc,
+            double* __restrict__ rhsc, double* __restrict__ solc) {
+  const int cJ[3] = {(int)(blockIdx.x * 32 + threadIdx.x), (int)(blockIdx.y * 8 + threadIdx.y), (int)blockIdx.z};
+  if (cJ[0] >= MC || cJ[1] >= MC) return;
+  const long long J = cJ[0] + (long long)MC * (cJ[1] + (long long)MC * cJ[2]);
+  bool dj = false;
+  for (int k = 0; k < 3; ++k) dj = dj || face_dir(cJ[k], MC, k, dmask);
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (!dj) {
+    long long off[3][5] = {{0}, {0}, {0}};
+    double w[3][5] = {{1.0}, {1.0}, {1.0}};
+    int cnt[3];
+    for (int k = 0; k < 3; ++k) cnt[k] = restrict_1d<P>(cJ[k], off[k], w[k]);
+    for (int z = 0; z < cnt[2]; ++z)
+      for (int y = 0; y < cnt[1]; ++y)
+        for (int xx = 0; xx < cnt[0]; ++xx) {
+          const int fi[3] = {2 * cJ[0] + (int)off[0][xx], 2 * cJ[1] + (int)off[1][y], 2 * cJ[2] + (int)off[2][z]};
+          bool skip = false;
+          for (int k = 0; k < 3; ++k) skip = skip || fi[k] < 0 || fi[k] >= MF || face_dir(fi[k], MF, k, dmask);
+          if (skip) continue;
+          const double ww = w[0][xx] * w[1][y] * w[2][z];
+          const long long f = fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2]);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[c] = fma(ww, rf[3 * f + c], acc[c]);
+        }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    rc[3 * J + c] = acc[c];
+    rhsc[3 * J + c] = acc[c];
+    solc[3 * J + c] = 0.0;
+  }
+}
+
+// xf := xf + I xc per component (constrained)
+template <int P>
+__global__ void __launch_bounds__(kBlock)
+k_prolong3(int MF, int MC, int dmask, const double* __restrict__ xc, double* __restrict__ xf) {
+  const int fi[3] = {(int)(blockIdx.x * 32 + threadIdx.x), (int)(blockIdx.y * 8 + threadIdx.y), (int)blockIdx.z};
+  if (fi[0] >= MF || fi[1] >= MF) return;
+  for (int k = 0; k < 3; ++k)
+    if (face_dir(fi[k], MF, k, dmask)) return;
+  const long long i = fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2]);
+  long long J[3][3] = {{0}, {0}, {0}};
+  double w[3][3] = {{1.0}, {1.0}, {1.0}};
+  int cnt[3];
+  for (int k = 0; k < 3; ++k) cnt[k] = prolong_1d<P>(fi[k], J[k], w[k]);
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int z = 0; z < cnt[2]; ++z)
+    for (int y = 0; y < cnt[1]; ++y)
+      for (int xx = 0; xx < cnt[0]; ++xx) {
+        const int cj[3] = {(int)J[0][xx], (int)J[1][y], (int)J[2][z]};
+        bool dj = false;
+        for (int k = 0; k < 3; ++k) dj = dj || face_dir(cj[k], MC, k, dmask);
+        if (dj) continue;
+        const double ww = w[0][xx] * w[1][y] * w[2][z];
+        const long long j = cj[0] + (long long)MC * (cj[1] + (long long)MC * cj[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] = fma(ww, xc[3 * j + c], acc[c]);
+      }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) xf[3 * i + c] = xf[3 * i + c] + acc[c];
+}
+
+// Elasticity stiffness by gather (the vector form of k_assemble): for node i,
+// slot s and block entry (k, l), the sum over the cells containing both nodes,
+// in increasing cell index, of E_c Ebar[a][b][k][l] (top level, E per cell)
+// or sum_q fma(E(x_q), Etab[q][a][b][k][l], .) (coarse levels, E sampled at
+// the cell's Gauss points); Dirichlet nodes get identity blocks, Dirichlet
+// columns are dropped.  a.Kbar = Ebar, a.Ctab = Etab, a.fvec the force.
+template <int P>
+__global__ void __launch_bounds__(kBlock)
+k_assemble3(AsmArgs g) {
+  constexpr int NS = St<3, P>::NS;
+  constexpr int C = St<3, P>::CENTER;
+  constexpr int W = 2 * P + 1;
+  constexpr int P1 = P + 1;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  long long ci[3];
+  node_coords(i, g.M, 3, ci);
+  const int nl = g.nl, nq = g.nq;
+  if (node_dirichlet(ci, g.M, 3, g.dmask)) {
+    for (int s = 0; s < NS; ++s)
+      for (int e = 0; e < 9; ++e) g.A[((long long)s * 9 + e) * g.Np + i] = (s == C && e % 4 == 0) ? 1.0 : 0.0;
+    if (g.rhs)
+      for (int k = 0; k < 3; ++k) g.rhs[3 * i + k] = 0.0;
+    return;
+  }
+  for (int s = 0; s < NS; ++s) {
+    const long long o[3] = {s % W - P, (s / W) % W - P, s / (W * W) - P};
+    long long cj[3], lo[3], hi[3];
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+      cj[k] = ci[k] + o[k];
+      if (cj[k] < 0 || cj[k] >= g.M) ok = false;
+      const long long mx = ci[k] > cj[k] ? ci[k] : cj[k];
+      const long long mn = ci[k] < cj[k] ? ci[k] : cj[k];
+      lo[k] = mx >= P ? (mx - 1) / P : 0;
+      hi[k] = mn / P;
+      if (hi[k] > g.n - 1) hi[k] = g.n - 1;
+    }
+    double v[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) v[e] = 0.0;
+    if (ok && !node_dirichlet(cj, g.M, 3, g.dmask)) {
+      for (long long cz = lo[2]; cz <= hi[2]; ++cz)
+        for (long long cy = lo[1]; cy <= hi[1]; ++cy)
+          for (long long cx = lo[0]; cx <= hi[0]; ++cx) {
+            const long long cc[3] = {cx, cy, cz};
+            const long long cidx = cx + g.n * (cy + g.n * cz);
+            int a = 0, b = 0, mul = 1;
+            for (int k = 0; k < 3; ++k) {
+              a += (int)(ci[k] - P * cc[k]) * mul;
+              b += (int)(cj[k] - P * cc[k]) * mul;
+              mul *= P1;
+            }
+            const long long ab = ((long long)a * nl + b) * 9;
+            if (g.kq == nullptr) {
+              const double kc = g.kcell ? g.kcell[cidx] : g.kconst;
+#pragma unroll
+              for (int e = 0; e < 9; ++e) v[e] = v[e] + kc * __ldg(g.Kbar + ab + e);
+            } else {
+#pragma unroll
+              for (int e = 0; e < 9; ++e) {
+                double ee = 0.0;
+                for (int q = 0; q < nq; ++q)
+                  ee = fma(__ldg(g.kq + cidx * nq + q), __ldg(g.Ctab + (long long)q * nl * nl * 9 + ab + e), ee);
+                v[e] = v[e] + ee;
+              }
+            }
+          }
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) g.A[((long long)s * 9 + e) * g.Np + i] = v[e];
+  }
+  if (g.rhs) {
+    long long lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = ci[k] >= P ? (ci[k] - 1) / P : 0;
+      hi[k] = ci[k] / P;
+      if (hi[k] > g.n - 1) hi[k] = g.n - 1;
+    }
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long cz = lo[2]; cz <= hi[2]; ++cz)
+      for (long long cy = lo[1]; cy <= hi[1]; ++cy)
+        for (long long cx = lo[0]; cx <= hi[0]; ++cx) {
+          const long long cc[3] = {cx, cy, cz};
+          int a = 0, mul = 1;
+          for (int k = 0; k < 3; ++k) { a += (int)(ci[k] - P * cc[k]) * mul; mul *= P1; }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            double bl = 0.0;
+            const double f = g.fvec_on ? g.fvec[k] : g.fconst;
+            for (int q = 0; q < nq; ++q) bl = fma(f, g.Phi[q * nl + a], bl);
+            acc[k] = acc[k] + bl;
+          }
+        }
+    for (int k = 0; k < 3; ++k) g.rhs[3 * i + k] = acc[k];
+  }
+}
+
+// dense (3N x 3N) copy of a small block level matrix, for the coarse LU
+template <int P>
+__global__ void k_densify3(const double* __restrict__ A, long long N, long long Np, long long M,
+                           double* __restrict__ Dm) {
+  constexpr int NS = St<3, P>::NS;
+  constexpr int W = 2 * P + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N * NS) return;
+  const long long i = t / NS;
+  const int s = (int)(t % NS);
+  long long ci[3];
+  node_coords(i, M, 3, ci);
+  const long long o[3] = {s % W - P, (s / W) % W - P, s / (W * W) - P};
+  long long cj[3];
+  for (int k = 0; k < 3; ++k) {
+    cj[k] = ci[k] + o[k];
+    if (cj[k] < 0 || cj[k] >= M) return;
+  }
+  const long long j = cj[0] + M * (cj[1] + M * cj[2]);
+  const long long n = 3 * N;
+  for (int k = 0; k < 3; ++k)
+    for (int m = 0; m < 3; ++m) Dm[(3 * i + k) * n + 3 * j + m] = A[((long long)s * 9 + k * 3 + m) * Np + i];
+}
+
 // ---------------------------------------------------------- dispatchers
 #define FMG_DISPATCH(D_, P_, ...)                                             \
   do {                                                                        \
@@ -745,6 +1074,18 @@ static inline unsigned grid1(long long n, int bs = kBlock) { return (unsigned)((
 
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
                  const Reduce* R, cudaStream_t st) {
+  if (L.nc == 3) {  // 3 x 3 blocks: the reduction, if any, as a separate DR4096 pass
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (L.order == 2) {
+      if (b) k_spmv3<2, true><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y);
+      else k_spmv3<2, false><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y);
+    } else {
+      if (b) k_spmv3<1, true><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y);
+      else k_spmv3<1, false><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y);
+    }
+    if (dv) launch_dot(y, dv, 3 * L.N, *R, st);
+    return;
+  }
   g_launches.fetch_add(1, std::memory_order_relaxed);
   const unsigned g = nchunks(L.N);
   Reduce r0 = R ? *R : Reduce{};
@@ -758,6 +1099,10 @@ void launch_spmv(const LevelView& L, const double* x, const double* b, double* y
 
 void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.nc == 3) {
+    k_jacobi3<<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.center, damp, L.omega, x, r, write_r ? 1 : 0);
+    return;
+  }
   const double* Dg = L.A + (long long)L.center * L.Np;
   k_jacobi<<<grid1(L.N), kBlock, 0, st>>>(Dg, L.N, damp, L.omega, x, r, write_r ? 1 : 0);
 }
@@ -765,6 +1110,16 @@ void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool w
 void launch_jacobi_res(const LevelView& L, double damp, const double* x, const double* b, double* xout,
                        double* r, bool write_r, const double* dv, const Reduce* R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.nc == 3) {
+    if (L.order == 2)
+      k_jacobi_res3<2><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+                                                        write_r ? 1 : 0);
+    else
+      k_jacobi_res3<1><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+                                                        write_r ? 1 : 0);
+    if (dv) launch_dot(xout, dv, 3 * L.N, *R, st);
+    return;
+  }
   const unsigned g = nchunks(L.N);
   Reduce r0 = R ? *R : Reduce{};
   FMG_DISPATCH(L.dim, L.order, {
@@ -797,6 +1152,13 @@ static inline dim3 xfer_grid(long long M, int dim) {
 void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, double* rc, double* rhsc,
                      double* solc, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (F.nc == 3) {
+    if (F.order == 2)
+      k_restrict3<2><<<xfer_grid(Cl.M, 3), dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc);
+    else
+      k_restrict3<1><<<xfer_grid(Cl.M, 3), dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc);
+    return;
+  }
   FMG_DISPATCH(F.dim, F.order, {
     k_restrict<D, P><<<xfer_grid(Cl.M, D), dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc);
   });
@@ -804,6 +1166,13 @@ void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, 
 
 void launch_prolong(const LevelView& Cl, const LevelView& F, const double* xc, double* xf, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (F.nc == 3) {
+    if (F.order == 2)
+      k_prolong3<2><<<xfer_grid(F.M, 3), dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf);
+    else
+      k_prolong3<1><<<xfer_grid(F.M, 3), dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf);
+    return;
+  }
   FMG_DISPATCH(F.dim, F.order, {
     k_prolong<D, P><<<xfer_grid(F.M, D), dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf);
   });
@@ -811,7 +1180,16 @@ void launch_prolong(const LevelView& Cl, const LevelView& F, const double* xc, d
 
 void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_coarse_solve<<<1, 1024, 0, st>>>(AinvT, n, damp, x, r);
+  if (n <= 1024) {
+    k_coarse_solve<<<1, 1024, 0, st>>>(AinvT, n, damp, x, r);
+  } else {
+    static bool init = false;
+    if (!init) {
+      cudaFuncSetAttribute(k_coarse_solve_big, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024 * 4);
+      init = true;
+    }
+    k_coarse_solve_big<<<1, 1024, (size_t)n * sizeof(double), st>>>(AinvT, n, damp, x, r);
+  }
 }
 
 void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t st) {
@@ -875,6 +1253,11 @@ void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_to
 void launch_assemble(int dim, int order, const AsmArgs& a, const double* kbar_h, const double* ctab_h,
                      cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (a.nc == 3) {  // elasticity: a.Kbar / a.Ctab hold the elastic tables
+    if (order == 2) k_assemble3<2><<<grid1(a.N), kBlock, 0, st>>>(a);
+    else k_assemble3<1><<<grid1(a.N), kBlock, 0, st>>>(a);
+    return;
+  }
   if (dim == 3 && order == 1 && a.nl == 8 && a.nq == 8 && kbar_h && ctab_h && a.M < (1 << 20)) {
     Q1Tab tab;
     std::memcpy(tab.K, kbar_h, sizeof tab.K);
@@ -912,6 +1295,11 @@ __global__ void k_densify(const double* __restrict__ A, long long N, long long N
 
 void launch_densify(const LevelView& L, double* Dm, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.nc == 3) {
+    if (L.order == 2) k_densify3<2><<<grid1(L.N * St<3, 2>::NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);
+    else k_densify3<1><<<grid1(L.N * St<3, 1>::NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);
+    return;
+  }
   FMG_DISPATCH(L.dim, L.order, {
     constexpr int NS = St<D, P>::NS;
     k_densify<D, P><<<grid1(L.N * NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);

@@ -44,6 +44,11 @@ extern "C" {
 #define FMG_F_CONST 2           /* constant source, n = 1 (default 1.0) */
 #define FMG_F_IP 3              /* source at the Gauss points of every top-level
                                    cell, n = cells * (order+1)^dim */
+#define FMG_LAMBDA_MU_CELL 4    /* elasticity (ncomp 3): the Lame constants
+                                   lambda = mu = E per top-level cell, n = cells
+                                   (isotropic-elasticity-tensor, elasticity.lisp:71-88);
+                                   coarse levels sample E at their Gauss points */
+#define FMG_F_VEC 5             /* elasticity: constant force vector, n = ncomp */
 
 /* ------------------------------------------------------------ iteration */
 #define FMG_JACOBI 0            /* <jacobi> :damp (linit.lisp:220-250) */
@@ -97,9 +102,13 @@ int fmg_launch_count(long long* out);
 /* A level hierarchy base_level..top_level of the uniformly refined unit
    n-cube (uniformly-refined-hierarchical-mesh, meshgen.lisp:180-183) with
    Lagrange order `order` (lagrange-fe, lagrange.lisp:176-202) and `ncomp`
-   components.  dirichlet_mask bit 2k / 2k+1 marks the face x_k = 0 / 1 as
-   essential boundary (the :external-boundary constraint coefficient,
-   cdr.lisp:184-185). */
+   components: 1 (the cdr problem) or 3 with dim 3 (linear elasticity,
+   elasticity-model-problem, elasticity.lisp:112-123: vectors hold 3 values
+   per node, node-major; level matrices 3 x 3 blocks per stencil slot, layout
+   [slot][k][l][node]; the Jacobi smoother inverts the 3 x 3 diagonal blocks;
+   CG / MG with Jacobi only).  dirichlet_mask bit 2k / 2k+1 marks the face
+   x_k = 0 / 1 as essential boundary, all components of its nodes (the
+   :external-boundary constraint coefficient, cdr.lisp:184-185). */
 int fmg_grid_create(fmg_ctx* ctx, int dim, int order, int ncomp, int n0, int top_level,
                     int base_level, int dirichlet_mask, fmg_grid** grid);
 int fmg_grid_destroy(fmg_grid* grid);

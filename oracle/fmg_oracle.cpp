@@ -128,6 +128,8 @@ struct Tables {
   std::vector<double> C;     // [q][a][b]: (W_q vol) * grad phi_a . grad phi_b
   std::vector<double> Kbar;  // [a][b]: sum_q C
   std::vector<double> Phi;   // [q][a]: (W_q vol) * phi_a
+  std::vector<double> G;     // [q][a][3]: grad phi_a at point q
+  std::vector<double> Wv;    // [q]: W_q vol
 };
 
 Tables make_tables(int dim, int order, double h) {
@@ -161,6 +163,8 @@ Tables make_tables(int dim, int order, double h) {
         G[a * 3 + kd] = g * invh;
       }
     }
+    T.Wv.push_back(Wv);
+    T.G.insert(T.G.end(), G.begin(), G.end());
     for (int a = 0; a < T.nl; ++a) {
       T.Phi[(size_t)q * T.nl + a] = Wv * phi[a];
       for (int b = 0; b < T.nl; ++b) {
@@ -173,6 +177,43 @@ Tables make_tables(int dim, int order, double h) {
   for (int q = 0; q < T.nq; ++q)
     for (int ab = 0; ab < T.nl * T.nl; ++ab) T.Kbar[ab] = T.Kbar[ab] + T.C[(size_t)q * T.nl * T.nl + ab];
   return T;
+}
+
+// Isotropic elasticity with lambda = mu = E (isotropic-elasticity-tensor,
+// elasticity.lisp:71-88: A^{kl}_{ij} = lambda d_ik d_jl + mu (d_ij d_kl +
+// d_kj d_il)) in the A-term of discretize-locally (ellsys-fe.lisp:120-127,
+// block (k,l) += w (G D^{kl}) G^T), per unit E at point q:
+//   E_q[a][b][k][l] = (W_q vol) (G_ak G_bl + G_al G_bk + d_kl G_a . G_b)
+// formed as t = fma(G_al, G_bk, G_ak * G_bl), t = t + G_a . G_b when k = l,
+// with G_a . G_b = fma chain over the directions; Ebar = sum_q E_q.
+struct ElasticTables {
+  std::vector<double> E;     // [q][a][b][k][l]
+  std::vector<double> Ebar;  // [a][b][k][l]
+};
+
+ElasticTables make_elastic_tables(const Tables& T) {
+  ElasticTables X;
+  const int nl = T.nl, nq = T.nq, d = T.dim;
+  const size_t per_q = (size_t)nl * nl * d * d;
+  X.E.assign(per_q * nq, 0.0);
+  X.Ebar.assign(per_q, 0.0);
+  for (int q = 0; q < nq; ++q) {
+    const double* G = &T.G[(size_t)q * nl * 3];
+    for (int a = 0; a < nl; ++a)
+      for (int b = 0; b < nl; ++b) {
+        double gg = G[a * 3] * G[b * 3];
+        for (int kd = 1; kd < d; ++kd) gg = std::fma(G[a * 3 + kd], G[b * 3 + kd], gg);
+        for (int k = 0; k < d; ++k)
+          for (int l = 0; l < d; ++l) {
+            double t = std::fma(G[a * 3 + l], G[b * 3 + k], G[a * 3 + k] * G[b * 3 + l]);
+            if (k == l) t = t + gg;
+            X.E[(size_t)q * per_q + (((size_t)a * nl + b) * d + k) * d + l] = T.Wv[q] * t;
+          }
+      }
+  }
+  for (int q = 0; q < nq; ++q)
+    for (size_t e = 0; e < per_q; ++e) X.Ebar[e] = X.Ebar[e] + X.E[(size_t)q * per_q + e];
+  return X;
 }
 
 // ---------------------------------------------------------------- hierarchy
@@ -192,6 +233,7 @@ struct Hier {
   std::vector<double> kcell;    // top-level cells
   int fkind = ORA_F_CONST;
   double fconst = 1.0;
+  double fvec[3] = {0.0, 0.0, 0.0};  // ORA_F_VEC: constant force per component
   std::vector<double> fip;      // top-level cells x nq
   std::vector<Level> lev;
   std::vector<double> rhs;
@@ -247,11 +289,13 @@ double k_at(const Hier& H, int l, const Tables& T, const long cc[3], int q) {
   return H.kcell[idx];
 }
 
+int assemble_level_vec(Hier& H, int l);
+
 int assemble_level(Hier& H, int l) {
   Level& L = H.lev[l];
   Tables T = make_tables(H.dim, H.order, L.h);
   const int p = H.order, p1 = p + 1, nl = T.nl, nq = T.nq, nc = H.nc;
-  if (nc != 1) return -2;  // vector-valued assembly: elasticity path not in this oracle build
+  if (nc != 1) return assemble_level_vec(H, l);
   L.A.assign((size_t)H.nslots * L.N, 0.0);
   const bool top = (l == H.top);
   const bool cellconst = (H.kkind == ORA_K_CONST) || top;
@@ -316,14 +360,94 @@ int assemble_level(Hier& H, int l) {
   return 0;
 }
 
+// the vector (nc = dim) elasticity form of assemble_level: the same gather,
+// each node pair contributing an nc x nc block; layout [slot][k][l][node],
+// the rhs [node][k]
+int assemble_level_vec(Hier& H, int l) {
+  Level& L = H.lev[l];
+  Tables T = make_tables(H.dim, H.order, L.h);
+  ElasticTables X = make_elastic_tables(T);
+  const int p = H.order, p1 = p + 1, nl = T.nl, nq = T.nq, nc = H.nc;
+  if (nc != H.dim) return -2;
+  L.A.assign((size_t)H.nslots * nc * nc * L.N, 0.0);
+  const bool top = (l == H.top);
+  const bool cellconst = (H.kkind == ORA_K_CONST) || top;
+  if (top) H.rhs.assign((size_t)L.N * nc, 0.0);
+  const long n = L.n, M = L.M, N = L.N;
+  const int center = [&] { long z[3] = {0, 0, 0}; return slot_of(H, z); }();
+  auto at = [&](int s, int k, int m, long i) -> double& { return L.A[(((size_t)s * nc + k) * nc + m) * N + i]; };
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < N; ++i) {
+    long ci[3];
+    coords(H, M, i, ci);
+    if (is_dirichlet(H, M, ci)) {
+      for (int k = 0; k < nc; ++k) at(center, k, k, i) = 1.0;
+      continue;
+    }
+    long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int k = 0; k < H.dim; ++k) {
+      lo[k] = ci[k] >= p ? (ci[k] - 1) / p : 0;
+      hi[k] = std::min(n - 1, ci[k] / p);
+    }
+    double acc_b[3] = {0.0, 0.0, 0.0};
+    for (long cz = lo[2]; cz <= hi[2]; ++cz)
+      for (long cy = lo[1]; cy <= hi[1]; ++cy)
+        for (long cx = lo[0]; cx <= hi[0]; ++cx) {
+          long cc[3] = {cx, cy, cz};
+          long cidx = cx + n * (cy + n * cz);
+          int ai[3] = {0, 0, 0};
+          for (int k = 0; k < H.dim; ++k) ai[k] = (int)(ci[k] - p * cc[k]);
+          int a = ai[0] + p1 * (ai[1] + p1 * ai[2]);
+          double kc = 0.0;
+          double kq[27];
+          if (cellconst) kc = (H.kkind == ORA_K_CONST) ? H.kconst : H.kcell[cidx];
+          else
+            for (int q = 0; q < nq; ++q) kq[q] = k_at(H, l, T, cc, q);
+          for (int b = 0; b < nl; ++b) {
+            int bi[3] = {b % p1, (b / p1) % p1, b / (p1 * p1)};
+            long cj[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+            for (int k = 0; k < H.dim; ++k) { cj[k] = p * cc[k] + bi[k]; o[k] = cj[k] - ci[k]; }
+            if (is_dirichlet(H, M, cj)) continue;
+            int s = slot_of(H, o);
+            for (int k = 0; k < nc; ++k)
+              for (int m = 0; m < nc; ++m) {
+                const size_t e = (((size_t)a * nl + b) * nc + k) * nc + m;
+                double v;
+                if (cellconst) v = kc * X.Ebar[e];
+                else {
+                  v = 0.0;
+                  for (int q = 0; q < nq; ++q) v = std::fma(kq[q], X.E[(size_t)q * nl * nl * nc * nc + e], v);
+                }
+                double& dst = at(s, k, m, i);
+                dst = dst + v;
+              }
+          }
+          if (top) {
+            for (int k = 0; k < nc; ++k) {
+              double bl = 0.0;
+              for (int q = 0; q < nq; ++q) {
+                double f = (H.fkind == ORA_F_VEC) ? H.fvec[k] : H.fconst;
+                bl = std::fma(f, T.Phi[(size_t)q * nl + a], bl);
+              }
+              acc_b[k] = acc_b[k] + bl;
+            }
+          }
+        }
+    if (top)
+      for (int k = 0; k < nc; ++k) H.rhs[(size_t)i * nc + k] = acc_b[k];
+  }
+  return 0;
+}
+
 // dense LU with partial pivoting and explicit inverse of the base level
 // (replaces the sparse LDU of sparselu.lisp:61-216; both are exact solves)
 void build_coarse_inverse(Hier& H) {
   Level& L = H.lev[H.base];
-  long n = L.N;  // nc == 1
+  const int nc = H.nc;
+  long n = L.N * nc;
   H.nbase = n;
   std::vector<double> A((size_t)n * n, 0.0);
-  for (long i = 0; i < n; ++i)
+  for (long i = 0; i < L.N; ++i)
     for (int s = 0; s < H.nslots; ++s) {
       long o[3];
       slot_offset(H, s, o);
@@ -334,7 +458,9 @@ void build_coarse_inverse(Hier& H) {
       for (int k = 0; k < H.dim; ++k) if (cj[k] < 0 || cj[k] >= L.M) in = false;
       if (!in) continue;
       long j = cj[0] + L.M * (cj[1] + L.M * cj[2]);
-      A[(size_t)i * n + j] = L.A[(size_t)s * L.N + i];
+      for (int k = 0; k < nc; ++k)
+        for (int m = 0; m < nc; ++m)
+          A[(size_t)(i * nc + k) * n + (j * nc + m)] = L.A[(((size_t)s * nc + k) * nc + m) * L.N + i];
     }
   std::vector<long> piv(n);
   for (long k = 0; k < n; ++k) {
@@ -391,9 +517,40 @@ inline double row_sum(const Hier& H, const Level& L, long i, const double* x) {
   return acc;
 }
 
+// row (i, k) of a block (nc > 1) level: slots ascending, the nc columns of
+// each block ascending: acc = fma(A[s][k][m][i], x[j nc + m], acc)
+inline double row_sum_vec(const Hier& H, const Level& L, long i, int k, const double* x) {
+  const int nc = H.nc;
+  long ci[3];
+  coords(H, L.M, i, ci);
+  double acc = 0.0;
+  for (int s = 0; s < H.nslots; ++s) {
+    long o[3];
+    slot_offset(H, s, o);
+    bool in = true;
+    long cj[3];
+    for (int kk = 0; kk < 3; ++kk) {
+      cj[kk] = ci[kk] + o[kk];
+      if (kk < H.dim && (cj[kk] < 0 || cj[kk] >= L.M)) in = false;
+    }
+    if (!in) continue;
+    long j = cj[0] + L.M * (cj[1] + L.M * cj[2]);
+    for (int m = 0; m < nc; ++m)
+      acc = std::fma(L.A[(((size_t)s * nc + k) * nc + m) * L.N + i], x[j * nc + m], acc);
+  }
+  return acc;
+}
+
 // gemm! 1.0 A x 0.0 y (sparse-matrix.lisp:392-405)
 void matvec(const Hier& H, int l, const double* x, double* y) {
   const Level& L = H.lev[l];
+  const int nc = H.nc;
+  if (nc > 1) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < L.N; ++i)
+      for (int k = 0; k < nc; ++k) y[i * nc + k] = row_sum_vec(H, L, i, k, x);
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < L.N; ++i) y[i] = row_sum(H, L, i, x);
 }
@@ -401,10 +558,51 @@ void matvec(const Hier& H, int l, const double* x, double* y) {
 // compute-residual r := b - A x (linit.lisp:73-80); b may alias r
 void residual(const Hier& H, int l, const double* x, const double* b, double* r) {
   const Level& L = H.lev[l];
+  const int nc = H.nc;
+  if (nc > 1) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < L.N; ++i) {
+      double sv[3];
+      for (int k = 0; k < nc; ++k) sv[k] = row_sum_vec(H, L, i, k, x);
+      for (int k = 0; k < nc; ++k) r[i * nc + k] = b[i * nc + k] - sv[k];
+    }
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < L.N; ++i) {
     double s = row_sum(H, L, i, x);
     r[i] = b[i] - s;
+  }
+}
+
+// t := B^-1 r for one 3 x 3 (nc x nc) diagonal block: LU with partial
+// pivoting (first largest |entry| of the column, LAPACK dgetrf semantics)
+// and substitution, the operation order fixed as written
+void block_solve(const double* Bm, int nc, const double* r, double* t) {
+  double M[3][3], b[3];
+  for (int k = 0; k < nc; ++k) {
+    b[k] = r[k];
+    for (int m = 0; m < nc; ++m) M[k][m] = Bm[k * nc + m];
+  }
+  for (int c = 0; c < nc; ++c) {
+    int pr = c;
+    double mx = std::fabs(M[c][c]);
+    for (int rr = c + 1; rr < nc; ++rr)
+      if (std::fabs(M[rr][c]) > mx) { mx = std::fabs(M[rr][c]); pr = rr; }
+    if (pr != c) {
+      for (int m = 0; m < nc; ++m) std::swap(M[c][m], M[pr][m]);
+      std::swap(b[c], b[pr]);
+    }
+    for (int rr = c + 1; rr < nc; ++rr) {
+      const double f = M[rr][c] / M[c][c];
+      for (int m = c + 1; m < nc; ++m) M[rr][m] = std::fma(-f, M[c][m], M[rr][m]);
+      b[rr] = std::fma(-f, b[c], b[rr]);
+    }
+  }
+  for (int c = nc - 1; c >= 0; --c) {
+    double sacc = b[c];
+    for (int m = c + 1; m < nc; ++m) sacc = std::fma(-M[c][m], t[m], sacc);
+    t[c] = sacc / M[c][c];
   }
 }
 
@@ -418,6 +616,24 @@ inline double diag(const Hier& H, const Level& L, long i) {
 void jacobi(const Hier& H, int l, double damp, double* x, double* r) {
   const Level& L = H.lev[l];
   const double* w = L.omega.empty() ? nullptr : L.omega.data();
+  const int nc = H.nc;
+  if (nc > 1) {  // 3 x 3 blocks (linit.lisp:234: gesv! on the diagonal block)
+    long z[3] = {0, 0, 0};
+    const int center = slot_of(H, z);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < L.N; ++i) {
+      double Bm[9], t[3];
+      for (int k = 0; k < nc; ++k)
+        for (int m = 0; m < nc; ++m) Bm[k * nc + m] = L.A[(((size_t)center * nc + k) * nc + m) * L.N + i];
+      block_solve(Bm, nc, r + i * nc, t);
+      const double om = w ? w[i] : damp;
+      for (int k = 0; k < nc; ++k) {
+        r[i * nc + k] = t[k];
+        x[i * nc + k] = std::fma(om, t[k], x[i * nc + k]);
+      }
+    }
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < L.N; ++i) {
     double t = r[i] / diag(H, L, i);
@@ -491,12 +707,13 @@ void restrict_(const Hier& H, int lf, const double* rf, double* rc) {
   for (long J = 0; J < C.N; ++J) {
     long cJ[3];
     coords(H, C.M, J, cJ);
-    if (is_dirichlet(H, C.M, cJ)) { rc[J] = 0.0; continue; }
+    const int nc = H.nc;
+    if (is_dirichlet(H, C.M, cJ)) { for (int c = 0; c < nc; ++c) rc[J * nc + c] = 0.0; continue; }
     long off[3][5] = {{0}, {0}, {0}};
     double w[3][5] = {{1.0}, {1.0}, {1.0}};
     int cnt[3] = {1, 1, 1};
     for (int k = 0; k < H.dim; ++k) cnt[k] = restrict_stencil1d(H.order, cJ[k], off[k], w[k]);
-    double acc = 0.0;
+    double acc[3] = {0.0, 0.0, 0.0};
     for (int z = 0; z < cnt[2]; ++z)
       for (int y = 0; y < cnt[1]; ++y)
         for (int x = 0; x < cnt[0]; ++x) {
@@ -509,9 +726,9 @@ void restrict_(const Hier& H, int lf, const double* rf, double* rc) {
           if (H.dim > 1) ww = ww * w[1][y];
           if (H.dim > 2) ww = ww * w[2][z];
           long i = fi[0] + F.M * (fi[1] + F.M * fi[2]);
-          acc = std::fma(ww, rf[i], acc);
+          for (int c = 0; c < nc; ++c) acc[c] = std::fma(ww, rf[i * nc + c], acc[c]);
         }
-    rc[J] = acc;
+    for (int c = 0; c < nc; ++c) rc[J * nc + c] = acc[c];
   }
 }
 
@@ -528,7 +745,8 @@ void prolongate(const Hier& H, int lc, const double* xc, double* xf, bool constr
     double w[3][3] = {{1.0}, {1.0}, {1.0}};
     int cnt[3] = {1, 1, 1};
     for (int k = 0; k < H.dim; ++k) cnt[k] = prolong_stencil1d(H.order, fi[k], J[k], w[k]);
-    double acc = 0.0;
+    const int nc = H.nc;
+    double acc[3] = {0.0, 0.0, 0.0};
     for (int z = 0; z < cnt[2]; ++z)
       for (int y = 0; y < cnt[1]; ++y)
         for (int x = 0; x < cnt[0]; ++x) {
@@ -538,9 +756,9 @@ void prolongate(const Hier& H, int lc, const double* xc, double* xf, bool constr
           if (H.dim > 1) ww = ww * w[1][y];
           if (H.dim > 2) ww = ww * w[2][z];
           long j = cj[0] + C.M * (cj[1] + C.M * cj[2]);
-          acc = std::fma(ww, xc[j], acc);
+          for (int c = 0; c < nc; ++c) acc[c] = std::fma(ww, xc[j * nc + c], acc[c]);
         }
-    xf[i] = xf[i] + acc;
+    for (int c = 0; c < nc; ++c) xf[i * nc + c] = xf[i * nc + c] + acc[c];
   }
 }
 
@@ -674,8 +892,8 @@ extern "C" {
 
 void* ora_create(int dim, int order, int ncomp, int n0, int top_level, int base_level,
                  int dirichlet_mask) {
-  if (dim < 1 || dim > 3 || order < 1 || order > 2 || ncomp < 1 || n0 < 1 || base_level < 0 ||
-      base_level > top_level || top_level > 12)
+  if (dim < 1 || dim > 3 || order < 1 || order > 2 || (ncomp != 1 && ncomp != dim) || n0 < 1 ||
+      base_level < 0 || base_level > top_level || top_level > 12)
     return nullptr;
   Hier* H = new Hier();
   H->dim = dim; H->order = order; H->nc = ncomp; H->n0 = n0;
@@ -706,7 +924,13 @@ int ora_set_coefficient(void* h, int kind, const double* vals, long n) {
     case ORA_K_CONST: if (n != 1) return -1; H.kkind = kind; H.kconst = vals[0]; break;
     case ORA_K_CELL: if (n != ncell) return -1; H.kkind = kind; H.kcell.assign(vals, vals + n); break;
     case ORA_F_CONST: if (n != 1) return -1; H.fkind = kind; H.fconst = vals[0]; break;
-    case ORA_F_IP: if (n != ncell * T.nq) return -1; H.fkind = kind; H.fip.assign(vals, vals + n); break;
+    case ORA_F_IP: if (n != ncell * T.nq || H.nc != 1) return -1; H.fkind = kind; H.fip.assign(vals, vals + n); break;
+    case ORA_LAMBDA_MU_CELL:  // lambda = mu = E per top-level cell (nc = dim)
+      if (n != ncell || H.nc == 1) return -1;
+      H.kkind = ORA_K_CELL;
+      H.kcell.assign(vals, vals + n);
+      break;
+    case ORA_F_VEC: if (n != H.nc) return -1; H.fkind = kind; for (int k = 0; k < n; ++k) H.fvec[k] = vals[k]; break;
     default: return -1;
   }
   H.assembled = false;
@@ -786,6 +1010,7 @@ int ora_jacobi(void* h, int level, double damp, double* x, double* r) {
   return 0;
 }
 int ora_sor(void* h, int level, double omega, double* x, const double* b, double* r) {
+  if (((Hier*)h)->nc != 1) return -2;
   sor(*(Hier*)h, level, omega, x, b, r);
   return 0;
 }
@@ -809,6 +1034,7 @@ int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* 
 int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hist_len, int* nsteps) {
   Hier& H = *(Hier*)h;
   if (!H.assembled) return -1;
+  if (H.nc != 1 && cfg->smoother == ORA_SOR) return -2;
   const ora_solve_cfg& c = *cfg;
   const int top = H.top;
   const long n = vec_len(H, top);

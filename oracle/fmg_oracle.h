@@ -46,7 +46,7 @@ extern "C" {
 #endif
 
 /* coefficient kinds (shared numbering with include/fmgpu.h) */
-enum { ORA_K_CONST = 0, ORA_K_CELL = 1, ORA_F_CONST = 2, ORA_F_IP = 3, ORA_LAMBDA_MU_CELL = 4 };
+enum { ORA_K_CONST = 0, ORA_K_CELL = 1, ORA_F_CONST = 2, ORA_F_IP = 3, ORA_LAMBDA_MU_CELL = 4, ORA_F_VEC = 5 };
 
 /* smoother kinds */
 enum { ORA_JACOBI = 0, ORA_SOR = 1 };
@@ -76,7 +76,7 @@ int ora_set_node_damping(void* h, int level, const double* w, long n);
 
 long ora_nnodes(void* h, int level);
 int ora_nslots(void* h);
-int ora_get_matrix(void* h, int level, double* out);      /* [slot][node][a][b] */
+int ora_get_matrix(void* h, int level, double* out);      /* [slot][k][l][node] (nc x nc blocks) */
 int ora_get_rhs(void* h, double* out);
 int ora_get_coarse_inverse(void* h, double* out);           /* n*n row-major */
 

@@ -16,7 +16,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libfmg_oracle.so")
 
-K_CONST, K_CELL, F_CONST, F_IP, LAMBDA_MU_CELL = 0, 1, 2, 3, 4
+K_CONST, K_CELL, F_CONST, F_IP, LAMBDA_MU_CELL, F_VEC = 0, 1, 2, 3, 4, 5
 JACOBI, SOR = 0, 1
 METHOD_MG, METHOD_CG_MG, METHOD_CG = 0, 1, 2
 
@@ -124,7 +124,7 @@ class Oracle:
     (meshgen.lisp:180-183) with Lagrange Q1/Q2 (lagrange.lisp:176-202)."""
 
     def __init__(self, dim, order, level, base_level=0, ncomp=1, n0=1, dirichlet_mask=None):
-        self.dim, self.order, self.top, self.base = dim, order, level, base_level
+        self.dim, self.order, self.top, self.base, self.nc = dim, order, level, base_level, ncomp
         if dirichlet_mask is None:
             dirichlet_mask = (1 << (2 * dim)) - 1
         self.h = lib().ora_create(dim, order, ncomp, n0, level, base_level, dirichlet_mask)
@@ -158,17 +158,17 @@ class Oracle:
 
     def matrix(self, level=None):
         level = self.top if level is None else level
-        out = np.zeros(self.nslots * self.nnodes(level))
+        out = np.zeros(self.nslots * self.nc * self.nc * self.nnodes(level))
         assert lib().ora_get_matrix(self.h, level, _p(out)) == 0
-        return out.reshape(self.nslots, -1)
+        return out.reshape(self.nslots * self.nc * self.nc, -1)
 
     def rhs(self):
-        out = np.zeros(self.nnodes())
+        out = np.zeros(self.nnodes() * self.nc)
         assert lib().ora_get_rhs(self.h, _p(out)) == 0
         return out
 
     def coarse_inverse(self):
-        n = self.nnodes(self.base)
+        n = self.nnodes(self.base) * self.nc
         out = np.zeros(n * n)
         assert lib().ora_get_coarse_inverse(self.h, _p(out)) == 0
         return out.reshape(n, n)
@@ -197,7 +197,7 @@ class Oracle:
 
     def restrict(self, rf, fine_level):
         rf = np.ascontiguousarray(rf, dtype=np.float64)
-        rc = np.zeros(self.nnodes(fine_level - 1))
+        rc = np.zeros(self.nnodes(fine_level - 1) * self.nc)
         lib().ora_restrict(self.h, fine_level, _p(rf), _p(rc))
         return rc
 
@@ -246,7 +246,7 @@ class Oracle:
         return x, b, r
 
     def solve(self, cfg: SolveCfg, x0=None) -> SolveResult:
-        n = self.nnodes()
+        n = self.nnodes() * self.nc
         x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
         hist = np.zeros(cfg.maxsteps + 2)
         steps = ctypes.c_int(0)
