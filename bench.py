@@ -47,9 +47,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--matvec-reps", type=int, default=20)
     ap.add_argument("--no-learned", action="store_true", help="mixed precision without the damping network")
-    ap.add_argument("--config", choices=["c2", "c3", "c4"], default="c3",
+    ap.add_argument("--config", choices=["c2", "c3", "c4", "c5"], default="c3",
                     help=("c2: plain FP64 Q2 SOR multigrid on 64^3 cells vs the oracle; c4: the learned "
-                          "smoother on 128^2 block fields, 256 held-out seeds; each its own JSON line"))
+                          "smoother on 128^2 block fields, 256 held-out seeds; c5: vector-Q2 elasticity on "
+                          "48^3 cells, FP64 CG + block-Jacobi V(2,2); each its own JSON line"))
+    ap.add_argument("--c5-level", type=int, default=4, help="c5: 3 x 2^level cells per direction")
     ap.add_argument("--c4-fields", type=int, default=256)
     ap.add_argument("--profile", choices=["solve", "net"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
@@ -630,6 +632,114 @@ def run_c2(args):
     print(json.dumps(line), flush=True)
 
 
+def run_c5(args):
+    """3D linear elasticity, vector Q2 with 3 x 3 nodal blocks on 48^3 cells
+    (2,738,019 DoF), lambda = mu = E log-normal (sigma 0.5), the x = 0 face
+    clamped, body force -z: CG preconditioned by the block-Jacobi V(2,2)
+    cycle, FP64 on the GPU, from x = 0 to 1e-10; the oracle (C++
+    restatement, all host threads) timed beside it on the same problem one
+    level down (24^3 cells), its per-step time scaled by the DoF ratio."""
+    import torch
+
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    from oracle import oracle as O
+    C = G._capi
+    wl = problems.c5(level=args.c5_level)
+    nd = wl.dofs
+    ctx = G.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def timed(fn, reps):
+        ctx.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        out = None
+        for _ in range(reps):
+            out = fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        ctx.synchronize()
+        return ev0.elapsed_time(ev1) / 1e3 / reps, out
+
+    g = G.Grid(ctx, 3, wl.order, wl.level, base_level=wl.base_level, n0=wl.n0, ncomp=3,
+               dirichlet_mask=wl.dirichlet_mask)
+    g.set_coefficient(C.FMG_LAMBDA_MU_CELL, wl.ecell)
+    g.set_coefficient(C.FMG_F_VEC, list(wl.force))
+    g.assemble()
+    t_asm, _ = timed(lambda: g.assemble(), 2)
+    cfg = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, wl.damp, wl.pre, wl.post, 1, 0, 1.0, wl.rtol, 0.0, 300,
+                     C.FMG_MULTIPLICATIVE)
+    x = g.vector()
+
+    def solve():
+        x.fill(0.0)
+        return g.solve(cfg, x)
+    for _ in range(max(args.warmup, 1)):
+        solve()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_solve, (hist, steps, status) = timed(solve, args.steps)
+    B = g.vector(values=g.rhs())
+    R, X = g.vector(), g.vector()
+    one = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_JACOBI, wl.damp, wl.pre, wl.post, 1, 0, 1.0, 0.0, 0.0, 1,
+                     C.FMG_MULTIPLICATIVE)
+    for _ in range(3):
+        g.vcycle(one, X, B, R)
+    t_cycle, _ = timed(lambda: g.vcycle(one, X, B, R), 5)
+    P = g.vector(values=np.random.default_rng(1).standard_normal(nd))
+    Y = g.vector()
+    for _ in range(3):
+        g.matvec(P, Y)
+    t_mv, _ = timed(lambda: g.matvec(P, Y), args.matvec_reps)
+    clk = clocks.stop()
+    if status != 0:
+        raise RuntimeError(f"C5 solve did not converge in {steps} steps")
+    nnz = 9 * ((8 if wl.order == 2 else 3) * wl.n_cells + 1) ** 3  # scalar nonzeros of the 3 x 3 blocks
+    alg_bytes = 8 * nnz + 16 * nd
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / t_mv / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        O.build()
+        sl = max(wl.level - 1, 1)
+        ws = problems.c5(level=sl)
+        o = O.Oracle(3, ws.order, sl, base_level=ws.base_level, ncomp=3, n0=ws.n0, dirichlet_mask=ws.dirichlet_mask)
+        o.set_coefficient(O.LAMBDA_MU_CELL, ws.ecell)
+        o.set_coefficient(O.F_VEC, list(ws.force))
+        t0 = time.perf_counter()
+        o.assemble()
+        t_asm_cpu = time.perf_counter() - t0
+        ocfg = O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.JACOBI, damp=ws.damp, pre=ws.pre, post=ws.post,
+                           compat=False, rtol=ws.rtol, maxsteps=2)
+        t0 = time.perf_counter()
+        r = o.solve(ocfg)
+        per_step = (time.perf_counter() - t0) / max(r.steps, 1) * (nd / ws.dofs)
+        t_cpu = per_step * steps
+        cpu = {"value": nd / t_cpu / 1e6, "unit": "MDoF/s to 1e-10 (DoF / time-to-solution)",
+               "cores": O.num_threads(), "kind": "port",
+               "sample": (f"oracle C++ restatement, {O.num_threads()} OpenMP threads, on the same problem at "
+                          f"{ws.n_cells}^3 cells ({ws.dofs} DoF): assembly {t_asm_cpu:.1f} s, {r.steps} CG steps; "
+                          f"per-step time x {nd / ws.dofs:.2f} (DoF ratio) x {steps} steps"),
+               "time_to_solution_est_s": t_cpu}
+    line = {"metric": "C5 time to 1e-10 (plain FP64 GPU, vector-Q2 elasticity, CG + block-Jacobi V(2,2))",
+            "value": nd / t_solve / 1e6, "unit": "MDoF/s to 1e-10 (DoF / time-to-solution)", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_solve * 1e3, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "dofs": nd, "nnz_scalar": nnz,
+                       "solver": f"CG + V({wl.pre},{wl.post}) 3x3 block Jacobi({wl.damp}), base level 0 dense LU",
+                       "l2": "inputs larger than L2 (8.2 GB level matrix)"},
+            "time_to_solution_s": t_solve, "cg_steps": int(steps), "assembly_s": t_asm,
+            "vcycle_ms": t_cycle * 1e3, "mdof_per_s_per_vcycle": nd / t_cycle / 1e6,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_spmv3<2> (top-level FP64 block matvec)", "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
+            "cpu_baseline": cpu, "clocks": clk,
+            "history_tail": [float(v) for v in hist[-3:]]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
@@ -643,6 +753,9 @@ def main():
         elif args.config == "c2":
             if rank == 0:
                 run_c2(args)
+        elif args.config == "c5":
+            if rank == 0:
+                run_c5(args)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

@@ -95,3 +95,44 @@ def c3(seed: int = 0, level: int = 8) -> Workload:
     n = 1 << level
     k = np.exp(fourier_log_field(n, 3, seed))
     return Workload(f"C3 3D Q1 {n}^3 variable-k diffusion", 3, 1, level, 2, k, 1.0, 0, 0.6, 1, 1)
+
+
+@dataclass
+class ElasticityWorkload:
+    name: str
+    order: int
+    n0: int
+    level: int
+    base_level: int
+    ecell: np.ndarray             # lambda = mu = E per top-level cell
+    force: tuple
+    dirichlet_mask: int           # bit 0: the x = 0 face clamped (all components)
+    damp: float
+    pre: int
+    post: int
+    rtol: float = 1e-10
+
+    @property
+    def n_cells(self) -> int:
+        return self.n0 << self.level
+
+    @property
+    def nodes(self) -> int:
+        return (self.order * self.n_cells + 1) ** 3
+
+    @property
+    def dofs(self) -> int:
+        return 3 * self.nodes
+
+
+def c5(seed: int = 0, level: int = 4) -> ElasticityWorkload:
+    """3D linear elasticity, vector Q2 on (3 * 2^level)^3 cells (48^3 at
+    level 4: 97^3 nodes, 2,738,019 DoF), lambda = mu = E = exp(0.5 g) per
+    cell with g the seeded 64-mode Fourier field of unit standard deviation
+    (log-normal, sigma 0.5), body force (0, 0, -1), the x = 0 face clamped;
+    CG + V(2,2) block Jacobi(0.6), base level 0 (3^3 cells, dense LU)."""
+    n = 3 << level
+    e = np.exp(0.5 * fourier_log_field(n, 3, seed))
+    return ElasticityWorkload(f"C5 3D vector-Q2 elasticity {n}^3 cells", 2, 3, level, 0, e, (0.0, 0.0, -1.0),
+                              0b000001, 0.6, 2, 2)
+
