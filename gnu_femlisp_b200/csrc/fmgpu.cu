@@ -770,9 +770,23 @@ int fmg_get_matrix(fmg_grid* g, int level, double* host) {
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   if (level < g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d out of range", level);
   const Lvl& L = g->lev[level];
+  const size_t rows = (size_t)g->nslots * g->nc * g->nc;
   FMG_CK(g->ctx, cudaMemcpy2DAsync(host, L.N * sizeof(double), L.A, L.Np * sizeof(double), L.N * sizeof(double),
-                                   (size_t)g->nslots * g->nc * g->nc, cudaMemcpyDeviceToHost, g->ctx->stream));
+                                   rows, cudaMemcpyDeviceToHost, g->ctx->stream));
   FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+  if (g->order == 2) {  // sliced storage -> one entry per node and slot, structural zeros included
+    std::vector<double> raw((size_t)L.N);
+    const int nblk = g->nc * g->nc;
+    for (size_t row = 0; row < rows; ++row) {
+      double* h = host + row * L.N;
+      std::copy(h, h + L.N, raw.begin());
+      const int s = (int)(row / nblk);
+      for (long long i = 0; i < L.N; ++i) {
+        const long long p = q2_slot_pos(g->dim, L.M, i, s, g->nc == 1);
+        h[i] = p >= 0 ? raw[(size_t)p] : 0.0;
+      }
+    }
+  }
   return FMG_OK;
 }
 
@@ -1131,7 +1145,8 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
   if (X.epoch != g->epoch) {  // convert the current assembly
     for (int l = g->base; l <= g->top; ++l) {
       const Lvl& L = g->lev[l];
-      mx_f64_to_f32(L.A, X.A32[l], (long long)g->nslots * L.Np, st);
+      if (g->order == 2) launch_level_to_f32(view(g, l), g->nslots, X.A32[l], st);  // sliced -> full slots
+      else mx_f64_to_f32(L.A, X.A32[l], (long long)g->nslots * L.Np, st);
     }
     if (g->kkind == FMG_K_CELL) {
       long long ncell = 1;
@@ -1695,8 +1710,8 @@ int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
   int rc = check_cfg(g, cf);
   if (rc) return rc;
   if (cf->smoother != FMG_JACOBI || cf->combination != FMG_MULTIPLICATIVE || cf->pre_steps != 1 ||
-      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base || g->nc != 1)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training loss: scalar Jacobi V(1,1) with at least two levels");
+      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base || g->nc != 1 || g->order != 1)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training loss: scalar Q1 Jacobi V(1,1) with at least two levels");
   return FMG_OK;
 }
 

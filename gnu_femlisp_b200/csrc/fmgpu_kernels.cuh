@@ -32,6 +32,13 @@ struct AsmArgs {
   int fvec_on = 0;
 };
 
+// FP32 copy of a Q2 level in the full slot layout (structural zeros
+// included) from its sliced storage, [slot][block entry][Np]
+void launch_level_to_f32(const LevelView& L, int nslots, float* out, cudaStream_t st);
+// host-side: the node's position in slot s of a Q2 level's sliced storage
+// (colour-major for scalar levels), or -1 when the slot is a structural zero
+// of that node
+long long q2_slot_pos(int dim, long long M, long long i, int s, bool colour_major);
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
                  const Reduce* R, cudaStream_t st);
 void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st);

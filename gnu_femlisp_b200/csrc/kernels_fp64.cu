@@ -37,12 +37,270 @@ __device__ __forceinline__ void node_coords(long long i, long long M, int dim, l
   c[2] = dim > 2 ? i / (M * M) : 0;
 }
 
+// node_coords in 32-bit arithmetic (levels of fewer than 2^31 nodes)
+__device__ __forceinline__ void node_coords32(long long i, long long M, int dim, long long c[3]) {
+  const unsigned u = (unsigned)i, m = (unsigned)M;
+  const unsigned q = u / m;
+  c[0] = u - q * m;
+  c[1] = dim > 1 ? q % m : 0;
+  c[2] = dim > 2 ? q / m : 0;
+}
+
 __device__ __forceinline__ bool node_dirichlet(const long long c[3], long long M, int dim, int dmask) {
   for (int k = 0; k < dim; ++k) {
     if (c[k] == 0 && ((dmask >> (2 * k)) & 1)) return true;
     if (c[k] == M - 1 && ((dmask >> (2 * k + 1)) & 1)) return true;
   }
   return false;
+}
+
+// --------------------------------------------------- Q2 sliced storage
+// A Q2 node couples at offset +-2 along direction k only when its coordinate k
+// is even (a cell vertex); an odd coordinate (an edge / face / cell midpoint)
+// couples within +-1.  Slot s of a Q2 level therefore stores only the nodes
+// that admit it: those even along every direction where |offset_k| = 2 (the
+// slot's pattern r, bit k).  They sit at the front of the slot's array, in
+// lexicographic order of the coordinates halved along the restricted
+// directions, so a level holds exactly its structural nonzeros (boundary and
+// Dirichlet zeros aside) and a Q2 sweep streams no structural zero.  Q1
+// levels and the centre slot (pattern 0) keep one entry per node.
+template <int D>
+__host__ __device__ __forceinline__ int q2_pattern(int s) {
+  int r = 0;
+  for (int k = 0; k < D; ++k) {
+    const int o = s % 5 - 2;
+    if (o == 2 || o == -2) r |= 1 << k;
+    s /= 5;
+  }
+  return r;
+}
+
+// a node's index in the slot arrays of every pattern, and which patterns it admits
+template <int D>
+struct Q2Rows {
+  long long idx[1 << D];
+  unsigned valid;  // bit r: the node is stored in pattern-r slots
+};
+
+template <int D>
+__host__ __device__ __forceinline__ void q2_rows(const long long c[3], long long M, Q2Rows<D>& q) {
+  const long long H = (M + 1) / 2;
+  q.valid = 0;
+  for (int r = 0; r < (1 << D); ++r) {
+    bool ok = true;
+    long long id = 0, mul = 1;
+    for (int k = 0; k < D; ++k) {
+      const bool rk = (r >> k) & 1;
+      if (rk && (c[k] & 1)) ok = false;
+      id += (rk ? c[k] / 2 : c[k]) * mul;
+      mul *= rk ? H : M;
+    }
+    q.idx[r] = id;
+    if (ok) q.valid |= 1u << r;
+  }
+}
+
+// Visits the stored slots of Q2 node c in ascending slot order (the order of
+// every row sum): f(slot, neighbour offset, position in the slot's array).
+// The z and y offsets are loops, the 5 x offsets unrolled; the row's index
+// in a slot array depends only on which directions the slot restricts.
+template <int D, typename F>
+__device__ __forceinline__ void q2_row(const long long c[3], long long M, F&& f) {
+  const long long H = (M + 1) / 2;
+  const bool ex = !(c[0] & 1), ey = D > 1 && !(c[1] & 1), ez = D > 2 && !(c[2] & 1);
+  for (int sz = 0; sz < (D > 2 ? 5 : 1); ++sz) {
+    const int oz = D > 2 ? sz - 2 : 0;
+    const bool rz = oz == 2 || oz == -2;
+    if (rz && !ez) continue;
+    for (int sy = 0; sy < (D > 1 ? 5 : 1); ++sy) {
+      const int oy = D > 1 ? sy - 2 : 0;
+      const bool ry = oy == 2 || oy == -2;
+      if (ry && !ey) continue;
+      const long long yz = (ry ? c[1] / 2 : c[1]) + (ry ? H : M) * (rz ? c[2] / 2 : c[2]);
+      const long long p0 = c[0] + M * yz, p1 = c[0] / 2 + H * yz;
+      const long long obase = (long long)oy * M + (long long)oz * M * M;
+#pragma unroll
+      for (int sx = 0; sx < 5; ++sx) {
+        const int ox = sx - 2;
+        const bool rx = ox == 2 || ox == -2;
+        if (rx && !ex) continue;
+        f(sx + 5 * (sy + 5 * sz), obase + ox, rx ? p1 : p0);
+      }
+    }
+  }
+}
+
+// Scalar Q2 levels go one step further: rows are grouped by colour class
+// (coordinates mod 3 -- the classes of the multicolour <sor>), classes in
+// ascending order, and inside a class a slot array holds the rows that admit
+// the slot in lexicographic order of their place in the class grid.  Along a
+// direction the class's coordinates are d, d+3, d+6, .. (d = coordinate mod 3),
+// or, where the slot restricts the direction to even coordinates, x0(d),
+// x0(d)+6, .. with x0 = 0, 4, 2 for d = 0, 1, 2.  A colour sweep then streams
+// one contiguous block of every slot array.  off[r][colour] is where the
+// class's block starts in the arrays of pattern-r slots.
+struct Q2Layout {
+  long long off[8][27];
+};
+
+__host__ __device__ __forceinline__ int q2c_x0(int d) { return d == 0 ? 0 : (d == 1 ? 4 : 2); }
+// rows of class digit d along one direction (M coordinates), restricted or not
+__host__ __device__ __forceinline__ long long q2c_ext(long long M, int d, bool r) {
+  if (!r) return (M - d + 2) / 3;
+  const int x0 = q2c_x0(d);
+  return x0 < M ? (M - x0 + 5) / 6 : 0;
+}
+// place of coordinate c (digit d = c mod 3) in its class grid along one direction
+__host__ __device__ __forceinline__ long long q2c_j(long long c, int d, bool r) {
+  return r ? (c - q2c_x0(d)) / 6 : (c - d) / 3;
+}
+
+Q2Layout q2_layout(int D, long long M) {
+  Q2Layout L{};
+  int ncol = 1;
+  for (int k = 0; k < D; ++k) ncol *= 3;
+  for (int r = 0; r < (1 << D); ++r) {
+    long long acc = 0;
+    for (int col = 0; col < ncol; ++col) {
+      L.off[r][col] = acc;
+      long long cnt = 1;
+      int t = col;
+      for (int k = 0; k < D; ++k) {
+        cnt *= q2c_ext(M, t % 3, (r >> k) & 1);
+        t /= 3;
+      }
+      acc += cnt;
+    }
+  }
+  return L;
+}
+
+// storage position of node c in the arrays of pattern-r slots (the node must
+// be even along the restricted directions)
+template <int D>
+__host__ __device__ __forceinline__ long long q2c_pos(const Q2Layout& L, const long long c[3], long long M, int r) {
+  int col = 0, m3 = 1;
+  long long p = 0, mul = 1;
+  for (int k = 0; k < D; ++k) {
+    const int d = (int)(c[k] % 3);
+    const bool rk = (r >> k) & 1;
+    col += d * m3;
+    m3 *= 3;
+    p += q2c_j(c[k], d, rk) * mul;
+    mul *= q2c_ext(M, d, rk);
+  }
+  return L.off[r][col] + p;
+}
+
+// q2_row for the colour-major layout of scalar Q2 levels
+template <int D, typename F>
+__device__ __forceinline__ void q2c_row(const Q2Layout& L, const long long c[3], long long M, F&& f) {
+  int col = 0, m3 = 1;
+  long long j[3][2] = {{0, 0}, {0, 0}, {0, 0}}, e[3][2] = {{1, 1}, {1, 1}, {1, 1}};
+  bool ev[3] = {false, false, false};
+  for (int k = 0; k < D; ++k) {
+    const int d = (int)(c[k] % 3);
+    col += d * m3;
+    m3 *= 3;
+    ev[k] = !(c[k] & 1);
+    for (int rk = 0; rk < 2; ++rk) {
+      j[k][rk] = q2c_j(c[k], d, rk);
+      e[k][rk] = q2c_ext(M, d, rk);
+    }
+  }
+  for (int sz = 0; sz < (D > 2 ? 5 : 1); ++sz) {
+    const int oz = D > 2 ? sz - 2 : 0;
+    const int rz = (oz == 2 || oz == -2) ? 1 : 0;
+    if (rz && !ev[2]) continue;
+    for (int sy = 0; sy < (D > 1 ? 5 : 1); ++sy) {
+      const int oy = D > 1 ? sy - 2 : 0;
+      const int ry = (oy == 2 || oy == -2) ? 1 : 0;
+      if (ry && !ev[1]) continue;
+      const long long yz = j[1][ry] + e[1][ry] * j[2][rz];
+      const long long b0 = L.off[(ry << 1) | (rz << 2)][col] + j[0][0] + e[0][0] * yz;
+      const long long b1 = L.off[1 | (ry << 1) | (rz << 2)][col] + j[0][1] + e[0][1] * yz;
+      const long long obase = (long long)oy * M + (long long)oz * M * M;
+#pragma unroll
+      for (int sx = 0; sx < 5; ++sx) {
+        const int ox = sx - 2;
+        const bool rx = ox == 2 || ox == -2;
+        if (rx && !ev[0]) continue;
+        f(sx + 5 * (sy + 5 * sz), obase + ox, rx ? b1 : b0);
+      }
+    }
+  }
+}
+
+// A node's position in the slot arrays of every pattern (32-bit: levels have
+// fewer than 2^31 nodes) and the patterns it admits, in the colour-major
+// layout of scalar Q2 levels (colour) or the natural sliced one (vector
+// levels); visited with every slot unrolled, so the pattern of a slot is a
+// compile-time constant and the loads can be issued ahead.
+template <int D>
+struct Q2Base {
+  int p[1 << D];
+  unsigned valid;
+};
+
+// CLAMP: keep every position in bounds (callers that load unstored slots too)
+template <int D, bool COLOUR, bool CLAMP = false>
+__device__ __forceinline__ void q2_base(const Q2Layout& lay, const long long c[3], long long M, Q2Base<D>& b) {
+  long long nmax_l = 1;
+  for (int k = 0; k < D; ++k) nmax_l *= M;
+  const int nmax = (int)nmax_l;
+  // per direction, unrestricted (0) and restricted (1): place and extent in
+  // 32-bit arithmetic with constant divisors
+  const int Mi = (int)M;
+  int j[3][2] = {{0, 0}, {0, 0}, {0, 0}}, e[3][2] = {{1, 1}, {1, 1}, {1, 1}};
+  int col = 0, m3 = 1;
+  unsigned odd = 0;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    const int ck = (int)c[k];
+    if (ck & 1) odd |= 1u << k;
+    if (COLOUR) {
+      const int d = ck % 3, x0 = q2c_x0(d);
+      col += d * m3;
+      m3 *= 3;
+      j[k][0] = (ck - d) / 3;
+      j[k][1] = (ck - x0) / 6;
+      e[k][0] = (Mi - d + 2) / 3;
+      e[k][1] = x0 < Mi ? (Mi - x0 + 5) / 6 : 0;
+    } else {
+      j[k][0] = ck;
+      j[k][1] = ck >> 1;
+      e[k][0] = Mi;
+      e[k][1] = (Mi + 1) >> 1;
+    }
+  }
+  b.valid = 0;
+#pragma unroll
+  for (int r = 0; r < (1 << D); ++r) {
+    if (!(r & odd)) b.valid |= 1u << r;
+    const int rx = r & 1, ry = (r >> 1) & 1, rz = (r >> 2) & 1;
+    const int p = j[0][rx] + e[0][rx] * (j[1][ry] + e[1][ry] * j[2][rz]);
+    const int q = COLOUR ? (int)lay.off[r][col] + p : p;
+    b.p[r] = (CLAMP && q >= nmax) ? nmax - 1 : q;
+  }
+}
+
+// Visits every slot (structural zeros too): f(slot, neighbour offset,
+// position, stored).  A position is in bounds even where the slot is not
+// stored for the node (the halved coordinate of an odd one), so callers load
+// unconditionally and use 0 where !stored -- the structural zero the full
+// layout would hold, in the same place of the row sum -- which lets the
+// loads be issued ahead.
+// ALL = false visits only the stored slots (the streaming kernels); ALL =
+// true every slot, for the latency-bound colour sweeps of the SOR.
+template <int D, bool ALL, typename F>
+__device__ __forceinline__ void q2_visit(const Q2Base<D>& b, long long M, F&& f) {
+  constexpr int NS = D == 1 ? 5 : (D == 2 ? 25 : 125);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int r = q2_pattern<D>(s);
+    const bool st = ((b.valid >> r) & 1) != 0;
+    if (ALL || st) f(s, slot_off<D, 2>(s, M), (long long)b.p[r], st);
+  }
 }
 
 // ----------------------------------------------------------------- matvec
@@ -85,6 +343,64 @@ k_spmv(const double* __restrict__ A, long long N, long long Np, long long M,
     }
   }
   if (DOT) dr_finish(acc, R, smem);
+}
+
+// y = A x or r = b - A x on a Q2 level in sliced storage, one row per thread
+// (the fused reduction of k_spmv runs as a separate DR4096 pass)
+template <int D, bool RES>
+__global__ void __launch_bounds__(kBlock)
+k_spmv_q2(const double* __restrict__ A, long long N, long long Np, long long M, const double* __restrict__ x,
+          const double* b, double* y, const __grid_constant__ Q2Layout lay) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  long long c[3];
+  node_coords32(i, M, D, c);
+  double acc = 0.0;
+  Q2Base<D> qb;
+  q2_base<D, true>(lay, c, M, qb);
+  q2_visit<D, false>(qb, M, [&](int s, long long o, long long p, bool) {
+    acc = fma(__ldg(A + (long long)s * Np + p), __ldg(x + clampi(i + o, N)), acc);
+  });
+  y[i] = RES ? b[i] - acc : acc;
+}
+
+// k_jacobi_res on a Q2 level in sliced storage, one row per thread
+template <int D>
+__global__ void __launch_bounds__(kBlock)
+k_jacobi_res_q2(const double* __restrict__ A, long long N, long long Np, long long M, double damp,
+                const double* __restrict__ omega, const double* __restrict__ x, const double* b,
+                double* __restrict__ xout, double* r, int write_r, const __grid_constant__ Q2Layout lay) {
+  constexpr int C = St<D, 2>::CENTER;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  long long c[3];
+  node_coords32(i, M, D, c);
+  double acc = 0.0, d = 1.0;
+  Q2Base<D> qb;
+  q2_base<D, true>(lay, c, M, qb);
+  q2_visit<D, false>(qb, M, [&](int s, long long o, long long p, bool) {
+    const double a = __ldg(A + (long long)s * Np + p);
+    if (s == C) d = a;
+    acc = fma(a, __ldg(x + clampi(i + o, N)), acc);
+  });
+  const double t = (b[i] - acc) / d;
+  if (write_r) r[i] = t;
+  xout[i] = fma(omega ? omega[i] : damp, t, x[i]);
+}
+
+// k_jacobi on a scalar Q2 level (the diagonal sits at the node's colour-major place)
+template <int D>
+__global__ void __launch_bounds__(kBlock)
+k_jacobi_q2(const double* __restrict__ A, long long N, long long Np, long long M, double damp,
+            const double* __restrict__ omega, double* x, double* r, int write_r, const __grid_constant__ Q2Layout lay) {
+  constexpr int C = St<D, 2>::CENTER;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  long long c[3];
+  node_coords32(i, M, D, c);
+  const double t = r[i] / A[(long long)C * Np + q2c_pos<D>(lay, c, M, 0)];
+  if (write_r) r[i] = t;
+  x[i] = fma(omega ? omega[i] : damp, t, x[i]);
 }
 
 // ------------------------------------------------------------- smoothers
@@ -151,7 +467,8 @@ k_jacobi_res(const double* __restrict__ A, long long N, long long Np, long long 
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
 k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long M, int colour,
-             double omega_s, const double* __restrict__ omega, double* x, const double* b, double* r) {
+             double omega_s, const double* __restrict__ omega, double* x, const double* b, double* r,
+             const __grid_constant__ Q2Layout lay) {
   constexpr int NS = St<D, P>::NS;
   constexpr int C = St<D, P>::CENTER;
   constexpr int Q = P + 1;
@@ -161,15 +478,29 @@ k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long 
   const long long nz = D > 2 ? (M - cz + Q - 1) / Q : 1;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nx * ny * nz) return;
-  const long long jx = t % nx, jy = (t / nx) % ny, jz = t / (nx * ny);
+  const unsigned tu = (unsigned)t, nxu = (unsigned)nx, nyu = (unsigned)ny;
+  const unsigned tq = tu / nxu;
+  const long long jx = tu - tq * nxu, jy = tq % nyu, jz = tq / nyu;
   const long long i = (cx + Q * jx) + M * ((D > 1 ? cy + Q * jy : 0) + M * (D > 2 ? cz + Q * jz : 0));
   double s = 0.0, d = 1.0;
+  if constexpr (P == 2) {  // colour-major sliced storage: the class's rows are contiguous
+    const long long c[3] = {cx + Q * jx, D > 1 ? cy + Q * jy : 0, D > 2 ? cz + Q * jz : 0};
+    Q2Base<D> qb;
+    q2_base<D, true, true>(lay, c, M, qb);
+    q2_visit<D, true>(qb, M, [&](int k, long long o, long long p, bool st) {
+      double a = A[(long long)k * Np + p];
+      a = st ? a : 0.0;
+      if (k == C) d = a;
+      s = fma(a, x[clampi(i + o, N)], s);
+    });
+  } else {
 #pragma unroll
-  for (int k = 0; k < NS; ++k) {
-    const long long o = slot_off<D, P>(k, M);
-    const double a = A[(long long)k * Np + i];
-    if (k == C) d = a;
-    s = fma(a, x[clampi(i + o, N)], s);
+    for (int k = 0; k < NS; ++k) {
+      const long long o = slot_off<D, P>(k, M);
+      const double a = A[(long long)k * Np + i];
+      if (k == C) d = a;
+      s = fma(a, x[clampi(i + o, N)], s);
+    }
   }
   const double tt = (b[i] - s) / d;
   r[i] = tt;
@@ -575,7 +906,7 @@ __global__ void k_sample_kq(long long ncells_l, long long n_l, long long n_top, 
 // right-hand side is gathered the same way.
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
-k_assemble(AsmArgs g) {
+k_assemble(AsmArgs g, const __grid_constant__ Q2Layout lay) {
   constexpr int NS = St<D, P>::NS;
   constexpr int C = St<D, P>::CENTER;
   constexpr int W = 2 * P + 1;
@@ -584,13 +915,25 @@ k_assemble(AsmArgs g) {
   if (i >= g.N) return;
   long long ci[3];
   node_coords(i, g.M, D, ci);
+  // the storage position of slot s of this node (-1: not stored, a structural zero)
+  auto pos = [&](int s) -> long long {
+    if (P != 2) return (long long)s * g.Np + i;
+    const int r = q2_pattern<D>(s);
+    for (int k = 0; k < D; ++k)
+      if (((r >> k) & 1) && (ci[k] & 1)) return -1;
+    return (long long)s * g.Np + q2c_pos<D>(lay, ci, g.M, r);
+  };
   if (node_dirichlet(ci, g.M, D, g.dmask)) {
-    for (int s = 0; s < NS; ++s) g.A[(long long)s * g.Np + i] = (s == C) ? 1.0 : 0.0;
+    for (int s = 0; s < NS; ++s) {
+      const long long p = pos(s);
+      if (p >= 0) g.A[p] = (s == C) ? 1.0 : 0.0;
+    }
     if (g.rhs) g.rhs[i] = 0.0;
     return;
   }
   const int nl = g.nl, nq = g.nq;
   for (int s = 0; s < NS; ++s) {
+    if (pos(s) < 0) continue;
     long long o[3] = {s % W - P, D > 1 ? (s / W) % W - P : 0, D > 2 ? (s / (W * W)) % W - P : 0};
     long long cj[3], lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     bool ok = true;
@@ -628,7 +971,7 @@ k_assemble(AsmArgs g) {
             v = v + e;
           }
     }
-    g.A[(long long)s * g.Np + i] = v;
+    g.A[pos(s)] = v;
   }
   if (g.rhs) {
     long long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -802,18 +1145,27 @@ __device__ __forceinline__ void row_sums3(const double* __restrict__ A, long lon
   constexpr int NS = St<3, P>::NS;
   constexpr int C = St<3, P>::CENTER;
   s[0] = s[1] = s[2] = 0.0;
-#pragma unroll 5
-  for (int sl = 0; sl < NS; ++sl) {
-    const long long j = clampi(i + slot_off<3, P>(sl, M), N);
+  auto blk = [&](int sl, long long o, long long p, bool) {
+    const long long j = clampi(i + o, N);
     const double xj[3] = {__ldg(x + 3 * j), __ldg(x + 3 * j + 1), __ldg(x + 3 * j + 2)};
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
-        const double a = __ldg(A + ((long long)(sl * 3 + k) * 3 + m) * Np + i);
+        const double a = __ldg(A + ((long long)(sl * 3 + k) * 3 + m) * Np + p);
         if (dblk && sl == C) dblk[k * 3 + m] = a;
         s[k] = fma(a, xj[m], s[k]);
       }
+  };
+  if constexpr (P == 2) {  // sliced storage
+    long long c[3];
+    node_coords32(i, M, 3, c);
+    Q2Base<3> qb;
+    q2_base<3, false>(Q2Layout{}, c, M, qb);
+    q2_visit<3, false>(qb, M, blk);
+  } else {
+#pragma unroll 3
+    for (int sl = 0; sl < NS; ++sl) blk(sl, slot_off<3, P>(sl, M), i, true);
   }
 }
 
@@ -955,14 +1307,26 @@ k_assemble3(AsmArgs g) {
   long long ci[3];
   node_coords(i, g.M, 3, ci);
   const int nl = g.nl, nq = g.nq;
+  Q2Rows<3> q2;
+  if (P == 2) q2_rows<3>(ci, g.M, q2);
+  auto pos = [&](int s) -> long long {  // the node's entry in slot s (-1: a structural zero, not stored)
+    if (P != 2) return i;
+    const int r = q2_pattern<3>(s);
+    return ((q2.valid >> r) & 1) ? q2.idx[r] : -1;
+  };
   if (node_dirichlet(ci, g.M, 3, g.dmask)) {
-    for (int s = 0; s < NS; ++s)
-      for (int e = 0; e < 9; ++e) g.A[((long long)s * 9 + e) * g.Np + i] = (s == C && e % 4 == 0) ? 1.0 : 0.0;
+    for (int s = 0; s < NS; ++s) {
+      const long long p = pos(s);
+      if (p < 0) continue;
+      for (int e = 0; e < 9; ++e) g.A[((long long)s * 9 + e) * g.Np + p] = (s == C && e % 4 == 0) ? 1.0 : 0.0;
+    }
     if (g.rhs)
       for (int k = 0; k < 3; ++k) g.rhs[3 * i + k] = 0.0;
     return;
   }
   for (int s = 0; s < NS; ++s) {
+    const long long ps = pos(s);
+    if (ps < 0) continue;
     const long long o[3] = {s % W - P, (s / W) % W - P, s / (W * W) - P};
     long long cj[3], lo[3], hi[3];
     bool ok = true;
@@ -1007,7 +1371,7 @@ k_assemble3(AsmArgs g) {
           }
     }
 #pragma unroll
-    for (int e = 0; e < 9; ++e) g.A[((long long)s * 9 + e) * g.Np + i] = v[e];
+    for (int e = 0; e < 9; ++e) g.A[((long long)s * 9 + e) * g.Np + ps] = v[e];
   }
   if (g.rhs) {
     long long lo[3], hi[3];
@@ -1055,8 +1419,35 @@ __global__ void k_densify3(const double* __restrict__ A, long long N, long long 
   }
   const long long j = cj[0] + M * (cj[1] + M * cj[2]);
   const long long n = 3 * N;
+  long long p = i;
+  if constexpr (P == 2) {  // sliced storage
+    Q2Rows<3> q;
+    q2_rows<3>(ci, M, q);
+    const int r = q2_pattern<3>(s);
+    if (!((q.valid >> r) & 1)) return;
+    p = q.idx[r];
+  }
   for (int k = 0; k < 3; ++k)
-    for (int m = 0; m < 3; ++m) Dm[(3 * i + k) * n + 3 * j + m] = A[((long long)s * 9 + k * 3 + m) * Np + i];
+    for (int m = 0; m < 3; ++m) Dm[(3 * i + k) * n + 3 * j + m] = A[((long long)s * 9 + k * 3 + m) * Np + p];
+}
+
+// The full slot layout of a level (structural zeros included) in FP32 -- the
+// layout the stored-level kernels of the mixed cycle read -- from a Q2
+// level's sliced storage; one thread per (slot, node)
+template <int D>
+__global__ void k_expand_q2_f32(const double* __restrict__ A, long long N, long long Np, long long M, int nslots,
+                                float* __restrict__ out, const __grid_constant__ Q2Layout lay) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nslots * N) return;
+  const int s = (int)(t / N);
+  const long long i = t - (long long)s * N;
+  long long c[3];
+  node_coords(i, M, D, c);
+  const int r = q2_pattern<D>(s);
+  bool ok = true;
+  for (int k = 0; k < D; ++k)
+    if (((r >> k) & 1) && (c[k] & 1)) ok = false;
+  out[(long long)s * Np + i] = ok ? (float)A[(long long)s * Np + q2c_pos<D>(lay, c, M, r)] : 0.f;
 }
 
 // ---------------------------------------------------------- dispatchers
@@ -1069,6 +1460,14 @@ __global__ void k_densify3(const double* __restrict__ A, long long N, long long 
     else if ((D_) == 2 && (P_) == 2) { constexpr int D = 2, P = 2; __VA_ARGS__; } \
     else { constexpr int D = 3, P = 2; __VA_ARGS__; }                         \
   } while (0)
+
+#define Q1_DISPATCH(D_, ...)                                              \
+  do {                                                                    \
+    if ((D_) == 1) { constexpr int D = 1; __VA_ARGS__; }                  \
+    else if ((D_) == 2) { constexpr int D = 2; __VA_ARGS__; }             \
+    else { constexpr int D = 3; __VA_ARGS__; }                            \
+  } while (0)
+#define Q2_DISPATCH Q1_DISPATCH
 
 static inline unsigned grid1(long long n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
 
@@ -1087,13 +1486,22 @@ void launch_spmv(const LevelView& L, const double* x, const double* b, double* y
     return;
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.order == 2) {  // sliced storage: one row per thread, the reduction as a separate DR4096 pass
+    const Q2Layout lay = q2_layout(L.dim, L.M);
+    Q2_DISPATCH(L.dim, {
+      if (b) k_spmv_q2<D, true><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, lay);
+      else k_spmv_q2<D, false><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, lay);
+    });
+    if (dv) launch_dot(y, dv, L.N, *R, st);
+    return;
+  }
   const unsigned g = nchunks(L.N);
   Reduce r0 = R ? *R : Reduce{};
-  FMG_DISPATCH(L.dim, L.order, {
-    if (b && dv) k_spmv<D, P, true, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
-    else if (b) k_spmv<D, P, true, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
-    else if (dv) k_spmv<D, P, false, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
-    else k_spmv<D, P, false, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+  Q1_DISPATCH(L.dim, {
+    if (b && dv) k_spmv<D, 1, true, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+    else if (b) k_spmv<D, 1, true, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+    else if (dv) k_spmv<D, 1, false, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
+    else k_spmv<D, 1, false, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
   });
 }
 
@@ -1101,6 +1509,13 @@ void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool w
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if (L.nc == 3) {
     k_jacobi3<<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.center, damp, L.omega, x, r, write_r ? 1 : 0);
+    return;
+  }
+  if (L.order == 2) {  // colour-major sliced storage
+    const Q2Layout lay = q2_layout(L.dim, L.M);
+    Q2_DISPATCH(L.dim, {
+      k_jacobi_q2<D><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, r, write_r ? 1 : 0, lay);
+    });
     return;
   }
   const double* Dg = L.A + (long long)L.center * L.Np;
@@ -1120,17 +1535,27 @@ void launch_jacobi_res(const LevelView& L, double damp, const double* x, const d
     if (dv) launch_dot(xout, dv, 3 * L.N, *R, st);
     return;
   }
+  if (L.order == 2) {  // sliced storage
+    const Q2Layout lay = q2_layout(L.dim, L.M);
+    Q2_DISPATCH(L.dim, {
+      k_jacobi_res_q2<D><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+                                                        write_r ? 1 : 0, lay);
+    });
+    if (dv) launch_dot(xout, dv, L.N, *R, st);
+    return;
+  }
   const unsigned g = nchunks(L.N);
   Reduce r0 = R ? *R : Reduce{};
-  FMG_DISPATCH(L.dim, L.order, {
-    if (dv) k_jacobi_res<D, P, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+  Q1_DISPATCH(L.dim, {
+    if (dv) k_jacobi_res<D, 1, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
                                                              write_r ? 1 : 0, dv, r0);
-    else k_jacobi_res<D, P, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
+    else k_jacobi_res<D, 1, false><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
                                                          write_r ? 1 : 0, dv, r0);
   });
 }
 
 void launch_sor(const LevelView& L, double omega, double* x, const double* b, double* r, cudaStream_t st) {
+  const Q2Layout lay = q2_layout(L.dim, L.M);
   int Q = L.order + 1, ncol = 1;
   for (int k = 0; k < L.dim; ++k) ncol *= Q;
   g_launches.fetch_add(ncol, std::memory_order_relaxed);
@@ -1140,7 +1565,7 @@ void launch_sor(const LevelView& L, double omega, double* x, const double* b, do
     if (L.dim > 1) cnt *= (L.M - cy + Q - 1) / Q;
     if (L.dim > 2) cnt *= (L.M - cz + Q - 1) / Q;
     FMG_DISPATCH(L.dim, L.order, {
-      k_sor_colour<D, P><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, L.omega, x, b, r);
+      k_sor_colour<D, P><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, L.omega, x, b, r, lay);
     });
   }
 }
@@ -1266,7 +1691,8 @@ void launch_assemble(int dim, int order, const AsmArgs& a, const double* kbar_h,
     else k_assemble_q1_3d<false><<<grid1(a.N), kBlock, 0, st>>>(a, tab);
     return;
   }
-  FMG_DISPATCH(dim, order, { k_assemble<D, P><<<grid1(a.N), kBlock, 0, st>>>(a); });
+  const Q2Layout lay = q2_layout(dim, a.M);
+  FMG_DISPATCH(dim, order, { k_assemble<D, P><<<grid1(a.N), kBlock, 0, st>>>(a, lay); });
 }
 
 }  // namespace fmg
@@ -1276,7 +1702,7 @@ namespace fmg {
 // dense row-major copy of a (small) level matrix, for the coarse LU
 template <int D, int P>
 __global__ void k_densify(const double* __restrict__ A, long long N, long long Np, long long M,
-                          double* __restrict__ Dm) {
+                          double* __restrict__ Dm, const __grid_constant__ Q2Layout lay) {
   constexpr int NS = St<D, P>::NS;
   constexpr int W = 2 * P + 1;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1290,7 +1716,56 @@ __global__ void k_densify(const double* __restrict__ A, long long N, long long N
   for (int k = 0; k < 3; ++k) cj[k] = ci[k] + o[k];
   for (int k = 0; k < D; ++k) if (cj[k] < 0 || cj[k] >= M) return;
   const long long j = cj[0] + M * (cj[1] + M * cj[2]);
-  Dm[i * N + j] = A[(long long)s * Np + i];
+  long long p = i;
+  if constexpr (P == 2) {  // colour-major sliced storage
+    const int r = q2_pattern<D>(s);
+    for (int k = 0; k < D; ++k)
+      if (((r >> k) & 1) && (ci[k] & 1)) return;
+    p = q2c_pos<D>(lay, ci, M, r);
+  }
+  Dm[i * N + j] = A[(long long)s * Np + p];
+}
+
+void launch_level_to_f32(const LevelView& L, int nslots, float* out, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const long long n = (long long)nslots * L.N;
+  const Q2Layout lay = q2_layout(L.dim, L.M);
+  Q1_DISPATCH(L.dim, { k_expand_q2_f32<D><<<grid1(n), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, nslots, out, lay); });
+}
+
+long long q2_slot_pos(int dim, long long M, long long i, int s, bool colour_major) {
+  const long long c[3] = {i % M, dim > 1 ? (i / M) % M : 0, dim > 2 ? i / (M * M) : 0};
+  if (colour_major) {
+    const Q2Layout lay = q2_layout(dim, M);
+    int r = 0, t = s;
+    for (int k = 0; k < dim; ++k) {
+      const int o = t % 5 - 2;
+      if (o == 2 || o == -2) {
+        if (c[k] & 1) return -1;
+        r |= 1 << k;
+      }
+      t /= 5;
+    }
+    if (dim == 3) return q2c_pos<3>(lay, c, M, r);
+    if (dim == 2) return q2c_pos<2>(lay, c, M, r);
+    return q2c_pos<1>(lay, c, M, r);
+  }
+  if (dim == 3) {
+    Q2Rows<3> q;
+    q2_rows<3>(c, M, q);
+    const int r = q2_pattern<3>(s);
+    return ((q.valid >> r) & 1) ? q.idx[r] : -1;
+  }
+  if (dim == 2) {
+    Q2Rows<2> q;
+    q2_rows<2>(c, M, q);
+    const int r = q2_pattern<2>(s);
+    return ((q.valid >> r) & 1) ? q.idx[r] : -1;
+  }
+  Q2Rows<1> q;
+  q2_rows<1>(c, M, q);
+  const int r = q2_pattern<1>(s);
+  return ((q.valid >> r) & 1) ? q.idx[r] : -1;
 }
 
 void launch_densify(const LevelView& L, double* Dm, cudaStream_t st) {
@@ -1300,9 +1775,10 @@ void launch_densify(const LevelView& L, double* Dm, cudaStream_t st) {
     else k_densify3<1><<<grid1(L.N * St<3, 1>::NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);
     return;
   }
+  const Q2Layout lay = q2_layout(L.dim, L.M);
   FMG_DISPATCH(L.dim, L.order, {
     constexpr int NS = St<D, P>::NS;
-    k_densify<D, P><<<grid1(L.N * NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);
+    k_densify<D, P><<<grid1(L.N * NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm, lay);
   });
 }
 
