@@ -80,6 +80,7 @@ struct fmg_grid {
   bool assembled_once = false;
   long long epoch = 0;         // incremented by every assembly
   struct MixedState* mx = nullptr;
+  struct MixedVec* mxv = nullptr;  // mixed solve state of the vector (elasticity) form
   double* kq = nullptr;        // Gauss-point coefficient samples of a coarse level
   double *lu = nullptr, *lux = nullptr;  // coarse LU factors and inverse workspace
   int* piv = nullptr;
@@ -582,6 +583,7 @@ static void grid_release(fmg_grid* g) {
   if (g->mx)
     for (auto& e : g->mx->graphs) cudaGraphExecDestroy(e.exec);
   delete g->mx;
+  delete g->mxv;
   delete g;
   c->grids -= 1;
   if (c->closed && c->grids == 0) ctx_release(c);
@@ -1343,17 +1345,167 @@ int run_step_graph(fmg_grid* g, const fmg_solve_cfg& c, const double* x, Body bo
 // When the recursive residual meets the tolerance the true residual is
 // recomputed with the assembled FP64 matrix and reported; if it does not meet
 // the tolerance, CG restarts from it.
+// ------------------------------------------------ mixed solve, vector form
+// FP64 flexible CG (FCG(1): rho = (z, r), beta = -(z, a)/(p, a) of the last
+// step, p = z + beta p, lam = rho / (a, p)) with FP64 x, r, p and a = A p on
+// the assembled FP64 blocks; its preconditioner is one V(pre, post) cycle in
+// FP32 -- 3 x 3 block Jacobi on FP32 copies of the level matrices, FP32
+// transfers -- with the base level's dense solve in FP64.  The residual is
+// handed to the cycle scaled to unit norm and its result scaled back.  At
+// convergence of the recursive residual the true FP64 residual is checked,
+// and CG restarts from it if it has not converged.
+struct MixedVec {
+  long long epoch = -1;
+  std::vector<float*> A32, x, xs, b, r;  // per level
+  double *b64 = nullptr, *x64 = nullptr;  // base level in FP64
+  double* z = nullptr;                    // preconditioned residual, FP64
+};
+
+static int mixed_vec_prepare(fmg_grid* g) {
+  if (!g->mxv) g->mxv = new MixedVec();
+  MixedVec& V = *g->mxv;
+  cudaStream_t st = g->ctx->stream;
+  int rc;
+  const int nl = g->top + 1;
+  if (V.A32.empty()) {
+    V.A32.assign(nl, nullptr); V.x.assign(nl, nullptr); V.xs.assign(nl, nullptr);
+    V.b.assign(nl, nullptr); V.r.assign(nl, nullptr);
+    for (int l = g->base; l <= g->top; ++l) {
+      const Lvl& L = g->lev[l];
+      const long long nv = 3 * L.Np;
+      if ((rc = mx_alloc_f(g, &V.A32[l], (long long)g->nslots * 9 * L.Np)) || (rc = mx_alloc_f(g, &V.x[l], nv)) ||
+          (rc = mx_alloc_f(g, &V.xs[l], nv)) || (rc = mx_alloc_f(g, &V.b[l], nv)) || (rc = mx_alloc_f(g, &V.r[l], nv)))
+        return rc;
+    }
+    if ((rc = dalloc(g, &V.b64, g->nbase)) || (rc = dalloc(g, &V.x64, g->nbase)) ||
+        (rc = dalloc(g, &V.z, 3 * g->lev[g->top].Np)))
+      return rc;
+  }
+  if (V.epoch != g->epoch) {  // FP32 copies of the current assembly (same layout)
+    for (int l = g->base; l <= g->top; ++l) {
+      const Lvl& L = g->lev[l];
+      vec_f64_to_f32(L.A, V.A32[l], (long long)g->nslots * 9 * L.Np, st);
+    }
+    V.epoch = g->epoch;
+  }
+  return launched(g->ctx, "mixed prepare (vector form)");
+}
+
+// V.x[l] := V_l V.b[l] in FP32 from a zero guess (correction scheme)
+static void vcycle32_vec(fmg_grid* g, const fmg_solve_cfg& cf, int l, cudaStream_t st) {
+  MixedVec& V = *g->mxv;
+  const Lvl& L = g->lev[l];
+  const long long n = 3 * L.N;
+  if (l == g->base) {
+    vec_to64(V.b[l], nullptr, 0, 0, V.b64, n, st);
+    launch_fill(V.x64, n, 0.0, st);
+    launch_coarse_solve(g->ainvT, g->nbase, cf.coarse_damp, V.x64, V.b64, st);
+    vec_to32(V.x64, nullptr, 0, 0, V.x[l], n, st);
+    return;
+  }
+  float *x = V.x[l], *xs = V.xs[l];
+  if (cf.pre_steps > 0) {
+    vec32_jacobi0(V.A32[l], L.N, L.Np, g->center, (float)cf.damp, V.b[l], x, st);
+    for (int s = 1; s < cf.pre_steps; ++s) {
+      vec32_jacobi_res(g->order, V.A32[l], L.N, L.Np, L.M, cf.damp, x, V.b[l], xs, st);
+      std::swap(x, xs);
+    }
+  } else {
+    cudaMemsetAsync(x, 0, (size_t)n * sizeof(float), st);
+  }
+  vec32_spmv(g->order, V.A32[l], L.N, L.Np, L.M, x, V.b[l], V.r[l], st);  // r = b - A x
+  const Lvl& C = g->lev[l - 1];
+  vec32_restrict(g->order, C.M, L.M, g->dmask, V.r[l], V.b[l - 1], V.x[l - 1], st);
+  vcycle32_vec(g, cf, l - 1, st);
+  vec32_prolong(g->order, L.M, C.M, g->dmask, V.x[l - 1], x, st);
+  for (int s = 0; s < cf.post_steps; ++s) {
+    vec32_jacobi_res(g->order, V.A32[l], L.N, L.Np, L.M, cf.damp, x, V.b[l], xs, st);
+    std::swap(x, xs);
+  }
+  if (x != V.x[l]) cudaMemcpyAsync(V.x[l], x, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+}
+
+static int solve_mixed_vec(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* xv,
+                           double* hist, int hist_len, int* nouter, int* ninner, int* status) {
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const fmg_solve_cfg& cf = *cfg;
+  if (cf.method != FMG_METHOD_CG_MG)
+    return set_err(c, FMG_ERR_UNSUPPORTED, "mixed solve: CG preconditioned by the multigrid cycle");
+  int rc;
+  if ((rc = mixed_vec_prepare(g))) return rc;
+  MixedVec& V = *g->mxv;
+  const int top = g->top;
+  const LevelView T = view(g, top);
+  const long long n = 3 * T.N;
+  double *x = xv->d, *r = g->r, *p = g->p, *a = g->a, *z = V.z;
+  const double* b = g->rhs;
+  const int max_restart = mcfg->max_outer > 0 ? mcfg->max_outer : 20;
+  double initial = -1.0;
+  int step = 0, iters = 0;
+  *status = 1;
+  *nouter = 0;
+  *ninner = 0;
+  for (int restart = 0; restart <= max_restart; ++restart) {
+    launch_spmv(T, x, b, r, nullptr, nullptr, st);  // true FP64 residual
+    launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
+    if ((rc = read_scalars(g))) return rc;
+    const double dn = std::sqrt(c->host_scal[S_RR]);
+    if (!std::isfinite(dn)) return set_err(c, FMG_ERR_NUMERIC, "defnorm is %g", dn);
+    if (initial < 0) initial = dn;
+    if (hist && step < hist_len) hist[step] = dn;
+    *nouter = restart;
+    *ninner = iters;
+    if ((cf.rtol > 0 && (initial == 0.0 || dn / initial < cf.rtol)) || (cf.atol > 0 && dn < cf.atol)) {
+      *status = 0;
+      break;
+    }
+    if (restart == max_restart || iters > cf.maxsteps) break;
+    launch_fill(p, n, 0.0, st);
+    bool first = true, converged = false;
+    while (iters <= cf.maxsteps) {
+      vec_to32(r, g->scal, S_RR, 1, V.b[top], n, st);  // r / |r|
+      vcycle32_vec(g, cf, top, st);
+      vec_to64(V.x[top], g->scal, S_RR, 2, z, n, st);  // z = |r| V(r / |r|)
+      launch_dot(z, r, n, reducer(g, EPI_STORE, S_ALPHA), st);           // rho
+      if (!first) launch_dot(z, a, n, reducer(g, EPI_STORE, S_TMP), st);  // (z, a) of the last a
+      launch_fcg_beta(g->scal, first, st);
+      launch_p_update(g->scal, p, z, n, st);                             // p = beta p + z
+      const Reduce Rl = reducer(g, EPI_CG_LAMBDA, 0);
+      launch_spmv(T, p, nullptr, a, p, &Rl, st);                         // a = A p; (a, p); lam
+      const Reduce Rr = reducer(g, EPI_STORE, S_RR);
+      launch_cg_update(g->scal, x, p, r, a, nullptr, nullptr, nullptr, n, Rr, st);  // x, r; (r, r)
+      if ((rc = launched(c, "mixed step (vector form)"))) return rc;
+      if ((rc = read_scalars(g))) return rc;
+      first = false;
+      ++iters;
+      ++step;
+      const double rn = std::sqrt(c->host_scal[S_RR]);
+      if (!std::isfinite(rn)) return set_err(c, FMG_ERR_NUMERIC, "residual is %g at step %d", rn, step);
+      if (hist && step < hist_len) hist[step] = rn;
+      if ((cf.rtol > 0 && rn / initial < cf.rtol) || (cf.atol > 0 && rn < cf.atol)) { converged = true; break; }
+    }
+    if (!converged && iters > cf.maxsteps) {
+      *ninner = iters;
+      break;
+    }
+    ++step;  // the true-residual check takes one history slot
+  }
+  FMG_CK(c, cudaStreamSynchronize(st));
+  return launched(c, "solve_mixed (vector form)");
+}
+
 extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* xv,
                                double* hist, int hist_len, int* nouter, int* ninner, int* status) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (!mcfg || vec_check(xv, g, g->top) || !nouter || !ninner || !status) return FMG_ERR_ARG;
-  if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed solve: scalar grids only");
   if (cfg->smoother != FMG_JACOBI || cfg->combination != FMG_MULTIPLICATIVE || cfg->gamma != 1 ||
       g->base >= g->top || cfg->post_steps < 1)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
                    "mixed solve: Jacobi V(pre,post>=1) cycles with gamma 1 and at least two levels");
+  if (g->nc == 3) return solve_mixed_vec(g, cfg, mcfg, xv, hist, hist_len, nouter, ninner, status);
   fmg_ctx* c = g->ctx;
   cudaStream_t st = c->stream;
   if ((rc = mixed_prepare(g, mcfg->matrix_free != 0))) return rc;

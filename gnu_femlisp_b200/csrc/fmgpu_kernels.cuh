@@ -39,6 +39,25 @@ void launch_level_to_f32(const LevelView& L, int nslots, float* out, cudaStream_
 // (colour-major for scalar levels), or -1 when the slot is a structural zero
 // of that node
 long long q2_slot_pos(int dim, long long M, long long i, int s, bool colour_major);
+// FP32 mixed cycle of the vector form (3 x 3 blocks, FP32 copies of the level
+// matrices in the same layout): residual r = b - A x, first Jacobi step from a
+// zero guess, fused residual + Jacobi step, transfers (restriction writes the
+// coarse rhs and zeroes the coarse solution)
+void vec32_spmv(int order, const float* A, long long N, long long Np, long long M, const float* x, const float* b,
+                float* y, cudaStream_t st);
+void vec32_jacobi0(const float* A, long long N, long long Np, int center, float damp, const float* b, float* x,
+                   cudaStream_t st);
+void vec32_jacobi_res(int order, const float* A, long long N, long long Np, long long M, double damp,
+                      const float* x, const float* b, float* xout, cudaStream_t st);
+void vec32_restrict(int order, long long MC, long long MF, int dmask, const float* rf, float* bc, float* xc,
+                    cudaStream_t st);
+void vec32_prolong(int order, long long MF, long long MC, int dmask, const float* xc, float* xf, cudaStream_t st);
+// y = f x between precisions; mode 0: f = 1, 1: f = 1/sqrt(sc[slot]), 2: f = sqrt(sc[slot])
+void vec_to32(const double* x, const double* sc, int slot, int mode, float* y, long long n, cudaStream_t st);
+void vec_to64(const float* x, const double* sc, int slot, int mode, double* y, long long n, cudaStream_t st);
+void vec_f64_to_f32(const double* x, float* y, long long n, cudaStream_t st);
+// sc[S_RATIO] = first ? 0 : -sc[S_TMP] / sc[S_BETA] (FCG(1) beta)
+void launch_fcg_beta(double* sc, bool first, cudaStream_t st);
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
                  const Reduce* R, cudaStream_t st);
 void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st);

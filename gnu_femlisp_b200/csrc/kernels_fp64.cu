@@ -1097,8 +1097,9 @@ k_assemble_q1_3d(AsmArgs g, const __grid_constant__ Q1Tab tab) {
 // t := B^-1 r for one diagonal block: LU with partial pivoting (the first
 // largest |entry| of the column, LAPACK dgetrf semantics) and substitution
 // -- the gesv! of <jacobi> on a 3 x 3 block (linit.lisp:234)
-__device__ __forceinline__ void block_solve3(const double* B, const double* r, double* t) {
-  double M[3][3], b[3];
+template <typename T>
+__device__ __forceinline__ void block_solve3(const T* B, const T* r, T* t) {
+  T M[3][3], b[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     b[k] = r[k];
@@ -1108,7 +1109,7 @@ __device__ __forceinline__ void block_solve3(const double* B, const double* r, d
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     int pr = c;
-    double mx = fabs(M[c][c]);
+    T mx = fabs(M[c][c]);
 #pragma unroll
     for (int rr = c + 1; rr < 3; ++rr)
       if (fabs(M[rr][c]) > mx) { mx = fabs(M[rr][c]); pr = rr; }
@@ -1117,13 +1118,13 @@ __device__ __forceinline__ void block_solve3(const double* B, const double* r, d
       for (int rr = c + 1; rr < 3; ++rr)
         if (rr == pr) {
 #pragma unroll
-          for (int m = 0; m < 3; ++m) { const double tt = M[c][m]; M[c][m] = M[rr][m]; M[rr][m] = tt; }
-          const double tb = b[c]; b[c] = b[rr]; b[rr] = tb;
+          for (int m = 0; m < 3; ++m) { const T tt = M[c][m]; M[c][m] = M[rr][m]; M[rr][m] = tt; }
+          const T tb = b[c]; b[c] = b[rr]; b[rr] = tb;
         }
     }
 #pragma unroll
     for (int rr = c + 1; rr < 3; ++rr) {
-      const double f = M[rr][c] / M[c][c];
+      const T f = M[rr][c] / M[c][c];
 #pragma unroll
       for (int m = c + 1; m < 3; ++m) M[rr][m] = fma(-f, M[c][m], M[rr][m]);
       b[rr] = fma(-f, b[c], b[rr]);
@@ -1131,7 +1132,7 @@ __device__ __forceinline__ void block_solve3(const double* B, const double* r, d
   }
 #pragma unroll
   for (int c = 2; c >= 0; --c) {
-    double sacc = b[c];
+    T sacc = b[c];
 #pragma unroll
     for (int m = c + 1; m < 3; ++m) sacc = fma(-M[c][m], t[m], sacc);
     t[c] = sacc / M[c][c];
@@ -1139,20 +1140,20 @@ __device__ __forceinline__ void block_solve3(const double* B, const double* r, d
 }
 
 // the three block-row sums of node i: slots ascending, columns ascending
-template <int P>
-__device__ __forceinline__ void row_sums3(const double* __restrict__ A, long long N, long long Np, long long M,
-                                          const double* __restrict__ x, long long i, double* s, double* dblk) {
+template <int P, typename T>
+__device__ __forceinline__ void row_sums3(const T* __restrict__ A, long long N, long long Np, long long M,
+                                          const T* __restrict__ x, long long i, T* s, T* dblk) {
   constexpr int NS = St<3, P>::NS;
   constexpr int C = St<3, P>::CENTER;
-  s[0] = s[1] = s[2] = 0.0;
+  s[0] = s[1] = s[2] = T(0);
   auto blk = [&](int sl, long long o, long long p, bool) {
     const long long j = clampi(i + o, N);
-    const double xj[3] = {__ldg(x + 3 * j), __ldg(x + 3 * j + 1), __ldg(x + 3 * j + 2)};
+    const T xj[3] = {__ldg(x + 3 * j), __ldg(x + 3 * j + 1), __ldg(x + 3 * j + 2)};
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
-        const double a = __ldg(A + ((long long)(sl * 3 + k) * 3 + m) * Np + p);
+        const T a = __ldg(A + ((long long)(sl * 3 + k) * 3 + m) * Np + p);
         if (dblk && sl == C) dblk[k * 3 + m] = a;
         s[k] = fma(a, xj[m], s[k]);
       }
@@ -1170,14 +1171,14 @@ __device__ __forceinline__ void row_sums3(const double* __restrict__ A, long lon
 }
 
 // y = A x or r = b - A x (b may alias r)
-template <int P, bool RES>
+template <int P, bool RES, typename T = double>
 __global__ void __launch_bounds__(kBlock)
-k_spmv3(const double* __restrict__ A, long long N, long long Np, long long M, const double* __restrict__ x,
-        const double* b, double* y) {
+k_spmv3(const T* __restrict__ A, long long N, long long Np, long long M, const T* __restrict__ x,
+        const T* b, T* y) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  double s[3];
-  row_sums3<P>(A, N, Np, M, x, i, s, nullptr);
+  T s[3];
+  row_sums3<P, T>(A, N, Np, M, x, i, s, (T*)nullptr);
 #pragma unroll
   for (int k = 0; k < 3; ++k) y[3 * i + k] = RES ? b[3 * i + k] - s[k] : s[k];
 }
@@ -1192,7 +1193,7 @@ k_jacobi3(const double* __restrict__ A, long long N, long long Np, int center, d
 #pragma unroll
   for (int e = 0; e < 9; ++e) B[e] = A[((long long)center * 9 + e) * Np + i];
   const double rr[3] = {r[3 * i], r[3 * i + 1], r[3 * i + 2]};
-  block_solve3(B, rr, t);
+  block_solve3<double>(B, rr, t);
   const double w = omega ? omega[i] : damp;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -1203,18 +1204,18 @@ k_jacobi3(const double* __restrict__ A, long long N, long long Np, int center, d
 
 // compute-residual fused with the following block <jacobi> step:
 // r_i = b_i - (A x)_i, t = B^-1 r_i, xout_i = x_i + w t, r_i := t
-template <int P>
+template <int P, typename T = double>
 __global__ void __launch_bounds__(kBlock)
-k_jacobi_res3(const double* __restrict__ A, long long N, long long Np, long long M, double damp,
-              const double* __restrict__ omega, const double* __restrict__ x, const double* b,
-              double* __restrict__ xout, double* r, int write_r) {
+k_jacobi_res3(const T* __restrict__ A, long long N, long long Np, long long M, double damp,
+              const double* __restrict__ omega, const T* __restrict__ x, const T* b,
+              T* __restrict__ xout, T* r, int write_r) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  double s[3], B[9], t[3];
-  row_sums3<P>(A, N, Np, M, x, i, s, B);
-  const double rr[3] = {b[3 * i] - s[0], b[3 * i + 1] - s[1], b[3 * i + 2] - s[2]};
-  block_solve3(B, rr, t);
-  const double w = omega ? omega[i] : damp;
+  T s[3], B[9], t[3];
+  row_sums3<P, T>(A, N, Np, M, x, i, s, B);
+  const T rr[3] = {b[3 * i] - s[0], b[3 * i + 1] - s[1], b[3 * i + 2] - s[2]};
+  block_solve3<T>(B, rr, t);
+  const T w = omega ? (T)omega[i] : (T)damp;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     if (write_r) r[3 * i + k] = t[k];
@@ -1223,16 +1224,16 @@ k_jacobi_res3(const double* __restrict__ A, long long N, long long Np, long long
 }
 
 // rc := I^T rf per component (constrained), rhs_c := rc, sol_c := 0
-template <int P>
+template <int P, typename T = double>
 __global__ void __launch_bounds__(kBlock)
-k_restrict3(int MC, int MF, int dmask, const double* __restrict__ rf, double* __restrict__ rc,
-            double* __restrict__ rhsc, double* __restrict__ solc) {
+k_restrict3(int MC, int MF, int dmask, const T* __restrict__ rf, T* __restrict__ rc,
+            T* __restrict__ rhsc, T* __restrict__ solc) {
   const int cJ[3] = {(int)(blockIdx.x * 32 + threadIdx.x), (int)(blockIdx.y * 8 + threadIdx.y), (int)blockIdx.z};
   if (cJ[0] >= MC || cJ[1] >= MC) return;
   const long long J = cJ[0] + (long long)MC * (cJ[1] + (long long)MC * cJ[2]);
   bool dj = false;
   for (int k = 0; k < 3; ++k) dj = dj || face_dir(cJ[k], MC, k, dmask);
-  double acc[3] = {0.0, 0.0, 0.0};
+  T acc[3] = {T(0), T(0), T(0)};
   if (!dj) {
     long long off[3][5] = {{0}, {0}, {0}};
     double w[3][5] = {{1.0}, {1.0}, {1.0}};
@@ -1245,7 +1246,7 @@ k_restrict3(int MC, int MF, int dmask, const double* __restrict__ rf, double* __
           bool skip = false;
           for (int k = 0; k < 3; ++k) skip = skip || fi[k] < 0 || fi[k] >= MF || face_dir(fi[k], MF, k, dmask);
           if (skip) continue;
-          const double ww = w[0][xx] * w[1][y] * w[2][z];
+          const T ww = (T)(w[0][xx] * w[1][y] * w[2][z]);
           const long long f = fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2]);
 #pragma unroll
           for (int c = 0; c < 3; ++c) acc[c] = fma(ww, rf[3 * f + c], acc[c]);
@@ -1255,14 +1256,14 @@ k_restrict3(int MC, int MF, int dmask, const double* __restrict__ rf, double* __
   for (int c = 0; c < 3; ++c) {
     rc[3 * J + c] = acc[c];
     rhsc[3 * J + c] = acc[c];
-    solc[3 * J + c] = 0.0;
+    solc[3 * J + c] = T(0);
   }
 }
 
 // xf := xf + I xc per component (constrained)
-template <int P>
+template <int P, typename T = double>
 __global__ void __launch_bounds__(kBlock)
-k_prolong3(int MF, int MC, int dmask, const double* __restrict__ xc, double* __restrict__ xf) {
+k_prolong3(int MF, int MC, int dmask, const T* __restrict__ xc, T* __restrict__ xf) {
   const int fi[3] = {(int)(blockIdx.x * 32 + threadIdx.x), (int)(blockIdx.y * 8 + threadIdx.y), (int)blockIdx.z};
   if (fi[0] >= MF || fi[1] >= MF) return;
   for (int k = 0; k < 3; ++k)
@@ -1272,7 +1273,7 @@ k_prolong3(int MF, int MC, int dmask, const double* __restrict__ xc, double* __r
   double w[3][3] = {{1.0}, {1.0}, {1.0}};
   int cnt[3];
   for (int k = 0; k < 3; ++k) cnt[k] = prolong_1d<P>(fi[k], J[k], w[k]);
-  double acc[3] = {0.0, 0.0, 0.0};
+  T acc[3] = {T(0), T(0), T(0)};
   for (int z = 0; z < cnt[2]; ++z)
     for (int y = 0; y < cnt[1]; ++y)
       for (int xx = 0; xx < cnt[0]; ++xx) {
@@ -1280,7 +1281,7 @@ k_prolong3(int MF, int MC, int dmask, const double* __restrict__ xc, double* __r
         bool dj = false;
         for (int k = 0; k < 3; ++k) dj = dj || face_dir(cj[k], MC, k, dmask);
         if (dj) continue;
-        const double ww = w[0][xx] * w[1][y] * w[2][z];
+        const T ww = (T)(w[0][xx] * w[1][y] * w[2][z]);
         const long long j = cj[0] + (long long)MC * (cj[1] + (long long)MC * cj[2]);
 #pragma unroll
         for (int c = 0; c < 3; ++c) acc[c] = fma(ww, xc[3 * j + c], acc[c]);
@@ -1448,6 +1449,42 @@ __global__ void k_expand_q2_f32(const double* __restrict__ A, long long N, long 
   for (int k = 0; k < D; ++k)
     if (((r >> k) & 1) && (c[k] & 1)) ok = false;
   out[(long long)s * Np + i] = ok ? (float)A[(long long)s * Np + q2c_pos<D>(lay, c, M, r)] : 0.f;
+}
+
+// ---- FP32 forms for the mixed cycle of the vector form
+// first smoothing step from a zero guess: x = w B^-1 b
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+k_jacobi0_3(const T* __restrict__ A, long long N, long long Np, int center, float damp, const T* __restrict__ b,
+            T* __restrict__ x) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T B[9], t[3];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) B[e] = A[((long long)center * 9 + e) * Np + i];
+  const T bb[3] = {b[3 * i], b[3 * i + 1], b[3 * i + 2]};
+  block_solve3<T>(B, bb, t);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) x[3 * i + k] = (T)damp * t[k];
+}
+
+// y = f x with f from a grid scalar: mode 0: 1, mode 1: 1/sqrt(sc[slot]), mode 2: sqrt(sc[slot])
+template <typename TI, typename TO>
+__global__ void k_vscale(const TI* __restrict__ x, const double* __restrict__ sc, int slot, int mode,
+                         TO* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double f = 1.0;
+  if (mode) {
+    const double v = sc[slot];
+    f = v > 0.0 ? (mode == 1 ? 1.0 / sqrt(v) : sqrt(v)) : 1.0;
+  }
+  y[i] = (TO)((double)x[i] * f);
+}
+
+// the FCG(1) coefficient beta = -(z, a) / (p, a) of the previous step (0 on a restart)
+__global__ void k_fcg_beta(double* sc, int first) {
+  sc[S_RATIO] = first ? 0.0 : -sc[S_TMP] / sc[S_BETA];
 }
 
 // ---------------------------------------------------------- dispatchers
@@ -1731,6 +1768,55 @@ void launch_level_to_f32(const LevelView& L, int nslots, float* out, cudaStream_
   const long long n = (long long)nslots * L.N;
   const Q2Layout lay = q2_layout(L.dim, L.M);
   Q1_DISPATCH(L.dim, { k_expand_q2_f32<D><<<grid1(n), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, nslots, out, lay); });
+}
+
+void vec32_spmv(int order, const float* A, long long N, long long Np, long long M, const float* x, const float* b,
+                float* y, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (order == 2) k_spmv3<2, true, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, x, b, y);
+  else k_spmv3<1, true, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, x, b, y);
+}
+void vec32_jacobi0(const float* A, long long N, long long Np, int center, float damp, const float* b, float* x,
+                   cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_jacobi0_3<float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, center, damp, b, x);
+}
+void vec32_jacobi_res(int order, const float* A, long long N, long long Np, long long M, double damp,
+                      const float* x, const float* b, float* xout, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (order == 2)
+    k_jacobi_res3<2, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, damp, nullptr, x, b, xout, (float*)nullptr, 0);
+  else
+    k_jacobi_res3<1, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, damp, nullptr, x, b, xout, (float*)nullptr, 0);
+}
+void vec32_restrict(int order, long long MC, long long MF, int dmask, const float* rf, float* bc, float* xc,
+                    cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (order == 2)
+    k_restrict3<2, float><<<xfer_grid(MC, 3), dim3(32, 8), 0, st>>>((int)MC, (int)MF, dmask, rf, bc, bc, xc);
+  else
+    k_restrict3<1, float><<<xfer_grid(MC, 3), dim3(32, 8), 0, st>>>((int)MC, (int)MF, dmask, rf, bc, bc, xc);
+}
+void vec32_prolong(int order, long long MF, long long MC, int dmask, const float* xc, float* xf, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (order == 2) k_prolong3<2, float><<<xfer_grid(MF, 3), dim3(32, 8), 0, st>>>((int)MF, (int)MC, dmask, xc, xf);
+  else k_prolong3<1, float><<<xfer_grid(MF, 3), dim3(32, 8), 0, st>>>((int)MF, (int)MC, dmask, xc, xf);
+}
+void vec_to32(const double* x, const double* sc, int slot, int mode, float* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_vscale<double, float><<<grid1(n), kBlock, 0, st>>>(x, sc, slot, mode, y, n);
+}
+void vec_to64(const float* x, const double* sc, int slot, int mode, double* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_vscale<float, double><<<grid1(n), kBlock, 0, st>>>(x, sc, slot, mode, y, n);
+}
+void vec_f64_to_f32(const double* x, float* y, long long n, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_vscale<double, float><<<grid1(n), kBlock, 0, st>>>(x, nullptr, 0, 0, y, n);
+}
+void launch_fcg_beta(double* sc, bool first, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_fcg_beta<<<1, 1, 0, st>>>(sc, first ? 1 : 0);
 }
 
 long long q2_slot_pos(int dim, long long M, long long i, int s, bool colour_major) {

@@ -116,8 +116,29 @@ def test_unsupported_forms_fail_loudly(G, ctx):
     sor = G.SolveCfg(0, G._capi.FMG_SOR, 1.2, 2, 2, 1, 0, 1.0, 1e-10, 0.0, 10, 0)
     with pytest.raises(G.FmgError):
         g.solve(sor, g.vector())
-    jac = G.SolveCfg(1, G._capi.FMG_JACOBI, 0.5, 2, 2, 1, 0, 1.0, 1e-10, 0.0, 10, 0)
+    mg = G.SolveCfg(0, G._capi.FMG_JACOBI, 0.5, 2, 2, 1, 0, 1.0, 1e-10, 0.0, 10, 0)
     with pytest.raises(G.FmgError):
-        g.solve_mixed(jac, g.vector())
+        g.solve_mixed(mg, g.vector())  # the mixed form is CG + cycle
     with pytest.raises(G.FmgError):
         G.Grid(ctx, 2, 2, 1, ncomp=3)
+
+
+@pytest.mark.parametrize("order,level,n0", [(2, 1, 3), (2, 2, 3), (1, 2, 3)])
+def test_mixed_solve_matches_fp64(oracle_mod, G, ctx, order, level, n0):
+    # FP32 block-Jacobi V(2,2) cycle inside FP64 flexible CG: the same discrete
+    # solution as the FP64 path, in about as many CG steps
+    _, g = make_pair(oracle_mod, G, ctx, order, level, 0, n0, seed=6)
+    cfg = G.SolveCfg(1, G._capi.FMG_JACOBI, 0.6, 2, 2, 1, 0, 1.0, 1e-10, 0.0, 300, G._capi.FMG_MULTIPLICATIVE)
+    X = g.vector()
+    hist, steps, status = g.solve(cfg, X)
+    assert status == 0
+    XM = g.vector()
+    mh, nouter, ninner, mst = g.solve_mixed(cfg, XM)
+    assert mst == 0 and mh[-1] / mh[0] < 1e-10, (mh[-3:], nouter, ninner)
+    assert ninner <= steps + 3, (steps, ninner)
+    a, b = XM.get(), X.get()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-8
+    # the true residual of the mixed solution
+    B, R = g.vector(values=g.rhs()), g.vector()
+    g.residual(XM, B, R)
+    assert np.linalg.norm(R.get()) / np.linalg.norm(g.rhs()) < 1e-9
