@@ -16,6 +16,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "fmgpu.h")
 FMG_OK = 0
 FMG_K_CONST, FMG_K_CELL, FMG_F_CONST, FMG_F_IP, FMG_LAMBDA_MU_CELL, FMG_F_VEC = 0, 1, 2, 3, 4, 5
 FMG_JACOBI, FMG_SOR = 0, 1
+FMG_ASSEMBLE_REDISCRETIZE, FMG_ASSEMBLE_GALERKIN = 0, 1
 FMG_METHOD_MG, FMG_METHOD_CG_MG, FMG_METHOD_CG = 0, 1, 2
 FMG_MULTIPLICATIVE, FMG_ADDITIVE = 0, 1
 
@@ -99,6 +100,7 @@ SIGNATURES = {
     "fmg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "fmg_dot_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_long, _vp]),
+    "fmg_assemble_levels": (ctypes.c_int, [_vp, ctypes.c_int]),
     "fmg_solve_mixed": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), ctypes.POINTER(MixedCfg), _vp, _dp,
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),

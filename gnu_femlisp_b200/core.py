@@ -102,8 +102,11 @@ class Grid:
         self.ctx.check(self._lib.fmg_set_coefficient(self.h, kind, C.dptr(v), v.size), "set_coefficient")
         self.assembled = False
 
-    def assemble(self) -> "Grid":
-        self.ctx.check(self._lib.fmg_assemble(self.h), "assemble")
+    def assemble(self, galerkin: bool = False) -> "Grid":
+        """``fmg_assemble_levels``: coarse levels re-discretised, or Galerkin
+        products I^T A I of the level above (``galerkin=True``, Q1)."""
+        mode = C.FMG_ASSEMBLE_GALERKIN if galerkin else C.FMG_ASSEMBLE_REDISCRETIZE
+        self.ctx.check(self._lib.fmg_assemble_levels(self.h, mode), "assemble")
         self.assembled = True
         return self
 

@@ -710,9 +710,15 @@ static int ensure_buffers(fmg_grid* g) {
   return FMG_OK;
 }
 
-int fmg_assemble(fmg_grid* g) {
+int fmg_assemble(fmg_grid* g) { return fmg_assemble_levels(g, FMG_ASSEMBLE_REDISCRETIZE); }
+
+int fmg_assemble_levels(fmg_grid* g, int mode) {
   if (!g) return FMG_ERR_ARG;
   fmg_ctx* c = g->ctx;
+  if (mode != FMG_ASSEMBLE_REDISCRETIZE && mode != FMG_ASSEMBLE_GALERKIN)
+    return set_err(c, FMG_ERR_ARG, "unknown assembly mode %d", mode);
+  if (mode == FMG_ASSEMBLE_GALERKIN && (g->order != 1 || g->nc != 1))
+    return set_err(c, FMG_ERR_UNSUPPORTED, "Galerkin coarse operators: scalar Q1 grids");
   cudaStream_t st = c->stream;
   int rc;
   FMG_CK(c, cudaSetDevice(c->device));
@@ -721,6 +727,11 @@ int fmg_assemble(fmg_grid* g) {
   const long long n_top = g->lev[g->top].n;
   for (int l = g->top; l >= g->base; --l) {
     Lvl& L = g->lev[l];
+    if (mode == FMG_ASSEMBLE_GALERKIN && l < g->top) {  // I^T A_{l+1} I (geomg.lisp:122-123)
+      launch_galerkin(view(g, l + 1), view(g, l), L.A, st);
+      if ((rc = launched(c, "galerkin"))) return rc;
+      continue;
+    }
     long long ncells = 1;
     for (int k = 0; k < g->dim; ++k) ncells *= L.n;
     const bool sample = (l < g->top && g->kkind == FMG_K_CELL);

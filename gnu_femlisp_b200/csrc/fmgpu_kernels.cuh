@@ -58,6 +58,8 @@ void vec_to64(const float* x, const double* sc, int slot, int mode, double* y, l
 void vec_f64_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 // sc[S_RATIO] = first ? 0 : -sc[S_TMP] / sc[S_BETA] (FCG(1) beta)
 void launch_fcg_beta(double* sc, bool first, cudaStream_t st);
+// A_C := I^T A_F I for a scalar Q1 level below F (constrained interpolation)
+void launch_galerkin(const LevelView& F, const LevelView& Cl, double* AC, cudaStream_t st);
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
                  const Reduce* R, cudaStream_t st);
 void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st);

@@ -1451,6 +1451,80 @@ __global__ void k_expand_q2_f32(const double* __restrict__ A, long long N, long 
   out[(long long)s * Np + i] = ok ? (float)A[(long long)s * Np + q2c_pos<D>(lay, c, M, r)] : 0.f;
 }
 
+// Galerkin coarse operator A_C = I^T A_F I of a scalar Q1 level (constrained
+// interpolation: fine Dirichlet rows and coarse Dirichlet columns removed;
+// identity rows at coarse Dirichlet nodes), one coarse row per thread: fine i
+// over the restriction stencil of I (z, y, x), fine slots ascending, coarse J
+// over the interpolation stencil of j (z, y, x), acc[J - I] = fma(w_iI a_ij,
+// w_jJ, acc[J - I]) -- the oracle's order
+template <int D>
+__global__ void __launch_bounds__(kBlock)
+k_galerkin_q1(const double* __restrict__ AF, long long NF, long long NpF, int MF, double* __restrict__ AC,
+              long long NC, long long NpC, int MC, int dmask) {
+  constexpr int NS = St<D, 1>::NS;
+  constexpr int C = St<D, 1>::CENTER;
+  const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= NC) return;
+  long long cI[3];
+  node_coords(I, MC, D, cI);
+  if (node_dirichlet(cI, MC, D, dmask)) {
+    for (int s = 0; s < NS; ++s) AC[(long long)s * NpC + I] = (s == C) ? 1.0 : 0.0;
+    return;
+  }
+  double acc[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) acc[s] = 0.0;
+  long long off[3][5] = {{0}, {0}, {0}};
+  double w[3][5] = {{1.0}, {1.0}, {1.0}};
+  int cnt[3] = {1, 1, 1};
+  for (int k = 0; k < D; ++k) cnt[k] = restrict_1d<1>(cI[k], off[k], w[k]);
+  for (int z = 0; z < cnt[2]; ++z)
+    for (int y = 0; y < cnt[1]; ++y)
+      for (int x = 0; x < cnt[0]; ++x) {
+        const long long fi[3] = {2 * cI[0] + off[0][x], 2 * cI[1] + off[1][y], 2 * cI[2] + off[2][z]};
+        bool skip = false;
+        for (int k = 0; k < D; ++k) skip = skip || fi[k] < 0 || fi[k] >= MF || face_dir((int)fi[k], MF, k, dmask);
+        if (skip) continue;
+        double wi = w[0][x];
+        if (D > 1) wi = wi * w[1][y];
+        if (D > 2) wi = wi * w[2][z];
+        const long long i = fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2]);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const long long o[3] = {s % 3 - 1, D > 1 ? (s / 3) % 3 - 1 : 0, D > 2 ? s / 9 - 1 : 0};
+          const long long fj[3] = {fi[0] + o[0], fi[1] + o[1], fi[2] + o[2]};
+          bool sj = false;
+          for (int k = 0; k < D; ++k) sj = sj || fj[k] < 0 || fj[k] >= MF || face_dir((int)fj[k], MF, k, dmask);
+          if (sj) continue;
+          const double wa = wi * AF[(long long)s * NpF + i];
+          long long J[3][3] = {{0}, {0}, {0}};
+          double wj[3][3] = {{1.0}, {1.0}, {1.0}};
+          int cj[3] = {1, 1, 1};
+          for (int k = 0; k < D; ++k) cj[k] = prolong_1d<1>(fj[k], J[k], wj[k]);
+          for (int zz = 0; zz < cj[2]; ++zz)
+            for (int yy = 0; yy < cj[1]; ++yy)
+              for (int xx = 0; xx < cj[0]; ++xx) {
+                const long long cJ[3] = {J[0][xx], J[1][yy], J[2][zz]};
+                bool dj = false;
+                for (int k = 0; k < D; ++k) dj = dj || face_dir((int)cJ[k], MC, k, dmask);
+                if (dj) continue;
+                double ww = wj[0][xx];
+                if (D > 1) ww = ww * wj[1][yy];
+                if (D > 2) ww = ww * wj[2][zz];
+                int S = (int)(cJ[0] - cI[0] + 1);
+                if (D > 1) S += 3 * (int)(cJ[1] - cI[1] + 1);
+                if (D > 2) S += 9 * (int)(cJ[2] - cI[2] + 1);
+                // S is one of the level's slots (the terms couple nodes of one coarse cell)
+#pragma unroll
+                for (int t = 0; t < NS; ++t)
+                  if (t == S) acc[t] = fma(wa, ww, acc[t]);
+              }
+        }
+      }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) AC[(long long)s * NpC + I] = acc[s];
+}
+
 // ---- FP32 forms for the mixed cycle of the vector form
 // first smoothing step from a zero guess: x = w B^-1 b
 template <typename T>
@@ -1768,6 +1842,13 @@ void launch_level_to_f32(const LevelView& L, int nslots, float* out, cudaStream_
   const long long n = (long long)nslots * L.N;
   const Q2Layout lay = q2_layout(L.dim, L.M);
   Q1_DISPATCH(L.dim, { k_expand_q2_f32<D><<<grid1(n), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, nslots, out, lay); });
+}
+
+void launch_galerkin(const LevelView& F, const LevelView& Cl, double* AC, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  Q1_DISPATCH(F.dim, {
+    k_galerkin_q1<D><<<grid1(Cl.N), kBlock, 0, st>>>(F.A, F.N, F.Np, (int)F.M, AC, Cl.N, Cl.Np, (int)Cl.M, F.dmask);
+  });
 }
 
 void vec32_spmv(int order, const float* A, long long N, long long Np, long long M, const float* x, const float* b,

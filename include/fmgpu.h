@@ -127,6 +127,15 @@ int fmg_set_coefficient(fmg_grid* grid, int kind, const double* host, long n);
    + m+! P (constraints.lisp:323-411, fedisc.lisp:244-253, geomg.lisp:128-137),
    and getrf! of the <lu> coarse-grid iteration (linit.lisp:137-151). */
 int fmg_assemble(fmg_grid* grid);
+/* fmg_assemble with the coarse levels chosen like multilevel-decomposition
+   (geomg.lisp:109-142): FMG_ASSEMBLE_REDISCRETIZE assembles every level
+   (assemble-interior :refined); FMG_ASSEMBLE_GALERKIN assembles the top
+   level and forms each coarser one as the Galerkin product I^T A_{l+1} I with
+   the constrained interpolation (:galerkin-p t, geomg.lisp:122-123; scalar Q1
+   grids). */
+#define FMG_ASSEMBLE_REDISCRETIZE 0
+#define FMG_ASSEMBLE_GALERKIN 1
+int fmg_assemble_levels(fmg_grid* grid, int mode);
 /* Level matrix to the host, layout [slot][node] (debug / parity). */
 int fmg_get_matrix(fmg_grid* grid, int level, double* host);
 /* Top-level right-hand side (the assembled rhs of discretize-globally,

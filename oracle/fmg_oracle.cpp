@@ -762,6 +762,77 @@ void prolongate(const Hier& H, int lc, const double* xc, double* xf, bool constr
   }
 }
 
+// Galerkin coarse operator (multilevel-decomposition with :galerkin-p t,
+// geomg.lisp:109-142): A_l = I^T A_{l+1} I with the constrained
+// interpolation (constraints.lisp:58-72: rows of fine Dirichlet nodes and
+// columns of coarse Dirichlet nodes removed), identity rows at coarse
+// Dirichlet nodes.  For nested Lagrange spaces every nonzero term couples two
+// nodes of one coarse cell, so the product has the level's own stencil.
+// Order: fine i over the restriction stencil of I (z, y, x ascending), fine
+// slots ascending, coarse J over the interpolation stencil of j (z, y, x
+// ascending): acc[J - I] = fma(w_iI * a_ij, w_jJ, acc[J - I]).  Q1, nc = 1.
+int galerkin_level(Hier& H, int l) {
+  if (H.order != 1 || H.nc != 1) return -2;
+  Level& C = H.lev[l];
+  const Level& F = H.lev[l + 1];
+  C.A.assign((size_t)H.nslots * C.N, 0.0);
+  const int center = [&] { long z[3] = {0, 0, 0}; return slot_of(H, z); }();
+#pragma omp parallel for schedule(static)
+  for (long I = 0; I < C.N; ++I) {
+    long cI[3];
+    coords(H, C.M, I, cI);
+    if (is_dirichlet(H, C.M, cI)) {
+      C.A[(size_t)center * C.N + I] = 1.0;
+      continue;
+    }
+    double acc[27];
+    for (int s = 0; s < H.nslots; ++s) acc[s] = 0.0;
+    long off[3][5] = {{0}, {0}, {0}};
+    double w[3][5] = {{1.0}, {1.0}, {1.0}};
+    int cnt[3] = {1, 1, 1};
+    for (int k = 0; k < H.dim; ++k) cnt[k] = restrict_stencil1d(H.order, cI[k], off[k], w[k]);
+    for (int z = 0; z < cnt[2]; ++z)
+      for (int y = 0; y < cnt[1]; ++y)
+        for (int x = 0; x < cnt[0]; ++x) {
+          long fi[3] = {2 * cI[0] + off[0][x], 2 * cI[1] + off[1][y], 2 * cI[2] + off[2][z]};
+          bool in = true;
+          for (int k = 0; k < H.dim; ++k) if (fi[k] < 0 || fi[k] >= F.M) in = false;
+          if (!in || is_dirichlet(H, F.M, fi)) continue;
+          double wi = w[0][x];
+          if (H.dim > 1) wi = wi * w[1][y];
+          if (H.dim > 2) wi = wi * w[2][z];
+          const long i = fi[0] + F.M * (fi[1] + F.M * fi[2]);
+          for (int s = 0; s < H.nslots; ++s) {
+            long o[3];
+            slot_offset(H, s, o);
+            long fj[3] = {fi[0] + o[0], fi[1] + o[1], fi[2] + o[2]};
+            bool inj = true;
+            for (int k = 0; k < H.dim; ++k) if (fj[k] < 0 || fj[k] >= F.M) inj = false;
+            if (!inj || is_dirichlet(H, F.M, fj)) continue;
+            const double wa = wi * F.A[(size_t)s * F.N + i];
+            long J[3][3] = {{0}, {0}, {0}};
+            double wj[3][3] = {{1.0}, {1.0}, {1.0}};
+            int cj[3] = {1, 1, 1};
+            for (int k = 0; k < H.dim; ++k) cj[k] = prolong_stencil1d(H.order, fj[k], J[k], wj[k]);
+            for (int zz = 0; zz < cj[2]; ++zz)
+              for (int yy = 0; yy < cj[1]; ++yy)
+                for (int xx = 0; xx < cj[0]; ++xx) {
+                  long cJ[3] = {J[0][xx], J[1][yy], J[2][zz]};
+                  if (is_dirichlet(H, C.M, cJ)) continue;
+                  double ww = wj[0][xx];
+                  if (H.dim > 1) ww = ww * wj[1][yy];
+                  if (H.dim > 2) ww = ww * wj[2][zz];
+                  long d[3] = {cJ[0] - cI[0], cJ[1] - cI[1], cJ[2] - cI[2]};
+                  const int S = slot_of(H, d);
+                  acc[S] = std::fma(wa, ww, acc[S]);
+                }
+          }
+        }
+    for (int s = 0; s < H.nslots; ++s) C.A[(size_t)s * C.N + I] = acc[s];
+  }
+  return 0;
+}
+
 // <lu> coarse-grid iterator (linit.lisp:137-162): r := A^-1 r; x += damp r
 void coarse_solve(const Hier& H, double damp, double* x, double* r) {
   long n = H.nbase;
@@ -934,6 +1005,19 @@ int ora_set_coefficient(void* h, int kind, const double* vals, long n) {
     default: return -1;
   }
   H.assembled = false;
+  return 0;
+}
+
+int ora_assemble_levels(void* h, int mode) {
+  Hier& H = *(Hier*)h;
+  if (mode != 0 && mode != 1) return -1;
+  for (int l = H.top; l >= H.base; --l) {
+    int rc = (mode == 1 && l < H.top) ? galerkin_level(H, l) : assemble_level(H, l);
+    if (rc) return rc;
+  }
+  build_coarse_inverse(H);
+  H.assembled = true;
+  ensure_state(H);
   return 0;
 }
 

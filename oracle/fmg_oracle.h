@@ -72,6 +72,9 @@ void* ora_create(int dim, int order, int ncomp, int n0, int top_level, int base_
 void ora_destroy(void* h);
 int ora_set_coefficient(void* h, int kind, const double* vals, long n);
 int ora_assemble(void* h);
+/* mode 0: every level re-discretised (ora_assemble); 1: levels below the top
+   as Galerkin products I^T A_{l+1} I (geomg.lisp:122-123), Q1 scalar only */
+int ora_assemble_levels(void* h, int mode);
 int ora_set_node_damping(void* h, int level, const double* w, long n);
 
 long ora_nnodes(void* h, int level);

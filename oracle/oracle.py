@@ -60,6 +60,7 @@ def lib():
         L.ora_destroy.argtypes = [ctypes.c_void_p]
         L.ora_set_coefficient.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_long]
         L.ora_assemble.argtypes = [ctypes.c_void_p]
+        L.ora_assemble_levels.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ora_set_node_damping.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_long]
         L.ora_nnodes.restype = ctypes.c_long
         L.ora_nnodes.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -143,8 +144,8 @@ class Oracle:
         if rc:
             raise ValueError(f"ora_set_coefficient rc={rc}")
 
-    def assemble(self):
-        rc = lib().ora_assemble(self.h)
+    def assemble(self, galerkin=False):
+        rc = lib().ora_assemble_levels(self.h, 1 if galerkin else 0)
         if rc:
             raise RuntimeError(f"ora_assemble rc={rc}")
         return self

@@ -216,3 +216,28 @@ def test_exact_nodal_value_on_gpu(G, ctx):
     res = G.solve({"matrix": A, "rhs": b, "solver": G.LinearSolver(cs, "(< :reduction 1.0e-14)",
                                                                    "(> :step 3)")})
     assert res["solution"][2] == 0.125
+
+
+@pytest.mark.parametrize("dim,level,base,dmask", [(1, 5, 0, None), (2, 4, 1, None), (3, 3, 1, None),
+                                                  (3, 3, 0, 0b000001)])
+def test_galerkin_levels(oracle_mod, G, ctx, dim, level, base, dmask):
+    # multilevel-decomposition with :galerkin-p t: I^T A I from the top level down
+    O = oracle_mod
+    o = O.Oracle(dim, 1, level, base_level=base, dirichlet_mask=dmask)
+    g = G.Grid(ctx, dim, 1, level, base_level=base, dirichlet_mask=dmask)
+    k = np.exp(np.random.default_rng(dim).standard_normal((1 << level) ** dim))
+    o.set_coefficient(O.K_CELL, k)
+    g.set_coefficient(1, k)
+    o.assemble(galerkin=True)
+    g.assemble(galerkin=True)
+    for l in range(base, level + 1):
+        assert_same(g.matrix(l), o.matrix(l), f"A level {l}")
+    oc, gc = _cfg(O, G, 1, 0, 0.6, 1, 1, False, maxsteps=80)
+    ro = o.solve(oc)
+    X = g.vector()
+    hist, steps, status = g.solve(gc, X)
+    assert status == 0 and steps == ro.steps
+    assert_same(hist, ro.history, "defnorm history")
+    assert_same(X.get(), ro.x, "solution")
+    with pytest.raises(G.FmgError):
+        G.Grid(ctx, 2, 2, 2, base_level=0).assemble(galerkin=True)  # Q2: re-discretised only

@@ -123,3 +123,28 @@ def test_dot_chunked_equals_parallel(oracle_mod):
         d = O.dot(x, y)
         assert d == O.dot_par(x, y)
         assert abs(d - float(np.dot(x, y))) <= 1e-12 * np.sqrt(n) * np.linalg.norm(x) * np.linalg.norm(y)
+
+
+def test_galerkin_rate_bound_3d(oracle_mod):
+    # (test-v-cycle-convergence 3 1 2 :galerkin-p t :cr-max 0.15): 3D Q1 on
+    # 4^3 cells, Galerkin coarse operators, base level 1, Gauss-Seidel
+    # (colour order), V(1,0), 20 steps of the multigrid iteration
+    O = oracle_mod
+    o = O.Oracle(3, 1, 2, base_level=1)
+    o.assemble(galerkin=True)
+    cfg = O.solve_cfg(method=O.METHOD_MG, smoother=O.SOR, damp=1.0, pre=1, post=0, compat=True, rtol=0.0,
+                      atol=1e-12, maxsteps=20)
+    r = o.solve(cfg)
+    assert r.convergence_rate < 0.15, r.convergence_rate
+
+
+def test_galerkin_equals_rediscretisation_for_constant_coefficients(oracle_mod):
+    # for nested spaces and exact quadrature I^T A_f I is the coarse stiffness
+    # matrix itself (the variational property), up to rounding
+    O = oracle_mod
+    for dim, level in ((1, 5), (2, 3), (3, 2)):
+        a = O.Oracle(dim, 1, level, base_level=0).assemble()
+        b = O.Oracle(dim, 1, level, base_level=0).assemble(galerkin=True)
+        for l in range(level):
+            A, B = a.matrix(l), b.matrix(l)
+            assert np.abs(A - B).max() <= 1e-12 * np.abs(A).max(), (dim, l)
