@@ -435,6 +435,7 @@ def run_mine(args, world, rank, local):
     ctx.close()
 
 
+WEIGHTS_ELASTIC = os.path.join(ROOT, "gnu_femlisp_b200", "weights", "damping3d_elastic.fmgnet")
 WEIGHTS2D = os.path.join(ROOT, "gnu_femlisp_b200", "weights", "damping2d.fmgnet")
 
 
@@ -686,7 +687,23 @@ def run_c5(args):
     clocks = ClockSampler(0)
     clocks.start()
     t_solve, (hist, steps, status) = timed(solve, args.steps)
+    t_mixed_plain, (_, _, ninner_plain, _) = timed(solve_mixed, args.steps)
+    # the learned per-node damping of the block Jacobi (every level), judged by
+    # the plain cycle with the mixed solve's CG probe
+    from gnu_femlisp_b200.learn import DampingNet
+    net = DampingNet.load(ctx, WEIGHTS_ELASTIC)
+    t0 = time.perf_counter()
+    net.apply(g)
+    ok, rp, rl = g.learned_judge_mixed(cfg)
+    ctx.synchronize()
+    t_setup = time.perf_counter() - t0
+    for _ in range(max(args.warmup, 1)):
+        solve_mixed()
     t_mixed, (mhist, nouter, ninner, mstatus) = timed(solve_mixed, args.steps)
+    learned_info = {"weights": os.path.relpath(WEIGHTS_ELASTIC, ROOT), "accepted": ok, "rho_plain": rp,
+                    "rho_learned": rl, "setup_s": t_setup, "status": g.learned_status(),
+                    "mixed_without_learned": {"time_to_solution_s": t_mixed_plain,
+                                              "inner_iterations": int(ninner_plain)}}
     x64, xmx = x.get(), xm.get()
     tight = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, wl.damp, wl.pre, wl.post, 1, 0, 1.0, 1e-13, 0.0, 400,
                        C.FMG_MULTIPLICATIVE)
@@ -737,18 +754,20 @@ def run_c5(args):
                           f"{ws.n_cells}^3 cells ({ws.dofs} DoF): assembly {t_asm_cpu:.1f} s, {r.steps} CG steps; "
                           f"per-step time x {nd / ws.dofs:.2f} (DoF ratio) x {steps} steps"),
                "time_to_solution_est_s": t_cpu}
-    line = {"metric": "C5 time to 1e-10 (vector-Q2 elasticity: FP32 block-Jacobi V(2,2) inside FP64 flexible CG)",
+    line = {"metric": ("C5 time to 1e-10 (vector-Q2 elasticity: FP32 block-Jacobi V(2,2) with learned per-node "
+                       "damping inside FP64 flexible CG)"),
             "value": nd / t_mixed / 1e6, "unit": "MDoF/s to 1e-10 (DoF / time-to-solution)", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": True,
             "dtype": "f64 outer residual/update + f32 V-cycle", "data": "synthetic",
             "config": {"workload": wl.name, "dofs": nd, "nnz_scalar": nnz,
-                       "solver": (f"FP64 flexible CG + FP32 V({wl.pre},{wl.post}) 3x3 block Jacobi({wl.damp}), "
-                                  "base level 0 FP64 dense LU"),
+                       "solver": (f"FP64 flexible CG + FP32 V({wl.pre},{wl.post}) 3x3 block Jacobi with per-node "
+                                  f"damping from the damping network (plain {wl.damp}), base level 0 FP64 dense LU"),
                        "l2": "inputs larger than L2 (8.2 GB level matrix)"},
             "time_to_solution_s": t_mixed, "inner_iterations": int(ninner), "outer_steps": int(nouter),
             "error_vs_fp64": {"mixed_vs_fp64_1e-13": err_mixed, "plain_vs_fp64_1e-13": err_plain},
             "plain_fp64": {"time_to_solution_s": t_solve, "cg_steps": int(steps),
                            "speedup_mixed_vs_plain": t_solve / t_mixed},
+            "learned": learned_info,
             "cg_steps": int(steps), "assembly_s": t_asm,
             "vcycle_ms": t_cycle * 1e3, "mdof_per_s_per_vcycle": nd / t_cycle / 1e6,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1416,9 +1416,9 @@ static void vcycle32_vec(fmg_grid* g, const fmg_solve_cfg& cf, int l, cudaStream
   }
   float *x = V.x[l], *xs = V.xs[l];
   if (cf.pre_steps > 0) {
-    vec32_jacobi0(V.A32[l], L.N, L.Np, g->center, (float)cf.damp, V.b[l], x, st);
+    vec32_jacobi0(V.A32[l], L.N, L.Np, g->center, (float)cf.damp, L.omega, V.b[l], x, st);
     for (int s = 1; s < cf.pre_steps; ++s) {
-      vec32_jacobi_res(g->order, V.A32[l], L.N, L.Np, L.M, cf.damp, x, V.b[l], xs, st);
+      vec32_jacobi_res(g->order, V.A32[l], L.N, L.Np, L.M, cf.damp, L.omega, x, V.b[l], xs, st);
       std::swap(x, xs);
     }
   } else {
@@ -1430,7 +1430,7 @@ static void vcycle32_vec(fmg_grid* g, const fmg_solve_cfg& cf, int l, cudaStream
   vcycle32_vec(g, cf, l - 1, st);
   vec32_prolong(g->order, L.M, C.M, g->dmask, V.x[l - 1], x, st);
   for (int s = 0; s < cf.post_steps; ++s) {
-    vec32_jacobi_res(g->order, V.A32[l], L.N, L.Np, L.M, cf.damp, x, V.b[l], xs, st);
+    vec32_jacobi_res(g->order, V.A32[l], L.N, L.Np, L.M, cf.damp, L.omega, x, V.b[l], xs, st);
     std::swap(x, xs);
   }
   if (x != V.x[l]) cudaMemcpyAsync(V.x[l], x, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st);
@@ -1457,6 +1457,11 @@ static int solve_mixed_vec(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixe
   *status = 1;
   *nouter = 0;
   *ninner = 0;
+  // learned damping, judged as it runs: only divergence (100x the restart's
+  // residual) drops it -- hidden for the rest of the solve, restored after --
+  // and CG restarts from the true residual with the plain cycle
+  bool judge_active = g->learned;
+  std::vector<double*> hidden;
   for (int restart = 0; restart <= max_restart; ++restart) {
     launch_spmv(T, x, b, r, nullptr, nullptr, st);  // true FP64 residual
     launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
@@ -1495,6 +1500,12 @@ static int solve_mixed_vec(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixe
       if (!std::isfinite(rn)) return set_err(c, FMG_ERR_NUMERIC, "residual is %g at step %d", rn, step);
       if (hist && step < hist_len) hist[step] = rn;
       if ((cf.rtol > 0 && rn / initial < cf.rtol) || (cf.atol > 0 && rn < cf.atol)) { converged = true; break; }
+      if (judge_active && rn > 100.0 * dn) {
+        for (Lvl& Lh : g->lev) { hidden.push_back(Lh.omega); Lh.omega = nullptr; }
+        judge_active = false;
+        g->reverts += 1;
+        break;
+      }
     }
     if (!converged && iters > cf.maxsteps) {
       *ninner = iters;
@@ -1503,6 +1514,8 @@ static int solve_mixed_vec(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixe
     ++step;  // the true-residual check takes one history slot
   }
   FMG_CK(c, cudaStreamSynchronize(st));
+  if (!hidden.empty())
+    for (size_t l = 0; l < g->lev.size(); ++l) g->lev[l].omega = hidden[l];
   return launched(c, "solve_mixed (vector form)");
 }
 
@@ -1676,8 +1689,8 @@ int net_grid_check(fmg_net* net, fmg_grid* g) {
   if (!net || !g) return FMG_ERR_ARG;
   if (g->ctx != net->ctx) return set_err(g->ctx, FMG_ERR_ARG, "net and grid belong to different contexts");
   if (g->dim != net->dim) return set_err(g->ctx, FMG_ERR_ARG, "net is %dD, grid %dD", net->dim, g->dim);
-  if (g->order != 1 || g->nc != 1)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "damping network: scalar Q1 levels only");
+  if (!((g->order == 1 && g->nc == 1) || (g->order == 2 && g->nc == 3 && g->dim == 3)))
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "damping network: scalar Q1 levels or 3D Q2 elasticity");
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   return FMG_OK;
 }
@@ -1701,7 +1714,7 @@ int net_level_forward(fmg_net* net, fmg_grid* g, int l, bool with_mean) {
     else launch_set_scalar(net->stat, std::log(g->kconst), st);
   }
   const ActGeom ag = act_geom(g->dim, (int)L.M, 1);
-  if ((rc = launch_features(net, ag, (int)L.n, T.n, std::ldexp(1.0, g->top - l), g->np, g->xi_d,
+  if ((rc = launch_features(net, ag, (int)L.n, g->order, T.n, std::ldexp(1.0, g->top - l), g->np, g->xi_d,
                             kc ? g->kcell_d : nullptr, g->kconst, net->stat, st)))
     return set_err(c, rc, "damping network: no memory");
   if ((rc = net_forward(net, ag, L.omega, st))) return set_err(c, rc, "damping network forward failed");
@@ -1719,7 +1732,7 @@ int learn_vectors(fmg_grid* g) {
   if (g->lt[0]) return FMG_OK;
   int rc;
   for (double*& v : g->lt)
-    if ((rc = dalloc(g, &v, g->lev[g->top].Np))) return rc;
+    if ((rc = dalloc(g, &v, g->lev[g->top].Np * g->nc))) return rc;
   return FMG_OK;
 }
 
@@ -1787,7 +1800,7 @@ int linv_vectors(fmg_grid* g) {
   int rc;
   for (int l = g->base; l <= g->top; ++l)
     for (int v = 0; v < LV_COUNT; ++v)
-      if ((rc = dalloc(g, &g->lvv[l][v], g->lev[l].Np))) return rc;
+      if ((rc = dalloc(g, &g->lvv[l][v], g->lev[l].Np * g->nc))) return rc;
   return FMG_OK;
 }
 
@@ -1799,49 +1812,71 @@ struct LinV {
   void fwd(int l, const double* f, double* x) {
     std::vector<double*>& V = g->lvv[l];
     const LevelView L = view(g, l);
-    const long long n = L.N;
+    const long long n = L.N, nv = L.N * g->nc;
+    const bool vec = g->nc == 3;  // D = the 3 x 3 diagonal blocks
     if (l == g->base) {
-      launch_copy(f, V[LV_T1], n, st);
-      launch_fill(x, n, 0.0, st);
+      launch_copy(f, V[LV_T1], nv, st);
+      launch_fill(x, nv, 0.0, st);
       launch_coarse_solve(g->ainvT, g->nbase, 1.0, x, V[LV_T1], st);
       return;
     }
     std::vector<double*>& C = g->lvv[l - 1];
     const LevelView Lc = view(g, l - 1);
-    launch_dinv(L.A, L.center, L.Np, f, V[LV_DF], n, st);          // D^-1 f
-    launch_wg_dinv(L.A, L.center, L.Np, w(l), f, V[LV_X], n, st);  // x1
+    if (vec) {
+      launch_bdiag3(L, 0, nullptr, f, V[LV_DF], st);  // D^-1 f
+      launch_bdiag3(L, 1, w(l), f, V[LV_X], st);      // x1
+    } else {
+      launch_dinv(L.A, L.center, L.Np, f, V[LV_DF], n, st);          // D^-1 f
+      launch_wg_dinv(L.A, L.center, L.Np, w(l), f, V[LV_X], n, st);  // x1
+    }
     launch_spmv(L, V[LV_X], f, V[LV_T1], nullptr, nullptr, st);    // r1 = f - A x1
     launch_restrict(L, Lc, V[LV_T1], C[LV_F], C[LV_T2], C[LV_X], st);
     fwd(l - 1, C[LV_F], C[LV_X]);
     launch_prolong(Lc, L, C[LV_X], V[LV_X], st);                    // x2 = x1 + P c
     launch_spmv(L, V[LV_X], f, V[LV_T1], nullptr, nullptr, st);    // r2 = f - A x2
-    launch_dinv(L.A, L.center, L.Np, V[LV_T1], V[LV_DR2], n, st);  // D^-1 r2
-    launch_xpwv(V[LV_X], w(l), V[LV_DR2], x, n, st);               // x3
+    if (vec) {
+      launch_bdiag3(L, 0, nullptr, V[LV_T1], V[LV_DR2], st);       // D^-1 r2
+      launch_xpwv3(V[LV_X], w(l), V[LV_DR2], x, n, st);            // x3
+    } else {
+      launch_dinv(L.A, L.center, L.Np, V[LV_T1], V[LV_DR2], n, st);  // D^-1 r2
+      launch_xpwv(V[LV_X], w(l), V[LV_DR2], x, n, st);               // x3
+    }
   }
   // given xbar = dL/dx3 (destroyed), fbar = dL/df; dL/dw added to LV_WBAR
   void bwd(int l, double* xbar, double* fbar) {
     std::vector<double*>& V = g->lvv[l];
     const LevelView L = view(g, l);
-    const long long n = L.N;
+    const long long n = L.N, nv = L.N * g->nc;
+    const bool vec = g->nc == 3;  // D symmetric 3 x 3 blocks: the adjoint uses the same solves
     if (l == g->base) {  // A symmetric: fbar = A^-1 xbar
-      launch_fill(fbar, n, 0.0, st);
+      launch_fill(fbar, nv, 0.0, st);
       launch_coarse_solve(g->ainvT, g->nbase, 1.0, fbar, xbar, st);
       return;
     }
     std::vector<double*>& C = g->lvv[l - 1];
     const LevelView Lc = view(g, l - 1);
-    launch_acc_prod(V[LV_WBAR], xbar, V[LV_DR2], n, st);                 // x3 = x2 + w D^-1 r2
-    launch_wg_dinv(L.A, L.center, L.Np, w(l), xbar, V[LV_T1], n, st);    // r2bar
-    launch_copy(V[LV_T1], fbar, n, st);                                  // r2 = f - A x2
+    if (vec) {
+      launch_acc_prod3(V[LV_WBAR], xbar, V[LV_DR2], n, st);
+      launch_bdiag3(L, 1, w(l), xbar, V[LV_T1], st);
+    } else {
+      launch_acc_prod(V[LV_WBAR], xbar, V[LV_DR2], n, st);                 // x3 = x2 + w D^-1 r2
+      launch_wg_dinv(L.A, L.center, L.Np, w(l), xbar, V[LV_T1], n, st);    // r2bar
+    }
+    launch_copy(V[LV_T1], fbar, nv, st);                                 // r2 = f - A x2
     launch_spmv(L, V[LV_T1], xbar, V[LV_T2], nullptr, nullptr, st);      // x2bar = xbar - A r2bar
     launch_restrict(L, Lc, V[LV_T2], C[LV_F], C[LV_T2], C[LV_X], st);    // cbar = R x2bar
     bwd(l - 1, C[LV_F], C[LV_X]);                                        // fcbar
-    launch_fill(V[LV_T1], n, 0.0, st);
+    launch_fill(V[LV_T1], nv, 0.0, st);
     launch_prolong(Lc, L, C[LV_X], V[LV_T1], st);                        // r1bar = P fcbar
-    launch_add(V[LV_T1], fbar, n, st);                                   // r1 = f - A x1
+    launch_add(V[LV_T1], fbar, nv, st);                                  // r1 = f - A x1
     launch_spmv(L, V[LV_T1], V[LV_T2], V[LV_T3], nullptr, nullptr, st);  // x1bar = x2bar - A r1bar
-    launch_acc_prod(V[LV_WBAR], V[LV_T3], V[LV_DF], n, st);              // x1 = w D^-1 f
-    launch_wg_dinv_acc(L.A, L.center, L.Np, w(l), V[LV_T3], fbar, n, st);
+    if (vec) {
+      launch_acc_prod3(V[LV_WBAR], V[LV_T3], V[LV_DF], n, st);
+      launch_bdiag3(L, 2, w(l), V[LV_T3], fbar, st);
+    } else {
+      launch_acc_prod(V[LV_WBAR], V[LV_T3], V[LV_DF], n, st);              // x1 = w D^-1 f
+      launch_wg_dinv_acc(L.A, L.center, L.Np, w(l), V[LV_T3], fbar, n, st);
+    }
   }
 };
 
@@ -1852,7 +1887,7 @@ void learn_loss_grad_levels(fmg_grid* g, const fmg_solve_cfg& cf, const double* 
   LinV lv{g, st};
   const int t = g->top;
   const LevelView T = view(g, t);
-  const long long n = T.N;
+  const long long n = T.N * g->nc;  // vector length
   std::vector<double*>& V = g->lvv[t];
   for (int l = g->base + 1; l <= t; ++l)
     if (!g->lev[l].omega) launch_fill(g->lvv[l][LV_W], g->lev[l].N, cf.damp, st);
@@ -1873,8 +1908,10 @@ int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
   int rc = check_cfg(g, cf);
   if (rc) return rc;
   if (cf->smoother != FMG_JACOBI || cf->combination != FMG_MULTIPLICATIVE || cf->pre_steps != 1 ||
-      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base || g->nc != 1 || g->order != 1)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training loss: scalar Q1 Jacobi V(1,1) with at least two levels");
+      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base ||
+      !((g->nc == 1 && g->order == 1) || (g->nc == 3 && g->order == 2 && g->dim == 3)))
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
+                   "training loss: Jacobi V(1,1), scalar Q1 or 3D Q2 elasticity, at least two levels");
   return FMG_OK;
 }
 
@@ -2010,6 +2047,8 @@ int fmg_learn_loss(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* e0, dou
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   int rc = learn_cfg_check(g, cfg);
   if (rc) return rc;
+  if (g->nc != 1)  // the top-level form; fmg_learn_loss_levels covers the vector form
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "fmg_learn_loss: scalar grids (use fmg_learn_loss_levels)");
   if (vec_check(e0, g, g->top)) return FMG_ERR_ARG;
   if ((rc = learn_vectors(g))) return rc;
   fmg_ctx* c = g->ctx;
@@ -2082,11 +2121,11 @@ int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsam
     launch_fill(g->lvv[l][LV_WBAR], g->lev[l].N, 0.0, st);
   }
   Lvl& T = g->lev[g->top];
-  const long long n = T.N;
+  const long long n = T.N * g->nc;
   double* e = g->xs;
   double* spare = g->w2;
   for (int s = 0; s < nsamples; ++s) {
-    launch_rand_fill(e, g->dim, T.M, g->dmask, seed * 1000003ull + (unsigned long long)s, st);
+    launch_rand_fill(e, g->dim, T.M, g->dmask, seed * 1000003ull + (unsigned long long)s, st, g->nc);
     if (max_cycles > 0) {  // power iterations of the current (learned) cycle: A e = 0
       MG mg{g, *cfg, false, st};
       launch_fill(g->q, n, 0.0, st);  // b = 0
@@ -2122,10 +2161,10 @@ int cycle_contraction(fmg_grid* g, const fmg_solve_cfg& cf, int k, unsigned long
   fmg_ctx* c = g->ctx;
   cudaStream_t st = c->stream;
   const Lvl& T = g->lev[g->top];
-  const long long n = T.N;
+  const long long n = T.N * g->nc;
   double* e = g->xs;
   double* spare = g->w2;
-  launch_rand_fill(e, g->dim, T.M, g->dmask, seed, st);
+  launch_rand_fill(e, g->dim, T.M, g->dmask, seed, st, g->nc);
   launch_fill(g->q, n, 0.0, st);
   MG mg{g, cf, false, st};
   for (int it = 0; it < k; ++it) {
@@ -2165,9 +2204,9 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   cudaStream_t st = ctx->stream;
   const Lvl& T = g->lev[g->top];
   const LevelView TV = view(g, g->top);
-  const long long n = T.N;
+  const long long n = T.N * g->nc;
   double *xs = g->lt[9], *b = g->lt[7], *e = g->lt[6], *u = g->lt[5];
-  launch_rand_fill(xs, g->dim, T.M, g->dmask, seed, st);
+  launch_rand_fill(xs, g->dim, T.M, g->dmask, seed, st, g->nc);
   launch_spmv(TV, xs, nullptr, b, nullptr, nullptr, st);
   launch_dot(xs, b, n, reducer(g, EPI_STORE, S_E0), st);
   fmg_solve_cfg c = cf;
@@ -2227,8 +2266,8 @@ int learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mc
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
-  if (cfg->smoother != FMG_JACOBI || g->top <= g->base || g->nc != 1)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: scalar Jacobi cycles with at least two levels");
+  if (cfg->smoother != FMG_JACOBI || g->top <= g->base)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: Jacobi cycles with at least two levels");
   const bool cg = cfg->method == FMG_METHOD_CG_MG;
   if (mc && !cg) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed judge: the CG+MG method only");
   bool any = false;

@@ -45,10 +45,15 @@ long long q2_slot_pos(int dim, long long M, long long i, int s, bool colour_majo
 // coarse rhs and zeroes the coarse solution)
 void vec32_spmv(int order, const float* A, long long N, long long Np, long long M, const float* x, const float* b,
                 float* y, cudaStream_t st);
-void vec32_jacobi0(const float* A, long long N, long long Np, int center, float damp, const float* b, float* x,
-                   cudaStream_t st);
+void vec32_jacobi0(const float* A, long long N, long long Np, int center, float damp, const double* omega,
+                   const float* b, float* x, cudaStream_t st);
 void vec32_jacobi_res(int order, const float* A, long long N, long long Np, long long M, double damp,
-                      const float* x, const float* b, float* xout, cudaStream_t st);
+                      const double* omega, const float* x, const float* b, float* xout, cudaStream_t st);
+// diagonal-block operations of the recorded cycle (vector form); mode 0:
+// y = B^-1 x, 1: y = w B^-1 x, 2: y += w B^-1 x (w per node)
+void launch_bdiag3(const LevelView& L, int mode, const double* w, const double* x, double* y, cudaStream_t st);
+void launch_xpwv3(const double* x, const double* w, const double* v, double* y, long long N, cudaStream_t st);
+void launch_acc_prod3(double* acc, const double* a, const double* b, long long N, cudaStream_t st);
 void vec32_restrict(int order, long long MC, long long MF, int dmask, const float* rf, float* bc, float* xc,
                     cudaStream_t st);
 void vec32_prolong(int order, long long MF, long long MC, int dmask, const float* xc, float* xf, cudaStream_t st);

@@ -89,8 +89,9 @@ void launch_logmean(const double* k, long long n, double* scratch, double* out, 
 // per direction of each level cell (ratio = n_top / n_l); kconst used when
 // kcell is null
 // (written to net->X0; the level's cell log-coefficients go to net->lk first)
-int launch_features(fmg_net* net, const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
-                    const double* kcell, double kconst, const double* mean, cudaStream_t st);
+// sub = 2 for Q2 node grids: a node's 2^D adjacent half-cells, each in a cell
+int launch_features(fmg_net* net, const ActGeom& g, int n_l, int sub, long long n_top, double ratio, int np,
+                    const double* xi, const double* kcell, double kconst, const double* mean, cudaStream_t st);
 // the three forward convolutions; omega (level order, FP64) written when non-null
 int net_forward(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st);
 // backward from dL/domega (level order) through the net of the last forward
@@ -100,7 +101,8 @@ void launch_adam(fmg_net* net, float lr, float b1, float b2, float eps, cudaStre
 int net_check_error(fmg_net* net, cudaStream_t st, const char** msg);
 
 // FP64 helpers of the training loss (level vectors of length n)
-void launch_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed, cudaStream_t st);
+// nc values per node (vector form), nodes on the Dirichlet faces zero
+void launch_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed, cudaStream_t st, int nc = 1);
 // v = u / diag(A)   (diag: slot `center` of the stencil storage)
 void launch_dinv(const double* A, int center, long long Np, const double* u, double* v, long long n, cudaStream_t st);
 // y = x - w .* v

@@ -1525,12 +1525,53 @@ k_galerkin_q1(const double* __restrict__ AF, long long NF, long long NpF, int MF
   for (int s = 0; s < NS; ++s) AC[(long long)s * NpC + I] = acc[s];
 }
 
+// ---- diagonal-block operations of the recorded cycle (vector form)
+// mode 0: y_i = B_i^-1 x_i; 1: y_i = w_i B_i^-1 x_i; 2: y_i += w_i B_i^-1 x_i
+// (B_i the 3 x 3 diagonal block, symmetric, so the same solve serves the adjoint)
+__global__ void __launch_bounds__(kBlock)
+k_bdiag3(const double* __restrict__ A, long long N, long long Np, int center, int mode,
+         const double* __restrict__ w, const double* __restrict__ x, double* __restrict__ y) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double B[9], t[3];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) B[e] = A[((long long)center * 9 + e) * Np + i];
+  const double xx[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+  block_solve3<double>(B, xx, t);
+  const double wi = mode == 0 ? 1.0 : w[i];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double v = mode == 0 ? t[k] : wi * t[k];
+    y[3 * i + k] = mode == 2 ? y[3 * i + k] + v : v;
+  }
+}
+
+// y = x + w .* v with w per node (y may be x)
+__global__ void k_xpwv3(const double* x, const double* __restrict__ w, const double* __restrict__ v, double* y,
+                        long long N) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) y[3 * i + k] = x[3 * i + k] + w[i] * v[3 * i + k];
+}
+
+// acc_i += sum_k a_ik b_ik (per-node dot of two vectors)
+__global__ void k_acc_prod3(double* __restrict__ acc, const double* __restrict__ a, const double* __restrict__ b,
+                            long long N) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s = a[3 * i] * b[3 * i];
+  s = fma(a[3 * i + 1], b[3 * i + 1], s);
+  s = fma(a[3 * i + 2], b[3 * i + 2], s);
+  acc[i] += s;
+}
+
 // ---- FP32 forms for the mixed cycle of the vector form
 // first smoothing step from a zero guess: x = w B^-1 b
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-k_jacobi0_3(const T* __restrict__ A, long long N, long long Np, int center, float damp, const T* __restrict__ b,
-            T* __restrict__ x) {
+k_jacobi0_3(const T* __restrict__ A, long long N, long long Np, int center, float damp,
+            const double* __restrict__ omega, const T* __restrict__ b, T* __restrict__ x) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   T B[9], t[3];
@@ -1539,7 +1580,9 @@ k_jacobi0_3(const T* __restrict__ A, long long N, long long Np, int center, floa
   const T bb[3] = {b[3 * i], b[3 * i + 1], b[3 * i + 2]};
   block_solve3<T>(B, bb, t);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) x[3 * i + k] = (T)damp * t[k];
+  const T w = omega ? (T)omega[i] : (T)damp;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) x[3 * i + k] = w * t[k];
 }
 
 // y = f x with f from a grid scalar: mode 0: 1, mode 1: 1/sqrt(sc[slot]), mode 2: sqrt(sc[slot])
@@ -1851,24 +1894,37 @@ void launch_galerkin(const LevelView& F, const LevelView& Cl, double* AC, cudaSt
   });
 }
 
+void launch_bdiag3(const LevelView& L, int mode, const double* w, const double* x, double* y, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_bdiag3<<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.center, mode, w, x, y);
+}
+void launch_xpwv3(const double* x, const double* w, const double* v, double* y, long long N, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_xpwv3<<<grid1(N), kBlock, 0, st>>>(x, w, v, y, N);
+}
+void launch_acc_prod3(double* acc, const double* a, const double* b, long long N, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_acc_prod3<<<grid1(N), kBlock, 0, st>>>(acc, a, b, N);
+}
+
 void vec32_spmv(int order, const float* A, long long N, long long Np, long long M, const float* x, const float* b,
                 float* y, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if (order == 2) k_spmv3<2, true, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, x, b, y);
   else k_spmv3<1, true, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, x, b, y);
 }
-void vec32_jacobi0(const float* A, long long N, long long Np, int center, float damp, const float* b, float* x,
-                   cudaStream_t st) {
+void vec32_jacobi0(const float* A, long long N, long long Np, int center, float damp, const double* omega,
+                   const float* b, float* x, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_jacobi0_3<float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, center, damp, b, x);
+  k_jacobi0_3<float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, center, damp, omega, b, x);
 }
 void vec32_jacobi_res(int order, const float* A, long long N, long long Np, long long M, double damp,
-                      const float* x, const float* b, float* xout, cudaStream_t st) {
+                      const double* omega, const float* x, const float* b, float* xout, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if (order == 2)
-    k_jacobi_res3<2, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, damp, nullptr, x, b, xout, (float*)nullptr, 0);
+    k_jacobi_res3<2, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, damp, omega, x, b, xout, (float*)nullptr, 0);
   else
-    k_jacobi_res3<1, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, damp, nullptr, x, b, xout, (float*)nullptr, 0);
+    k_jacobi_res3<1, float><<<grid1(N), kBlock, 0, st>>>(A, N, Np, M, damp, omega, x, b, xout, (float*)nullptr, 0);
 }
 void vec32_restrict(int order, long long MC, long long MF, int dmask, const float* rf, float* bc, float* xc,
                     cudaStream_t st) {

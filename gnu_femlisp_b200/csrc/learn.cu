@@ -758,7 +758,7 @@ __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, cons
 // node features of one Q1 level from the level's cell log-coefficients lk
 // (null: the constant log kconst)
 template <int D>
-__global__ void k_features(TileGeo t, int n_l, const double* __restrict__ lkc, double kconst,
+__global__ void k_features(TileGeo t, int n_l, int sub, const double* __restrict__ lkc, double kconst,
                            const double* __restrict__ mean, bf16* __restrict__ X0) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)t.Mx * t.My * t.Mz) return;
@@ -774,9 +774,10 @@ __global__ void k_features(TileGeo t, int n_l, const double* __restrict__ lkc, d
   for (int c = 0; c < NC; ++c) {
     int cc[3] = {0, 0, 0};
     bool in = true;
-    for (int k = 0; k < D; ++k) {
-      cc[k] = node[k] - 1 + ((c >> k) & 1);
-      in = in && cc[k] >= 0 && cc[k] < n_l;
+    for (int k = 0; k < D; ++k) {  // adjacent cell (sub = 2: half-cell of a Q2 node, then its cell)
+      const int h = node[k] - 1 + ((c >> k) & 1);
+      in = in && h >= 0 && h < n_l * sub;
+      cc[k] = h / sub;
     }
     if (!in) continue;
     const double lk = lkc ? __ldg(lkc + cc[0] + (long long)n_l * (cc[1] + (long long)n_l * cc[2])) : log(kconst);
@@ -796,19 +797,20 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
   return z ^ (z >> 31);
 }
 
-__global__ void k_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed) {
+__global__ void k_rand_fill(double* e, int D, long long M, int dmask, int nc, unsigned long long seed) {
   long long N = M;
   for (int k = 1; k < D; ++k) N *= M;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // entry nc i + component
+  if (t >= N * nc) return;
+  const long long i = t / nc;
   const long long c[3] = {i % M, D > 1 ? (i / M) % M : 0, D > 2 ? i / (M * M) : 0};
   bool dir = false;
   for (int k = 0; k < D; ++k) {
     if (c[k] == 0 && ((dmask >> (2 * k)) & 1)) dir = true;
     if (c[k] == M - 1 && ((dmask >> (2 * k + 1)) & 1)) dir = true;
   }
-  const unsigned long long h = mix64(seed * 0x100000001B3ull ^ (unsigned long long)i);
-  e[i] = dir ? 0.0 : (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  const unsigned long long h = mix64(seed * 0x100000001B3ull ^ (unsigned long long)t);
+  e[t] = dir ? 0.0 : (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
 __global__ void k_dinv(const double* __restrict__ A, long long Np, const double* __restrict__ u, double* __restrict__ v,
@@ -1057,8 +1059,8 @@ void launch_logmean(const double* k, long long n, double* scratch, double* out, 
   k_logmean_final<<<1, kBlock, 0, st>>>(scratch, nb, n, out);
 }
 
-int launch_features(fmg_net* net, const ActGeom& g, int n_l, long long n_top, double ratio, int np, const double* xi,
-                    const double* kcell, double kconst, const double* mean, cudaStream_t st) {
+int launch_features(fmg_net* net, const ActGeom& g, int n_l, int sub, long long n_top, double ratio, int np,
+                    const double* xi, const double* kcell, double kconst, const double* mean, cudaStream_t st) {
   const TileGeo t = tile_geo(g);
   long long ncell = n_l;
   for (int k = 1; k < g.D; ++k) ncell *= n_l;
@@ -1075,10 +1077,10 @@ int launch_features(fmg_net* net, const ActGeom& g, int n_l, long long n_top, do
   g_launches.fetch_add(kcell ? 2 : 1, std::memory_order_relaxed);
   if (g.D == 3) {
     if (kcell) k_cell_logk<3><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, net->lk);
-    k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, lk, kconst, mean, net->X0);
+    k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, sub, lk, kconst, mean, net->X0);
   } else {
     if (kcell) k_cell_logk<2><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, net->lk);
-    k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, lk, kconst, mean, net->X0);
+    k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, sub, lk, kconst, mean, net->X0);
   }
   return FMG_OK;
 }
@@ -1121,11 +1123,11 @@ int net_check_error(fmg_net* net, cudaStream_t st, const char** msg) {
   return FMG_OK;
 }
 
-void launch_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed, cudaStream_t st) {
+void launch_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed, cudaStream_t st, int nc) {
   long long N = M;
   for (int k = 1; k < D; ++k) N *= M;
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_rand_fill<<<blocks_for(N), 256, 0, st>>>(e, D, M, dmask, seed);
+  k_rand_fill<<<blocks_for(N * nc), 256, 0, st>>>(e, D, M, dmask, nc, seed);
 }
 
 void launch_dinv(const double* A, int center, long long Np, const double* u, double* v, long long n, cudaStream_t st) {

@@ -203,6 +203,28 @@ def training_grids(ctx: Context, spec: TrainSpec):
     return grids
 
 
+def elasticity_training_grids(ctx: Context, level: int = 3, count: int = 8, seed: int = 1000,
+                              scales=(0.25, 0.5, 1.0), sigma: float = 0.5):
+    """Grids of the clamped-cube elasticity problem (vector Q2, 3 * 2^level
+    cells per direction, base level 0, the x = 0 face clamped, force -z) with
+    Young's-modulus fields drawn like the benchmark's, E = exp(sigma g) with g
+    the unit-std Fourier field, on windows of side `scale` of the unit cube
+    (field seeds seed .. seed+count-1; the benchmark uses seed 0)."""
+    rng = np.random.default_rng(seed)
+    n = 3 << level
+    grids = []
+    for i in range(count):
+        scale = scales[i % len(scales)]
+        off = rng.uniform(0.0, 1.0 - scale, 3) if scale < 1.0 else np.zeros(3)
+        e = np.exp(sigma * fourier_log_window(n, 3, seed + i, off, scale))
+        g = Grid(ctx, 3, 2, level, 0, n0=3, ncomp=3, dirichlet_mask=0b000001)
+        g.set_coefficient(C.FMG_LAMBDA_MU_CELL, e)
+        g.set_coefficient(C.FMG_F_VEC, [0.0, 0.0, -1.0])
+        g.assemble()
+        grids.append(g)
+    return grids
+
+
 def train(net: DampingNet, grids, cfg: C.SolveCfg, steps: int, lr: float, nsamples: int = 4,
           max_cycles: int = 4, seed: int = 0, lr_end: float | None = None, log=None):
     """Adam on the mean V-cycle loss, cycling through the training grids, the

@@ -2,6 +2,7 @@
 
     python -m gnu_femlisp_b200.weights.train_damping --dim 3 [--out PATH]
     python -m gnu_femlisp_b200.weights.train_damping --dim 2 [--out PATH]
+    python -m gnu_femlisp_b200.weights.train_damping --dim 3 --elastic [--out PATH]
 
 Both minimise the A-norm contraction of one V(1,1) Jacobi cycle on errors the
 multigrid itself makes (random vectors after 4 cycles of A e = 0 with the
@@ -14,6 +15,12 @@ coefficient is the benchmark field's recipe (64 random Fourier modes,
 |kappa| in [1, 10], unit standard deviation) on windows of side 1/8, 1/4,
 1/2 and 1 of the unit cube, field seeds 1000-1011 (the benchmark uses seed
 0); 1500 steps, lr 2e-3; about 15 s on one B200.
+
+3D elasticity (--elastic; the clamped-cube vector-Q2 problem of 48^3 cells):
+eight grids of 24^3 cells, Young's modulus E = exp(0.5 g) with g the same
+Fourier recipe on windows of side 1/4, 1/2 and 1 (seeds 1000-1007; the
+benchmark uses seed 0), the per-node damping of the 3 x 3 block Jacobi
+differentiated through the block V(1,1) cycle; 800 steps, lr 2e-3.
 
 2D (the block-field set): 128^2-cell grids, k piecewise constant on an 8 x 8
 block partition with log10 k ~ U[-3, 3]; one new field per step, seeds
@@ -38,6 +45,7 @@ def main(argv=None):
     ap.add_argument("--dim", type=int, default=3)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--elastic", action="store_true", help="the 3D elasticity net (vector Q2, block Jacobi)")
     a = ap.parse_args(argv)
     C = G._capi
     ctx = G.Context(0)
@@ -45,7 +53,10 @@ def main(argv=None):
                      C.FMG_MULTIPLICATIVE)
     net = learn.DampingNet(ctx, a.dim, seed=1)
     t0 = time.time()
-    if a.dim == 3:
+    if a.elastic:
+        grids = learn.elasticity_training_grids(ctx, level=3, count=8)
+        hist = learn.train(net, grids, cfg, a.steps or 800, 2e-3, 4, 4, log=print)
+    elif a.dim == 3:
         spec = learn.TrainSpec(dim=3, level=5, base=2, count=12, steps=a.steps or 1500, lr=2e-3, nsamples=4,
                                max_cycles=4)
         grids = learn.training_grids(ctx, spec)
@@ -57,7 +68,7 @@ def main(argv=None):
     ctx.synchronize()
     print(f"trained {len(hist)} steps in {time.time() - t0:.1f} s, mean loss first 50 {np.mean(hist[:50]):.4f}, "
           f"last 50 {np.mean(hist[-50:]):.4f}")
-    out = a.out or os.path.join(HERE, f"damping{a.dim}d.fmgnet")
+    out = a.out or os.path.join(HERE, "damping3d_elastic.fmgnet" if a.elastic else f"damping{a.dim}d.fmgnet")
     net.save(out)
     print("wrote", out)
 

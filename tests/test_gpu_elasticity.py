@@ -142,3 +142,91 @@ def test_mixed_solve_matches_fp64(oracle_mod, G, ctx, order, level, n0):
     B, R = g.vector(values=g.rhs()), g.vector()
     g.residual(XM, B, R)
     assert np.linalg.norm(R.get()) / np.linalg.norm(g.rhs()) < 1e-9
+
+
+def _vcfg11(G):
+    return G.SolveCfg(1, G._capi.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 200, G._capi.FMG_MULTIPLICATIVE)
+
+
+def test_block_cycle_gradient_matches_finite_differences(oracle_mod, G, ctx):
+    # dL/domega of the per-node damping of the 3 x 3 block Jacobi, through the
+    # whole V(1,1) cycle (the recorded cycle's adjoint with block solves), on
+    # the top level and the level below, against central differences
+    from gnu_femlisp_b200.learn import learn_loss_levels
+    _, g = make_pair(oracle_mod, G, ctx, 2, 2, 0, 3, seed=8)
+    cfg = _vcfg11(G)
+    rng = np.random.default_rng(4)
+    ws = {}
+    for lev in range(g.base + 1, g.top + 1):
+        ws[lev] = rng.uniform(0.4, 0.8, g.nnodes(lev))
+        g.set_node_damping(lev, ws[lev])
+    n = g.nnodes()
+    m = round(n ** (1 / 3))
+    e0 = rng.uniform(-1, 1, (n, 3))
+    e0[np.arange(n) % m == 0] = 0.0  # the clamped face x = 0
+    ev = g.vector(values=e0.reshape(-1))
+    for lev in (g.top - 1, g.top):
+        L0, grad = learn_loss_levels(g, cfg, ev, lev)
+        assert 0 < L0 < 1 and grad.shape == (g.nnodes(lev),)
+        d = rng.standard_normal(ws[lev].size)
+        eps = 1e-5
+        g.set_node_damping(lev, ws[lev] + eps * d)
+        Lp, _ = learn_loss_levels(g, cfg, ev, lev, want_grad=False)
+        g.set_node_damping(lev, ws[lev] - eps * d)
+        Lm, _ = learn_loss_levels(g, cfg, ev, lev, want_grad=False)
+        g.set_node_damping(lev, ws[lev])
+        fd = (Lp - Lm) / (2 * eps)
+        assert abs(fd - grad @ d) <= 1e-6 * max(1e-3, abs(fd)), (lev, fd, grad @ d)
+
+
+def test_network_damping_on_elasticity_levels(oracle_mod, G, ctx):
+    # the damping network on Q2 node grids (features from E on each node's 8
+    # half-cells), the judge with both probes, and solves with the damping
+    from gnu_femlisp_b200.learn import DampingNet
+    _, g = make_pair(oracle_mod, G, ctx, 2, 2, 0, 3, seed=9)
+    net = DampingNet(ctx, 3, seed=5)
+    om = net.damping(g, g.top)
+    assert om.shape == (g.nnodes(),) and om.min() >= 0.1 and om.max() <= 1.3
+    net.apply(g)
+    cfg = G.SolveCfg(1, G._capi.FMG_JACOBI, 0.6, 2, 2, 1, 0, 1.0, 1e-10, 0.0, 300, G._capi.FMG_MULTIPLICATIVE)
+    ok, rp, rl = g.learned_judge(cfg)
+    assert 0 < rp < 1 and np.isfinite(rl)
+    net.apply(g)
+    ok2, rp2, rl2 = g.learned_judge_mixed(cfg)
+    assert 0 < rp2 < 1 and np.isfinite(rl2)
+    if not ok2:
+        net.apply(g)  # install it anyway: the solves must still reach the tolerance
+    X = g.vector()
+    hist, _, _, st = g.solve_mixed(cfg, X)
+    assert st == 0 and hist[-1] / hist[0] < 1e-10
+
+
+def test_trained_elasticity_net_beats_the_plain_cycle(G, ctx):
+    # the shipped network (trained on fields of seeds 1000-1007) on the
+    # benchmark's field recipe with its seed 0, at 24^3 cells: the judge keeps
+    # it, and CG + V(2,2) block Jacobi needs fewer steps, FP64 and mixed
+    import os
+    from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.learn import DampingNet
+    C = G._capi
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    net = DampingNet.load(ctx, os.path.join(root, "gnu_femlisp_b200", "weights", "damping3d_elastic.fmgnet"))
+    wl = problems.c5(level=3)
+    g = G.Grid(ctx, 3, 2, wl.level, base_level=0, n0=3, ncomp=3, dirichlet_mask=wl.dirichlet_mask)
+    g.set_coefficient(C.FMG_LAMBDA_MU_CELL, wl.ecell)
+    g.set_coefficient(C.FMG_F_VEC, list(wl.force))
+    g.assemble()
+    cfg = G.SolveCfg(1, C.FMG_JACOBI, 0.6, 2, 2, 1, 0, 1.0, 1e-10, 0.0, 300, C.FMG_MULTIPLICATIVE)
+    x = g.vector()
+    _, ns_p, st = g.solve(cfg, x)
+    xp = x.get()
+    _, _, ni_p, _ = g.solve_mixed(cfg, g.vector())
+    net.apply(g)
+    ok, rp, rl = g.learned_judge_mixed(cfg)
+    assert ok and rl < rp, (rp, rl)
+    x.fill(0.0)
+    _, ns_l, st = g.solve(cfg, x)
+    assert st == 0 and ns_l < ns_p, (ns_p, ns_l)
+    assert np.linalg.norm(x.get() - xp) / np.linalg.norm(xp) < 1e-8
+    _, _, ni_l, st = g.solve_mixed(cfg, g.vector())
+    assert st == 0 and ni_l < ni_p and g.learned_status()["reverts"] == 0, (ni_p, ni_l)
