@@ -53,9 +53,11 @@ def parse_args():
                           "48^3 cells, FP64 CG + block-Jacobi V(2,2); each its own JSON line"))
     ap.add_argument("--c5-level", type=int, default=4, help="c5: 3 x 2^level cells per direction")
     ap.add_argument("--c4-fields", type=int, default=256)
-    ap.add_argument("--profile", choices=["solve", "net"], default=None,
+    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
-                         "the launch count, one more solve; net: the damping network on every level, 8 times)")
+                         "the launch count, one more solve; net: the damping network on every level, 8 times; "
+                         "c5: the elasticity setup, two mixed+learned solves, the launch count, one more; "
+                         "c5mv: the elasticity FP64 block matvec, 5 times)")
     return ap.parse_args()
 
 
@@ -482,12 +484,52 @@ def run_c4(args):
     ctx.close()
 
 
+def run_profile_c5(args):
+    """The elasticity workloads for ncu captures at `--c5-level`."""
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.learn import DampingNet
+    C = G._capi
+    wl = problems.c5(level=args.c5_level)
+    ctx = G.Context(0)
+    g = G.Grid(ctx, 3, wl.order, wl.level, base_level=wl.base_level, n0=wl.n0, ncomp=3,
+               dirichlet_mask=wl.dirichlet_mask)
+    g.set_coefficient(C.FMG_LAMBDA_MU_CELL, wl.ecell)
+    g.set_coefficient(C.FMG_F_VEC, list(wl.force))
+    g.assemble()
+    if args.profile == "c5mv":
+        P = g.vector(values=np.random.default_rng(1).standard_normal(wl.dofs))
+        Y = g.vector()
+        for _ in range(5):
+            g.matvec(P, Y)
+        ctx.synchronize()
+        print("launches", ctypes_count(C), flush=True)
+        return
+    cfg = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, wl.damp, wl.pre, wl.post, 1, 0, 1.0, wl.rtol, 0.0, 300,
+                     C.FMG_MULTIPLICATIVE)
+    net = DampingNet.load(ctx, WEIGHTS_ELASTIC)
+    net.apply(g)
+    g.learned_judge_mixed(cfg)
+    x = g.vector()
+    for _ in range(2):
+        x.fill(0.0)
+        g.solve_mixed(cfg, x)
+    ctx.synchronize()
+    print("launches_before_last", ctypes_count(C), flush=True)
+    x.fill(0.0)
+    _, _, ninner, _ = g.solve_mixed(cfg, x)
+    ctx.synchronize()
+    print("launches_after", ctypes_count(C), "inner_iterations", ninner, flush=True)
+
+
 def run_profile(args):
     """Workloads for ncu captures (profiles/ names the commands)."""
     import gnu_femlisp_b200 as G
     from gnu_femlisp_b200 import problems
     from gnu_femlisp_b200.learn import DampingNet
     C = G._capi
+    if args.profile in ("c5", "c5mv"):
+        return run_profile_c5(args)
     wl = problems.c3(seed=0, level=args.level)
     ctx = G.Context(0)
     g = G.Grid(ctx, 3, 1, wl.level, base_level=wl.base_level)
