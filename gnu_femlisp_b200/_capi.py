@@ -50,6 +50,7 @@ class SolveCfg(ctypes.Structure):
         ("atol", ctypes.c_double),
         ("maxsteps", ctypes.c_int),
         ("combination", ctypes.c_int),
+        ("fmg", ctypes.c_int),
     ]
 
 

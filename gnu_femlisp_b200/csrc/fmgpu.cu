@@ -431,6 +431,17 @@ struct MG {
       prolongate();
     }
   }
+  // f-cycle (multigrid.lisp:290-297): restrict from the top to the base
+  // level, then from the base up a cycle on each level and, below the top,
+  // the prolongation of its solution to the level above
+  void fcycle() {
+    const int top = g->cur;
+    for (int l = top; l > g->base; --l) restrict_();
+    for (int l = g->base; l <= top; ++l) {
+      lmgc();
+      if (l != top) prolongate();
+    }
+  }
   // the iterate closure of the multigrid iterator (multigrid.lisp:366-386);
   // *x may be swapped with *spare (ping-pong of fused Jacobi steps)
   void iterate(double** x, double** spare, double* b, double* r) {
@@ -439,7 +450,8 @@ struct MG {
     g->rhsp[top] = b; g->resp[top] = r;
     g->rp[top] = 1;
     g->cur = top;
-    lmgc();
+    if (c.fmg) fcycle();
+    else lmgc();
     *x = g->solp[top];
     *spare = g->sparep[top];
   }
@@ -457,6 +469,7 @@ int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
     return set_err(g->ctx, FMG_ERR_ARG, "bad combination");
   if (c->method < FMG_METHOD_MG || c->method > FMG_METHOD_CG)
     return set_err(g->ctx, FMG_ERR_ARG, "bad method");
+  if (c->fmg != 0 && c->fmg != 1) return set_err(g->ctx, FMG_ERR_ARG, "fmg is 0 or 1");
   return FMG_OK;
 }
 
@@ -1525,6 +1538,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (!mcfg || vec_check(xv, g, g->top) || !nouter || !ninner || !status) return FMG_ERR_ARG;
+  if (cfg->fmg) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed solve: V/W cycles (fmg = 0)");
   if (cfg->smoother != FMG_JACOBI || cfg->combination != FMG_MULTIPLICATIVE || cfg->gamma != 1 ||
       g->base >= g->top || cfg->post_steps < 1)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
@@ -1908,7 +1922,7 @@ int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
   int rc = check_cfg(g, cf);
   if (rc) return rc;
   if (cf->smoother != FMG_JACOBI || cf->combination != FMG_MULTIPLICATIVE || cf->pre_steps != 1 ||
-      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base ||
+      cf->post_steps != 1 || cf->gamma != 1 || g->top <= g->base || cf->fmg ||
       !((g->nc == 1 && g->order == 1) || (g->nc == 3 && g->order == 2 && g->dim == 3)))
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
                    "training loss: Jacobi V(1,1), scalar Q1 or 3D Q2 elasticity, at least two levels");

@@ -179,6 +179,7 @@ class GeometricCS:
     base_level: int = 0
     coarse_grid_iteration: Any = None
     combination: str = "multiplicative"
+    fmg: bool = False            # the f-cycle of :fmg t (multigrid.lisp:290-297)
 
 
 def geometric_cs(**kw) -> GeometricCS:
@@ -274,6 +275,7 @@ def make_cfg(iteration, success_if: str, failure_if: str) -> tuple[C.SolveCfg, i
             raise NotImplementedError(f"smoother {sm!r}")
         cfg.pre_steps, cfg.post_steps, cfg.gamma = cs.pre_steps, cs.post_steps, cs.gamma
         cfg.combination = C.FMG_ADDITIVE if cs.combination == "additive" else C.FMG_MULTIPLICATIVE
+        cfg.fmg = 1 if cs.fmg else 0
         cgi = cs.coarse_grid_iteration or LU()
         if not isinstance(cgi, LU):
             raise NotImplementedError("only the <lu> coarse-grid iteration is built")

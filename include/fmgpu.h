@@ -80,6 +80,11 @@ typedef struct {
   double atol;         /* success if :defnorm < atol (<= 0: off) */
   int maxsteps;        /* failure if :step > maxsteps */
   int combination;     /* FMG_MULTIPLICATIVE or FMG_ADDITIVE */
+  int fmg;             /* 1: the iterator's cycle is the F-cycle (:fmg t,
+                          f-cycle, multigrid.lisp:290-297): the residual
+                          restricted to the base level, then from the base up a
+                          cycle on each level and a prolongation to the next;
+                          fmg_solve and fmg_vcycle only */
 } fmg_solve_cfg;
 
 /* ------------------------------------------------------------- context */

@@ -98,8 +98,9 @@ n-cube with Lagrange Q1/Q2; the coefficients are sampled on the host."))
         (setq *gpu-context* (aref ctx 0)))))
 
 (defun %cfg-bytes (method smoother damp pre post rtol maxsteps)
-  "fmg_solve_cfg laid out as the C struct (64 bytes with x86-64 alignment)."
-  (let ((v (make-array 64 :element-type '(unsigned-byte 8) :initial-element 0)))
+  "fmg_solve_cfg laid out as the C struct (72 bytes with x86-64 alignment;
+the last int, fmg at byte 64, stays 0: V/W cycles)."
+  (let ((v (make-array 72 :element-type '(unsigned-byte 8) :initial-element 0)))
     (flet ((int! (off x) (setf (fl.port:sap-ref-32 v off) x))
            (dbl! (off x) (setf (fl.port:sap-ref-double v off) x)))
       (int! 0 method) (int! 4 smoother) (dbl! 8 damp)

@@ -935,12 +935,25 @@ void lmgc(Hier& H, const ora_solve_cfg& c) {  // multigrid.lisp:254-288
 
 // the multigrid iterator's iterate function (multigrid.lisp:366-386): the
 // top-level sol/rhs/res are the caller's vectors, with no copy
+// f-cycle (multigrid.lisp:290-297): restrict from the top to the base level,
+// then from the base up a cycle on each level and, below the top, the
+// prolongation of its solution to the level above
+void f_cycle(Hier& H, const ora_solve_cfg& c) {
+  const int top = H.cur;
+  for (int l = top; l > H.base; --l) mg_restrict(H);
+  for (int l = H.base; l <= top; ++l) {
+    lmgc(H, c);
+    if (l != top) mg_prolongate(H);
+  }
+}
+
 void mg_iterate(Hier& H, const ora_solve_cfg& c, double* x, double* b, double* r) {
   int top = H.top;
   H.sol[top] = x; H.rhsv[top] = b; H.res[top] = r;
   H.rp[top] = 1;
   H.cur = top;
-  lmgc(H, c);
+  if (c.fmg) f_cycle(H, c);
+  else lmgc(H, c);
 }
 
 void ensure_state(Hier& H) {

@@ -65,6 +65,7 @@ typedef struct {
   double atol;         /* success if defnorm < atol (<=0: off) */
   int maxsteps;        /* failure if step > maxsteps */
   int combination;     /* 0 :multiplicative, 1 :additive (multigrid.lisp:55-70) */
+  int fmg;             /* 1: f-cycle (multigrid.lisp:290-297) */
 } ora_solve_cfg;
 
 void* ora_create(int dim, int order, int ncomp, int n0, int top_level, int base_level,

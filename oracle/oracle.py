@@ -37,6 +37,7 @@ class SolveCfg(ctypes.Structure):
         ("atol", ctypes.c_double),
         ("maxsteps", ctypes.c_int),
         ("combination", ctypes.c_int),
+        ("fmg", ctypes.c_int),
     ]
 
 
@@ -115,9 +116,9 @@ MULTIPLICATIVE, ADDITIVE = 0, 1
 
 def solve_cfg(method=METHOD_CG_MG, smoother=JACOBI, damp=0.6, pre=1, post=1, gamma=1,
               compat=True, coarse_damp=1.0, rtol=1e-10, atol=0.0, maxsteps=200,
-              combination=MULTIPLICATIVE) -> SolveCfg:
+              combination=MULTIPLICATIVE, fmg=False) -> SolveCfg:
     return SolveCfg(method, smoother, damp, pre, post, gamma, 1 if compat else 0, coarse_damp,
-                    rtol, atol, maxsteps, combination)
+                    rtol, atol, maxsteps, combination, 1 if fmg else 0)
 
 
 class Oracle:

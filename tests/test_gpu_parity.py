@@ -241,3 +241,22 @@ def test_galerkin_levels(oracle_mod, G, ctx, dim, level, base, dmask):
     assert_same(X.get(), ro.x, "solution")
     with pytest.raises(G.FmgError):
         G.Grid(ctx, 2, 2, 2, base_level=0).assemble(galerkin=True)  # Q2: re-discretised only
+
+
+@pytest.mark.parametrize("dim,order,level,base,method,sm,damp", [(2, 1, 6, 1, 0, 0, 0.6), (3, 1, 4, 1, 1, 0, 0.6),
+                                                                  (3, 2, 3, 1, 0, 1, 1.2), (2, 1, 5, 0, 1, 0, 0.6)])
+def test_f_cycle_solve_history(oracle_mod, G, ctx, dim, order, level, base, method, sm, damp):
+    # the f-cycle (:fmg t, multigrid.lisp:290-297) as the iteration and as the preconditioner
+    O = oracle_mod
+    o, g = make_pair(O, G, ctx, dim, order, level, base, kcell=(dim == 3), seed=12)
+    oc, gc = _cfg(O, G, method, sm, damp, 1, 1, False, maxsteps=80)
+    oc.fmg = 1
+    gc.fmg = 1
+    ro = o.solve(oc)
+    X = g.vector()
+    hist, steps, status = g.solve(gc, X)
+    assert status == 0 and steps == ro.steps
+    assert_same(hist, ro.history, "defnorm history")
+    assert_same(X.get(), ro.x, "solution")
+    with pytest.raises(G.FmgError):
+        g.solve_mixed(gc, g.vector())  # the mixed cycle is a V/W cycle
