@@ -81,6 +81,7 @@ struct fmg_grid {
   long long epoch = 0;         // incremented by every assembly
   struct MixedState* mx = nullptr;
   struct MixedVec* mxv = nullptr;  // mixed solve state of the vector (elasticity) form
+  bool x_zero = false;             // the judge's probe: the next solve starts from x = 0 (r = b, no matvec)
   double* kq = nullptr;        // Gauss-point coefficient samples of a coarse level
   double *lu = nullptr, *lux = nullptr;  // coarse LU factors and inverse workspace
   int* piv = nullptr;
@@ -1020,7 +1021,8 @@ int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, 
   launch_fill(g->p, n, 0.0, st);
   for (int step = 0;; ++step) {
     if (!rp) {  // intermediate :before -> ensure-residual (problem.lisp:109-116)
-      launch_spmv(T, x, b, g->r, nullptr, nullptr, st);
+      if (step == 0 && g->x_zero) launch_copy(b, g->r, n, st);  // x = 0: r = b exactly
+      else launch_spmv(T, x, b, g->r, nullptr, nullptr, st);
       launch_dot(g->r, g->r, n, reducer(g, EPI_STORE, S_RR), st);
       if ((rc = launched(c, "residual"))) return rc;
       rp = true;
@@ -1476,7 +1478,8 @@ static int solve_mixed_vec(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixe
   bool judge_active = g->learned;
   std::vector<double*> hidden;
   for (int restart = 0; restart <= max_restart; ++restart) {
-    launch_spmv(T, x, b, r, nullptr, nullptr, st);  // true FP64 residual
+    if (restart == 0 && g->x_zero) launch_copy(b, r, n, st);  // x = 0: r = b exactly
+    else launch_spmv(T, x, b, r, nullptr, nullptr, st);      // true FP64 residual
     launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
     if ((rc = read_scalars(g))) return rc;
     const double dn = std::sqrt(c->host_scal[S_RR]);
@@ -1563,8 +1566,9 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   double initial = -1.0;
   int step = 0, iters = 0;  // history slots, CG iterations
   for (int restart = 0; restart <= max_restart; ++restart) {
-    // true FP64 residual with the assembled matrix
-    launch_spmv(T, x, b, r, nullptr, nullptr, st);
+    // true FP64 residual with the assembled matrix (x = 0: r = b exactly)
+    if (restart == 0 && g->x_zero) launch_copy(b, r, n, st);
+    else launch_spmv(T, x, b, r, nullptr, nullptr, st);
     launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
     if ((rc = read_scalars(g))) return rc;
     const double dn = std::sqrt(c->host_scal[S_RR]);
@@ -2219,7 +2223,7 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   const Lvl& T = g->lev[g->top];
   const LevelView TV = view(g, g->top);
   const long long n = T.N * g->nc;
-  double *xs = g->lt[9], *b = g->lt[7], *e = g->lt[6], *u = g->lt[5];
+  double *xs = g->lt[9], *b = g->lt[7], *e = g->lt[6];
   launch_rand_fill(xs, g->dim, T.M, g->dmask, seed, st, g->nc);
   launch_spmv(TV, xs, nullptr, b, nullptr, nullptr, st);
   launch_dot(xs, b, n, reducer(g, EPI_STORE, S_E0), st);
@@ -2237,6 +2241,7 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   const bool learned = g->learned;
   g->rhs = b;
   g->learned = false;
+  g->x_zero = true;
   int ns = 0, status = 0, nouter = 0, rc;
   if (mc) {
     fmg_mixed_cfg m = *mc;
@@ -2247,10 +2252,11 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   }
   g->rhs = rhs;
   g->learned = learned;
+  g->x_zero = false;
   if (rc) return rc;
+  // |e_k|_A^2 = e_k . A e_k with A e_k = b - A x_k, the solve's FP64 residual
   launch_sub_wv(xs, nullptr, x.d, e, n, st);
-  launch_spmv(TV, e, nullptr, u, nullptr, nullptr, st);
-  launch_dot(e, u, n, reducer(g, EPI_STORE, S_E3), st);
+  launch_dot(e, g->r, n, reducer(g, EPI_STORE, S_E3), st);
   if ((rc = launched(ctx, "judge probe"))) return rc;
   if ((rc = read_scalars(g))) return rc;
   const double e0 = ctx->host_scal[S_E0], ek = ctx->host_scal[S_E3];
