@@ -39,7 +39,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_report_the_slowest_rank():
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_rank, args=(world, _free_port(), out), nprocs=world, start_method="spawn", join=True)
     for r in range(world):
