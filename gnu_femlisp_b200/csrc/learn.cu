@@ -24,6 +24,9 @@
 #include <cstdio>
 #include <cstring>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "fmgpu_learn.cuh"
 #include "umma.cuh"
 
@@ -294,10 +297,11 @@ __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
 // mbarriers, one per plane parity, each with at most one commit pending).
 constexpr int kSeg = 8;    // output planes per work item
 constexpr int kRing = 4;   // halo plane slots
+constexpr int kSlotB = (kPlaneB + 127) / 128 * 128;  // 2944: ring slots 128-byte aligned (TMA destinations)
 
 template <int CIN, int COUT>
 struct Z3 {
-  static constexpr int CHB = kRing * kPlaneB;      // one 8-channel chunk of the ring
+  static constexpr int CHB = kRing * kSlotB;       // one 8-channel chunk of the ring
   static constexpr int RING = (CIN / 8) * CHB;
   static constexpr int WTAP = 3 * COUT * CIN * 2;  // one xy tap: the dz = 0, 1, 2 slices, K-major
   static constexpr int WBYTES = 9 * WTAP;
@@ -318,34 +322,27 @@ __device__ __forceinline__ void stage_weights_z3(uint8_t* ws, const bf16* __rest
   }
 }
 
-// padded input plane P of column (tx, ty) -> ring slot P % kRing; chunk c of
-// halo node (hx, hy) at byte c CHB + slot kPlaneB + hy kHyB + 16 hx
-template <int CIN>
-__device__ __forceinline__ void stage_plane_z3(uint8_t* hs, const bf16* __restrict__ in, const TileGeo& t, int tx,
-                                               int ty, int P) {
-  constexpr int ROWS = HX * HY, CHB = kRing * kPlaneB;
-  uint8_t* base = hs + (P % kRing) * kPlaneB;
-  for (int idx = threadIdx.x; idx < (CIN / 8) * ROWS; idx += kThreads) {
-    const int c = idx / ROWS, r = idx - c * ROWS;
-    const int hx = r % HX, hy = r / HX;
-    const int px = tx * TX + hx, py = ty * TY + hy;
-    const bool ok = px < t.Px && py < t.Py && P < t.Pz;
-    const long long node = ok ? ((long long)P * t.Py + py) * t.Px + px : 0;
-    cp16(base + c * CHB + r * kRowB, reinterpret_cast<const uint4*>(in + node * CIN) + c, ok);
-  }
-}
-
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
 
+// The halo planes arrive by TMA: thread 0 issues, per plane, CIN/8 tiled
+// copies of the (8 channels) x 10 x 18 box of the activation tensor
+// [z][y][x][C] (viewed as 5D: 8 channels, C/8 chunks, x, y, z; nodes beyond
+// the array read as zeros) into the plane's ring slot, completing on that
+// slot's mbarrier; it waits for the plane (bounded) before its MMAs.  The
+// other threads only wait for MMA completion before their epilogue, so no
+// block-wide barrier is taken per plane; one per work item orders the
+// epilogue's tensor-memory reads before the next item's MMAs.
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a) {
+__global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_constant__ CUtensorMap tin) {
   using Z = Z3<CIN, COUT>;
+  constexpr uint32_t kPlaneTx = (CIN / 8) * kPlaneB;  // bytes of one plane's copies
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* ws = smem;
   uint8_t* hs = smem + Z::WBYTES;
   __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t full[kRing];
   __shared__ uint32_t tslot;
+  __shared__ int halo_timeout;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const TileGeo& t = a.t;
   const int nseg = (t.Mz + kSeg - 1) / kSeg;
@@ -354,95 +351,128 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a) {
   stage_weights_z3<CIN, COUT>(ws, a.w);
   cp_commit();
   asm volatile("cp.async.wait_group 0;" ::: "memory");
+  umma::fence_async_smem();  // the staged weights -> the tensor core's proxy
   if (warp == 0) umma::tmem_alloc(&tslot, Z::TCOLS);
-  if (tid == 0) { umma::mbar_init(&bar[0]); umma::mbar_init(&bar[1]); }
+  if (tid == 0) {
+    umma::mbar_init(&bar[0]);
+    umma::mbar_init(&bar[1]);
+    for (int i = 0; i < kRing; ++i) umma::mbar_init(&full[i]);
+    halo_timeout = 0;
+  }
   umma::fence_before();
   __syncthreads();
   umma::fence_after();
   const uint32_t tmem = tslot;
   const uint32_t hb = umma::smem_u32(hs), wb = umma::smem_u32(ws);
-  uint32_t phase = 0u;  // bit i: parity of bar[i]'s next phase
-  uint32_t pend = 0u;   // bit i: a commit on bar[i] not yet waited for
+  uint32_t phase = 0u;   // bit i: parity of bar[i]'s next phase
+  uint32_t pend = 0u;    // bit i: a commit on bar[i] not yet waited for
+  uint32_t fphase = 0u;  // thread 0, bit s: parity of full[s]'s next phase
+  uint32_t fpend = 0u;   // thread 0, bit s: a plane load on full[s] not yet waited for
   bool failed = false;
-  auto wait_plane = [&](int i) {  // all threads: the MMAs committed to bar[i] are done
-    const bool ok = !__syncthreads_or(!umma::mbar_wait(&bar[i], (phase >> i) & 1u));
-    if (ok) { phase ^= 1u << i; pend &= ~(1u << i); }
-    return ok;
+  int tx = 0, ty = 0;
+  auto load_plane = [&](int P) {  // thread 0
+    const int sl = P % kRing;
+    umma::mbar_arrive_expect_tx(&full[sl], kPlaneTx);
+    uint8_t* dst = hs + sl * kSlotB;
+    for (int c = 0; c < CIN / 8; ++c) umma::tma_load_5d(dst + c * Z::CHB, &tin, &full[sl], 0, c, tx * TX, ty * TY, P);
+    fpend |= 1u << sl;
   };
-  auto epilogue = [&](int z0, int z, int tx, int ty) {
+  auto wait_mma = [&](int i) {  // this thread: the MMAs committed to bar[i] are done
+    if (umma::mbar_wait(&bar[i], (phase >> i) & 1u)) {
+      phase ^= 1u << i;
+      pend &= ~(1u << i);
+      return true;
+    }
+    return false;
+  };
+  auto epilogue = [&](int z0, int z) {
     umma::fence_after();
     float v[COUT];
     umma::tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(COUT * (kSeg - 1 - (z - z0))), v);
     const int r = warp * 32 + lane;
     conv_epilogue<3, COUT, EPI>(a, v, tx * TX + (r & 7), ty * TY + (r >> 3), z);
   };
-  for (long long id = blockIdx.x; id < items && !failed; id += gridDim.x) {
-    const int tx = (int)(id % t.ntx);
+  for (long long id = blockIdx.x; id < items; id += gridDim.x) {
+    tx = (int)(id % t.ntx);
     const long long rest = id / t.ntx;
-    const int ty = (int)(rest % t.nty), z0 = (int)(rest / t.nty) * kSeg;
+    ty = (int)(rest % t.nty);
+    const int z0 = (int)(rest / t.nty) * kSeg;
     const int S = min(kSeg, t.Mz - z0);
     const int nplanes = S + 2;  // padded input planes z0 .. z0+S+1
-    stage_plane_z3<CIN>(hs, a.in, t, tx, ty, z0);
-    cp_commit();
-    stage_plane_z3<CIN>(hs, a.in, t, tx, ty, z0 + 1);
-    cp_commit();
+    if (tid == 0) {
+      load_plane(z0);
+      load_plane(z0 + 1);
+    }
     for (int k = 0; k < nplanes; ++k) {
       const int P = z0 + k;
-      // the slot of plane P + 2 was last read by the MMAs of plane P - 2, waited for at step k - 1
-      if (k + 2 < nplanes) stage_plane_z3<CIN>(hs, a.in, t, tx, ty, P + 2);
-      cp_commit();
-      cp_wait_2();  // plane P has landed (this thread's copies)
-      umma::fence_async_smem();
-      umma::fence_before();
-      __syncthreads();
       if (tid == 0) {
+        // the slot of plane P + 2 was last read by the MMAs of plane P - 2, waited for at step k - 1
+        if (k + 2 < nplanes) load_plane(P + 2);
+        const int sl = P % kRing;
+        const bool landed = umma::mbar_wait(&full[sl], (fphase >> sl) & 1u);
+        if (landed) {
+          fphase ^= 1u << sl;
+          fpend &= ~(1u << sl);
+        } else {
+          halo_timeout = 1;
+        }
         umma::fence_after();
-        const int dlo = max(0, P - (z0 + S - 1)), dhi = min(2, P - z0);
-        const uint32_t dcol = tmem + (uint32_t)(COUT * (kSeg - 1 - (P - dlo - z0)));
-        const uint32_t aslot = hb + (uint32_t)((P % kRing) * kPlaneB);
-        const uint32_t idesc = umma::idesc_bf16(128, (dhi - dlo + 1) * COUT, false, false);
-        const uint32_t brow = (uint32_t)(dlo * (COUT / 8) * (CIN / 8) * 128);  // row dlo COUT of the B tile
-        bool first = dlo == 0;  // this plane opens output plane P
-        for (int tap = 0; tap < 9; ++tap) {
-          const uint32_t aoff = (uint32_t)((tap / 3) * kHyB + (tap % 3) * kRowB);
+        if (landed) {
+          const int dlo = max(0, P - (z0 + S - 1)), dhi = min(2, P - z0);
+          const uint32_t dcol = tmem + (uint32_t)(COUT * (kSeg - 1 - (P - dlo - z0)));
+          const uint32_t aslot = hb + (uint32_t)(sl * kSlotB);
+          const uint32_t idesc = umma::idesc_bf16(128, (dhi - dlo + 1) * COUT, false, false);
+          const uint32_t brow = (uint32_t)(dlo * (COUT / 8) * (CIN / 8) * 128);  // row dlo COUT of the B tile
+          bool first = dlo == 0;  // this plane opens output plane P
+          for (int tap = 0; tap < 9; ++tap) {
+            const uint32_t aoff = (uint32_t)((tap / 3) * kHyB + (tap % 3) * kRowB);
 #pragma unroll
-          for (int kh = 0; kh < CIN / 16; ++kh) {
-            // A: 8 x-nodes 16 B apart x 16 y-rows kHyB apart, K chunks CHB apart
-            const uint64_t ad = umma::make_desc(aslot + aoff + 2 * kh * Z::CHB, Z::CHB, kHyB);
-            const uint32_t wt = wb + tap * Z::WTAP + kh * 256;
-            if (first) {
-              // output P alone (slice dz = 0, N = COUT) with accumulate off, then the other slices
-              umma::mma_bf16(dcol, ad, umma::make_desc(wt, 128, (CIN / 8) * 128),
-                             umma::idesc_bf16(128, COUT, false, false), 0u);
-              if (dhi > 0)
-                umma::mma_bf16(dcol + COUT, ad, umma::make_desc(wt + (COUT / 8) * (CIN / 8) * 128, 128, (CIN / 8) * 128),
-                               umma::idesc_bf16(128, dhi * COUT, false, false), 1u);
-              first = false;
-            } else {
-              umma::mma_bf16(dcol, ad, umma::make_desc(wt + brow, 128, (CIN / 8) * 128), idesc, 1u);
+            for (int kh = 0; kh < CIN / 16; ++kh) {
+              // A: 8 x-nodes 16 B apart x 16 y-rows kHyB apart, K chunks CHB apart
+              const uint64_t ad = umma::make_desc(aslot + aoff + 2 * kh * Z::CHB, Z::CHB, kHyB);
+              const uint32_t wt = wb + tap * Z::WTAP + kh * 256;
+              if (first) {
+                // output P alone (slice dz = 0, N = COUT) with accumulate off, then the other slices
+                umma::mma_bf16(dcol, ad, umma::make_desc(wt, 128, (CIN / 8) * 128),
+                               umma::idesc_bf16(128, COUT, false, false), 0u);
+                if (dhi > 0)
+                  umma::mma_bf16(dcol + COUT, ad,
+                                 umma::make_desc(wt + (COUT / 8) * (CIN / 8) * 128, 128, (CIN / 8) * 128),
+                                 umma::idesc_bf16(128, dhi * COUT, false, false), 1u);
+                first = false;
+              } else {
+                umma::mma_bf16(dcol, ad, umma::make_desc(wt + brow, 128, (CIN / 8) * 128), idesc, 1u);
+              }
             }
           }
         }
-        umma::mma_commit(&bar[k & 1]);
+        umma::mma_commit(&bar[k & 1]);  // also when nothing was issued: every commit has its wait
       }
       pend |= 1u << (k & 1);
       if (k >= 1) {
-        if (!wait_plane((k - 1) & 1)) { failed = true; break; }
-        if (k >= 3) epilogue(z0, P - 3, tx, ty);
+        if (!wait_mma((k - 1) & 1)) failed = true;
+        if (!failed && k >= 3) epilogue(z0, P - 3);
         umma::fence_before();
       }
     }
-    if (failed) break;
-    if (!wait_plane((nplanes - 1) & 1)) { failed = true; break; }
-    epilogue(z0, z0 + S - 1, tx, ty);
-    umma::fence_before();  // the loads above precede the next item's MMAs (barrier before them)
+    if (!wait_mma((nplanes - 1) & 1)) failed = true;
+    if (!failed) epilogue(z0, z0 + S - 1);
+    umma::fence_before();  // the tensor-memory reads above precede the next item's MMAs
+    const bool stop = __syncthreads_or(failed || halo_timeout != 0);
+    umma::fence_after();
+    if (stop) {
+      failed = true;
+      break;
+    }
   }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (failed) {
     if (tid == 0) atomicOr(a.err, 1u);
     for (int i = 0; i < 2; ++i)
       if ((pend >> i) & 1u) umma::mbar_wait(&bar[i], (phase >> i) & 1u);  // bounded: let issued MMAs drain
   }
+  if (tid == 0)  // bounded: no copy may still be landing when the CTA exits
+    for (int sl = 0; sl < kRing; ++sl)
+      if ((fpend >> sl) & 1u) umma::mbar_wait(&full[sl], (fphase >> sl) & 1u);
   umma::fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -882,8 +912,30 @@ int sm_count() {
   return n;
 }
 
+// the activation tensor [Pz][Py][Px][C] (BF16) as the 5D TMA view (8
+// channels, C/8 chunks, x, y, z) with a box of one chunk over the 10 x 18 halo
+// of one plane; nodes beyond the array are read as zeros
+bool act_tensor_map(const bf16* base, int C, const TileGeo& t, CUtensorMap* out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[5] = {8, (cuuint64_t)(C / 8), (cuuint64_t)t.Px, (cuuint64_t)t.Py, (cuuint64_t)t.Pz};
+  const cuuint64_t strides[4] = {16, (cuuint64_t)C * 2, (cuuint64_t)t.Px * C * 2, (cuuint64_t)t.Py * t.Px * C * 2};
+  const cuuint32_t box[5] = {8, 1, (cuuint32_t)HX, (cuuint32_t)HY, 1};
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  return encode(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(base), dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int D, int CIN, int COUT, int EPI>
-void conv(const ConvArgs& a, cudaStream_t st) {
+int conv(const ConvArgs& a, cudaStream_t st) {
   if constexpr (D == 3) {
     constexpr size_t smem = Z3<CIN, COUT>::SMEM;
     static bool init3 = false;
@@ -891,10 +943,12 @@ void conv(const ConvArgs& a, cudaStream_t st) {
       cudaFuncSetAttribute(k_conv3z<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       init3 = true;
     }
+    CUtensorMap tin;
+    if (!act_tensor_map(a.in, CIN, a.t, &tin)) return FMG_ERR_CUDA;
     const long long items = (long long)a.t.ntx * a.t.nty * ((a.t.Mz + kSeg - 1) / kSeg);
     const long long grid = std::min<long long>(items, 2LL * sm_count());
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    k_conv3z<CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a);
+    k_conv3z<CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a, tin);
   } else {
     constexpr size_t smem = (size_t)Tp<D>::TAPS * COUT * CIN * 2 + (size_t)(CIN / 8) * Tp<D>::CHB;
     static bool init = false;
@@ -906,6 +960,7 @@ void conv(const ConvArgs& a, cudaStream_t st) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     k_conv<D, CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a);
   }
+  return FMG_OK;
 }
 
 template <int D, int CG, int CX>
@@ -952,13 +1007,14 @@ int forward_d(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st) {
   zero_ghosts<D>(t, kNetHid, net->H2, st);
   ConvArgs a{};
   a.t = t; a.err = net->err; a.omin = net->omega_min; a.omax = net->omega_max;
+  int rc;
   a.in = net->X0; a.w = net->wf1; a.bias = net->P + L.b1; a.out = net->H1;
-  conv<D, kNetIn, kNetHid, EPI_RELU>(a, st);
+  if ((rc = conv<D, kNetIn, kNetHid, EPI_RELU>(a, st))) return rc;
   a.in = net->H1; a.w = net->wf2; a.bias = net->P + L.b2; a.out = net->H2;
-  conv<D, kNetHid, kNetHid, EPI_RELU>(a, st);
+  if ((rc = conv<D, kNetHid, kNetHid, EPI_RELU>(a, st))) return rc;
   if (omega) {
     a.in = net->H2; a.w = net->wf3; a.bias = net->P + L.b3; a.out = nullptr; a.omega = omega;
-    conv<D, kNetHid, kNetOut, EPI_OMEGA>(a, st);
+    if ((rc = conv<D, kNetHid, kNetOut, EPI_OMEGA>(a, st))) return rc;
   }
   return FMG_OK;
 }
@@ -981,12 +1037,12 @@ int backward_d(fmg_net* net, const double* gomega, const double* omega, cudaStre
   ConvArgs a{};
   a.t = t; a.err = net->err;
   a.in = net->dZ; a.w = net->wb3; a.mask = net->H2; a.out = net->dP2;
-  conv<D, kNetOut, kNetHid, EPI_MASK>(a, st);
+  if ((rc = conv<D, kNetOut, kNetHid, EPI_MASK>(a, st))) return rc;
   // layer 2
   if ((rc = wgrad<D, kNetHid, kNetHid>(net, t, net->dP2, net->H1, L.w2, kNetHid, st))) return rc;
   colsum<kNetHid>(net, net->dP2, npad, L.b2, kNetHid, st);
   a.in = net->dP2; a.w = net->wb2; a.mask = net->H1; a.out = net->dP1;
-  conv<D, kNetHid, kNetHid, EPI_MASK>(a, st);
+  if ((rc = conv<D, kNetHid, kNetHid, EPI_MASK>(a, st))) return rc;
   // layer 1
   if ((rc = wgrad<D, kNetHid, kNetIn>(net, t, net->dP1, net->X0, L.w1, kNetHid, st))) return rc;
   colsum<kNetHid>(net, net->dP1, npad, L.b1, kNetHid, st);

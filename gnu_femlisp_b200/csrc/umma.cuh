@@ -79,6 +79,24 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// one arrival on the mbarrier that also expects `bytes` of asynchronous
+// transactions (the TMA copies that complete on it)
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// tiled TMA load of a 5D box into this CTA's shared memory, completing on
+// the mbarrier (no multicast); tmap: the address of a __grid_constant__
+// CUtensorMap parameter
+__device__ __forceinline__ void tma_load_5d(void* dst, const void* tmap, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // D[tmem] (+)= A * B^T; issued by one thread
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
                                          uint32_t accumulate) {
