@@ -5,7 +5,7 @@ with damped-Jacobi / multicolour-SOR smoothing on Lagrange Q1/Q2 level
 matrices, all on one GPU behind the C-ABI in ``include/fmgpu.h``.
 """
 from ._capi import FmgError, MixedCfg, SolveCfg  # noqa: F401
-from .core import Context, Grid, Vector  # noqa: F401
+from .core import Context, Grid, Vector, slots_to_csr  # noqa: F401
 from .iteration import (CG, LU, SOR, CdrProblem, GaussSeidel, GeometricCS, Jacobi,  # noqa: F401
                         LagrangeFE, LinearSolver, Mesh, cdr_model_problem, discretize_globally,
                         geometric_cs, lagrange_fe, sample_at_gauss_points, solve,

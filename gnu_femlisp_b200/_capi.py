@@ -17,6 +17,7 @@ FMG_OK = 0
 FMG_K_CONST, FMG_K_CELL, FMG_F_CONST, FMG_F_IP, FMG_LAMBDA_MU_CELL, FMG_F_VEC = 0, 1, 2, 3, 4, 5
 FMG_JACOBI, FMG_SOR = 0, 1
 FMG_ASSEMBLE_REDISCRETIZE, FMG_ASSEMBLE_GALERKIN = 0, 1
+FMG_CSR, FMG_CCS = 0, 1
 FMG_METHOD_MG, FMG_METHOD_CG_MG, FMG_METHOD_CG = 0, 1, 2
 FMG_MULTIPLICATIVE, FMG_ADDITIVE = 0, 1
 
@@ -79,6 +80,9 @@ SIGNATURES = {
     "fmg_set_coefficient": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_long]),
     "fmg_assemble": (ctypes.c_int, [_vp]),
     "fmg_get_matrix": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "fmg_set_matrix": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), _dp, ctypes.c_long]),
+    "fmg_set_rhs": (ctypes.c_int, [_vp, _dp, ctypes.c_long]),
     "fmg_get_rhs": (ctypes.c_int, [_vp, _dp]),
     "fmg_set_node_damping": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_long]),
     "fmg_vec_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),

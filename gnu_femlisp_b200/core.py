@@ -69,6 +69,40 @@ class Context:
             pass
 
 
+def slots_to_csr(A: np.ndarray, dim: int, order: int, nc: int = 1):
+    """Stencil-slot storage ``[slot][k][l][node]`` (slot = sum over directions
+    of (offset + order) * (2 order + 1)^d, the layout ``fmg_get_matrix``
+    returns) to compressed rows ``(start, index, values)``, node-major dofs,
+    exact zeros left out."""
+    w = 2 * order + 1
+    nslots = w ** dim
+    A = np.asarray(A).reshape(nslots, nc, nc, -1)
+    N = A.shape[-1]
+    M = int(round(N ** (1.0 / dim)))
+    assert M ** dim == N, "level is not a full n-cube"
+    idx = np.arange(N, dtype=np.int64)
+    c = np.stack([(idx // M ** d) % M for d in range(dim)], 1)
+    rows, cols, vals = [], [], []
+    for s in range(nslots):
+        off = np.array([(s // w ** d) % w - order for d in range(dim)])
+        cj = c + off
+        ok = np.all((cj >= 0) & (cj < M), 1)
+        j = sum(cj[:, d] * M ** d for d in range(dim))
+        for k in range(nc):
+            for l in range(nc):
+                v = A[s, k, l]
+                m = ok & (v != 0.0)
+                rows.append(idx[m] * nc + k)
+                cols.append(j[m] * nc + l)
+                vals.append(v[m])
+    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+    order_ = np.lexsort((cols, rows))
+    rows, cols, vals = rows[order_], cols[order_], vals[order_]
+    start = np.zeros(N * nc + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=N * nc), out=start[1:])
+    return start, cols, vals
+
+
 class Grid:
     """A level hierarchy of the uniformly refined unit n-cube with a Lagrange
     Q1/Q2 space (``fmg_grid_create``); levels base_level..level."""
@@ -115,6 +149,32 @@ class Grid:
         out = np.zeros(self.nslots * self.nc * self.nc * self.nnodes(level))
         self.ctx.check(self._lib.fmg_get_matrix(self.h, level, C.dptr(out)), "get_matrix")
         return out.reshape(self.nslots * self.nc * self.nc, -1)
+
+    def matrix_csr(self, level: int | None = None):
+        """The level matrix as compressed rows ``(start, index, values)`` in the
+        grid's node-major lexicographic numbering (the inverse of
+        ``set_matrix``); exact zeros are left out."""
+        level = self.top if level is None else level
+        return slots_to_csr(self.matrix(level), self.dim, self.order, self.nc)
+
+    def set_matrix(self, level: int, start, index, values, layout: str = "csr") -> "Grid":
+        """``fmg_set_matrix``: a level matrix from compressed rows (``"csr"``)
+        or columns (``"ccs"``, the form of Femlisp's ``sparse-matrix->ccs``)
+        in the grid's node-major lexicographic numbering.  The grid counts as
+        assembled once every level has a matrix."""
+        lay = {"csr": C.FMG_CSR, "ccs": C.FMG_CCS}[layout]
+        st = np.ascontiguousarray(start, dtype=np.int32)
+        ix = np.ascontiguousarray(index, dtype=np.int32)
+        va = np.ascontiguousarray(values, dtype=np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self.ctx.check(self._lib.fmg_set_matrix(self.h, level, lay, st.ctypes.data_as(ip), ix.ctypes.data_as(ip),
+                                                C.dptr(va), st.size - 1), "set_matrix")
+        return self
+
+    def set_rhs(self, values) -> "Grid":
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        self.ctx.check(self._lib.fmg_set_rhs(self.h, C.dptr(v), v.size), "set_rhs")
+        return self
 
     def rhs(self) -> np.ndarray:
         out = np.zeros(self.nnodes() * self.nc)

@@ -78,6 +78,8 @@ struct fmg_grid {
          *xs = nullptr, *xs2 = nullptr;
   bool assembled = false;
   bool assembled_once = false;
+  std::vector<char> have;      // levels whose matrix is in place
+  bool uploaded = false;       // some level matrix came from fmg_set_matrix
   long long epoch = 0;         // incremented by every assembly
   struct MixedState* mx = nullptr;
   struct MixedVec* mxv = nullptr;  // mixed solve state of the vector (elasticity) form
@@ -589,6 +591,8 @@ int fmg_grid_create(fmg_ctx* c, int dim, int order, int ncomp, int n0, int top_l
   return FMG_OK;
 }
 
+static void mixed_vec_delete(MixedVec* m);
+
 static void grid_release(fmg_grid* g) {
   fmg_ctx* c = g->ctx;
   cudaStreamSynchronize(c->stream);
@@ -597,7 +601,7 @@ static void grid_release(fmg_grid* g) {
   if (g->mx)
     for (auto& e : g->mx->graphs) cudaGraphExecDestroy(e.exec);
   delete g->mx;
-  delete g->mxv;
+  mixed_vec_delete(g->mxv);
   delete g;
   c->grids -= 1;
   if (c->closed && c->grids == 0) ctx_release(c);
@@ -726,6 +730,8 @@ static int ensure_buffers(fmg_grid* g) {
 
 int fmg_assemble(fmg_grid* g) { return fmg_assemble_levels(g, FMG_ASSEMBLE_REDISCRETIZE); }
 
+static int finish_levels(fmg_grid* g);
+
 int fmg_assemble_levels(fmg_grid* g, int mode) {
   if (!g) return FMG_ERR_ARG;
   fmg_ctx* c = g->ctx;
@@ -770,6 +776,17 @@ int fmg_assemble_levels(fmg_grid* g, int mode) {
     launch_assemble(g->dim, g->order, a, L.Kbar_h.data(), L.Ctab_h.data(), st);
     if ((rc = launched(c, "assemble"))) return rc;
   }
+  g->have.assign(g->top + 1, 1);
+  g->uploaded = false;
+  return finish_levels(g);
+}
+
+// The coarse LU and the multigrid state of a hierarchy whose level matrices
+// are all in place (assembled, formed, or uploaded).
+static int finish_levels(fmg_grid* g) {
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  int rc;
   // dense LU of the base level and its explicit inverse
   const Lvl& B = g->lev[g->base];
   const long long nb = B.N * g->nc;
@@ -789,6 +806,77 @@ int fmg_assemble_levels(fmg_grid* g, int mode) {
   FMG_CK(c, cudaStreamSynchronize(st));
   g->assembled = true;
   g->epoch += 1;
+  return FMG_OK;
+}
+
+// A level matrix given as compressed rows (CSR) or columns (CCS, the form of
+// sparse-matrix->ccs, sparselu.lisp:226-263) over the grid's numbering
+// (node-major, lexicographic nodes, x fastest), scattered into the stencil-slot
+// storage on the host and copied to the device in one piece.
+int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const int* index, const double* values,
+                   long n) {
+  if (!g || !start || (!index && n > 0) || (!values && n > 0)) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  if (level < g->base || level > g->top) return set_err(c, FMG_ERR_ARG, "level %d out of range", level);
+  if (layout != FMG_CSR && layout != FMG_CCS) return set_err(c, FMG_ERR_ARG, "unknown matrix layout %d", layout);
+  const Lvl& L = g->lev[level];
+  const int nc = g->nc, dim = g->dim, ord = g->order, w = 2 * ord + 1;
+  if (n != L.N * nc) return set_err(c, FMG_ERR_ARG, "level %d has %lld rows, got %ld", level, L.N * nc, n);
+  if (start[0] != 0) return set_err(c, FMG_ERR_ARG, "start[0] must be 0");
+  for (long a = 0; a < n; ++a)
+    if (start[a + 1] < start[a]) return set_err(c, FMG_ERR_ARG, "start decreases at %ld", a);
+  int rc;
+  FMG_CK(c, cudaSetDevice(c->device));
+  if ((rc = ensure_buffers(g))) return rc;
+  const long long M = L.M, Np = L.Np;
+  std::vector<double> H((size_t)g->nslots * nc * nc * Np, 0.0);
+  for (long a = 0; a < n; ++a) {
+    for (int e = start[a]; e < start[a + 1]; ++e) {
+      const long b = index[e];
+      if (b < 0 || b >= n) return set_err(c, FMG_ERR_ARG, "index %ld out of range at entry %d", b, e);
+      const long row = layout == FMG_CSR ? a : b, col = layout == FMG_CSR ? b : a;
+      const long long i = row / nc, j = col / nc;
+      const int k = (int)(row % nc), l = (int)(col % nc);
+      long long ti = i, tj = j;
+      int s = 0, wk = 1;
+      bool in = true;
+      for (int d = 0; d < dim; ++d) {
+        const long long o = tj % M - ti % M;
+        if (o < -ord || o > ord) in = false;
+        s += (int)(o + ord) * wk;
+        wk *= w;
+        ti /= M; tj /= M;
+      }
+      const long long p = !in ? -1 : ord == 2 ? q2_slot_pos(dim, M, i, s, nc == 1) : i;
+      if (p < 0) {
+        if (values[e] != 0.0)
+          return set_err(c, FMG_ERR_ARG, "entry (%ld,%ld) lies outside the Q%d stencil of the level", row, col, ord);
+        continue;
+      }
+      H[((size_t)s * nc * nc + (size_t)k * nc + l) * Np + p] += values[e];
+    }
+  }
+  g->assembled = false;
+  FMG_CK(c, cudaMemcpyAsync(L.A, H.data(), H.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
+  if ((int)g->have.size() != g->top + 1) g->have.assign(g->top + 1, 0);
+  g->have[level] = 1;
+  g->uploaded = true;
+  for (int m = g->base; m <= g->top; ++m)
+    if (!g->have[m]) return FMG_OK;  // the hierarchy is complete with the last level
+  return finish_levels(g);
+}
+
+int fmg_set_rhs(fmg_grid* g, const double* host, long n) {
+  if (!g || !host) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  const Lvl& T = g->lev[g->top];
+  if (n != T.N * g->nc) return set_err(c, FMG_ERR_ARG, "rhs wants %lld values, got %ld", T.N * g->nc, n);
+  int rc;
+  FMG_CK(c, cudaSetDevice(c->device));
+  if ((rc = ensure_buffers(g))) return rc;
+  FMG_CK(c, cudaMemcpyAsync(g->rhs, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FMG_CK(c, cudaStreamSynchronize(c->stream));
   return FMG_OK;
 }
 
@@ -1143,7 +1231,8 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
   if (!g->mx) g->mx = new MixedState();
   MixedState& X = *g->mx;
   const int nl = g->top + 1;
-  const bool mf = want_mf && g->dim == 3 && g->order == 1 && g->nc == 1;
+  // the matrix-free top level rebuilds A from the coefficients: not for uploaded matrices
+  const bool mf = want_mf && g->dim == 3 && g->order == 1 && g->nc == 1 && !g->uploaded;
   if (X.lv.empty()) {  // first use: allocate
     X.lv.assign(nl, Lev32{});
     X.A32.assign(nl, nullptr); X.om32.assign(nl, nullptr);
@@ -1386,6 +1475,8 @@ struct MixedVec {
   double *b64 = nullptr, *x64 = nullptr;  // base level in FP64
   double* z = nullptr;                    // preconditioned residual, FP64
 };
+
+static void mixed_vec_delete(MixedVec* m) { delete m; }
 
 static int mixed_vec_prepare(fmg_grid* g) {
   if (!g->mxv) g->mxv = new MixedVec();

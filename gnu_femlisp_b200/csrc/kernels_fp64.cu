@@ -1579,7 +1579,6 @@ k_jacobi0_3(const T* __restrict__ A, long long N, long long Np, int center, floa
   for (int e = 0; e < 9; ++e) B[e] = A[((long long)center * 9 + e) * Np + i];
   const T bb[3] = {b[3 * i], b[3 * i + 1], b[3 * i + 2]};
   block_solve3<T>(B, bb, t);
-#pragma unroll
   const T w = omega ? (T)omega[i] : (T)damp;
 #pragma unroll
   for (int k = 0; k < 3; ++k) x[3 * i + k] = w * t[k];

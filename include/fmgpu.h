@@ -141,6 +141,27 @@ int fmg_assemble(fmg_grid* grid);
 #define FMG_ASSEMBLE_REDISCRETIZE 0
 #define FMG_ASSEMBLE_GALERKIN 1
 int fmg_assemble_levels(fmg_grid* grid, int mode);
+/* Upload a level matrix assembled elsewhere: the parity path for matrices
+   Femlisp builds itself (assemble-interior with any coefficient functions,
+   fedisc.lisp:108-206; Galerkin products, geomg.lisp:122-123), handed over
+   in the compressed-column form of sparse-matrix->ccs (sparselu.lisp:226-263,
+   the form interface/superlu.c:51-88 takes) or as compressed rows.  Rows and
+   columns use the grid's numbering: node-major (dof = node * ncomp + comp),
+   nodes lexicographic with x fastest; n is the number of rows.  start has
+   n + 1 offsets, index / values start[n] entries; duplicate entries add up.
+   Every entry must lie in the level's Lagrange stencil (|offset| <= order per
+   direction; for Q2 also the element coupling), else FMG_ERR_ARG, except for
+   explicit zeros, which are dropped.  Dirichlet rows are taken as given.  A
+   hierarchy is complete, and solvable, once every level base..top has a
+   matrix (uploaded, or from an earlier assembly); the base level's LU is then
+   formed.  A grid with an uploaded matrix applies its mixed form through the
+   stored FP32 matrix, not matrix-free from the coefficients. */
+#define FMG_CSR 0
+#define FMG_CCS 1
+int fmg_set_matrix(fmg_grid* grid, int level, int layout, const int* start, const int* index,
+                   const double* values, long n);
+/* Top-level right-hand side (the rhs of an uploaded system); n = nodes * ncomp. */
+int fmg_set_rhs(fmg_grid* grid, const double* host, long n);
 /* Level matrix to the host, layout [slot][node] (debug / parity). */
 int fmg_get_matrix(fmg_grid* grid, int level, double* host);
 /* Top-level right-hand side (the assembled rhs of discretize-globally,

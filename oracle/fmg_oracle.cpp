@@ -1034,6 +1034,35 @@ int ora_assemble_levels(void* h, int mode) {
   return 0;
 }
 
+// Level matrices handed over from outside (the counterpart of fmg_set_matrix):
+// the slot layout of ora_get_matrix; ora_finish_levels then forms the coarse
+// inverse once every level is in place.
+int ora_set_matrix(void* h, int level, const double* a) {
+  Hier& H = *(Hier*)h;
+  if (level < H.base || level > H.top) return -1;
+  Level& L = H.lev[level];
+  L.A.assign(a, a + (size_t)H.nslots * H.nc * H.nc * L.N);
+  H.assembled = false;
+  return 0;
+}
+
+int ora_set_rhs(void* h, const double* b) {
+  Hier& H = *(Hier*)h;
+  H.rhs.assign(b, b + (size_t)H.lev[H.top].N * H.nc);
+  return 0;
+}
+
+int ora_finish_levels(void* h) {
+  Hier& H = *(Hier*)h;
+  for (int l = H.base; l <= H.top; ++l)
+    if (H.lev[l].A.size() != (size_t)H.nslots * H.nc * H.nc * H.lev[l].N) return -1;
+  if (H.rhs.size() != (size_t)H.lev[H.top].N * H.nc) H.rhs.assign((size_t)H.lev[H.top].N * H.nc, 0.0);
+  build_coarse_inverse(H);
+  H.assembled = true;
+  ensure_state(H);
+  return 0;
+}
+
 int ora_assemble(void* h) {
   Hier& H = *(Hier*)h;
   for (int l = H.top; l >= H.base; --l) {

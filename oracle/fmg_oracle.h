@@ -80,6 +80,9 @@ int ora_set_node_damping(void* h, int level, const double* w, long n);
 
 long ora_nnodes(void* h, int level);
 int ora_nslots(void* h);
+int ora_set_matrix(void* h, int level, const double* a);   /* level matrix in the ora_get_matrix layout */
+int ora_set_rhs(void* h, const double* b);                 /* top-level rhs */
+int ora_finish_levels(void* h);                            /* coarse inverse once every level is set */
 int ora_get_matrix(void* h, int level, double* out);      /* [slot][k][l][node] (nc x nc blocks) */
 int ora_get_rhs(void* h, double* out);
 int ora_get_coarse_inverse(void* h, double* out);           /* n*n row-major */

@@ -66,8 +66,10 @@ def lib():
         L.ora_nnodes.restype = ctypes.c_long
         L.ora_nnodes.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ora_nslots.argtypes = [ctypes.c_void_p]
-        for name in ("ora_get_matrix",):
+        for name in ("ora_get_matrix", "ora_set_matrix"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.ora_set_rhs.argtypes = [ctypes.c_void_p, _dp]
+        L.ora_finish_levels.argtypes = [ctypes.c_void_p]
         L.ora_get_rhs.argtypes = [ctypes.c_void_p, _dp]
         L.ora_get_coarse_inverse.argtypes = [ctypes.c_void_p, _dp]
         L.ora_matvec.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
@@ -149,6 +151,21 @@ class Oracle:
         rc = lib().ora_assemble_levels(self.h, 1 if galerkin else 0)
         if rc:
             raise RuntimeError(f"ora_assemble rc={rc}")
+        return self
+
+    def set_levels(self, mats, rhs):
+        """Level matrices given in the ``matrix()`` layout (a dict level ->
+        array) and the top-level rhs, then the coarse inverse."""
+        for level, a in mats.items():
+            a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+            assert a.size == self.nslots * self.nc * self.nc * self.nnodes(level)
+            assert lib().ora_set_matrix(self.h, level, _p(a)) == 0
+        b = np.ascontiguousarray(rhs, dtype=np.float64)
+        assert b.size == self.nnodes() * self.nc
+        assert lib().ora_set_rhs(self.h, _p(b)) == 0
+        rc = lib().ora_finish_levels(self.h)
+        if rc:
+            raise RuntimeError(f"ora_finish_levels rc={rc}")
         return self
 
     def nnodes(self, level=None):
