@@ -53,7 +53,7 @@ def parse_args():
                           "48^3 cells, FP64 CG + block-Jacobi V(2,2); each its own JSON line"))
     ap.add_argument("--c5-level", type=int, default=4, help="c5: 3 x 2^level cells per direction")
     ap.add_argument("--c4-fields", type=int, default=256)
-    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv"], default=None,
+    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv", "ssc"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
                          "the launch count, one more solve; net: the damping network on every level, 8 times; "
                          "c5: the elasticity setup, two mixed+learned solves, the launch count, one more; "
@@ -530,6 +530,29 @@ def run_profile_c5(args):
     print("launches_after", ctypes_count(C), "inner_iterations", ninner, flush=True)
 
 
+def run_profile_ssc(args):
+    """Geometric SSC sweeps on the C2 problem (3D Q2 Poisson) at `--level`:
+    the block factorisation once, then 4 sweeps (4 x 8 colour launches)."""
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.iteration import sample_at_gauss_points
+    C = G._capi
+    wl = problems.c2()
+    level = min(args.level, wl.level)
+    ctx = G.Context(0)
+    g = G.Grid(ctx, 3, 2, level, base_level=wl.base_level)
+    g.set_coefficient(C.FMG_F_IP, sample_at_gauss_points(wl.source, 3, 2, 1 << level))
+    g.assemble()
+    n = g.nnodes()
+    x, b, r = g.vector(), g.vector(values=g.rhs()), g.vector()
+    for _ in range(4):
+        g.ssc(x, b, r, 1.0)
+    ctx.synchronize()
+    print("launches", ctypes_count(C), "nodes", n, flush=True)
+    g.close()
+    ctx.close()
+
+
 def run_profile(args):
     """Workloads for ncu captures (profiles/ names the commands)."""
     import gnu_femlisp_b200 as G
@@ -538,6 +561,8 @@ def run_profile(args):
     C = G._capi
     if args.profile in ("c5", "c5mv"):
         return run_profile_c5(args)
+    if args.profile == "ssc":
+        return run_profile_ssc(args)
     wl = problems.c3(seed=0, level=args.level)
     ctx = G.Context(0)
     g = G.Grid(ctx, 3, 1, wl.level, base_level=wl.base_level)
@@ -635,9 +660,25 @@ def run_c2(args):
     for _ in range(3):
         g.matvec(P, Y)
     t_mv, _ = timed(lambda: g.matvec(P, Y), args.matvec_reps)
+    # the reference's own default smoother for Q2 (select-smoother,
+    # geomg.lisp:48-60): the vertex-centred geometric SSC, V(1,1), omega 1
+    cfg_ssc = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_SSC, 1.0, 1, 1, 1, 0, 1.0, wl.rtol, 0.0, 200,
+                         C.FMG_MULTIPLICATIVE)
+
+    def solve_ssc():
+        x.fill(0.0)
+        return g.solve(cfg_ssc, x)
+    solve_ssc()
+    t_ssc, (hist_ssc, cycles_ssc, status_ssc) = timed(solve_ssc, args.steps)
+    one_ssc = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_SSC, 1.0, 1, 1, 1, 0, 1.0, 0.0, 0.0, 1, C.FMG_MULTIPLICATIVE)
+    g.vcycle(one_ssc, X, B, R)
+    t_cycle_ssc, _ = timed(lambda: g.vcycle(one_ssc, X, B, R), 5)
     clk = clocks.stop()
     if status != 0:
         raise RuntimeError(f"C2 solve did not converge in {cycles} cycles")
+    ssc = {"solver": "MG iteration, V(1,1) geometric SSC (vertex-centred 3^3 blocks, omega 1)",
+           "time_to_solution_s": t_ssc, "cycles": int(cycles_ssc), "status": int(status_ssc),
+           "vcycle_ms": t_cycle_ssc * 1e3, "history_tail": [float(v) for v in hist_ssc[-2:]]}
     nnz = (8 * wl.n_cells + 1) ** 3
     alg_bytes = 8 * nnz + 16 * n
     peak, peak_kind = measured_peaks()
@@ -679,7 +720,7 @@ def run_c2(args):
                          "kernel": "k_spmv<3,2> (top-level FP64 Q2 matvec)", "peak_kind": peak_kind,
                          "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
             "cpu_baseline": cpu, "clocks": clk,
-            "history_tail": [float(v) for v in hist[-3:]]}
+            "history_tail": [float(v) for v in hist[-3:]], "ssc": ssc}
     print(json.dumps(line), flush=True)
 
 

@@ -214,6 +214,10 @@ class Grid:
     def sor(self, x: "Vector", b: "Vector", r: "Vector", omega: float):
         self.ctx.check(self._lib.fmg_sor(self.h, x.level, omega, x.h, b.h, r.h), "sor")
 
+    def ssc(self, x: "Vector", b: "Vector", r: "Vector", omega: float = 1.0):
+        """One <geometric-ssc> sweep (vertex-centred blocks); b may be r."""
+        self.ctx.check(self._lib.fmg_ssc(self.h, x.level, omega, x.h, b.h, r.h), "ssc")
+
     def coarse_solve(self, x: "Vector", r: "Vector", damp: float = 1.0):
         self.ctx.check(self._lib.fmg_coarse_solve(self.h, damp, x.h, r.h), "coarse_solve")
 

@@ -80,6 +80,11 @@ struct fmg_grid {
   bool assembled_once = false;
   std::vector<char> have;      // levels whose matrix is in place
   bool uploaded = false;       // some level matrix came from fmg_set_matrix
+  // <geometric-ssc>: LU factors of the vertex blocks per level, formed once per assembly
+  std::vector<double*> sscF;
+  std::vector<unsigned char*> sscP;
+  std::vector<long long> sscEpoch;
+  bool ssc_unprepared = false; // a sweep found no factors (and was not run)
   long long epoch = 0;         // incremented by every assembly
   struct MixedState* mx = nullptr;
   struct MixedVec* mxv = nullptr;  // mixed solve state of the vector (elasticity) form
@@ -385,6 +390,20 @@ struct MG {
         need = true;          // the product-iterator recomputes after every step
       }
       if (steps > 1 && (literal || alias(l))) residual(l);
+    } else if (c.smoother == FMG_SSC) {
+      // residual-before t, residual-after nil (blockit.lisp:118-204): the
+      // block sweep reads b and x only, so the residuals of ensure-mg-residual
+      // and of the product-iterator matter only where they are seen (a
+      // user's r) or where r is b (the alias inside <cg>)
+      const bool keep = literal || alias(l);
+      const bool ready = g->order == 1 || ((int)g->sscF.size() > l && g->sscF[l] && g->sscEpoch[l] == g->epoch);
+      if (!ready) { g->ssc_unprepared = true; g->rp[l] = 0; return; }
+      if (keep) ensure_res();
+      for (int s = 0; s < steps; ++s) {
+        launch_ssc(view(g, l), c.damp, g->solp[l], g->rhsp[l], g->resp[l], g->order == 2 ? g->sscF[l] : nullptr,
+                   g->order == 2 ? g->sscP[l] : nullptr, st);
+        if (steps > 1 && keep) residual(l);
+      }
     } else {
       for (int s = 0; s < steps; ++s) launch_sor(view(g, l), c.damp, g->solp[l], g->rhsp[l], g->resp[l], st);
     }
@@ -460,11 +479,35 @@ struct MG {
   }
 };
 
+// the LU factors of the vertex blocks of level l (scalar Q2) for the SSC
+// sweeps, formed once per assembly
+int ssc_prepare(fmg_grid* g, int l) {
+  if ((int)g->sscF.size() != g->top + 1) {
+    g->sscF.assign(g->top + 1, nullptr);
+    g->sscP.assign(g->top + 1, nullptr);
+    g->sscEpoch.assign(g->top + 1, -1);
+  }
+  const LevelView v = view(g, l);
+  const long long nb = ssc_blocks(v);
+  if (nb == 0 || g->sscEpoch[l] == g->epoch) return FMG_OK;
+  const int bs = ssc_block_size(g->dim);
+  int rc;
+  if (!g->sscF[l]) {
+    double* p = nullptr;
+    if ((rc = dalloc(g, &g->sscF[l], nb * bs * bs)) || (rc = dalloc(g, &p, (nb * bs + 7) / 8))) return rc;
+    g->sscP[l] = (unsigned char*)p;
+  }
+  launch_ssc_factor(v, g->sscF[l], g->sscP[l], g->ctx->stream);
+  if ((rc = launched(g->ctx, "ssc factor"))) return rc;
+  g->sscEpoch[l] = g->epoch;
+  return FMG_OK;
+}
+
 int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (!c) return set_err(g->ctx, FMG_ERR_ARG, "null configuration");
   if (g->nc != 1 && c->smoother != FMG_JACOBI)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "3-component grids: the (block) Jacobi smoother only");
-  if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR)
+  if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR && c->smoother != FMG_SSC)
     return set_err(g->ctx, FMG_ERR_ARG, "unknown smoother %d", c->smoother);
   if (c->pre_steps < 0 || c->post_steps < 0 || c->gamma < 0 || c->gamma > 4)
     return set_err(g->ctx, FMG_ERR_ARG, "bad cycle parameters");
@@ -473,6 +516,13 @@ int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (c->method < FMG_METHOD_MG || c->method > FMG_METHOD_CG)
     return set_err(g->ctx, FMG_ERR_ARG, "bad method");
   if (c->fmg != 0 && c->fmg != 1) return set_err(g->ctx, FMG_ERR_ARG, "fmg is 0 or 1");
+  if (c->smoother == FMG_SSC) {  // factors of every smoothed level before the cycle runs
+    g->ssc_unprepared = false;
+    for (int l = g->base + 1; l <= g->top; ++l) {
+      const int rc = ssc_prepare(g, l);
+      if (rc) return rc;
+    }
+  }
   return FMG_OK;
 }
 
@@ -1060,6 +1110,18 @@ int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
   return launched(g->ctx, "sor");
 }
 
+int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric SSC: scalar grids");
+  if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level) || x == b || x == r)
+    return FMG_ERR_ARG;
+  int rc = ssc_prepare(g, level);
+  if (rc) return rc;
+  launch_ssc(view(g, level), omega, x->d, b->d, r->d, g->order == 2 ? g->sscF[level] : nullptr,
+             g->order == 2 ? g->sscP[level] : nullptr, g->ctx->stream);
+  return launched(g->ctx, "ssc");
+}
+
 int fmg_coarse_solve(fmg_grid* g, double damp, fmg_vec* x, fmg_vec* r) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, g->base) || vec_check(r, g, g->base)) return FMG_ERR_ARG;
@@ -1078,6 +1140,7 @@ int fmg_vcycle(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fm
   double* sp = g->xs;
   mg.iterate(&xp, &sp, b->d, r->d);
   if (xp != x->d) launch_copy(xp, x->d, x->n, g->ctx->stream);
+  if (g->ssc_unprepared) return set_err(g->ctx, FMG_ERR_STATE, "SSC factors missing");
   return launched(g->ctx, "vcycle");
 }
 
@@ -1199,6 +1262,7 @@ int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, 
   if (!hidden.empty())
     for (size_t l = 0; l < g->lev.size(); ++l) g->lev[l].omega = hidden[l];
   FMG_CK(c, cudaStreamSynchronize(st));
+  if (g->ssc_unprepared) return set_err(c, FMG_ERR_STATE, "SSC factors missing");
   return launched(c, "solve");
 }
 

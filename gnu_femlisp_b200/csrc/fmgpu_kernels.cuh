@@ -71,6 +71,15 @@ void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool w
 void launch_jacobi_res(const LevelView& L, double damp, const double* x, const double* b, double* xout,
                        double* r, bool write_r, const double* dv, const Reduce* R, cudaStream_t st);
 void launch_sor(const LevelView& L, double omega, double* x, const double* b, double* r, cudaStream_t st);
+// <geometric-ssc>: the number of vertex blocks of a Q2 level (0 for Q1, whose
+// blocks are single nodes), the block size 3^dim, the LU factors of every
+// block (F: blocks x size^2 doubles, P: blocks x size bytes), and one sweep
+// with them (b may be r)
+long long ssc_blocks(const LevelView& L);
+int ssc_block_size(int dim);
+void launch_ssc_factor(const LevelView& L, double* F, unsigned char* P, cudaStream_t st);
+void launch_ssc(const LevelView& L, double omega, double* x, const double* b, double* r, const double* F,
+                const unsigned char* P, cudaStream_t st);
 void launch_restrict(const LevelView& F, const LevelView& C, const double* rf, double* rc, double* rhsc,
                      double* solc, cudaStream_t st);
 void launch_prolong(const LevelView& C, const LevelView& F, const double* xc, double* xf, cudaStream_t st);

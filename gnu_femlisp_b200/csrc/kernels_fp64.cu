@@ -463,8 +463,11 @@ k_jacobi_res(const double* __restrict__ A, long long N, long long Np, long long 
   if (DOT) dr_finish(acc, R, smem);
 }
 
-// one colour of the multicolour <sor> sweep: rows with (i_k mod (P+1)) = col_k
-template <int D, int P>
+// one colour of the multicolour <sor> sweep: rows with (i_k mod (P+1)) = col_k.
+// SSC: the <geometric-ssc> sweep of a Q1 level, whose vertex blocks hold one
+// node -- the same update, with r keeping the unscaled residual
+// (blockit.lisp:131-138) instead of the <sor> correction (linit.lisp:312-322)
+template <int D, int P, bool SSC = false>
 __global__ void __launch_bounds__(kBlock)
 k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long M, int colour,
              double omega_s, const double* __restrict__ omega, double* x, const double* b, double* r,
@@ -502,9 +505,219 @@ k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long 
       s = fma(a, x[clampi(i + o, N)], s);
     }
   }
-  const double tt = (b[i] - s) / d;
-  r[i] = tt;
+  const double rr = b[i] - s;
+  const double tt = rr / d;
+  r[i] = SSC ? rr : tt;
   x[i] = fma(omega ? omega[i] : omega_s, tt, x[i]);
+}
+
+// Step K of the warp's LU factorisation of a vertex block (rows in lanes):
+// the pivot is the first position holding the largest magnitude, the lane at
+// position K and the pivot's lane exchange positions (the rows stay put), the
+// rows below keep their multiplier in column K.  The recursion keeps every
+// index a compile-time constant, so the row stays in registers.
+template <int NB, int K>
+__device__ __forceinline__ void ssc_lu_step(double (&a)[NB], int& pos, int lane) {
+  if constexpr (K < NB) {
+    constexpr unsigned FULL = 0xffffffffu;
+    double val = (lane < NB && pos >= K) ? fabs(a[K]) : -1.0;
+    int key = pos, ln = lane;
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+      const double ov = __shfl_xor_sync(FULL, val, m);
+      const int ok = __shfl_xor_sync(FULL, key, m);
+      const int ol = __shfl_xor_sync(FULL, ln, m);
+      if (ov > val || (ov == val && ok < key)) { val = ov; key = ok; ln = ol; }
+    }
+    if (pos == K) pos = key;  // row interchange
+    if (lane == ln) pos = K;
+    const double piv = __shfl_sync(FULL, a[K], ln);
+    const double rcp = 1.0 / piv;
+    const bool below = lane < NB && pos > K;
+    const double mlt = a[K] * rcp;
+#pragma unroll
+    for (int j = K + 1; j < NB; ++j) {
+      const double pj = __shfl_sync(FULL, a[j], ln);
+      if (below) a[j] = a[j] - mlt * pj;
+    }
+    if (below) a[K] = mlt;
+    ssc_lu_step<NB, K + 1>(a, pos, lane);
+  }
+}
+
+// Column K of the forward substitution with the stored unit lower factor:
+// the row at position K is final, the rows below subtract their multiplier
+// times it (the operations, in order, of carrying the right-hand side
+// through the elimination).
+template <int NB, int K>
+__device__ __forceinline__ void ssc_fwd_step(const double (&a)[NB], double& rr, int pos, int lane) {
+  if constexpr (K < NB) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const unsigned who = __ballot_sync(FULL, lane < NB && pos == K);
+    const double rk = __shfl_sync(FULL, rr, __ffs(who) - 1);
+    if (lane < NB && pos > K) rr = rr - a[K] * rk;
+    ssc_fwd_step<NB, K + 1>(a, rr, pos, lane);
+  }
+}
+
+// Column K of the backward substitution: the lane at position K divides,
+// the rows above subtract; the lane of member K keeps the solution.
+template <int NB, int K>
+__device__ __forceinline__ void ssc_back_step(const double (&a)[NB], double& rr, int pos, int lane, double& corr) {
+  if constexpr (K >= 0) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const unsigned who = __ballot_sync(FULL, lane < NB && pos == K);
+    const int kl = __ffs(who) - 1;
+    const double xk = __shfl_sync(FULL, rr / a[K], kl);
+    if (lane < NB && pos < K) rr = rr - xk * a[K];
+    if (lane == K) corr = xk;
+    ssc_back_step<NB, K - 1>(a, rr, pos, lane, corr);
+  }
+}
+
+// Member `lane` of the vertex block of vertex v (2 x vertex index): its node
+// coordinates and offsets, whether it is in the domain, and whether it is a
+// member of the block (the vertex itself, or a non-Dirichlet node).
+template <int D>
+struct SscMember {
+  int dm[3], c[3];
+  bool real;
+};
+
+template <int D>
+__device__ __forceinline__ SscMember<D> ssc_member(const int v[3], int lane, int Mi, int dmask) {
+  constexpr int NB = D == 1 ? 3 : (D == 2 ? 9 : 27);
+  SscMember<D> m;
+  bool in = lane < NB, dir = false;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { m.dm[k] = 0; m.c[k] = v[k]; }
+#pragma unroll
+  for (int k = 0, q = lane; k < D; ++k, q /= 3) {
+    m.dm[k] = q % 3 - 1;
+    m.c[k] = v[k] + m.dm[k];
+    in = in && m.c[k] >= 0 && m.c[k] < Mi;
+    dir = dir || (m.c[k] == 0 && ((dmask >> (2 * k)) & 1)) || (m.c[k] == Mi - 1 && ((dmask >> (2 * k + 1)) & 1));
+  }
+  m.real = in && (lane == NB / 2 || !dir);
+  return m;
+}
+
+// The LU factors of every vertex block of a scalar Q2 level (all colours in
+// one launch), for the <geometric-ssc> sweeps: the local matrix A_BB
+// (blockit.lisp:150-153) gathered by the member lanes -- every entry lies in
+// a pattern-0 slot: a row that is odd along a direction meets the box only
+// within +-1 there -- members outside the domain, and Dirichlet members
+// other than the vertex, as identity rows with zero columns (the pivots and
+// the arithmetic of the real rows are those of the compact block), then
+// factored as by gesv! (right-looking, partial pivoting).  The factors depend
+// on the matrix only, so a sweep that reuses them repeats exactly the
+// operations of factoring afresh.  Layout: F[block][k][member], the row's
+// final position in P[block][member]; block = lexicographic vertex index.
+template <int D>
+__global__ void __launch_bounds__(128)
+k_ssc_factor_q2(const double* __restrict__ A, long long Np, long long M, int dmask, double* F, unsigned char* P,
+                const __grid_constant__ Q2Layout lay) {
+  constexpr int NB = D == 1 ? 3 : (D == 2 ? 9 : 27);
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // uniform per warp
+  const int Mi = (int)M;
+  const int nv = (Mi + 1) / 2;
+  const long long nblk = D == 1 ? nv : (D == 2 ? (long long)nv * nv : (long long)nv * nv * nv);
+  if (w >= nblk) return;  // the whole warp leaves together
+  const int wi = (int)w;
+  const int v[3] = {2 * (wi % nv), D > 1 ? 2 * ((wi / nv) % nv) : 0, D > 2 ? 2 * (wi / (nv * nv)) : 0};
+  const SscMember<D> mb = ssc_member<D>(v, lane, Mi, dmask);
+  const unsigned realmask = __ballot_sync(FULL, mb.real);
+  double a[NB];
+  if (mb.real) {
+    const long long cl[3] = {mb.c[0], mb.c[1], mb.c[2]};
+    Q2Base<D> qb;
+    q2_base<D, true, true>(lay, cl, M, qb);
+    const long long p0 = qb.p[0];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      bool near = true;
+      int sl = 0;
+#pragma unroll
+      for (int k = 0, q = u, m5 = 1; k < D; ++k, q /= 3, m5 *= 5) {
+        const int o = (q % 3 - 1) - mb.dm[k];
+        near = near && o >= -1 && o <= 1;
+        sl += (o + 2) * m5;
+      }
+      a[u] = (near && ((realmask >> u) & 1)) ? A[(long long)sl * Np + p0] : 0.0;
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < NB; ++u) a[u] = (u == lane) ? 1.0 : 0.0;
+  }
+  int pos = lane;  // lanes >= NB are never candidates
+  ssc_lu_step<NB, 0>(a, pos, lane);
+  if (lane < NB) {
+    double* f = F + w * NB * NB + lane;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) f[k * NB] = a[k];
+    P[w * NB + lane] = (unsigned char)pos;
+  }
+}
+
+// One colour of the <geometric-ssc> sweep on a scalar Q2 level
+// (blockit.lisp:118-204 with the vertex-centred blocks of geoblock.lisp:72-158):
+// a warp per vertex block, lane t holding member t of the 3^D box around the
+// vertex (x fastest).  Each member lane forms its row's residual r = b - A x
+// (b may alias r: the alias inside <cg>), then the warp solves A_BB c = r_B
+// with the stored factors (forward in position order, backward column by
+// column) and x_B += omega c.  Blocks of one colour (vertex index mod 2 per
+// direction) share no node and read no unknown another one writes.
+template <int D>
+__global__ void __launch_bounds__(128)
+k_ssc_q2(const double* __restrict__ A, long long N, long long Np, long long M, int dmask, int colour,
+         double omega, double* x, const double* b, double* r, const double* __restrict__ F,
+         const unsigned char* __restrict__ P, const __grid_constant__ Q2Layout lay) {
+  constexpr int NB = D == 1 ? 3 : (D == 2 ? 9 : 27);
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // uniform per warp
+  const int Mi = (int)M;
+  const int nv = (Mi + 1) / 2;  // vertices per direction
+  const int bx = colour & 1, by = (colour >> 1) & 1, bz = (colour >> 2) & 1;
+  const int ex = (nv - bx + 1) / 2, ey = D > 1 ? (nv - by + 1) / 2 : 1, ez = D > 2 ? (nv - bz + 1) / 2 : 1;
+  if (w >= (long long)ex * ey * ez) return;  // the whole warp leaves together
+  const int wi = (int)w;
+  const int jx = wi % ex, jq = wi / ex, jy = jq % ey, jz = jq / ey;
+  const int ax = bx + 2 * jx, ay = D > 1 ? by + 2 * jy : 0, az = D > 2 ? bz + 2 * jz : 0;
+  const int v[3] = {2 * ax, 2 * ay, 2 * az};
+  const long long blk = ax + (long long)nv * (ay + (long long)nv * az);
+  const SscMember<D> mb = ssc_member<D>(v, lane, Mi, dmask);
+  double a[NB];
+  int pos = lane;
+  if (lane < NB) {
+    const double* f = F + blk * NB * NB + lane;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) a[k] = __ldg(f + k * NB);
+    pos = P[blk * NB + lane];
+  } else {
+#pragma unroll
+    for (int k = 0; k < NB; ++k) a[k] = 0.0;
+  }
+  const long long i = mb.real ? (long long)mb.c[0] + M * ((long long)mb.c[1] + M * (long long)mb.c[2]) : 0;
+  double rr = 0.0;
+  if (mb.real) {
+    const long long cl[3] = {mb.c[0], mb.c[1], mb.c[2]};
+    Q2Base<D> qb;
+    q2_base<D, true, true>(lay, cl, M, qb);
+    double s = 0.0;
+    q2_visit<D, true>(qb, M, [&](int k, long long o, long long p, bool st) {
+      double av = A[(long long)k * Np + p];
+      av = st ? av : 0.0;
+      s = fma(av, x[clampi(i + o, N)], s);
+    });
+    rr = b[i] - s;
+    r[i] = rr;
+  }
+  ssc_fwd_step<NB, 0>(a, rr, pos, lane);
+  double corr = 0.0;
+  ssc_back_step<NB, NB - 1>(a, rr, pos, lane, corr);
+  if (mb.real) x[i] = fma(omega, corr, x[i]);
 }
 
 // -------------------------------------------------------------- transfers
@@ -1719,6 +1932,53 @@ void launch_sor(const LevelView& L, double omega, double* x, const double* b, do
     if (L.dim > 2) cnt *= (L.M - cz + Q - 1) / Q;
     FMG_DISPATCH(L.dim, L.order, {
       k_sor_colour<D, P><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, L.omega, x, b, r, lay);
+    });
+  }
+}
+
+long long ssc_blocks(const LevelView& L) {
+  if (L.order != 2) return 0;
+  long long nv = (L.M + 1) / 2, n = 1;
+  for (int k = 0; k < L.dim; ++k) n *= nv;
+  return n;
+}
+
+int ssc_block_size(int dim) { return dim == 1 ? 3 : (dim == 2 ? 9 : 27); }
+
+void launch_ssc_factor(const LevelView& L, double* F, unsigned char* P, cudaStream_t st) {
+  if (L.order != 2) return;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const Q2Layout lay = q2_layout(L.dim, L.M);
+  const unsigned grid = (unsigned)((ssc_blocks(L) * 32 + 127) / 128);
+  Q2_DISPATCH(L.dim, { k_ssc_factor_q2<D><<<grid, 128, 0, st>>>(L.A, L.Np, L.M, L.dmask, F, P, lay); });
+}
+
+void launch_ssc(const LevelView& L, double omega, double* x, const double* b, double* r, const double* F,
+                const unsigned char* P, cudaStream_t st) {
+  const int ncol = 1 << L.dim;
+  g_launches.fetch_add(ncol, std::memory_order_relaxed);
+  if (L.order == 1) {  // one-node blocks: the colour sweep of the SOR with the SSC residual
+    for (int col = 0; col < ncol; ++col) {
+      const int cx = col & 1, cy = (col >> 1) & 1, cz = (col >> 2) & 1;
+      long long cnt = (L.M - cx + 1) / 2;
+      if (L.dim > 1) cnt *= (L.M - cy + 1) / 2;
+      if (L.dim > 2) cnt *= (L.M - cz + 1) / 2;
+      Q1_DISPATCH(L.dim, {
+        k_sor_colour<D, 1, true><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, nullptr, x, b, r,
+                                                                  Q2Layout{});
+      });
+    }
+    return;
+  }
+  const Q2Layout lay = q2_layout(L.dim, L.M);
+  const long long nv = (L.M + 1) / 2;
+  for (int col = 0; col < ncol; ++col) {
+    long long cnt = (nv - (col & 1) + 1) / 2;
+    if (L.dim > 1) cnt *= (nv - ((col >> 1) & 1) + 1) / 2;
+    if (L.dim > 2) cnt *= (nv - ((col >> 2) & 1) + 1) / 2;
+    const unsigned grid = (unsigned)((cnt * 32 + 127) / 128);
+    Q2_DISPATCH(L.dim, {
+      k_ssc_q2<D><<<grid, 128, 0, st>>>(L.A, L.N, L.Np, L.M, L.dmask, col, omega, x, b, r, F, P, lay);
     });
   }
 }

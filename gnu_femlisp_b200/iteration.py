@@ -166,6 +166,18 @@ class GaussSeidel(SOR):
 
 
 @dataclass
+class GeometricSSC:
+    """(geometric-ssc) -- successive subspace correction over the
+    vertex-centred blocks (geoblock.lisp:37-158, blockit.lisp:118-204): the
+    default smoother of higher-order discretisations (geomg.lisp:48-60)."""
+    omega: float = 1.0
+
+
+def geometric_ssc(**kw) -> GeometricSSC:
+    return GeometricSSC(**kw)
+
+
+@dataclass
 class LU:
     damp: float = 1.0
 
@@ -256,7 +268,7 @@ class SolveReport:
     extra: dict = field(default_factory=dict)
 
 
-def make_cfg(iteration, success_if: str, failure_if: str) -> tuple[C.SolveCfg, int, bool]:
+def make_cfg(iteration, success_if: str, failure_if: str, order: int = 1) -> tuple[C.SolveCfg, int, bool]:
     cs = iteration.preconditioner if isinstance(iteration, CG) else iteration
     cfg = C.SolveCfg()
     if isinstance(iteration, CG):
@@ -266,9 +278,12 @@ def make_cfg(iteration, success_if: str, failure_if: str) -> tuple[C.SolveCfg, i
         cfg.method = C.FMG_METHOD_MG
     base = 0
     if cs is not None:
-        sm = cs.smoother or GaussSeidel()
+        # select-smoother (geomg.lisp:48-60): Gauss-Seidel for order 1, SSC above
+        sm = cs.smoother or (GaussSeidel() if order == 1 else GeometricSSC())
         if isinstance(sm, Jacobi):
             cfg.smoother, cfg.damp = C.FMG_JACOBI, sm.damp
+        elif isinstance(sm, GeometricSSC):
+            cfg.smoother, cfg.damp = C.FMG_SSC, sm.omega
         elif isinstance(sm, SOR):
             cfg.smoother, cfg.damp = C.FMG_SOR, sm.omega
         else:
@@ -294,7 +309,7 @@ def solve(blackboard: dict) -> dict:
     blackboard with :solution, :report and :history filled in."""
     A: DiscreteSystem = blackboard["matrix"]
     solver: LinearSolver = blackboard["solver"]
-    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if)
+    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if, A.fe.order)
     g = A.grid(base)
     x = g.vector()
     if "solution" in blackboard and blackboard["solution"] is not None:

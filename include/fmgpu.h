@@ -53,6 +53,8 @@ extern "C" {
 /* ------------------------------------------------------------ iteration */
 #define FMG_JACOBI 0            /* <jacobi> :damp (linit.lisp:220-250) */
 #define FMG_SOR 1               /* <sor> :omega, colour ordering (linit.lisp:288-323) */
+#define FMG_SSC 2               /* (geometric-ssc) :omega, vertex-centred blocks (geoblock.lisp:37-158,
+                                   blockit.lisp:118-204); scalar grids */
 
 #define FMG_METHOD_MG 0         /* <linear-solver> :iteration <geometric-cs> */
 #define FMG_METHOD_CG_MG 1      /* <cg> :preconditioner <geometric-cs> */
@@ -70,7 +72,7 @@ typedef struct fmg_vec fmg_vec;
    forms of <linear-solver> (iterate.lisp:105-123). */
 typedef struct {
   int method;          /* FMG_METHOD_* */
-  int smoother;        /* FMG_JACOBI or FMG_SOR */
+  int smoother;        /* FMG_JACOBI, FMG_SOR or FMG_SSC */
   double damp;         /* :damp of <jacobi>, :omega of <sor> */
   int pre_steps, post_steps, gamma;
   int compat_alias;    /* 1: the preconditioner is called as (iterate q w w),
@@ -201,6 +203,14 @@ int fmg_prolongate(fmg_grid* grid, int coarse_level, const fmg_vec* xc, fmg_vec*
 int fmg_jacobi(fmg_grid* grid, int level, double damp, fmg_vec* x, fmg_vec* r);
 /* one multicolour <sor> sweep (linit.lisp:288-323); b may be r */
 int fmg_sor(fmg_grid* grid, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r);
+/* one (geometric-ssc) sweep (blockit.lisp:118-204) over the vertex-centred
+   blocks of geoblock.lisp:72-158 -- on the structured grid the 3^d box of
+   nodes around each even node (Q2), the node alone (Q1), Dirichlet members
+   other than the vertex left out: per block r_B := b_B - (A x)_B, the dense
+   local system solved by LU with partial pivoting, x_B += omega c.  Blocks in
+   colour order (vertex index mod 2 per direction), lexicographic within a
+   colour; b may be r (the alias inside <cg>). */
+int fmg_ssc(fmg_grid* grid, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r);
 /* the <lu> coarse-grid iteration on the base level: r := A^-1 r,
    x := x + damp r (linit.lisp:156-161) */
 int fmg_coarse_solve(fmg_grid* grid, double damp, fmg_vec* x, fmg_vec* r);

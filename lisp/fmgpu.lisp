@@ -27,10 +27,13 @@
 (defconstant +fmg-f-ip+ 3)
 (defconstant +fmg-jacobi+ 0)
 (defconstant +fmg-sor+ 1)
+(defconstant +fmg-ssc+ 2)
 (defconstant +fmg-method-mg+ 0)
 (defconstant +fmg-method-cg-mg+ 1)
 (defconstant +fmg-multiplicative+ 0)
 (defconstant +fmg-additive+ 1)
+(defconstant +fmg-csr+ 0)
+(defconstant +fmg-ccs+ 1)
 
 ;;;; foreign functions (handles are passed as (* :char) pointers)
 
@@ -69,6 +72,15 @@
 (fl.port:def-function ("fmg_solve" fmg-solve)
     ((grid (* :char)) (cfg (* :char)) (x (* :char))
      (hist (* :double)) (hist-len :int) (nsteps (* :int)) (status (* :int)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_set_matrix" fmg-set-matrix)
+    ((grid (* :char)) (level :int) (layout :int) (starts (* :int)) (indices (* :int))
+     (values (* :double)) (n :long))
+  :returning :int)
+
+(fl.port:def-function ("fmg_set_rhs" fmg-set-rhs)
+    ((grid (* :char)) (values (* :double)) (n :long))
   :returning :int)
 
 (defun check (status what)
@@ -141,3 +153,32 @@ x fastest) and the :defnorm history."
              (sol (make-array n :element-type 'double-float)))
         (check (fl.port:foreign-call #'fmg-vec-get (aref x 0) sol n) "fmg_vec_get")
         (values sol (subseq hist 0 (1+ (aref nsteps 0))))))))
+
+;;;; matrices Femlisp assembled itself
+
+(defun lexicographic-keys (matrix)
+  "The row keys of MATRIX in the library's node order: by the midpoint of the
+key's cell, last coordinate slowest (the numbering of sparse-matrix->ccs is
+the order of the keys it is given, sparselu.lisp:226-233)."
+  (let ((keys (coerce (fl.matlisp:row-keys matrix) 'vector)))
+    (flet ((mid (key) (fl.mesh:midpoint (fl.mesh:representative key))))
+      (sort keys (lambda (a b)
+                   (let ((pa (mid a)) (pb (mid b)))
+                     (loop for k from (1- (length pa)) downto 0
+                           when (< (aref pa k) (aref pb k)) return t
+                           when (> (aref pa k) (aref pb k)) return nil
+                           finally (return nil))))))))
+
+(defun upload-level-matrix (grid level matrix)
+  "Hands the level matrix MATRIX (a <sparse-matrix> of the structured
+hierarchy, constraints eliminated) to the library through fmg_set_matrix in
+the compressed-column form of sparse-matrix->ccs."
+  (let* ((keys (lexicographic-keys matrix))
+         (ccs (fl.matlisp:sparse-matrix->ccs matrix :keys keys))
+         (pattern (fl.matlisp:pattern ccs))
+         (starts (slot-value pattern 'fl.matlisp::starts))
+         (indices (slot-value pattern 'fl.matlisp::indices))
+         (n (1- (length starts))))
+    (check (fl.port:foreign-call #'fmg-set-matrix grid level +fmg-ccs+ starts indices
+                                 (fl.matlisp:store ccs) n)
+           "fmg_set_matrix")))

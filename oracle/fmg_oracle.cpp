@@ -671,6 +671,109 @@ void sor(const Hier& H, int l, double omega, double* x, const double* b, double*
   }
 }
 
+// <geometric-ssc> with vertex-centred blocks (geoblock.lisp:37-158,
+// blockit.lisp:118-204), one sweep.  The block of a vertex is the vertex and
+// every non-Dirichlet degree of freedom whose subcell contains it
+// (find-vertex-centered-block, geoblock.lisp:72-100): on the structured grid
+// the 3^d box of nodes around an even node for Q2, the node alone for Q1.
+// For each block in turn: r_k := b_k - sum_j A_kj x_j on its rows (b may be r,
+// the alias inside <cg>), the local system A_BB c = r_B solved by LU with
+// partial pivoting, x_B += omega c (blockit.lisp:131-180).
+// Order: vertices by colour (vertex index mod 2 per direction, colours
+// ascending), lexicographic inside a colour; blocks of one colour neither
+// share nodes nor read each other's unknowns, so they run in any order.
+// The block is kept as the full box: members outside the domain or
+// Dirichlet (other than the vertex) become identity rows and zero columns,
+// which leaves every pivot choice and every operation on the real rows as in
+// the compact block.  LU: right-looking, row interchanges to the first
+// position holding the largest magnitude, multipliers scaled by the pivot's
+// reciprocal, no fused multiply-adds (the dgetf2 + dgetrs sequence of gesv!).
+void ssc_block(const Hier& H, const Level& L, const long v[3], double omega, double* x, const double* b,
+               double* r) {
+  const int D = H.dim;
+  const int NB = H.order == 2 ? (D == 1 ? 3 : D == 2 ? 9 : 27) : 1;
+  const int centre = NB / 2;
+  long node[27];
+  bool real[27];
+  long cn[27][3];
+  for (int u = 0; u < NB; ++u) {
+    int t = u;
+    bool in = true;
+    for (int k = 0; k < 3; ++k) {
+      const long d = (k < D && NB > 1) ? (t % 3) - 1 : 0;
+      if (k < D && NB > 1) t /= 3;
+      cn[u][k] = v[k] + d;
+      if (k < D && (cn[u][k] < 0 || cn[u][k] >= L.M)) in = false;
+    }
+    real[u] = in && (u == centre || !is_dirichlet(H, L.M, cn[u]));
+    node[u] = in ? cn[u][0] + L.M * (cn[u][1] + L.M * cn[u][2]) : -1;
+  }
+  double a[27][27], rr[27];
+  for (int t = 0; t < NB; ++t) {
+    if (!real[t]) {
+      for (int u = 0; u < NB; ++u) a[t][u] = u == t ? 1.0 : 0.0;
+      rr[t] = 0.0;
+      continue;
+    }
+    const long i = node[t];
+    rr[t] = b[i] - row_sum(H, L, i, x);
+    r[i] = rr[t];
+    for (int u = 0; u < NB; ++u) {
+      if (!real[u]) { a[t][u] = 0.0; continue; }
+      long o[3] = {0, 0, 0};
+      bool near = true;
+      for (int k = 0; k < D; ++k) {
+        o[k] = cn[u][k] - cn[t][k];
+        if (o[k] < -H.span || o[k] > H.span) near = false;
+      }
+      a[t][u] = near ? L.A[(size_t)slot_of(H, o) * L.N + i] : 0.0;
+    }
+  }
+  for (int k = 0; k < NB; ++k) {
+    int p = k;
+    double amax = std::fabs(a[k][k]);
+    for (int i = k + 1; i < NB; ++i)
+      if (std::fabs(a[i][k]) > amax) { amax = std::fabs(a[i][k]); p = i; }
+    if (p != k) {
+      for (int j = 0; j < NB; ++j) std::swap(a[k][j], a[p][j]);
+      std::swap(rr[k], rr[p]);
+    }
+    const double rcp = 1.0 / a[k][k];
+    for (int i = k + 1; i < NB; ++i) {
+      const double m = a[i][k] * rcp;
+      a[i][k] = m;
+      for (int j = k + 1; j < NB; ++j) a[i][j] = a[i][j] - m * a[k][j];
+      rr[i] = rr[i] - m * rr[k];
+    }
+  }
+  for (int k = NB - 1; k >= 0; --k) {
+    rr[k] = rr[k] / a[k][k];
+    for (int i = 0; i < k; ++i) rr[i] = rr[i] - rr[k] * a[i][k];
+  }
+  for (int u = 0; u < NB; ++u)
+    if (real[u]) x[node[u]] = std::fma(omega, rr[u], x[node[u]]);
+}
+
+void ssc(const Hier& H, int l, double omega, double* x, const double* b, double* r) {
+  const Level& L = H.lev[l];
+  const int D = H.dim;
+  const long nv = H.order == 2 ? (L.M + 1) / 2 : L.M;  // vertices per direction
+  long nvert = 1;
+  for (int k = 0; k < D; ++k) nvert *= nv;
+  for (int col = 0; col < (1 << D); ++col) {
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < nvert; ++q) {
+      long a[3] = {q % nv, D > 1 ? (q / nv) % nv : 0, D > 2 ? q / (nv * nv) : 0};
+      int c = 0;
+      for (int k = 0; k < D; ++k) c |= (int)(a[k] & 1) << k;
+      if (c != col) continue;
+      long v[3];
+      for (int k = 0; k < 3; ++k) v[k] = a[k] * H.order;
+      ssc_block(H, L, v, omega, x, b, r);
+    }
+  }
+}
+
 // 1D interpolation stencils (fetransfer.lisp:73-195 evaluated for uniform
 // Lagrange Q1/Q2): coarse node J <-> fine node 2J.
 int restrict_stencil1d(int order, long J, long* off, double* w) {
@@ -846,12 +949,14 @@ void coarse_solve(const Hier& H, double damp, double* x, double* r) {
 }
 
 // ---------------------------------------------------------------- multigrid
-// One smoother step (the base iterator) and its flags (linit.lisp:220-323):
-// <jacobi> residual-before t, <sor> residual-before nil; both residual-after nil.
-bool smoother_residual_before(const ora_solve_cfg& c) { return c.smoother == ORA_JACOBI; }
+// One smoother step (the base iterator) and its flags (linit.lisp:220-323,
+// blockit.lisp:118-204): <jacobi> and the block iterations residual-before t,
+// <sor> residual-before nil; all residual-after nil.
+bool smoother_residual_before(const ora_solve_cfg& c) { return c.smoother != ORA_SOR; }
 
 void smoother_step(Hier& H, const ora_solve_cfg& c, int l, double* x, double* b, double* r) {
   if (c.smoother == ORA_JACOBI) jacobi(H, l, c.damp, x, r);
+  else if (c.smoother == ORA_SSC) ssc(H, l, c.damp, x, b, r);
   else sor(H, l, c.damp, x, b, r);
 }
 
@@ -1140,6 +1245,11 @@ int ora_sor(void* h, int level, double omega, double* x, const double* b, double
   sor(*(Hier*)h, level, omega, x, b, r);
   return 0;
 }
+int ora_ssc(void* h, int level, double omega, double* x, const double* b, double* r) {
+  if (((Hier*)h)->nc != 1) return -2;
+  ssc(*(Hier*)h, level, omega, x, b, r);
+  return 0;
+}
 int ora_coarse_solve(void* h, double damp, double* x, double* r) {
   coarse_solve(*(Hier*)h, damp, x, r);
   return 0;
@@ -1160,7 +1270,7 @@ int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* 
 int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hist_len, int* nsteps) {
   Hier& H = *(Hier*)h;
   if (!H.assembled) return -1;
-  if (H.nc != 1 && cfg->smoother == ORA_SOR) return -2;
+  if (H.nc != 1 && cfg->smoother != ORA_JACOBI) return -2;
   const ora_solve_cfg& c = *cfg;
   const int top = H.top;
   const long n = vec_len(H, top);

@@ -17,7 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libfmg_oracle.so")
 
 K_CONST, K_CELL, F_CONST, F_IP, LAMBDA_MU_CELL, F_VEC = 0, 1, 2, 3, 4, 5
-JACOBI, SOR = 0, 1
+JACOBI, SOR, SSC = 0, 1, 2
 METHOD_MG, METHOD_CG_MG, METHOD_CG = 0, 1, 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -79,6 +79,7 @@ def lib():
         L.ora_inject.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.ora_jacobi.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.ora_sor.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.ora_ssc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
         L.ora_coarse_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp, _dp]
         L.ora_dot.restype = ctypes.c_double
         L.ora_dot.argtypes = [_dp, _dp, ctypes.c_long]
@@ -245,6 +246,16 @@ class Oracle:
         b = np.ascontiguousarray(b, dtype=np.float64)
         r = np.array(r, dtype=np.float64, copy=True)
         lib().ora_sor(self.h, level, omega, _p(x), _p(b), _p(r))
+        return x, r
+
+    def ssc(self, x, b, r, omega=1.0, level=None):
+        """One <geometric-ssc> sweep (vertex-centred blocks); b may be r."""
+        level = self.top if level is None else level
+        alias = b is r
+        x = np.array(x, dtype=np.float64, copy=True)
+        r = np.array(r, dtype=np.float64, copy=True)
+        bb = r if alias else np.ascontiguousarray(b, dtype=np.float64)
+        lib().ora_ssc(self.h, level, omega, _p(x), _p(bb), _p(r))
         return x, r
 
     def coarse_solve(self, x, r, damp=1.0):

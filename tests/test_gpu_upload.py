@@ -31,7 +31,9 @@ def ctx(G):
 
 def _cfg(G, smoother=0, damp=0.6, pre=1, post=1, rtol=1e-10, maxsteps=200):
     C = G._capi
-    return G.SolveCfg(C.FMG_METHOD_CG_MG, smoother, damp, pre, post, 1, 1, 1.0, rtol, 0.0, maxsteps,
+    # a separate residual for the preconditioner (with the alias of krylow.lisp:120
+    # CG stagnates under the multiplicative cycle)
+    return G.SolveCfg(C.FMG_METHOD_CG_MG, smoother, damp, pre, post, 1, 0, 1.0, rtol, 0.0, maxsteps,
                       C.FMG_MULTIPLICATIVE, 0)
 
 
@@ -69,7 +71,7 @@ def test_round_trip_scalar(G, ctx, dim, order, level, base, layout, smoother):
     b = _upload_all(G, ctx, a, layout=layout)
     for l in range(base, level + 1):
         assert np.array_equal(a.matrix(l), b.matrix(l)), l
-    cfg = _cfg(G, smoother=smoother, damp=0.6 if smoother == 0 else 1.2)
+    cfg = _cfg(G) if smoother == 0 else _cfg(G, smoother=1, damp=1.0, pre=2, post=2)
     ha, xa, sa = _solve(G, a, cfg)
     hb, xb, sb = _solve(G, b, cfg)
     assert sa == 0 and sb == 0
@@ -102,7 +104,7 @@ def test_oracle_matrices_solve_like_the_oracle(oracle_mod, G, ctx):
     for l in range(1, 5):
         g.set_matrix(l, *G.slots_to_csr(o.matrix(l), 3, 1))
     g.set_rhs(o.rhs())
-    r = o.solve(O.solve_cfg(damp=0.6))
+    r = o.solve(O.solve_cfg(damp=0.6, compat=False))
     hist, x, st = _solve(G, g, _cfg(G))
     assert st == 0 and np.array_equal(hist, r.history) and np.array_equal(x, r.x)
 
@@ -168,7 +170,7 @@ def test_q2_galerkin_hierarchy(oracle_mod, G, ctx, dim, level):
     g.set_rhs(rhs)
     for l in mats:
         assert np.array_equal(g.matrix(l), o.matrix(l)), l
-    r = o.solve(O.solve_cfg(smoother=O.SOR, damp=1.2, pre=2, post=2))
+    r = o.solve(O.solve_cfg(smoother=O.SOR, damp=1.2, pre=2, post=2, compat=False))
     hist, x, st = _solve(G, g, _cfg(G, smoother=1, damp=1.2, pre=2, post=2))
     assert st == 0 and r.status == 0
     assert np.array_equal(hist, r.history) and np.array_equal(x, r.x)

@@ -163,3 +163,68 @@ def test_f_cycle_contracts_faster_than_v_cycle(oracle_mod):
         assert r.status == 0
         rates[fmg] = r.convergence_rate
     assert rates[True] < rates[False], rates
+
+
+def test_geometric_ssc_rate_bound_2d(oracle_mod):
+    # (test-v-cycle-convergence 2 4 3 :smoother (geometric-ssc) :cr-max 0.06)
+    # pins the vertex-centred SSC at Q4; Q2 (the highest order here) on the
+    # same mesh, base level 1, V(1,0), 20 multigrid steps meets the bound too
+    O = oracle_mod
+    o = O.Oracle(2, 2, 3, base_level=1).assemble()
+    cfg = O.solve_cfg(method=O.METHOD_MG, smoother=O.SSC, damp=1.0, pre=1, post=0, rtol=0.0,
+                      atol=1e-12, maxsteps=20)
+    r = o.solve(cfg)
+    assert r.convergence_rate < 0.06, r.convergence_rate
+
+
+def _dense(o, level, dim, order):
+    from gnu_femlisp_b200.core import slots_to_csr
+    start, index, values = slots_to_csr(o.matrix(level), dim, order)
+    n = start.size - 1
+    D = np.zeros((n, n))
+    for i in range(n):
+        D[i, index[start[i]:start[i + 1]]] = values[start[i]:start[i + 1]]
+    return D
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_ssc_block_solve_zeroes_the_block_residual(oracle_mod, dim):
+    # after a block's correction (omega = 1) its rows' residual vanishes
+    # (the debugging check of blockit.lisp:183-196).  On 2^d Q2 cells the
+    # box of the centre vertex holds every interior node, and its colour
+    # (vertex index 1 in every direction) is swept last.
+    O = oracle_mod
+    level = 1
+    o = O.Oracle(dim, 2, level, base_level=0)
+    k = np.exp(np.random.default_rng(dim).standard_normal((1 << level) ** dim))
+    o.set_coefficient(O.K_CELL, k)
+    o.assemble()
+    n = o.nnodes()
+    rng = np.random.default_rng(7)
+    b = rng.standard_normal(n)
+    x0 = rng.standard_normal(n)
+    x, r = o.ssc(x0, b, np.zeros(n), omega=1.0)
+    A = _dense(o, level, dim, 2)
+    M = 5
+    idx = np.arange(n)
+    c = np.stack([(idx // M ** d) % M for d in range(dim)], 1)
+    interior = np.all((c > 0) & (c < M - 1), 1)
+    res = b - A @ x
+    assert interior.sum() == 3 ** dim
+    assert np.all(np.abs(res[interior]) < 1e-12 * np.abs(b).max()), res[interior]
+    assert not np.array_equal(x, x0)
+
+
+def test_ssc_q1_is_gauss_seidel_in_colour_order(oracle_mod):
+    # Q1 vertex blocks hold one node: SSC(omega) is the colour-ordered SOR(omega)
+    O = oracle_mod
+    o = O.Oracle(2, 1, 4, base_level=1)
+    k = np.exp(np.random.default_rng(3).standard_normal(16 * 16))
+    o.set_coefficient(O.K_CELL, k)
+    o.assemble()
+    n = o.nnodes()
+    rng = np.random.default_rng(8)
+    b, x0 = rng.standard_normal(n), rng.standard_normal(n)
+    xs, _ = o.ssc(x0, b, np.zeros(n), omega=1.2)
+    xo, _ = o.sor(x0, b, np.zeros(n), omega=1.2)
+    assert np.array_equal(xs, xo)
