@@ -670,7 +670,7 @@ k_ssc_factor_q2(const double* __restrict__ A, long long Np, long long M, int dma
 // column) and x_B += omega c.  Blocks of one colour (vertex index mod 2 per
 // direction) share no node and read no unknown another one writes.
 template <int D>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 6)
 k_ssc_q2(const double* __restrict__ A, long long N, long long Np, long long M, int dmask, int colour,
          double omega, double* x, const double* b, double* r, const double* __restrict__ F,
          const unsigned char* __restrict__ P, const __grid_constant__ Q2Layout lay) {
@@ -688,6 +688,36 @@ k_ssc_q2(const double* __restrict__ A, long long N, long long Np, long long M, i
   const int v[3] = {2 * ax, 2 * ay, 2 * az};
   const long long blk = ax + (long long)nv * (ay + (long long)nv * az);
   const SscMember<D> mb = ssc_member<D>(v, lane, Mi, dmask);
+  // the unknowns the block's rows read: the 7^D nodes within 3 of the
+  // vertex, staged in shared memory (0 outside the domain, where the rows'
+  // stored coefficients are 0 as well)
+  constexpr int W7 = D == 1 ? 7 : (D == 2 ? 49 : 343);
+  __shared__ double xs_all[4][W7];
+  double* xs = xs_all[threadIdx.x >> 5];
+  for (int e = lane; e < W7; e += 32) {
+    const int lx = e % 7, ly = (e / 7) % 7, lz = e / 49;
+    const int gx = v[0] + lx - 3, gy = D > 1 ? v[1] + ly - 3 : 0, gz = D > 2 ? v[2] + lz - 3 : 0;
+    const bool inside = gx >= 0 && gx < Mi && (D < 2 || (gy >= 0 && gy < Mi)) && (D < 3 || (gz >= 0 && gz < Mi));
+    xs[e] = inside ? x[gx + M * ((long long)gy + M * (long long)gz)] : 0.0;
+  }
+  __syncwarp();
+  const long long i = mb.real ? (long long)mb.c[0] + M * ((long long)mb.c[1] + M * (long long)mb.c[2]) : 0;
+  double rr = 0.0;
+  if (mb.real) {
+    const long long cl[3] = {mb.c[0], mb.c[1], mb.c[2]};
+    Q2Base<D> qb;
+    q2_base<D, true, true>(lay, cl, M, qb);
+    const int lc = (mb.dm[0] + 3) + 7 * (D > 1 ? mb.dm[1] + 3 : 0) + 49 * (D > 2 ? mb.dm[2] + 3 : 0);
+    double s = 0.0;
+    q2_visit<D, true>(qb, M, [&](int k, long long, long long p, bool st) {
+      double av = A[(long long)k * Np + p];
+      av = st ? av : 0.0;
+      const int lo = (k % 5 - 2) + (D > 1 ? 7 * ((k / 5) % 5 - 2) : 0) + (D > 2 ? 49 * (k / 25 - 2) : 0);
+      s = fma(av, xs[lc + lo], s);
+    });
+    rr = b[i] - s;
+    r[i] = rr;
+  }
   double a[NB];
   int pos = lane;
   if (lane < NB) {
@@ -698,21 +728,6 @@ k_ssc_q2(const double* __restrict__ A, long long N, long long Np, long long M, i
   } else {
 #pragma unroll
     for (int k = 0; k < NB; ++k) a[k] = 0.0;
-  }
-  const long long i = mb.real ? (long long)mb.c[0] + M * ((long long)mb.c[1] + M * (long long)mb.c[2]) : 0;
-  double rr = 0.0;
-  if (mb.real) {
-    const long long cl[3] = {mb.c[0], mb.c[1], mb.c[2]};
-    Q2Base<D> qb;
-    q2_base<D, true, true>(lay, cl, M, qb);
-    double s = 0.0;
-    q2_visit<D, true>(qb, M, [&](int k, long long o, long long p, bool st) {
-      double av = A[(long long)k * Np + p];
-      av = st ? av : 0.0;
-      s = fma(av, x[clampi(i + o, N)], s);
-    });
-    rr = b[i] - s;
-    r[i] = rr;
   }
   ssc_fwd_step<NB, 0>(a, rr, pos, lane);
   double corr = 0.0;
