@@ -117,6 +117,7 @@ struct fmg_vec {
 // device data of the mixed-precision solve, built from an assembly
 struct MixedState {
   long long epoch = -1;             // assembly it was converted from
+  bool top32 = false;               // the top level's FP32 copy is of that assembly
   bool mf = false;                  // top level applied matrix-free
   std::vector<Lev32> lv;            // per level (FP32 matrices)
   std::vector<float*> A32, om32, x0, x1;
@@ -1288,6 +1289,21 @@ namespace {
 
 int mx_alloc_f(fmg_grid* g, float** p, long long n) { return dalloc(g, (double**)p, (n + 1) / 2); }
 
+// the mixed solve applies its top level matrix-free (3D scalar Q1 with cell
+// coefficients, the matrix not uploaded) when asked to
+bool mixed_top_mf(const fmg_grid* g, bool want_mf) {
+  return want_mf && g->dim == 3 && g->order == 1 && g->nc == 1 && !g->uploaded && g->kkind == FMG_K_CELL;
+}
+
+// the FP64 matrix-free operator of the top level
+MFArgs64 mf64_args(const fmg_grid* g, double damp) {
+  const Lvl& L = g->lev[g->top];
+  MFArgs64 m;
+  m.k = g->kcell_d; m.omega = nullptr; m.N = L.N; m.M = (int)L.M; m.n = (int)L.n; m.dmask = g->dmask;
+  m.hs = L.h / 12.0; m.w = damp;
+  return m;
+}
+
 int mixed_prepare(fmg_grid* g, bool want_mf) {
   fmg_ctx* c = g->ctx;
   cudaStream_t st = c->stream;
@@ -1296,7 +1312,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
   MixedState& X = *g->mx;
   const int nl = g->top + 1;
   // the matrix-free top level rebuilds A from the coefficients: not for uploaded matrices
-  const bool mf = want_mf && g->dim == 3 && g->order == 1 && g->nc == 1 && !g->uploaded;
+  const bool mf = mixed_top_mf(g, want_mf);
   if (X.lv.empty()) {  // first use: allocate
     X.lv.assign(nl, Lev32{});
     X.A32.assign(nl, nullptr); X.om32.assign(nl, nullptr);
@@ -1323,18 +1339,24 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
       return rc;
     if (!X.host) FMG_CK(c, cudaMallocHost((void**)&X.host, M_COUNT * sizeof(double)));
   }
-  if (X.epoch != g->epoch) {  // convert the current assembly
-    for (int l = g->base; l <= g->top; ++l) {
-      const Lvl& L = g->lev[l];
-      if (g->order == 2) launch_level_to_f32(view(g, l), g->nslots, X.A32[l], st);  // sliced -> full slots
-      else mx_f64_to_f32(L.A, X.A32[l], (long long)g->nslots * L.Np, st);
-    }
+  auto to32 = [&](int l) {
+    const Lvl& L = g->lev[l];
+    if (g->order == 2) launch_level_to_f32(view(g, l), g->nslots, X.A32[l], st);  // sliced -> full slots
+    else mx_f64_to_f32(L.A, X.A32[l], (long long)g->nslots * L.Np, st);
+  };
+  if (X.epoch != g->epoch) {  // convert the current assembly (the top level only where it is stored)
+    for (int l = g->base; l < g->top; ++l) to32(l);
     if (g->kkind == FMG_K_CELL) {
       long long ncell = 1;
       for (int k = 0; k < g->dim; ++k) ncell *= g->lev[g->top].n;
       mx_f64_to_f32(g->kcell_d, X.k32, ncell, st);
     }
     X.epoch = g->epoch;
+    X.top32 = false;
+  }
+  if (!mf && !X.top32) {
+    to32(g->top);
+    X.top32 = true;
   }
   for (int l = g->base; l <= g->top; ++l) {  // per-node damping may change between solves
     const Lvl& L = g->lev[l];
@@ -1410,11 +1432,7 @@ struct MixedMG {
   void matvec64(const float* p, double* a, const Reduce2& Rl) {
     const LevelView T = view(g, g->top);
     if (top_mf()) {
-      const Lvl& L = g->lev[g->top];
-      MFArgs64 m;
-      m.k = g->kcell_d; m.omega = nullptr; m.N = L.N; m.M = (int)L.M; m.n = (int)L.n; m.dmask = g->dmask;
-      m.hs = L.h / 12.0; m.w = c.damp;
-      mx_top_apply64(m, p, a, p, &Rl, st);
+      mx_top_apply64(mf64_args(g, c.damp), p, a, p, &Rl, st);
     } else {  // stored FP64 matrix: widen p first
       mx_f32_to_f64(p, g->xs2, T.N, st);
       launch_spmv(T, g->xs2, nullptr, a, nullptr, nullptr, st);
@@ -1721,8 +1739,10 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   double initial = -1.0;
   int step = 0, iters = 0;  // history slots, CG iterations
   for (int restart = 0; restart <= max_restart; ++restart) {
-    // true FP64 residual with the assembled matrix (x = 0: r = b exactly)
+    // true FP64 residual (x = 0: r = b exactly), from the cell coefficients
+    // where the top level is matrix-free, else with the assembled matrix
     if (restart == 0 && g->x_zero) launch_copy(b, r, n, st);
+    else if (mg.top_mf()) mx_top_residual64(mf64_args(g, cfg->damp), x, b, r, st);
     else launch_spmv(T, x, b, r, nullptr, nullptr, st);
     launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
     if ((rc = read_scalars(g))) return rc;
@@ -2380,7 +2400,10 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   const long long n = T.N * g->nc;
   double *xs = g->lt[9], *b = g->lt[7], *e = g->lt[6];
   launch_rand_fill(xs, g->dim, T.M, g->dmask, seed, st, g->nc);
-  launch_spmv(TV, xs, nullptr, b, nullptr, nullptr, st);
+  if (mc && mixed_top_mf(g, mc->matrix_free != 0))  // the operator the mixed solve applies
+    mx_top_apply64x(mf64_args(g, cf.damp), xs, b, st);
+  else
+    launch_spmv(TV, xs, nullptr, b, nullptr, nullptr, st);
   launch_dot(xs, b, n, reducer(g, EPI_STORE, S_E0), st);
   fmg_solve_cfg c = cf;
   c.rtol = 0.0;

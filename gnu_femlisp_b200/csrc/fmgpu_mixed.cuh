@@ -45,6 +45,11 @@ void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, flo
 // FP64 y = A x on the top level for an FP32 x, with (y, v) reduced (epilogue of R)
 void mx_top_apply64(const MFArgs64& g, const float* x, double* y, const float* v, const Reduce2* R,
                     cudaStream_t st);
+// the FP64 operator of FP64 vectors: y = A x (the probe's right-hand side)
+// and r = b - A x (the true residual of the mixed solve), from the cell
+// coefficients like the FP64 CG operator
+void mx_top_apply64x(const MFArgs64& g, const double* x, double* y, cudaStream_t st);
+void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, double* r, cudaStream_t st);
 long long mx_top_blocks(int M);  // blocks of the matrix-free kernel (reduction partials)
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
                     const double* v, const double* v2, const Reduce2* R, cudaStream_t st);

@@ -758,6 +758,18 @@ void mx_top_apply64(const MFArgs64& g, const float* x, double* y, const float* v
   mf_launch<double, float, float>(0, g, x, nullptr, y, v, nullptr, R, st);
 }
 
+void mx_top_apply64x(const MFArgs64& g, const double* x, double* y, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_mf4<double, double, double, kZS2, 0, false><<<mf2_grid(g.M), kMFThreads, 0, st>>>(g, x, nullptr, y, nullptr,
+                                                                                     nullptr, Reduce2{});
+}
+
+void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, double* r, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_mf4<double, double, double, kZS2, 1, false><<<mf2_grid(g.M), kMFThreads, 0, st>>>(g, x, b, r, nullptr, nullptr,
+                                                                                     Reduce2{});
+}
+
 long long mx_top_blocks(int M) {
   const dim3 gr = mf2_grid(M);
   return (long long)gr.x * gr.y * gr.z;
