@@ -80,6 +80,7 @@ struct fmg_grid {
   bool assembled_once = false;
   std::vector<char> have;      // levels whose matrix is in place
   bool uploaded = false;       // some level matrix came from fmg_set_matrix
+  bool top_deferred = false;   // the top level's matrix is formed on first use (its rhs is in place)
   // <geometric-ssc>: LU factors of the vertex blocks per level, formed once per assembly
   std::vector<double*> sscF;
   std::vector<unsigned char*> sscP;
@@ -142,6 +143,12 @@ struct MixedState {
   bool graphs_off = false;          // a capture failed: launch eagerly from then on
 };
 
+// the top level's matrix where its assembly was deferred (defined below,
+// among the entry points)
+extern "C" {
+static int ensure_top(fmg_grid* g);
+}
+
 // ------------------------------------------------------------------ errors
 namespace {
 
@@ -161,6 +168,12 @@ int cuda_err(fmg_ctx* c, cudaError_t e, const char* what) {
   return set_err(c, FMG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+// return a non-zero status
+#define FMG_RC(expr)                   \
+  do {                                 \
+    const int rc_ = (expr);            \
+    if (rc_) return rc_;               \
+  } while (0)
 #define FMG_CK(ctx, call)                                   \
   do {                                                      \
     cudaError_t e_ = (call);                                \
@@ -488,6 +501,7 @@ int ssc_prepare(fmg_grid* g, int l) {
     g->sscP.assign(g->top + 1, nullptr);
     g->sscEpoch.assign(g->top + 1, -1);
   }
+  if (l == g->top) FMG_RC(ensure_top(g));
   const LevelView v = view(g, l);
   const long long nb = ssc_blocks(v);
   if (nb == 0 || g->sscEpoch[l] == g->epoch) return FMG_OK;
@@ -782,6 +796,8 @@ static int ensure_buffers(fmg_grid* g) {
 int fmg_assemble(fmg_grid* g) { return fmg_assemble_levels(g, FMG_ASSEMBLE_REDISCRETIZE); }
 
 static int finish_levels(fmg_grid* g);
+static AsmArgs asm_args(fmg_grid* g, int l, bool sample);
+static int ensure_top(fmg_grid* g);
 
 int fmg_assemble_levels(fmg_grid* g, int mode) {
   if (!g) return FMG_ERR_ARG;
@@ -811,25 +827,50 @@ int fmg_assemble_levels(fmg_grid* g, int mode) {
                        st);
       if ((rc = launched(c, "sample_kq"))) return rc;
     }
-    AsmArgs a;
-    a.N = L.N; a.Np = L.Np; a.M = L.M; a.n = L.n;
-    a.dmask = g->dmask; a.nl = g->nl; a.nq = g->nq;
-    a.A = L.A;
-    a.rhs = (l == g->top) ? g->rhs : nullptr;
-    a.Kbar = L.Kbar; a.Ctab = L.Ctab; a.Phi = L.Phi;
-    a.kcell = (l == g->top && g->kkind == FMG_K_CELL) ? g->kcell_d : nullptr;
-    a.kq = sample ? g->kq : nullptr;
-    a.fip = g->fkind == FMG_F_IP ? g->fip_d : nullptr;
-    a.kconst = g->kconst; a.fconst = g->fconst;
-    a.nc = g->nc;
-    a.fvec_on = g->fkind == FMG_F_VEC ? 1 : 0;
-    for (int k = 0; k < 3; ++k) a.fvec[k] = g->fvec[k];
+    AsmArgs a = asm_args(g, l, sample);
+    // the top level's matrix of the unrolled Q1 path waits for its first
+    // use (the mixed solve applies that level from the cell coefficients and
+    // never reads it); its rhs is formed now
+    const bool defer = l == g->top && mode == FMG_ASSEMBLE_REDISCRETIZE && assemble_splits(g->dim, g->order, g->nc, a);
+    if (defer) a.A = nullptr;
     launch_assemble(g->dim, g->order, a, L.Kbar_h.data(), L.Ctab_h.data(), st);
     if ((rc = launched(c, "assemble"))) return rc;
+    if (l == g->top) g->top_deferred = defer;
   }
   g->have.assign(g->top + 1, 1);
   g->uploaded = false;
   return finish_levels(g);
+}
+
+// The arguments of level l's assembly (the rhs on the top level; sample:
+// the coarse level's coefficient samples are in g->kq).
+static AsmArgs asm_args(fmg_grid* g, int l, bool sample) {
+  const Lvl& L = g->lev[l];
+  AsmArgs a;
+  a.N = L.N; a.Np = L.Np; a.M = L.M; a.n = L.n;
+  a.dmask = g->dmask; a.nl = g->nl; a.nq = g->nq;
+  a.A = L.A;
+  a.rhs = (l == g->top) ? g->rhs : nullptr;
+  a.Kbar = L.Kbar; a.Ctab = L.Ctab; a.Phi = L.Phi;
+  a.kcell = (l == g->top && g->kkind == FMG_K_CELL) ? g->kcell_d : nullptr;
+  a.kq = sample ? g->kq : nullptr;
+  a.fip = g->fkind == FMG_F_IP ? g->fip_d : nullptr;
+  a.kconst = g->kconst; a.fconst = g->fconst;
+  a.nc = g->nc;
+  a.fvec_on = g->fkind == FMG_F_VEC ? 1 : 0;
+  for (int k = 0; k < 3; ++k) a.fvec[k] = g->fvec[k];
+  return a;
+}
+
+// The top level's matrix where its assembly was deferred (see above).
+static int ensure_top(fmg_grid* g) {
+  if (!g->top_deferred) return FMG_OK;
+  Lvl& L = g->lev[g->top];
+  AsmArgs a = asm_args(g, g->top, false);
+  a.rhs = nullptr;
+  launch_assemble(g->dim, g->order, a, L.Kbar_h.data(), L.Ctab_h.data(), g->ctx->stream);
+  g->top_deferred = false;
+  return launched(g->ctx, "assemble (top level)");
 }
 
 // The coarse LU and the multigrid state of a hierarchy whose level matrices
@@ -913,6 +954,7 @@ int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const i
   if ((int)g->have.size() != g->top + 1) g->have.assign(g->top + 1, 0);
   g->have[level] = 1;
   g->uploaded = true;
+  if (level == g->top) g->top_deferred = false;
   for (int m = g->base; m <= g->top; ++m)
     if (!g->have[m]) return FMG_OK;  // the hierarchy is complete with the last level
   return finish_levels(g);
@@ -935,6 +977,7 @@ int fmg_get_matrix(fmg_grid* g, int level, double* host) {
   if (!g || !host) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   if (level < g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d out of range", level);
+  if (level == g->top) FMG_RC(ensure_top(g));
   const Lvl& L = g->lev[level];
   const size_t rows = (size_t)g->nslots * g->nc * g->nc;
   FMG_CK(g->ctx, cudaMemcpy2DAsync(host, L.N * sizeof(double), L.A, L.Np * sizeof(double), L.N * sizeof(double),
@@ -1068,6 +1111,7 @@ int fmg_l2_norm(const fmg_vec* x, double* out) {
 int fmg_matvec(fmg_grid* g, int level, const fmg_vec* x, fmg_vec* y) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(y, g, level) || x == y) return FMG_ERR_ARG;
+  if (level == g->top) FMG_RC(ensure_top(g));
   launch_spmv(view(g, level), x->d, nullptr, y->d, nullptr, nullptr, g->ctx->stream);
   return launched(g->ctx, "matvec");
 }
@@ -1075,6 +1119,7 @@ int fmg_matvec(fmg_grid* g, int level, const fmg_vec* x, fmg_vec* y) {
 int fmg_residual(fmg_grid* g, int level, const fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level) || x == r) return FMG_ERR_ARG;
+  if (level == g->top) FMG_RC(ensure_top(g));
   launch_spmv(view(g, level), x->d, b->d, r->d, nullptr, nullptr, g->ctx->stream);
   return launched(g->ctx, "residual");
 }
@@ -1100,6 +1145,7 @@ int fmg_prolongate(fmg_grid* g, int coarse_level, const fmg_vec* xc, fmg_vec* xf
 int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
+  if (level == g->top) FMG_RC(ensure_top(g));
   launch_jacobi(view(g, level), damp, x->d, r->d, true, g->ctx->stream);
   return launched(g->ctx, "jacobi");
 }
@@ -1107,6 +1153,7 @@ int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
 int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
+  if (level == g->top) FMG_RC(ensure_top(g));
   launch_sor(view(g, level), omega, x->d, b->d, r->d, g->ctx->stream);
   return launched(g->ctx, "sor");
 }
@@ -1116,7 +1163,7 @@ int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
   if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric SSC: scalar grids");
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level) || x == b || x == r)
     return FMG_ERR_ARG;
-  int rc = ssc_prepare(g, level);
+  int rc = ssc_prepare(g, level);  // forms a deferred top level first
   if (rc) return rc;
   launch_ssc(view(g, level), omega, x->d, b->d, r->d, g->order == 2 ? g->sscF[level] : nullptr,
              g->order == 2 ? g->sscP[level] : nullptr, g->ctx->stream);
@@ -1132,6 +1179,7 @@ int fmg_coarse_solve(fmg_grid* g, double damp, fmg_vec* x, fmg_vec* r) {
 
 int fmg_vcycle(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fmg_vec* r) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  FMG_RC(ensure_top(g));
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (vec_check(x, g, g->top) || vec_check(b, g, g->top) || vec_check(r, g, g->top) || x == b || x == r)
@@ -1148,6 +1196,7 @@ int fmg_vcycle(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fm
 int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, int hist_len, int* nsteps,
               int* status) {
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  FMG_RC(ensure_top(g));
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (vec_check(xv, g, g->top) || !nsteps || !status) return FMG_ERR_ARG;
@@ -1355,6 +1404,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     X.top32 = false;
   }
   if (!mf && !X.top32) {
+    FMG_RC(ensure_top(g));
     to32(g->top);
     X.top32 = true;
   }
@@ -2105,7 +2155,7 @@ int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
       !((g->nc == 1 && g->order == 1) || (g->nc == 3 && g->order == 2 && g->dim == 3)))
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
                    "training loss: Jacobi V(1,1), scalar Q1 or 3D Q2 elasticity, at least two levels");
-  return FMG_OK;
+  return g->assembled ? ensure_top(g) : FMG_OK;  // the FP64 cycles read the top level's matrix
 }
 
 }  // namespace
@@ -2400,10 +2450,13 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   const long long n = T.N * g->nc;
   double *xs = g->lt[9], *b = g->lt[7], *e = g->lt[6];
   launch_rand_fill(xs, g->dim, T.M, g->dmask, seed, st, g->nc);
-  if (mc && mixed_top_mf(g, mc->matrix_free != 0))  // the operator the mixed solve applies
+  int rc0;
+  if (mc && mixed_top_mf(g, mc->matrix_free != 0)) {  // the operator the mixed solve applies
     mx_top_apply64x(mf64_args(g, cf.damp), xs, b, st);
-  else
+  } else {
+    if ((rc0 = ensure_top(g))) return rc0;
     launch_spmv(TV, xs, nullptr, b, nullptr, nullptr, st);
+  }
   launch_dot(xs, b, n, reducer(g, EPI_STORE, S_E0), st);
   fmg_solve_cfg c = cf;
   c.rtol = 0.0;
@@ -2471,6 +2524,7 @@ int learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mc
   bool any = false;
   for (int l = g->base + 1; l <= g->top; ++l) any = any || g->lev[l].omega;
   if (!any) return set_err(g->ctx, FMG_ERR_STATE, "no node damping installed");
+  if (!(mc && mixed_top_mf(g, mc->matrix_free != 0)) && (rc = ensure_top(g))) return rc;
   if ((rc = learn_vectors(g))) return rc;
   auto figure = [&](double* rho) {
     return cg ? cg_probe(g, *cfg, mc, 6, 0x4A554447ull, rho) : cycle_contraction(g, *cfg, 8, 0x4A554447ull, rho);

@@ -96,6 +96,9 @@ void launch_p_update(const double* sc, double* p, const double* q, long long n, 
 void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_top, double ratio, int np,
                       const double* xi, const double* kcell, double* kq, cudaStream_t st);
 // kbar_h / ctab_h: host copies of a.Kbar / a.Ctab (null: the generic kernel)
+// whether launch_assemble can form a level's rhs and matrix in separate passes
+// (a.A or a.rhs null): the unrolled 3D scalar Q1 kernel
+bool assemble_splits(int dim, int order, int nc, const AsmArgs& a);
 void launch_assemble(int dim, int order, const AsmArgs& a, const double* kbar_h, const double* ctab_h,
                      cudaStream_t st);
 void launch_densify(const LevelView& L, double* Dm, cudaStream_t st);

@@ -1252,8 +1252,10 @@ k_assemble_q1_3d(AsmArgs g, const __grid_constant__ Q1Tab tab) {
   const int ix = (int)(i % M), iy = (int)((i / M) % M), iz = (int)(i / ((long long)M * M));
   const long long ci[3] = {ix, iy, iz};
   if (node_dirichlet(ci, g.M, 3, g.dmask)) {
+    if (g.A) {
 #pragma unroll
-    for (int s = 0; s < 27; ++s) g.A[(long long)s * g.Np + i] = (s == 13) ? 1.0 : 0.0;
+      for (int s = 0; s < 27; ++s) g.A[(long long)s * g.Np + i] = (s == 13) ? 1.0 : 0.0;
+    }
     if (g.rhs) g.rhs[i] = 0.0;
     return;
   }
@@ -1262,6 +1264,7 @@ k_assemble_q1_3d(AsmArgs g, const __grid_constant__ Q1Tab tab) {
   for (int s = 0; s < 27; ++s) v[s] = 0.0;
 #pragma unroll
   for (int b = 0; b < 8; ++b) {
+    if (!g.A) break;  // the right-hand side alone
     const int cx = ix - 1 + (b & 1), cy = iy - 1 + ((b >> 1) & 1), cz = iz - 1 + (b >> 2);
     if (cx < 0 || cx >= n || cy < 0 || cy >= n || cz < 0 || cz >= n) continue;
     const long long cidx = cx + (long long)n * (cy + (long long)n * cz);
@@ -1289,13 +1292,15 @@ k_assemble_q1_3d(AsmArgs g, const __grid_constant__ Q1Tab tab) {
       v[s] = v[s] + e;
     }
   }
+  if (g.A) {
 #pragma unroll
-  for (int s = 0; s < 27; ++s) {
-    const int ox = s % 3 - 1, oy = (s / 3) % 3 - 1, oz = s / 9 - 1;
-    const long long cj[3] = {ix + ox, iy + oy, iz + oz};
-    const bool ok = cj[0] >= 0 && cj[0] < g.M && cj[1] >= 0 && cj[1] < g.M && cj[2] >= 0 && cj[2] < g.M &&
-                    !node_dirichlet(cj, g.M, 3, g.dmask);
-    g.A[(long long)s * g.Np + i] = ok ? v[s] : 0.0;
+    for (int s = 0; s < 27; ++s) {
+      const int ox = s % 3 - 1, oy = (s / 3) % 3 - 1, oz = s / 9 - 1;
+      const long long cj[3] = {ix + ox, iy + oy, iz + oz};
+      const bool ok = cj[0] >= 0 && cj[0] < g.M && cj[1] >= 0 && cj[1] < g.M && cj[2] >= 0 && cj[2] < g.M &&
+                      !node_dirichlet(cj, g.M, 3, g.dmask);
+      g.A[(long long)s * g.Np + i] = ok ? v[s] : 0.0;
+    }
   }
   if (g.rhs) {
     double acc = 0.0;
@@ -2101,6 +2106,10 @@ void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_to
   if (dim == 1) k_sample_kq<1><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
   else if (dim == 2) k_sample_kq<2><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
   else k_sample_kq<3><<<g, kBlock, 0, st>>>(ncells_l, n_l, n_top, ratio, np, xi, kcell, kq);
+}
+
+bool assemble_splits(int dim, int order, int nc, const AsmArgs& a) {
+  return nc == 1 && dim == 3 && order == 1 && a.nl == 8 && a.nq == 8 && a.M < (1 << 20);
 }
 
 void launch_assemble(int dim, int order, const AsmArgs& a, const double* kbar_h, const double* ctab_h,

@@ -260,3 +260,23 @@ def test_f_cycle_solve_history(oracle_mod, G, ctx, dim, order, level, base, meth
     assert_same(X.get(), ro.x, "solution")
     with pytest.raises(G.FmgError):
         g.solve_mixed(gc, g.vector())  # the mixed cycle is a V/W cycle
+
+
+def test_deferred_top_level_matrix(oracle_mod, G, ctx):
+    # 3D scalar Q1: the top level's matrix is formed on its first use; a
+    # mixed solve (matrix-free top level) before it, then the FP64 solve and
+    # the matrices, all as the oracle has them
+    O = oracle_mod
+    o, g = make_pair(O, G, ctx, 3, 1, 4, 1, kcell=True, seed=21)
+    C = G._capi
+    cfg = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 100,
+                     C.FMG_MULTIPLICATIVE, 0)
+    xm = g.vector()
+    hist_m, _, _, st_m = g.solve_mixed(cfg, xm, matrix_free=True)
+    assert st_m == 0
+    x = g.vector()
+    hist, steps, st = g.solve(cfg, x)
+    r = o.solve(O.solve_cfg(damp=0.6, compat=False, rtol=1e-10, maxsteps=100))
+    assert st == 0 and np.array_equal(hist, r.history) and np.array_equal(x.get(), r.x)
+    assert_same(g.matrix(4), o.matrix(4), "top level")
+    assert np.linalg.norm(xm.get() - r.x) <= 1e-8 * np.linalg.norm(r.x)
