@@ -126,6 +126,10 @@ struct MixedState {
   float* k32 = nullptr;             // top-level cell coefficients (FP32)
   float *rtop = nullptr, *r = nullptr, *q = nullptr, *qs = nullptr;  // FP32 top-level vectors
   float* p32 = nullptr;             // FP32 search direction of the flexible CG
+  float* wd = nullptr;              // top level: damping / diagonal per node (matrix-free smoothing)
+  const float* wd_om = nullptr;     // the node damping and scalar damping wd was formed with
+  float wd_w = 0.f;
+  bool wd_ok = false;
   double* sc = nullptr;
   double* part = nullptr;
   unsigned* counter = nullptr;
@@ -1378,7 +1382,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     const Lvl& T = g->lev[g->top];
     long long ncell = 1;
     for (int k = 0; k < g->dim; ++k) ncell *= T.n;
-    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32};
+    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32, &X.wd};
     for (float** v : tv)
       if ((rc = mx_alloc_f(g, v, T.Np))) return rc;
     if ((rc = mx_alloc_f(g, &X.k32, ncell))) return rc;
@@ -1434,7 +1438,20 @@ struct MixedMG {
     a.N = T.N; a.M = (int)T.M; a.n = (int)T.n; a.dmask = g->dmask;
     a.hs = (float)(T.h / 12.0);
     a.w = (float)c.damp;
+    const bool wd = X.wd_ok && X.wd_om == a.omega && X.wd_w == a.w;
+    a.wd = wd ? X.wd : nullptr;
     return a;
+  }
+  // damping / diagonal of the top level for the damping now in use (once per
+  // solve, and again after a revert to the plain damping)
+  void prepare_wd() {
+    X.wd_ok = false;
+    if (!top_mf()) return;
+    const MFArgs a = mf_args();
+    mx_top_wd(a, X.wd, st);
+    X.wd_om = a.omega;
+    X.wd_w = a.w;
+    X.wd_ok = true;
   }
   // one FP32 operator application on level l (modes of k_mf_q1 / k_st32)
   void apply(int l, int mode, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16, const double* v,
@@ -1524,7 +1541,8 @@ std::vector<uint64_t> step_key(const fmg_grid* g, const MixedState& X, const fmg
   std::memcpy(&d, &c.damp, sizeof d);
   k.push_back(d);
   k.push_back((uint64_t)c.pre_steps << 32 | (uint32_t)c.post_steps);
-  k.push_back((uint64_t)(X.mf ? 1 : 0) << 8 | (uint64_t)g->kkind);
+  k.push_back((uint64_t)(X.mf ? 1 : 0) << 8 | (uint64_t)g->kkind | (uint64_t)(X.wd_ok ? 1 : 0) << 16);
+  P(X.wd_om);
   return k;
 }
 
@@ -1775,6 +1793,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   if ((rc = mixed_prepare(g, mcfg->matrix_free != 0))) return rc;
   MixedState& X = *g->mx;
   MixedMG mg{g, X, *cfg, st};
+  mg.prepare_wd();
   const LevelView T = view(g, g->top);
   const long long n = T.N;
   double* x = xv->d;
@@ -1851,6 +1870,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       // node damping; the flexible CG then restarts from the true residual
       if (judge_active && iters > it0 && rn > 100.0 * dn) {
         for (auto& V : X.lv) V.om = nullptr;  // plain damping for the rest of the solve
+        mg.prepare_wd();
         judge_active = false;
         g->reverts += 1;
         revert_restart = true;

@@ -27,6 +27,7 @@ struct MFArgsT {
   int M, n, dmask;
   T hs;                // h / 12
   T w;                 // scalar damping
+  const T* wd = nullptr;  // per-node damping / diagonal (mx_top_wd), or nullptr: formed in the kernel
 };
 typedef MFArgsT<float> MFArgs;
 typedef MFArgsT<double> MFArgs64;
@@ -51,6 +52,9 @@ void mx_top_apply64(const MFArgs64& g, const float* x, double* y, const float* v
 void mx_top_apply64x(const MFArgs64& g, const double* x, double* y, cudaStream_t st);
 void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, double* r, cudaStream_t st);
 long long mx_top_blocks(int M);  // blocks of the matrix-free kernel (reduction partials)
+// wd = damping / diagonal per top-level node (Dirichlet nodes: the damping)
+// for the smoothing modes of mx_top_apply
+void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st);
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
                     const double* v, const double* v2, const Reduce2* R, cudaStream_t st);
 void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, __nv_bfloat16* bc, float* xc,

@@ -160,6 +160,7 @@ k_mf4(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __rest
       const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
   constexpr bool HX = MODE != 3;
   constexpr bool HB = MODE != 0;
+  constexpr bool DIFF = sizeof(T) == 8;  // the FP64 operator in difference form
   constexpr bool HO = MODE == 2 || MODE == 3;
   __shared__ TX xs[kStages][HX ? kNH4 : 1];
   __shared__ T ks[kStages][kNC4];
@@ -216,7 +217,7 @@ k_mf4(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __rest
       const bool ok = in && (r ? own1 : own0);
       const long long i = zb + (r ? col1 : col0);
       o.b[r] = (HB && ok) ? __ldg(b + i) : T(0);
-      o.o[r] = (HO && omv && ok) ? __ldg(g.omega + i) : g.w;
+      o.o[r] = (HO && g.wd && ok) ? __ldg(g.wd + i) : ((HO && omv && ok) ? __ldg(g.omega + i) : g.w);
       o.v[r] = (RED && ok) ? __ldg(v + i) : TV(0);
       o.v2[r] = (RED && ok && v2) ? __ldg(v2 + i) : TV(0);
     }
@@ -263,26 +264,30 @@ k_mf4(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __rest
           const int h = (2 * ly + r + 1) * kHX + lx + 1;
           const TX* X1 = xs[s1];  // x plane iz
           xc = (T)X1[h];
+          // FP64: the row as sum_j w_j (x_i - x_j) -- the weights sum to 4 K,
+          // and the differences of a smooth iterate are small, so the true
+          // residual's rounding is far below that of 4 K x_i - sum_j w_j x_j
+          auto term = [&](T w, T xj) { sacc = DIFF ? fma(w, xc - xj, sacc) : fma(w, xj, sacc); };
 #pragma unroll
           for (int sy = 0; sy < 2; ++sy)
 #pragma unroll
-            for (int sx = 0; sx < 2; ++sx) sacc = fma(wc[sy][sx], (T)X1[h + (2 * sy - 1) * kHX + 2 * sx - 1], sacc);
+            for (int sx = 0; sx < 2; ++sx) term(wc[sy][sx], (T)X1[h + (2 * sy - 1) * kHX + 2 * sx - 1]);
 #pragma unroll
           for (int cz = 0; cz < 2; ++cz) {
             const TX* Xz = xs[cz ? s0 : s2];  // x plane iz+1 / iz-1
 #pragma unroll
             for (int sx = 0; sx < 2; ++sx)   // face diagonals (sx, 0, sz): cells (sx, *, sz)
-              sacc = fma(k[cz][0][sx] + k[cz][1][sx], (T)Xz[h + 2 * sx - 1], sacc);
+              term(k[cz][0][sx] + k[cz][1][sx], (T)Xz[h + 2 * sx - 1]);
 #pragma unroll
             for (int sy = 0; sy < 2; ++sy)   // face diagonals (0, sy, sz): cells (*, sy, sz)
-              sacc = fma(k[cz][sy][0] + k[cz][sy][1], (T)Xz[h + (2 * sy - 1) * kHX], sacc);
+              term(k[cz][sy][0] + k[cz][sy][1], (T)Xz[h + (2 * sy - 1) * kHX]);
 #pragma unroll
             for (int sy = 0; sy < 2; ++sy)
 #pragma unroll
               for (int sx = 0; sx < 2; ++sx)  // body diagonals
-                sacc = fma(k[cz][sy][sx], (T)Xz[h + (2 * sy - 1) * kHX + 2 * sx - 1], sacc);
+                term(k[cz][sy][sx], (T)Xz[h + (2 * sy - 1) * kHX + 2 * sx - 1]);
           }
-          sacc = fma(T(4) * ksum, xc, -sacc);
+          if (!DIFF) sacc = fma(T(4) * ksum, xc, -sacc);
         }
         d = T(4) * hs * ksum;
         ax = hs * sacc;
@@ -290,8 +295,8 @@ k_mf4(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __rest
       T out;
       if (MODE == 0) out = ax;
       else if (MODE == 1) out = cur.b[r] - ax;
-      else if (MODE == 2) out = fma(cur.o[r], (cur.b[r] - ax) / d, xc);
-      else out = cur.o[r] * (cur.b[r] / d);
+      else if (MODE == 2) out = g.wd ? fma(cur.o[r], cur.b[r] - ax, xc) : fma(cur.o[r], (cur.b[r] - ax) / d, xc);
+      else out = g.wd ? cur.o[r] * cur.b[r] : cur.o[r] * (cur.b[r] / d);
       y[i] = out;
       if (RED) {
         acc0 = fma((double)out, (double)cur.v[r], acc0);
@@ -748,8 +753,57 @@ static void mf_launch(int mode, const MFArgsT<T>& g, const TX* x, const T* b, T*
   }
 }
 
+// pre-smoothing from zero with the damping over the diagonal formed: y = wd b
+__global__ void __launch_bounds__(kBlock) k_wd_scale(const float* __restrict__ wd, const float* __restrict__ b,
+                                                     float* __restrict__ y, long long n) {
+  const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
+  if (i < n) y[i] = __ldg(wd + i) * __ldg(b + i);
+}
+
+// wd = damping / diagonal of the matrix-free top level, the diagonal formed
+// as in k_mf4 (4 hs times the sum of the node's 8 cell coefficients, summed
+// in the same order; cells outside the grid count zero); Dirichlet nodes
+// (identity rows) get the damping itself
+__global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ wd) {
+  const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
+  if (i >= g.N) return;
+  const int M = g.M, n = g.n, dm = g.dmask;
+  const int ix = (int)(i % M), iy = (int)((i / M) % M), iz = (int)(i / ((long long)M * M));
+  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+  const float om = g.omega ? __ldg(g.omega + i) : g.w;
+  if (dirf(ix, 1, 2) || dirf(iy, 4, 8) || dirf(iz, 16, 32)) {
+    wd[i] = om;
+    return;
+  }
+  float k[2][2][2];
+#pragma unroll
+  for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+    for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+      for (int cx = 0; cx < 2; ++cx) {
+        const int x = ix - 1 + cx, y = iy - 1 + cy, z = iz - 1 + cz;
+        const bool in = x >= 0 && x < n && y >= 0 && y < n && z >= 0 && z < n;
+        k[cz][cy][cx] = in ? __ldg(g.k + x + (long long)n * (y + (long long)n * z)) : 0.f;
+      }
+  const float wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
+                          {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
+  const float ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
+  wd[i] = om / (4.f * g.hs * ksum);
+}
+
+void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_mf_wd<<<g1(g.N), kBlock, 0, st>>>(g, wd);
+}
+
 void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,
                   const double* v2, const Reduce2* R, cudaStream_t st) {
+  if (mode == 3 && g.wd && !R) {  // a stream of two reads and a write
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_wd_scale<<<g1(g.N), kBlock, 0, st>>>(g.wd, b, y, g.N);
+    return;
+  }
   mf_launch<float, double, float>(mode, g, x, b, y, v, v2, R, st);
 }
 
