@@ -940,6 +940,96 @@ __global__ void __launch_bounds__(1024) k_lu_factor_smem(double* A, int n, int* 
   for (int idx = tid; idx < n * n; idx += nt) A[idx] = S[idx];
 }
 
+// k_lu_factor_smem with two block barriers per column instead of five: warp 0
+// finds the pivot (the first logical row holding the largest magnitude) and
+// interchanges logical rows through a permutation; every thread then updates
+// the trailing submatrix, forming the multiplier it needs as the quotient the
+// column will hold, and scales the previous column (which no later step
+// reads before that).  Factors and pivots are bitwise those of k_lu_factor.
+__global__ void __launch_bounds__(1024) k_lu_factor_smem2(double* A, int n, int* piv) {
+  extern __shared__ double S[];
+  int* perm = reinterpret_cast<int*>(S + (size_t)n * n);
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+  for (int idx = tid; idx < n * n; idx += nt) S[idx] = A[idx];
+  for (int i = tid; i < n; i += nt) perm[i] = i;
+  __syncthreads();
+  double dprev = 1.0;
+  for (int k = 0; k < n; ++k) {
+    if (tid < 32) {
+      double best = -1.0;
+      int besti = n;
+      for (int i = k + lane; i < n; i += 32) {
+        const double v = fabs(S[perm[i] * n + k]);
+        if (v > best || (v == best && i < besti)) { best = v; besti = i; }
+      }
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+        if (ov > best || (ov == best && oi < besti)) { best = ov; besti = oi; }
+      }
+      if (lane == 0) {
+        piv[k] = besti;
+        const int t = perm[k];
+        perm[k] = perm[besti];
+        perm[besti] = t;
+      }
+    }
+    __syncthreads();
+    const int pr = perm[k];
+    const double d = S[pr * n + k];
+    const int m = n - k - 1;
+    const int mm = m * m, nprev = k > 0 ? n - k : 0;  // previous column: logical rows k .. n-1
+    for (int idx = tid; idx < mm + nprev; idx += nt) {
+      if (idx < mm) {
+        const int i = k + 1 + idx / m, j = k + 1 + idx % m;
+        const int ri = perm[i];
+        const double l = S[ri * n + k] / d;
+        S[ri * n + j] = fma(-l, S[pr * n + j], S[ri * n + j]);
+      } else {
+        const int ri = perm[k + (idx - mm)];
+        S[ri * n + k - 1] = S[ri * n + k - 1] / dprev;
+      }
+    }
+    dprev = d;
+    __syncthreads();
+  }
+  for (int idx = tid; idx < n * n; idx += nt) A[idx] = S[perm[idx / n] * n + idx % n];
+}
+
+// k_lu_inverse with one CTA per column of X: the threads share the rows, a
+// block barrier per elimination column; every element sees the same
+// operations in the same order as in k_lu_inverse.
+__global__ void __launch_bounds__(256) k_lu_inverse_col(const double* __restrict__ LU, const int* __restrict__ piv,
+                                                        int n, double* X) {
+  extern __shared__ double S[];
+  double* L = S;              // n x n
+  double* xv = S + n * n;     // the column, forward
+  double* out = xv + n;       // the column, backward
+  const int tid = threadIdx.x, nt = blockDim.x, j = blockIdx.x;
+  for (int idx = tid; idx < n * n; idx += nt) L[idx] = LU[idx];
+  for (int i = tid; i < n; i += nt) xv[i] = (i == j) ? 1.0 : 0.0;
+  __syncthreads();
+  if (tid == 0)
+    for (int k = 0; k < n; ++k) {
+      const int p = piv[k];
+      if (p != k) { const double t = xv[k]; xv[k] = xv[p]; xv[p] = t; }
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    const double bk = xv[k];
+    for (int i = k + 1 + tid; i < n; i += nt) xv[i] = fma(-L[i * n + k], bk, xv[i]);
+    __syncthreads();
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const double bk = xv[k] / L[k * n + k];
+    if (tid == 0) out[k] = bk;
+    for (int i = tid; i < k; i += nt) xv[i] = fma(-L[i * n + k], bk, xv[i]);
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += nt) X[(long long)i * n + j] = out[i];
+}
+
 // k_lu_inverse with the factors and a block of 32 columns of X in shared
 // memory: thread = column, the same operations in the same order.
 __global__ void __launch_bounds__(32) k_lu_inverse_smem(const double* __restrict__ LU, const int* __restrict__ piv,
@@ -2057,12 +2147,12 @@ void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t s
   if (i_smem <= kMaxSmem) {  // the factors fit in shared memory (n <= 144)
     static bool init = false;
     if (!init) {
-      cudaFuncSetAttribute(k_lu_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
-      cudaFuncSetAttribute(k_lu_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+      cudaFuncSetAttribute(k_lu_factor_smem2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+      cudaFuncSetAttribute(k_lu_inverse_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
       init = true;
     }
-    k_lu_factor_smem<<<1, 1024, f_smem, st>>>(A, n, piv);
-    k_lu_inverse_smem<<<grid1(n, 32), 32, i_smem, st>>>(A, piv, n, X);
+    k_lu_factor_smem2<<<1, 1024, f_smem + (size_t)n * sizeof(int), st>>>(A, n, piv);
+    k_lu_inverse_col<<<n, 256, f_smem + 2 * (size_t)n * sizeof(double), st>>>(A, piv, n, X);
   } else {
     k_lu_factor<<<1, 1024, 0, st>>>(A, n, piv);
     k_lu_inverse<<<grid1(n, 64), 64, 0, st>>>(A, piv, n, X);
