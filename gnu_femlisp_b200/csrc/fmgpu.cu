@@ -535,8 +535,8 @@ int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (c->method < FMG_METHOD_MG || c->method > FMG_METHOD_CG)
     return set_err(g->ctx, FMG_ERR_ARG, "bad method");
   if (c->fmg != 0 && c->fmg != 1) return set_err(g->ctx, FMG_ERR_ARG, "fmg is 0 or 1");
+  g->ssc_unprepared = false;
   if (c->smoother == FMG_SSC) {  // factors of every smoothed level before the cycle runs
-    g->ssc_unprepared = false;
     for (int l = g->base + 1; l <= g->top; ++l) {
       const int rc = ssc_prepare(g, l);
       if (rc) return rc;
