@@ -783,8 +783,11 @@ def run_c5(args):
     # the plain cycle with the mixed solve's CG probe
     from gnu_femlisp_b200.learn import DampingNet
     net = DampingNet.load(ctx, WEIGHTS_ELASTIC)
+    ctx.synchronize()
     t0 = time.perf_counter()
     net.apply(g)
+    ctx.synchronize()
+    t_apply = time.perf_counter() - t0
     ok, rp, rl = g.learned_judge_mixed(cfg)
     ctx.synchronize()
     t_setup = time.perf_counter() - t0
@@ -792,7 +795,8 @@ def run_c5(args):
         solve_mixed()
     t_mixed, (mhist, nouter, ninner, mstatus) = timed(solve_mixed, args.steps)
     learned_info = {"weights": os.path.relpath(WEIGHTS_ELASTIC, ROOT), "accepted": ok, "rho_plain": rp,
-                    "rho_learned": rl, "setup_s": t_setup, "status": g.learned_status(),
+                    "rho_learned": rl, "setup_s": t_setup, "net_apply_s": t_apply, "judge_s": t_setup - t_apply,
+                    "status": g.learned_status(),
                     "mixed_without_learned": {"time_to_solution_s": t_mixed_plain,
                                               "inner_iterations": int(ninner_plain)}}
     x64, xmx = x.get(), xm.get()

@@ -836,6 +836,142 @@ k_prolong(int MF, int MC, int dmask, const double* __restrict__ xc, double* __re
 }
 
 // -------------------------------------------------------------- coarse LU
+// Blocked form of k_lu_factor for matrices beyond shared memory: panels of
+// kLuB columns, rows interchanged through a logical permutation (physical rows
+// stay put), every element updated by the same fma's in the same ascending
+// order of elimination steps as in the unblocked loop, so factors and pivots
+// are bitwise those of k_lu_factor.
+constexpr int kLuB = 32;
+
+// the panel k0..k1-1: per column the pivot (the first logical row holding the
+// largest magnitude), the interchange, and the updates of the panel's later
+// columns; the multipliers (column / pivot) are stored one step later, and
+// the panel's last column's after the loop
+__global__ void __launch_bounds__(1024) k_lu_panel(double* A, int n, int k0, int k1, int* piv, int* perm) {
+  __shared__ double bv[32];
+  __shared__ int bi[32];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double dprev = 1.0;
+  for (int k = k0; k < k1; ++k) {
+    double best = -1.0;
+    int besti = n;
+    for (int i = k + tid; i < n; i += nt) {
+      const double v = fabs(A[(long long)perm[i] * n + k]);
+      if (v > best || (v == best && i < besti)) { best = v; besti = i; }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+      if (ov > best || (ov == best && oi < besti)) { best = ov; besti = oi; }
+    }
+    if ((tid & 31) == 0) { bv[tid >> 5] = best; bi[tid >> 5] = besti; }
+    __syncthreads();
+    if (tid == 0) {
+      double b = bv[0];
+      int ib = bi[0];
+      for (int w = 1; w < (nt + 31) / 32; ++w)
+        if (bv[w] > b || (bv[w] == b && bi[w] < ib)) { b = bv[w]; ib = bi[w]; }
+      piv[k] = ib;
+      const int t = perm[k];
+      perm[k] = perm[ib];
+      perm[ib] = t;
+    }
+    __syncthreads();
+    const long long pr = perm[k];
+    const double d = A[pr * n + k];
+    const int m = n - k - 1, w = k1 - k - 1;
+    const long long mw = (long long)m * w, nprev = k > k0 ? n - k : 0;  // previous column: logical rows k ..
+    for (long long idx = tid; idx < mw + nprev; idx += nt) {
+      if (idx < mw) {
+        const int i = k + 1 + (int)(idx / w), j = k + 1 + (int)(idx % w);
+        const long long ri = perm[i];
+        const double l = A[ri * n + k] / d;
+        A[ri * n + j] = fma(-l, A[pr * n + j], A[ri * n + j]);
+      } else {
+        const long long ri = perm[k + (int)(idx - mw)];
+        A[ri * n + k - 1] = A[ri * n + k - 1] / dprev;
+      }
+    }
+    dprev = d;
+    __syncthreads();
+  }
+  for (int i = k1 + tid; i < n; i += nt) {  // the panel's last column, logical rows k1 ..
+    const long long ri = perm[i];
+    A[ri * n + k1 - 1] = A[ri * n + k1 - 1] / dprev;
+  }
+}
+
+// the panel's rows right of the panel: column j (one thread) takes the
+// panel's elimination steps in order
+__global__ void k_lu_urows(double* A, int n, int k0, int k1, const int* __restrict__ perm) {
+  const int j = k1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int k = k0; k < k1; ++k) {
+    const double ukj = A[(long long)perm[k] * n + j];
+    for (int i = k + 1; i < k1; ++i) {
+      const long long ri = perm[i];
+      A[ri * n + j] = fma(-A[ri * n + k], ukj, A[ri * n + j]);
+    }
+  }
+}
+
+// the trailing rows and columns: each element takes the panel's steps in order
+__global__ void __launch_bounds__(256) k_lu_trail(double* A, int n, int k0, int k1, const int* __restrict__ perm) {
+  const int j = k1 + blockIdx.x * 32 + threadIdx.x;
+  const int i = k1 + blockIdx.y * 8 + threadIdx.y;
+  if (i >= n || j >= n) return;
+  const long long ri = perm[i];
+  double a = A[ri * n + j];
+  for (int k = k0; k < k1; ++k) a = fma(-A[ri * n + k], A[(long long)perm[k] * n + j], a);
+  A[ri * n + j] = a;
+}
+
+__global__ void k_lu_permute(const double* __restrict__ A, int n, const int* __restrict__ perm, double* X) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const long long i = t / n, j = t % n;
+  X[t] = A[(long long)perm[i] * n + j];
+}
+
+__global__ void k_iota(int* p, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = i;
+}
+
+// k_lu_inverse with one CTA per column of X reading the factors transposed
+// (LT[k][i] = LU[i][k], coalesced over the rows): every element sees the same
+// operations in the same order
+__global__ void __launch_bounds__(256) k_lu_inverse_colT(const double* __restrict__ LT, const int* __restrict__ piv,
+                                                         int n, double* X) {
+  extern __shared__ double S[];
+  double* xv = S;
+  double* out = S + n;
+  const int tid = threadIdx.x, nt = blockDim.x, j = blockIdx.x;
+  for (int i = tid; i < n; i += nt) xv[i] = (i == j) ? 1.0 : 0.0;
+  __syncthreads();
+  if (tid == 0)
+    for (int k = 0; k < n; ++k) {
+      const int p = piv[k];
+      if (p != k) { const double t = xv[k]; xv[k] = xv[p]; xv[p] = t; }
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    const double bk = xv[k];
+    const double* col = LT + (long long)k * n;
+    for (int i = k + 1 + tid; i < n; i += nt) xv[i] = fma(-col[i], bk, xv[i]);
+    __syncthreads();
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const double* col = LT + (long long)k * n;
+    const double bk = xv[k] / col[k];
+    if (tid == 0) out[k] = bk;
+    for (int i = tid; i < k; i += nt) xv[i] = fma(-col[i], bk, xv[i]);
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += nt) X[(long long)i * n + j] = out[i];
+}
+
 // Single-block dense LU with partial pivoting, row-major, in place.
 __global__ void __launch_bounds__(1024) k_lu_factor(double* A, int n, int* piv) {
   __shared__ double bv[32];
@@ -2153,9 +2289,23 @@ void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t s
     }
     k_lu_factor_smem2<<<1, 1024, f_smem + (size_t)n * sizeof(int), st>>>(A, n, piv);
     k_lu_inverse_col<<<n, 256, f_smem + 2 * (size_t)n * sizeof(double), st>>>(A, piv, n, X);
-  } else {
-    k_lu_factor<<<1, 1024, 0, st>>>(A, n, piv);
-    k_lu_inverse<<<grid1(n, 64), 64, 0, st>>>(A, piv, n, X);
+  } else {  // blocked in global memory (L2-resident); perm lives in XT until the end
+    int* perm = reinterpret_cast<int*>(XT);
+    k_iota<<<grid1(n), kBlock, 0, st>>>(perm, n);
+    for (int k0 = 0; k0 < n; k0 += kLuB) {
+      const int k1 = std::min(n, k0 + kLuB);
+      k_lu_panel<<<1, 1024, 0, st>>>(A, n, k0, k1, piv, perm);
+      if (k1 < n) {
+        k_lu_urows<<<grid1(n - k1, 128), 128, 0, st>>>(A, n, k0, k1, perm);
+        k_lu_trail<<<dim3((unsigned)((n - k1 + 31) / 32), (unsigned)((n - k1 + 7) / 8)), dim3(32, 8), 0, st>>>(
+            A, n, k0, k1, perm);
+      }
+      g_launches.fetch_add(3, std::memory_order_relaxed);
+    }
+    k_lu_permute<<<grid1((long long)n * n), kBlock, 0, st>>>(A, n, perm, X);   // X: the factors, rows interchanged
+    k_transpose<<<grid1((long long)n * n), kBlock, 0, st>>>(X, n, A);         // A: the factors transposed
+    k_lu_inverse_colT<<<n, 256, 2 * (size_t)n * sizeof(double), st>>>(A, piv, n, X);
+    g_launches.fetch_add(4, std::memory_order_relaxed);
   }
   k_transpose<<<grid1((long long)n * n), kBlock, 0, st>>>(X, n, XT);
 }
