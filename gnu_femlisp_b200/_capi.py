@@ -15,7 +15,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "fmgpu.h")
 
 FMG_OK = 0
 FMG_K_CONST, FMG_K_CELL, FMG_F_CONST, FMG_F_IP, FMG_LAMBDA_MU_CELL, FMG_F_VEC = 0, 1, 2, 3, 4, 5
-FMG_JACOBI, FMG_SOR, FMG_SSC = 0, 1, 2
+FMG_JACOBI, FMG_SOR, FMG_SSC, FMG_PSC = 0, 1, 2, 3
 FMG_ASSEMBLE_REDISCRETIZE, FMG_ASSEMBLE_GALERKIN = 0, 1
 FMG_CSR, FMG_CCS = 0, 1
 FMG_METHOD_MG, FMG_METHOD_CG_MG, FMG_METHOD_CG = 0, 1, 2
@@ -101,6 +101,7 @@ SIGNATURES = {
     "fmg_jacobi": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp]),
     "fmg_sor": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp, _vp]),
     "fmg_ssc": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp, _vp]),
+    "fmg_psc": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp]),
     "fmg_coarse_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "fmg_vcycle": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _vp, _vp]),
     "fmg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, ctypes.c_int,

@@ -218,6 +218,10 @@ class Grid:
         """One <geometric-ssc> sweep (vertex-centred blocks); b may be r."""
         self.ctx.check(self._lib.fmg_ssc(self.h, x.level, omega, x.h, b.h, r.h), "ssc")
 
+    def psc(self, x: "Vector", r: "Vector", damp: float = 1.0):
+        """One <geometric-psc> sweep (vertex-centred blocks) with the residual r."""
+        self.ctx.check(self._lib.fmg_psc(self.h, x.level, damp, x.h, r.h), "psc")
+
     def coarse_solve(self, x: "Vector", r: "Vector", damp: float = 1.0):
         self.ctx.check(self._lib.fmg_coarse_solve(self.h, damp, x.h, r.h), "coarse_solve")
 

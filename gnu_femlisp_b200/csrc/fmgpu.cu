@@ -84,6 +84,7 @@ struct fmg_grid {
   // <geometric-ssc>: LU factors of the vertex blocks per level, formed once per assembly
   std::vector<double*> sscF;
   std::vector<unsigned char*> sscP;
+  std::vector<double*> sscC;   // <geometric-psc>: the blocks' corrections
   std::vector<long long> sscEpoch;
   bool ssc_unprepared = false; // a sweep found no factors (and was not run)
   long long epoch = 0;         // incremented by every assembly
@@ -422,6 +423,19 @@ struct MG {
                    g->order == 2 ? g->sscP[l] : nullptr, st);
         if (steps > 1 && keep) residual(l);
       }
+    } else if (c.smoother == FMG_PSC) {
+      // residual-before t, residual-after nil, r read and not written
+      // (blockit.lisp:118-204): the residual before every step, as for <jacobi>
+      const bool ready = g->order == 1 || ((int)g->sscF.size() > l && g->sscF[l] && g->sscEpoch[l] == g->epoch);
+      if (!ready) { g->ssc_unprepared = true; g->rp[l] = 0; return; }
+      bool need = !g->rp[l];
+      for (int s = 0; s < steps; ++s) {
+        if (need) residual(l);
+        launch_psc(view(g, l), c.damp, g->solp[l], g->resp[l], g->order == 2 ? g->sscF[l] : nullptr,
+                   g->order == 2 ? g->sscP[l] : nullptr, g->order == 2 ? g->sscC[l] : nullptr, st);
+        need = true;
+      }
+      if (steps > 1 && (literal || alias(l))) residual(l);
     } else {
       for (int s = 0; s < steps; ++s) launch_sor(view(g, l), c.damp, g->solp[l], g->rhsp[l], g->resp[l], st);
     }
@@ -503,6 +517,7 @@ int ssc_prepare(fmg_grid* g, int l) {
   if ((int)g->sscF.size() != g->top + 1) {
     g->sscF.assign(g->top + 1, nullptr);
     g->sscP.assign(g->top + 1, nullptr);
+    g->sscC.assign(g->top + 1, nullptr);
     g->sscEpoch.assign(g->top + 1, -1);
   }
   if (l == g->top) FMG_RC(ensure_top(g));
@@ -513,7 +528,9 @@ int ssc_prepare(fmg_grid* g, int l) {
   int rc;
   if (!g->sscF[l]) {
     double* p = nullptr;
-    if ((rc = dalloc(g, &g->sscF[l], nb * bs * bs)) || (rc = dalloc(g, &p, (nb * bs + 7) / 8))) return rc;
+    if ((rc = dalloc(g, &g->sscF[l], nb * bs * bs)) || (rc = dalloc(g, &p, (nb * bs + 7) / 8)) ||
+        (rc = dalloc(g, &g->sscC[l], nb * bs)))
+      return rc;
     g->sscP[l] = (unsigned char*)p;
   }
   launch_ssc_factor(v, g->sscF[l], g->sscP[l], g->ctx->stream);
@@ -526,7 +543,7 @@ int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (!c) return set_err(g->ctx, FMG_ERR_ARG, "null configuration");
   if (g->nc != 1 && c->smoother != FMG_JACOBI)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "3-component grids: the (block) Jacobi smoother only");
-  if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR && c->smoother != FMG_SSC)
+  if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR && c->smoother != FMG_SSC && c->smoother != FMG_PSC)
     return set_err(g->ctx, FMG_ERR_ARG, "unknown smoother %d", c->smoother);
   if (c->pre_steps < 0 || c->post_steps < 0 || c->gamma < 0 || c->gamma > 4)
     return set_err(g->ctx, FMG_ERR_ARG, "bad cycle parameters");
@@ -536,7 +553,7 @@ int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
     return set_err(g->ctx, FMG_ERR_ARG, "bad method");
   if (c->fmg != 0 && c->fmg != 1) return set_err(g->ctx, FMG_ERR_ARG, "fmg is 0 or 1");
   g->ssc_unprepared = false;
-  if (c->smoother == FMG_SSC) {  // factors of every smoothed level before the cycle runs
+  if (c->smoother == FMG_SSC || c->smoother == FMG_PSC) {  // block factors of every smoothed level
     for (int l = g->base + 1; l <= g->top; ++l) {
       const int rc = ssc_prepare(g, l);
       if (rc) return rc;
@@ -1172,6 +1189,18 @@ int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
   launch_ssc(view(g, level), omega, x->d, b->d, r->d, g->order == 2 ? g->sscF[level] : nullptr,
              g->order == 2 ? g->sscP[level] : nullptr, g->ctx->stream);
   return launched(g->ctx, "ssc");
+}
+
+int fmg_psc(fmg_grid* g, int level, double damp, fmg_vec* x, const fmg_vec* r) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric PSC: scalar grids");
+  if (vec_check(x, g, level) || vec_check(r, g, level) || x == r) return FMG_ERR_ARG;
+  int rc = ssc_prepare(g, level);  // forms a deferred top level first
+  if (rc) return rc;
+  if (level == g->top && g->order == 1) FMG_RC(ensure_top(g));
+  launch_psc(view(g, level), damp, x->d, r->d, g->order == 2 ? g->sscF[level] : nullptr,
+             g->order == 2 ? g->sscP[level] : nullptr, g->order == 2 ? g->sscC[level] : nullptr, g->ctx->stream);
+  return launched(g->ctx, "psc");
 }
 
 int fmg_coarse_solve(fmg_grid* g, double damp, fmg_vec* x, fmg_vec* r) {

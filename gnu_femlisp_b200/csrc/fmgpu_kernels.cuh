@@ -80,6 +80,10 @@ int ssc_block_size(int dim);
 void launch_ssc_factor(const LevelView& L, double* F, unsigned char* P, cudaStream_t st);
 void launch_ssc(const LevelView& L, double omega, double* x, const double* b, double* r, const double* F,
                 const unsigned char* P, cudaStream_t st);
+// one <geometric-psc> sweep with the residual r (not written): block
+// corrections into C (blocks x size doubles, Q2), added to x in block order
+void launch_psc(const LevelView& L, double damp, double* x, const double* r, const double* F,
+                const unsigned char* P, double* C, cudaStream_t st);
 void launch_restrict(const LevelView& F, const LevelView& C, const double* rf, double* rc, double* rhsc,
                      double* solc, cudaStream_t st);
 void launch_prolong(const LevelView& C, const LevelView& F, const double* xc, double* xf, cudaStream_t st);

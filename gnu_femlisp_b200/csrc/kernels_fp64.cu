@@ -735,6 +735,99 @@ k_ssc_q2(const double* __restrict__ A, long long N, long long Np, long long M, i
   if (mb.real) x[i] = fma(omega, corr, x[i]);
 }
 
+// <geometric-psc> on a scalar Q1 level: one-node blocks, x_i += damp r_i /
+// a_ii (the 1 x 1 LU divides by the pivot), r unchanged
+template <int D>
+__global__ void __launch_bounds__(kBlock)
+k_psc_q1(const double* __restrict__ A, long long N, long long Np, double damp, double* x, const double* r) {
+  constexpr int C = St<D, 1>::CENTER;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  x[i] = fma(damp, r[i] / A[(long long)C * Np + i], x[i]);
+}
+
+// <geometric-psc> on a scalar Q2 level, first pass: every vertex block (warp
+// per block, all blocks in one launch) solves A_BB c = r_B with the stored
+// factors and the residual as it stands (r is read, not written); member t's
+// correction goes to C[block][t] (zero for padded members).
+template <int D>
+__global__ void __launch_bounds__(128, 6)
+k_psc_block_q2(long long M, int dmask, const double* __restrict__ r, const double* __restrict__ F,
+               const unsigned char* __restrict__ P, double* __restrict__ C) {
+  constexpr int NB = D == 1 ? 3 : (D == 2 ? 9 : 27);
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // uniform per warp
+  const int Mi = (int)M;
+  const int nv = (Mi + 1) / 2;
+  const long long nblk = D == 1 ? nv : (D == 2 ? (long long)nv * nv : (long long)nv * nv * nv);
+  if (w >= nblk) return;  // the whole warp leaves together
+  const int wi = (int)w;
+  const int v[3] = {2 * (wi % nv), D > 1 ? 2 * ((wi / nv) % nv) : 0, D > 2 ? 2 * (wi / (nv * nv)) : 0};
+  const SscMember<D> mb = ssc_member<D>(v, lane, Mi, dmask);
+  double rr = mb.real ? r[(long long)mb.c[0] + M * ((long long)mb.c[1] + M * (long long)mb.c[2])] : 0.0;
+  double a[NB];
+  int pos = lane;
+  if (lane < NB) {
+    const double* f = F + w * NB * NB + lane;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) a[k] = __ldg(f + k * NB);
+    pos = P[w * NB + lane];
+  } else {
+#pragma unroll
+    for (int k = 0; k < NB; ++k) a[k] = 0.0;
+  }
+  ssc_fwd_step<NB, 0>(a, rr, pos, lane);
+  double corr = 0.0;
+  ssc_back_step<NB, NB - 1>(a, rr, pos, lane, corr);
+  if (lane < NB) C[w * NB + lane] = corr;
+}
+
+// second pass: node i adds, in increasing vertex order, damp times its
+// correction from each block holding it as a member (the vertices within 1
+// of it along every direction; a Dirichlet node belongs to its own block only)
+template <int D>
+__global__ void __launch_bounds__(kBlock)
+k_psc_gather_q2(long long N, long long M, int dmask, double damp, const double* __restrict__ C, double* x) {
+  constexpr int NB = D == 1 ? 3 : (D == 2 ? 9 : 27);
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int Mi = (int)M, nv = (Mi + 1) / 2;
+  int c[3] = {(int)(i % M), D > 1 ? (int)((i / M) % M) : 0, D > 2 ? (int)(i / (M * M)) : 0};
+  bool dir = false;
+#pragma unroll
+  for (int k = 0; k < D; ++k)
+    dir = dir || (c[k] == 0 && ((dmask >> (2 * k)) & 1)) || (c[k] == Mi - 1 && ((dmask >> (2 * k + 1)) & 1));
+  // candidate vertex coordinates per direction, ascending
+  int vc[3][2], nvc[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    nvc[k] = 1;
+    vc[k][0] = vc[k][1] = 0;
+    if (k >= D) continue;
+    if (c[k] & 1) {
+      nvc[k] = 2;
+      vc[k][0] = c[k] - 1;
+      vc[k][1] = c[k] + 1;
+    } else {
+      vc[k][0] = c[k];
+    }
+  }
+  double xi = x[i];
+  for (int iz = 0; iz < nvc[2]; ++iz)
+    for (int iy = 0; iy < nvc[1]; ++iy)
+      for (int ix = 0; ix < nvc[0]; ++ix) {
+        const int vx = vc[0][ix], vy = vc[1][iy], vz = vc[2][iz];
+        const bool own = vx == c[0] && (D < 2 || vy == c[1]) && (D < 3 || vz == c[2]);  // i is the vertex
+        if (dir && !own) continue;
+        const long long blk = (vx >> 1) + (long long)nv * ((vy >> 1) + (long long)nv * (vz >> 1));
+        int t = c[0] - vx + 1;
+        if (D > 1) t += 3 * (c[1] - vy + 1);
+        if (D > 2) t += 9 * (c[2] - vz + 1);
+        xi = fma(damp, C[blk * NB + t], xi);
+      }
+  x[i] = xi;
+}
+
 // -------------------------------------------------------------- transfers
 template <int P>
 __device__ __forceinline__ int restrict_1d(long long J, long long* off, double* w) {
@@ -2227,6 +2320,21 @@ void launch_ssc(const LevelView& L, double omega, double* x, const double* b, do
       k_ssc_q2<D><<<grid, 128, 0, st>>>(L.A, L.N, L.Np, L.M, L.dmask, col, omega, x, b, r, F, P, lay);
     });
   }
+}
+
+void launch_psc(const LevelView& L, double damp, double* x, const double* r, const double* F,
+                const unsigned char* P, double* C, cudaStream_t st) {
+  if (L.order == 1) {  // one-node blocks: x_i += damp r_i / a_ii, r unchanged
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    Q1_DISPATCH(L.dim, { k_psc_q1<D><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, damp, x, r); });
+    return;
+  }
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  const unsigned grid = (unsigned)((ssc_blocks(L) * 32 + 127) / 128);
+  Q2_DISPATCH(L.dim, {
+    k_psc_block_q2<D><<<grid, 128, 0, st>>>(L.M, L.dmask, r, F, P, C);
+    k_psc_gather_q2<D><<<grid1(L.N), kBlock, 0, st>>>(L.N, L.M, L.dmask, damp, C, x);
+  });
 }
 
 static inline dim3 xfer_grid(long long M, int dim) {

@@ -178,6 +178,17 @@ def geometric_ssc(**kw) -> GeometricSSC:
 
 
 @dataclass
+class GeometricPSC:
+    """(geometric-psc) -- parallel subspace correction over the vertex-centred
+    blocks (geoblock.lisp:37-158, blockit.lisp:118-204), damped by :damp."""
+    damp: float = 1.0
+
+
+def geometric_psc(**kw) -> GeometricPSC:
+    return GeometricPSC(**kw)
+
+
+@dataclass
 class LU:
     damp: float = 1.0
 
@@ -284,6 +295,8 @@ def make_cfg(iteration, success_if: str, failure_if: str, order: int = 1) -> tup
             cfg.smoother, cfg.damp = C.FMG_JACOBI, sm.damp
         elif isinstance(sm, GeometricSSC):
             cfg.smoother, cfg.damp = C.FMG_SSC, sm.omega
+        elif isinstance(sm, GeometricPSC):
+            cfg.smoother, cfg.damp = C.FMG_PSC, sm.damp
         elif isinstance(sm, SOR):
             cfg.smoother, cfg.damp = C.FMG_SOR, sm.omega
         else:

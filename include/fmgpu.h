@@ -55,6 +55,8 @@ extern "C" {
 #define FMG_SOR 1               /* <sor> :omega, colour ordering (linit.lisp:288-323) */
 #define FMG_SSC 2               /* (geometric-ssc) :omega, vertex-centred blocks (geoblock.lisp:37-158,
                                    blockit.lisp:118-204); scalar grids */
+#define FMG_PSC 3               /* (geometric-psc) :damp, the same blocks, corrections from one residual
+                                   added (blockit.lisp:118-204); scalar grids */
 
 #define FMG_METHOD_MG 0         /* <linear-solver> :iteration <geometric-cs> */
 #define FMG_METHOD_CG_MG 1      /* <cg> :preconditioner <geometric-cs> */
@@ -72,7 +74,7 @@ typedef struct fmg_vec fmg_vec;
    forms of <linear-solver> (iterate.lisp:105-123). */
 typedef struct {
   int method;          /* FMG_METHOD_* */
-  int smoother;        /* FMG_JACOBI, FMG_SOR or FMG_SSC */
+  int smoother;        /* FMG_JACOBI, FMG_SOR, FMG_SSC or FMG_PSC */
   double damp;         /* :damp of <jacobi>, :omega of <sor> */
   int pre_steps, post_steps, gamma;
   int compat_alias;    /* 1: the preconditioner is called as (iterate q w w),
@@ -211,6 +213,11 @@ int fmg_sor(fmg_grid* grid, int level, double omega, fmg_vec* x, const fmg_vec* 
    colour order (vertex index mod 2 per direction), lexicographic within a
    colour; b may be r (the alias inside <cg>). */
 int fmg_ssc(fmg_grid* grid, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r);
+/* one (geometric-psc) sweep: every vertex block of fmg_ssc solves its local
+   system with the residual r as given (r is read, not written), and the
+   corrections are added in increasing vertex order, x_B += damp c_B
+   (overlapping blocks sum theirs) */
+int fmg_psc(fmg_grid* grid, int level, double damp, fmg_vec* x, const fmg_vec* r);
 /* the <lu> coarse-grid iteration on the base level: r := A^-1 r,
    x := x + damp r (linit.lisp:156-161) */
 int fmg_coarse_solve(fmg_grid* grid, double damp, fmg_vec* x, fmg_vec* r);

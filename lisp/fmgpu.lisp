@@ -28,6 +28,7 @@
 (defconstant +fmg-jacobi+ 0)
 (defconstant +fmg-sor+ 1)
 (defconstant +fmg-ssc+ 2)
+(defconstant +fmg-psc+ 3)
 (defconstant +fmg-method-mg+ 0)
 (defconstant +fmg-method-cg-mg+ 1)
 (defconstant +fmg-multiplicative+ 0)

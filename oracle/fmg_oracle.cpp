@@ -688,42 +688,50 @@ void sor(const Hier& H, int l, double omega, double* x, const double* b, double*
 // the compact block.  LU: right-looking, row interchanges to the first
 // position holding the largest magnitude, multipliers scaled by the pivot's
 // reciprocal, no fused multiply-adds (the dgetf2 + dgetrs sequence of gesv!).
-void ssc_block(const Hier& H, const Level& L, const long v[3], double omega, double* x, const double* b,
-               double* r) {
-  const int D = H.dim;
-  const int NB = H.order == 2 ? (D == 1 ? 3 : D == 2 ? 9 : 27) : 1;
-  const int centre = NB / 2;
+//
+// VBlock / vertex_block: the vertex block's members (the full 3^d box, real
+// members marked); vertex_block_solve: c = A_BB^-1 rr by the LU above, rr the
+// members' right-hand side on entry (zero for the padded ones), c on return.
+struct VBlock {
+  int NB;
   long node[27];
   bool real[27];
   long cn[27][3];
-  for (int u = 0; u < NB; ++u) {
+};
+
+void vertex_block(const Hier& H, const Level& L, const long v[3], VBlock& B) {
+  const int D = H.dim;
+  B.NB = H.order == 2 ? (D == 1 ? 3 : D == 2 ? 9 : 27) : 1;
+  const int centre = B.NB / 2;
+  for (int u = 0; u < B.NB; ++u) {
     int t = u;
     bool in = true;
     for (int k = 0; k < 3; ++k) {
-      const long d = (k < D && NB > 1) ? (t % 3) - 1 : 0;
-      if (k < D && NB > 1) t /= 3;
-      cn[u][k] = v[k] + d;
-      if (k < D && (cn[u][k] < 0 || cn[u][k] >= L.M)) in = false;
+      const long d = (k < D && B.NB > 1) ? (t % 3) - 1 : 0;
+      if (k < D && B.NB > 1) t /= 3;
+      B.cn[u][k] = v[k] + d;
+      if (k < D && (B.cn[u][k] < 0 || B.cn[u][k] >= L.M)) in = false;
     }
-    real[u] = in && (u == centre || !is_dirichlet(H, L.M, cn[u]));
-    node[u] = in ? cn[u][0] + L.M * (cn[u][1] + L.M * cn[u][2]) : -1;
+    B.real[u] = in && (u == centre || !is_dirichlet(H, L.M, B.cn[u]));
+    B.node[u] = in ? B.cn[u][0] + L.M * (B.cn[u][1] + L.M * B.cn[u][2]) : -1;
   }
-  double a[27][27], rr[27];
+}
+
+void vertex_block_solve(const Hier& H, const Level& L, const VBlock& B, double* rr) {
+  const int NB = B.NB, D = H.dim;
+  double a[27][27];
   for (int t = 0; t < NB; ++t) {
-    if (!real[t]) {
+    if (!B.real[t]) {
       for (int u = 0; u < NB; ++u) a[t][u] = u == t ? 1.0 : 0.0;
-      rr[t] = 0.0;
       continue;
     }
-    const long i = node[t];
-    rr[t] = b[i] - row_sum(H, L, i, x);
-    r[i] = rr[t];
+    const long i = B.node[t];
     for (int u = 0; u < NB; ++u) {
-      if (!real[u]) { a[t][u] = 0.0; continue; }
+      if (!B.real[u]) { a[t][u] = 0.0; continue; }
       long o[3] = {0, 0, 0};
       bool near = true;
       for (int k = 0; k < D; ++k) {
-        o[k] = cn[u][k] - cn[t][k];
+        o[k] = B.cn[u][k] - B.cn[t][k];
         if (o[k] < -H.span || o[k] > H.span) near = false;
       }
       a[t][u] = near ? L.A[(size_t)slot_of(H, o) * L.N + i] : 0.0;
@@ -750,8 +758,47 @@ void ssc_block(const Hier& H, const Level& L, const long v[3], double omega, dou
     rr[k] = rr[k] / a[k][k];
     for (int i = 0; i < k; ++i) rr[i] = rr[i] - rr[k] * a[i][k];
   }
-  for (int u = 0; u < NB; ++u)
-    if (real[u]) x[node[u]] = std::fma(omega, rr[u], x[node[u]]);
+}
+
+// <geometric-psc> (geoblock.lisp:43-45, blockit.lisp:118-204 without the
+// per-block residual update): every vertex block solves A_BB c_B = r_B with
+// the residual r as it was before the sweep (r is not written), and the
+// corrections are added in block order, x_B += damp c_B -- overlapping blocks
+// sum their corrections (the block loop reads x_B after the earlier blocks
+// wrote it).  Order: vertices lexicographic.
+void psc(const Hier& H, int l, double damp, double* x, const double* r) {
+  const Level& L = H.lev[l];
+  const int D = H.dim;
+  const long nv = H.order == 2 ? (L.M + 1) / 2 : L.M;
+  long nvert = 1;
+  for (int k = 0; k < D; ++k) nvert *= nv;
+  for (long q = 0; q < nvert; ++q) {
+    const long v[3] = {(q % nv) * H.order, D > 1 ? ((q / nv) % nv) * H.order : 0, D > 2 ? (q / (nv * nv)) * H.order : 0};
+    VBlock B;
+    vertex_block(H, L, v, B);
+    double rr[27];
+    for (int t = 0; t < B.NB; ++t) rr[t] = B.real[t] ? r[B.node[t]] : 0.0;
+    vertex_block_solve(H, L, B, rr);
+    for (int u = 0; u < B.NB; ++u)
+      if (B.real[u]) x[B.node[u]] = std::fma(damp, rr[u], x[B.node[u]]);
+  }
+}
+
+void ssc_block(const Hier& H, const Level& L, const long v[3], double omega, double* x, const double* b,
+               double* r) {
+  VBlock B;
+  vertex_block(H, L, v, B);
+  double rr[27];
+  for (int t = 0; t < B.NB; ++t) {
+    rr[t] = 0.0;
+    if (!B.real[t]) continue;
+    const long i = B.node[t];
+    rr[t] = b[i] - row_sum(H, L, i, x);
+    r[i] = rr[t];
+  }
+  vertex_block_solve(H, L, B, rr);
+  for (int u = 0; u < B.NB; ++u)
+    if (B.real[u]) x[B.node[u]] = std::fma(omega, rr[u], x[B.node[u]]);
 }
 
 void ssc(const Hier& H, int l, double omega, double* x, const double* b, double* r) {
@@ -957,6 +1004,7 @@ bool smoother_residual_before(const ora_solve_cfg& c) { return c.smoother != ORA
 void smoother_step(Hier& H, const ora_solve_cfg& c, int l, double* x, double* b, double* r) {
   if (c.smoother == ORA_JACOBI) jacobi(H, l, c.damp, x, r);
   else if (c.smoother == ORA_SSC) ssc(H, l, c.damp, x, b, r);
+  else if (c.smoother == ORA_PSC) psc(H, l, c.damp, x, r);
   else sor(H, l, c.damp, x, b, r);
 }
 
@@ -1243,6 +1291,11 @@ int ora_jacobi(void* h, int level, double damp, double* x, double* r) {
 int ora_sor(void* h, int level, double omega, double* x, const double* b, double* r) {
   if (((Hier*)h)->nc != 1) return -2;
   sor(*(Hier*)h, level, omega, x, b, r);
+  return 0;
+}
+int ora_psc(void* h, int level, double damp, double* x, const double* r) {
+  if (((Hier*)h)->nc != 1) return -2;
+  psc(*(Hier*)h, level, damp, x, r);
   return 0;
 }
 int ora_ssc(void* h, int level, double omega, double* x, const double* b, double* r) {

@@ -49,14 +49,14 @@ extern "C" {
 enum { ORA_K_CONST = 0, ORA_K_CELL = 1, ORA_F_CONST = 2, ORA_F_IP = 3, ORA_LAMBDA_MU_CELL = 4, ORA_F_VEC = 5 };
 
 /* smoother kinds */
-enum { ORA_JACOBI = 0, ORA_SOR = 1, ORA_SSC = 2 };
+enum { ORA_JACOBI = 0, ORA_SOR = 1, ORA_SSC = 2, ORA_PSC = 3 };
 
 /* iteration methods of the solver loop */
 enum { ORA_METHOD_MG = 0, ORA_METHOD_CG_MG = 1, ORA_METHOD_CG = 2 };
 
 typedef struct {
   int method;          /* ORA_METHOD_* */
-  int smoother;        /* ORA_JACOBI, ORA_SOR or ORA_SSC (geometric-ssc, vertex blocks) */
+  int smoother;        /* ORA_JACOBI, ORA_SOR, ORA_SSC or ORA_PSC (geometric-ssc / -psc, vertex blocks) */
   double damp;         /* <jacobi> :damp or <sor> :omega */
   int pre_steps, post_steps, gamma;
   int compat_alias;    /* 1: CG calls the preconditioner as (iterate q w w) */
@@ -94,6 +94,7 @@ int ora_prolongate(void* h, int coarse_level, const double* xc, double* xf, int 
 int ora_inject(void* h, int coarse_level, const double* xf, double* xc);
 int ora_jacobi(void* h, int level, double damp, double* x, double* r);
 int ora_sor(void* h, int level, double omega, double* x, const double* b, double* r);
+int ora_psc(void* h, int level, double damp, double* x, const double* r);
 int ora_ssc(void* h, int level, double omega, double* x, const double* b, double* r);
 int ora_coarse_solve(void* h, double damp, double* x, double* r);
 double ora_dot(const double* x, const double* y, long n);

@@ -17,7 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libfmg_oracle.so")
 
 K_CONST, K_CELL, F_CONST, F_IP, LAMBDA_MU_CELL, F_VEC = 0, 1, 2, 3, 4, 5
-JACOBI, SOR, SSC = 0, 1, 2
+JACOBI, SOR, SSC, PSC = 0, 1, 2, 3
 METHOD_MG, METHOD_CG_MG, METHOD_CG = 0, 1, 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -80,6 +80,7 @@ def lib():
         L.ora_jacobi.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.ora_sor.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
         L.ora_ssc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.ora_psc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.ora_coarse_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp, _dp]
         L.ora_dot.restype = ctypes.c_double
         L.ora_dot.argtypes = [_dp, _dp, ctypes.c_long]
@@ -257,6 +258,15 @@ class Oracle:
         bb = r if alias else np.ascontiguousarray(b, dtype=np.float64)
         lib().ora_ssc(self.h, level, omega, _p(x), _p(bb), _p(r))
         return x, r
+
+    def psc(self, x, r, damp=1.0, level=None):
+        """One <geometric-psc> sweep (vertex-centred blocks, corrections added
+        in block order); r is read, not written."""
+        level = self.top if level is None else level
+        x = np.array(x, dtype=np.float64, copy=True)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        lib().ora_psc(self.h, level, damp, _p(x), _p(r))
+        return x
 
     def coarse_solve(self, x, r, damp=1.0):
         x = np.array(x, dtype=np.float64, copy=True)

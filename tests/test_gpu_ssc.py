@@ -1,5 +1,6 @@
-"""The vertex-centred successive subspace correction (geometric-ssc,
-geoblock.lisp:37-158, blockit.lisp:118-204) on the GPU against the oracle,
+"""The vertex-centred successive and parallel subspace corrections
+(geometric-ssc / geometric-psc, geoblock.lisp:37-158, blockit.lisp:118-204)
+on the GPU against the oracle,
 bitwise: single sweeps (separate b and r, and b aliased to r as inside
 <cg>), Q1 (one-node blocks) and Q2 (3^d boxes) in 1, 2 and 3 dimensions, a
 partially clamped boundary (blocks cut by Neumann faces), and whole
@@ -114,3 +115,36 @@ def test_default_smoother_of_q2_is_ssc(G, ctx):
     bb = I.solve({"matrix": A, "solver": solver})
     assert bb["report"].status == "success"
     assert bb["report"].steps < 20
+
+
+# ---------------------------------------------------------------- geometric PSC
+
+@pytest.mark.parametrize("dim,order,level", SWEEPS)
+@pytest.mark.parametrize("dmask", [None, 0b000001])
+def test_psc_sweep(oracle_mod, G, ctx, dim, order, level, dmask):
+    o, g = make_pair(oracle_mod, G, ctx, dim, order, level, 0, seed=dim + 2 * level, dmask=dmask)
+    n = g.nnodes()
+    rng = np.random.default_rng(23)
+    x0, r0 = rng.standard_normal(n), rng.standard_normal(n)
+    x, r = g.vector(values=x0), g.vector(values=r0)
+    xo = o.psc(x0, r0, damp=0.7)
+    g.psc(x, r, damp=0.7)
+    assert np.array_equal(x.get(), xo), np.max(np.abs(x.get() - xo))
+    assert np.array_equal(r.get(), r0)   # the residual is read, not written
+    assert not np.array_equal(xo, x0)
+
+
+@pytest.mark.parametrize("dim,level,base", [(2, 4, 1), (3, 3, 1)])
+def test_psc_cg_histories(oracle_mod, G, ctx, dim, level, base):
+    # additive Schwarz over the vertex blocks is symmetric: CG + V(1,1) PSC
+    O = oracle_mod
+    o, g = make_pair(O, G, ctx, dim, 2, level, base, seed=6)
+    C = G._capi
+    damp = 0.4 if dim == 2 else 0.2  # a node lies in up to 2^d blocks
+    r = o.solve(O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.PSC, damp=damp, pre=1, post=1, compat=False,
+                            rtol=1e-10, maxsteps=80))
+    cfg = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_PSC, damp, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 80, C.FMG_MULTIPLICATIVE, 0)
+    x = g.vector()
+    hist, steps, st = g.solve(cfg, x)
+    assert st == 0 and r.status == 0
+    assert np.array_equal(hist, r.history) and np.array_equal(x.get(), r.x)

@@ -228,3 +228,27 @@ def test_ssc_q1_is_gauss_seidel_in_colour_order(oracle_mod):
     xs, _ = o.ssc(x0, b, np.zeros(n), omega=1.2)
     xo, _ = o.sor(x0, b, np.zeros(n), omega=1.2)
     assert np.array_equal(xs, xo)
+
+
+def test_psc_q1_is_damped_jacobi(oracle_mod):
+    # Q1 vertex blocks hold one node: PSC(damp) is x + damp r / a_ii, r kept
+    O = oracle_mod
+    o = O.Oracle(2, 1, 4, base_level=1)
+    o.set_coefficient(O.K_CELL, np.exp(np.random.default_rng(4).standard_normal(16 * 16)))
+    o.assemble()
+    n = o.nnodes()
+    rng = np.random.default_rng(9)
+    x0, r0 = rng.standard_normal(n), rng.standard_normal(n)
+    xp = o.psc(x0, r0, damp=0.6)
+    xj, _ = o.jacobi(x0, r0, 0.6)
+    assert np.array_equal(xp, xj)
+
+
+def test_psc_preconditioned_cg_converges(oracle_mod):
+    O = oracle_mod
+    o = O.Oracle(2, 2, 4, base_level=1).assemble()
+    # a node lies in up to 2^d vertex blocks: the summed corrections want a
+    # damping of about 1 / 2^(d-1)
+    r = o.solve(O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.PSC, damp=0.4, pre=1, post=1, compat=False,
+                            rtol=1e-10, maxsteps=60))
+    assert r.status == 0 and r.steps < 20, r.steps
