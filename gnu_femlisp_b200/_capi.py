@@ -74,6 +74,10 @@ SIGNATURES = {
     "fmg_get_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "fmg_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong)]),
     "fmg_grid_create": (ctypes.c_int, [_vp] + [ctypes.c_int] * 7 + [ctypes.POINTER(_vp)]),
+    "fmg_grid_create_algebraic": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_long),
+                                                 ctypes.POINTER(_vp)]),
+    "fmg_set_interpolation": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int), _dp, ctypes.c_long, ctypes.c_long]),
     "fmg_grid_destroy": (ctypes.c_int, [_vp]),
     "fmg_grid_nnodes": (ctypes.c_long, [_vp, ctypes.c_int]),
     "fmg_grid_nslots": (ctypes.c_int, [_vp]),

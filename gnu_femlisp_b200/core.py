@@ -120,6 +120,37 @@ class Grid:
         self.n_cells = n0 << level
         self.assembled = False
 
+    @classmethod
+    def algebraic(cls, ctx: Context, sizes) -> "Grid":
+        """``fmg_grid_create_algebraic``: levels 0 .. len(sizes)-1 without
+        geometry; matrices by ``set_matrix``, interpolations by
+        ``set_interpolation``, the rhs by ``set_rhs``."""
+        g = cls.__new__(cls)
+        sz = np.ascontiguousarray(sizes, dtype=np.int64)
+        g.ctx, g.dim, g.order, g.top, g.base, g.nc = ctx, 0, 1, sz.size - 1, 0, 1
+        h = ctypes.c_void_p()
+        ctx.check(ctx._lib.fmg_grid_create_algebraic(ctx.h, int(sz.size), sz.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                                     ctypes.byref(h)), "grid_create_algebraic")
+        g.h = h
+        g.n_cells = 0
+        g.assembled = False
+        return g
+
+    def set_interpolation(self, fine_level: int, start, index, values, ncoarse: int, layout: str = "csr") -> "Grid":
+        """``fmg_set_interpolation``: I from level fine_level-1 to fine_level
+        (rows fine, columns coarse; ``"ccs"``: the arrays of the transpose's
+        rows)."""
+        lay = {"csr": C.FMG_CSR, "ccs": C.FMG_CCS}[layout]
+        st = np.ascontiguousarray(start, dtype=np.int32)
+        ix = np.ascontiguousarray(index, dtype=np.int32)
+        va = np.ascontiguousarray(values, dtype=np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        nfine = self.nnodes(fine_level)
+        self.ctx.check(self._lib.fmg_set_interpolation(self.h, fine_level, lay, st.ctypes.data_as(ip),
+                                                       ix.ctypes.data_as(ip), C.dptr(va), nfine, ncoarse),
+                       "set_interpolation")
+        return self
+
     @property
     def _lib(self):
         return self.ctx._lib

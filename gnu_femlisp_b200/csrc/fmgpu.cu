@@ -18,6 +18,7 @@
 #include <cstring>
 #include <new>
 #include <algorithm>
+#include <string>
 #include <utility>
 
 #include "fmgpu_kernels.cuh"
@@ -49,6 +50,14 @@ struct Lvl {
   double* Ctab = nullptr;
   double* Phi = nullptr;
   std::vector<double> Kbar_h, Ctab_h;  // host copies of the element tables
+  // algebraic levels: the matrix, the interpolation from the level below and
+  // its transpose in compressed rows, and the matrix diagonal (device)
+  struct Csr {
+    long long* start = nullptr;
+    int* index = nullptr;
+    double* value = nullptr;
+  } ca, cp, cpt;
+  double* diag = nullptr;
 };
 
 }  // namespace
@@ -80,6 +89,8 @@ struct fmg_grid {
   bool assembled_once = false;
   std::vector<char> have;      // levels whose matrix is in place
   bool uploaded = false;       // some level matrix came from fmg_set_matrix
+  bool algebraic = false;      // levels without geometry: matrices and interpolations from the host
+  std::vector<char> haveP;     // algebraic: levels whose interpolation from the level below is in place
   bool top_deferred = false;   // the top level's matrix is formed on first use (its rhs is in place)
   // <geometric-ssc>: LU factors of the vertex blocks per level, formed once per assembly
   std::vector<double*> sscF;
@@ -363,6 +374,13 @@ LevelView view(const fmg_grid* g, int l) {
   v.dim = g->dim; v.order = g->order; v.dmask = g->dmask; v.center = g->center;
   v.omega = L.omega;
   v.nc = g->nc;
+  if (g->algebraic) {
+    v.csr = true;
+    v.a = CsrView{L.ca.start, L.ca.index, L.ca.value};
+    v.p = CsrView{L.cp.start, L.cp.index, L.cp.value};
+    v.pt = CsrView{L.cpt.start, L.cpt.index, L.cpt.value};
+    v.diag = L.diag;
+  }
   return v;
 }
 
@@ -541,6 +559,8 @@ int ssc_prepare(fmg_grid* g, int l) {
 
 int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (!c) return set_err(g->ctx, FMG_ERR_ARG, "null configuration");
+  if (g->algebraic && c->smoother != FMG_JACOBI)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "algebraic grids: the Jacobi smoother");
   if (g->nc != 1 && c->smoother != FMG_JACOBI)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "3-component grids: the (block) Jacobi smoother only");
   if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR && c->smoother != FMG_SSC && c->smoother != FMG_PSC)
@@ -677,6 +697,78 @@ int fmg_grid_create(fmg_ctx* c, int dim, int order, int ncomp, int n0, int top_l
   return FMG_OK;
 }
 
+static int ensure_buffers(fmg_grid* g);
+static int finish_levels(fmg_grid* g);
+static bool host_csr(long nrows, long ncols, int layout, const int* start, const int* index, const double* values,
+                     std::vector<long long>& rs, std::vector<int>& ci, std::vector<double>& cv, std::string& err);
+static int upload_csr(fmg_grid* g, Lvl::Csr& d, const std::vector<long long>& rs, const std::vector<int>& ci,
+                      const std::vector<double>& cv);
+static bool hierarchy_complete(const fmg_grid* g);
+
+// A hierarchy of algebraic levels 0 .. nlevels-1 (0 the coarsest) with the
+// given numbers of unknowns: no geometry, the level matrices and the
+// interpolations between the levels come from the host (fmg_set_matrix,
+// fmg_set_interpolation) -- the matrices Femlisp forms on an unstructured or
+// adaptively refined mesh (multilevel-decomposition, geomg.lisp:109-142, with
+// the constrained interpolation of constraints.lisp:58-72).
+int fmg_grid_create_algebraic(fmg_ctx* c, int nlevels, const long* sizes, fmg_grid** out) {
+  if (!c || !out || !sizes) return FMG_ERR_ARG;
+  *out = nullptr;
+  if (nlevels < 1 || nlevels > kMaxLevels) return set_err(c, FMG_ERR_ARG, "nlevels %d out of range", nlevels);
+  for (int l = 0; l < nlevels; ++l)
+    if (sizes[l] < 1 || sizes[l] > (1L << 31) - 1) return set_err(c, FMG_ERR_ARG, "level %d: %ld unknowns", l, sizes[l]);
+  fmg_grid* g = new (std::nothrow) fmg_grid();
+  if (!g) return FMG_ERR_NOMEM;
+  g->ctx = c;
+  c->grids += 1;
+  g->algebraic = true;
+  g->dim = 0; g->order = 1; g->nc = 1; g->n0 = 1;
+  g->top = nlevels - 1; g->base = 0; g->dmask = 0;
+  g->nslots = 1; g->center = 0;
+  g->lev.resize(nlevels);
+  for (int l = 0; l < nlevels; ++l) {
+    Lvl& L = g->lev[l];
+    L.N = sizes[l];
+    L.Np = pad64(L.N);
+    L.n = 0; L.M = 0; L.h = 0.0;
+  }
+  *out = g;
+  return FMG_OK;
+}
+
+// The interpolation I from level fine_level - 1 to fine_level of an algebraic
+// grid (nfine x ncoarse, compressed rows or columns): prolongate xf += I xc,
+// restrict rc = I^T rf (multigrid.lisp:202-252).  Rows of constrained fine
+// unknowns and columns of constrained coarse ones are empty, as in Femlisp's
+// constrained interpolation.
+int fmg_set_interpolation(fmg_grid* g, int fine_level, int layout, const int* start, const int* index,
+                          const double* values, long nfine, long ncoarse) {
+  if (!g || !start) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  if (!g->algebraic) return set_err(c, FMG_ERR_UNSUPPORTED, "interpolations are built in on structured grids");
+  if (fine_level <= g->base || fine_level > g->top) return set_err(c, FMG_ERR_ARG, "level %d has no level below", fine_level);
+  if (layout != FMG_CSR && layout != FMG_CCS) return set_err(c, FMG_ERR_ARG, "unknown matrix layout %d", layout);
+  Lvl& F = g->lev[fine_level];
+  if (nfine != F.N || ncoarse != g->lev[fine_level - 1].N)
+    return set_err(c, FMG_ERR_ARG, "interpolation to level %d is %lld x %lld, got %ld x %ld", fine_level, F.N,
+                   g->lev[fine_level - 1].N, nfine, ncoarse);
+  int rc;
+  FMG_CK(c, cudaSetDevice(c->device));
+  if ((rc = ensure_buffers(g))) return rc;
+  std::vector<long long> rs, rst;
+  std::vector<int> ci, cit;
+  std::vector<double> cv, cvt;
+  std::string err;
+  if (!host_csr(nfine, ncoarse, layout, start, index, values, rs, ci, cv, err) ||
+      !host_csr(ncoarse, nfine, layout == FMG_CSR ? FMG_CCS : FMG_CSR, start, index, values, rst, cit, cvt, err))
+    return set_err(c, FMG_ERR_ARG, "%s", err.c_str());
+  if ((rc = upload_csr(g, F.cp, rs, ci, cv)) || (rc = upload_csr(g, F.cpt, rst, cit, cvt))) return rc;
+  g->assembled = false;
+  if ((int)g->haveP.size() != g->top + 1) g->haveP.assign(g->top + 1, 0);
+  g->haveP[fine_level] = 1;
+  return hierarchy_complete(g) ? finish_levels(g) : FMG_OK;
+}
+
 static void mixed_vec_delete(MixedVec* m);
 
 static void grid_release(fmg_grid* g) {
@@ -710,6 +802,7 @@ long fmg_grid_nnodes(const fmg_grid* g, int level) {
 int fmg_grid_nslots(const fmg_grid* g) { return g ? g->nslots : -1; }
 
 int fmg_set_coefficient(fmg_grid* g, int kind, const double* host, long n) {
+  if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !host) return FMG_ERR_ARG;
   long long ncell = 1;
   for (int k = 0; k < g->dim; ++k) ncell *= g->lev[g->top].n;
@@ -763,8 +856,40 @@ int fmg_set_coefficient(fmg_grid* g, int kind, const double* host, long n) {
 
 // device buffers of a hierarchy, allocated by the first assembly and reused
 // by later ones (only the coefficient data change between assemblies)
+// the device buffers of an algebraic hierarchy (level vectors, coarse LU,
+// solver vectors); the matrices and interpolations arrive separately
+static int ensure_buffers_alg(fmg_grid* g) {
+  int rc;
+  const Lvl& T = g->lev[g->top];
+  if ((rc = dalloc(g, &g->rhs, T.Np))) return rc;
+  const long long nb = g->lev[g->base].N;
+  if (nb > 1024)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "base level has %lld unknowns; the dense coarse solve takes <= 1024",
+                   nb);
+  g->nbase = (int)nb;
+  const long long nn = nb * nb;
+  if ((rc = dalloc(g, &g->lu, nn)) || (rc = dalloc(g, &g->lux, nn)) || (rc = dalloc(g, &g->ainvT, nn)) ||
+      (rc = dalloc(g, (double**)&g->piv, nb)))
+    return rc;
+  for (int l = g->base; l < g->top; ++l) {
+    Lvl& L = g->lev[l];
+    if ((rc = dalloc(g, &L.sol[0], L.Np)) || (rc = dalloc(g, &L.sol[1], L.Np)) || (rc = dalloc(g, &L.rhs, L.Np)) ||
+        (rc = dalloc(g, &L.res, L.Np)))
+      return rc;
+  }
+  if ((rc = dalloc(g, &g->scal, S_COUNT))) return rc;
+  if ((rc = dalloc(g, &g->part, nchunks(T.Np) + 1))) return rc;
+  if ((rc = dalloc(g, (double**)&g->counter, 1))) return rc;
+  double** tv[] = {&g->p, &g->a, &g->w, &g->w2, &g->q, &g->r, &g->xs, &g->xs2};
+  for (double** v : tv)
+    if ((rc = dalloc(g, v, T.Np))) return rc;
+  g->assembled_once = true;
+  return FMG_OK;
+}
+
 static int ensure_buffers(fmg_grid* g) {
   if (g->assembled_once) return FMG_OK;
+  if (g->algebraic) return ensure_buffers_alg(g);
   int rc;
   const Lvl& T = g->lev[g->top];
   long long ncell_top = 1, ncell_kq = 0;
@@ -822,6 +947,7 @@ static int ensure_top(fmg_grid* g);
 
 int fmg_assemble_levels(fmg_grid* g, int mode) {
   if (!g) return FMG_ERR_ARG;
+  if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   fmg_ctx* c = g->ctx;
   if (mode != FMG_ASSEMBLE_REDISCRETIZE && mode != FMG_ASSEMBLE_GALERKIN)
     return set_err(c, FMG_ERR_ARG, "unknown assembly mode %d", mode);
@@ -926,6 +1052,98 @@ static int finish_levels(fmg_grid* g) {
 // sparse-matrix->ccs, sparselu.lisp:226-263) over the grid's numbering
 // (node-major, lexicographic nodes, x fastest), scattered into the stencil-slot
 // storage on the host and copied to the device in one piece.
+// Compressed rows (columns ascending, duplicates summed, exact zeros dropped)
+// of an nrows x ncols matrix given as compressed rows or columns; false (and
+// the message) on a malformed input.
+static bool host_csr(long nrows, long ncols, int layout, const int* start, const int* index, const double* values,
+                     std::vector<long long>& rs, std::vector<int>& ci, std::vector<double>& cv, std::string& err) {
+  const long nlines = layout == FMG_CSR ? nrows : ncols, nother = layout == FMG_CSR ? ncols : nrows;
+  if (start[0] != 0) { err = "start[0] must be 0"; return false; }
+  std::vector<std::vector<std::pair<int, double>>> rows((size_t)nrows);
+  for (long a = 0; a < nlines; ++a) {
+    if (start[a + 1] < start[a]) { err = "start decreases at " + std::to_string(a); return false; }
+    for (int e = start[a]; e < start[a + 1]; ++e) {
+      const long b = index[e];
+      if (b < 0 || b >= nother) { err = "index out of range at entry " + std::to_string(e); return false; }
+      if (values[e] == 0.0) continue;
+      const long row = layout == FMG_CSR ? a : b, col = layout == FMG_CSR ? b : a;
+      rows[(size_t)row].push_back({(int)col, values[e]});
+    }
+  }
+  rs.assign((size_t)nrows + 1, 0);
+  ci.clear();
+  cv.clear();
+  for (long i = 0; i < nrows; ++i) {
+    auto& r = rows[(size_t)i];
+    std::stable_sort(r.begin(), r.end(), [](const std::pair<int, double>& x, const std::pair<int, double>& y) {
+      return x.first < y.first;
+    });
+    for (size_t k = 0; k < r.size(); ++k) {
+      if (!ci.empty() && (long long)ci.size() > rs[(size_t)i] && ci.back() == r[k].first) cv.back() += r[k].second;
+      else { ci.push_back(r[k].first); cv.push_back(r[k].second); }
+    }
+    rs[(size_t)i + 1] = (long long)ci.size();
+  }
+  return true;
+}
+
+static int upload_csr(fmg_grid* g, Lvl::Csr& d, const std::vector<long long>& rs, const std::vector<int>& ci,
+                      const std::vector<double>& cv) {
+  dfree(g, d.start); dfree(g, d.index); dfree(g, d.value);
+  d = Lvl::Csr{};
+  int rc;
+  if ((rc = dalloc(g, (double**)&d.start, (long long)rs.size())) ||
+      (rc = dalloc(g, (double**)&d.index, ((long long)ci.size() + 1) / 2)) ||
+      (rc = dalloc(g, &d.value, (long long)cv.size())))
+    return rc;
+  cudaStream_t st = g->ctx->stream;
+  FMG_CK(g->ctx, cudaMemcpyAsync(d.start, rs.data(), rs.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
+  if (!ci.empty()) {
+    FMG_CK(g->ctx, cudaMemcpyAsync(d.index, ci.data(), ci.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    FMG_CK(g->ctx, cudaMemcpyAsync(d.value, cv.data(), cv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  FMG_CK(g->ctx, cudaStreamSynchronize(st));
+  return FMG_OK;
+}
+
+// every level matrix in place and, on an algebraic grid, every interpolation
+static bool hierarchy_complete(const fmg_grid* g) {
+  for (int m = g->base; m <= g->top; ++m) {
+    if ((int)g->have.size() <= m || !g->have[m]) return false;
+    if (g->algebraic && m > g->base && ((int)g->haveP.size() <= m || !g->haveP[m])) return false;
+  }
+  return true;
+}
+
+// fmg_set_matrix on an algebraic grid: the level matrix as compressed rows
+// and its diagonal
+static int set_matrix_alg(fmg_grid* g, int level, int layout, const int* start, const int* index,
+                          const double* values, long n) {
+  Lvl& L = g->lev[level];
+  if (n != L.N) return set_err(g->ctx, FMG_ERR_ARG, "level %d has %lld rows, got %ld", level, L.N, n);
+  std::vector<long long> rs;
+  std::vector<int> ci;
+  std::vector<double> cv;
+  std::string err;
+  if (!host_csr(n, n, layout, start, index, values, rs, ci, cv, err))
+    return set_err(g->ctx, FMG_ERR_ARG, "%s", err.c_str());
+  std::vector<double> dg((size_t)n, 0.0);
+  for (long i = 0; i < n; ++i)
+    for (long long e = rs[(size_t)i]; e < rs[(size_t)i + 1]; ++e)
+      if (ci[(size_t)e] == i) dg[(size_t)i] = cv[(size_t)e];
+  int rc;
+  if ((rc = upload_csr(g, L.ca, rs, ci, cv))) return rc;
+  dfree(g, L.diag);
+  L.diag = nullptr;
+  if ((rc = upload(g, &L.diag, dg))) return rc;
+  FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+  g->assembled = false;
+  if ((int)g->have.size() != g->top + 1) g->have.assign(g->top + 1, 0);
+  g->have[level] = 1;
+  g->uploaded = true;
+  return hierarchy_complete(g) ? finish_levels(g) : FMG_OK;
+}
+
 int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const int* index, const double* values,
                    long n) {
   if (!g || !start || (!index && n > 0) || (!values && n > 0)) return FMG_ERR_ARG;
@@ -941,6 +1159,7 @@ int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const i
   int rc;
   FMG_CK(c, cudaSetDevice(c->device));
   if ((rc = ensure_buffers(g))) return rc;
+  if (g->algebraic) return set_matrix_alg(g, level, layout, start, index, values, n);
   const long long M = L.M, Np = L.Np;
   std::vector<double> H((size_t)g->nslots * nc * nc * Np, 0.0);
   for (long a = 0; a < n; ++a) {
@@ -976,9 +1195,7 @@ int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const i
   g->have[level] = 1;
   g->uploaded = true;
   if (level == g->top) g->top_deferred = false;
-  for (int m = g->base; m <= g->top; ++m)
-    if (!g->have[m]) return FMG_OK;  // the hierarchy is complete with the last level
-  return finish_levels(g);
+  return hierarchy_complete(g) ? finish_levels(g) : FMG_OK;  // complete with the last level
 }
 
 int fmg_set_rhs(fmg_grid* g, const double* host, long n) {
@@ -996,6 +1213,7 @@ int fmg_set_rhs(fmg_grid* g, const double* host, long n) {
 
 int fmg_get_matrix(fmg_grid* g, int level, double* host) {
   if (!g || !host) return FMG_ERR_ARG;
+  if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   if (level < g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d out of range", level);
   if (level == g->top) FMG_RC(ensure_top(g));
@@ -1172,6 +1390,7 @@ int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
 }
 
 int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
   if (level == g->top) FMG_RC(ensure_top(g));
@@ -1180,6 +1399,7 @@ int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
 }
 
 int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric SSC: scalar grids");
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level) || x == b || x == r)
@@ -1192,6 +1412,7 @@ int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
 }
 
 int fmg_psc(fmg_grid* g, int level, double damp, fmg_vec* x, const fmg_vec* r) {
+  if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric PSC: scalar grids");
   if (vec_check(x, g, level) || vec_check(r, g, level) || x == r) return FMG_ERR_ARG;
@@ -1811,6 +2032,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (!mcfg || vec_check(xv, g, g->top) || !nouter || !ninner || !status) return FMG_ERR_ARG;
+  if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed solve: structured grids");
   if (cfg->fmg) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "mixed solve: V/W cycles (fmg = 0)");
   if (cfg->smoother != FMG_JACOBI || cfg->combination != FMG_MULTIPLICATIVE || cfg->gamma != 1 ||
       g->base >= g->top || cfg->post_steps < 1)
@@ -2197,6 +2419,7 @@ void learn_loss_grad_levels(fmg_grid* g, const fmg_solve_cfg& cf, const double* 
 }
 
 int learn_cfg_check(fmg_grid* g, const fmg_solve_cfg* cf) {
+  if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "training: structured grids");
   int rc = check_cfg(g, cf);
   if (rc) return rc;
   if (cf->smoother != FMG_JACOBI || cf->combination != FMG_MULTIPLICATIVE || cf->pre_steps != 1 ||
@@ -2564,6 +2787,7 @@ int learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mc
                   double* rho_learned, int* accepted) {
   if (!g || !accepted) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
+  if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "judge: structured grids");
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
   if (cfg->smoother != FMG_JACOBI || g->top <= g->base)

@@ -6,12 +6,25 @@
 namespace fmg {
 
 // what a kernel needs to know about one level
+// compressed rows of a sparse matrix on the device (columns ascending in a row)
+struct CsrView {
+  const long long* start = nullptr;  // rows + 1 offsets
+  const int* index = nullptr;
+  const double* value = nullptr;
+};
+
 struct LevelView {
   const double* A;      // [slot][Np], or [slot][k][l][Np] for nc = 3
   long long N, Np, M;   // nodes, padded stride, nodes per direction
   int dim, order, dmask, center;
   const double* omega;  // per-node damping or nullptr
   int nc = 1;           // components per node (1, or 3 for elasticity)
+  // algebraic levels (no geometry): the matrix in compressed rows, its
+  // diagonal, and the interpolation from the level below, I (rows of this
+  // level) and I^T (rows of the level below); A, M and dim are then unused
+  bool csr = false;
+  CsrView a, p, pt;
+  const double* diag = nullptr;
 };
 
 // arguments of the assembly kernel of one level

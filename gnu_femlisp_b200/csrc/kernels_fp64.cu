@@ -828,6 +828,67 @@ k_psc_gather_q2(long long N, long long M, int dmask, double damp, const double* 
   x[i] = xi;
 }
 
+// ------------------------------------------------------ algebraic levels
+// Compressed-row forms of the level operators (matrices handed over by the
+// host, e.g. from sparse-matrix->ccs on an unstructured or adaptive mesh).
+// Each row sums its entries in stored (column-ascending) order with fma, the
+// order in which the stencil forms sum their slots, so a structured level
+// given as compressed rows yields the structured results bit for bit.
+
+// y = A x, or r = b - A x (b may alias r)
+__global__ void __launch_bounds__(kBlock)
+k_csr_spmv(long long N, CsrView a, const double* __restrict__ x, const double* b, double* y, int res) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s = 0.0;
+  for (long long e = a.start[i]; e < a.start[i + 1]; ++e) s = fma(a.value[e], __ldg(x + a.index[e]), s);
+  y[i] = res ? b[i] - s : s;
+}
+
+// compute-residual fused with the following <jacobi> step (as k_jacobi_res)
+__global__ void __launch_bounds__(kBlock)
+k_csr_jacobi_res(long long N, CsrView a, const double* __restrict__ diag, double damp,
+                 const double* __restrict__ omega, const double* __restrict__ x, const double* b,
+                 double* __restrict__ xout, double* r, int write_r) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s = 0.0;
+  for (long long e = a.start[i]; e < a.start[i + 1]; ++e) s = fma(a.value[e], __ldg(x + a.index[e]), s);
+  const double t = (b[i] - s) / diag[i];
+  if (write_r) r[i] = t;
+  xout[i] = fma(omega ? omega[i] : damp, t, x[i]);
+}
+
+// rc = I^T rf row by row of I^T (fine entries ascending); the coarse rhs
+// takes rc, the coarse solution 0 (the :after methods of restrict)
+__global__ void __launch_bounds__(kBlock)
+k_csr_restrict(long long NC, CsrView pt, const double* __restrict__ rf, double* rc, double* rhsc, double* solc) {
+  const long long J = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= NC) return;
+  double s = 0.0;
+  for (long long e = pt.start[J]; e < pt.start[J + 1]; ++e) s = fma(pt.value[e], __ldg(rf + pt.index[e]), s);
+  rc[J] = s;
+  if (rhsc) rhsc[J] = s;
+  if (solc) solc[J] = 0.0;
+}
+
+// xf += I xc (coarse entries ascending)
+__global__ void __launch_bounds__(kBlock)
+k_csr_prolong(long long NF, CsrView p, const double* __restrict__ xc, double* xf) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NF || p.start[i] == p.start[i + 1]) return;  // constrained rows keep their value
+  double s = 0.0;
+  for (long long e = p.start[i]; e < p.start[i + 1]; ++e) s = fma(p.value[e], __ldg(xc + p.index[e]), s);
+  xf[i] = xf[i] + s;
+}
+
+// the level matrix as a dense row-major n x n array (zeros written beforehand)
+__global__ void __launch_bounds__(kBlock) k_csr_densify(long long N, CsrView a, double* Dm) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (long long e = a.start[i]; e < a.start[i + 1]; ++e) Dm[i * N + a.index[e]] = a.value[e];
+}
+
 // -------------------------------------------------------------- transfers
 template <int P>
 __device__ __forceinline__ int restrict_1d(long long J, long long* off, double* w) {
@@ -2178,6 +2239,12 @@ static inline unsigned grid1(long long n, int bs = kBlock) { return (unsigned)((
 
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
                  const Reduce* R, cudaStream_t st) {
+  if (L.csr) {  // the reduction as a separate DR4096 pass
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_csr_spmv<<<grid1(L.N), kBlock, 0, st>>>(L.N, L.a, x, b, y, b ? 1 : 0);
+    if (dv) launch_dot(y, dv, L.N, *R, st);
+    return;
+  }
   if (L.nc == 3) {  // 3 x 3 blocks: the reduction, if any, as a separate DR4096 pass
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (L.order == 2) {
@@ -2212,6 +2279,10 @@ void launch_spmv(const LevelView& L, const double* x, const double* b, double* y
 
 void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool write_r, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.csr) {
+    k_jacobi<<<grid1(L.N), kBlock, 0, st>>>(L.diag, L.N, damp, L.omega, x, r, write_r ? 1 : 0);
+    return;
+  }
   if (L.nc == 3) {
     k_jacobi3<<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.center, damp, L.omega, x, r, write_r ? 1 : 0);
     return;
@@ -2230,6 +2301,12 @@ void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool w
 void launch_jacobi_res(const LevelView& L, double damp, const double* x, const double* b, double* xout,
                        double* r, bool write_r, const double* dv, const Reduce* R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.csr) {
+    k_csr_jacobi_res<<<grid1(L.N), kBlock, 0, st>>>(L.N, L.a, L.diag, damp, L.omega, x, b, xout, r,
+                                                      write_r ? 1 : 0);
+    if (dv) launch_dot(xout, dv, L.N, *R, st);
+    return;
+  }
   if (L.nc == 3) {
     if (L.order == 2)
       k_jacobi_res3<2><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
@@ -2344,6 +2421,10 @@ static inline dim3 xfer_grid(long long M, int dim) {
 void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, double* rc, double* rhsc,
                      double* solc, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (F.csr) {
+    k_csr_restrict<<<grid1(Cl.N), kBlock, 0, st>>>(Cl.N, F.pt, rf, rc, rhsc, solc);
+    return;
+  }
   if (F.nc == 3) {
     if (F.order == 2)
       k_restrict3<2><<<xfer_grid(Cl.M, 3), dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc);
@@ -2358,6 +2439,10 @@ void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, 
 
 void launch_prolong(const LevelView& Cl, const LevelView& F, const double* xc, double* xf, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (F.csr) {
+    k_csr_prolong<<<grid1(F.N), kBlock, 0, st>>>(F.N, F.p, xc, xf);
+    return;
+  }
   if (F.nc == 3) {
     if (F.order == 2)
       k_prolong3<2><<<xfer_grid(F.M, 3), dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf);
@@ -2624,6 +2709,10 @@ long long q2_slot_pos(int dim, long long M, long long i, int s, bool colour_majo
 
 void launch_densify(const LevelView& L, double* Dm, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (L.csr) {
+    k_csr_densify<<<grid1(L.N), kBlock, 0, st>>>(L.N, L.a, Dm);
+    return;
+  }
   if (L.nc == 3) {
     if (L.order == 2) k_densify3<2><<<grid1(L.N * St<3, 2>::NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);
     else k_densify3<1><<<grid1(L.N * St<3, 1>::NS), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, Dm);

@@ -120,6 +120,28 @@ int fmg_launch_count(long long* out);
    :external-boundary constraint coefficient, cdr.lisp:184-185). */
 int fmg_grid_create(fmg_ctx* ctx, int dim, int order, int ncomp, int n0, int top_level,
                     int base_level, int dirichlet_mask, fmg_grid** grid);
+/* A hierarchy of algebraic levels 0 .. nlevels-1 (0 the coarsest, sizes[l]
+   unknowns each) without geometry, for the matrices Femlisp forms on
+   unstructured or adaptively refined meshes (multilevel-decomposition,
+   geomg.lisp:109-142; constraints.lisp:58-151): the level matrices come
+   through fmg_set_matrix (compressed rows or the columns of
+   sparse-matrix->ccs over the caller's numbering), the interpolation between
+   each level and the one below through fmg_set_interpolation, the top-level
+   rhs through fmg_set_rhs.  Once every matrix and interpolation is in place
+   the base level's LU is formed and fmg_solve / fmg_vcycle / the level
+   operators run the same iteration as on structured grids (Jacobi smoother;
+   the base level at most 1024 unknowns).  Rows sum in column order, so a
+   structured level handed over this way gives its structured results bit
+   for bit.  Geometry-bound calls (fmg_assemble*, fmg_set_coefficient,
+   fmg_get_matrix, SOR/SSC/PSC, the mixed solve, the damping network) return
+   FMG_ERR_UNSUPPORTED. */
+int fmg_grid_create_algebraic(fmg_ctx* ctx, int nlevels, const long* sizes, fmg_grid** grid);
+/* The interpolation I from level fine_level - 1 to fine_level (nfine x
+   ncoarse; FMG_CSR or FMG_CCS): prolongate xf += I xc, restrict rc = I^T rf
+   (multigrid.lisp:202-252); constrained fine rows and coarse columns empty
+   (constrained-interpolation-matrix, constraints.lisp:58-72). */
+int fmg_set_interpolation(fmg_grid* grid, int fine_level, int layout, const int* start, const int* index,
+                          const double* values, long nfine, long ncoarse);
 int fmg_grid_destroy(fmg_grid* grid);
 long fmg_grid_nnodes(const fmg_grid* grid, int level);
 int fmg_grid_nslots(const fmg_grid* grid);

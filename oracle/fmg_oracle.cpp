@@ -217,11 +217,22 @@ ElasticTables make_elastic_tables(const Tables& T) {
 }
 
 // ---------------------------------------------------------------- hierarchy
+// compressed rows, columns ascending
+struct Csr {
+  std::vector<long> start;
+  std::vector<int> index;
+  std::vector<double> value;
+};
+
 struct Level {
   long n = 0, M = 0, N = 0;
   double h = 0;
   std::vector<double> A;        // [slot][node][nc][nc]
   std::vector<double> omega;    // optional per-node damping (size N)
+  // algebraic levels: the matrix, its diagonal, the interpolation from the
+  // level below (rows of this level) and its transpose (rows of the level below)
+  Csr a, p, pt;
+  std::vector<double> dg;
 };
 
 struct Hier {
@@ -240,6 +251,7 @@ struct Hier {
   std::vector<double> ainv;     // base-level inverse, row-major
   long nbase = 0;
   bool assembled = false;
+  bool algebraic = false;       // levels without geometry (matrices and interpolations given)
 
   // V-cycle state (multigrid.lisp:101-116)
   std::vector<double*> sol, rhsv, res;
@@ -447,7 +459,10 @@ void build_coarse_inverse(Hier& H) {
   long n = L.N * nc;
   H.nbase = n;
   std::vector<double> A((size_t)n * n, 0.0);
-  for (long i = 0; i < L.N; ++i)
+  if (H.algebraic)
+    for (long i = 0; i < L.N; ++i)
+      for (long e = L.a.start[i]; e < L.a.start[i + 1]; ++e) A[(size_t)i * n + L.a.index[e]] = L.a.value[e];
+  for (long i = 0; i < (H.algebraic ? 0 : L.N); ++i)
     for (int s = 0; s < H.nslots; ++s) {
       long o[3];
       slot_offset(H, s, o);
@@ -498,6 +513,11 @@ void build_coarse_inverse(Hier& H) {
 
 // ---------------------------------------------------------------- kernels
 inline double row_sum(const Hier& H, const Level& L, long i, const double* x) {
+  if (H.algebraic) {  // stored entries, columns ascending
+    double acc = 0.0;
+    for (long e = L.a.start[i]; e < L.a.start[i + 1]; ++e) acc = std::fma(L.a.value[e], x[L.a.index[e]], acc);
+    return acc;
+  }
   long ci[3];
   coords(H, L.M, i, ci);
   double acc = 0.0;
@@ -607,6 +627,7 @@ void block_solve(const double* Bm, int nc, const double* r, double* t) {
 }
 
 inline double diag(const Hier& H, const Level& L, long i) {
+  if (H.algebraic) return L.dg[i];
   long z[3] = {0, 0, 0};
   return L.A[(size_t)slot_of(H, z) * L.N + i];
 }
@@ -853,6 +874,14 @@ int prolong_stencil1d(int order, long I, long* J, double* w) {
 void restrict_(const Hier& H, int lf, const double* rf, double* rc) {
   const Level& F = H.lev[lf];
   const Level& C = H.lev[lf - 1];
+  if (H.algebraic) {  // rc = I^T rf, fine entries ascending
+    for (long J = 0; J < C.N; ++J) {
+      double acc = 0.0;
+      for (long e = F.pt.start[J]; e < F.pt.start[J + 1]; ++e) acc = std::fma(F.pt.value[e], rf[F.pt.index[e]], acc);
+      rc[J] = acc;
+    }
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (long J = 0; J < C.N; ++J) {
     long cJ[3];
@@ -886,6 +915,15 @@ void restrict_(const Hier& H, int lf, const double* rf, double* rc) {
 void prolongate(const Hier& H, int lc, const double* xc, double* xf, bool constrained) {
   const Level& C = H.lev[lc];
   const Level& F = H.lev[lc + 1];
+  if (H.algebraic) {  // xf += I xc, coarse entries ascending; empty (constrained) rows untouched
+    for (long i = 0; i < F.N; ++i) {
+      if (F.p.start[i] == F.p.start[i + 1]) continue;
+      double acc = 0.0;
+      for (long e = F.p.start[i]; e < F.p.start[i + 1]; ++e) acc = std::fma(F.p.value[e], xc[F.p.index[e]], acc);
+      xf[i] = xf[i] + acc;
+    }
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < F.N; ++i) {
     long fi[3];
@@ -1199,6 +1237,57 @@ int ora_set_matrix(void* h, int level, const double* a) {
   return 0;
 }
 
+// Algebraic hierarchies (the counterpart of fmg_grid_create_algebraic):
+// levels 0 .. nlevels-1 of the given sizes, matrices and interpolations as
+// compressed rows with columns ascending.
+void* ora_create_algebraic(int nlevels, const long* sizes) {
+  if (nlevels < 1 || nlevels > 16) return nullptr;
+  Hier* H = new Hier();
+  H->algebraic = true;
+  H->dim = 0; H->order = 1; H->nc = 1; H->n0 = 1;
+  H->top = nlevels - 1; H->base = 0; H->dmask = 0;
+  H->span = 1; H->nslots = 1;
+  H->lev.resize(nlevels);
+  for (int l = 0; l < nlevels; ++l) H->lev[l].N = sizes[l];
+  return H;
+}
+
+int ora_set_csr_matrix(void* h, int level, const long* start, const int* index, const double* value) {
+  Hier& H = *(Hier*)h;
+  if (!H.algebraic || level < H.base || level > H.top) return -1;
+  Level& L = H.lev[level];
+  L.a.start.assign(start, start + L.N + 1);
+  L.a.index.assign(index, index + start[L.N]);
+  L.a.value.assign(value, value + start[L.N]);
+  L.dg.assign(L.N, 0.0);
+  for (long i = 0; i < L.N; ++i)
+    for (long e = start[i]; e < start[i + 1]; ++e)
+      if (index[e] == i) L.dg[i] = value[e];
+  H.assembled = false;
+  return 0;
+}
+
+int ora_set_interpolation(void* h, int fine_level, const long* start, const int* index, const double* value) {
+  Hier& H = *(Hier*)h;
+  if (!H.algebraic || fine_level <= H.base || fine_level > H.top) return -1;
+  Level& F = H.lev[fine_level];
+  const long NC = H.lev[fine_level - 1].N;
+  F.p.start.assign(start, start + F.N + 1);
+  F.p.index.assign(index, index + start[F.N]);
+  F.p.value.assign(value, value + start[F.N]);
+  std::vector<std::vector<std::pair<int, double>>> cols(NC);
+  for (long i = 0; i < F.N; ++i)
+    for (long e = start[i]; e < start[i + 1]; ++e) cols[index[e]].push_back({(int)i, value[e]});
+  F.pt = Csr{};
+  F.pt.start.assign(1, 0);
+  for (long J = 0; J < NC; ++J) {
+    for (auto& q : cols[J]) { F.pt.index.push_back(q.first); F.pt.value.push_back(q.second); }
+    F.pt.start.push_back((long)F.pt.index.size());
+  }
+  H.assembled = false;
+  return 0;
+}
+
 int ora_set_rhs(void* h, const double* b) {
   Hier& H = *(Hier*)h;
   H.rhs.assign(b, b + (size_t)H.lev[H.top].N * H.nc);
@@ -1207,8 +1296,12 @@ int ora_set_rhs(void* h, const double* b) {
 
 int ora_finish_levels(void* h) {
   Hier& H = *(Hier*)h;
-  for (int l = H.base; l <= H.top; ++l)
-    if (H.lev[l].A.size() != (size_t)H.nslots * H.nc * H.nc * H.lev[l].N) return -1;
+  for (int l = H.base; l <= H.top; ++l) {
+    const Level& L = H.lev[l];
+    if (H.algebraic ? (L.a.start.size() != (size_t)L.N + 1 || (l > H.base && L.p.start.size() != (size_t)L.N + 1))
+                    : L.A.size() != (size_t)H.nslots * H.nc * H.nc * L.N)
+      return -1;
+  }
   if (H.rhs.size() != (size_t)H.lev[H.top].N * H.nc) H.rhs.assign((size_t)H.lev[H.top].N * H.nc, 0.0);
   build_coarse_inverse(H);
   H.assembled = true;
@@ -1323,7 +1416,7 @@ int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* 
 int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hist_len, int* nsteps) {
   Hier& H = *(Hier*)h;
   if (!H.assembled) return -1;
-  if (H.nc != 1 && cfg->smoother != ORA_JACOBI) return -2;
+  if ((H.nc != 1 || H.algebraic) && cfg->smoother != ORA_JACOBI) return -2;
   const ora_solve_cfg& c = *cfg;
   const int top = H.top;
   const long n = vec_len(H, top);

@@ -82,6 +82,10 @@ long ora_nnodes(void* h, int level);
 int ora_nslots(void* h);
 int ora_set_matrix(void* h, int level, const double* a);   /* level matrix in the ora_get_matrix layout */
 int ora_set_rhs(void* h, const double* b);                 /* top-level rhs */
+/* algebraic hierarchies: levels 0 .. nlevels-1, compressed rows (columns ascending) */
+void* ora_create_algebraic(int nlevels, const long* sizes);
+int ora_set_csr_matrix(void* h, int level, const long* start, const int* index, const double* value);
+int ora_set_interpolation(void* h, int fine_level, const long* start, const int* index, const double* value);
 int ora_finish_levels(void* h);                            /* coarse inverse once every level is set */
 int ora_get_matrix(void* h, int level, double* out);      /* [slot][k][l][node] (nc x nc blocks) */
 int ora_get_rhs(void* h, double* out);

@@ -69,6 +69,11 @@ def lib():
         for name in ("ora_get_matrix", "ora_set_matrix"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.ora_set_rhs.argtypes = [ctypes.c_void_p, _dp]
+        L.ora_create_algebraic.restype = ctypes.c_void_p
+        L.ora_create_algebraic.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
+        _lp, _ip = ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)
+        L.ora_set_csr_matrix.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _ip, _dp]
+        L.ora_set_interpolation.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _ip, _dp]
         L.ora_finish_levels.argtypes = [ctypes.c_void_p]
         L.ora_get_rhs.argtypes = [ctypes.c_void_p, _dp]
         L.ora_get_coarse_inverse.argtypes = [ctypes.c_void_p, _dp]
@@ -164,6 +169,40 @@ class Oracle:
             assert lib().ora_set_matrix(self.h, level, _p(a)) == 0
         b = np.ascontiguousarray(rhs, dtype=np.float64)
         assert b.size == self.nnodes() * self.nc
+        assert lib().ora_set_rhs(self.h, _p(b)) == 0
+        rc = lib().ora_finish_levels(self.h)
+        if rc:
+            raise RuntimeError(f"ora_finish_levels rc={rc}")
+        return self
+
+    @classmethod
+    def algebraic(cls, sizes):
+        """An algebraic hierarchy (levels 0 .. len(sizes)-1 without geometry)."""
+        o = cls.__new__(cls)
+        sz = np.ascontiguousarray(sizes, dtype=np.int64)
+        o.h = lib().ora_create_algebraic(int(sz.size), sz.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
+        assert o.h
+        o.dim, o.order, o.nc, o.top, o.base = 0, 1, 1, sz.size - 1, 0
+        return o
+
+    @staticmethod
+    def _csr_args(start, index, value):
+        st = np.ascontiguousarray(start, dtype=np.int64)
+        ix = np.ascontiguousarray(index, dtype=np.int32)
+        va = np.ascontiguousarray(value, dtype=np.float64)
+        return (st, ix, va), (st.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                              ix.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(va))
+
+    def set_csr_matrix(self, level, start, index, value):
+        keep, args = self._csr_args(start, index, value)
+        assert lib().ora_set_csr_matrix(self.h, level, *args) == 0
+
+    def set_interpolation(self, fine_level, start, index, value):
+        keep, args = self._csr_args(start, index, value)
+        assert lib().ora_set_interpolation(self.h, fine_level, *args) == 0
+
+    def finish(self, rhs):
+        b = np.ascontiguousarray(rhs, dtype=np.float64)
         assert lib().ora_set_rhs(self.h, _p(b)) == 0
         rc = lib().ora_finish_levels(self.h)
         if rc:

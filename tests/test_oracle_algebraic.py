@@ -1,0 +1,37 @@
+"""The oracle's algebraic hierarchies (no GPU): a structured hierarchy given as
+compressed rows (its level matrices and its constrained interpolations)
+iterates bit for bit like the structured one, and an irregular problem with
+no grid behind it (a graph Laplacian on random points, aggregation
+interpolations, Galerkin coarse matrices) is solved by CG + V(1,1) Jacobi."""
+import numpy as np
+import pytest
+
+from _hier import from_structured, irregular, oracle_of
+
+
+@pytest.mark.parametrize("dim,order,level,base", [(2, 1, 4, 1), (3, 1, 3, 1), (2, 2, 3, 1)])
+@pytest.mark.parametrize("method,compat", [("cg", False), ("cg", True), ("mg", False)])
+def test_structured_as_algebraic(oracle_mod, dim, order, level, base, method, compat):
+    O = oracle_mod
+    o = O.Oracle(dim, order, level, base_level=base)
+    o.set_coefficient(O.K_CELL, np.exp(np.random.default_rng(dim).standard_normal((1 << level) ** dim)))
+    o.assemble()
+    a = oracle_of(O, *from_structured(o, dim, order))
+    m = O.METHOD_CG_MG if method == "cg" else O.METHOD_MG
+    cfg = O.solve_cfg(method=m, smoother=O.JACOBI, damp=0.6, pre=1, post=1, compat=compat, rtol=1e-10,
+                      maxsteps=60)
+    rs, ra = o.solve(cfg), a.solve(cfg)
+    assert np.array_equal(rs.history, ra.history) and np.array_equal(rs.x, ra.x)
+
+
+def test_irregular_problem_converges(oracle_mod):
+    O = oracle_mod
+    sizes, mats, interp, rhs = irregular()
+    a = oracle_of(O, sizes, mats, interp, rhs)
+    r = a.solve(O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.JACOBI, damp=0.6, pre=2, post=2, compat=False,
+                            rtol=1e-10, maxsteps=200))
+    assert r.status == 0, r.steps
+    import scipy.sparse as sp
+    s_, i_, v_ = mats[len(sizes) - 1]
+    A = sp.csr_matrix((v_, i_, s_), shape=(sizes[-1], sizes[-1]))
+    assert np.linalg.norm(A @ r.x - rhs) <= 1e-9 * np.linalg.norm(rhs)
