@@ -80,6 +80,15 @@
      (values (* :double)) (n :long))
   :returning :int)
 
+(fl.port:def-function ("fmg_grid_create_algebraic" fmg-grid-create-algebraic)
+    ((ctx (* :char)) (nlevels :int) (sizes (* :long)) (grid (* (* :char))))
+  :returning :int)
+
+(fl.port:def-function ("fmg_set_interpolation" fmg-set-interpolation)
+    ((grid (* :char)) (fine-level :int) (layout :int) (starts (* :int)) (indices (* :int))
+     (values (* :double)) (nfine :long) (ncoarse :long))
+  :returning :int)
+
 (fl.port:def-function ("fmg_set_rhs" fmg-set-rhs)
     ((grid (* :char)) (values (* :double)) (n :long))
   :returning :int)
@@ -183,3 +192,37 @@ the compressed-column form of sparse-matrix->ccs."
     (check (fl.port:foreign-call #'fmg-set-matrix grid level +fmg-ccs+ starts indices
                                  (fl.matlisp:store ccs) n)
            "fmg_set_matrix")))
+
+;;;; hierarchies on unstructured or adaptively refined meshes
+
+(defun upload-algebraic-hierarchy (matrices interpolations rhs)
+  "MATRICES: the level matrices of a multilevel decomposition, coarsest
+first (<sparse-matrix>, constraints eliminated, multilevel-decomposition
+geomg.lisp:109-142); INTERPOLATIONS: the constrained interpolation into each
+level above the coarsest (constrained-interpolation-matrix,
+constraints.lisp:58-72), coarsest first; RHS: the top-level right-hand side
+as a double vector in the top level's key order.  Returns the grid handle."
+  (let* ((keys (mapcar (lambda (m) (coerce (fl.matlisp:row-keys m) 'vector)) matrices))
+         (sizes (map '(vector (signed-byte 64)) #'length keys))
+         (grid (make-array 1 :element-type '(unsigned-byte 64))))
+    (check (fl.port:foreign-call #'fmg-grid-create-algebraic (gpu-context) (length sizes) sizes grid)
+           "fmg_grid_create_algebraic")
+    (loop for m in matrices for k in keys for level from 0 do
+      (let* ((ccs (fl.matlisp:sparse-matrix->ccs m :keys k))
+             (pattern (fl.matlisp:pattern ccs)))
+        (check (fl.port:foreign-call #'fmg-set-matrix (aref grid 0) level +fmg-ccs+
+                                     (slot-value pattern 'fl.matlisp::starts)
+                                     (slot-value pattern 'fl.matlisp::indices)
+                                     (fl.matlisp:store ccs) (length k))
+               "fmg_set_matrix")))
+    (loop for i in interpolations for level from 1 do
+      (let* ((ccs (fl.matlisp:sparse-matrix->ccs i :row-keys (nth level keys) :col-keys (nth (1- level) keys)))
+             (pattern (fl.matlisp:pattern ccs)))
+        (check (fl.port:foreign-call #'fmg-set-interpolation (aref grid 0) level +fmg-ccs+
+                                     (slot-value pattern 'fl.matlisp::starts)
+                                     (slot-value pattern 'fl.matlisp::indices)
+                                     (fl.matlisp:store ccs) (length (nth level keys))
+                                     (length (nth (1- level) keys)))
+               "fmg_set_interpolation")))
+    (check (fl.port:foreign-call #'fmg-set-rhs (aref grid 0) rhs (length rhs)) "fmg_set_rhs")
+    (aref grid 0)))
