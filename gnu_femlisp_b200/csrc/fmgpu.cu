@@ -1391,6 +1391,7 @@ int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
 
 int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
   if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
+  if (g && g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "SOR: scalar grids");
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
   if (level == g->top) FMG_RC(ensure_top(g));
