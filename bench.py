@@ -184,7 +184,45 @@ def cpu_baseline(wl, steps_gpu: int, budget_s: float = 25.0) -> dict:
             "sample": (f"oracle C++ restatement, {O.num_threads()} OpenMP threads: assembly of levels "
                        f"{wl.base_level}..{wl.level} ({t_asm:.1f} s) + {r.steps} CG steps "
                        f"({t_sample:.1f} s), per-step time x {steps_gpu} steps of the full solve"),
-            "assembly_s": t_asm, "cg_step_s": per_step, "time_to_solution_est_s": t_solve}
+            "assembly_s": t_asm, "cg_step_s": per_step, "time_to_solution_est_s": t_solve,
+            "host": host_info(), "one_thread": one_thread_step(wl, per_step)}
+
+
+def host_info() -> dict:
+    """nproc and the CPU model of the host the baseline ran on."""
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model, "omp_threads": os.environ.get("OMP_NUM_THREADS")}
+
+
+def one_thread_step(wl, per_step_all: float) -> dict:
+    """One CG step of the same algorithm on one thread, timed one level below
+    the workload (8x fewer unknowns) and scaled by the unknowns, beside the
+    all-thread step time."""
+    from gnu_femlisp_b200 import problems
+    from oracle import oracle as O
+    nthreads = O.num_threads()
+    small = problems.c3(seed=0, level=wl.level - 1)
+    o = O.Oracle(3, 1, small.level, base_level=small.base_level)
+    o.set_coefficient(O.K_CELL, small.kcell)
+    o.assemble()
+    cfg = O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=1e-10, maxsteps=1)
+    O.set_num_threads(1)
+    try:
+        t0 = time.perf_counter()
+        r = o.solve(cfg)
+        t1 = (time.perf_counter() - t0) / max(r.steps, 1) * (wl.nodes / small.nodes)
+    finally:
+        O.set_num_threads(nthreads)
+    return {"cg_step_s": t1, "speedup_all_threads": t1 / per_step_all,
+            "sample": f"1 thread, {r.steps} CG steps at {small.nodes} unknowns, scaled by {wl.nodes / small.nodes:.2f}"}
 
 
 def run_reference(args, world, rank):
@@ -227,6 +265,7 @@ def run_reference(args, world, rank):
         "config": {"workload": wl.name, "nodes": n, "solver": "CG + V(1,1) Jacobi(0.6), base level 2",
                    "inputs": "larger than L2"},
         "cpu_baseline": {"value": val, "unit": "MDoF/s to 1e-10", "cores": O.num_threads(), "kind": "port",
+                         "host": host_info(),
                          "sample": (f"{sample_steps} CG steps per timed step ({per_step:.2f} s/step) x "
                                     f"{full_steps} steps + assembly {t_asm:.1f} s")},
         "e2e": {"value": val, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",

@@ -1485,4 +1485,14 @@ int ora_num_threads(void) {
 #endif
 }
 
+// the OpenMP thread count of the following calls (the 1-thread timing of the
+// CPU baseline); the results do not depend on it (fixed loop orders)
+void ora_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
 }  // extern "C"

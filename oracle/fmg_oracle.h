@@ -115,6 +115,7 @@ int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hi
               int* nsteps);
 
 int ora_num_threads(void);
+void ora_set_num_threads(int n);
 
 #ifdef __cplusplus
 }

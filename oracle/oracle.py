@@ -350,3 +350,9 @@ def dot_par(x, y) -> float:
 
 def num_threads() -> int:
     return lib().ora_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    L = lib()
+    L.ora_set_num_threads.argtypes = [ctypes.c_int]
+    L.ora_set_num_threads(int(n))
