@@ -990,11 +990,19 @@ k_prolong(int MF, int MC, int dmask, const double* __restrict__ xc, double* __re
 }
 
 // -------------------------------------------------------------- coarse LU
-// Blocked form of k_lu_factor for matrices beyond shared memory: panels of
-// kLuB columns, rows interchanged through a logical permutation (physical rows
-// stay put), every element updated by the same fma's in the same ascending
-// order of elimination steps as in the unblocked loop, so factors and pivots
-// are bitwise those of k_lu_factor.
+// The dense LU with partial pivoting of the base level and its explicit
+// inverse (the <lu> coarse-grid iteration; the oracle's dense LU).  Every
+// form below performs, for every element, the operations of the unblocked
+// right-looking loop in the same order -- pivot: the first row holding the
+// largest magnitude among the rows not yet eliminated; multiplier: column
+// entry / pivot; update: a_ij = fma(-l_ik, a_kj, a_ij) for k ascending;
+// inverse: the interchanges, then per column the unit-lower forward and the
+// upper backward substitution (x_k = b_k / u_kk, then b_i = fma(-u_ik, x_k,
+// b_i) for the rows above) -- so factors, pivots and inverse are the same bit
+// for bit whichever form runs.
+//
+// Blocked form for matrices beyond shared memory: panels of kLuB columns,
+// rows interchanged through a logical permutation (physical rows stay put).
 constexpr int kLuB = 32;
 
 // the panel k0..k1-1: per column the pivot (the first logical row holding the
@@ -1093,9 +1101,8 @@ __global__ void k_iota(int* p, int n) {
   if (i < n) p[i] = i;
 }
 
-// k_lu_inverse with one CTA per column of X reading the factors transposed
-// (LT[k][i] = LU[i][k], coalesced over the rows): every element sees the same
-// operations in the same order
+// The inverse with one CTA per column of X reading the factors transposed
+// (LT[k][i] = LU[i][k], coalesced over the rows)
 __global__ void __launch_bounds__(256) k_lu_inverse_colT(const double* __restrict__ LT, const int* __restrict__ piv,
                                                          int n, double* X) {
   extern __shared__ double S[];
@@ -1126,116 +1133,14 @@ __global__ void __launch_bounds__(256) k_lu_inverse_colT(const double* __restric
   for (int i = tid; i < n; i += nt) X[(long long)i * n + j] = out[i];
 }
 
-// Single-block dense LU with partial pivoting, row-major, in place.
-__global__ void __launch_bounds__(1024) k_lu_factor(double* A, int n, int* piv) {
-  __shared__ double bv[32];
-  __shared__ int bi[32];
-  __shared__ int pk_s;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int k = 0; k < n; ++k) {
-    double best = -1.0;
-    int besti = n;
-    for (int i = k + tid; i < n; i += nt) {
-      const double v = fabs(A[(long long)i * n + k]);
-      if (v > best || (v == best && i < besti)) { best = v; besti = i; }
-    }
-    for (int o = 16; o >= 1; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
-      if (ov > best || (ov == best && oi < besti)) { best = ov; besti = oi; }
-    }
-    if ((tid & 31) == 0) { bv[tid >> 5] = best; bi[tid >> 5] = besti; }
-    __syncthreads();
-    if (tid == 0) {
-      double b = bv[0];
-      int ib = bi[0];
-      for (int w = 1; w < (nt + 31) / 32; ++w)
-        if (bv[w] > b || (bv[w] == b && bi[w] < ib)) { b = bv[w]; ib = bi[w]; }
-      pk_s = ib;
-      piv[k] = ib;
-    }
-    __syncthreads();
-    const int pk = pk_s;
-    if (pk != k)
-      for (int j = tid; j < n; j += nt) {
-        const double t = A[(long long)k * n + j];
-        A[(long long)k * n + j] = A[(long long)pk * n + j];
-        A[(long long)pk * n + j] = t;
-      }
-    __syncthreads();
-    const double d = A[(long long)k * n + k];
-    for (int i = k + 1 + tid; i < n; i += nt) A[(long long)i * n + k] = A[(long long)i * n + k] / d;
-    __syncthreads();
-    const int m = n - k - 1;
-    for (long long idx = tid; idx < (long long)m * m; idx += nt) {
-      const int i = k + 1 + (int)(idx / m), j = k + 1 + (int)(idx % m);
-      A[(long long)i * n + j] = fma(-A[(long long)i * n + k], A[(long long)k * n + j], A[(long long)i * n + j]);
-    }
-    __syncthreads();
-  }
-}
 
-// k_lu_factor on a shared-memory copy of A (n x n doubles fit in one CTA's
-// shared memory): the same operations in the same order, so the factors and
-// pivots are bitwise equal, at shared-memory instead of global latency.
-__global__ void __launch_bounds__(1024) k_lu_factor_smem(double* A, int n, int* piv) {
-  extern __shared__ double S[];
-  __shared__ double bv[32];
-  __shared__ int bi[32];
-  __shared__ int pk_s;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int idx = tid; idx < n * n; idx += nt) S[idx] = A[idx];
-  __syncthreads();
-  for (int k = 0; k < n; ++k) {
-    double best = -1.0;
-    int besti = n;
-    for (int i = k + tid; i < n; i += nt) {
-      const double v = fabs(S[i * n + k]);
-      if (v > best || (v == best && i < besti)) { best = v; besti = i; }
-    }
-    for (int o = 16; o >= 1; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
-      if (ov > best || (ov == best && oi < besti)) { best = ov; besti = oi; }
-    }
-    if ((tid & 31) == 0) { bv[tid >> 5] = best; bi[tid >> 5] = besti; }
-    __syncthreads();
-    if (tid == 0) {
-      double b = bv[0];
-      int ib = bi[0];
-      for (int w = 1; w < (nt + 31) / 32; ++w)
-        if (bv[w] > b || (bv[w] == b && bi[w] < ib)) { b = bv[w]; ib = bi[w]; }
-      pk_s = ib;
-      piv[k] = ib;
-    }
-    __syncthreads();
-    const int pk = pk_s;
-    if (pk != k)
-      for (int j = tid; j < n; j += nt) {
-        const double t = S[k * n + j];
-        S[k * n + j] = S[pk * n + j];
-        S[pk * n + j] = t;
-      }
-    __syncthreads();
-    const double d = S[k * n + k];
-    for (int i = k + 1 + tid; i < n; i += nt) S[i * n + k] = S[i * n + k] / d;
-    __syncthreads();
-    const int m = n - k - 1;
-    for (int idx = tid; idx < m * m; idx += nt) {
-      const int i = k + 1 + idx / m, j = k + 1 + idx % m;
-      S[i * n + j] = fma(-S[i * n + k], S[k * n + j], S[i * n + j]);
-    }
-    __syncthreads();
-  }
-  for (int idx = tid; idx < n * n; idx += nt) A[idx] = S[idx];
-}
 
-// k_lu_factor_smem with two block barriers per column instead of five: warp 0
-// finds the pivot (the first logical row holding the largest magnitude) and
+// The factorisation on a shared-memory copy of A (n x n doubles fit in one
+// CTA), two block barriers per column: warp 0 finds the pivot and
 // interchanges logical rows through a permutation; every thread then updates
 // the trailing submatrix, forming the multiplier it needs as the quotient the
-// column will hold, and scales the previous column (which no later step
-// reads before that).  Factors and pivots are bitwise those of k_lu_factor.
+// column will hold, and scales the previous column (which no later step reads
+// before that).
 __global__ void __launch_bounds__(1024) k_lu_factor_smem2(double* A, int n, int* piv) {
   extern __shared__ double S[];
   int* perm = reinterpret_cast<int*>(S + (size_t)n * n);
@@ -1287,9 +1192,8 @@ __global__ void __launch_bounds__(1024) k_lu_factor_smem2(double* A, int n, int*
   for (int idx = tid; idx < n * n; idx += nt) A[idx] = S[perm[idx / n] * n + idx % n];
 }
 
-// k_lu_inverse with one CTA per column of X: the threads share the rows, a
-// block barrier per elimination column; every element sees the same
-// operations in the same order as in k_lu_inverse.
+// The inverse with the factors in shared memory and one CTA per column of X:
+// the threads share the rows, a block barrier per elimination column.
 __global__ void __launch_bounds__(256) k_lu_inverse_col(const double* __restrict__ LU, const int* __restrict__ piv,
                                                         int n, double* X) {
   extern __shared__ double S[];
@@ -1320,62 +1224,7 @@ __global__ void __launch_bounds__(256) k_lu_inverse_col(const double* __restrict
   for (int i = tid; i < n; i += nt) X[(long long)i * n + j] = out[i];
 }
 
-// k_lu_inverse with the factors and a block of 32 columns of X in shared
-// memory: thread = column, the same operations in the same order.
-__global__ void __launch_bounds__(32) k_lu_inverse_smem(const double* __restrict__ LU, const int* __restrict__ piv,
-                                                        int n, double* X) {
-  extern __shared__ double S[];
-  double* L = S;           // n x n
-  double* Xs = S + n * n;  // n x 32
-  const int lane = threadIdx.x, j = blockIdx.x * 32 + lane;
-  for (int idx = lane; idx < n * n; idx += 32) L[idx] = LU[idx];
-  __syncwarp();
-  if (j < n) {
-    for (int i = 0; i < n; ++i) Xs[i * 32 + lane] = (i == j) ? 1.0 : 0.0;
-    for (int k = 0; k < n; ++k) {
-      const int p = piv[k];
-      if (p != k) {
-        const double t = Xs[k * 32 + lane];
-        Xs[k * 32 + lane] = Xs[p * 32 + lane];
-        Xs[p * 32 + lane] = t;
-      }
-    }
-    for (int k = 0; k < n; ++k) {
-      const double bk = Xs[k * 32 + lane];
-      for (int i = k + 1; i < n; ++i) Xs[i * 32 + lane] = fma(-L[i * n + k], bk, Xs[i * 32 + lane]);
-    }
-    for (int k = n - 1; k >= 0; --k) {
-      const double bk = Xs[k * 32 + lane] / L[k * n + k];
-      Xs[k * 32 + lane] = bk;
-      for (int i = 0; i < k; ++i) Xs[i * 32 + lane] = fma(-L[i * n + k], bk, Xs[i * 32 + lane]);
-    }
-    for (int i = 0; i < n; ++i) X[(long long)i * n + j] = Xs[i * 32 + lane];
-  }
-}
 
-// Column j of A^-1 per thread, from the LU factors; X row-major (j fastest).
-__global__ void k_lu_inverse(const double* __restrict__ LU, const int* __restrict__ piv, int n, double* X) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  for (int i = 0; i < n; ++i) X[(long long)i * n + j] = (i == j) ? 1.0 : 0.0;
-  for (int k = 0; k < n; ++k) {
-    const int p = piv[k];
-    if (p != k) {
-      const double t = X[(long long)k * n + j];
-      X[(long long)k * n + j] = X[(long long)p * n + j];
-      X[(long long)p * n + j] = t;
-    }
-  }
-  for (int k = 0; k < n; ++k) {
-    const double bk = X[(long long)k * n + j];
-    for (int i = k + 1; i < n; ++i) X[(long long)i * n + j] = fma(-LU[(long long)i * n + k], bk, X[(long long)i * n + j]);
-  }
-  for (int k = n - 1; k >= 0; --k) {
-    const double bk = X[(long long)k * n + j] / LU[(long long)k * n + k];
-    X[(long long)k * n + j] = bk;
-    for (int i = 0; i < k; ++i) X[(long long)i * n + j] = fma(-LU[(long long)i * n + k], bk, X[(long long)i * n + j]);
-  }
-}
 
 __global__ void k_transpose(const double* __restrict__ X, int n, double* __restrict__ XT) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
