@@ -128,3 +128,22 @@ def test_refusals_and_incomplete_hierarchy(G, ctx):
         assert e.value.code == -6
     hist, steps, st = g.solve(_cfg(G, "cg", False), x)
     assert st == 0
+
+
+@pytest.mark.parametrize("gamma,fmg,comb", [(2, False, 0), (1, True, 0), (1, False, 1)])
+def test_algebraic_cycles(oracle_mod, G, ctx, gamma, fmg, comb):
+    O = oracle_mod
+    C = G._capi
+    o = O.Oracle(3, 1, 3, base_level=1)
+    o.set_coefficient(O.K_CELL, np.exp(np.random.default_rng(12).standard_normal(8 ** 3)))
+    o.assemble()
+    g = gpu_of(G, ctx, *from_structured(o, 3, 1))
+    post = 1 if comb == 0 else 0
+    r = o.solve(O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.JACOBI, damp=0.6, pre=1, post=post, gamma=gamma,
+                            fmg=fmg, combination=comb, compat=False, rtol=1e-10, maxsteps=60))
+    cfg = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, 0.6, 1, post, gamma, 0, 1.0, 1e-10, 0.0, 60, comb,
+                     1 if fmg else 0)
+    x = g.vector()
+    hist, steps, st = g.solve(cfg, x)
+    assert st == r.status == 0
+    assert np.array_equal(hist, r.history) and np.array_equal(x.get(), r.x)

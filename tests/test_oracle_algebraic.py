@@ -35,3 +35,19 @@ def test_irregular_problem_converges(oracle_mod):
     s_, i_, v_ = mats[len(sizes) - 1]
     A = sp.csr_matrix((v_, i_, s_), shape=(sizes[-1], sizes[-1]))
     assert np.linalg.norm(A @ r.x - rhs) <= 1e-9 * np.linalg.norm(rhs)
+
+
+@pytest.mark.parametrize("gamma,fmg,comb", [(2, False, 0), (1, True, 0), (1, False, 1)])
+def test_structured_as_algebraic_cycles(oracle_mod, gamma, fmg, comb):
+    # W-cycle, F-cycle and the additive combination through the same
+    # algebraic levels
+    O = oracle_mod
+    o = O.Oracle(2, 1, 5, base_level=1)
+    o.set_coefficient(O.K_CELL, np.exp(np.random.default_rng(11).standard_normal(32 * 32)))
+    o.assemble()
+    a = oracle_of(O, *from_structured(o, 2, 1))
+    cfg = O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.JACOBI, damp=0.6, pre=1, post=1 if comb == 0 else 0,
+                      gamma=gamma, fmg=fmg, combination=comb, compat=False, rtol=1e-10, maxsteps=60)
+    rs, ra = o.solve(cfg), a.solve(cfg)
+    assert rs.status == 0
+    assert np.array_equal(rs.history, ra.history) and np.array_equal(rs.x, ra.x)
