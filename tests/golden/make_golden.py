@@ -34,6 +34,12 @@ CASES = {
     # 2D Q2 with multicolour SOR(1.2) V(2,2) as the iteration (config C2's smoother)
     "q2_2d_sor_mg": (2, 2, 3, 1, 3, dict(method=O.METHOD_MG, smoother=O.SOR, damp=1.2, pre=2, post=2,
                                          rtol=1e-10, maxsteps=60)),
+    # the vertex-centred SSC of higher-order discretisations as the iteration, V(1,0)
+    "q2_2d_ssc_mg": (2, 2, 3, 1, 5, dict(method=O.METHOD_MG, smoother=O.SSC, damp=1.0, pre=1, post=0,
+                                         rtol=1e-10, maxsteps=60)),
+    # 3D Q2, CG + V(1,1) PSC(0.2) (additive vertex blocks)
+    "q2_3d_psc_cg": (3, 2, 2, 0, 9, dict(method=O.METHOD_CG_MG, smoother=O.PSC, damp=0.2, compat=False,
+                                         rtol=1e-10, maxsteps=100)),
 }
 
 
