@@ -93,6 +93,51 @@
     ((grid (* :char)) (values (* :double)) (n :long))
   :returning :int)
 
+(fl.port:def-function ("fmg_grid_destroy" fmg-grid-destroy)
+    ((grid (* :char)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_last_error" fmg-last-error)
+    ((ctx (* :char)) (buf (* :char)) (len :int))
+  :returning :int)
+
+(fl.port:def-function ("fmg_vec_set" fmg-vec-set)
+    ((vec (* :char)) (host (* :double)) (n :long))
+  :returning :int)
+
+(fl.port:def-function ("fmg_vec_destroy" fmg-vec-destroy)
+    ((vec (* :char)))
+  :returning :int)
+
+;;; one application of the <geometric-cs> iterator (b and r may be the same
+;;; vector: the alias inside <cg>)
+(fl.port:def-function ("fmg_vcycle" fmg-vcycle)
+    ((grid (* :char)) (cfg (* :char)) (x (* :char)) (b (* :char)) (r (* :char)))
+  :returning :int)
+
+;;; the mixed-precision solve and the learned damping
+(fl.port:def-function ("fmg_solve_mixed" fmg-solve-mixed)
+    ((grid (* :char)) (cfg (* :char)) (mcfg (* :char)) (x (* :char)) (hist (* :double))
+     (hist-len :int) (nouter (* :int)) (ninner (* :int)) (status (* :int)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_net_load" fmg-net-load)
+    ((ctx (* :char)) (path :c-string) (out (* (* :char))))
+  :returning :int)
+
+(fl.port:def-function ("fmg_net_destroy" fmg-net-destroy)
+    ((net (* :char)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_net_apply" fmg-net-apply)
+    ((net (* :char)) (grid (* :char)))
+  :returning :int)
+
+(fl.port:def-function ("fmg_learned_judge_mixed" fmg-learned-judge-mixed)
+    ((grid (* :char)) (cfg (* :char)) (mcfg (* :char)) (rho-plain (* :double))
+     (rho-learned (* :double)) (accepted (* :int)))
+  :returning :int)
+
 (defun check (status what)
   (unless (= status +fmg-ok+)
     (error "libfmgpu: ~A failed with status ~D" what status)))
@@ -226,3 +271,44 @@ as a double vector in the top level's key order.  Returns the grid handle."
                "fmg_set_interpolation")))
     (check (fl.port:foreign-call #'fmg-set-rhs (aref grid 0) rhs (length rhs)) "fmg_set_rhs")
     (aref grid 0)))
+
+;;;; the mixed-precision solve with the learned damping
+
+(defun %mixed-cfg-bytes (inner-rtol max-inner max-outer matrix-free)
+  "fmg_mixed_cfg laid out as the C struct (24 bytes)."
+  (let ((v (make-array 24 :element-type '(unsigned-byte 8) :initial-element 0)))
+    (setf (fl.port:sap-ref-double v 0) inner-rtol
+          (fl.port:sap-ref-32 v 8) max-inner
+          (fl.port:sap-ref-32 v 12) max-outer
+          (fl.port:sap-ref-32 v 16) (if matrix-free 1 0))
+    v))
+
+(defun gpu-solve-mixed (grid level weights-path &key (damp 0.6d0) (reduction 1d-10) (maxsteps 200))
+  "On an assembled GRID whose top level is LEVEL: installs the per-node damping the network in
+WEIGHTS-PATH predicts, lets the plain cycle judge it (it stays only if no
+worse), and solves with FP64 flexible CG around the FP32/BF16 V(1,1) Jacobi
+cycle.  Returns the solution vector handle and the :defnorm history."
+  (let* ((ctx (gpu-context))
+         (net (make-array 1 :element-type '(unsigned-byte 64)))
+         (x (make-array 1 :element-type '(unsigned-byte 64)))
+         (cfg (%cfg-bytes +fmg-method-cg-mg+ +fmg-jacobi+ damp 1 1 reduction maxsteps))
+         (mcfg (%mixed-cfg-bytes 1d-5 200 20 t))
+         (rho-plain (make-array 1 :element-type 'double-float))
+         (rho-learned (make-array 1 :element-type 'double-float))
+         (accepted (make-array 1 :element-type '(signed-byte 32)))
+         (hist (make-array (+ maxsteps 24) :element-type 'double-float))
+         (nouter (make-array 1 :element-type '(signed-byte 32)))
+         (ninner (make-array 1 :element-type '(signed-byte 32)))
+         (status (make-array 1 :element-type '(signed-byte 32))))
+    (check (fl.port:foreign-call #'fmg-net-load ctx weights-path net) "fmg_net_load")
+    (unwind-protect
+         (progn
+           (check (fl.port:foreign-call #'fmg-net-apply (aref net 0) grid) "fmg_net_apply")
+           (check (fl.port:foreign-call #'fmg-learned-judge-mixed grid cfg mcfg rho-plain rho-learned accepted)
+                  "fmg_learned_judge_mixed"))
+      (fl.port:foreign-call #'fmg-net-destroy (aref net 0)))
+    (check (fl.port:foreign-call #'fmg-vec-create grid level x) "fmg_vec_create")
+    (check (fl.port:foreign-call #'fmg-solve-mixed grid cfg mcfg (aref x 0) hist (length hist)
+                                 nouter ninner status)
+           "fmg_solve_mixed")
+    (values (aref x 0) (subseq hist 0 (+ (aref nouter 0) (aref ninner 0) 1)))))
