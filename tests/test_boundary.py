@@ -35,25 +35,42 @@ def test_init_fails_loudly_without_gpu():
         Context(0)
 
 
-def test_solve_cfg_layout_matches_header(tmp_path):
-    """The ctypes mirror of fmg_solve_cfg has the C compiler's layout."""
+@pytest.mark.parametrize("cname,pyname", [("fmg_solve_cfg", "SolveCfg"), ("fmg_mixed_cfg", "MixedCfg")])
+def test_cfg_layout_matches_header(tmp_path, cname, pyname):
+    """The ctypes mirrors of the configuration structs have the C compiler's layout."""
     import shutil
     import subprocess
     from gnu_femlisp_b200 import _capi
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
+    cls = getattr(_capi, pyname)
     src = tmp_path / "layout.c"
-    fields = [f for f, _ in _capi.SolveCfg._fields_]
+    fields = [f for f, _ in cls._fields_]
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fmgpu.h"\nint main(void){'
-                   'printf("%zu", sizeof(fmg_solve_cfg));'
-                   + "".join(f'printf(" %zu", offsetof(fmg_solve_cfg, {f}));' for f in fields)
+                   f'printf("%zu", sizeof({cname}));'
+                   + "".join(f'printf(" %zu", offsetof({cname}, {f}));' for f in fields)
                    + "return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
-    assert out[0] == ctypes.sizeof(_capi.SolveCfg)
-    assert out[1:] == [getattr(_capi.SolveCfg, f).offset for f in fields]
+    assert out[0] == ctypes.sizeof(cls)
+    assert out[1:] == [getattr(cls, f).offset for f in fields]
+
+
+def test_ctypes_signatures_match_header():
+    """Every declared function has a ctypes signature with the header's
+    number of arguments."""
+    from gnu_femlisp_b200 import _capi
+    h = open(os.path.join(ROOT, "include", "fmgpu.h")).read()
+    h = re.sub(r"/\*.*?\*/", "", h, flags=re.S)
+    arity = {}
+    for m in re.finditer(r"\b(?:int|long|void)\s+(fmg_\w+)\s*\(([^)]*)\)\s*;", h):
+        args = [a for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
+        arity[m.group(1)] = len(args)
+    assert set(arity) == set(_capi.SIGNATURES), set(arity) ^ set(_capi.SIGNATURES)
+    bad = {n: (len(_capi.SIGNATURES[n][1]), k) for n, k in arity.items() if len(_capi.SIGNATURES[n][1]) != k}
+    assert not bad, bad
 
 
 def test_femlisp_forms():
