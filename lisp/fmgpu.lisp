@@ -153,7 +153,8 @@
    (reduction :initarg :reduction :initform 1d-10)
    (maxsteps :initarg :maxsteps :initform 200))
   (:documentation "<cg> preconditioned by <geometric-cs>, run by libfmgpu on
-the GPU.  The problem must be a cdr problem on a uniformly refined unit
+the GPU; SMOOTHER is :jacobi, :sor, :ssc or :psc (the vertex-centred
+geometric-ssc / geometric-psc, the default of higher-order discretisations).  The problem must be a cdr problem on a uniformly refined unit
 n-cube with Lagrange Q1/Q2; the coefficients are sampled on the host."))
 
 (defvar *gpu-context* nil)
@@ -200,7 +201,10 @@ x fastest) and the :defnorm history."
       (check (fl.port:foreign-call #'fmg-vec-create (aref grid 0) level x) "fmg_vec_create")
       (check (fl.port:foreign-call
               #'fmg-solve (aref grid 0)
-              (%cfg-bytes +fmg-method-cg-mg+ (if (eq smoother :sor) +fmg-sor+ +fmg-jacobi+)
+              (%cfg-bytes +fmg-method-cg-mg+
+                          (ecase smoother
+                            (:jacobi +fmg-jacobi+) (:sor +fmg-sor+)
+                            (:ssc +fmg-ssc+) (:psc +fmg-psc+))   ; geometric-ssc / -psc
                           damp pre-steps post-steps reduction maxsteps)
               (aref x 0) hist (length hist) nsteps status)
              "fmg_solve")
