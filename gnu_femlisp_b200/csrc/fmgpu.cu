@@ -978,7 +978,9 @@ int fmg_assemble_levels(fmg_grid* g, int mode) {
     // the top level's matrix of the unrolled Q1 path waits for its first
     // use (the mixed solve applies that level from the cell coefficients and
     // never reads it); its rhs is formed now
-    const bool defer = l == g->top && mode == FMG_ASSEMBLE_REDISCRETIZE && assemble_splits(g->dim, g->order, g->nc, a);
+    // (not where the top level is the base: the coarse LU reads it right away)
+    const bool defer = l == g->top && l > g->base && mode == FMG_ASSEMBLE_REDISCRETIZE &&
+                       assemble_splits(g->dim, g->order, g->nc, a);
     if (defer) a.A = nullptr;
     launch_assemble(g->dim, g->order, a, L.Kbar_h.data(), L.Ctab_h.data(), st);
     if ((rc = launched(c, "assemble"))) return rc;
