@@ -181,7 +181,10 @@ int fmg_assemble_levels(fmg_grid* grid, int mode);
    hierarchy is complete, and solvable, once every level base..top has a
    matrix (uploaded, or from an earlier assembly); the base level's LU is then
    formed.  A grid with an uploaded matrix applies its mixed form through the
-   stored FP32 matrix, not matrix-free from the coefficients. */
+   stored FP32 matrix, not matrix-free from the coefficients.  On an
+   algebraic grid (fmg_grid_create_algebraic) any pattern is accepted: the
+   matrix is kept as compressed rows (columns ascending, duplicates summed,
+   explicit zeros dropped) with its diagonal for the Jacobi smoother. */
 #define FMG_CSR 0
 #define FMG_CCS 1
 int fmg_set_matrix(fmg_grid* grid, int level, int layout, const int* start, const int* index,
