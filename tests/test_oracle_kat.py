@@ -252,3 +252,26 @@ def test_psc_preconditioned_cg_converges(oracle_mod):
     r = o.solve(O.solve_cfg(method=O.METHOD_CG_MG, smoother=O.PSC, damp=0.4, pre=1, post=1, compat=False,
                             rtol=1e-10, maxsteps=60))
     assert r.status == 0 and r.steps < 20, r.steps
+
+
+def _centre_value(O, dim, order, level):
+    o = O.Oracle(dim, order, level, base_level=min(1, level - 1)).assemble()
+    r = o.solve(O.solve_cfg(damp=0.6, compat=False, rtol=1e-12, maxsteps=200))
+    assert r.status == 0
+    M = order * (1 << level) + 1
+    return r.x[sum((M - 1) // 2 * M ** d for d in range(dim))]
+
+
+def test_h_convergence_to_the_continuum_values(oracle_mod):
+    # model-problem.lisp:184-199 (check-h-convergence): -Delta u = 1, u = 0 on
+    # the boundary, u(1/2,1/2) = 0.0736713532..., u(1/2,1/2,1/2) = 0.0562128...
+    O = oracle_mod
+    u2, u3 = 0.0736713532, 0.0562128
+    e = [abs(_centre_value(O, 2, 1, l) - u2) for l in (3, 4, 5, 6)]
+    assert all(3.8 < a / b < 4.2 for a, b in zip(e, e[1:])), e        # Q1: second order
+    assert e[-1] < 2e-5
+    e = [abs(_centre_value(O, 2, 2, l) - u2) for l in (3, 4)]
+    assert e[0] / e[1] > 12 and e[1] < 2e-7, e                        # Q2: fourth order at the nodes
+    e = [abs(_centre_value(O, 3, 1, l) - u3) for l in (2, 3, 4)]
+    assert all(3.8 < a / b < 4.8 for a, b in zip(e, e[1:])), e
+    assert abs(_centre_value(O, 3, 2, 3) - u3) < 1e-5
