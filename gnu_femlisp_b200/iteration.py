@@ -140,6 +140,55 @@ class DiscreteSystem:
         return self._grids[base_level]
 
 
+def _csr_triple(m):
+    """(start, index, values) of a scipy sparse matrix or of such a triple."""
+    if hasattr(m, "tocsr"):
+        m = m.tocsr()
+        return m.indptr, m.indices, m.data
+    return tuple(m)
+
+
+class AlgebraicSystem:
+    """A multilevel decomposition formed elsewhere -- the level matrices,
+    coarsest first, the interpolation into each level above the coarsest, and
+    the top-level rhs -- as Femlisp forms it on an unstructured or adaptively
+    refined mesh (multilevel-decomposition, geomg.lisp:109-142).  Matrices are
+    scipy sparse matrices or (start, index, values) compressed rows.  The
+    blackboard solve runs it on an algebraic grid (fmg_grid_create_algebraic);
+    with no ansatz space to choose from, the default smoother is <jacobi>."""
+
+    fe = None
+
+    def __init__(self, matrices, interpolations, rhs, ctx: Context | None = None):
+        if len(interpolations) != len(matrices) - 1:
+            raise ValueError("one interpolation per level above the coarsest")
+        self.matrices = [_csr_triple(m) for m in matrices]
+        self.interpolations = [_csr_triple(p) for p in interpolations]
+        self.sizes = [len(s) - 1 for s, _, _ in self.matrices]
+        for l, (s, _, _) in enumerate(self.interpolations, start=1):
+            if len(s) - 1 != self.sizes[l]:
+                raise ValueError(f"interpolation into level {l} has {len(s) - 1} rows, the level {self.sizes[l]}")
+        self.rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        if self.rhs.size != self.sizes[-1]:
+            raise ValueError("rhs size differs from the top level's")
+        self.ctx = ctx
+        self._grids: dict[int, Grid] = {}
+
+    def grid(self, base_level: int = 0) -> Grid:
+        """The algebraic grid of levels base_level .. top (renumbered from 0)."""
+        if base_level not in self._grids:
+            if self.ctx is None:
+                self.ctx = Context()
+            g = Grid.algebraic(self.ctx, self.sizes[base_level:])
+            for l, (s, i, v) in enumerate(self.matrices[base_level:]):
+                g.set_matrix(l, s, i, v)
+            for l, (s, i, v) in enumerate(self.interpolations[base_level:], start=1):
+                g.set_interpolation(l, s, i, v, self.sizes[base_level + l - 1])
+            g.set_rhs(self.rhs)
+            self._grids[base_level] = g
+        return self._grids[base_level]
+
+
 def discretize_globally(problem: CdrProblem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
     """Returns (A, b) like Femlisp; here A is the DiscreteSystem and b its
     assembled right-hand side on the host."""
@@ -279,7 +328,7 @@ class SolveReport:
     extra: dict = field(default_factory=dict)
 
 
-def make_cfg(iteration, success_if: str, failure_if: str, order: int = 1) -> tuple[C.SolveCfg, int, bool]:
+def make_cfg(iteration, success_if: str, failure_if: str, order: int | None = 1) -> tuple[C.SolveCfg, int, bool]:
     cs = iteration.preconditioner if isinstance(iteration, CG) else iteration
     cfg = C.SolveCfg()
     if isinstance(iteration, CG):
@@ -289,8 +338,9 @@ def make_cfg(iteration, success_if: str, failure_if: str, order: int = 1) -> tup
         cfg.method = C.FMG_METHOD_MG
     base = 0
     if cs is not None:
-        # select-smoother (geomg.lisp:48-60): Gauss-Seidel for order 1, SSC above
-        sm = cs.smoother or (GaussSeidel() if order == 1 else GeometricSSC())
+        # select-smoother (geomg.lisp:48-60): Gauss-Seidel for order 1, SSC
+        # above; <jacobi> for an algebraic system (order None)
+        sm = cs.smoother or (Jacobi() if order is None else GaussSeidel() if order == 1 else GeometricSSC())
         if isinstance(sm, Jacobi):
             cfg.smoother, cfg.damp = C.FMG_JACOBI, sm.damp
         elif isinstance(sm, GeometricSSC):
@@ -320,9 +370,10 @@ def make_cfg(iteration, success_if: str, failure_if: str, order: int = 1) -> tup
 def solve(blackboard: dict) -> dict:
     """(solve (blackboard :matrix A :rhs b :solver solver)) -- returns the
     blackboard with :solution, :report and :history filled in."""
-    A: DiscreteSystem = blackboard["matrix"]
+    A: DiscreteSystem | AlgebraicSystem = blackboard["matrix"]
     solver: LinearSolver = blackboard["solver"]
-    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if, A.fe.order)
+    order = A.fe.order if A.fe is not None else None
+    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if, order)
     g = A.grid(base)
     x = g.vector()
     if "solution" in blackboard and blackboard["solution"] is not None:

@@ -98,3 +98,25 @@ def test_gauss_sampling_layout():
     xi = gauss_points_1d(1)
     # cell 1 = (cx=1, cy=0), point 2 = (qx=0, qy=1)
     assert v[1, 2] == pytest.approx((1 + xi[0]) * 0.5 + 10 * (0 + xi[1]) * 0.5)
+
+
+def test_algebraic_system_checks_and_default_smoother():
+    # no GPU needed: the shapes are checked on construction, the device grid
+    # is made only when a solve asks for it
+    import numpy as np
+    import scipy.sparse as sp
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200.iteration import make_cfg, CG, geometric_cs
+    A1 = sp.diags([2.0] * 4).tocsr()
+    A0 = sp.diags([2.0] * 2).tocsr()
+    P = sp.csr_matrix(np.array([[1.0, 0.0], [1.0, 0.0], [0.0, 1.0], [0.0, 1.0]]))
+    s = G.AlgebraicSystem([A0, A1], [P], np.ones(4))
+    assert s.sizes == [2, 4] and s.fe is None
+    with pytest.raises(ValueError):
+        G.AlgebraicSystem([A0, A1], [], np.ones(4))
+    with pytest.raises(ValueError):
+        G.AlgebraicSystem([A0, A1], [P.T.tocsr()], np.ones(4))
+    with pytest.raises(ValueError):
+        G.AlgebraicSystem([A0, A1], [P], np.ones(3))
+    cfg, _, _ = make_cfg(CG(preconditioner=geometric_cs()), "(< :reduction 1e-10)", "(> :step 50)", order=None)
+    assert cfg.smoother == G._capi.FMG_JACOBI
