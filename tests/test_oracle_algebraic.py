@@ -51,3 +51,25 @@ def test_structured_as_algebraic_cycles(oracle_mod, gamma, fmg, comb):
     rs, ra = o.solve(cfg), a.solve(cfg)
     assert rs.status == 0
     assert np.array_equal(rs.history, ra.history) and np.array_equal(rs.x, ra.x)
+
+
+def test_algebraic_level_operators_against_scipy(oracle_mod):
+    # the oracle's compressed-row operators against plain sparse arithmetic
+    import scipy.sparse as sp
+    O = oracle_mod
+    sizes, mats, interp, rhs = irregular(n=500, levels=3, seed=2)
+    a = oracle_of(O, sizes, mats, interp, rhs)
+    top = len(sizes) - 1
+    A = sp.csr_matrix((mats[top][2], mats[top][1], mats[top][0]), shape=(sizes[top], sizes[top]))
+    P = sp.csr_matrix((interp[top][2], interp[top][1], interp[top][0]), shape=(sizes[top], sizes[top - 1]))
+    rng = np.random.default_rng(4)
+    x, b = rng.standard_normal(sizes[top]), rng.standard_normal(sizes[top])
+    tol = 1e-13 * np.abs(A).sum(axis=1).max() * np.abs(x).max()
+    assert np.max(np.abs(a.matvec(x) - A @ x)) <= tol
+    assert np.max(np.abs(a.residual(x, b) - (b - A @ x))) <= tol
+    assert np.max(np.abs(a.restrict(b, top) - P.T @ b)) <= 1e-13 * np.abs(P).sum(axis=0).max() * np.abs(b).max()
+    xc = rng.standard_normal(sizes[top - 1])
+    assert np.max(np.abs(a.prolongate(xc, x, top - 1) - (x + P @ xc))) <= 1e-13 * (1 + np.abs(x).max())
+    xj, rj = a.jacobi(x, b, 0.7)
+    d = A.diagonal()
+    assert np.allclose(rj, b / d, rtol=0, atol=0) and np.max(np.abs(xj - (x + 0.7 * b / d))) <= 1e-15 * np.abs(xj).max()
