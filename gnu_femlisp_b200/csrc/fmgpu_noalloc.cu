@@ -16,6 +16,9 @@
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture begins;
+//   * every call makes the context's device current for its own duration and
+//     gives the calling thread back the device that was current before, so a
+//     host that works on several devices keeps its own current device;
 //   * every call shares the one array, so calls that overlap on the GPU (on
 //     different streams, or from different host threads) race and must not be
 //     issued; the completion counter is cleared at the start of every call.
@@ -38,6 +41,24 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_addr[kMaxDevices] = {nullptr};
 
+// Makes a device current and, on leaving the scope, restores the device that
+// was current before (only when it differs).
+struct DeviceScope {
+  int prev = -1;
+  bool switched = false;
+  cudaError_t enter(int dev) {
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return e;
+    if (prev == dev) return cudaSuccess;
+    e = cudaSetDevice(dev);
+    switched = e == cudaSuccess;
+    return e;
+  }
+  ~DeviceScope() {
+    if (switched) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 
 namespace fmg {  // context accessors, defined in fmgpu.cu
@@ -56,12 +77,14 @@ extern "C" int fmg_dot_noalloc(fmg_ctx* ctx, const double* x, const double* y, l
   const int dev = ctx_device(ctx);
   cudaStream_t st = ctx_stream(ctx);
   if (dev < 0 || dev >= kMaxDevices) return ctx_error(ctx, FMG_ERR_ARG, "fmg_dot_noalloc: device id");
+  // the context's device is current for the call; the caller's is restored
+  DeviceScope scope;
+  if (cudaError_t e = scope.enter(dev); e != cudaSuccess) return ctx_error(ctx, FMG_ERR_CUDA, cudaGetErrorString(e));
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_addr[dev]) {  // set-up, once per device, with that device current
-      cudaError_t e = cudaSetDevice(dev);
-      if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&g_noalloc_addr[dev], g_noalloc_scratch);
+      cudaError_t e = cudaGetSymbolAddress((void**)&g_noalloc_addr[dev], g_noalloc_scratch);
       if (e != cudaSuccess) {
         g_noalloc_addr[dev] = nullptr;
         return ctx_error(ctx, FMG_ERR_CUDA, cudaGetErrorString(e));
