@@ -35,6 +35,12 @@ sys.path.insert(0, ROOT)
 METRIC = "time to 1e-10 rel. residual + MDoF/s per V-cycle: mixed/learned vs FP64 GMG"
 WEIGHTS = os.path.join(ROOT, "gnu_femlisp_b200", "weights", "damping3d.fmgnet")
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes per top-level node of one launch (read + write), from the ncu
+# capture of the 257^3 case (profiles/k_mf4_q1_3d_mixed_257cube.md): mode 2
+# 628.9 MB, FP64 mode 0 322.3 MB, mode 1 257.6 MB over 16,974,593 nodes
+TOP_TRAFFIC_B_PER_NODE = {"k_mf4<float,double,float,32,2,1>": 628.9e6 / 16974593,
+                          "k_mf4<double,float,float,32,0,1>": 322.3e6 / 16974593,
+                          "k_mf4<float,double,float,32,1,0>": 257.6e6 / 16974593}
 
 
 def parse_args():
@@ -45,6 +51,8 @@ def parse_args():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--level", type=int, default=8, help="top level (256^3 cells = 8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=300.0,
+                    help="--impl reference: seconds of timed steps after which no further step starts")
     ap.add_argument("--matvec-reps", type=int, default=20)
     ap.add_argument("--no-learned", action="store_true", help="mixed precision without the damping network")
     ap.add_argument("--config", choices=["c2", "c3", "c4", "c5"], default="c3",
@@ -53,11 +61,12 @@ def parse_args():
                           "48^3 cells, FP64 CG + block-Jacobi V(2,2); each its own JSON line"))
     ap.add_argument("--c5-level", type=int, default=4, help="c5: 3 x 2^level cells per direction")
     ap.add_argument("--c4-fields", type=int, default=256)
-    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv", "ssc"], default=None,
+    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv", "ssc", "mfs"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
                          "the launch count, one more solve; net: the damping network on every level, 8 times; "
                          "c5: the elasticity setup, two mixed+learned solves, the launch count, one more; "
-                         "c5mv: the elasticity FP64 block matvec, 5 times)")
+                         "c5mv: the elasticity FP64 block matvec, 5 times; mfs: one mixed solve, then inside "
+                         "the NVTX range 'mfs' one launch of each top-level kernel of the mixed solve)")
     return ap.parse_args()
 
 
@@ -161,31 +170,80 @@ def plain_cfg(G, maxsteps=200):
                       C.FMG_MULTIPLICATIVE)
 
 
-def cpu_baseline(wl, steps_gpu: int, budget_s: float = 25.0) -> dict:
-    """The oracle (C++ restatement, OpenMP) on a bounded sample of the same
-    workload: assembly of all levels plus CG steps until the budget is spent,
-    per-step time extrapolated to the step count of the full solve."""
+def _rel(a, b) -> float:
+    """max |a - b| / max |b| (0 when both are zero)."""
+    den = float(np.max(np.abs(b))) if np.size(b) else 0.0
+    num = float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) if np.size(b) else 0.0
+    return num / den if den > 0 else num
+
+
+def parity_block(o, ref, g, gpu_hist, gpu_x, levels) -> dict:
+    """The GPU's plain FP64 path against the oracle on the same workload:
+    every assembled level matrix and the top-level rhs (bitwise count and the
+    largest relative difference), the complete :defnorm history and the
+    solution of the solve to 1e-10 (bitwise and relative).  The bar is 1e-12
+    relative; the GPU path follows the oracle's operation order, so bitwise
+    equality is expected."""
+    nbit, worst = 0, 0.0
+    for lev in levels:
+        a, b = g.matrix(lev), o.matrix(lev)
+        nbit += int(np.array_equal(a, b))
+        worst = max(worst, _rel(a, b))
+        del a, b
+    rg, ro = g.rhs(), o.rhs()
+    hist_same = len(gpu_hist) == len(ref.history) and np.array_equal(gpu_hist, ref.history)
+    hist_rel = (float(np.max(np.abs(gpu_hist - ref.history) / np.abs(ref.history)))
+                if len(gpu_hist) == len(ref.history) else float("inf"))
+    x_rel = _rel(gpu_x, ref.x)
+    return {"levels": len(levels), "levels_bitwise": nbit, "matrix_rel": worst,
+            "rhs_bitwise": bool(np.array_equal(rg, ro)), "rhs_rel": _rel(rg, ro),
+            "steps_gpu": int(len(gpu_hist) - 1), "steps_oracle": int(ref.steps),
+            "history_bitwise": bool(hist_same), "history_rel": hist_rel,
+            "x_bitwise": bool(np.array_equal(gpu_x, ref.x)), "x_rel": x_rel, "_x_oracle": ref.x,
+            "ok": bool(hist_rel <= 1e-12 and x_rel <= 1e-12 and worst <= 1e-12),
+            "bar": "1e-12 relative (history, solution, level matrices)"}
+
+
+def oracle_c3(wl):
+    """The oracle on the benchmark workload: a hierarchy with its
+    coefficients (not yet assembled)."""
     from oracle import oracle as O
     o = O.Oracle(3, 1, wl.level, base_level=wl.base_level)
     o.set_coefficient(O.K_CELL, wl.kcell)
+    return o
+
+
+def oracle_cg_cfg(rtol=1e-10):
+    from oracle import oracle as O
+    return O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=rtol, maxsteps=200)
+
+
+def cpu_baseline(wl, g, gpu_hist, gpu_x) -> tuple:
+    """The oracle (C++ restatement, OpenMP, all host threads) on the same
+    workload, measured, not extrapolated: assembly of every level, then one
+    complete CG + V(1,1) Jacobi(0.6) solve to 1e-10 with the oracle's own step
+    count.  The same oracle run pins the GPU's plain FP64 path at full size
+    (``parity_block``).  Beside it, one complete solve on one thread one level
+    down (129^3 nodes), timed whole."""
+    from oracle import oracle as O
+    o = oracle_c3(wl)
     t0 = time.perf_counter()
     o.assemble()
     t_asm = time.perf_counter() - t0
-    nsteps = 2
-    cfg = O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=1e-10, maxsteps=nsteps - 1)
     t0 = time.perf_counter()
-    r = o.solve(cfg)
-    t_sample = time.perf_counter() - t0
-    per_step = t_sample / max(r.steps, 1)
-    t_solve = per_step * steps_gpu
+    ref = o.solve(oracle_cg_cfg())
+    t_solve = time.perf_counter() - t0
+    par = parity_block(o, ref, g, gpu_hist, gpu_x, range(wl.base_level, wl.level + 1))
+    del o
     n = wl.nodes
-    return {"value": n / t_solve / 1e6, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
-            "cores": O.num_threads(), "kind": "port",
-            "sample": (f"oracle C++ restatement, {O.num_threads()} OpenMP threads: assembly of levels "
-                       f"{wl.base_level}..{wl.level} ({t_asm:.1f} s) + {r.steps} CG steps "
-                       f"({t_sample:.1f} s), per-step time x {steps_gpu} steps of the full solve"),
-            "assembly_s": t_asm, "cg_step_s": per_step, "time_to_solution_est_s": t_solve,
-            "host": host_info(), "one_thread": one_thread_step(wl, per_step)}
+    cpu = {"value": n / t_solve / 1e6, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
+           "cores": O.num_threads(), "kind": "port",
+           "sample": (f"oracle C++ restatement, {O.num_threads()} OpenMP threads: one complete solve to 1e-10 "
+                      f"({ref.steps} CG steps, {t_solve:.1f} s) from the assembled hierarchy (assembly of levels "
+                      f"{wl.base_level}..{wl.level}: {t_asm:.1f} s, not in value)"),
+           "assembly_s": t_asm, "time_to_solution_s": t_solve, "cg_steps": int(ref.steps),
+           "e2e_s": t_asm + t_solve, "host": host_info(), "one_thread": one_thread_solve(wl)}
+    return cpu, par
 
 
 def host_info() -> dict:
@@ -202,31 +260,37 @@ def host_info() -> dict:
     return {"nproc": os.cpu_count(), "cpu_model": model, "omp_threads": os.environ.get("OMP_NUM_THREADS")}
 
 
-def one_thread_step(wl, per_step_all: float) -> dict:
-    """One CG step of the same algorithm on one thread, timed one level below
-    the workload (8x fewer unknowns) and scaled by the unknowns, beside the
-    all-thread step time."""
+def one_thread_solve(wl) -> dict:
+    """One complete solve of the same algorithm on one thread, one level below
+    the workload (8x fewer unknowns), timed whole (assembly and solve)."""
     from gnu_femlisp_b200 import problems
     from oracle import oracle as O
     nthreads = O.num_threads()
     small = problems.c3(seed=0, level=wl.level - 1)
-    o = O.Oracle(3, 1, small.level, base_level=small.base_level)
-    o.set_coefficient(O.K_CELL, small.kcell)
-    o.assemble()
-    cfg = O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=1e-10, maxsteps=1)
     O.set_num_threads(1)
     try:
+        o = oracle_c3(small)
         t0 = time.perf_counter()
-        r = o.solve(cfg)
-        t1 = (time.perf_counter() - t0) / max(r.steps, 1) * (wl.nodes / small.nodes)
+        o.assemble()
+        t_asm = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        r = o.solve(oracle_cg_cfg())
+        t_solve = time.perf_counter() - t0
     finally:
         O.set_num_threads(nthreads)
-    return {"cg_step_s": t1, "speedup_all_threads": t1 / per_step_all,
-            "sample": f"1 thread, {r.steps} CG steps at {small.nodes} unknowns, scaled by {wl.nodes / small.nodes:.2f}"}
+    return {"nodes": small.nodes, "assembly_s": t_asm, "time_to_solution_s": t_solve, "cg_steps": int(r.steps),
+            "mdof_per_s": small.nodes / t_solve / 1e6,
+            "sample": f"1 thread, one complete solve to 1e-10 at {small.nodes} unknowns ({r.steps} CG steps)"}
 
 
 def run_reference(args, world, rank):
-    """CPU restatement of the reference algorithm, all host threads."""
+    """The reference algorithm on the host cores: the CPU restatement (C++,
+    OpenMP, all host threads).  The hierarchy is assembled once (timed and
+    reported beside the line); one step = one complete CG + V(1,1)
+    Jacobi(0.6) solve from it to 1e-10 with the oracle's own step count,
+    timed whole -- the definition of the GPU arm's value.  Steps run until
+    --steps are done or the timed region has used --ref-budget seconds (at
+    least one); "steps" is the number actually timed."""
     if rank != 0:
         return
     from gnu_femlisp_b200 import problems
@@ -234,40 +298,47 @@ def run_reference(args, world, rank):
     O.build()
     wl = problems.c3(seed=0, level=args.level)
     n = wl.nodes
-    o = O.Oracle(3, 1, wl.level, base_level=wl.base_level)
-    o.set_coefficient(O.K_CELL, wl.kcell)
+    o = oracle_c3(wl)
     t0 = time.perf_counter()
     o.assemble()
     t_asm = time.perf_counter() - t0
-    # sample: a fixed number of CG steps per timed step, extrapolated by the
-    # number of steps the full solve takes (measured once on a warm-up solve
-    # of the same algorithm when it fits, else assumed equal to `calib`)
-    sample_steps = 2
-    cfg = O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=1e-10, maxsteps=sample_steps - 1)
-    times = []
-    for it in range(args.warmup + args.steps):
+    cfg = oracle_cg_cfg()
+
+    def step():
         t0 = time.perf_counter()
         r = o.solve(cfg)
         dt = time.perf_counter() - t0
-        if it >= args.warmup:
-            times.append(dt / max(r.steps, 1))
-    per_step = float(np.mean(times))
-    # the plain FP64 GPU path runs this algorithm with bitwise the oracle's
-    # arithmetic and takes 17 CG steps on this workload
-    full_steps = int(os.environ.get("FMG_C3_STEPS", "0")) or 17
-    t_solve = per_step * full_steps + t_asm
+        if r.status != 0:
+            raise RuntimeError(f"oracle solve did not converge in {r.steps} steps")
+        return dt, r.steps
+
+    nwarm = min(args.warmup, 1)  # one warm-up solve touches every page; more add nothing on the host
+    for _ in range(nwarm):
+        step()
+    sol, steps = [], 0
+    t_start = time.perf_counter()
+    while len(sol) < args.steps:
+        dt, steps = step()
+        sol.append(dt)
+        if time.perf_counter() - t_start + dt > args.ref_budget:
+            break
+    t_solve = float(np.mean(sol))
     val = n / t_solve / 1e6
     line = {
         "metric": METRIC, "value": val, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
-        "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "impl": "reference", "n_gpus": world, "steps": len(sol), "warmup": nwarm,
+        "steps_requested": args.steps, "warmup_requested": args.warmup,
         "ms_per_step": t_solve * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl.name, "nodes": n, "solver": "CG + V(1,1) Jacobi(0.6), base level 2",
                    "inputs": "larger than L2"},
-        "cpu_baseline": {"value": val, "unit": "MDoF/s to 1e-10", "cores": O.num_threads(), "kind": "port",
-                         "host": host_info(),
-                         "sample": (f"{sample_steps} CG steps per timed step ({per_step:.2f} s/step) x "
-                                    f"{full_steps} steps + assembly {t_asm:.1f} s")},
+        "time_to_solution_s": t_solve, "cg_steps": int(steps),
+        "assembly_s": t_asm, "assembly_note": "assembly of all levels, once before the timed steps (not in value)",
+        "cpu_baseline": {"value": val, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
+                         "cores": O.num_threads(), "kind": "port", "host": host_info(),
+                         "sample": (f"{len(sol)} timed steps, each one complete solve to 1e-10 from the assembled "
+                                    f"hierarchy ({steps} CG steps, {t_solve:.2f} s); the oracle C++ restatement of "
+                                    f"the reference algorithm")},
         "e2e": {"value": val, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -413,7 +484,29 @@ def run_mine(args, world, rank, local):
         vcyc()
     t_cycle, _ = timed(vcyc, 10)
 
-    # ---- dominant kernel of the plain path: the FP64 stencil matvec of the top level
+    # ---- the headline step's top-level kernels, each timed alone (CUDA events
+    # on the library's stream, inputs larger than L2) against the measured
+    # copy peak: per launch, algorithmic bytes / mean launch time
+    peak, peak_kind = measured_peaks()
+    xm.fill(0.0)
+    g.solve_mixed(cfg, xm, matrix_free=True)  # leaves the buffers the kernels run on
+    cells = wl.n_cells ** 3
+    top_kernels = []
+    for kind, name, alg, per_solve in (
+            (C.FMG_MXK_SMOOTH, "k_mf4<float,double,float,32,2,1> (top-level post-smoothing + the flexible CG's (z,r), (z,a))",
+             n * (5 * 4 + 2 * 8) + 4 * cells, ninner),
+            (C.FMG_MXK_MATVEC64, "k_mf4<double,float,float,32,0,1> (FP64 a = A p of the FP32 direction + (a,p))",
+             n * (4 + 8) + 8 * cells, ninner + 1),
+            (C.FMG_MXK_RESIDUAL, "k_mf4<float,double,float,32,1,0> (top-level FP32 residual)", n * 3 * 4 + 4 * cells, ninner + 1)):
+        g.mixed_top_kernel(kind, 3)
+        t_k, _ = timed(lambda kind=kind: g.mixed_top_kernel(kind, args.matvec_reps), 1)
+        t_k /= args.matvec_reps
+        top_kernels.append({"kernel": name, "algorithmic_bytes": int(alg), "launch_ms": t_k * 1e3,
+                            "achieved_gbs": alg / t_k / 1e9, "frac": alg / t_k / 1e9 / peak,
+                            "launches_per_solve": int(per_solve), "ms_per_solve": t_k * 1e3 * per_solve})
+    dom = max(top_kernels, key=lambda r: r["ms_per_solve"])
+    # ---- the north star's matvec criterion: the plain path's FP64 stencil
+    # matvec of the top level (assembled matrix)
     P = g.vector(values=np.random.default_rng(1).standard_normal(n))
     Y = g.vector()
 
@@ -424,10 +517,6 @@ def run_mine(args, world, rank, local):
     t_mv, _ = timed(mv, args.matvec_reps)
     nnz = (3 * wl.n_cells + 1) ** 3
     alg_bytes = 8 * nnz + 16 * n
-    # DRAM traffic of one launch: 233.7 B per row, from the ncu capture at
-    # 129^3 (profiles/k_spmv_q1_3d_fp64_128cube.md), scaled by rows
-    traffic = 233.7 * n
-    peak, peak_kind = measured_peaks()
     achieved = alg_bytes / t_mv / 1e9
 
     line = {
@@ -450,15 +539,22 @@ def run_mine(args, world, rank, local):
         "mixed_without_learned": {"time_to_solution_s": t_mp_max, "inner_iterations": int(ni_p),
                                   "speedup_vs_plain_fp64": t_plain_max / t_mp_max},
         "speedup_vs_plain_fp64": t_plain_max / t_head_max,
+        "time_to_solution_incl_learned_setup_s": t_head_max + (t_setup or 0.0),
+        "speedup_incl_learned_setup_vs_plain_fp64": t_plain_max / (t_head_max + (t_setup or 0.0)),
         "error_vs_fp64": {"vs_plain_same_tol": err_plain, "vs_fp64_1e-13": err_tight,
                           "plain_vs_fp64_1e-13": err_plain_tight},
         "mdof_per_s_per_vcycle": n / t_cycle / 1e6,
         "vcycle_ms": t_cycle * 1e3,
         "ms_per_inner_iteration": t_head_max * 1e3 / max(int(ninner), 1),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "k_spmv<3,1> (top-level FP64 matvec, outer residual)", "peak_kind": peak_kind,
-                     "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
+        "roofline": {"bound": "hbm", "achieved": dom["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": dom["frac"], "traffic": TOP_TRAFFIC_B_PER_NODE.get(dom["kernel"].split(" ")[0], 0) * n or None,
+                     "kernel": dom["kernel"], "peak_kind": peak_kind,
+                     "algorithmic_bytes": dom["algorithmic_bytes"], "launch_ms": dom["launch_ms"],
+                     "top_level_kernels": top_kernels},
+        "matvec_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": 233.7 * n,
+                            "kernel": "k_spmv<3,1> (top-level FP64 matvec of the assembled matrix, plain path)",
+                            "peak_kind": peak_kind, "algorithmic_bytes": alg_bytes, "launch_ms": t_mv * 1e3},
         "e2e": {"value": world * n / t_e2e_max / 1e6, "unit": "MDoF/s to 1e-10 (N_top / time-to-solution)",
                 "h2d_bytes_per_step": int(k_np.nbytes), "d2h_bytes_per_step": int(x_np.nbytes),
                 "time_s": t_e2e_max,
@@ -472,9 +568,13 @@ def run_mine(args, world, rank, local):
                            "judge": judge, "status": status_learned,
                            "setup": "damping network on levels 3..8 (tcgen05 convolutions) + plain-cycle judge"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl, int(steps))
-        line["cpu_baseline"]["note"] = ("plain FP64 algorithm (the reference's), CG step count of the "
-                                        "GPU plain solve")
+        cpu, par = cpu_baseline(wl, g, hist, x_plain)
+        line["cpu_baseline"] = cpu
+        line["parity"] = par
+        head = line["error_vs_fp64"]
+        xo = par.pop("_x_oracle")
+        head["mixed_vs_oracle"] = float(np.linalg.norm(x_head - xo) / np.linalg.norm(xo))
+        head["mixed_vs_oracle_max_rel"] = _rel(x_head, xo)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del P, Y, B, R, X, x, xm
@@ -592,6 +692,34 @@ def run_profile_ssc(args):
     ctx.close()
 
 
+def run_profile_mfs(args):
+    """The matrix-free top-level kernels of the mixed solve at `--level`: one
+    plain mixed solve (no damping network) leaves their buffers, then one
+    launch of each (FMG_MXK_SMOOTH, FMG_MXK_MATVEC64, FMG_MXK_RESIDUAL)
+    inside the NVTX range 'mfs' (ncu --nvtx --nvtx-include mfs/)."""
+    import torch
+
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    C = G._capi
+    wl = problems.c3(seed=0, level=args.level)
+    ctx = G.Context(0)
+    g = G.Grid(ctx, 3, 1, wl.level, base_level=wl.base_level)
+    g.set_coefficient(C.FMG_K_CELL, wl.kcell)
+    g.assemble()
+    x = g.vector()
+    g.solve_mixed(plain_cfg(G), x, matrix_free=True)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_push("mfs")
+    for kind in (C.FMG_MXK_SMOOTH, C.FMG_MXK_MATVEC64, C.FMG_MXK_RESIDUAL):
+        g.mixed_top_kernel(kind, 1)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print("mfs kernels launched", flush=True)
+    g.close()
+    ctx.close()
+
+
 def run_profile(args):
     """Workloads for ncu captures (profiles/ names the commands)."""
     import gnu_femlisp_b200 as G
@@ -602,6 +730,8 @@ def run_profile(args):
         return run_profile_c5(args)
     if args.profile == "ssc":
         return run_profile_ssc(args)
+    if args.profile == "mfs":
+        return run_profile_mfs(args)
     wl = problems.c3(seed=0, level=args.level)
     ctx = G.Context(0)
     g = G.Grid(ctx, 3, 1, wl.level, base_level=wl.base_level)

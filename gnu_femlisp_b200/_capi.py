@@ -20,6 +20,7 @@ FMG_ASSEMBLE_REDISCRETIZE, FMG_ASSEMBLE_GALERKIN = 0, 1
 FMG_CSR, FMG_CCS = 0, 1
 FMG_METHOD_MG, FMG_METHOD_CG_MG, FMG_METHOD_CG = 0, 1, 2
 FMG_MULTIPLICATIVE, FMG_ADDITIVE = 0, 1
+FMG_MXK_RESIDUAL, FMG_MXK_SMOOTH, FMG_MXK_MATVEC64 = 1, 2, 3
 
 _ERRNAMES = {-1: "FMG_ERR_ARG", -2: "FMG_ERR_CUDA", -3: "FMG_ERR_STATE", -4: "FMG_ERR_NOMEM",
              -5: "FMG_ERR_NUMERIC", -6: "FMG_ERR_UNSUPPORTED", -7: "FMG_ERR_IO"}
@@ -111,6 +112,10 @@ SIGNATURES = {
     "fmg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp, _dp, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "fmg_dot_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_long, _vp]),
+    "fmg_mixed_top_kernel": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "fmg_wait_selftest": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_longlong]),
+    "fmg_cg_start": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), _vp]),
+    "fmg_cg_step": (ctypes.c_int, [_vp, _vp, _vp, _dp]),
     "fmg_assemble_levels": (ctypes.c_int, [_vp, ctypes.c_int]),
     "fmg_solve_mixed": (ctypes.c_int, [_vp, ctypes.POINTER(SolveCfg), ctypes.POINTER(MixedCfg), _vp, _dp,
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

@@ -103,6 +103,24 @@ def slots_to_csr(A: np.ndarray, dim: int, order: int, nc: int = 1):
     return start, cols, vals
 
 
+def _compressed(start, index, values):
+    """Compressed rows (or columns) as the C-ABI reads them: 32-bit starts and
+    indices, FP64 values.  The starts must begin at 0 and never decrease, and
+    the index and value arrays must hold the start[-1] entries they promise
+    (the library reads that many)."""
+    st = np.ascontiguousarray(start, dtype=np.int32)
+    ix = np.ascontiguousarray(index, dtype=np.int32)
+    va = np.ascontiguousarray(values, dtype=np.float64)
+    if st.ndim != 1 or st.size < 1:
+        raise ValueError("start must be a 1-D array of at least one entry")
+    if st[0] != 0 or np.any(np.diff(st) < 0):
+        raise ValueError("start must begin at 0 and be nondecreasing")
+    nnz = int(st[-1])
+    if ix.size < nnz or va.size < nnz:
+        raise ValueError(f"start promises {nnz} entries; index holds {ix.size}, values hold {va.size}")
+    return st, ix, va
+
+
 class Grid:
     """A level hierarchy of the uniformly refined unit n-cube with a Lagrange
     Q1/Q2 space (``fmg_grid_create``); levels base_level..level."""
@@ -141,9 +159,7 @@ class Grid:
         (rows fine, columns coarse; ``"ccs"``: the arrays of the transpose's
         rows)."""
         lay = {"csr": C.FMG_CSR, "ccs": C.FMG_CCS}[layout]
-        st = np.ascontiguousarray(start, dtype=np.int32)
-        ix = np.ascontiguousarray(index, dtype=np.int32)
-        va = np.ascontiguousarray(values, dtype=np.float64)
+        st, ix, va = _compressed(start, index, values)
         ip = ctypes.POINTER(ctypes.c_int)
         nfine = self.nnodes(fine_level)
         self.ctx.check(self._lib.fmg_set_interpolation(self.h, fine_level, lay, st.ctypes.data_as(ip),
@@ -194,9 +210,7 @@ class Grid:
         in the grid's node-major lexicographic numbering.  The grid counts as
         assembled once every level has a matrix."""
         lay = {"csr": C.FMG_CSR, "ccs": C.FMG_CCS}[layout]
-        st = np.ascontiguousarray(start, dtype=np.int32)
-        ix = np.ascontiguousarray(index, dtype=np.int32)
-        va = np.ascontiguousarray(values, dtype=np.float64)
+        st, ix, va = _compressed(start, index, values)
         ip = ctypes.POINTER(ctypes.c_int)
         self.ctx.check(self._lib.fmg_set_matrix(self.h, level, lay, st.ctypes.data_as(ip), ix.ctypes.data_as(ip),
                                                 C.dptr(va), st.size - 1), "set_matrix")
@@ -266,6 +280,16 @@ class Grid:
                                            ctypes.byref(ns), ctypes.byref(st)), "solve")
         return hist[: ns.value + 1].copy(), ns.value, st.value
 
+    def cg_start(self, cfg: C.SolveCfg, r: "Vector"):
+        """``fmg_cg_start``: the <cg> iterator's initialize (restart from r)."""
+        self.ctx.check(self._lib.fmg_cg_start(self.h, ctypes.byref(cfg), r.h), "cg_start")
+
+    def cg_step(self, x: "Vector", r: "Vector") -> float:
+        """``fmg_cg_step``: one <cg> iterate on x and its residual r; returns ||r||."""
+        dn = ctypes.c_double()
+        self.ctx.check(self._lib.fmg_cg_step(self.h, x.h, r.h, ctypes.byref(dn)), "cg_step")
+        return dn.value
+
     def solve_mixed(self, cfg: C.SolveCfg, x: "Vector", inner_rtol: float = 1e-5, max_inner: int = 200,
                     max_outer: int = 20, matrix_free: bool = True):
         """FP64 flexible CG preconditioned by the FP32/BF16 V-cycle; returns
@@ -279,6 +303,12 @@ class Grid:
                                                  hist.size, ctypes.byref(no), ctypes.byref(ni), ctypes.byref(st)),
                        "solve_mixed")
         return hist[: no.value + ni.value + 1].copy(), no.value, ni.value, st.value
+
+    def mixed_top_kernel(self, kind: int, reps: int = 1):
+        """``fmg_mixed_top_kernel``: `reps` launches of one top-level kernel of
+        the mixed solve (FMG_MXK_RESIDUAL, FMG_MXK_SMOOTH, FMG_MXK_MATVEC64) on
+        the buffers the last matrix-free mixed solve left; nothing waits."""
+        self.ctx.check(self._lib.fmg_mixed_top_kernel(self.h, kind, reps), "mixed_top_kernel")
 
     def learned_judge(self, cfg: C.SolveCfg):
         """Plain cycle vs the installed node damping (``fmg_learned_judge``);

@@ -115,6 +115,11 @@ struct fmg_grid {
   double rho_plain = 0.0;      // judge: slow-mode contraction of the plain cycle (0: not measured)
   double rho_learned = 0.0;    //        and of the learned cycle
   int reverts = 0;             // mixed solves whose runtime judge fell back to the plain cycle
+  // <cg> iterator run step by step (fmg_cg_start / fmg_cg_step): alpha of the
+  // last restart or step, and the configuration it was started with
+  double cg_alpha = 0.0;
+  bool cg_started = false;
+  fmg_solve_cfg cg_cfg{};
   std::vector<void*> allocs;
   int vecs = 0;                // live vectors: the grid outlives them
   bool destroyed = false;      // fmg_grid_destroy called while vectors were alive
@@ -1573,7 +1578,99 @@ int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, 
   return launched(c, "solve");
 }
 
+// <cg>'s iterator one call at a time (krylow.lisp:72-132), for a host whose
+// own solver loop drives it (linsolve.lisp:58-73): fmg_cg_start is the
+// iterator's initialize (restart: w := r, p := M(w), alpha := (p, r)),
+// fmg_cg_step its iterate (a := A p, lam := alpha / (a, p), x += lam p,
+// r -= lam a, q := M(r), alpha' := (q, r), p := (alpha'/alpha) p + q).  The
+// search direction and the preconditioner's vectors stay in the grid between
+// calls; x and r are the caller's vectors (r up to date at the start,
+// :residual-before t; kept up to date by every step, :residual-after t).
+int fmg_cg_start(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* rv) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  FMG_RC(ensure_top(g));
+  int rc = check_cfg(g, cfg);
+  if (rc) return rc;
+  if (vec_check(rv, g, g->top)) return FMG_ERR_ARG;
+  if (cfg->method == FMG_METHOD_MG) return set_err(g->ctx, FMG_ERR_ARG, "fmg_cg_start: a CG method");
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const long long n = g->lev[g->top].N * g->nc;
+  MG mg{g, *cfg, false, st};
+  double* r = rv->d;
+  if (cfg->method == FMG_METHOD_CG_MG) {
+    launch_fill(g->p, n, 0.0, st);  // the preconditioner starts from x = 0 (make-domain-vector-for)
+    if (cfg->compat_alias) {
+      launch_copy(r, g->w, n, st);
+      mg.iterate(&g->p, &g->xs, g->w, g->w);
+    } else {
+      launch_copy(r, g->w2, n, st);
+      mg.iterate(&g->p, &g->xs, r, g->w2);
+    }
+  } else {
+    launch_copy(r, g->p, n, st);
+  }
+  launch_dot(g->p, r, n, reducer(g, EPI_STORE, S_ALPHA), st);
+  if ((rc = launched(c, "cg start"))) return rc;
+  if ((rc = read_scalars(g))) return rc;
+  g->cg_alpha = c->host_scal[S_ALPHA];
+  g->cg_cfg = *cfg;
+  g->cg_started = true;
+  return FMG_OK;
+}
+
+int fmg_cg_step(fmg_grid* g, fmg_vec* xv, fmg_vec* rv, double* defnorm) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (!g->cg_started) return set_err(g->ctx, FMG_ERR_STATE, "fmg_cg_step before fmg_cg_start");
+  if (vec_check(xv, g, g->top) || vec_check(rv, g, g->top) || xv == rv) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const fmg_solve_cfg& cf = g->cg_cfg;
+  const LevelView T = view(g, g->top);
+  const long long n = T.N * g->nc;
+  double *x = xv->d, *r = rv->d;
+  MG mg{g, cf, false, st};
+  int rc;
+  if (g->cg_alpha != 0.0) {  // krylow.lisp:106-127, as in fmg_solve
+    const bool pre = cf.method == FMG_METHOD_CG_MG;
+    const Reduce Rl = reducer(g, EPI_CG_LAMBDA, 0);
+    launch_spmv(T, g->p, nullptr, g->a, g->p, &Rl, st);
+    const Reduce Rr = reducer(g, EPI_STORE, S_RR);
+    if (pre && cf.compat_alias)
+      launch_cg_update(g->scal, x, g->p, r, g->a, g->w, nullptr, g->q, n, Rr, st);
+    else if (pre)
+      launch_cg_update(g->scal, x, g->p, r, g->a, nullptr, g->w2, g->q, n, Rr, st);
+    else
+      launch_cg_update(g->scal, x, g->p, r, g->a, g->q, nullptr, nullptr, n, Rr, st);
+    if (pre) {
+      if (cf.compat_alias) mg.iterate(&g->q, &g->xs, g->w, g->w);
+      else mg.iterate(&g->q, &g->xs, r, g->w2);
+    }
+    launch_dot(g->q, r, n, reducer(g, EPI_CG_ALPHA, 0), st);
+    launch_p_update(g->scal, g->p, g->q, n, st);
+  } else {  // nothing to do: the residual norm is reported as it stands
+    launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
+  }
+  if ((rc = launched(c, "cg step"))) return rc;
+  if ((rc = read_scalars(g))) return rc;
+  if (g->cg_alpha != 0.0) g->cg_alpha = c->host_scal[S_ALPHA];
+  const double dn = std::sqrt(c->host_scal[S_RR]);
+  if (!std::isfinite(dn)) return set_err(c, FMG_ERR_NUMERIC, "defnorm is %g", dn);
+  if (defnorm) *defnorm = dn;
+  return FMG_OK;
+}
+
 }  // extern "C"
+
+// the give-up path of the bounded device waits, run alone
+extern "C" int fmg_wait_selftest(fmg_ctx* c, int arrive, int max_polls, long long max_ns) {
+  if (!c) return FMG_ERR_ARG;
+  if (max_polls < 1 || max_polls > (1 << 24) || max_ns < 1 || max_ns > 2000000000ll)
+    return set_err(c, FMG_ERR_ARG, "fmg_wait_selftest: polls in [1, 2^24], ns in [1, 2e9]");
+  const char* msg = nullptr;
+  const int rc = wait_selftest(arrive != 0, max_polls, max_ns, c->stream, &msg);
+  return rc == FMG_OK ? FMG_OK : set_err(c, rc, "%s", msg);
+}
 
 // context accessors for the allocation-free entry point (fmgpu_noalloc.cu)
 namespace fmg {
@@ -2142,6 +2239,31 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   return launched(c, "solve_mixed");
 }
 
+
+// The measurement hook over the mixed solve's top-level kernels: `reps`
+// launches of one of them on the buffers the last matrix-free mixed solve of
+// this grid left (FP32 cycle vectors, the FP32 search direction, the FP64
+// residual and a = A p), with the damping it formed the per-node
+// damping/diagonal for.  Nothing waits; the caller times the stream.
+extern "C" int fmg_mixed_top_kernel(fmg_grid* g, int kind, int reps) {
+  if (!g) return FMG_ERR_ARG;
+  if (!g->mx || !g->mx->mf || !g->mx->wd_ok || !g->r || !g->a)
+    return set_err(g->ctx, FMG_ERR_STATE, "fmg_mixed_top_kernel: no matrix-free mixed solve has run on this grid");
+  if (reps < 1 || kind < FMG_MXK_RESIDUAL || kind > FMG_MXK_MATVEC64)
+    return set_err(g->ctx, FMG_ERR_ARG, "fmg_mixed_top_kernel: kind %d, reps %d", kind, reps);
+  MixedState& X = *g->mx;
+  fmg_solve_cfg c{};
+  c.damp = (double)X.wd_w;
+  c.pre_steps = c.post_steps = c.gamma = 1;
+  MixedMG mg{g, X, c, g->ctx->stream};
+  const Reduce2 R = red2(X, EPI2_STORE, M_TMP, M_TMP);
+  for (int k = 0; k < reps; ++k) {
+    if (kind == FMG_MXK_RESIDUAL) mg.apply(g->top, 1, X.q, X.r, false, X.rtop, false, nullptr, nullptr, nullptr);
+    else if (kind == FMG_MXK_SMOOTH) mg.apply(g->top, 2, X.q, X.r, false, X.qs, false, g->r, g->a, &R);
+    else mg.matvec64(X.p32, g->a, R);
+  }
+  return launched(g->ctx, "mixed_top_kernel");
+}
 
 // ========================================================= learned damping
 // The damping network predicts per-node Jacobi damping for every level above

@@ -99,6 +99,9 @@ int net_forward(fmg_net* net, const ActGeom& g, double* omega, cudaStream_t st);
 int net_backward(fmg_net* net, const double* gomega, const double* omega, cudaStream_t st);
 void launch_adam(fmg_net* net, float lr, float b1, float b2, float eps, cudaStream_t st);
 int net_check_error(fmg_net* net, cudaStream_t st, const char** msg);
+// one CTA waits on an mbarrier with the given limits (arrive: a thread arrives
+// first); FMG_ERR_CUDA with *msg set when the wait gave up
+int wait_selftest(int arrive, int max_polls, long long max_ns, cudaStream_t st, const char** msg);
 
 // FP64 helpers of the training loss (level vectors of length n)
 // nc values per node (vector form), nodes on the Dirichlet faces zero

@@ -1179,6 +1179,43 @@ int net_check_error(fmg_net* net, cudaStream_t st, const char** msg) {
   return FMG_OK;
 }
 
+// The give-up path of the bounded waits, run alone: one CTA initialises an
+// mbarrier, optionally arrives on it, and waits with the given limits; a wait
+// that runs out records the error word, as the tensor-core kernels do, and the
+// kernel returns.  Nothing else (no MMA, no bulk copy) is in flight.
+__global__ void k_wait_selftest(unsigned* err, int arrive, int max_polls, unsigned long long max_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) umma::mbar_init(&bar);
+  __syncthreads();
+  if (arrive && threadIdx.x == 0) umma::mbar_arrive(&bar);
+  __syncthreads();
+  const bool ok = umma::mbar_wait_for(&bar, 0u, max_polls, max_ns);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(err, 1u);
+}
+
+int wait_selftest(int arrive, int max_polls, long long max_ns, cudaStream_t st, const char** msg) {
+  unsigned* err = nullptr;
+  unsigned h = 0;
+  *msg = "CUDA error in the wait self-test";
+  if (cudaMalloc((void**)&err, sizeof(unsigned)) != cudaSuccess) return FMG_ERR_CUDA;
+  int rc = FMG_OK;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess) rc = FMG_ERR_CUDA;
+  if (rc == FMG_OK) {
+    k_wait_selftest<<<1, 128, 0, st>>>(err, arrive, max_polls, (unsigned long long)max_ns);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(&h, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      rc = FMG_ERR_CUDA;
+  }
+  cudaFree(err);
+  if (rc == FMG_OK && h) {
+    *msg = "a bounded device wait timed out (the kernel gave up, recorded its error word and returned)";
+    rc = FMG_ERR_CUDA;
+  }
+  return rc;
+}
+
 void launch_rand_fill(double* e, int D, long long M, int dmask, unsigned long long seed, cudaStream_t st, int nc) {
   long long N = M;
   for (int k = 1; k < D; ++k) N *= M;

@@ -122,10 +122,11 @@ __device__ __forceinline__ uint64_t global_ns() {
 // bounded wait for the completion of the mbarrier phase with this parity:
 // gives up after kWaitNs of global time or kSpinLimit polls, whichever first
 constexpr uint64_t kWaitNs = 2000000000ull;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// the same wait with explicit limits (max_polls polls, max_ns of global time)
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, int max_polls, uint64_t max_ns) {
   const uint32_t a = smem_u32(bar);
   const uint64_t t0 = global_ns();
-  for (int it = 0; it < kSpinLimit; ++it) {
+  for (int it = 0; it < max_polls; ++it) {
     uint32_t done;
     asm volatile(
         "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
@@ -133,9 +134,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 255) == 255 && global_ns() - t0 > kWaitNs) return false;
+    if ((it & 255) == 255 && global_ns() - t0 > max_ns) return false;
   }
   return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, kSpinLimit, kWaitNs);
+}
+
+// one plain arrival on the mbarrier
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // whole warp: 32 (x32) or 16 (x16) consecutive FP32 columns of this thread's

@@ -14,6 +14,13 @@ Femlisp reads the same here:
   CG                                src/iteration/krylow.lisp:67-132
   LinearSolver, solve               src/iteration/linsolve.lisp:40-73,
                                     solve.lisp:113-164, iterate.lisp:105-250
+  elasticity_model_problem          src/problem/elasticity.lisp:71-123
+  Iterator, make_iterator           src/iteration/linit.lisp:48-67 (<iterator>,
+                                    make-iterator), multigrid.lisp:303-393,
+                                    krylow.lisp:72-132
+  solve_iterating                   the <linear-solver> loop driving an
+                                    iterator: linsolve.lisp:58-73,
+                                    solve.lisp:139-155, iterate.lisp:239-250
 
 Success/failure conditions are given as Femlisp forms, e.g.
 ``"(or (< :defnorm 1.0e-12) (> :step 10))"``.  Coefficients are sampled on
@@ -49,6 +56,28 @@ class CdrProblem:
 def cdr_model_problem(dim: int, diffusion=None, source=None, dirichlet_mask=None) -> CdrProblem:
     return CdrProblem(dim, 1.0 if diffusion is None else diffusion, 1.0 if source is None else source,
                       dirichlet_mask)
+
+
+@dataclass
+class ElasticityProblem:
+    """Linear elasticity -div(C : eps(u)) = f on the unit 3-cube with the
+    isotropic elasticity tensor of Lame parameters lambda = mu = E
+    (isotropic-elasticity-tensor, elasticity.lisp:71-88): E a constant, one
+    value per top-level cell, or callable(x) at the cell centres; a constant
+    body force; every component clamped (u = 0) on the faces in
+    ``dirichlet_mask`` (bit 0: x = 0)."""
+    dim: int
+    lame: Any = 1.0
+    force: tuple = (0.0, 0.0, -1.0)
+    dirichlet_mask: int = 0b000001
+
+
+def elasticity_model_problem(dim: int = 3, lame=None, force=None, dirichlet_mask=0b000001) -> ElasticityProblem:
+    """elasticity-model-problem (elasticity.lisp:112-123) with lambda = mu = E."""
+    if dim != 3:
+        raise ValueError("the vector form is built for 3D")
+    return ElasticityProblem(dim, 1.0 if lame is None else lame,
+                             (0.0, 0.0, -1.0) if force is None else tuple(force), dirichlet_mask)
 
 
 @dataclass
@@ -111,9 +140,10 @@ class DiscreteSystem:
     solver asks for (the reference assembles coarse levels when the
     multigrid iterator is made, geomg.lisp:109-142)."""
 
-    def __init__(self, problem: CdrProblem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
-        if fe.nr_comps != 1:
-            raise NotImplementedError("vector-valued problems are not built yet")
+    def __init__(self, problem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
+        vector = isinstance(problem, ElasticityProblem)
+        if vector != (fe.nr_comps == 3):
+            raise ValueError("an elasticity problem takes lagrange_fe(order, nr_comps=3), a cdr problem nr_comps=1")
         self.problem, self.mesh, self.fe = problem, mesh, fe
         self.ctx = ctx or Context()
         self._grids: dict[int, Grid] = {}
@@ -121,6 +151,9 @@ class DiscreteSystem:
     def grid(self, base_level: int = 0) -> Grid:
         if base_level not in self._grids:
             p, m = self.problem, self.mesh
+            if isinstance(p, ElasticityProblem):
+                self._grids[base_level] = self._elasticity_grid(base_level)
+                return self._grids[base_level]
             g = Grid(self.ctx, p.dim, self.fe.order, m.level, base_level=base_level, n0=m.n0,
                      dirichlet_mask=p.dirichlet_mask)
             ncell = g.n_cells
@@ -138,6 +171,23 @@ class DiscreteSystem:
                 g.set_coefficient(C.FMG_F_CONST, [float(f)])
             self._grids[base_level] = g.assemble()
         return self._grids[base_level]
+
+    def _elasticity_grid(self, base_level: int) -> Grid:
+        """Vector Q1/Q2 with 3 x 3 node blocks: E per top-level cell, the body
+        force, the clamped faces (ellsys-fe.lisp:68-218 with the tensor of
+        elasticity.lisp:71-88)."""
+        p, m = self.problem, self.mesh
+        g = Grid(self.ctx, 3, self.fe.order, m.level, base_level=base_level, n0=m.n0, ncomp=3,
+                 dirichlet_mask=p.dirichlet_mask)
+        ncell = g.n_cells
+        e = p.lame
+        if callable(e):
+            e = np.ascontiguousarray(e(cell_centres(3, ncell))).ravel()
+        elif np.ndim(e) == 0:
+            e = np.full(ncell ** 3, float(e))
+        g.set_coefficient(C.FMG_LAMBDA_MU_CELL, np.asarray(e, dtype=np.float64).ravel())
+        g.set_coefficient(C.FMG_F_VEC, list(p.force))
+        return g.assemble()
 
 
 def _csr_triple(m):
@@ -189,7 +239,7 @@ class AlgebraicSystem:
         return self._grids[base_level]
 
 
-def discretize_globally(problem: CdrProblem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
+def discretize_globally(problem, mesh: Mesh, fe: LagrangeFE, ctx: Context | None = None):
     """Returns (A, b) like Femlisp; here A is the DiscreteSystem and b its
     assembled right-hand side on the host."""
     sysm = DiscreteSystem(problem, mesh, fe, ctx)
@@ -328,7 +378,13 @@ class SolveReport:
     extra: dict = field(default_factory=dict)
 
 
-def make_cfg(iteration, success_if: str, failure_if: str, order: int | None = 1) -> tuple[C.SolveCfg, int, bool]:
+def make_cfg(iteration, success_if: str, failure_if: str, order: int | None = 1,
+             vector: bool = False) -> tuple[C.SolveCfg, int, bool]:
+    """The fmg_solve_cfg of an iteration and the solver's forms.  The default
+    smoother is select-smoother's (geomg.lisp:48-60): Gauss-Seidel for order
+    1, geometric SSC above; for an algebraic system, and for node blocks (the
+    GPU's block smoother is <jacobi> on the 3 x 3 diagonal blocks, linit.lisp:234),
+    <jacobi>."""
     cs = iteration.preconditioner if isinstance(iteration, CG) else iteration
     cfg = C.SolveCfg()
     if isinstance(iteration, CG):
@@ -340,7 +396,8 @@ def make_cfg(iteration, success_if: str, failure_if: str, order: int | None = 1)
     if cs is not None:
         # select-smoother (geomg.lisp:48-60): Gauss-Seidel for order 1, SSC
         # above; <jacobi> for an algebraic system (order None)
-        sm = cs.smoother or (Jacobi() if order is None else GaussSeidel() if order == 1 else GeometricSSC())
+        sm = cs.smoother or (Jacobi() if (order is None or vector) else GaussSeidel() if order == 1
+                             else GeometricSSC())
         if isinstance(sm, Jacobi):
             cfg.smoother, cfg.damp = C.FMG_JACOBI, sm.damp
         elif isinstance(sm, GeometricSSC):
@@ -373,7 +430,8 @@ def solve(blackboard: dict) -> dict:
     A: DiscreteSystem | AlgebraicSystem = blackboard["matrix"]
     solver: LinearSolver = blackboard["solver"]
     order = A.fe.order if A.fe is not None else None
-    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if, order)
+    vector = A.fe is not None and A.fe.nr_comps > 1
+    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if, order, vector)
     g = A.grid(base)
     x = g.vector()
     if "solution" in blackboard and blackboard["solution"] is not None:
@@ -386,4 +444,139 @@ def solve(blackboard: dict) -> dict:
     out["solution"] = x.get()
     out["history"] = hist
     out["report"] = SolveReport(st, steps, hist, rate)
+    return out
+
+
+# ------------------------------------------------------------- iterators
+
+
+@dataclass
+class Iterator:
+    """<iterator> (linit.lisp:48-67): what make_iterator returns -- the
+    matrix, an initialize function (or None) and an iterate function of
+    (x, b, r), and whether the residual must be up to date before a step and
+    is up to date after it.  Vectors are host arrays in the grid's node
+    order (node-major for node blocks), updated in place."""
+    matrix: Any
+    initialize: Callable | None
+    iterate: Callable
+    residual_before: bool
+    residual_after: bool
+    initializedp: bool = False
+
+
+def _system_of(A):
+    order = A.fe.order if A.fe is not None else None
+    vector = A.fe is not None and A.fe.nr_comps > 1
+    return order, vector
+
+
+def make_iterator(linit, A) -> Iterator:
+    """make-iterator (linit.lisp:48-67) of a GeometricCS or a CG on the
+    system A (a DiscreteSystem or an AlgebraicSystem).
+
+    GeometricCS: one cycle of the <mg-iteration> iterator per iterate
+    (multigrid.lisp:366-386, fmg_vcycle): the top-level solution, rhs and
+    residual are the given arrays; passing the same array as b and r is the
+    alias of <cg>'s preconditioner call (krylow.lisp:120).  :residual-after
+    nil.
+
+    CG (preconditioned by a GeometricCS): initialize restarts from the
+    residual (fmg_cg_start), iterate is one CG step (fmg_cg_step) with x and
+    r brought back up to date; :residual-before and :residual-after t
+    (krylow.lisp:72-132)."""
+    order, vector = _system_of(A)
+    if isinstance(linit, CG):
+        cfg, base, _ = make_cfg(linit, "(< :reduction 0.0)", "(> :step 0)", order, vector)
+        g = A.grid(base)
+        X, R = g.vector(), g.vector()
+
+        def initialize(x, b, r):
+            X.set(x)
+            R.set(r)
+            g.cg_start(cfg, R)
+
+        def iterate(x, b, r):
+            g.cg_step(X, R)
+            X.get(out=x)
+            R.get(out=r)
+            return {"residual_after": True}
+
+        it = Iterator(A, initialize, iterate, True, True)
+        it.grid, it.vectors = g, (X, R)
+        return it
+    if isinstance(linit, GeometricCS):
+        cfg, base, _ = make_cfg(linit, "(< :reduction 0.0)", "(> :step 0)", order, vector)
+        g = A.grid(base)
+        X, B, R = g.vector(), g.vector(), g.vector()
+
+        def iterate(x, b, r):
+            alias = b is r
+            X.set(x)
+            B.set(b)
+            if not alias:
+                R.set(r)
+            g.vcycle(cfg, X, B, B if alias else R)
+            X.get(out=x)
+            B.get(out=b)
+            if not alias:
+                R.get(out=r)
+            return {}
+
+        it = Iterator(A, None, iterate, True, False)
+        it.grid, it.vectors = g, (X, B, R)
+        return it
+    raise NotImplementedError(f"no GPU iterator for {linit!r}")
+
+
+def solve_iterating(blackboard: dict) -> dict:
+    """The <linear-solver> loop with the solver's iterator, step by step as
+    Femlisp runs it: (solve (blackboard :matrix A :rhs b :solver solver)).
+    Each step: ensure the residual (r = b - A x when it is not up to date;
+    ensure-residual, solve.lisp:139-155), :defnorm = l2 norm of r on the host,
+    the success/failure forms, then next-step (linsolve.lisp:58-73):
+    initialize once, iterate, and the iterator's :residual-after flag.
+    Returns the blackboard with :solution, :history and :report."""
+    A = blackboard["matrix"]
+    solver: LinearSolver = blackboard["solver"]
+    order, vector = _system_of(A)
+    cfg, base, step_success = make_cfg(solver.iteration, solver.success_if, solver.failure_if, order, vector)
+    it = make_iterator(solver.iteration, A)
+    g = it.grid
+    b = np.array(blackboard["rhs"] if blackboard.get("rhs") is not None else g.rhs(), dtype=np.float64)
+    x = np.array(blackboard.get("solution") if blackboard.get("solution") is not None else np.zeros(b.size))
+    Xv, Bv, Rv = g.vector(), g.vector(values=b), g.vector()
+    r = np.zeros_like(b)
+    residual_p = False
+    hist = []
+    status = "failure"
+    step = 0
+    while True:
+        if not residual_p:  # compute-residual (linit.lisp:73-80) on the device
+            Xv.set(x)
+            g.residual(Xv, Bv, Rv)
+            Rv.get(out=r)
+            residual_p = True
+        defnorm = float(np.sqrt(np.dot(r, r)))
+        hist.append(defnorm)
+        red = defnorm / hist[0] if hist[0] != 0 else 0.0
+        if (cfg.rtol > 0 and red < cfg.rtol) or (cfg.atol > 0 and defnorm < cfg.atol):
+            status = "success"
+            break
+        if step > cfg.maxsteps:
+            status = "success" if step_success else "failure"
+            break
+        if not it.initializedp:
+            if it.initialize is not None:
+                it.initialize(x, b, r)
+            it.initializedp = True
+        flags = it.iterate(x, b, r)
+        residual_p = it.residual_after and bool(flags.get("residual_after"))
+        step += 1
+    hist = np.array(hist)
+    rate = (hist[-1] / hist[0]) ** (1.0 / step) if step > 0 and hist[0] != 0 else float("nan")
+    out = dict(blackboard)
+    out["solution"] = x
+    out["history"] = hist
+    out["report"] = SolveReport(status, step, hist, rate)
     return out

@@ -258,6 +258,18 @@ int fmg_vcycle(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b,
    last step index, *status 0 = success, 1 = failure (maxsteps). */
 int fmg_solve(fmg_grid* grid, const fmg_solve_cfg* cfg, fmg_vec* x, double* hist, int hist_len,
               int* nsteps, int* status);
+/* The <cg> iterator (make-iterator, krylow.lisp:72-132) one call at a time,
+   for a host whose own <linear-solver> loop drives it (linsolve.lisp:58-73).
+   fmg_cg_start is the iterator's initialize: restart from the residual r
+   (up to date, :residual-before t): w := r, p := M(w) with the cycle of cfg
+   (method CG+MG; plain CG: p := r), alpha := (p, r).  fmg_cg_step is its
+   iterate: a := A p, lam := alpha / (a, p), x += lam p, r -= lam a,
+   q := M(r), alpha' := (q, r), p := (alpha'/alpha) p + q; r stays up to
+   date (:residual-after t) and *defnorm (may be NULL) receives ||r||.  The
+   search direction and the cycle's vectors stay in the grid between calls;
+   the arithmetic is fmg_solve's, step for step. */
+int fmg_cg_start(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_vec* r);
+int fmg_cg_step(fmg_grid* grid, fmg_vec* x, fmg_vec* r, double* defnorm);
 
 /* ------------------------------------------------------ mixed precision */
 /* No counterpart in the reference.  Mixed-precision variant of fmg_solve for
@@ -366,6 +378,30 @@ int fmg_learned_judge_mixed(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_
    runtime judge fell back to the plain cycle */
 int fmg_learned_status(const fmg_grid* grid, int* active, double* rho_plain, double* rho_learned, int* reverts);
 
+/* No counterpart in the reference: a measurement hook for the mixed solve's
+   top-level kernels.  Runs `reps` back-to-back launches of one of them on the
+   grid's own mixed-solve buffers, as an earlier fmg_solve_mixed on this grid
+   with the matrix-free top level left them (FMG_ERR_STATE otherwise), on the
+   context's stream without waiting, so that a caller can time them with
+   events on that stream.  The launches overwrite scratch vectors of the mixed
+   solve only; the next solve starts afresh. */
+#define FMG_MXK_RESIDUAL 1   /* FP32 r = b - A x, matrix-free */
+#define FMG_MXK_SMOOTH 2     /* FP32 y = x + w (b - A x) / d with the flexible CG's two FP64 dot products */
+#define FMG_MXK_MATVEC64 3   /* FP64 a = A p of the FP32 search direction, with (a, p) */
+int fmg_mixed_top_kernel(fmg_grid* grid, int kind, int reps);
+
+/* No counterpart in the reference: a self-test of the device-side give-up
+   path of the library's bounded waits (the mbarrier waits of the tensor-core
+   kernels, which otherwise give up only after 2^24 polls or 2 s).  One CTA
+   initialises an mbarrier and waits on it with the limits given (max_polls
+   polls in [1, 2^24], max_ns nanoseconds of global time in [1, 2e9]); no MMA
+   or bulk copy is in flight.  arrive = 1: a thread arrives first, the wait
+   completes, FMG_OK.  arrive = 0: nothing arrives, the wait gives up, the
+   kernel records its error word and returns, and the call reports
+   FMG_ERR_CUDA with the message of a timed-out wait (fmg_last_error); the
+   context stays usable. */
+int fmg_wait_selftest(fmg_ctx* ctx, int arrive, int max_polls, long long max_ns);
+
 /* ------------------------------------------------- allocation-free variant */
 /* No counterpart in the reference.  The dot product of fmg_dot for callers
    that cannot allocate device memory: hosts whose device memory is already
@@ -376,8 +412,9 @@ int fmg_learned_status(const fmg_grid* grid, int* active, double* rho_plain, dou
    reduction scratch is a fixed ~256 KB array inside the library, held by every
    GPU that loads it until exit.  n <= FMG_NOALLOC_MAX_N, else FMG_ERR_ARG.
    The first call on a device looks up the scratch address and should come
-   before any stream capture.  All calls share the scratch: calls that overlap
-   on the GPU race. */
+   before any stream capture.  Each call makes the context's device current
+   while it runs and restores the caller's current device before returning.
+   All calls share the scratch: calls that overlap on the GPU race. */
 #define FMG_NOALLOC_MAX_N 134217728L
 int fmg_dot_noalloc(fmg_ctx* ctx, const double* x, const double* y, long n, double* out);
 

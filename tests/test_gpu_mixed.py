@@ -48,7 +48,7 @@ def test_mixed_reaches_tolerance_and_matches_fp64(G, ctx, matrix_free):
     assert hist[-1] / hist[0] < 1e-10          # true FP64 residual reduction
     a, b = xm.get(), x64.get()
     rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-    assert rel < 1e-8, rel
+    assert rel <= 1e-10, rel                     # the north star's bound on the mixed result
     assert 1 <= nouter <= 3
     assert ninner <= 30
 

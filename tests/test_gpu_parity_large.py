@@ -1,0 +1,77 @@
+"""The plain FP64 path against the oracle on the benchmark's recipe at sizes
+the small parity cases do not reach: 3D Q1, log k a seeded 64-mode Fourier
+field, CG + V(1,1) Jacobi(0.6) to 1e-10, base level 2, at 65^3 and 129^3
+nodes (up to 2.1M unknowns, 56M stored matrix entries).  Every assembled level,
+the rhs, the complete :defnorm history and the solution are compared bitwise
+and against the 1e-12 bar (krylow.lisp:72-132, multigrid.lisp:254-288); the
+mixed-precision solve of the same problem must end within 1e-10 of the
+oracle's solution (relative, l2)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def G():
+    import gnu_femlisp_b200 as G
+    return G
+
+
+@pytest.fixture(scope="module")
+def ctx(G):
+    return G.Context(0)
+
+
+def _pair(O, G, ctx, level):
+    from gnu_femlisp_b200 import problems
+    wl = problems.c3(seed=0, level=level)
+    o = O.Oracle(3, 1, level, base_level=wl.base_level)
+    o.set_coefficient(O.K_CELL, wl.kcell)
+    o.assemble()
+    g = G.Grid(ctx, 3, 1, level, base_level=wl.base_level)
+    g.set_coefficient(G._capi.FMG_K_CELL, wl.kcell)
+    g.assemble()
+    return wl, o, g
+
+
+def _cfg(G, rtol=1e-10):
+    C = G._capi
+    return G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, rtol, 0.0, 200,
+                      C.FMG_MULTIPLICATIVE)
+
+
+@pytest.mark.parametrize("level", [6, 7])
+def test_benchmark_recipe_plain_path_bitwise(oracle_mod, G, ctx, level):
+    O = oracle_mod
+    wl, o, g = _pair(O, G, ctx, level)
+    x = g.vector()
+    hist, steps, st = g.solve(_cfg(G), x)
+    ref = o.solve(O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=1e-10, maxsteps=200))
+    assert st == 0 and ref.status == 0 and steps == ref.steps
+    rel_h = np.max(np.abs(hist - ref.history) / ref.history)
+    xs = x.get()
+    rel_x = np.max(np.abs(xs - ref.x)) / np.max(np.abs(ref.x))
+    assert rel_h <= REL and rel_x <= REL, (rel_h, rel_x)
+    assert np.array_equal(hist, ref.history) and np.array_equal(xs, ref.x)
+    for lev in range(wl.base_level, level + 1):
+        a, b = g.matrix(lev), o.matrix(lev)
+        assert np.array_equal(a, b), f"level {lev}: max diff {np.max(np.abs(a - b)):.3e}"
+    assert np.array_equal(g.rhs(), o.rhs())
+
+
+def test_benchmark_recipe_mixed_error_vs_oracle(oracle_mod, G, ctx):
+    # the mixed-precision solve (FP32/BF16 cycle in FP64 flexible CG) to 1e-10
+    # against the oracle's FP64 solution driven to 1e-13: within 1e-10
+    O = oracle_mod
+    wl, o, g = _pair(O, G, ctx, 6)
+    ref = o.solve(O.solve_cfg(method=O.METHOD_CG_MG, damp=0.6, compat=False, rtol=1e-13, maxsteps=200))
+    assert ref.status == 0
+    for mf in (True, False):
+        xm = g.vector()
+        hist, nouter, ninner, st = g.solve_mixed(_cfg(G), xm, matrix_free=mf)
+        assert st == 0 and hist[-1] / hist[0] < 1e-10
+        err = np.linalg.norm(xm.get() - ref.x) / np.linalg.norm(ref.x)
+        assert err <= 1e-10, (mf, err)

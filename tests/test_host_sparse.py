@@ -40,3 +40,19 @@ def test_slots_to_csr_matches_the_oracle_matvec(oracle_mod, dim, order, level, n
     y = _apply(start, index, values, x)
     ref = o.matvec(x)
     assert np.max(np.abs(y - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("start,index,values,msg", [
+    ([0, 2, 5], [0, 1, 0, 1], [1.0, 2.0, 3.0, 4.0, 5.0], "index holds 4"),
+    ([0, 2, 5], [0, 1, 0, 1, 2], [1.0, 2.0], "values hold 2"),
+    ([0, 3, 2], [0, 1, 2], [1.0, 2.0, 3.0], "nondecreasing"),
+    ([1, 2, 3], [0, 1, 2], [1.0, 2.0, 3.0], "begin at 0"),
+])
+def test_compressed_arrays_are_checked_before_the_c_call(start, index, values, msg):
+    # a short index or value array would make the library read past the end
+    # of host memory: the host wrapper refuses it before any C call
+    from gnu_femlisp_b200.core import _compressed
+    with pytest.raises(ValueError, match=msg):
+        _compressed(start, index, values)
+    st, ix, va = _compressed([0, 1, 3], [0, 0, 1], [2.0, -1.0, 2.0])
+    assert st.dtype == np.int32 and ix.dtype == np.int32 and va.dtype == np.float64
