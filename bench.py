@@ -35,6 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "time to 1e-10 rel. residual + MDoF/s per V-cycle: mixed/learned vs FP64 GMG"
 WEIGHTS = os.path.join(ROOT, "gnu_femlisp_b200", "weights", "damping3d.fmgnet")
 HBM_FALLBACK_GBS = 6650.0
+JUDGE_STEPS = 2  # CG steps after each (re)start on which the plain cycle judges the learned one
 # DRAM bytes per top-level node of one launch (read + write), from the ncu
 # capture of the 257^3 case (profiles/k_mf4_q1_3d_mixed_257cube.md): mode 2
 # 628.9 MB, FP64 mode 0 322.3 MB, mode 1 257.6 MB over 16,974,593 nodes
@@ -364,16 +365,15 @@ def run_mine(args, world, rank, local):
     cfg = plain_cfg(G)
     net = None if args.no_learned else DampingNet.load(ctx, WEIGHTS)
     x, xm = g.vector(), g.vector()
-    judge = {}
 
     def clear_damping():
         for lev in range(g.base + 1, g.top + 1):
             g.set_node_damping(lev, None)
 
     def install_learned():
+        # the damping network on every level; the plain cycle judges it inside
+        # the solve (JUDGE_STEPS shadowed CG steps after each (re)start)
         net.apply(g)
-        ok, rp, rl = g.learned_judge_mixed(cfg)
-        judge.update(accepted=ok, rho_plain=rp, rho_learned=rl, probe="6 mixed flexible-CG steps")
 
     def setup():
         g.set_coefficient(C.FMG_K_CELL, k_np)
@@ -385,9 +385,11 @@ def run_mine(args, world, rank, local):
         x.fill(0.0)
         return g.solve(cfg, x)
 
+    judge_steps = JUDGE_STEPS if net is not None else 0
+
     def mixed_step():
         xm.fill(0.0)
-        return g.solve_mixed(cfg, xm, matrix_free=True)
+        return g.solve_mixed(cfg, xm, matrix_free=True, judge=judge_steps)
 
     def e2e_step():
         setup()
@@ -565,8 +567,14 @@ def run_mine(args, world, rank, local):
     }
     if net is not None:
         line["learned"] = {"weights": os.path.relpath(WEIGHTS, ROOT), "setup_s": t_setup,
-                           "judge": judge, "status": status_learned,
-                           "setup": "damping network on levels 3..8 (tcgen05 convolutions) + plain-cycle judge"}
+                           "judge": {"kind": "in-solve: the plain cycle shadows the learned one on the first "
+                                             f"{JUDGE_STEPS} CG steps after each (re)start, a step along each "
+                                             "direction scored by its energy decrease (z,r)^2/(z,Az)",
+                                     "accepted": status_learned["reverts"] == 0,
+                                     "energy_decrease_learned": status_learned["rho_learned"],
+                                     "energy_decrease_plain": status_learned["rho_plain"]},
+                           "status": status_learned,
+                           "setup": "damping network on levels 3..8 (tcgen05 convolutions); the judge runs in the solve"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, par = cpu_baseline(wl, g, hist, x_plain)
         line["cpu_baseline"] = cpu

@@ -63,6 +63,7 @@ class MixedCfg(ctypes.Structure):
         ("max_inner", ctypes.c_int),
         ("max_outer", ctypes.c_int),
         ("matrix_free", ctypes.c_int),
+        ("judge", ctypes.c_int),
     ]
 
 

@@ -291,12 +291,14 @@ class Grid:
         return dn.value
 
     def solve_mixed(self, cfg: C.SolveCfg, x: "Vector", inner_rtol: float = 1e-5, max_inner: int = 200,
-                    max_outer: int = 20, matrix_free: bool = True):
+                    max_outer: int = 20, matrix_free: bool = True, judge: int = 0):
         """FP64 flexible CG preconditioned by the FP32/BF16 V-cycle; returns
         (defnorm history: true FP64 residuals at the start and at every
         restart, recursive residuals in between; restarts; CG iterations;
-        status)."""
-        mc = C.MixedCfg(inner_rtol, max_inner, max_outer, 1 if matrix_free else 0)
+        status).  judge > 0: installed node damping is judged against the
+        plain cycle on that many CG steps after each (re)start, inside the
+        solve (reverted when the plain cycle does better)."""
+        mc = C.MixedCfg(inner_rtol, max_inner, max_outer, 1 if matrix_free else 0, int(judge))
         hist = np.zeros(cfg.maxsteps + max_outer + 4)
         no, ni, st = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
         self.ctx.check(self._lib.fmg_solve_mixed(self.h, ctypes.byref(cfg), ctypes.byref(mc), x.h, C.dptr(hist),
@@ -322,7 +324,7 @@ class Grid:
         """``fmg_learned_judge_mixed``: the judge's CG probe run with the
         mixed-precision cycle of ``solve_mixed``; returns (accepted,
         rho_plain, rho_learned)."""
-        mc = C.MixedCfg(0.0, 0, 1, 1 if matrix_free else 0)
+        mc = C.MixedCfg(0.0, 0, 1, 1 if matrix_free else 0, 0)
         rp, rl, ok = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         self.ctx.check(self._lib.fmg_learned_judge_mixed(self.h, ctypes.byref(cfg), ctypes.byref(mc), ctypes.byref(rp),
                                                          ctypes.byref(rl), ctypes.byref(ok)), "learned_judge_mixed")

@@ -142,6 +142,7 @@ struct MixedState {
   std::vector<__nv_bfloat16*> bc, rc;  // coarse rhs and residual (BF16)
   float* k32 = nullptr;             // top-level cell coefficients (FP32)
   float *rtop = nullptr, *r = nullptr, *q = nullptr, *qs = nullptr;  // FP32 top-level vectors
+  float *zp = nullptr, *zs = nullptr;  // the in-solve judge: the plain cycle's result and its spare
   float* p32 = nullptr;             // FP32 search direction of the flexible CG
   float* wd = nullptr;              // top level: damping / diagonal per node (matrix-free smoothing)
   const float* wd_om = nullptr;     // the node damping and scalar damping wd was formed with
@@ -1732,7 +1733,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     const Lvl& T = g->lev[g->top];
     long long ncell = 1;
     for (int k = 0; k < g->dim; ++k) ncell *= T.n;
-    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32, &X.wd};
+    float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32, &X.wd, &X.zp, &X.zs};
     for (float** v : tv)
       if ((rc = mx_alloc_f(g, v, T.Np))) return rc;
     if ((rc = mx_alloc_f(g, &X.k32, ncell))) return rc;
@@ -2156,6 +2157,11 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   *ninner = 0;
   const int max_restart = mcfg->max_outer > 0 ? mcfg->max_outer : 20;
   bool judge_active = g->learned, revert_restart = false;
+  // the in-solve judge: some level carries node damping and judged steps are asked for
+  bool shadow = false;
+  if (mcfg->judge > 0)
+    for (const auto& V : X.lv) shadow = shadow || V.om != nullptr;
+  if (shadow && !g->w) return set_err(c, FMG_ERR_STATE, "solve_mixed: work vectors missing");
   double initial = -1.0;
   int step = 0, iters = 0;  // history slots, CG iterations
   for (int restart = 0; restart <= max_restart; ++restart) {
@@ -2202,6 +2208,40 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     };
     while (iters <= cfg->maxsteps) {
       if (iters == it0) {
+        mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
+        mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
+        if ((rc = launched(c, "mixed step"))) return rc;
+        if ((rc = mx_read(g))) return rc;
+      } else if (shadow && iters - it0 <= mcfg->judge) {
+        // a judged step: the learned cycle (the step's own, with its FCG dots)
+        // and the plain cycle on the same residual, each direction scored by
+        // the energy decrease (z, r)^2 / (z, A z) of a step along it
+        const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
+        mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
+        mx_dot2_64(r, X.q, nullptr, n, red2(X, EPI2_STORE, M_ZRL, M_TMP), st);
+        mg.matvec64(X.q, g->w, red2(X, EPI2_STORE, M_ZAL, M_TMP));
+        std::vector<const float*> om(X.lv.size());
+        for (size_t l = 0; l < X.lv.size(); ++l) { om[l] = X.lv[l].om; X.lv[l].om = nullptr; }
+        mg.vcycle(g->top, X.r, &X.zp, &X.zs, nullptr, nullptr, nullptr);
+        for (size_t l = 0; l < X.lv.size(); ++l) X.lv[l].om = om[l];
+        mx_dot2_64(r, X.zp, nullptr, n, red2(X, EPI2_STORE, M_ZRP, M_TMP), st);
+        mg.matvec64(X.zp, g->w, red2(X, EPI2_STORE, M_ZAP, M_TMP));
+        if ((rc = launched(c, "judged step"))) return rc;
+        if ((rc = mx_read(g))) return rc;
+        const double el = X.host[M_ZRL] * X.host[M_ZRL] / X.host[M_ZAL];
+        const double ep = X.host[M_ZRP] * X.host[M_ZRP] / X.host[M_ZAP];
+        g->rho_learned = el;
+        g->rho_plain = ep;
+        if (!(el >= ep)) {  // the plain cycle does better (or the learned figure is not finite)
+          for (auto& V : X.lv) V.om = nullptr;
+          mg.prepare_wd();
+          judge_active = false;
+          shadow = false;
+          g->reverts += 1;
+          revert_restart = true;
+          break;
+        }
+        mx_fcg64_p(X.sc, p, X.q, n, false, st);
         mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
         mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
         if ((rc = launched(c, "mixed step"))) return rc;

@@ -283,12 +283,22 @@ int fmg_cg_step(fmg_grid* grid, fmg_vec* x, fmg_vec* r, double* defnorm);
    coefficient applies its top-level operator (FP64 and FP32) from the cell
    coefficients instead of the stored matrix.  hist receives the true residual
    at the start and at every restart check and the recursive residual after
-   each CG iteration; *nouter counts restart checks, *ninner CG iterations. */
+   each CG iteration; *nouter counts restart checks, *ninner CG iterations.
+   With judge > 0 and per-node damping installed (fmg_net_apply or
+   fmg_set_node_damping), the plain cycle (scalar :damp) judges the learned
+   one inside the solve: on each of the first `judge` CG steps after every
+   (re)start both cycles are applied to the same residual r, and each
+   direction z is scored by the energy decrease (z, r)^2 / (z, A z) a step
+   along it gives; if the plain cycle's is larger the node damping is dropped
+   for the rest of the solve, which restarts from the true residual with the
+   plain cycle (fmg_learned_status counts the revert and reports the last
+   judged step's two figures). */
 typedef struct {
   double inner_rtol;   /* reserved, 0 */
   int max_inner;       /* reserved, 0 */
   int max_outer;       /* restart checks allowed (default 20) */
   int matrix_free;     /* 1: matrix-free top level where available */
+  int judge;           /* CG steps after each (re)start judged against the plain cycle (0: none) */
 } fmg_mixed_cfg;
 
 int fmg_solve_mixed(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* x,

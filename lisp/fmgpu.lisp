@@ -219,9 +219,10 @@ non-zero status is an error carrying the library's message."
            `(32 :double ,coarse-damp) `(40 :double ,rtol) `(48 :double ,atol)
            `(56 :int ,maxsteps) `(60 :int ,combination) `(64 :int ,fmg)))
 
-(defun %mixed-cfg-bytes (&key (max-outer 20) (matrix-free t))
+(defun %mixed-cfg-bytes (&key (max-outer 20) (matrix-free t) (judge 0))
   "fmg_mixed_cfg (24 bytes on x86-64)."
-  (%struct 24 '(0 :double 0d0) '(8 :int 0) `(12 :int ,max-outer) `(16 :int ,(if matrix-free 1 0))))
+  (%struct 24 '(0 :double 0d0) '(8 :int 0) `(12 :int ,max-outer) `(16 :int ,(if matrix-free 1 0))
+           `(20 :int ,judge)))
 
 ;;;; the key <-> index numbering of a level
 

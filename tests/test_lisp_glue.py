@@ -189,17 +189,33 @@ def test_drop_in_classes_have_their_methods():
     assert ("fl.iteration:solve", "<gpu-linear-solver>") in methods
 
 
+def _struct_offsets(forms, defun_name):
+    """Byte offsets of the fields of the (%struct size ...) form in the defun."""
+    def find(form):
+        if isinstance(form, list):
+            if form and form[0] == "%struct":
+                return form
+            for x in form:
+                got = find(x)
+                if got is not None:
+                    return got
+        return None
+    for f in forms:
+        if isinstance(f, list) and len(f) > 1 and f[0] == "defun" and f[1] == defun_name:
+            st = find(f)
+            return int(st[1]), [int(fl[0]) for fl in st[2:] if isinstance(fl, list)]
+    raise AssertionError(defun_name)
+
+
 def test_config_struct_offsets_match_the_header():
     # fmg_solve_cfg / fmg_mixed_cfg as the binding lays them out (x86-64)
     import ctypes
 
     from gnu_femlisp_b200 import _capi as C
-    text = open(LISP).read()
-    m = re.search(r"\(%struct 72 (.*?)\)\)\n", text, re.S)
-    offs = [int(o) for o in re.findall(r"`\((\d+) :(?:int|double)", m.group(1))]
-    fields = [getattr(C.SolveCfg, f).offset for f, _ in C.SolveCfg._fields_]
-    assert offs == fields and ctypes.sizeof(C.SolveCfg) == 72
-    m = re.search(r"\(%struct 24 (.*?)\)\)\n", text, re.S)
-    offs = [int(o) for o in re.findall(r"\((\d+) :(?:int|double)", m.group(1))]
+    forms = _forms()
+    size, offs = _struct_offsets(forms, "%cfg-bytes")
+    assert size == ctypes.sizeof(C.SolveCfg) == 72
+    assert offs == [getattr(C.SolveCfg, f).offset for f, _ in C.SolveCfg._fields_]
+    size, offs = _struct_offsets(forms, "%mixed-cfg-bytes")
+    assert size == ctypes.sizeof(C.MixedCfg) == 24
     assert offs == [getattr(C.MixedCfg, f).offset for f, _ in C.MixedCfg._fields_]
-    assert ctypes.sizeof(C.MixedCfg) == 24
