@@ -2216,19 +2216,21 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
         // a judged step: the learned cycle (the step's own, with its FCG dots)
         // and the plain cycle on the same residual, each direction scored by
         // the energy decrease (z, r)^2 / (z, A z) of a step along it
+        // (z, r) of each comes from its cycle's fused reduction: the learned
+        // one's as rho = (z, r) / s (s the residual's scale), the plain one's raw
         const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
         mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
-        mx_dot2_64(r, X.q, nullptr, n, red2(X, EPI2_STORE, M_ZRL, M_TMP), st);
         mg.matvec64(X.q, g->w, red2(X, EPI2_STORE, M_ZAL, M_TMP));
         std::vector<const float*> om(X.lv.size());
         for (size_t l = 0; l < X.lv.size(); ++l) { om[l] = X.lv[l].om; X.lv[l].om = nullptr; }
-        mg.vcycle(g->top, X.r, &X.zp, &X.zs, nullptr, nullptr, nullptr);
+        const Reduce2 Rp = red2(X, EPI2_STORE, M_ZRP, M_TMP);
+        mg.vcycle(g->top, X.r, &X.zp, &X.zs, r, nullptr, &Rp);
         for (size_t l = 0; l < X.lv.size(); ++l) X.lv[l].om = om[l];
-        mx_dot2_64(r, X.zp, nullptr, n, red2(X, EPI2_STORE, M_ZRP, M_TMP), st);
         mg.matvec64(X.zp, g->w, red2(X, EPI2_STORE, M_ZAP, M_TMP));
         if ((rc = launched(c, "judged step"))) return rc;
         if ((rc = mx_read(g))) return rc;
-        const double el = X.host[M_ZRL] * X.host[M_ZRL] / X.host[M_ZAL];
+        const double zrl = X.host[M_ALPHA] * X.host[M_SUSED];
+        const double el = zrl * zrl / X.host[M_ZAL];
         const double ep = X.host[M_ZRP] * X.host[M_ZRP] / X.host[M_ZAP];
         g->rho_learned = el;
         g->rho_plain = ep;

@@ -9,7 +9,7 @@ namespace fmg {
 
 // scalar slots of the mixed solve (FP64)
 enum MScal { M_ALPHA = 0, M_PA, M_LAM, M_BETA, M_QA, M_RR, M_SCALE, M_SUSED, M_TMP, M_SINV,
-             M_ZRL, M_ZAL, M_ZRP, M_ZAP,  // the in-solve judge: (z, r) and (z, A z) of the learned / plain cycle
+             M_ZAL, M_ZRP, M_ZAP,  // the in-solve judge: (z, A z) of the learned cycle, (z, r) and (z, A z) of the plain one
              M_COUNT = 16 };
 enum Epi2 { EPI2_STORE = 0, EPI2_LAMBDA = 1, EPI2_FCG = 2, EPI2_RHO = 3, EPI2_UPDATE = 4 };
 
