@@ -185,7 +185,8 @@ class Grid:
 
     def assemble(self, galerkin: bool = False) -> "Grid":
         """``fmg_assemble_levels``: coarse levels re-discretised, or Galerkin
-        products I^T A I of the level above (``galerkin=True``, Q1)."""
+        products I^T A I of the level above (``galerkin=True``; every
+        structured form: Q1, Q2, 3 x 3 node blocks)."""
         mode = C.FMG_ASSEMBLE_GALERKIN if galerkin else C.FMG_ASSEMBLE_REDISCRETIZE
         self.ctx.check(self._lib.fmg_assemble_levels(self.h, mode), "assemble")
         self.assembled = True

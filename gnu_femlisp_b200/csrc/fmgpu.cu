@@ -957,8 +957,6 @@ int fmg_assemble_levels(fmg_grid* g, int mode) {
   fmg_ctx* c = g->ctx;
   if (mode != FMG_ASSEMBLE_REDISCRETIZE && mode != FMG_ASSEMBLE_GALERKIN)
     return set_err(c, FMG_ERR_ARG, "unknown assembly mode %d", mode);
-  if (mode == FMG_ASSEMBLE_GALERKIN && (g->order != 1 || g->nc != 1))
-    return set_err(c, FMG_ERR_UNSUPPORTED, "Galerkin coarse operators: scalar Q1 grids");
   cudaStream_t st = c->stream;
   int rc;
   FMG_CK(c, cudaSetDevice(c->device));

@@ -1913,78 +1913,115 @@ __global__ void k_expand_q2_f32(const double* __restrict__ A, long long N, long 
   out[(long long)s * Np + i] = ok ? (float)A[(long long)s * Np + q2c_pos<D>(lay, c, M, r)] : 0.f;
 }
 
-// Galerkin coarse operator A_C = I^T A_F I of a scalar Q1 level (constrained
-// interpolation: fine Dirichlet rows and coarse Dirichlet columns removed;
-// identity rows at coarse Dirichlet nodes), one coarse row per thread: fine i
-// over the restriction stencil of I (z, y, x), fine slots ascending, coarse J
-// over the interpolation stencil of j (z, y, x), acc[J - I] = fma(w_iI a_ij,
-// w_jJ, acc[J - I]) -- the oracle's order
-template <int D>
+// Galerkin coarse operator A_C = I^T A_F I of a structured level -- scalar
+// Q1/Q2 and 3 x 3 node blocks -- with the constrained interpolation (fine
+// Dirichlet rows and coarse Dirichlet columns removed; identity blocks at
+// coarse Dirichlet nodes).  One thread per (coarse slot S, coarse row I): it
+// walks the oracle's order -- fine i over the restriction stencil of I
+// (z, y, x), fine slots ascending, the coarse J = I + off_S looked up in j's
+// interpolation stencil -- and keeps the terms that land on S, so each entry
+// sums the oracle's terms in the oracle's order:
+// acc[k][m] = fma(w_iI * a_ij[k][m], w_jJ, acc[k][m]).  Fine entries a level
+// does not store (Q2: an odd-coordinate node's +-2 slots) are structural
+// zeros and are skipped.
+template <int D, int P>
+__device__ __forceinline__ long long gal_pos(const Q2Layout& lay, const long long c[3], long long M, int s, int nc) {
+  if (P == 1) return c[0] + M * (c[1] + M * c[2]);
+  const int r = q2_pattern<D>(s);
+  for (int k = 0; k < D; ++k)
+    if (((r >> k) & 1) && (c[k] & 1)) return -1;
+  if (nc == 1) return q2c_pos<D>(lay, c, M, r);  // scalar Q2: colour-major
+  const long long H = (M + 1) / 2;              // node blocks: lexicographic, halved where restricted
+  long long id = 0, mul = 1;
+  for (int k = 0; k < D; ++k) {
+    const bool rk = (r >> k) & 1;
+    id += (rk ? c[k] / 2 : c[k]) * mul;
+    mul *= rk ? H : M;
+  }
+  return id;
+}
+
+template <int D, int P, int NC>
 __global__ void __launch_bounds__(kBlock)
-k_galerkin_q1(const double* __restrict__ AF, long long NF, long long NpF, int MF, double* __restrict__ AC,
-              long long NC, long long NpC, int MC, int dmask) {
-  constexpr int NS = St<D, 1>::NS;
-  constexpr int C = St<D, 1>::CENTER;
-  const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= NC) return;
+k_galerkin(const double* __restrict__ AF, long long NpF, int MF, double* __restrict__ AC, long long NCN,
+           long long NpC, int MC, int dmask, Q2Layout layF, Q2Layout layC) {
+  constexpr int W = 2 * P + 1;
+  constexpr int NS = D == 1 ? W : (D == 2 ? W * W : W * W * W);
+  constexpr int CEN = (NS - 1) / 2;
+  constexpr int NE = NC * NC;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)NS * NCN) return;
+  const int S = (int)(t / NCN);
+  const long long I = t - (long long)S * NCN;
   long long cI[3];
   node_coords(I, MC, D, cI);
+  const long long pI = gal_pos<D, P>(layC, cI, MC, S, NC);
+  if (pI < 0) return;  // an entry the coarse level does not store
+  double acc[NE];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) acc[e] = 0.0;
   if (node_dirichlet(cI, MC, D, dmask)) {
-    for (int s = 0; s < NS; ++s) AC[(long long)s * NpC + I] = (s == C) ? 1.0 : 0.0;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) AC[((long long)S * NE + e) * NpC + pI] = (S == CEN && e % (NC + 1) == 0) ? 1.0 : 0.0;
     return;
   }
-  double acc[NS];
+  const int oS[3] = {S % W - P, D > 1 ? (S / W) % W - P : 0, D > 2 ? S / (W * W) - P : 0};
+  long long cJ[3] = {0, 0, 0};
+  bool okJ = true;
+  for (int k = 0; k < D; ++k) {
+    cJ[k] = cI[k] + oS[k];
+    okJ = okJ && cJ[k] >= 0 && cJ[k] < MC;
+  }
+  if (okJ && !node_dirichlet(cJ, MC, D, dmask)) {
+    long long off[3][5] = {{0}, {0}, {0}};
+    double w[3][5] = {{1.0}, {1.0}, {1.0}};
+    int cnt[3] = {1, 1, 1};
+    for (int k = 0; k < D; ++k) cnt[k] = restrict_1d<P>(cI[k], off[k], w[k]);
+    for (int z = 0; z < cnt[2]; ++z)
+      for (int y = 0; y < cnt[1]; ++y)
+        for (int x = 0; x < cnt[0]; ++x) {
+          const long long fi[3] = {2 * cI[0] + off[0][x], D > 1 ? 2 * cI[1] + off[1][y] : 0,
+                                   D > 2 ? 2 * cI[2] + off[2][z] : 0};
+          bool skip = false;
+          for (int k = 0; k < D; ++k) skip = skip || fi[k] < 0 || fi[k] >= MF || face_dir((int)fi[k], MF, k, dmask);
+          if (skip) continue;
+          double wi = w[0][x];
+          if (D > 1) wi = wi * w[1][y];
+          if (D > 2) wi = wi * w[2][z];
+          for (int oz = (D > 2 ? -P : 0); oz <= (D > 2 ? P : 0); ++oz)
+            for (int oy = (D > 1 ? -P : 0); oy <= (D > 1 ? P : 0); ++oy)
+              for (int ox = -P; ox <= P; ++ox) {
+                const int o[3] = {ox, oy, oz};
+                long long fj[3] = {0, 0, 0};
+                double wj[3] = {1.0, 1.0, 1.0};
+                bool hit = true;
+                for (int k = 0; k < D && hit; ++k) {
+                  fj[k] = fi[k] + o[k];
+                  if (fj[k] < 0 || fj[k] >= MF || face_dir((int)fj[k], MF, k, dmask)) { hit = false; break; }
+                  long long Jk[3];
+                  double wk[3];
+                  const int nk = prolong_1d<P>(fj[k], Jk, wk);
+                  bool found = false;
+                  for (int q = 0; q < nk; ++q)
+                    if (Jk[q] == cJ[k]) { wj[k] = wk[q]; found = true; }
+                  hit = found;
+                }
+                if (!hit) continue;
+                const int sf = (ox + P) + W * ((D > 1 ? oy : 0) + (D > 1 ? P : 0)) +
+                               W * W * ((D > 2 ? oz : 0) + (D > 2 ? P : 0));
+                const long long pF = gal_pos<D, P>(layF, fi, MF, sf, NC);
+                if (pF < 0) continue;  // a structural zero
+                double ww = wj[0];
+                if (D > 1) ww = ww * wj[1];
+                if (D > 2) ww = ww * wj[2];
 #pragma unroll
-  for (int s = 0; s < NS; ++s) acc[s] = 0.0;
-  long long off[3][5] = {{0}, {0}, {0}};
-  double w[3][5] = {{1.0}, {1.0}, {1.0}};
-  int cnt[3] = {1, 1, 1};
-  for (int k = 0; k < D; ++k) cnt[k] = restrict_1d<1>(cI[k], off[k], w[k]);
-  for (int z = 0; z < cnt[2]; ++z)
-    for (int y = 0; y < cnt[1]; ++y)
-      for (int x = 0; x < cnt[0]; ++x) {
-        const long long fi[3] = {2 * cI[0] + off[0][x], 2 * cI[1] + off[1][y], 2 * cI[2] + off[2][z]};
-        bool skip = false;
-        for (int k = 0; k < D; ++k) skip = skip || fi[k] < 0 || fi[k] >= MF || face_dir((int)fi[k], MF, k, dmask);
-        if (skip) continue;
-        double wi = w[0][x];
-        if (D > 1) wi = wi * w[1][y];
-        if (D > 2) wi = wi * w[2][z];
-        const long long i = fi[0] + (long long)MF * (fi[1] + (long long)MF * fi[2]);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          const long long o[3] = {s % 3 - 1, D > 1 ? (s / 3) % 3 - 1 : 0, D > 2 ? s / 9 - 1 : 0};
-          const long long fj[3] = {fi[0] + o[0], fi[1] + o[1], fi[2] + o[2]};
-          bool sj = false;
-          for (int k = 0; k < D; ++k) sj = sj || fj[k] < 0 || fj[k] >= MF || face_dir((int)fj[k], MF, k, dmask);
-          if (sj) continue;
-          const double wa = wi * AF[(long long)s * NpF + i];
-          long long J[3][3] = {{0}, {0}, {0}};
-          double wj[3][3] = {{1.0}, {1.0}, {1.0}};
-          int cj[3] = {1, 1, 1};
-          for (int k = 0; k < D; ++k) cj[k] = prolong_1d<1>(fj[k], J[k], wj[k]);
-          for (int zz = 0; zz < cj[2]; ++zz)
-            for (int yy = 0; yy < cj[1]; ++yy)
-              for (int xx = 0; xx < cj[0]; ++xx) {
-                const long long cJ[3] = {J[0][xx], J[1][yy], J[2][zz]};
-                bool dj = false;
-                for (int k = 0; k < D; ++k) dj = dj || face_dir((int)cJ[k], MC, k, dmask);
-                if (dj) continue;
-                double ww = wj[0][xx];
-                if (D > 1) ww = ww * wj[1][yy];
-                if (D > 2) ww = ww * wj[2][zz];
-                int S = (int)(cJ[0] - cI[0] + 1);
-                if (D > 1) S += 3 * (int)(cJ[1] - cI[1] + 1);
-                if (D > 2) S += 9 * (int)(cJ[2] - cI[2] + 1);
-                // S is one of the level's slots (the terms couple nodes of one coarse cell)
-#pragma unroll
-                for (int t = 0; t < NS; ++t)
-                  if (t == S) acc[t] = fma(wa, ww, acc[t]);
+                for (int e = 0; e < NE; ++e)
+                  acc[e] = fma(wi * AF[((long long)sf * NE + e) * NpF + pF], ww, acc[e]);
               }
         }
-      }
+  }
 #pragma unroll
-  for (int s = 0; s < NS; ++s) AC[(long long)s * NpC + I] = acc[s];
+  for (int e = 0; e < NE; ++e) AC[((long long)S * NE + e) * NpC + pI] = acc[e];
 }
 
 // ---- diagonal-block operations of the recorded cycle (vector form)
@@ -2454,9 +2491,20 @@ void launch_level_to_f32(const LevelView& L, int nslots, float* out, cudaStream_
 
 void launch_galerkin(const LevelView& F, const LevelView& Cl, double* AC, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  Q1_DISPATCH(F.dim, {
-    k_galerkin_q1<D><<<grid1(Cl.N), kBlock, 0, st>>>(F.A, F.N, F.Np, (int)F.M, AC, Cl.N, Cl.Np, (int)Cl.M, F.dmask);
-  });
+  const Q2Layout lf = q2_layout(F.dim, F.M), lc = q2_layout(Cl.dim, Cl.M);
+  const int ns = F.order == 1 ? (F.dim == 1 ? 3 : F.dim == 2 ? 9 : 27) : (F.dim == 1 ? 5 : F.dim == 2 ? 25 : 125);
+  const unsigned g = grid1((long long)ns * Cl.N);
+  const int mf = (int)F.M, mc = (int)Cl.M;
+  if (F.nc == 3) {
+    if (F.order == 2) k_galerkin<3, 2, 3><<<g, kBlock, 0, st>>>(F.A, F.Np, mf, AC, Cl.N, Cl.Np, mc, F.dmask, lf, lc);
+    else k_galerkin<3, 1, 3><<<g, kBlock, 0, st>>>(F.A, F.Np, mf, AC, Cl.N, Cl.Np, mc, F.dmask, lf, lc);
+    return;
+  }
+  if (F.order == 2) {
+    Q1_DISPATCH(F.dim, { k_galerkin<D, 2, 1><<<g, kBlock, 0, st>>>(F.A, F.Np, mf, AC, Cl.N, Cl.Np, mc, F.dmask, lf, lc); });
+  } else {
+    Q1_DISPATCH(F.dim, { k_galerkin<D, 1, 1><<<g, kBlock, 0, st>>>(F.A, F.Np, mf, AC, Cl.N, Cl.Np, mc, F.dmask, lf, lc); });
+  }
 }
 
 void launch_bdiag3(const LevelView& L, int mode, const double* w, const double* x, double* y, cudaStream_t st) {

@@ -162,8 +162,10 @@ int fmg_assemble(fmg_grid* grid);
    (geomg.lisp:109-142): FMG_ASSEMBLE_REDISCRETIZE assembles every level
    (assemble-interior :refined); FMG_ASSEMBLE_GALERKIN assembles the top
    level and forms each coarser one as the Galerkin product I^T A_{l+1} I with
-   the constrained interpolation (:galerkin-p t, geomg.lisp:122-123; scalar Q1
-   grids). */
+   the constrained interpolation (:galerkin-p t, geomg.lisp:122-123; every
+   structured form: scalar Q1/Q2 and 3 x 3 node blocks, each entry summed in
+   a fixed order, so the levels are deterministic; FMG_ERR_UNSUPPORTED on an
+   algebraic grid). */
 #define FMG_ASSEMBLE_REDISCRETIZE 0
 #define FMG_ASSEMBLE_GALERKIN 1
 int fmg_assemble_levels(fmg_grid* grid, int mode);

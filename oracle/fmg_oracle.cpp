@@ -951,30 +951,34 @@ void prolongate(const Hier& H, int lc, const double* xc, double* xf, bool constr
 }
 
 // Galerkin coarse operator (multilevel-decomposition with :galerkin-p t,
-// geomg.lisp:109-142): A_l = I^T A_{l+1} I with the constrained
-// interpolation (constraints.lisp:58-72: rows of fine Dirichlet nodes and
-// columns of coarse Dirichlet nodes removed), identity rows at coarse
-// Dirichlet nodes.  For nested Lagrange spaces every nonzero term couples two
-// nodes of one coarse cell, so the product has the level's own stencil.
-// Order: fine i over the restriction stencil of I (z, y, x ascending), fine
-// slots ascending, coarse J over the interpolation stencil of j (z, y, x
-// ascending): acc[J - I] = fma(w_iI * a_ij, w_jJ, acc[J - I]).  Q1, nc = 1.
+// geomg.lisp:109-142; galerkin-product, amg.lisp:247-285): A_l = I^T A_{l+1} I
+// with the constrained interpolation (constraints.lisp:58-72: rows of fine
+// Dirichlet nodes and columns of coarse Dirichlet nodes removed), identity
+// blocks at coarse Dirichlet nodes.  For nested Lagrange spaces every nonzero
+// term couples two nodes of one coarse cell, so the product has the level's
+// own stencil (Q2: an odd-coordinate node's +-2 entries come out exactly
+// zero, and terms reaching beyond the stencil multiply structural zeros).  Order, as galerkin-product associates it ((R_kl A_lm) P_mn, block
+// products componentwise, the interpolation acting on each component):
+// per coarse row I, fine i over the restriction stencil of I (z, y, x
+// ascending), fine slots ascending, coarse J over the interpolation stencil of
+// j (z, y, x ascending), block entries (k, m) row-major:
+// acc[J - I][k][m] = fma(w_iI * a_ij[k][m], w_jJ, acc[J - I][k][m]).
 int galerkin_level(Hier& H, int l) {
-  if (H.order != 1 || H.nc != 1) return -2;
+  const int nc = H.nc;
   Level& C = H.lev[l];
   const Level& F = H.lev[l + 1];
-  C.A.assign((size_t)H.nslots * C.N, 0.0);
+  C.A.assign((size_t)H.nslots * nc * nc * C.N, 0.0);
   const int center = [&] { long z[3] = {0, 0, 0}; return slot_of(H, z); }();
-#pragma omp parallel for schedule(static)
+  auto at = [&](const Level& L, int s, int k, int m, long i) { return (((size_t)s * nc + k) * nc + m) * L.N + i; };
+#pragma omp parallel for schedule(dynamic, 16)
   for (long I = 0; I < C.N; ++I) {
     long cI[3];
     coords(H, C.M, I, cI);
     if (is_dirichlet(H, C.M, cI)) {
-      C.A[(size_t)center * C.N + I] = 1.0;
+      for (int k = 0; k < nc; ++k) C.A[at(C, center, k, k, I)] = 1.0;
       continue;
     }
-    double acc[27];
-    for (int s = 0; s < H.nslots; ++s) acc[s] = 0.0;
+    std::vector<double> acc((size_t)H.nslots * nc * nc, 0.0);
     long off[3][5] = {{0}, {0}, {0}};
     double w[3][5] = {{1.0}, {1.0}, {1.0}};
     int cnt[3] = {1, 1, 1};
@@ -997,7 +1001,8 @@ int galerkin_level(Hier& H, int l) {
             bool inj = true;
             for (int k = 0; k < H.dim; ++k) if (fj[k] < 0 || fj[k] >= F.M) inj = false;
             if (!inj || is_dirichlet(H, F.M, fj)) continue;
-            const double wa = wi * F.A[(size_t)s * F.N + i];
+            double wa[9];
+            for (int e = 0; e < nc * nc; ++e) wa[e] = wi * F.A[at(F, s, e / nc, e % nc, i)];
             long J[3][3] = {{0}, {0}, {0}};
             double wj[3][3] = {{1.0}, {1.0}, {1.0}};
             int cj[3] = {1, 1, 1};
@@ -1011,12 +1016,20 @@ int galerkin_level(Hier& H, int l) {
                   if (H.dim > 1) ww = ww * wj[1][yy];
                   if (H.dim > 2) ww = ww * wj[2][zz];
                   long d[3] = {cJ[0] - cI[0], cJ[1] - cI[1], cJ[2] - cI[2]};
+                  // a coarse node beyond the stencil: the term multiplies a
+                  // structural zero (Q2: an odd-coordinate fine node has no
+                  // +-2 coupling) and adds nothing
+                  bool far = false;
+                  for (int k = 0; k < H.dim; ++k) far = far || d[k] < -H.span || d[k] > H.span;
+                  if (far) continue;
                   const int S = slot_of(H, d);
-                  acc[S] = std::fma(wa, ww, acc[S]);
+                  for (int e = 0; e < nc * nc; ++e)
+                    acc[(size_t)S * nc * nc + e] = std::fma(wa[e], ww, acc[(size_t)S * nc * nc + e]);
                 }
           }
         }
-    for (int s = 0; s < H.nslots; ++s) C.A[(size_t)s * C.N + I] = acc[s];
+    for (int S = 0; S < H.nslots; ++S)
+      for (int e = 0; e < nc * nc; ++e) C.A[at(C, S, e / nc, e % nc, I)] = acc[(size_t)S * nc * nc + e];
   }
   return 0;
 }
