@@ -102,6 +102,7 @@ SIGNATURES = {
     "fmg_l2_norm": (ctypes.c_int, [_vp, _dp]),
     "fmg_matvec": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "fmg_residual": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
+    "fmg_matvec_mf": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
     "fmg_restrict": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "fmg_prolongate": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "fmg_jacobi": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp]),

@@ -248,6 +248,15 @@ class Grid:
     def residual(self, x: "Vector", b: "Vector", r: "Vector"):
         self.ctx.check(self._lib.fmg_residual(self.h, x.level, x.h, b.h, r.h), "residual")
 
+    def matvec_mf(self, x: "Vector", y: "Vector", b: "Vector" = None, fp32=False):
+        """y = A x (b None) or y = b - A x on the top level, matrix-free from
+        the cell coefficients as the mixed solve applies it: FP64 difference
+        form (fp32 False), FP32 with the result widened (True), or FP64 on x
+        rounded to FP32 (2: the mixed solve's CG operator; b must be None)."""
+        mode = 2 if fp32 == 2 else (1 if fp32 else 0)
+        self.ctx.check(self._lib.fmg_matvec_mf(self.h, mode, x.h, b.h if b is not None else None, y.h),
+                       "matvec_mf")
+
     def restrict(self, rf: "Vector", rc: "Vector"):
         self.ctx.check(self._lib.fmg_restrict(self.h, rf.level, rf.h, rc.h), "restrict")
 

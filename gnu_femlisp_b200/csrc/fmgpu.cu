@@ -598,6 +598,11 @@ int read_scalars(fmg_grid* g) {
   fmg_ctx* c = g->ctx;
   FMG_CK(c, cudaMemcpyAsync(c->host_scal, g->scal, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FMG_CK(c, cudaStreamSynchronize(c->stream));
+  if (c->host_scal[S_MFERR] != 0.0) {  // a matrix-free kernel gave up on a copy: its results are void
+    FMG_CK(c, cudaMemsetAsync(g->scal + S_MFERR, 0, sizeof(double), c->stream));
+    if (g->mx) FMG_CK(c, cudaMemsetAsync(g->mx->counter, 0, sizeof(unsigned), c->stream));
+    return set_err(c, FMG_ERR_CUDA, "a bounded wait of the matrix-free operator timed out (the kernel gave up)");
+  }
   return FMG_OK;
 }
 
@@ -1703,6 +1708,7 @@ MFArgs64 mf64_args(const fmg_grid* g, double damp) {
   MFArgs64 m;
   m.k = g->kcell_d; m.omega = nullptr; m.N = L.N; m.M = (int)L.M; m.n = (int)L.n; m.dmask = g->dmask;
   m.hs = L.h / 12.0; m.w = damp;
+  m.err = g->scal + S_MFERR;
   return m;
 }
 
@@ -1789,6 +1795,7 @@ struct MixedMG {
     a.w = (float)c.damp;
     const bool wd = X.wd_ok && X.wd_om == a.omega && X.wd_w == a.w;
     a.wd = wd ? X.wd : nullptr;
+    a.err = g->scal + S_MFERR;
     return a;
   }
   // damping / diagonal of the top level for the damping now in use (once per
@@ -2285,6 +2292,42 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
 // this grid left (FP32 cycle vectors, the FP32 search direction, the FP64
 // residual and a = A p), with the damping it formed the per-node
 // damping/diagonal for.  Nothing waits; the caller times the stream.
+extern "C" int fmg_matvec_mf(fmg_grid* g, int fp32, const fmg_vec* x, const fmg_vec* b, fmg_vec* y) {
+  if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
+  if (vec_check(x, g, g->top) || vec_check(y, g, g->top) || x == y || (b && (vec_check(b, g, g->top) || b == y)))
+    return FMG_ERR_ARG;
+  if (!mixed_top_mf(g, true) || g->algebraic)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
+                   "matvec_mf: 3D scalar Q1 grids with cell-wise coefficients (no uploaded matrices)");
+  if (fp32 < 0 || fp32 > 2 || (fp32 == 2 && b)) return FMG_ERR_ARG;
+  cudaStream_t st = g->ctx->stream;
+  if (fp32 == 0) {
+    const MFArgs64 a = mf64_args(g, 0.0);
+    if (b) mx_top_residual64(a, x->d, b->d, y->d, st);
+    else mx_top_apply64x(a, x->d, y->d, st);
+  } else if (fp32 == 2) {  // the CG operator of the mixed solve: FP64 A of an FP32 direction
+    int rc = mixed_prepare(g, true);
+    if (rc) return rc;
+    MixedState& X = *g->mx;
+    mx_f64_to_f32(x->d, X.q, g->lev[g->top].N, st);
+    mx_top_apply64(mf64_args(g, 0.0), X.q, y->d, X.q, nullptr, st);
+  } else {
+    int rc = mixed_prepare(g, true);
+    if (rc) return rc;
+    MixedState& X = *g->mx;
+    const long long n = g->lev[g->top].N;
+    fmg_solve_cfg c{};
+    c.damp = 1.0;
+    MixedMG mg{g, X, c, st};
+    mx_f64_to_f32(x->d, X.q, n, st);
+    if (b) mx_f64_to_f32(b->d, X.r, n, st);
+    mx_top_apply(b ? 1 : 0, mg.mf_args(), X.q, b ? X.r : nullptr, X.qs, nullptr, nullptr, nullptr, st);
+    mx_f32_to_f64(X.qs, y->d, n, st);
+  }
+  FMG_RC(launched(g->ctx, "matvec_mf"));
+  return read_scalars(g);  // reports a kernel that gave up waiting for a copy
+}
+
 extern "C" int fmg_mixed_top_kernel(fmg_grid* g, int kind, int reps) {
   if (!g) return FMG_ERR_ARG;
   if (!g->mx || !g->mx->mf || !g->mx->wd_ok || !g->r || !g->a)

@@ -34,7 +34,9 @@ extern std::atomic<long long> g_launches;
 
 // device scalar slots of a grid (CG scalars, reduction results)
 enum Scal {
-  S_ALPHA = 0, S_BETA, S_LAM, S_NEGLAM, S_NEWALPHA, S_RATIO, S_RR, S_DOT, S_TMP, S_COUNT = 16
+  S_ALPHA = 0, S_BETA, S_LAM, S_NEGLAM, S_NEWALPHA, S_RATIO, S_RR, S_DOT, S_TMP,
+  S_MFERR = 15,         // non-zero: a matrix-free operator kernel gave up waiting for a copy
+  S_COUNT = 16
 };
 
 // epilogue of a chunked reduction, run by the last block on the folded value

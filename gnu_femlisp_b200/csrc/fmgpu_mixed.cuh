@@ -30,6 +30,7 @@ struct MFArgsT {
   T hs;                // h / 12
   T w;                 // scalar damping
   const T* wd = nullptr;  // per-node damping / diagonal (mx_top_wd), or nullptr: formed in the kernel
+  double* err = nullptr;  // set to 1 by a CTA whose bounded wait for a copy ran out
 };
 typedef MFArgsT<float> MFArgs;
 typedef MFArgsT<double> MFArgs64;

@@ -11,9 +11,15 @@
 // reads 27 neighbour values (L1-resident) and 8 cell coefficients instead of
 // 27 stored matrix entries: about 12 B/row of HBM traffic instead of 116.
 // Coarse levels use the assembled matrices converted to FP32.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <type_traits>
+
 #include "fmgpu_mixed.cuh"
+#include "umma.cuh"
 
 namespace fmg {
 
@@ -88,56 +94,403 @@ __device__ __forceinline__ void dr_finish2(double v0, double v1, const Reduce2& 
 }
 
 // ------------------------------------------------- matrix-free top level
-// The reductions of the z-marching kernels run over a 3D grid of blocks.
-__device__ __forceinline__ void dr_finish2_grid(double v0, double v1, const Reduce2& R, double* smem) {
-  __shared__ bool is_last;
-  const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-  double s0 = dr_fold256(v0, smem);
-  double s1 = dr_fold256(v1, smem);
-  if (threadIdx.x + threadIdx.y == 0) {
-    R.part[2 * bid] = s0;
-    R.part[2 * bid + 1] = s1;
-    __threadfence();
-    unsigned done = atomicAdd(R.counter, 1u);
-    is_last = (done == nb - 1);
+// The Q1 row of a node from the coefficients k[cz][cy][cx] of its 8 cells
+// (index 0: the cell on the lower side of the node along that axis) and the
+// values X(dx, dy, dz) of its neighbours, zero where eliminated: the diagonal
+// d = 4 hs K (K the sum of the 8 cells) and ax = (A x)_i, evaluated as 4 K x_i
+// minus, over the 12 face diagonals, the sum of the two cells sharing each
+// times its value, minus, over the 8 body diagonals, the one cell times its
+// value (the Q1 stiffness has weight zero between axis neighbours).  FP64
+// (DIFF): the row as sum_j w_j (x_i - x_j) -- the weights sum to 4 K, and the
+// differences of a smooth iterate are small, so the true residual's rounding
+// is far below that of 4 K x_i - sum_j w_j x_j.
+template <typename T, bool HX, bool DIFF, typename XF>
+__device__ __forceinline__ void mf_row(const T (&k)[2][2][2], const XF& X, T hs, T& ax, T& d, T& xc) {
+  const T wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
+                      {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
+  const T ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
+  T sacc = T(0);
+  xc = T(0);
+  if (HX) {
+    xc = X(0, 0, 0);
+    auto term = [&](T w, T xj) { sacc = DIFF ? fma(w, xc - xj, sacc) : fma(w, xj, sacc); };
+#pragma unroll
+    for (int sy = 0; sy < 2; ++sy)
+#pragma unroll
+      for (int sx = 0; sx < 2; ++sx) term(wc[sy][sx], X(2 * sx - 1, 2 * sy - 1, 0));
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz) {
+      const int dz = 2 * cz - 1;
+#pragma unroll
+      for (int sx = 0; sx < 2; ++sx)  // face diagonals (sx, 0, sz): cells (sx, *, sz)
+        term(k[cz][0][sx] + k[cz][1][sx], X(2 * sx - 1, 0, dz));
+#pragma unroll
+      for (int sy = 0; sy < 2; ++sy)  // face diagonals (0, sy, sz): cells (*, sy, sz)
+        term(k[cz][sy][0] + k[cz][sy][1], X(0, 2 * sy - 1, dz));
+#pragma unroll
+      for (int sy = 0; sy < 2; ++sy)
+#pragma unroll
+        for (int sx = 0; sx < 2; ++sx)  // body diagonals
+          term(k[cz][sy][sx], X(2 * sx - 1, 2 * sy - 1, dz));
+    }
+    if (!DIFF) sacc = fma(T(4) * ksum, xc, -sacc);
   }
-  __syncthreads();
-  if (!is_last) return;
-  __threadfence();
-  const unsigned t = threadIdx.x + blockDim.x * threadIdx.y;
-  double a0 = 0.0, a1 = 0.0;
-  for (unsigned k = t; k < nb; k += kBlock) {
-    a0 = a0 + __ldcg(R.part + 2 * k);
-    a1 = a1 + __ldcg(R.part + 2 * k + 1);
+  d = T(4) * hs * ksum;
+  ax = hs * sacc;
+}
+
+// mode 0: A x; 1: b - A x; 2: x + w (b - A x)/d; 3: w b/d (w over d formed
+// beforehand when use_wd)
+template <int MODE, typename T>
+__device__ __forceinline__ T mf_out(T ax, T d, T xc, T bb, T o, bool use_wd) {
+  if (MODE == 0) return ax;
+  if (MODE == 1) return bb - ax;
+  if (MODE == 2) return use_wd ? fma(o, bb - ax, xc) : fma(o, (bb - ax) / d, xc);
+  return use_wd ? o * bb : o * (bb / d);
+}
+
+// The operator as one launch over two kinds of CTA.
+// Tiled CTAs own a 32 x 16 column of nodes (thread (lx, ly): the y-adjacent
+// nodes 2ly, 2ly+1) and march z through 32 planes.  Each plane reaches shared
+// memory by TMA: its 18 x rows (y0-1 .. y0+16, each one 1D box from the
+// 16-byte boundary at or below node x0-1; rows outside the grid or on a
+// Dirichlet face are fetched from a coordinate below the vector's start, so
+// the copy fills them with zeros) and its 17 x 33 cell tile (one 3D box,
+// cells outside the grid read as zero).  A 5-plane ring keeps three planes in
+// flight.  Once a plane has landed, the CTA packs its x rows (the alignment
+// offset removed, Dirichlet columns zeroed, FP32 values widened for the FP64
+// operator) into a 4-plane ring, the only copy the rows read.  One barrier per
+// plane orders packing, reuse of ring slots and the next copies.
+// The nodes outside the tiled box (the faces x, y or z = 2^L where the box
+// stops short of the grid; the whole grid when it is below 32 cells a side)
+// go to face CTAs that evaluate the same row from global memory, 1024 nodes
+// each.  Every CTA adds its nodes to the two FP64 reductions of R.
+constexpr int kFX = 32, kFY = 16, kFZ = 32;   // tile: nodes along x, y; planes per CTA
+constexpr int kFRows = kFY + 2;               // x rows of a plane (y0-1 .. y0+16)
+constexpr int kFCRows = kFY + 1;              // cell rows of a plane (y0-1 .. y0+15)
+constexpr int kFPW = kFX + 2;                 // packed row: x0-1 .. x0+32
+constexpr int kFRing = 5, kFPack = 4;         // staged planes, packed planes
+constexpr int kFThreads = 256;
+constexpr int kFaceNodes = 1024;              // nodes per face CTA
+constexpr int kZeroRow = -4096;               // row coordinate whose whole box lies below the vector
+
+template <typename T, typename TX>
+struct MftLayout {
+  static constexpr int XA = 16 / (int)sizeof(TX);           // row copies start on 16-byte boundaries
+  static constexpr int XW = sizeof(TX) == 4 ? 40 : 36;      // elements per row copy: 34 + the offset
+  static constexpr int XP = sizeof(TX) == 4 ? 256 : 384;    // bytes per staged row (128-byte aligned copies)
+  static constexpr int CW = sizeof(T) == 4 ? 36 : 34;       // cells per copied row, from cell x0-1-COFF
+  static constexpr int COFF = sizeof(T) == 4 ? 3 : 1;       // where cell x0-1 sits in a copied row
+  static constexpr int XB = kFRows * XP;                    // x rows of a staged plane
+  static constexpr int CB = (kFCRows * CW * (int)sizeof(T) + 127) / 128 * 128;
+  static constexpr int SB = XB + CB;                        // bytes per staged plane
+  static constexpr int PS = kFRows * kFPW;                  // elements per packed plane
+  static constexpr int SMEM = kFRing * SB + kFPack * PS * (int)sizeof(T) + kFRing * 8 + 128;
+  static constexpr uint32_t XTX = kFRows * XW * sizeof(TX), CTX = kFCRows * CW * sizeof(T);
+};
+
+struct MftGeo {
+  int nbx, nby, nbz, nmain;   // tiled box: nbx x nby x nbz tiles from the origin
+  int nface;                  // face CTAs (they come first in the grid)
+  long long X1, Y1, Z1;       // the tiled box's extents in nodes
+  int ax, ay, az;             // the tiled CTAs write [ax, X1) x [ay, Y1) x [az, Z1) (1: the face at 0 is left out)
+  long long F;                // nodes outside what the tiled CTAs write
+};
+
+// the u-th coordinate outside [a, b) along an axis of M nodes
+__device__ __forceinline__ int outside(long long u, long long a, long long b) { return (int)(u < a ? u : u + (b - a)); }
+
+// node (ix, iy, iz) of the f-th node the face CTAs own: the planes z outside
+// [az, Z1), then the rows y outside [ay, Y1) of the planes inside, then the
+// columns x outside [ax, X1) of the rows inside
+__device__ __forceinline__ void face_node(long long f, const MftGeo& q, int M, int& ix, int& iy, int& iz) {
+  const long long MM = (long long)M * M;
+  const long long nz = q.Z1 - q.az, ny = q.Y1 - q.ay, nx = q.X1 - q.ax;
+  const long long s1 = MM * (M - nz);
+  if (f < s1) {
+    iz = outside(f / MM, q.az, q.Z1);
+    const long long r = f % MM;
+    iy = (int)(r / M);
+    ix = (int)(r % M);
+    return;
   }
-  double t0 = dr_fold256(a0, smem);
-  double t1 = dr_fold256(a1, smem);
-  if (t == 0) {
-    epi2_apply(R, t0, t1);
-    *R.counter = 0u;
+  f -= s1;
+  const long long a2 = (long long)M * (M - ny), s2 = a2 * nz;
+  if (f < s2) {
+    iz = (int)(q.az + f / a2);
+    const long long r = f % a2;
+    iy = outside(r / M, q.ay, q.Y1);
+    ix = (int)(r % M);
+    return;
+  }
+  f -= s2;
+  const long long cx = M - nx, a3 = cx * ny;
+  iz = (int)(q.az + f / a3);
+  const long long r = f % a3;
+  iy = (int)(q.ay + r / cx);
+  ix = outside(r % cx, q.ax, q.X1);
+}
+
+template <typename T, typename TV, typename TX, int MODE, bool RED>
+__device__ __forceinline__ void mf_face_cta(const MFArgsT<T>& g, const MftGeo& geo, int fb, const TX* __restrict__ x,
+                                            const T* __restrict__ b, T* __restrict__ y, const TV* __restrict__ v,
+                                            const TV* __restrict__ v2, double& acc0, double& acc1) {
+  constexpr bool HX = MODE != 3;
+  constexpr bool HB = MODE != 0;
+  constexpr bool DIFF = sizeof(T) == 8;
+  constexpr bool HO = MODE == 2 || MODE == 3;
+  const int M = g.M, n = g.n, dm = g.dmask;
+  const long long MM = (long long)M * M;
+  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+  const bool uwd = g.wd != nullptr;
+  const long long f0 = (long long)fb * kFaceNodes;
+#pragma unroll 1
+  for (int q = 0; q < kFaceNodes / kFThreads; ++q) {
+    const long long f = f0 + threadIdx.x + (long long)q * kFThreads;
+    if (f >= geo.F) break;
+    int ix, iy, iz;
+    face_node(f, geo, M, ix, iy, iz);
+    const long long i = (long long)iz * MM + (long long)iy * M + ix;
+    T ax, d, xc;
+    if (dirf(ix, 1, 2) || dirf(iy, 4, 8) || dirf(iz, 16, 32)) {
+      xc = HX ? (T)x[i] : T(0);
+      ax = xc;
+      d = T(1);
+    } else {
+      T k[2][2][2];
+#pragma unroll
+      for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+          for (int cx = 0; cx < 2; ++cx) {
+            const int ex = ix - 1 + cx, ey = iy - 1 + cy, ez = iz - 1 + cz;
+            const bool in = ex >= 0 && ex < n && ey >= 0 && ey < n && ez >= 0 && ez < n;
+            k[cz][cy][cx] = in ? __ldg(g.k + ex + (long long)n * (ey + (long long)n * ez)) : T(0);
+          }
+      auto X = [&](int dx, int dy, int dz) -> T {
+        const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+        const bool in = jx >= 0 && jx < M && jy >= 0 && jy < M && jz >= 0 && jz < M && !dirf(jx, 1, 2) &&
+                        !dirf(jy, 4, 8) && !dirf(jz, 16, 32);
+        return in ? (T)x[(long long)jz * MM + (long long)jy * M + jx] : T(0);
+      };
+      mf_row<T, HX, DIFF>(k, X, g.hs, ax, d, xc);
+    }
+    const T bb = HB ? __ldg(b + i) : T(0);
+    const T o = (HO && uwd) ? __ldg(g.wd + i) : ((HO && g.omega) ? __ldg(g.omega + i) : g.w);
+    const T out = mf_out<MODE>(ax, d, xc, bb, o, uwd);
+    y[i] = out;
+    if (RED) {
+      acc0 = fma((double)out, (double)v[i], acc0);
+      if (v2) acc1 = fma((double)out, (double)v2[i], acc1);
+    }
   }
 }
 
-// Matrix-free top-level operator, 2.5D blocking: a CTA owns a 32 x 16 column
-// of nodes (256 threads, thread (lx, ly) computes the y-adjacent nodes 2ly and
-// 2ly+1) and marches z through ZS planes.  The (32+2) x (16+2) halo of each x
-// plane and the 33 x 17 cells of each cell plane are copied into a 5-stage
-// shared-memory ring by cp.async (4/8-byte copies, masked entries zero-filled:
-// Dirichlet nodes and nodes outside the grid read as zero -- eliminated
-// columns -- and cells outside the grid as zero coefficient), two stages ahead
-// of the plane being computed.  Stage s holds x plane s+1 and cell plane s;
-// plane iz reads the x planes of stages iz-2 .. iz and the cell planes of
-// stages iz-1, iz.  The per-node operands (b, omega, v, v2) are register-
-// prefetched one plane ahead, and ring slots advance by increments.  The row
-// is evaluated in factored form: 4 K x_i minus, over the 12 face diagonals,
-// the sum of the two cells sharing each times its value, minus, over the 8
-// body diagonals, the one cell times its value (axis neighbours have weight
-// zero in the Q1 stiffness).
-constexpr int kMX = 32;                            // nodes along x of a CTA
-constexpr int kHX = kMX + 2, kCX = kMX + 1;        // halo / cell tile along x
-constexpr int kMFThreads = 256;
-constexpr int kStages = 5;
+template <typename T, typename TV, typename TX, int MODE, bool RED>
+__global__ void __launch_bounds__(kFThreads, 2)
+k_mft(MFArgsT<T> g, const __grid_constant__ CUtensorMap tx_rows, const __grid_constant__ CUtensorMap tk_cells,
+      MftGeo geo, const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
+      const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
+  typedef MftLayout<T, TX> L;
+  constexpr bool HX = MODE != 3;
+  constexpr bool HB = MODE != 0;
+  constexpr bool DIFF = sizeof(T) == 8;
+  constexpr bool HO = MODE == 2 || MODE == 3;
+  extern __shared__ __align__(128) unsigned char sm_dyn[];
+  __shared__ double red[8];
+  // the copies land on 128-byte boundaries: round the base up (the launch adds 128 bytes)
+  unsigned char* sm = sm_dyn + ((128u - (umma::smem_u32(sm_dyn) & 127u)) & 127u);
+  const int tid = threadIdx.x;
+  const int M = g.M, n = g.n, dm = g.dmask;
+  const long long MM = (long long)M * M;
+  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+  const bool omv = g.omega != nullptr, uwd = g.wd != nullptr;
+  const T hs = g.hs;
+  double acc0 = 0.0, acc1 = 0.0;
+  auto opnd = [&](long long i, T& bb, T& o) {  // per-node right-hand side and damping
+    bb = HB ? __ldg(b + i) : T(0);
+    o = (HO && uwd) ? __ldg(g.wd + i) : ((HO && omv) ? __ldg(g.omega + i) : g.w);
+  };
+  auto emit = [&](long long i, T out, TV vv, TV vv2) {
+    y[i] = out;
+    if (RED) {
+      acc0 = fma((double)out, (double)vv, acc0);
+      if (v2) acc1 = fma((double)out, (double)vv2, acc1);
+    }
+  };
+  if ((int)blockIdx.x >= geo.nface) {
+    // ------------------------------------------------------------ tiled CTA
+    const int bid = (int)blockIdx.x - geo.nface;
+    const int bx = bid % geo.nbx, by = (bid / geo.nbx) % geo.nby, bz = bid / (geo.nbx * geo.nby);
+    const int x0 = bx * kFX, y0 = by * kFY, z0 = bz * kFZ;
+    const int lx = tid & 31, ly = tid >> 5;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFRing * L::SB + kFPack * L::PS * sizeof(T));
+    T* pk = reinterpret_cast<T*>(sm + kFRing * L::SB);
+    if (tid == 0)
+      for (int s = 0; s < kFRing; ++s) umma::mbar_init(&bar[s]);
+    __syncthreads();
+    // stage j: x plane z0-1+j and cell plane z0-2+j, ring slot j % kFRing
+    auto issue = [&](int j) {  // warp 0
+      unsigned char* st = sm + (j % kFRing) * L::SB;
+      uint64_t* bj = bar + j % kFRing;
+      if (lx == 0) {
+        umma::fence_async_smem();
+        umma::mbar_arrive_expect_tx(bj, (HX ? L::XTX : 0u) + L::CTX);
+      }
+      __syncwarp();
+      if (HX && lx < kFRows) {
+        const int z = z0 - 1 + j, yy = y0 - 1 + lx;
+        const bool ok = z >= 0 && z < M && yy >= 0 && yy < M && !dirf(z, 16, 32) && !dirf(yy, 4, 8);
+        const long long lin = (long long)z * MM + (long long)yy * M + x0 - 1;
+        umma::tma_load_1d(st + lx * L::XP, &tx_rows, bj, ok ? (int)(lin & ~(long long)(L::XA - 1)) : kZeroRow);
+      }
+      if (lx == 31) umma::tma_load_3d(st + L::XB, &tk_cells, bj, x0 - 1 - L::COFF, y0 - 1, z0 - 2 + j);
+    };
+    // packing: thread tid handles packed elements tid, tid+256, tid+512 of a plane
+    int proff[3], plo[3];
+    bool pmask[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int e = tid + q * kFThreads;
+      const int r = e / kFPW, jj = e - r * kFPW;
+      const int xx = x0 - 1 + jj, yy = y0 - 1 + r;
+      proff[q] = r * (L::XP / (int)sizeof(TX)) + jj;
+      plo[q] = (int)(((long long)yy * M + x0 - 1) & (L::XA - 1));
+      pmask[q] = xx < 0 || (xx == 0 && (dm & 1)) || (xx == M - 1 && (dm & 2));
+    }
+    auto pack = [&](int j) {
+      const TX* raw = reinterpret_cast<const TX*>(sm + (j % kFRing) * L::SB);
+      T* P = pk + (j % kFPack) * L::PS;
+      const int zlo = (int)(((long long)(z0 - 1 + j) * MM) & (L::XA - 1));
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int e = tid + q * kFThreads;
+        if (q < 2 || e < L::PS) {
+          const TX xv = raw[proff[q] + ((zlo + plo[q]) & (L::XA - 1))];
+          P[e] = pmask[q] ? T(0) : (T)xv;
+        }
+      }
+    };
+    auto wait = [&](int j) { return umma::mbar_wait(bar + j % kFRing, (uint32_t)((j / kFRing) & 1)); };
+    const int last = kFZ + 1;  // the last stage a CTA needs
+    if (tid < 32)
+      for (int j = 0; j < kFRing; ++j) issue(j);
+    int issued = kFRing - 1, waited = 1;
+    bool ok = wait(0);
+    if (HX) pack(0);
+    ok = wait(1) && ok;
+    if (HX) pack(1);
+    const int ix = x0 + lx, iy0 = y0 + 2 * ly;
+    const bool dirx = dirf(ix, 1, 2);
+    const bool diry[2] = {dirf(iy0, 4, 8), dirf(iy0 + 1, 4, 8)};
+    struct Ops { T b[2], o[2]; TV v[2], v2[2]; };
+    auto ldops = [&](int jz, Ops& o) {
+      if (jz >= z0 + kFZ) return;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const long long i = (long long)jz * MM + (long long)(iy0 + r) * M + ix;
+        opnd(i, o.b[r], o.o[r]);
+        o.v[r] = RED ? __ldg(v + i) : TV(0);
+        o.v2[r] = (RED && v2) ? __ldg(v2 + i) : TV(0);
+      }
+    };
+    Ops cur, nxt;
+    ldops(z0, cur);
+    bool bad = false;
+#pragma unroll 1
+    for (int t = 0; t < kFZ; ++t) {
+      const int iz = z0 + t;
+      ok = wait(t + 2) && ok;
+      waited = t + 2;
+      if (HX) pack(t + 2);
+      if (__syncthreads_or(!ok)) {  // a copy that never landed: stop issuing
+        bad = true;
+        break;
+      }
+      if (t + kFRing <= last) {  // slot t % kFRing: stage t's cells and rows were last read in step t-1
+        if (tid < 32) issue(t + kFRing);
+        issued = t + kFRing;
+      }
+      ldops(iz + 1, nxt);
+      const T* X0 = pk + (t % kFPack) * L::PS;         // x plane iz-1
+      const T* X1 = pk + ((t + 1) % kFPack) * L::PS;   // x plane iz
+      const T* X2 = pk + ((t + 2) % kFPack) * L::PS;   // x plane iz+1
+      const T* K0 = reinterpret_cast<const T*>(sm + ((t + 1) % kFRing) * L::SB + L::XB);  // cell plane iz-1
+      const T* K1 = reinterpret_cast<const T*>(sm + ((t + 2) % kFRing) * L::SB + L::XB);  // cell plane iz
+      const bool dirz = dirf(iz, 16, 32);
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const long long i = (long long)iz * MM + (long long)(iy0 + r) * M + ix;
+        T ax, d, xc;
+        if (dirz || dirx || diry[r]) {  // identity row; the packed planes hold zero here
+          xc = HX ? (T)x[i] : T(0);
+          ax = xc;
+          d = T(1);
+        } else {
+          const int h = (2 * ly + r + 1) * kFPW + lx + 1;
+          const int kc = (2 * ly + r) * L::CW + lx + L::COFF;
+          T k[2][2][2];
+#pragma unroll
+          for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+            for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+              for (int cx = 0; cx < 2; ++cx) k[cz][cy][cx] = (cz ? K1 : K0)[kc + cy * L::CW + cx];
+          auto X = [&](int dx, int dy, int dz) -> T {
+            return (dz < 0 ? X0 : (dz > 0 ? X2 : X1))[h + dy * kFPW + dx];
+          };
+          mf_row<T, HX, DIFF>(k, X, hs, ax, d, xc);
+        }
+        emit(i, mf_out<MODE>(ax, d, xc, cur.b[r], cur.o[r], uwd), cur.v[r], cur.v2[r]);
+      }
+      cur = nxt;
+    }
+    if (bad) {  // let the copies in flight land (bounded) before the CTA's shared memory is released
+      if (tid == 0) {
+        for (int j = waited + 1; j <= issued; ++j) umma::mbar_wait(bar + j % kFRing, (uint32_t)((j / kFRing) & 1));
+        if (g.err) *g.err = 1.0;
+      }
+      __syncthreads();
+    }
+  } else {
+    // -------------------------------------------------------------- face CTA
+    mf_face_cta<T, TV, TX, MODE, RED>(g, geo, (int)blockIdx.x, x, b, y, v, v2, acc0, acc1);
+  }
+  if (RED) dr_finish2(acc0, acc1, R, red);
+}
+
+// FP32 form of the operator, fed by asynchronous copies three planes ahead.
+// Same tiles and face CTAs as k_mft.  A stage of the 6-slot shared-memory
+// ring holds what one step reads: the 18 x 34 x halo of the plane above
+// (cp.async, 4 bytes per element, eliminated and outside entries zero-filled
+// at the copy), the 17 x 36 cell tile (one TMA box) and the per-node operands
+// of the step's own plane (b, the damping, the two FP64 reduction vectors:
+// each thread copies its own two nodes').  All copies of a stage complete on
+// its full mbarrier (256 cp.async arrivals + the TMA's expect-tx arrival);
+// each warp releases a stage on its empty mbarrier once it has read it, and
+// a slot is refilled only after all 8 warps have released it, so warps drift
+// apart freely by a few steps and no block barrier is needed.  A thread keeps
+// the x values and cells its two nodes read in registers as it marches z,
+// reading each plane once (the loop runs six steps per turn so register roles
+// rotate at compile time).  Dirichlet nodes of the tile (on the faces x, y,
+// z = 0) are left to the face CTAs, which evaluate identity rows.
+constexpr int kCRing = 6;   // ring slots
+constexpr int kCLook = 5;   // stage j is requested at step j-5 and read at step j-2
+constexpr int kPX = kFPW;   // packed x row: x0-1 .. x0+32
+
+template <typename T, typename TV, int MODE, bool RED>
+struct MfcLayout {
+  static constexpr bool HB = MODE != 0, HO = MODE == 2 || MODE == 3, HX = MODE != 3;
+  static constexpr int up(int b) { return (b + 127) / 128 * 128; }
+  static constexpr int XS = HX ? up(kFRows * kPX * 4) : 0;         // packed x halo
+  static constexpr int CS = up(kFCRows * MftLayout<T, float>::CW * (int)sizeof(T));  // cell box (TMA)
+  static constexpr int OB = HB ? up(2 * kFThreads * (int)sizeof(T)) : 0;  // b of the step's plane
+  static constexpr int OO = HO ? up(2 * kFThreads * (int)sizeof(T)) : 0;  // damping
+  static constexpr int OV = RED ? up(2 * kFThreads * (int)sizeof(TV)) : 0;  // reduction vectors
+  static constexpr int SB = XS + CS + OB + OO + 2 * OV;
+  static constexpr int SMEM = kCRing * SB + 2 * kCRing * 8 + 128;
+};
 
 __device__ __forceinline__ void cpa(void* dst, const void* src, bool ok, int bytes) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -146,172 +499,209 @@ __device__ __forceinline__ void cpa(void* dst, const void* src, bool ok, int byt
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(ok ? 4 : 0) : "memory");
 }
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// one arrival on the mbarrier once this thread's earlier cp.async copies have landed
+__device__ __forceinline__ void cpa_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(umma::smem_u32(bar)) : "memory");
+}
 
-constexpr int kMY4 = 16;
-constexpr int kHY4 = kMY4 + 2, kCY4 = kMY4 + 1;
-constexpr int kNH4 = kHX * kHY4, kNC4 = kCX * kCY4;  // 612, 561
-
-template <typename T, typename TV, typename TX, int ZS, int MODE, bool RED>
-__global__ void __launch_bounds__(kMFThreads)
-k_mf4(MFArgsT<T> g, const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
-      const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
-  constexpr bool HX = MODE != 3;
-  constexpr bool HB = MODE != 0;
+template <typename T, typename TV, int MODE, bool RED>
+__global__ void __launch_bounds__(kFThreads, 2)
+k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, const float* __restrict__ x,
+      const T* __restrict__ b, T* __restrict__ y, const TV* __restrict__ v, const TV* __restrict__ v2,
+      Reduce2 R) {
+  typedef MfcLayout<T, TV, MODE, RED> L;
+  typedef MftLayout<T, float> LC;
   constexpr bool DIFF = sizeof(T) == 8;  // the FP64 operator in difference form
-  constexpr bool HO = MODE == 2 || MODE == 3;
-  __shared__ TX xs[kStages][HX ? kNH4 : 1];
-  __shared__ T ks[kStages][kNC4];
-  __shared__ double smem[8];
-  const int tid = threadIdx.x, lx = tid & (kMX - 1), ly = tid / kMX;
-  const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY4, z0 = blockIdx.z * ZS;
-  const int M = g.M, n = g.n, dm = g.dmask;
-  const long long MM = (long long)M * M, nn = (long long)n * n;
-  const int ix = x0 + lx, iy0 = y0 + 2 * ly;
-  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-  int hoff[3], coff[3];
-  bool hok[3], cok[3];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const int e = tid + q * kMFThreads;
-    const int jx = x0 - 1 + e % kHX, jy = y0 - 1 + e / kHX;
-    hok[q] = e < kNH4 && jx >= 0 && jx < M && jy >= 0 && jy < M && !dirf(jx, 1, 2) && !dirf(jy, 4, 8);
-    hoff[q] = hok[q] ? jy * M + jx : 0;
-    const int cx = x0 - 1 + e % kCX, cy = y0 - 1 + e / kCX;
-    cok[q] = e < kNC4 && cx >= 0 && cx < n && cy >= 0 && cy < n;
-    coff[q] = cok[q] ? cy * n + cx : 0;
-  }
-  const bool own0 = ix < M && iy0 < M, own1 = ix < M && iy0 + 1 < M;
-  const long long col0 = own0 ? (long long)iy0 * M + ix : 0;
-  const long long col1 = own1 ? (long long)(iy0 + 1) * M + ix : 0;
-  const bool omv = g.omega != nullptr;
-  const int zend = min(z0 + ZS, M);
-  auto issue = [&](int st, int sl) {  // x plane st+1 and cell plane st into slot sl
-    if (HX) {
-      const int jz = st + 1;
-      const bool vz = jz >= 0 && jz < M && !dirf(jz, 16, 32);
-      const TX* pl = x + (long long)(vz ? jz : 0) * MM;
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int e = tid + q * kMFThreads;
-        if (e < kNH4) cpa(&xs[sl][e], pl + hoff[q], vz && hok[q], (int)sizeof(TX));
+  constexpr bool HX = L::HX, HB = L::HB, HO = L::HO;
+  extern __shared__ __align__(128) unsigned char sm_dyn[];
+  __shared__ double red[8];
+  unsigned char* sm = sm_dyn + ((128u - (umma::smem_u32(sm_dyn) & 127u)) & 127u);
+  const int tid = threadIdx.x;
+  double acc0 = 0.0, acc1 = 0.0;
+  if ((int)blockIdx.x >= geo.nface) {
+    const int M = g.M, dm = g.dmask;
+    const long long MM = (long long)M * M;
+    auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+    const bool uwd = g.wd != nullptr;
+    const T* om_src = uwd ? g.wd : g.omega;  // per-node damping source, if any
+    const T hs = g.hs;
+    const int bid = (int)blockIdx.x - geo.nface;
+    const int bx = bid % geo.nbx, by = (bid / geo.nbx) % geo.nby, bz = bid / (geo.nbx * geo.nby);
+    const int x0 = bx * kFX, y0 = by * kFY, z0 = bz * kFZ;
+    const int lx = tid & 31, ly = tid >> 5;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + kCRing * L::SB);
+    uint64_t* empty = full + kCRing;
+    if (tid == 0)
+      for (int s = 0; s < kCRing; ++s) {
+        umma::mbar_init_count(&full[s], kFThreads + 1);
+        umma::mbar_init_count(&empty[s], kFThreads / 32);
       }
-    }
-    const bool vz = st >= 0 && st < n;
-    const T* pl = g.k + (long long)(vz ? st : 0) * nn;
+    __syncthreads();
+    const int last = kFZ + 1;
+    // this thread's share of the x halo: elements tid, tid+256, tid+512 of 18 x 34
+    int hoff[3];
+    bool hok[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const int e = tid + q * kMFThreads;
-      if (e < kNC4) cpa(&ks[sl][e], pl + coff[q], vz && cok[q], (int)sizeof(T));
+      const int e = tid + q * kFThreads;
+      const int r = e / kPX, jj = e - r * kPX;
+      const int xx = x0 - 1 + jj, yy = y0 - 1 + r;
+      hok[q] = e < kFRows * kPX && xx >= 0 && xx < M && yy >= 0 && yy < M && !dirf(xx, 1, 2) && !dirf(yy, 4, 8);
+      hoff[q] = hok[q] ? yy * M + xx : 0;
     }
-    cpa_commit();
-  };
-  struct Ops { T b[2], o[2]; TV v[2], v2[2]; };
-  auto ldops = [&](int jz, Ops& o) {  // per-node operands of a plane (two nodes)
-    const bool in = jz < zend;
-    const long long zb = (long long)jz * MM;
+    const int ix = x0 + lx, iy0 = y0 + 2 * ly;
+    const long long ibase = (long long)iy0 * M + ix;
+    bool ok = true;  // every wait of this warp so far completed; after one gives up, the rest wait 1 ms at most
+    auto wait = [&](uint64_t* bar, uint32_t parity) {
+      const bool w = ok ? umma::mbar_wait(bar, parity) : umma::mbar_wait_for(bar, parity, 1 << 16, 1000000ull);
+      ok = __all_sync(0xffffffffu, w) && ok;
+    };
+    // stage j: x plane z0-1+j, cell plane z0-2+j, operands of plane z0-2+j; slot j % kCRing
+    auto issue = [&](int j) {
+      const int s = j % kCRing;
+      if (j >= kCRing) wait(&empty[s], (uint32_t)(((j / kCRing) - 1) & 1));  // all warps released the slot
+      unsigned char* st = sm + s * L::SB;
+      if (tid == 0) {
+        umma::fence_async_smem();
+        umma::mbar_arrive_expect_tx(&full[s], LC::CTX);
+        umma::tma_load_3d(st + L::XS, &tk_cells, &full[s], x0 - 1 - LC::COFF, y0 - 1, z0 - 2 + j);
+      }
+      if (HX) {
+        const int z = z0 - 1 + j;
+        const bool zok = z >= 0 && z < M && !dirf(z, 16, 32);
+        const float* pl = x + (zok ? (long long)z * MM : 0ll);
+        float* xs = reinterpret_cast<float*>(st);
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const bool ok = in && (r ? own1 : own0);
-      const long long i = zb + (r ? col1 : col0);
-      o.b[r] = (HB && ok) ? __ldg(b + i) : T(0);
-      o.o[r] = (HO && g.wd && ok) ? __ldg(g.wd + i) : ((HO && omv && ok) ? __ldg(g.omega + i) : g.w);
-      o.v[r] = (RED && ok) ? __ldg(v + i) : TV(0);
-      o.v2[r] = (RED && ok && v2) ? __ldg(v2 + i) : TV(0);
-    }
-  };
-  issue(z0 - 2, 0);
-  issue(z0 - 1, 1);
-  issue(z0, 2);
-  issue(z0 + 1, 3);
-  int s2 = 0, s1 = 1, s0 = 2, si = 4;  // slots of stages iz-2, iz-1, iz and of the next issue
-  Ops cur, nxt;
-  ldops(z0, cur);
-  double acc0 = 0.0, acc1 = 0.0;
-  const bool dirx = dirf(ix, 1, 2);
-  const T hs = g.hs;
-#pragma unroll 1
-  for (int iz = z0; iz < zend; ++iz) {
-    issue(iz + 2, si);
-    ldops(iz + 1, nxt);
-    cpa_wait<2>();
-    __syncthreads();
-    const bool dirz = dirf(iz, 16, 32);
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      if (!(r ? own1 : own0)) continue;
-      const int iy = iy0 + r;
-      const long long i = (long long)iz * MM + (r ? col1 : col0);
-      const bool dir = dirz || dirx || dirf(iy, 4, 8);
-      T ax = T(0), d = T(1), xc = T(0);
-      if (dir) {
-        if (HX) { xc = (T)x[i]; ax = xc; }
-      } else {
-        T k[2][2][2];  // k[cz][cy][cx]: cz 0 cell plane iz-1 (slot s1), 1 cell plane iz (slot s0)
-#pragma unroll
-        for (int cz = 0; cz < 2; ++cz)
-#pragma unroll
-          for (int cy = 0; cy < 2; ++cy)
-#pragma unroll
-            for (int cx = 0; cx < 2; ++cx) k[cz][cy][cx] = ks[cz ? s0 : s1][(2 * ly + r + cy) * kCX + lx + cx];
-        const T wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
-                            {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
-        const T ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
-        T sacc = T(0);
-        if (HX) {
-          const int h = (2 * ly + r + 1) * kHX + lx + 1;
-          const TX* X1 = xs[s1];  // x plane iz
-          xc = (T)X1[h];
-          // FP64: the row as sum_j w_j (x_i - x_j) -- the weights sum to 4 K,
-          // and the differences of a smooth iterate are small, so the true
-          // residual's rounding is far below that of 4 K x_i - sum_j w_j x_j
-          auto term = [&](T w, T xj) { sacc = DIFF ? fma(w, xc - xj, sacc) : fma(w, xj, sacc); };
-#pragma unroll
-          for (int sy = 0; sy < 2; ++sy)
-#pragma unroll
-            for (int sx = 0; sx < 2; ++sx) term(wc[sy][sx], (T)X1[h + (2 * sy - 1) * kHX + 2 * sx - 1]);
-#pragma unroll
-          for (int cz = 0; cz < 2; ++cz) {
-            const TX* Xz = xs[cz ? s0 : s2];  // x plane iz+1 / iz-1
-#pragma unroll
-            for (int sx = 0; sx < 2; ++sx)   // face diagonals (sx, 0, sz): cells (sx, *, sz)
-              term(k[cz][0][sx] + k[cz][1][sx], (T)Xz[h + 2 * sx - 1]);
-#pragma unroll
-            for (int sy = 0; sy < 2; ++sy)   // face diagonals (0, sy, sz): cells (*, sy, sz)
-              term(k[cz][sy][0] + k[cz][sy][1], (T)Xz[h + (2 * sy - 1) * kHX]);
-#pragma unroll
-            for (int sy = 0; sy < 2; ++sy)
-#pragma unroll
-              for (int sx = 0; sx < 2; ++sx)  // body diagonals
-                term(k[cz][sy][sx], (T)Xz[h + (2 * sy - 1) * kHX + 2 * sx - 1]);
-          }
-          if (!DIFF) sacc = fma(T(4) * ksum, xc, -sacc);
+        for (int q = 0; q < 3; ++q) {
+          const int e = tid + q * kFThreads;
+          if (q < 2 || e < kFRows * kPX) cpa(xs + e, pl + hoff[q], zok && hok[q], 4);
         }
-        d = T(4) * hs * ksum;
-        ax = hs * sacc;
       }
-      T out;
-      if (MODE == 0) out = ax;
-      else if (MODE == 1) out = cur.b[r] - ax;
-      else if (MODE == 2) out = g.wd ? fma(cur.o[r], cur.b[r] - ax, xc) : fma(cur.o[r], (cur.b[r] - ax) / d, xc);
-      else out = g.wd ? cur.o[r] * cur.b[r] : cur.o[r] * (cur.b[r] / d);
-      y[i] = out;
-      if (RED) {
-        acc0 = fma((double)out, (double)cur.v[r], acc0);
-        if (v2) acc1 = fma((double)out, (double)cur.v2[r], acc1);
+      const int zo = z0 - 2 + j;  // the operands' plane
+      if (zo >= z0 && (HB || HO || RED)) {
+        unsigned char* op = st + L::XS + L::CS;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const long long i = (long long)zo * MM + ibase + r * M;
+          const int k = r * kFThreads + tid;
+          if (HB) cpa(reinterpret_cast<T*>(op) + k, b + i, true, (int)sizeof(T));
+          if (HO) cpa(reinterpret_cast<T*>(op + L::OB) + k, om_src ? om_src + i : b, om_src != nullptr, (int)sizeof(T));
+          if (RED) {
+            cpa(reinterpret_cast<TV*>(op + L::OB + L::OO) + k, v + i, true, (int)sizeof(TV));
+            cpa(reinterpret_cast<TV*>(op + L::OB + L::OO + L::OV) + k, v2 ? v2 + i : v, v2 != nullptr,
+                (int)sizeof(TV));
+          }
+        }
       }
+      cpa_arrive(&full[s]);
+    };
+    auto consume = [&](int j, T (&xv)[4][3], T (&kv)[3][2], bool want_k) {
+      const int s = j % kCRing;
+      wait(&full[s], (uint32_t)((j / kCRing) & 1));
+      const unsigned char* st = sm + s * L::SB;
+      if (HX) {
+        const float* xs = reinterpret_cast<const float*>(st);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xv[k][c] = (T)xs[(2 * ly + k) * kPX + lx + c];
+      }
+      if (want_k) {
+        const T* cs = reinterpret_cast<const T*>(st + L::XS);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) kv[r][c] = cs[(2 * ly + r) * LC::CW + lx + c + LC::COFF];
+      }
+    };
+    auto release = [&](int j) {
+      __syncwarp();
+      if (lx == 0) umma::mbar_arrive(&empty[j % kCRing]);
+    };
+    T xr[3][4][3], kr[2][3][2];
+    for (int j = 0; j < kCLook && j <= last; ++j) issue(j);
+    consume(0, xr[0], kr[1], false);  // x plane z0-1 (its cell plane is not read)
+    release(0);
+    consume(1, xr[1], kr[0], true);   // x plane z0, cell plane z0-1
+    release(1);
+    const bool dirx = dirf(ix, 1, 2);
+    const bool diry0 = dirf(iy0, 4, 8), diry1 = dirf(iy0 + 1, 4, 8);
+    // step t (plane z0+t): x planes iz-1, iz, iz+1 in xr[t%3], xr[(t+1)%3],
+    // xr[(t+2)%3] (the last one read now), cell planes iz-1, iz in kr[t%2],
+    // kr[(t+1)%2] (the last one read now); the operands come with stage t+2
+    auto step = [&](auto Qc, int t) {
+      constexpr int Q = decltype(Qc)::value;
+      constexpr int PM = Q % 3, P0 = (Q + 1) % 3, PP = (Q + 2) % 3, CM = Q % 2, C0 = (Q + 1) % 2;
+      if (t + kCLook <= last) issue(t + kCLook);
+      consume(t + 2, xr[PP], kr[C0], true);
+      const unsigned char* op = sm + ((t + 2) % kCRing) * L::SB + L::XS + L::CS;
+      T bb[2], oo[2];
+      TV vv[2], vv2[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int k = r * kFThreads + tid;
+        bb[r] = HB ? reinterpret_cast<const T*>(op)[k] : T(0);
+        oo[r] = HO ? (om_src ? reinterpret_cast<const T*>(op + L::OB)[k] : g.w) : T(0);
+        vv[r] = RED ? reinterpret_cast<const TV*>(op + L::OB + L::OO)[k] : TV(0);
+        vv2[r] = (RED && v2) ? reinterpret_cast<const TV*>(op + L::OB + L::OO + L::OV)[k] : TV(0);
+      }
+      release(t + 2);
+      const int iz = z0 + t;
+      const bool dirz = dirf(iz, 16, 32);
+      const long long i0 = (long long)iz * MM + ibase;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        T k[2][2][2];
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+          for (int cx = 0; cx < 2; ++cx) {
+            k[0][cy][cx] = kr[CM][r + cy][cx];
+            k[1][cy][cx] = kr[C0][r + cy][cx];
+          }
+        auto X = [&](int dx, int dy, int dz) -> T {
+          return xr[dz < 0 ? PM : (dz > 0 ? PP : P0)][r + 1 + dy][1 + dx];
+        };
+        T ax, d, xc;
+        mf_row<T, HX, DIFF>(k, X, hs, ax, d, xc);
+        const T out = mf_out<MODE>(ax, d, xc, bb[r], oo[r], uwd);
+        if (!(dirz || dirx || (r ? diry1 : diry0))) {  // identity rows: the face CTAs
+          y[i0 + r * M] = out;
+          if (RED) {
+            acc0 = fma((double)out, (double)vv[r], acc0);
+            if (v2) acc1 = fma((double)out, (double)vv2[r], acc1);
+          }
+        }
+      }
+    };
+    typedef std::integral_constant<int, 0> Q0;
+    typedef std::integral_constant<int, 1> Q1;
+    typedef std::integral_constant<int, 2> Q2;
+    typedef std::integral_constant<int, 3> Q3;
+    typedef std::integral_constant<int, 4> Q4;
+    typedef std::integral_constant<int, 5> Q5;
+    int t = 0;
+#pragma unroll 1
+    for (; t + 6 <= kFZ; t += 6) {
+      step(Q0{}, t);
+      step(Q1{}, t + 1);
+      step(Q2{}, t + 2);
+      step(Q3{}, t + 3);
+      step(Q4{}, t + 4);
+      step(Q5{}, t + 5);
     }
-    cur = nxt;
-    __syncthreads();  // slot s2 is refilled by the next issue
-    si = s2;
-    s2 = s1;
-    s1 = s0;
-    s0 = s0 + 1 == kStages ? 0 : s0 + 1;
+    if constexpr (kFZ % 6 > 0) step(Q0{}, t);
+    if constexpr (kFZ % 6 > 1) step(Q1{}, t + 1);
+    if constexpr (kFZ % 6 > 2) step(Q2{}, t + 2);
+    if constexpr (kFZ % 6 > 3) step(Q3{}, t + 3);
+    if constexpr (kFZ % 6 > 4) step(Q4{}, t + 4);
+    // every stage requested has been waited for; a wait that gave up voids the results
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (__syncthreads_or(!ok) && tid == 0 && g.err) *g.err = 1.0;
+  } else {
+    mf_face_cta<T, TV, float, MODE, RED>(g, geo, (int)blockIdx.x, x, b, y, v, v2, acc0, acc1);
   }
-  cpa_wait<0>();
-  if (RED) dr_finish2_grid(acc0, acc1, R, smem);
+  if (RED) dr_finish2(acc0, acc1, R, red);
 }
 
 // ------------------------------------------------------ stored FP32 levels
@@ -721,34 +1111,129 @@ k_dot2_64(const double* __restrict__ xv, const float* __restrict__ yv, const dou
 
 static inline unsigned g1(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
-constexpr int kZS2 = 32;  // planes per CTA of k_mf2
+// the tiled box of k_mft: whole 32 x 16 x 32 tiles from the origin, the rest
+// to face CTAs (all of it when a side is below a tile)
+// drop_dir: the tiled CTAs leave the Dirichlet faces x, y, z = 0 of their box
+// to the face CTAs (k_mfc); otherwise they evaluate those identity rows (k_mft)
+static MftGeo mft_geo(int M, int dmask, bool drop_dir) {
+  MftGeo q{};
+  const int n = M - 1;
+  q.nbx = n / kFX;
+  q.nby = n / kFY;
+  q.nbz = n / kFZ;
+  if (q.nbx == 0 || q.nby == 0 || q.nbz == 0) q.nbx = q.nby = q.nbz = 0;
+  q.nmain = q.nbx * q.nby * q.nbz;
+  q.X1 = (long long)q.nbx * kFX;
+  q.Y1 = (long long)q.nby * kFY;
+  q.Z1 = (long long)q.nbz * kFZ;
+  if (q.nmain > 0 && drop_dir) {
+    q.ax = (dmask & 1) ? 1 : 0;
+    q.ay = (dmask & 4) ? 1 : 0;
+    q.az = (dmask & 16) ? 1 : 0;
+  }
+  q.F = (long long)M * M * M - (q.X1 - q.ax) * (q.Y1 - q.ay) * (q.Z1 - q.az);
+  q.nface = (int)((q.F + kFaceNodes - 1) / kFaceNodes);
+  return q;
+}
 
-static dim3 mf2_grid(int M) {
-  return dim3((unsigned)((M + kMX - 1) / kMX), (unsigned)((M + kMY4 - 1) / kMY4), (unsigned)((M + kZS2 - 1) / kZS2));
+static unsigned mft_blocks(const MftGeo& q) { return (unsigned)(q.nmain + q.nface); }
+
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  return encode;
+}
+
+template <typename E>
+static CUtensorMapDataType tm_type() {
+  return sizeof(E) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+}
+
+// the vector as one dimension, boxes of one staged row; the cells as
+// n x n x n, boxes of one plane's cell tile; everything outside reads as zero
+template <typename T, typename TX>
+static bool mft_maps(const TX* x, long long N, const T* k, int n, CUtensorMap* tr, CUtensorMap* tk) {
+  typedef MftLayout<T, TX> L;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return false;
+  const cuuint32_t one[3] = {1, 1, 1};
+  if (x) {
+    const cuuint64_t dims[1] = {(cuuint64_t)N};
+    const cuuint64_t strides[1] = {0};
+    const cuuint32_t box[1] = {(cuuint32_t)L::XW};
+    if (enc(tr, tm_type<TX>(), 1, const_cast<TX*>(x), dims, strides, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)n};
+  const cuuint64_t strides[2] = {(cuuint64_t)n * sizeof(T), (cuuint64_t)n * n * sizeof(T)};
+  const cuuint32_t box[3] = {(cuuint32_t)L::CW, (cuuint32_t)kFCRows, 1};
+  return enc(tk, tm_type<T>(), 3, const_cast<T*>(k), dims, strides, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, typename TV, typename TX, int MODE, bool RED>
+static void mft_launch(const MFArgsT<T>& g, const TX* x, const T* b, T* y, const TV* v, const TV* v2,
+                       const Reduce2& R, cudaStream_t st) {
+  typedef MftLayout<T, TX> L;
+  constexpr bool F32 = sizeof(TX) == 4;  // an FP32 x: the cp.async-fed form (its x halo needs no map)
+  MftGeo q = mft_geo(g.M, g.dmask, F32);
+  CUtensorMap tr{}, tk{};
+  // the tensor maps need 16-byte aligned bases; without them every node goes to the face CTAs
+  if (q.nmain > 0 && !mft_maps<T, TX>((MODE != 3 && !F32) ? x : nullptr, g.N, g.k, g.n, &tr, &tk)) {
+    q = MftGeo{};
+    q.F = g.N;
+    q.nface = (int)((q.F + kFaceNodes - 1) / kFaceNodes);
+  }
+  static unsigned attr_set = 0;  // devices the shared-memory size was raised on
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 32 && !((attr_set >> dev) & 1u)) {
+    if constexpr (F32)
+      cudaFuncSetAttribute(k_mfc<T, TV, MODE, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           MfcLayout<T, TV, MODE, RED>::SMEM);
+    else
+      cudaFuncSetAttribute(k_mft<T, TV, TX, MODE, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+    attr_set |= 1u << dev;
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if constexpr (F32) {
+    k_mfc<T, TV, MODE, RED><<<mft_blocks(q), kFThreads, MfcLayout<T, TV, MODE, RED>::SMEM, st>>>(
+        g, tk, q, reinterpret_cast<const float*>(x), b, y, v, v2, R);
+  } else {
+    k_mft<T, TV, TX, MODE, RED><<<mft_blocks(q), kFThreads, L::SMEM, st>>>(g, tr, tk, q, x, b, y, v, v2, R);
+  }
 }
 
 template <typename T, typename TV, typename TX>
 static void mf_launch(int mode, const MFArgsT<T>& g, const TX* x, const T* b, T* y, const TV* v, const TV* v2,
                       const Reduce2* R, cudaStream_t st) {
-  const dim3 grid = mf2_grid(g.M);
-  Reduce2 r0 = R ? *R : Reduce2{};
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  if constexpr (sizeof(T) == 8) {  // the FP64 operator is only applied (mode 0)
-    if (R) k_mf4<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
-    else k_mf4<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+  const Reduce2 r0 = R ? *R : Reduce2{};
+  if constexpr (sizeof(T) == 8) {  // the FP64 operator: a = A p, or the true residual of FP64 vectors
+    if (mode == 1) mft_launch<T, TV, TX, 1, false>(g, x, b, y, v, v2, r0, st);
+    else if (R) mft_launch<T, TV, TX, 0, true>(g, x, b, y, v, v2, r0, st);
+    else mft_launch<T, TV, TX, 0, false>(g, x, b, y, v, v2, r0, st);
   } else if (R) {
     switch (mode) {
-      case 0: k_mf4<T, TV, TX, kZS2, 0, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 1: k_mf4<T, TV, TX, kZS2, 1, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 2: k_mf4<T, TV, TX, kZS2, 2, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      default: k_mf4<T, TV, TX, kZS2, 3, true><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+      case 0: mft_launch<T, TV, TX, 0, true>(g, x, b, y, v, v2, r0, st); break;
+      case 1: mft_launch<T, TV, TX, 1, true>(g, x, b, y, v, v2, r0, st); break;
+      case 2: mft_launch<T, TV, TX, 2, true>(g, x, b, y, v, v2, r0, st); break;
+      default: mft_launch<T, TV, TX, 3, true>(g, x, b, y, v, v2, r0, st);
     }
   } else {
     switch (mode) {
-      case 0: k_mf4<T, TV, TX, kZS2, 0, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 1: k_mf4<T, TV, TX, kZS2, 1, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      case 2: k_mf4<T, TV, TX, kZS2, 2, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0); break;
-      default: k_mf4<T, TV, TX, kZS2, 3, false><<<grid, kMFThreads, 0, st>>>(g, x, b, y, v, v2, r0);
+      case 0: mft_launch<T, TV, TX, 0, false>(g, x, b, y, v, v2, r0, st); break;
+      case 1: mft_launch<T, TV, TX, 1, false>(g, x, b, y, v, v2, r0, st); break;
+      case 2: mft_launch<T, TV, TX, 2, false>(g, x, b, y, v, v2, r0, st); break;
+      default: mft_launch<T, TV, TX, 3, false>(g, x, b, y, v, v2, r0, st);
     }
   }
 }
@@ -761,7 +1246,7 @@ __global__ void __launch_bounds__(kBlock) k_wd_scale(const float* __restrict__ w
 }
 
 // wd = damping / diagonal of the matrix-free top level, the diagonal formed
-// as in k_mf4 (4 hs times the sum of the node's 8 cell coefficients, summed
+// as in the matrix-free operator (4 hs times the sum of the node's 8 cell coefficients, summed
 // in the same order; cells outside the grid count zero); Dirichlet nodes
 // (identity rows) get the damping itself
 __global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ wd) {
@@ -813,20 +1298,15 @@ void mx_top_apply64(const MFArgs64& g, const float* x, double* y, const float* v
 }
 
 void mx_top_apply64x(const MFArgs64& g, const double* x, double* y, cudaStream_t st) {
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_mf4<double, double, double, kZS2, 0, false><<<mf2_grid(g.M), kMFThreads, 0, st>>>(g, x, nullptr, y, nullptr,
-                                                                                     nullptr, Reduce2{});
+  mf_launch<double, double, double>(0, g, x, nullptr, y, nullptr, nullptr, nullptr, st);
 }
 
 void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, double* r, cudaStream_t st) {
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_mf4<double, double, double, kZS2, 1, false><<<mf2_grid(g.M), kMFThreads, 0, st>>>(g, x, b, r, nullptr, nullptr,
-                                                                                     Reduce2{});
+  mf_launch<double, double, double>(1, g, x, b, r, nullptr, nullptr, nullptr, st);
 }
 
-long long mx_top_blocks(int M) {
-  const dim3 gr = mf2_grid(M);
-  return (long long)gr.x * gr.y * gr.z;
+long long mx_top_blocks(int M) {  // the larger of the two geometries
+  return std::max(mft_blocks(mft_geo(M, 63, true)), mft_blocks(mft_geo(M, 0, false)));
 }
 
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,

@@ -221,6 +221,17 @@ int fmg_l2_norm(const fmg_vec* x, double* out);
 /* ------------------------------------------------------------ operators */
 /* gemm! 1.0 A x 0.0 y on level `level` (sparse-matrix.lisp:392-405) */
 int fmg_matvec(fmg_grid* grid, int level, const fmg_vec* x, fmg_vec* y);
+/* gemm! 1.0 A x 0.0 y on the top level, or with b non-null compute-residual
+   y := b - A x (sparse-matrix.lisp:392-405, linit.lisp:73-80), applied
+   matrix-free from the cell coefficients as fmg_solve_mixed applies its top
+   level: fp32 = 0, FP64 in the difference form of that solve's CG operator;
+   fp32 = 1, FP32 arithmetic on x, b and the coefficients rounded to FP32 (the
+   V-cycle's top level), the result widened; fp32 = 2 (b must be NULL), FP64
+   arithmetic on x rounded to FP32 (the CG operator a = A p of that solve,
+   whose search direction is FP32).  3D scalar Q1 grids with
+   FMG_K_CELL coefficients only (FMG_ERR_UNSUPPORTED otherwise); y must differ
+   from x and b.  Waits for the result. */
+int fmg_matvec_mf(fmg_grid* grid, int fp32, const fmg_vec* x, const fmg_vec* b, fmg_vec* y);
 /* compute-residual r := b - A x (linit.lisp:73-80); b may be r */
 int fmg_residual(fmg_grid* grid, int level, const fmg_vec* x, const fmg_vec* b, fmg_vec* r);
 /* restrict: rc := I^T rf with the constrained interpolation

@@ -1416,6 +1416,66 @@ int ora_coarse_solve(void* h, double damp, double* x, double* r) {
 double ora_dot(const double* x, const double* y, long n) { return dr_dot(x, y, n, false); }
 double ora_dot_par(const double* x, const double* y, long n) { return dr_dot(x, y, n, true); }
 
+extern "C++" {
+namespace {
+template <typename T>
+void mf_apply(int M, int dm, const double* kc, const double* xd, const double* bd, double* y, bool x32) {
+  const int n = M - 1;
+  const long long MM = (long long)M * M, N = MM * M;
+  const T hs = (T)((1.0 / n) / 12.0);
+  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
+  auto xv = [&](long long i) { return x32 ? (T)(float)xd[i] : (T)xd[i]; };
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < N; ++i) {
+    const int ix = (int)(i % M), iy = (int)((i / M) % M), iz = (int)(i / MM);
+    T ax;
+    if (dirf(ix, 1, 2) || dirf(iy, 4, 8) || dirf(iz, 16, 32)) {
+      ax = xv(i);
+    } else {
+      T k[2][2][2];
+      for (int cz = 0; cz < 2; ++cz)
+        for (int cy = 0; cy < 2; ++cy)
+          for (int cx = 0; cx < 2; ++cx) {
+            const int ex = ix - 1 + cx, ey = iy - 1 + cy, ez = iz - 1 + cz;
+            const bool in = ex >= 0 && ex < n && ey >= 0 && ey < n && ez >= 0 && ez < n;
+            k[cz][cy][cx] = in ? (T)kc[ex + (long long)n * (ey + (long long)n * ez)] : T(0);
+          }
+      auto X = [&](int dx, int dy, int dz) -> T {
+        const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+        const bool in = jx >= 0 && jx < M && jy >= 0 && jy < M && jz >= 0 && jz < M && !dirf(jx, 1, 2) &&
+                        !dirf(jy, 4, 8) && !dirf(jz, 16, 32);
+        return in ? xv((long long)jz * MM + (long long)jy * M + jx) : T(0);
+      };
+      constexpr bool DIFF = sizeof(T) == 8;
+      const T wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
+                          {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
+      const T ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
+      const T xc = X(0, 0, 0);
+      T s = T(0);
+      auto term = [&](T w, T xj) { s = DIFF ? std::fma(w, xc - xj, s) : std::fma(w, xj, s); };
+      for (int sy = 0; sy < 2; ++sy)
+        for (int sx = 0; sx < 2; ++sx) term(wc[sy][sx], X(2 * sx - 1, 2 * sy - 1, 0));
+      for (int cz = 0; cz < 2; ++cz) {
+        const int dz = 2 * cz - 1;
+        for (int sx = 0; sx < 2; ++sx) term(k[cz][0][sx] + k[cz][1][sx], X(2 * sx - 1, 0, dz));
+        for (int sy = 0; sy < 2; ++sy) term(k[cz][sy][0] + k[cz][sy][1], X(0, 2 * sy - 1, dz));
+        for (int sy = 0; sy < 2; ++sy)
+          for (int sx = 0; sx < 2; ++sx) term(k[cz][sy][sx], X(2 * sx - 1, 2 * sy - 1, dz));
+      }
+      if (!DIFF) s = std::fma(T(4) * ksum, xc, -s);
+      ax = hs * s;
+    }
+    y[i] = (double)(bd ? (T)bd[i] - ax : ax);
+  }
+}
+}  // namespace
+}  // extern "C++"
+
+void ora_mf_apply(int M, int dmask, const double* k, int fp32, const double* x, const double* b, double* y) {
+  if (fp32 == 1) mf_apply<float>(M, dmask, k, x, b, y, false);
+  else mf_apply<double>(M, dmask, k, x, b, y, fp32 == 2);
+}
+
 int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* r) {
   Hier& H = *(Hier*)h;
   if (!H.assembled) return -1;

@@ -114,6 +114,21 @@ int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* 
 int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hist_len,
               int* nsteps);
 
+/* The 3D Q1 operator of a cell-wise coefficient applied matrix-free, in the
+   operation order of the GPU's matrix-free top level (the operator of its
+   mixed-precision solve; no counterpart in the reference, which always
+   assembles): per node, from the 8 cell coefficients k and the neighbour
+   values x (zero at Dirichlet nodes and outside the grid),
+     wc[sy][sx] = k[0][sy][sx] + k[1][sy][sx],  K = (wc00 + wc01) + (wc10 + wc11),
+     12 face-diagonal and 8 body-diagonal terms in a fixed order, each
+     s = fma(w, x_i - x_j, s) (FP64) or s = fma(w, x_j, s), s = fma(4K, x_i, -s) (FP32),
+     (A x)_i = (h/12) s; Dirichlet rows are identity rows.
+   It equals assemble-interior's matrix (fedisc.lisp:108-206) times x up to
+   rounding.  fp32 = 1: k, x, b and h/12 rounded to FP32 and FP32
+   arithmetic; fp32 = 2: x rounded to FP32, FP64 arithmetic.  b == NULL: y = A x, else y = b - A x.  M nodes a side,
+   k: (M-1)^3 cells, x fastest. */
+void ora_mf_apply(int M, int dmask, const double* k, int fp32, const double* x, const double* b, double* y);
+
 int ora_num_threads(void);
 void ora_set_num_threads(int n);
 

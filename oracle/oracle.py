@@ -91,6 +91,8 @@ def lib():
         L.ora_dot.argtypes = [_dp, _dp, ctypes.c_long]
         L.ora_dot_par.restype = ctypes.c_double
         L.ora_dot_par.argtypes = [_dp, _dp, ctypes.c_long]
+        L.ora_mf_apply.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp]
+        L.ora_mf_apply.restype = None
         L.ora_vcycle.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveCfg), _dp, _dp, _dp]
         L.ora_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveCfg), _dp, _dp, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_int)]
@@ -346,6 +348,20 @@ def dot_par(x, y) -> float:
     x = np.ascontiguousarray(x, dtype=np.float64)
     y = np.ascontiguousarray(y, dtype=np.float64)
     return lib().ora_dot_par(_p(x), _p(y), x.size)
+
+
+def mf_apply(M, dmask, kcell, x, b=None, fp32=False):
+    """The 3D Q1 operator of a cell-wise coefficient applied matrix-free in the
+    GPU's operation order (y = A x, or b - A x); see ora_mf_apply.  fp32:
+    False (FP64), True (FP32 throughout) or 2 (x rounded to FP32, FP64
+    arithmetic)."""
+    k = np.ascontiguousarray(kcell, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+    mode = 2 if fp32 == 2 else (1 if fp32 else 0)
+    lib().ora_mf_apply(int(M), int(dmask), _p(k), mode, _p(x), None if bb is None else _p(bb), _p(y))
+    return y
 
 
 def num_threads() -> int:
