@@ -38,10 +38,10 @@ HBM_FALLBACK_GBS = 6650.0
 JUDGE_STEPS = 1  # CG steps after each (re)start on which the plain cycle judges the learned one
 # DRAM bytes per top-level node of one launch (read + write), from the ncu
 # capture of the 257^3 case (profiles/k_mfc_q1_3d_mixed_257cube.md): mode 2
-# 654.5 MB, FP64 mode 0 322.3 MB, mode 1 268.4 MB over 16,974,593 nodes
-TOP_TRAFFIC_B_PER_NODE = {"k_mfc<float,double,2,1>": 654.5e6 / 16974593,
-                          "k_mfc<double,float,0,1>": 322.3e6 / 16974593,
-                          "k_mfc<float,double,1,0>": 268.4e6 / 16974593}
+# 654.5 MB, FP64 mode 0 320.4 MB, mode 1 268.4 MB over 16,974,593 nodes
+TOP_TRAFFIC_B_PER_NODE = {"k_mfc<float,double,float,2,1,7>": 654.5e6 / 16974593,
+                          "k_mfc<double,float,float,0,1,0>": 320.4e6 / 16974593,
+                          "k_mfc<float,double,float,1,0,0>": 268.4e6 / 16974593}
 
 
 def parse_args():
@@ -502,11 +502,11 @@ def run_mine(args, world, rank, local):
     cells = wl.n_cells ** 3
     top_kernels = []
     for kind, name, alg, per_solve in (
-            (C.FMG_MXK_SMOOTH, "k_mfc<float,double,2,1> (top-level post-smoothing + the flexible CG's (z,r), (z,a))",
+            (C.FMG_MXK_SMOOTH, "k_mfc<float,double,float,2,1,7> (top-level post-smoothing + the flexible CG's (z,r), (z,a))",
              n * (5 * 4 + 2 * 8) + 4 * cells, ninner),
-            (C.FMG_MXK_MATVEC64, "k_mfc<double,float,0,1> (FP64 a = A p of the FP32 direction + (a,p))",
+            (C.FMG_MXK_MATVEC64, "k_mfc<double,float,float,0,1,0> (FP64 a = A p of the FP32 direction + (a,p))",
              n * (4 + 8) + 8 * cells, ninner + 1),
-            (C.FMG_MXK_RESIDUAL, "k_mfc<float,double,1,0> (top-level FP32 residual)", n * 3 * 4 + 4 * cells, ninner + 1)):
+            (C.FMG_MXK_RESIDUAL, "k_mfc<float,double,float,1,0,0> (top-level FP32 residual)", n * 3 * 4 + 4 * cells, ninner + 1)):
         g.mixed_top_kernel(kind, 3)
         t_k, _ = timed(lambda kind=kind: g.mixed_top_kernel(kind, args.matvec_reps), 1)
         t_k /= args.matvec_reps

@@ -149,44 +149,20 @@ __device__ __forceinline__ T mf_out(T ax, T d, T xc, T bb, T o, bool use_wd) {
   return use_wd ? o * bb : o * (bb / d);
 }
 
-// The operator as one launch over two kinds of CTA.
-// Tiled CTAs own a 32 x 16 column of nodes (thread (lx, ly): the y-adjacent
-// nodes 2ly, 2ly+1) and march z through 32 planes.  Each plane reaches shared
-// memory by TMA: its 18 x rows (y0-1 .. y0+16, each one 1D box from the
-// 16-byte boundary at or below node x0-1; rows outside the grid or on a
-// Dirichlet face are fetched from a coordinate below the vector's start, so
-// the copy fills them with zeros) and its 17 x 33 cell tile (one 3D box,
-// cells outside the grid read as zero).  A 5-plane ring keeps three planes in
-// flight.  Once a plane has landed, the CTA packs its x rows (the alignment
-// offset removed, Dirichlet columns zeroed, FP32 values widened for the FP64
-// operator) into a 4-plane ring, the only copy the rows read.  One barrier per
-// plane orders packing, reuse of ring slots and the next copies.
-// The nodes outside the tiled box (the faces x, y or z = 2^L where the box
-// stops short of the grid; the whole grid when it is below 32 cells a side)
-// go to face CTAs that evaluate the same row from global memory, 1024 nodes
-// each.  Every CTA adds its nodes to the two FP64 reductions of R.
 constexpr int kFX = 32, kFY = 16, kFZ = 32;   // tile: nodes along x, y; planes per CTA
 constexpr int kFRows = kFY + 2;               // x rows of a plane (y0-1 .. y0+16)
 constexpr int kFCRows = kFY + 1;              // cell rows of a plane (y0-1 .. y0+15)
 constexpr int kFPW = kFX + 2;                 // packed row: x0-1 .. x0+32
-constexpr int kFRing = 5, kFPack = 4;         // staged planes, packed planes
 constexpr int kFThreads = 256;
 constexpr int kFaceNodes = 1024;              // nodes per face CTA
-constexpr int kZeroRow = -4096;               // row coordinate whose whole box lies below the vector
 
-template <typename T, typename TX>
-struct MftLayout {
-  static constexpr int XA = 16 / (int)sizeof(TX);           // row copies start on 16-byte boundaries
-  static constexpr int XW = sizeof(TX) == 4 ? 40 : 36;      // elements per row copy: 34 + the offset
-  static constexpr int XP = sizeof(TX) == 4 ? 256 : 384;    // bytes per staged row (128-byte aligned copies)
-  static constexpr int CW = sizeof(T) == 4 ? 36 : 34;       // cells per copied row, from cell x0-1-COFF
-  static constexpr int COFF = sizeof(T) == 4 ? 3 : 1;       // where cell x0-1 sits in a copied row
-  static constexpr int XB = kFRows * XP;                    // x rows of a staged plane
-  static constexpr int CB = (kFCRows * CW * (int)sizeof(T) + 127) / 128 * 128;
-  static constexpr int SB = XB + CB;                        // bytes per staged plane
-  static constexpr int PS = kFRows * kFPW;                  // elements per packed plane
-  static constexpr int SMEM = kFRing * SB + kFPack * PS * (int)sizeof(T) + kFRing * 8 + 128;
-  static constexpr uint32_t XTX = kFRows * XW * sizeof(TX), CTX = kFCRows * CW * sizeof(T);
+// the cell tile of a plane as one TMA box: cells x0-1-COFF .. x0-1-COFF+CW-1
+// (the box starts on a 16-byte boundary), rows y0-1 .. y0+15
+template <typename T>
+struct CellBox {
+  static constexpr int CW = sizeof(T) == 4 ? 36 : 34;       // cells per row
+  static constexpr int COFF = sizeof(T) == 4 ? 3 : 1;       // where cell x0-1 sits in a row
+  static constexpr uint32_t CTX = kFCRows * CW * sizeof(T);  // bytes per box
 };
 
 struct MftGeo {
@@ -287,204 +263,37 @@ __device__ __forceinline__ void mf_face_cta(const MFArgsT<T>& g, const MftGeo& g
   }
 }
 
-template <typename T, typename TV, typename TX, int MODE, bool RED>
-__global__ void __launch_bounds__(kFThreads, 2)
-k_mft(MFArgsT<T> g, const __grid_constant__ CUtensorMap tx_rows, const __grid_constant__ CUtensorMap tk_cells,
-      MftGeo geo, const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y,
-      const TV* __restrict__ v, const TV* __restrict__ v2, Reduce2 R) {
-  typedef MftLayout<T, TX> L;
-  constexpr bool HX = MODE != 3;
-  constexpr bool HB = MODE != 0;
-  constexpr bool DIFF = sizeof(T) == 8;
-  constexpr bool HO = MODE == 2 || MODE == 3;
-  extern __shared__ __align__(128) unsigned char sm_dyn[];
-  __shared__ double red[8];
-  // the copies land on 128-byte boundaries: round the base up (the launch adds 128 bytes)
-  unsigned char* sm = sm_dyn + ((128u - (umma::smem_u32(sm_dyn) & 127u)) & 127u);
-  const int tid = threadIdx.x;
-  const int M = g.M, n = g.n, dm = g.dmask;
-  const long long MM = (long long)M * M;
-  auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-  const bool omv = g.omega != nullptr, uwd = g.wd != nullptr;
-  const T hs = g.hs;
-  double acc0 = 0.0, acc1 = 0.0;
-  auto opnd = [&](long long i, T& bb, T& o) {  // per-node right-hand side and damping
-    bb = HB ? __ldg(b + i) : T(0);
-    o = (HO && uwd) ? __ldg(g.wd + i) : ((HO && omv) ? __ldg(g.omega + i) : g.w);
-  };
-  auto emit = [&](long long i, T out, TV vv, TV vv2) {
-    y[i] = out;
-    if (RED) {
-      acc0 = fma((double)out, (double)vv, acc0);
-      if (v2) acc1 = fma((double)out, (double)vv2, acc1);
-    }
-  };
-  if ((int)blockIdx.x >= geo.nface) {
-    // ------------------------------------------------------------ tiled CTA
-    const int bid = (int)blockIdx.x - geo.nface;
-    const int bx = bid % geo.nbx, by = (bid / geo.nbx) % geo.nby, bz = bid / (geo.nbx * geo.nby);
-    const int x0 = bx * kFX, y0 = by * kFY, z0 = bz * kFZ;
-    const int lx = tid & 31, ly = tid >> 5;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFRing * L::SB + kFPack * L::PS * sizeof(T));
-    T* pk = reinterpret_cast<T*>(sm + kFRing * L::SB);
-    if (tid == 0)
-      for (int s = 0; s < kFRing; ++s) umma::mbar_init(&bar[s]);
-    __syncthreads();
-    // stage j: x plane z0-1+j and cell plane z0-2+j, ring slot j % kFRing
-    auto issue = [&](int j) {  // warp 0
-      unsigned char* st = sm + (j % kFRing) * L::SB;
-      uint64_t* bj = bar + j % kFRing;
-      if (lx == 0) {
-        umma::fence_async_smem();
-        umma::mbar_arrive_expect_tx(bj, (HX ? L::XTX : 0u) + L::CTX);
-      }
-      __syncwarp();
-      if (HX && lx < kFRows) {
-        const int z = z0 - 1 + j, yy = y0 - 1 + lx;
-        const bool ok = z >= 0 && z < M && yy >= 0 && yy < M && !dirf(z, 16, 32) && !dirf(yy, 4, 8);
-        const long long lin = (long long)z * MM + (long long)yy * M + x0 - 1;
-        umma::tma_load_1d(st + lx * L::XP, &tx_rows, bj, ok ? (int)(lin & ~(long long)(L::XA - 1)) : kZeroRow);
-      }
-      if (lx == 31) umma::tma_load_3d(st + L::XB, &tk_cells, bj, x0 - 1 - L::COFF, y0 - 1, z0 - 2 + j);
-    };
-    // packing: thread tid handles packed elements tid, tid+256, tid+512 of a plane
-    int proff[3], plo[3];
-    bool pmask[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int e = tid + q * kFThreads;
-      const int r = e / kFPW, jj = e - r * kFPW;
-      const int xx = x0 - 1 + jj, yy = y0 - 1 + r;
-      proff[q] = r * (L::XP / (int)sizeof(TX)) + jj;
-      plo[q] = (int)(((long long)yy * M + x0 - 1) & (L::XA - 1));
-      pmask[q] = xx < 0 || (xx == 0 && (dm & 1)) || (xx == M - 1 && (dm & 2));
-    }
-    auto pack = [&](int j) {
-      const TX* raw = reinterpret_cast<const TX*>(sm + (j % kFRing) * L::SB);
-      T* P = pk + (j % kFPack) * L::PS;
-      const int zlo = (int)(((long long)(z0 - 1 + j) * MM) & (L::XA - 1));
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int e = tid + q * kFThreads;
-        if (q < 2 || e < L::PS) {
-          const TX xv = raw[proff[q] + ((zlo + plo[q]) & (L::XA - 1))];
-          P[e] = pmask[q] ? T(0) : (T)xv;
-        }
-      }
-    };
-    auto wait = [&](int j) { return umma::mbar_wait(bar + j % kFRing, (uint32_t)((j / kFRing) & 1)); };
-    const int last = kFZ + 1;  // the last stage a CTA needs
-    if (tid < 32)
-      for (int j = 0; j < kFRing; ++j) issue(j);
-    int issued = kFRing - 1, waited = 1;
-    bool ok = wait(0);
-    if (HX) pack(0);
-    ok = wait(1) && ok;
-    if (HX) pack(1);
-    const int ix = x0 + lx, iy0 = y0 + 2 * ly;
-    const bool dirx = dirf(ix, 1, 2);
-    const bool diry[2] = {dirf(iy0, 4, 8), dirf(iy0 + 1, 4, 8)};
-    struct Ops { T b[2], o[2]; TV v[2], v2[2]; };
-    auto ldops = [&](int jz, Ops& o) {
-      if (jz >= z0 + kFZ) return;
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const long long i = (long long)jz * MM + (long long)(iy0 + r) * M + ix;
-        opnd(i, o.b[r], o.o[r]);
-        o.v[r] = RED ? __ldg(v + i) : TV(0);
-        o.v2[r] = (RED && v2) ? __ldg(v2 + i) : TV(0);
-      }
-    };
-    Ops cur, nxt;
-    ldops(z0, cur);
-    bool bad = false;
-#pragma unroll 1
-    for (int t = 0; t < kFZ; ++t) {
-      const int iz = z0 + t;
-      ok = wait(t + 2) && ok;
-      waited = t + 2;
-      if (HX) pack(t + 2);
-      if (__syncthreads_or(!ok)) {  // a copy that never landed: stop issuing
-        bad = true;
-        break;
-      }
-      if (t + kFRing <= last) {  // slot t % kFRing: stage t's cells and rows were last read in step t-1
-        if (tid < 32) issue(t + kFRing);
-        issued = t + kFRing;
-      }
-      ldops(iz + 1, nxt);
-      const T* X0 = pk + (t % kFPack) * L::PS;         // x plane iz-1
-      const T* X1 = pk + ((t + 1) % kFPack) * L::PS;   // x plane iz
-      const T* X2 = pk + ((t + 2) % kFPack) * L::PS;   // x plane iz+1
-      const T* K0 = reinterpret_cast<const T*>(sm + ((t + 1) % kFRing) * L::SB + L::XB);  // cell plane iz-1
-      const T* K1 = reinterpret_cast<const T*>(sm + ((t + 2) % kFRing) * L::SB + L::XB);  // cell plane iz
-      const bool dirz = dirf(iz, 16, 32);
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const long long i = (long long)iz * MM + (long long)(iy0 + r) * M + ix;
-        T ax, d, xc;
-        if (dirz || dirx || diry[r]) {  // identity row; the packed planes hold zero here
-          xc = HX ? (T)x[i] : T(0);
-          ax = xc;
-          d = T(1);
-        } else {
-          const int h = (2 * ly + r + 1) * kFPW + lx + 1;
-          const int kc = (2 * ly + r) * L::CW + lx + L::COFF;
-          T k[2][2][2];
-#pragma unroll
-          for (int cz = 0; cz < 2; ++cz)
-#pragma unroll
-            for (int cy = 0; cy < 2; ++cy)
-#pragma unroll
-              for (int cx = 0; cx < 2; ++cx) k[cz][cy][cx] = (cz ? K1 : K0)[kc + cy * L::CW + cx];
-          auto X = [&](int dx, int dy, int dz) -> T {
-            return (dz < 0 ? X0 : (dz > 0 ? X2 : X1))[h + dy * kFPW + dx];
-          };
-          mf_row<T, HX, DIFF>(k, X, hs, ax, d, xc);
-        }
-        emit(i, mf_out<MODE>(ax, d, xc, cur.b[r], cur.o[r], uwd), cur.v[r], cur.v2[r]);
-      }
-      cur = nxt;
-    }
-    if (bad) {  // let the copies in flight land (bounded) before the CTA's shared memory is released
-      if (tid == 0) {
-        for (int j = waited + 1; j <= issued; ++j) umma::mbar_wait(bar + j % kFRing, (uint32_t)((j / kFRing) & 1));
-        if (g.err) *g.err = 1.0;
-      }
-      __syncthreads();
-    }
-  } else {
-    // -------------------------------------------------------------- face CTA
-    mf_face_cta<T, TV, TX, MODE, RED>(g, geo, (int)blockIdx.x, x, b, y, v, v2, acc0, acc1);
-  }
-  if (RED) dr_finish2(acc0, acc1, R, red);
-}
-
-// FP32 form of the operator, fed by asynchronous copies three planes ahead.
-// Same tiles and face CTAs as k_mft.  A stage of the 6-slot shared-memory
-// ring holds what one step reads: the 18 x 34 x halo of the plane above
-// (cp.async, 4 bytes per element, eliminated and outside entries zero-filled
-// at the copy), the 17 x 36 cell tile (one TMA box) and the per-node operands
-// of the step's own plane (b, the damping, the two FP64 reduction vectors:
-// each thread copies its own two nodes').  All copies of a stage complete on
-// its full mbarrier (256 cp.async arrivals + the TMA's expect-tx arrival);
-// each warp releases a stage on its empty mbarrier once it has read it, and
-// a slot is refilled only after all 8 warps have released it, so warps drift
-// apart freely by a few steps and no block barrier is needed.  A thread keeps
-// the x values and cells its two nodes read in registers as it marches z,
-// reading each plane once (the loop runs six steps per turn so register roles
-// rotate at compile time).  Dirichlet nodes of the tile (on the faces x, y,
-// z = 0) are left to the face CTAs, which evaluate identity rows.
+// The operator as one launch over two kinds of CTA.  Tiled CTAs own a 32 x 16
+// column of nodes (thread (lx, ly): the y-adjacent nodes 2ly, 2ly+1) and
+// march z through 32 planes.  Face CTAs (first in the grid) evaluate, from
+// global memory, the nodes outside the tiled box -- the faces x, y or z = 2^L
+// where the box stops short of the grid, the whole grid when it is below 32
+// cells a side -- and the Dirichlet faces x, y, z = 0 inside it (identity
+// rows), 1024 nodes each.  FP32 arithmetic, or FP64 in difference form with
+// each x value widened once as it enters the registers.
+// A stage of a tiled CTA's 6-slot shared-memory ring holds what one step
+// reads: the 18 x 34 x halo of the plane above (cp.async per element,
+// eliminated and outside entries zero-filled at the copy), the 17 x 36 cell
+// tile (one TMA box) and the per-node operands of the step's own plane (b, the
+// damping, the FP64 reduction vectors: each thread copies its own two
+// nodes').  All copies of a stage complete on its full mbarrier (256 cp.async
+// arrivals + the TMA's expect-tx arrival); each warp releases a stage on its
+// empty mbarrier once it has read it, and a slot is refilled only after all 8
+// warps have released it, so warps drift apart by a few steps and no block
+// barrier is needed.  Stages are requested three steps before they are read.
+// A thread keeps the x values and cells its two nodes read in registers as it
+// marches z, reading each plane once (the loop runs three steps per turn so
+// register roles rotate at compile time).
 constexpr int kCRing = 6;   // ring slots
 constexpr int kCLook = 5;   // stage j is requested at step j-5 and read at step j-2
 constexpr int kPX = kFPW;   // packed x row: x0-1 .. x0+32
 
-template <typename T, typename TV, int MODE, bool RED>
+template <typename T, typename TV, typename TX, int MODE, bool RED>
 struct MfcLayout {
   static constexpr bool HB = MODE != 0, HO = MODE == 2 || MODE == 3, HX = MODE != 3;
   static constexpr int up(int b) { return (b + 127) / 128 * 128; }
-  static constexpr int XS = HX ? up(kFRows * kPX * 4) : 0;         // packed x halo
-  static constexpr int CS = up(kFCRows * MftLayout<T, float>::CW * (int)sizeof(T));  // cell box (TMA)
+  static constexpr int XS = HX ? up(kFRows * kPX * (int)sizeof(TX)) : 0;  // packed x halo
+  static constexpr int CS = up(kFCRows * CellBox<T>::CW * (int)sizeof(T));  // cell box (TMA)
   static constexpr int OB = HB ? up(2 * kFThreads * (int)sizeof(T)) : 0;  // b of the step's plane
   static constexpr int OO = HO ? up(2 * kFThreads * (int)sizeof(T)) : 0;  // damping
   static constexpr int OV = RED ? up(2 * kFThreads * (int)sizeof(TV)) : 0;  // reduction vectors
@@ -504,15 +313,18 @@ __device__ __forceinline__ void cpa_arrive(uint64_t* bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(umma::smem_u32(bar)) : "memory");
 }
 
-template <typename T, typename TV, int MODE, bool RED>
-__global__ void __launch_bounds__(kFThreads, 2)
-k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, const float* __restrict__ x,
+// OPT: 1 per-node damping present (g.wd or g.omega), 2 a second reduction
+// vector, 4 the damping already divided by the diagonal (g.wd)
+template <typename T, typename TV, typename TX, int MODE, bool RED, int OPT>
+__global__ void __launch_bounds__(kFThreads, (sizeof(T) == 4 && MODE != 2) ? 3 : 2)
+k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, const TX* __restrict__ x,
       const T* __restrict__ b, T* __restrict__ y, const TV* __restrict__ v, const TV* __restrict__ v2,
       Reduce2 R) {
-  typedef MfcLayout<T, TV, MODE, RED> L;
-  typedef MftLayout<T, float> LC;
+  typedef MfcLayout<T, TV, TX, MODE, RED> L;
+  typedef CellBox<T> LC;
   constexpr bool DIFF = sizeof(T) == 8;  // the FP64 operator in difference form
   constexpr bool HX = L::HX, HB = L::HB, HO = L::HO;
+  constexpr bool OM = HO && (OPT & 1), V2 = RED && (OPT & 2), UWD = HO && (OPT & 4);
   extern __shared__ __align__(128) unsigned char sm_dyn[];
   __shared__ double red[8];
   unsigned char* sm = sm_dyn + ((128u - (umma::smem_u32(sm_dyn) & 127u)) & 127u);
@@ -522,8 +334,7 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     const int M = g.M, dm = g.dmask;
     const long long MM = (long long)M * M;
     auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
-    const bool uwd = g.wd != nullptr;
-    const T* om_src = uwd ? g.wd : g.omega;  // per-node damping source, if any
+    const T* om_src = UWD ? g.wd : g.omega;  // per-node damping source (OM)
     const T hs = g.hs;
     const int bid = (int)blockIdx.x - geo.nface;
     const int bx = bid % geo.nbx, by = (bid / geo.nbx) % geo.nby, bz = bid / (geo.nbx * geo.nby);
@@ -553,13 +364,17 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     const long long ibase = (long long)iy0 * M + ix;
     bool ok = true;  // every wait of this warp so far completed; after one gives up, the rest wait 1 ms at most
     auto wait = [&](uint64_t* bar, uint32_t parity) {
-      const bool w = ok ? umma::mbar_wait(bar, parity) : umma::mbar_wait_for(bar, parity, 1 << 16, 1000000ull);
+      bool w = umma::mbar_test(bar, parity);
+      if (!w) w = ok ? umma::mbar_wait(bar, parity) : umma::mbar_wait_for(bar, parity, 1 << 16, 1000000ull);
       ok = __all_sync(0xffffffffu, w) && ok;
     };
-    // stage j: x plane z0-1+j, cell plane z0-2+j, operands of plane z0-2+j; slot j % kCRing
+    // stage j: x plane z0-1+j, cell plane z0-2+j, operands of plane z0-2+j, in
+    // ring slot j % kCRing; the issue and read streams count slots and phases
+    int is = 0, rs = 0;          // slot of the next stage to request / to read
+    uint32_t ip = 0u, rp = 0u;   // its phase parity
     auto issue = [&](int j) {
-      const int s = j % kCRing;
-      if (j >= kCRing) wait(&empty[s], (uint32_t)(((j / kCRing) - 1) & 1));  // all warps released the slot
+      const int s = is;
+      if (j >= kCRing) wait(&empty[s], ip ^ 1u);  // all warps released the slot's previous stage
       unsigned char* st = sm + s * L::SB;
       if (tid == 0) {
         umma::fence_async_smem();
@@ -569,12 +384,12 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
       if (HX) {
         const int z = z0 - 1 + j;
         const bool zok = z >= 0 && z < M && !dirf(z, 16, 32);
-        const float* pl = x + (zok ? (long long)z * MM : 0ll);
-        float* xs = reinterpret_cast<float*>(st);
+        const TX* pl = x + (zok ? (long long)z * MM : 0ll);
+        TX* xs = reinterpret_cast<TX*>(st);
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
           const int e = tid + q * kFThreads;
-          if (q < 2 || e < kFRows * kPX) cpa(xs + e, pl + hoff[q], zok && hok[q], 4);
+          if (q < 2 || e < kFRows * kPX) cpa(xs + e, pl + hoff[q], zok && hok[q], (int)sizeof(TX));
         }
       }
       const int zo = z0 - 2 + j;  // the operands' plane
@@ -585,22 +400,22 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
           const long long i = (long long)zo * MM + ibase + r * M;
           const int k = r * kFThreads + tid;
           if (HB) cpa(reinterpret_cast<T*>(op) + k, b + i, true, (int)sizeof(T));
-          if (HO) cpa(reinterpret_cast<T*>(op + L::OB) + k, om_src ? om_src + i : b, om_src != nullptr, (int)sizeof(T));
-          if (RED) {
-            cpa(reinterpret_cast<TV*>(op + L::OB + L::OO) + k, v + i, true, (int)sizeof(TV));
-            cpa(reinterpret_cast<TV*>(op + L::OB + L::OO + L::OV) + k, v2 ? v2 + i : v, v2 != nullptr,
-                (int)sizeof(TV));
-          }
+          if (OM) cpa(reinterpret_cast<T*>(op + L::OB) + k, om_src + i, true, (int)sizeof(T));
+          if (RED) cpa(reinterpret_cast<TV*>(op + L::OB + L::OO) + k, v + i, true, (int)sizeof(TV));
+          if (V2) cpa(reinterpret_cast<TV*>(op + L::OB + L::OO + L::OV) + k, v2 + i, true, (int)sizeof(TV));
         }
       }
       cpa_arrive(&full[s]);
+      if (++is == kCRing) {
+        is = 0;
+        ip ^= 1u;
+      }
     };
-    auto consume = [&](int j, T (&xv)[4][3], T (&kv)[3][2], bool want_k) {
-      const int s = j % kCRing;
-      wait(&full[s], (uint32_t)((j / kCRing) & 1));
-      const unsigned char* st = sm + s * L::SB;
+    auto consume = [&](T (&xv)[4][3], T (&kv)[3][2], bool want_k) {  // the next stage in the read stream
+      wait(&full[rs], rp);
+      const unsigned char* st = sm + rs * L::SB;
       if (HX) {
-        const float* xs = reinterpret_cast<const float*>(st);
+        const TX* xs = reinterpret_cast<const TX*>(st);
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
@@ -614,16 +429,20 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
           for (int c = 0; c < 2; ++c) kv[r][c] = cs[(2 * ly + r) * LC::CW + lx + c + LC::COFF];
       }
     };
-    auto release = [&](int j) {
+    auto release = [&]() {  // the stage just read; the read stream moves on
       __syncwarp();
-      if (lx == 0) umma::mbar_arrive(&empty[j % kCRing]);
+      if (lx == 0) umma::mbar_arrive(&empty[rs]);
+      if (++rs == kCRing) {
+        rs = 0;
+        rp ^= 1u;
+      }
     };
-    T xr[3][4][3], kr[2][3][2];
+    T xr[3][4][3], kr[3][3][2];
     for (int j = 0; j < kCLook && j <= last; ++j) issue(j);
-    consume(0, xr[0], kr[1], false);  // x plane z0-1 (its cell plane is not read)
-    release(0);
-    consume(1, xr[1], kr[0], true);   // x plane z0, cell plane z0-1
-    release(1);
+    consume(xr[0], kr[1], false);  // stage 0: x plane z0-1 (its cell plane is not read)
+    release();
+    consume(xr[1], kr[0], true);   // stage 1: x plane z0, cell plane z0-1
+    release();
     const bool dirx = dirf(ix, 1, 2);
     const bool diry0 = dirf(iy0, 4, 8), diry1 = dirf(iy0 + 1, 4, 8);
     // step t (plane z0+t): x planes iz-1, iz, iz+1 in xr[t%3], xr[(t+1)%3],
@@ -631,21 +450,21 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     // kr[(t+1)%2] (the last one read now); the operands come with stage t+2
     auto step = [&](auto Qc, int t) {
       constexpr int Q = decltype(Qc)::value;
-      constexpr int PM = Q % 3, P0 = (Q + 1) % 3, PP = (Q + 2) % 3, CM = Q % 2, C0 = (Q + 1) % 2;
+      constexpr int PM = Q % 3, P0 = (Q + 1) % 3, PP = (Q + 2) % 3, CM = Q % 3, C0 = (Q + 1) % 3;
       if (t + kCLook <= last) issue(t + kCLook);
-      consume(t + 2, xr[PP], kr[C0], true);
-      const unsigned char* op = sm + ((t + 2) % kCRing) * L::SB + L::XS + L::CS;
+      consume(xr[PP], kr[C0], true);  // stage t+2
+      const unsigned char* op = sm + rs * L::SB + L::XS + L::CS;
       T bb[2], oo[2];
       TV vv[2], vv2[2];
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         const int k = r * kFThreads + tid;
         bb[r] = HB ? reinterpret_cast<const T*>(op)[k] : T(0);
-        oo[r] = HO ? (om_src ? reinterpret_cast<const T*>(op + L::OB)[k] : g.w) : T(0);
+        oo[r] = OM ? reinterpret_cast<const T*>(op + L::OB)[k] : g.w;
         vv[r] = RED ? reinterpret_cast<const TV*>(op + L::OB + L::OO)[k] : TV(0);
-        vv2[r] = (RED && v2) ? reinterpret_cast<const TV*>(op + L::OB + L::OO + L::OV)[k] : TV(0);
+        vv2[r] = V2 ? reinterpret_cast<const TV*>(op + L::OB + L::OO + L::OV)[k] : TV(0);
       }
-      release(t + 2);
+      release();
       const int iz = z0 + t;
       const bool dirz = dirf(iz, 16, 32);
       const long long i0 = (long long)iz * MM + ibase;
@@ -664,12 +483,12 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
         };
         T ax, d, xc;
         mf_row<T, HX, DIFF>(k, X, hs, ax, d, xc);
-        const T out = mf_out<MODE>(ax, d, xc, bb[r], oo[r], uwd);
+        const T out = mf_out<MODE>(ax, d, xc, bb[r], oo[r], UWD);
         if (!(dirz || dirx || (r ? diry1 : diry0))) {  // identity rows: the face CTAs
           y[i0 + r * M] = out;
           if (RED) {
             acc0 = fma((double)out, (double)vv[r], acc0);
-            if (v2) acc1 = fma((double)out, (double)vv2[r], acc1);
+            if (V2) acc1 = fma((double)out, (double)vv2[r], acc1);
           }
         }
       }
@@ -682,24 +501,18 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     typedef std::integral_constant<int, 5> Q5;
     int t = 0;
 #pragma unroll 1
-    for (; t + 6 <= kFZ; t += 6) {
+    for (; t + 3 <= kFZ; t += 3) {
       step(Q0{}, t);
       step(Q1{}, t + 1);
       step(Q2{}, t + 2);
-      step(Q3{}, t + 3);
-      step(Q4{}, t + 4);
-      step(Q5{}, t + 5);
     }
-    if constexpr (kFZ % 6 > 0) step(Q0{}, t);
-    if constexpr (kFZ % 6 > 1) step(Q1{}, t + 1);
-    if constexpr (kFZ % 6 > 2) step(Q2{}, t + 2);
-    if constexpr (kFZ % 6 > 3) step(Q3{}, t + 3);
-    if constexpr (kFZ % 6 > 4) step(Q4{}, t + 4);
+    if constexpr (kFZ % 3 > 0) step(Q0{}, t);
+    if constexpr (kFZ % 3 > 1) step(Q1{}, t + 1);
     // every stage requested has been waited for; a wait that gave up voids the results
     asm volatile("cp.async.wait_all;" ::: "memory");
     if (__syncthreads_or(!ok) && tid == 0 && g.err) *g.err = 1.0;
   } else {
-    mf_face_cta<T, TV, float, MODE, RED>(g, geo, (int)blockIdx.x, x, b, y, v, v2, acc0, acc1);
+    mf_face_cta<T, TV, TX, MODE, RED>(g, geo, (int)blockIdx.x, x, b, y, v, v2, acc0, acc1);
   }
   if (RED) dr_finish2(acc0, acc1, R, red);
 }
@@ -1111,11 +924,9 @@ k_dot2_64(const double* __restrict__ xv, const float* __restrict__ yv, const dou
 
 static inline unsigned g1(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
-// the tiled box of k_mft: whole 32 x 16 x 32 tiles from the origin, the rest
-// to face CTAs (all of it when a side is below a tile)
-// drop_dir: the tiled CTAs leave the Dirichlet faces x, y, z = 0 of their box
-// to the face CTAs (k_mfc); otherwise they evaluate those identity rows (k_mft)
-static MftGeo mft_geo(int M, int dmask, bool drop_dir) {
+// the tiled box (whole 32 x 16 x 32 tiles from the origin) and the nodes left
+// to the face CTAs: outside the box, and its Dirichlet faces x, y, z = 0
+static MftGeo mft_geo(int M, int dmask) {
   MftGeo q{};
   const int n = M - 1;
   q.nbx = n / kFX;
@@ -1126,7 +937,7 @@ static MftGeo mft_geo(int M, int dmask, bool drop_dir) {
   q.X1 = (long long)q.nbx * kFX;
   q.Y1 = (long long)q.nby * kFY;
   q.Z1 = (long long)q.nbz * kFZ;
-  if (q.nmain > 0 && drop_dir) {
+  if (q.nmain > 0) {
     q.ax = (dmask & 1) ? 1 : 0;
     q.ay = (dmask & 4) ? 1 : 0;
     q.az = (dmask & 16) ? 1 : 0;
@@ -1155,26 +966,16 @@ static CUtensorMapDataType tm_type() {
   return sizeof(E) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
 }
 
-// the vector as one dimension, boxes of one staged row; the cells as
-// n x n x n, boxes of one plane's cell tile; everything outside reads as zero
-template <typename T, typename TX>
-static bool mft_maps(const TX* x, long long N, const T* k, int n, CUtensorMap* tr, CUtensorMap* tk) {
-  typedef MftLayout<T, TX> L;
+// the cells as n x n x n, boxes of one plane's cell tile; cells outside
+// read as zero
+template <typename T>
+static bool cell_map(const T* k, int n, CUtensorMap* tk) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
   if (!enc) return false;
   const cuuint32_t one[3] = {1, 1, 1};
-  if (x) {
-    const cuuint64_t dims[1] = {(cuuint64_t)N};
-    const cuuint64_t strides[1] = {0};
-    const cuuint32_t box[1] = {(cuuint32_t)L::XW};
-    if (enc(tr, tm_type<TX>(), 1, const_cast<TX*>(x), dims, strides, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return false;
-  }
   const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)n};
   const cuuint64_t strides[2] = {(cuuint64_t)n * sizeof(T), (cuuint64_t)n * n * sizeof(T)};
-  const cuuint32_t box[3] = {(cuuint32_t)L::CW, (cuuint32_t)kFCRows, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)CellBox<T>::CW, (cuuint32_t)kFCRows, 1};
   return enc(tk, tm_type<T>(), 3, const_cast<T*>(k), dims, strides, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
@@ -1183,33 +984,37 @@ static bool mft_maps(const TX* x, long long N, const T* k, int n, CUtensorMap* t
 template <typename T, typename TV, typename TX, int MODE, bool RED>
 static void mft_launch(const MFArgsT<T>& g, const TX* x, const T* b, T* y, const TV* v, const TV* v2,
                        const Reduce2& R, cudaStream_t st) {
-  typedef MftLayout<T, TX> L;
-  constexpr bool F32 = sizeof(TX) == 4;  // an FP32 x: the cp.async-fed form (its x halo needs no map)
-  MftGeo q = mft_geo(g.M, g.dmask, F32);
-  CUtensorMap tr{}, tk{};
-  // the tensor maps need 16-byte aligned bases; without them every node goes to the face CTAs
-  if (q.nmain > 0 && !mft_maps<T, TX>((MODE != 3 && !F32) ? x : nullptr, g.N, g.k, g.n, &tr, &tk)) {
+  MftGeo q = mft_geo(g.M, g.dmask);
+  CUtensorMap tk{};
+  // the cell map needs a 16-byte aligned base; without it every node goes to the face CTAs
+  if (q.nmain > 0 && !cell_map<T>(g.k, g.n, &tk)) {
     q = MftGeo{};
     q.F = g.N;
     q.nface = (int)((q.F + kFaceNodes - 1) / kFaceNodes);
   }
-  static unsigned attr_set = 0;  // devices the shared-memory size was raised on
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 32 && !((attr_set >> dev) & 1u)) {
-    if constexpr (F32)
-      cudaFuncSetAttribute(k_mfc<T, TV, MODE, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           MfcLayout<T, TV, MODE, RED>::SMEM);
-    else
-      cudaFuncSetAttribute(k_mft<T, TV, TX, MODE, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-    attr_set |= 1u << dev;
-  }
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  if constexpr (F32) {
-    k_mfc<T, TV, MODE, RED><<<mft_blocks(q), kFThreads, MfcLayout<T, TV, MODE, RED>::SMEM, st>>>(
-        g, tk, q, reinterpret_cast<const float*>(x), b, y, v, v2, R);
-  } else {
-    k_mft<T, TV, TX, MODE, RED><<<mft_blocks(q), kFThreads, L::SMEM, st>>>(g, tr, tk, q, x, b, y, v, v2, R);
+  constexpr bool HO = MODE == 2 || MODE == 3;
+  const int opt = (HO && (g.wd || g.omega) ? 1 : 0) | (RED && v2 ? 2 : 0) | (HO && g.wd ? 4 : 0);
+  auto go = [&](auto oc) {
+    constexpr int OPT = decltype(oc)::value;
+    auto kern = k_mfc<T, TV, TX, MODE, RED, OPT>;
+    constexpr int smem = MfcLayout<T, TV, TX, MODE, RED>::SMEM;
+    static unsigned attr = 0;  // devices the shared-memory size was raised on
+    if (dev < 32 && !((attr >> dev) & 1u)) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      attr |= 1u << dev;
+    }
+    kern<<<mft_blocks(q), kFThreads, smem, st>>>(g, tk, q, x, b, y, v, v2, R);
+  };
+  switch (opt) {
+    case 1: if constexpr (HO) go(std::integral_constant<int, 1>{}); break;
+    case 2: if constexpr (RED) go(std::integral_constant<int, 2>{}); break;
+    case 3: if constexpr (HO && RED) go(std::integral_constant<int, 3>{}); break;
+    case 5: if constexpr (HO) go(std::integral_constant<int, 5>{}); break;
+    case 7: if constexpr (HO && RED) go(std::integral_constant<int, 7>{}); break;
+    default: go(std::integral_constant<int, 0>{});
   }
 }
 
@@ -1305,9 +1110,7 @@ void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, doub
   mf_launch<double, double, double>(1, g, x, b, r, nullptr, nullptr, nullptr, st);
 }
 
-long long mx_top_blocks(int M) {  // the larger of the two geometries
-  return std::max(mft_blocks(mft_geo(M, 63, true)), mft_blocks(mft_geo(M, 0, false)));
-}
+long long mx_top_blocks(int M) { return mft_blocks(mft_geo(M, 63)); }  // the most face CTAs any mask gives
 
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
                     const double* v, const double* v2, const Reduce2* R, cudaStream_t st) {

@@ -164,6 +164,17 @@ __device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, in
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return mbar_wait_for(bar, parity, kSpinLimit, kWaitNs);
 }
+// one test of the phase (no wait loop, no clock read): the fast path of a
+// wait whose phase has usually completed already
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
 
 // one plain arrival on the mbarrier
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
