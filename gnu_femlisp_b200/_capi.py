@@ -103,6 +103,10 @@ SIGNATURES = {
     "fmg_matvec": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "fmg_residual": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
     "fmg_matvec_mf": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
+    "fmg_batch_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "fmg_batch_load": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "fmg_batch_solve": (ctypes.c_int, [_vp, ctypes.c_void_p, _vp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
     "fmg_restrict": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "fmg_prolongate": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "fmg_jacobi": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp]),

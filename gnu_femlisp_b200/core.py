@@ -138,6 +138,42 @@ class Grid:
         self.n_cells = n0 << level
         self.assembled = False
 
+    nb = 1  # problems held (a batch: ``Grid.batch``)
+
+    @classmethod
+    def batch(cls, like: "Grid", nbatch: int) -> "Grid":
+        """``fmg_batch_create``: nbatch independent problems with the geometry
+        of ``like`` (1D/2D scalar Q1), loaded one by one from assembled grids
+        (``batch_load``) and solved together (``batch_solve``)."""
+        g = cls.__new__(cls)
+        g.ctx, g.dim, g.order, g.top, g.base, g.nc = like.ctx, like.dim, like.order, like.top, like.base, 1
+        h = ctypes.c_void_p()
+        like.ctx.check(like._lib.fmg_batch_create(like.h, int(nbatch), ctypes.byref(h)), "batch_create")
+        g.h = h
+        g.n_cells = like.n_cells
+        g.assembled = False
+        g.nb = int(nbatch)
+        return g
+
+    def batch_load(self, index: int, src: "Grid") -> "Grid":
+        """``fmg_batch_load``: problem ``index`` from the assembled grid ``src``
+        (its matrices, rhs, coarse inverse and node damping)."""
+        self.ctx.check(self._lib.fmg_batch_load(self.h, int(index), src.h), "batch_load")
+        return self
+
+    def batch_solve(self, cfg: C.SolveCfg, x: "Vector"):
+        """``fmg_batch_solve``: every problem from x to cfg's tolerance at once;
+        returns (defnorm histories, one row per problem, padded with zeros;
+        steps; status), each row as ``solve`` on the problem's own grid."""
+        hl = cfg.maxsteps + 2
+        hist = np.zeros(self.nb * hl)
+        steps = np.zeros(self.nb, dtype=np.int32)
+        status = np.zeros(self.nb, dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self.ctx.check(self._lib.fmg_batch_solve(self.h, ctypes.byref(cfg), x.h, C.dptr(hist), hl,
+                                                 steps.ctypes.data_as(ip), status.ctypes.data_as(ip)), "batch_solve")
+        return hist.reshape(self.nb, hl), steps, status
+
     @classmethod
     def algebraic(cls, ctx: Context, sizes) -> "Grid":
         """``fmg_grid_create_algebraic``: levels 0 .. len(sizes)-1 without
@@ -365,7 +401,7 @@ class Vector:
 
     def __init__(self, grid: Grid, level: int):
         self.grid, self.level = grid, level
-        self.n = grid.nnodes(level) * grid.nc
+        self.n = grid.nnodes(level) * grid.nc * grid.nb
         h = ctypes.c_void_p()
         grid.ctx.check(grid._lib.fmg_vec_create(grid.h, level, ctypes.byref(h)), "vec_create")
         self.h = h

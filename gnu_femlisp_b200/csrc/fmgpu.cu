@@ -120,6 +120,11 @@ struct fmg_grid {
   double cg_alpha = 0.0;
   bool cg_started = false;
   fmg_solve_cfg cg_cfg{};
+  // a batch (fmg_batch_create): nb problems of one geometry at fixed strides
+  // in every buffer; each is loaded from an assembled grid (fmg_batch_load)
+  int nb = 1;
+  std::vector<char> loaded;
+  double* frozen = nullptr;    // per problem: non-zero once its solve has stopped
   std::vector<void*> allocs;
   int vecs = 0;                // live vectors: the grid outlives them
   bool destroyed = false;      // fmg_grid_destroy called while vectors were alive
@@ -380,6 +385,7 @@ LevelView view(const fmg_grid* g, int l) {
   v.dim = g->dim; v.order = g->order; v.dmask = g->dmask; v.center = g->center;
   v.omega = L.omega;
   v.nc = g->nc;
+  v.nb = g->nb;
   if (g->algebraic) {
     v.csr = true;
     v.a = CsrView{L.ca.start, L.ca.index, L.ca.value};
@@ -481,7 +487,7 @@ struct MG {
   void lmgc() {  // multigrid.lisp:254-288
     const int l = g->cur;
     if (l == g->base) {
-      launch_coarse_solve(g->ainvT, g->nbase, c.coarse_damp, g->solp[l], g->resp[l], st);
+      launch_coarse_solve(g->ainvT, g->nbase, c.coarse_damp, g->solp[l], g->resp[l], st, g->nb, g->lev[l].Np);
       g->rp[l] = 0;
       return;
     }
@@ -754,6 +760,7 @@ int fmg_grid_create_algebraic(fmg_ctx* c, int nlevels, const long* sizes, fmg_gr
 // constrained interpolation.
 int fmg_set_interpolation(fmg_grid* g, int fine_level, int layout, const int* start, const int* index,
                           const double* values, long nfine, long ncoarse) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !start) return FMG_ERR_ARG;
   fmg_ctx* c = g->ctx;
   if (!g->algebraic) return set_err(c, FMG_ERR_UNSUPPORTED, "interpolations are built in on structured grids");
@@ -813,6 +820,7 @@ long fmg_grid_nnodes(const fmg_grid* g, int level) {
 int fmg_grid_nslots(const fmg_grid* g) { return g ? g->nslots : -1; }
 
 int fmg_set_coefficient(fmg_grid* g, int kind, const double* host, long n) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !host) return FMG_ERR_ARG;
   long long ncell = 1;
@@ -957,6 +965,7 @@ static AsmArgs asm_args(fmg_grid* g, int l, bool sample);
 static int ensure_top(fmg_grid* g);
 
 int fmg_assemble_levels(fmg_grid* g, int mode) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g) return FMG_ERR_ARG;
   if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   fmg_ctx* c = g->ctx;
@@ -1157,6 +1166,7 @@ static int set_matrix_alg(fmg_grid* g, int level, int layout, const int* start, 
 
 int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const int* index, const double* values,
                    long n) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !start || (!index && n > 0) || (!values && n > 0)) return FMG_ERR_ARG;
   fmg_ctx* c = g->ctx;
   if (level < g->base || level > g->top) return set_err(c, FMG_ERR_ARG, "level %d out of range", level);
@@ -1210,6 +1220,7 @@ int fmg_set_matrix(fmg_grid* g, int level, int layout, const int* start, const i
 }
 
 int fmg_set_rhs(fmg_grid* g, const double* host, long n) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !host) return FMG_ERR_ARG;
   fmg_ctx* c = g->ctx;
   const Lvl& T = g->lev[g->top];
@@ -1223,6 +1234,7 @@ int fmg_set_rhs(fmg_grid* g, const double* host, long n) {
 }
 
 int fmg_get_matrix(fmg_grid* g, int level, double* host) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !host) return FMG_ERR_ARG;
   if (g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
@@ -1250,6 +1262,7 @@ int fmg_get_matrix(fmg_grid* g, int level, double* host) {
 }
 
 int fmg_get_rhs(fmg_grid* g, double* host) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !host) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   const Lvl& T = g->lev[g->top];
@@ -1260,6 +1273,7 @@ int fmg_get_rhs(fmg_grid* g, double* host) {
 }
 
 int fmg_set_node_damping(fmg_grid* g, int level, const double* host, long n) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   if (level <= g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d has no smoother", level);
@@ -1281,9 +1295,9 @@ int fmg_vec_create(fmg_grid* g, int level, fmg_vec** out) {
   if (!g || !out || level < 0 || level > g->top) return FMG_ERR_ARG;
   fmg_vec* v = new (std::nothrow) fmg_vec();
   if (!v) return FMG_ERR_NOMEM;
-  v->g = g; v->level = level; v->n = g->lev[level].N * g->nc;
+  v->g = g; v->level = level; v->n = g->lev[level].N * g->nc * g->nb;
   g->vecs += 1;
-  const long long np = pad64(v->n);
+  const long long np = g->nb > 1 ? g->lev[level].Np * g->nb : pad64(v->n);  // a batch: problems Np apart
   cudaError_t e = cudaMalloc((void**)&v->d, np * sizeof(double));
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1309,6 +1323,13 @@ int fmg_vec_destroy(fmg_vec* v) {
 
 int fmg_vec_set(fmg_vec* v, const double* host, long n) {
   if (!v || !host || n != v->n) return FMG_ERR_ARG;
+  if (v->g->nb > 1) {  // host: the problems one after another; device: Np apart
+    const Lvl& L = v->g->lev[v->level];
+    FMG_CK(v->g->ctx, cudaMemcpy2DAsync(v->d, L.Np * sizeof(double), host, L.N * sizeof(double),
+                                        L.N * sizeof(double), v->g->nb, cudaMemcpyHostToDevice, v->g->ctx->stream));
+    FMG_CK(v->g->ctx, cudaStreamSynchronize(v->g->ctx->stream));
+    return FMG_OK;
+  }
   FMG_CK(v->g->ctx, cudaMemcpyAsync(v->d, host, n * sizeof(double), cudaMemcpyHostToDevice, v->g->ctx->stream));
   FMG_CK(v->g->ctx, cudaStreamSynchronize(v->g->ctx->stream));
   return FMG_OK;
@@ -1316,32 +1337,45 @@ int fmg_vec_set(fmg_vec* v, const double* host, long n) {
 
 int fmg_vec_get(const fmg_vec* v, double* host, long n) {
   if (!v || !host || n != v->n) return FMG_ERR_ARG;
+  if (v->g->nb > 1) {
+    const Lvl& L = v->g->lev[v->level];
+    FMG_CK(v->g->ctx, cudaMemcpy2DAsync(host, L.N * sizeof(double), v->d, L.Np * sizeof(double),
+                                        L.N * sizeof(double), v->g->nb, cudaMemcpyDeviceToHost, v->g->ctx->stream));
+    FMG_CK(v->g->ctx, cudaStreamSynchronize(v->g->ctx->stream));
+    return FMG_OK;
+  }
   FMG_CK(v->g->ctx, cudaMemcpyAsync(host, v->d, n * sizeof(double), cudaMemcpyDeviceToHost, v->g->ctx->stream));
   FMG_CK(v->g->ctx, cudaStreamSynchronize(v->g->ctx->stream));
   return FMG_OK;
 }
 
+// the device length of a vector (a batch's problems sit Np apart)
+static long long vec_len(const fmg_vec* v) {
+  return v->g->nb > 1 ? v->g->lev[v->level].Np * v->g->nb : v->n;
+}
+
 int fmg_vec_fill(fmg_vec* v, double value) {
   if (!v) return FMG_ERR_ARG;
-  launch_fill(v->d, v->n, value, v->g->ctx->stream);
+  launch_fill(v->d, vec_len(v), value, v->g->ctx->stream);
   return launched(v->g->ctx, "fill");
 }
 
 int fmg_copy(const fmg_vec* x, fmg_vec* y) {
   if (!x || !y || x->n != y->n) return FMG_ERR_ARG;
-  launch_copy(x->d, y->d, x->n, x->g->ctx->stream);
+  launch_copy(x->d, y->d, vec_len(x), x->g->ctx->stream);
   return launched(x->g->ctx, "copy");
 }
 
 int fmg_axpy(double alpha, const fmg_vec* x, fmg_vec* y) {
   if (!x || !y || x->n != y->n) return FMG_ERR_ARG;
-  launch_axpy(alpha, nullptr, -1, x->d, y->d, x->n, x->g->ctx->stream);
+  launch_axpy(alpha, nullptr, -1, x->d, y->d, vec_len(x), x->g->ctx->stream);
   return launched(x->g->ctx, "axpy");
 }
 
 int fmg_dot(const fmg_vec* x, const fmg_vec* y, double* out) {
   if (!x || !y || !out || x->n != y->n) return FMG_ERR_ARG;
   fmg_grid* g = x->g;
+  if (g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "fmg_dot: not on a batch");
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   launch_dot(x->d, y->d, x->n, reducer(g, EPI_STORE, S_DOT), g->ctx->stream);
   int rc = launched(g->ctx, "dot");
@@ -1401,6 +1435,7 @@ int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
 }
 
 int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (g && g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "SOR: scalar grids");
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
@@ -1411,6 +1446,7 @@ int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
 }
 
 int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric SSC: scalar grids");
@@ -1424,6 +1460,7 @@ int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
 }
 
 int fmg_psc(fmg_grid* g, int level, double damp, fmg_vec* x, const fmg_vec* r) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric PSC: scalar grids");
@@ -1437,6 +1474,7 @@ int fmg_psc(fmg_grid* g, int level, double damp, fmg_vec* x, const fmg_vec* r) {
 }
 
 int fmg_coarse_solve(fmg_grid* g, double damp, fmg_vec* x, fmg_vec* r) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, g->base) || vec_check(r, g, g->base)) return FMG_ERR_ARG;
   launch_coarse_solve(g->ainvT, g->nbase, damp, x->d, r->d, g->ctx->stream);
@@ -1444,6 +1482,7 @@ int fmg_coarse_solve(fmg_grid* g, double damp, fmg_vec* x, fmg_vec* r) {
 }
 
 int fmg_vcycle(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fmg_vec* r) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   FMG_RC(ensure_top(g));
   int rc = check_cfg(g, cfg);
@@ -1461,6 +1500,7 @@ int fmg_vcycle(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* x, fmg_vec* b, fm
 
 int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, int hist_len, int* nsteps,
               int* status) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   FMG_RC(ensure_top(g));
   int rc = check_cfg(g, cfg);
@@ -1591,6 +1631,7 @@ int fmg_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, 
 // calls; x and r are the caller's vectors (r up to date at the start,
 // :residual-before t; kept up to date by every step, :residual-after t).
 int fmg_cg_start(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* rv) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   FMG_RC(ensure_top(g));
   int rc = check_cfg(g, cfg);
@@ -1624,6 +1665,7 @@ int fmg_cg_start(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* rv) {
 }
 
 int fmg_cg_step(fmg_grid* g, fmg_vec* xv, fmg_vec* rv, double* defnorm) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (!g->cg_started) return set_err(g->ctx, FMG_ERR_STATE, "fmg_cg_step before fmg_cg_start");
   if (vec_check(xv, g, g->top) || vec_check(rv, g, g->top) || xv == rv) return FMG_ERR_ARG;
@@ -1662,6 +1704,226 @@ int fmg_cg_step(fmg_grid* g, fmg_vec* xv, fmg_vec* rv, double* defnorm) {
   if (!std::isfinite(dn)) return set_err(c, FMG_ERR_NUMERIC, "defnorm is %g", dn);
   if (defnorm) *defnorm = dn;
   return FMG_OK;
+}
+
+
+// ================================================================ batches
+// A batch holds nb independent problems of one geometry (a 1D or 2D scalar
+// Q1 hierarchy) in shared buffers, each problem at a fixed stride: the
+// multigrid iterator and CG run all of them in the same launches, the
+// kernels taking the problem from a grid coordinate, every reduction and
+// every CG scalar per problem.  The arithmetic per problem is that of
+// fmg_solve on the problem's own grid.
+int fmg_batch_create(fmg_grid* like, int nbatch, fmg_grid** out) {
+  if (!like || !out || nbatch < 1) return FMG_ERR_ARG;
+  *out = nullptr;
+  fmg_ctx* c = like->ctx;
+  if (like->nb > 1 || like->algebraic || like->nc != 1 || like->order != 1 || like->dim > 2)
+    return set_err(c, FMG_ERR_UNSUPPORTED, "fmg_batch_create: 1D or 2D scalar Q1 grids");
+  const long long nb_base = like->lev[like->base].N;
+  if (nb_base > 1024)
+    return set_err(c, FMG_ERR_UNSUPPORTED, "fmg_batch_create: base level has %lld unknowns (<= 1024)", nb_base);
+  fmg_grid* g = new (std::nothrow) fmg_grid();
+  if (!g) return FMG_ERR_NOMEM;
+  g->ctx = c;
+  c->grids += 1;
+  g->dim = like->dim; g->order = like->order; g->nc = 1; g->n0 = like->n0;
+  g->top = like->top; g->base = like->base; g->dmask = like->dmask;
+  g->nslots = like->nslots; g->center = like->center;
+  g->lev.resize(like->lev.size());
+  for (size_t l = 0; l < like->lev.size(); ++l) {
+    Lvl& L = g->lev[l];
+    const Lvl& S = like->lev[l];
+    L.n = S.n; L.M = S.M; L.N = S.N; L.Np = S.Np; L.h = S.h;
+  }
+  g->nb = nbatch;
+  g->loaded.assign(nbatch, 0);
+  g->nbase = (int)nb_base;
+  int rc = FMG_OK;
+  FMG_CK(c, cudaSetDevice(c->device));
+  const long long B = nbatch;
+  const Lvl& T = g->lev[g->top];
+  for (int l = g->base; l <= g->top && !rc; ++l) {
+    Lvl& L = g->lev[l];
+    rc = dalloc(g, &L.A, (long long)g->nslots * L.Np * B);
+    if (l < g->top) {
+      if (!rc) rc = dalloc(g, &L.sol[0], L.Np * B);
+      if (!rc) rc = dalloc(g, &L.sol[1], L.Np * B);
+      if (!rc) rc = dalloc(g, &L.rhs, L.Np * B);
+      if (!rc) rc = dalloc(g, &L.res, L.Np * B);
+    }
+  }
+  if (!rc) rc = dalloc(g, &g->rhs, T.Np * B);
+  if (!rc) rc = dalloc(g, &g->ainvT, nb_base * nb_base * B);
+  if (!rc) rc = dalloc(g, &g->scal, S_COUNT * B);
+  if (!rc) rc = dalloc(g, &g->part, (nchunks(T.Np) + 1) * B);
+  if (!rc) rc = dalloc(g, (double**)&g->counter, (B + 1) / 2);
+  if (!rc) rc = dalloc(g, &g->frozen, B);
+  double** tv[] = {&g->p, &g->a, &g->w, &g->w2, &g->q, &g->r, &g->xs, &g->xs2};
+  for (double** v : tv)
+    if (!rc) rc = dalloc(g, v, T.Np * B);
+  if (rc) {
+    grid_release(g);
+    return rc;
+  }
+  const int nlev = g->top + 1;
+  g->solp.assign(nlev, nullptr); g->sparep.assign(nlev, nullptr);
+  g->rhsp.assign(nlev, nullptr); g->resp.assign(nlev, nullptr);
+  g->rp.assign(nlev, 0);
+  for (int l = g->base; l < g->top; ++l) {
+    g->solp[l] = g->lev[l].sol[0]; g->sparep[l] = g->lev[l].sol[1];
+    g->rhsp[l] = g->lev[l].rhs; g->resp[l] = g->lev[l].res;
+  }
+  g->assembled_once = true;
+  *out = g;
+  return launched(c, "batch create");
+}
+
+// Problem `index` of the batch from an assembled grid of the same geometry:
+// its level matrices, top-level rhs, coarse inverse and node damping.  Node
+// damping must be present on a level for every problem or for none.
+int fmg_batch_load(fmg_grid* g, int index, fmg_grid* src) {
+  if (!g || !src || g->nb < 2 || index < 0 || index >= g->nb) return FMG_ERR_ARG;
+  fmg_ctx* c = g->ctx;
+  if (src->ctx != c || src->nb > 1 || src->algebraic || src->dim != g->dim || src->order != g->order ||
+      src->nc != 1 || src->n0 != g->n0 || src->top != g->top || src->base != g->base || src->dmask != g->dmask)
+    return set_err(c, FMG_ERR_ARG, "fmg_batch_load: the source grid's geometry differs from the batch's");
+  if (!src->assembled) return set_err(c, FMG_ERR_STATE, "fmg_batch_load: the source grid is not assembled");
+  FMG_RC(ensure_top(src));
+  cudaStream_t st = c->stream;
+  int rc;
+  for (int l = g->base; l <= g->top; ++l) {
+    Lvl& L = g->lev[l];
+    const Lvl& S = src->lev[l];
+    const size_t mb = (size_t)g->nslots * L.Np * sizeof(double);
+    FMG_CK(c, cudaMemcpyAsync(L.A + (size_t)index * g->nslots * L.Np, S.A, mb, cudaMemcpyDeviceToDevice, st));
+    const bool had = L.omega != nullptr;
+    bool first = true;
+    for (int k = 0; k < g->nb; ++k) first = first && (!g->loaded[k] || k == index);
+    if ((S.omega != nullptr) != had && !first)
+      return set_err(c, FMG_ERR_STATE, "fmg_batch_load: node damping on level %d for some problems only", l);
+    if (S.omega && !had && (rc = dalloc(g, &L.omega, L.Np * g->nb))) return rc;
+    if (!S.omega && had) L.omega = nullptr;  // the first problem loaded again, now without damping
+    if (S.omega)
+      FMG_CK(c, cudaMemcpyAsync(L.omega + (size_t)index * L.Np, S.omega, (size_t)L.N * sizeof(double),
+                                cudaMemcpyDeviceToDevice, st));
+  }
+  const Lvl& T = g->lev[g->top];
+  FMG_CK(c, cudaMemcpyAsync(g->rhs + (size_t)index * T.Np, src->rhs, (size_t)T.N * sizeof(double),
+                            cudaMemcpyDeviceToDevice, st));
+  const size_t nn = (size_t)g->nbase * g->nbase;
+  FMG_CK(c, cudaMemcpyAsync(g->ainvT + index * nn, src->ainvT, nn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  g->loaded[index] = 1;
+  bool all = true;
+  for (char k : g->loaded) all = all && k;
+  g->assembled = all;
+  return launched(c, "batch load");
+}
+
+// fmg_solve of every problem of the batch at once (CG + MG, MG or CG; the
+// Jacobi smoother, multiplicative cycles, the clean preconditioner call):
+// each problem stops at its own tolerance or maxsteps and keeps its iterate
+// from then on; steps, status and the defnorm histories (hist: hist_len
+// entries per problem) are per problem.  The judge of learned damping is not
+// run: each problem uses the node damping it was loaded with.
+int fmg_batch_solve(fmg_grid* g, const fmg_solve_cfg* cfg, fmg_vec* xv, double* hist, int hist_len, int* steps,
+                    int* status) {
+  if (!g || g->nb < 2) return g ? set_err(g->ctx, FMG_ERR_ARG, "fmg_batch_solve: not a batch") : FMG_ERR_ARG;
+  if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "fmg_batch_solve: problems not loaded");
+  int rc = check_cfg(g, cfg);
+  if (rc) return rc;
+  if (vec_check(xv, g, g->top) || !steps || !status) return FMG_ERR_ARG;
+  const fmg_solve_cfg& cf = *cfg;
+  if (cf.smoother != FMG_JACOBI || cf.combination != FMG_MULTIPLICATIVE || cf.fmg || cf.compat_alias)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED,
+                   "fmg_batch_solve: Jacobi, multiplicative cycles, no f-cycle, the clean preconditioner call");
+  fmg_ctx* c = g->ctx;
+  cudaStream_t st = c->stream;
+  const int nb = g->nb;
+  const Lvl& T = g->lev[g->top];
+  const LevelView TV = view(g, g->top);
+  const long long n = T.N, vs = T.Np, nall = vs * nb;
+  const double* b = g->rhs;
+  // CG updates x in place (a stopped problem's iterate stays frozen); the MG
+  // iteration moves every problem, so it runs on two internal vectors and a
+  // problem's iterate is copied to x when it stops
+  const bool mgit = cf.method == FMG_METHOD_MG;
+  double* x = mgit ? g->a : xv->d;
+  double* xspare = mgit ? g->q : g->xs2;
+  MG mg{g, cf, false, st};
+  std::vector<double> hs((size_t)S_COUNT * nb), initial(nb, -1.0), fz(nb, 0.0);
+  std::vector<char> done(nb, 0);
+  for (int k = 0; k < nb; ++k) { steps[k] = 0; status[k] = 1; }
+  auto read_all = [&]() -> int {
+    FMG_CK(c, cudaMemcpyAsync(hs.data(), g->scal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FMG_CK(c, cudaStreamSynchronize(st));
+    return FMG_OK;
+  };
+  auto reducer_b = [&](int epi, int slot) { return reducer(g, epi, slot); };
+  launch_fill(g->p, nall, 0.0, st);
+  launch_fill(g->frozen, nb, 0.0, st);
+  if (mgit) launch_copy(xv->d, x, nall, st);
+  bool initialized = false;
+  for (int step = 0;; ++step) {
+    if (step == 0) {
+      launch_spmv(TV, x, b, g->r, nullptr, nullptr, st);
+      launch_dot_b(g->r, g->r, n, vs, nb, reducer_b(EPI_STORE, S_RR), st);
+      if ((rc = launched(c, "batch residual"))) return rc;
+    }
+    if ((rc = read_all())) return rc;
+    bool changed = false, all = true;
+    for (int k = 0; k < nb; ++k) {
+      if (done[k]) continue;
+      const double dn = std::sqrt(hs[(size_t)k * S_COUNT + S_RR]);
+      if (!std::isfinite(dn)) return set_err(c, FMG_ERR_NUMERIC, "problem %d: defnorm is %g at step %d", k, dn, step);
+      if (initial[k] < 0) initial[k] = dn;
+      if (hist && step < hist_len) hist[(size_t)k * hist_len + step] = dn;
+      steps[k] = step;
+      const double red = initial[k] == 0.0 ? 0.0 : dn / initial[k];
+      const bool conv = (cf.rtol > 0 && red < cf.rtol) || (cf.atol > 0 && dn < cf.atol);
+      if (conv || step > cf.maxsteps) {
+        status[k] = conv ? 0 : 1;
+        done[k] = 1;
+        fz[k] = 1.0;
+        changed = true;
+        if (mgit)  // the iterate of this step is the problem's result
+          FMG_CK(c, cudaMemcpyAsync(xv->d + (size_t)k * vs, x + (size_t)k * vs, n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st));
+      }
+      all = all && done[k];
+    }
+    if (all) break;
+    if (changed) FMG_CK(c, cudaMemcpyAsync(g->frozen, fz.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (mgit) {
+      mg.iterate(&x, &xspare, const_cast<double*>(b), g->r);
+      launch_spmv(TV, x, b, g->r, nullptr, nullptr, st);
+      launch_dot_b(g->r, g->r, n, vs, nb, reducer_b(EPI_STORE, S_RR), st);
+      if ((rc = launched(c, "batch mg step"))) return rc;
+      continue;
+    }
+    const bool pre = cf.method == FMG_METHOD_CG_MG;
+    if (!initialized) {  // w := r; p := M(w) (or r); alpha := (p, r)
+      if (pre) {
+        launch_copy(g->r, g->w2, nall, st);
+        mg.iterate(&g->p, &g->xs, g->r, g->w2);
+      } else {
+        launch_copy(g->r, g->p, nall, st);
+      }
+      launch_dot_b(g->p, g->r, n, vs, nb, reducer_b(EPI_STORE, S_ALPHA), st);
+      initialized = true;
+    }
+    const Reduce Rl = reducer_b(EPI_CG_LAMBDA, 0);
+    launch_spmv(TV, g->p, nullptr, g->a, g->p, &Rl, st);  // a = A p; lam = alpha / (a, p)
+    const Reduce Rr = reducer_b(EPI_STORE, S_RR);
+    if (pre) launch_cg_update_b(g->scal, x, g->p, g->r, g->a, nullptr, g->w2, g->q, n, vs, nb, g->frozen, Rr, st);
+    else launch_cg_update_b(g->scal, x, g->p, g->r, g->a, g->q, nullptr, nullptr, n, vs, nb, g->frozen, Rr, st);
+    if (pre) mg.iterate(&g->q, &g->xs, g->r, g->w2);
+    launch_dot_b(g->q, g->r, n, vs, nb, reducer_b(EPI_CG_ALPHA, 0), st);
+    launch_p_update_b(g->scal, g->p, g->q, n, vs, nb, g->frozen, st);
+    if ((rc = launched(c, "batch cg step"))) return rc;
+  }
+  FMG_CK(c, cudaStreamSynchronize(st));
+  return launched(c, "batch solve");
 }
 
 }  // extern "C"
@@ -2134,6 +2396,7 @@ static int solve_mixed_vec(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixe
 
 extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, fmg_vec* xv,
                                double* hist, int hist_len, int* nouter, int* ninner, int* status) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   int rc = check_cfg(g, cfg);
   if (rc) return rc;
@@ -2293,6 +2556,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
 // residual and a = A p), with the damping it formed the per-node
 // damping/diagonal for.  Nothing waits; the caller times the stream.
 extern "C" int fmg_matvec_mf(fmg_grid* g, int fp32, const fmg_vec* x, const fmg_vec* b, fmg_vec* y) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, g->top) || vec_check(y, g, g->top) || x == y || (b && (vec_check(b, g, g->top) || b == y)))
     return FMG_ERR_ARG;
@@ -2329,6 +2593,7 @@ extern "C" int fmg_matvec_mf(fmg_grid* g, int fp32, const fmg_vec* x, const fmg_
 }
 
 extern "C" int fmg_mixed_top_kernel(fmg_grid* g, int kind, int reps) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g) return FMG_ERR_ARG;
   if (!g->mx || !g->mx->mf || !g->mx->wd_ok || !g->r || !g->a)
     return set_err(g->ctx, FMG_ERR_STATE, "fmg_mixed_top_kernel: no matrix-free mixed solve has run on this grid");
@@ -2727,6 +2992,7 @@ int fmg_net_adam(fmg_net* net, double lr, double beta1, double beta2, double eps
 }
 
 int fmg_net_damping(fmg_net* net, fmg_grid* g, int level, double* host_omega) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   int rc = net_grid_check(net, g);
   if (rc) return rc;
   if (level <= g->base || level > g->top) return set_err(g->ctx, FMG_ERR_ARG, "level %d has no smoother", level);
@@ -2741,6 +3007,7 @@ int fmg_net_damping(fmg_net* net, fmg_grid* g, int level, double* host_omega) {
 }
 
 int fmg_net_apply(fmg_net* net, fmg_grid* g) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   int rc = net_grid_check(net, g);
   if (rc) return rc;
   for (int l = g->top; l > g->base; --l)
@@ -2751,6 +3018,7 @@ int fmg_net_apply(fmg_net* net, fmg_grid* g) {
 }
 
 int fmg_net_backward(fmg_net* net, fmg_grid* g, int level, const double* host_gomega) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   int rc = net_grid_check(net, g);
   if (rc) return rc;
   if (!host_gomega || level <= g->base || level > g->top) return FMG_ERR_ARG;
@@ -2766,6 +3034,7 @@ int fmg_net_backward(fmg_net* net, fmg_grid* g, int level, const double* host_go
 }
 
 int fmg_learn_loss(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* e0, double* loss, double* host_gomega) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !loss) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   int rc = learn_cfg_check(g, cfg);
@@ -2799,6 +3068,7 @@ int fmg_learn_loss(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* e0, dou
 // damping is returned (N of that level values).
 int fmg_learn_loss_levels(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* e0, int level, double* loss,
                           double* host_gomega) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g || !loss) return FMG_ERR_ARG;
   if (!g->assembled) return set_err(g->ctx, FMG_ERR_STATE, "not assembled");
   int rc = learn_cfg_check(g, cfg);
@@ -2832,6 +3102,7 @@ int fmg_learn_loss_levels(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_vec* 
 // loss is mu^2 and the gradient that of mu^2.
 int fmg_learn_step(fmg_net* net, fmg_grid* g, const fmg_solve_cfg* cfg, int nsamples, unsigned long long seed,
                    int max_cycles, double* loss) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   int rc = net_grid_check(net, g);
   if (rc) return rc;
   if ((rc = learn_cfg_check(g, cfg))) return rc;
@@ -3038,11 +3309,13 @@ int learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mc
 extern "C" {
 
 int fmg_learned_judge(fmg_grid* g, const fmg_solve_cfg* cfg, double* rho_plain, double* rho_learned, int* accepted) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   return learned_judge(g, cfg, nullptr, rho_plain, rho_learned, accepted);
 }
 
 int fmg_learned_judge_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_mixed_cfg* mcfg, double* rho_plain,
                             double* rho_learned, int* accepted) {
+  if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!mcfg) return FMG_ERR_ARG;
   return learned_judge(g, cfg, mcfg, rho_plain, rho_learned, accepted);
 }

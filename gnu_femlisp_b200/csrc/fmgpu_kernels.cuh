@@ -19,6 +19,7 @@ struct LevelView {
   int dim, order, dmask, center;
   const double* omega;  // per-node damping or nullptr
   int nc = 1;           // components per node (1, or 3 for elasticity)
+  int nb = 1;           // problems of a batched level (scalar Q1, 1D/2D): vectors Np apart, matrices slots x Np
   // algebraic levels (no geometry): the matrix in compressed rows, its
   // diagonal, and the interpolation from the level below, I (rows of this
   // level) and I^T (rows of the level below); A, M and dim are then unused
@@ -100,16 +101,28 @@ void launch_psc(const LevelView& L, double damp, double* x, const double* r, con
 void launch_restrict(const LevelView& F, const LevelView& C, const double* rf, double* rc, double* rhsc,
                      double* solc, cudaStream_t st);
 void launch_prolong(const LevelView& C, const LevelView& F, const double* xc, double* xf, cudaStream_t st);
-void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st);
+// nb problems of a batched base level: inverses n x n apart, vectors vs apart
+void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st,
+                         int nb = 1, long long vs = 0);
 void launch_lu(double* A, int n, int* piv, double* X, double* XT, cudaStream_t st);
 void launch_fill(double* x, long long n, double v, cudaStream_t st);
 void launch_copy(const double* x, double* y, long long n, cudaStream_t st);
 void launch_axpy(double alpha, const double* sc, int aslot, const double* x, double* y, long long n,
                  cudaStream_t st);
 void launch_dot(const double* x, const double* y, long long n, const Reduce& R, cudaStream_t st);
+// per problem of nb batched vectors (vs apart): each problem's dot in its own reduction
+void launch_dot_b(const double* x, const double* y, long long n, long long vs, int nb, const Reduce& R,
+                  cudaStream_t st);
 void launch_cg_update(const double* sc, double* x, const double* p, double* r, const double* a, double* w,
                       double* w2, double* q, long long n, const Reduce& R, cudaStream_t st);
 void launch_p_update(const double* sc, double* p, const double* q, long long n, cudaStream_t st);
+// batched CG updates: per-problem scalars (S_COUNT apart); problems whose
+// frozen[] entry is non-zero keep x, r and p
+void launch_cg_update_b(const double* sc, double* x, const double* p, double* r, const double* a, double* w,
+                        double* w2, double* q, long long n, long long vs, int nb, const double* frozen,
+                        const Reduce& R, cudaStream_t st);
+void launch_p_update_b(const double* sc, double* p, const double* q, long long n, long long vs, int nb,
+                       const double* frozen, cudaStream_t st);
 void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_top, double ratio, int np,
                       const double* xi, const double* kcell, double* kq, cudaStream_t st);
 // kbar_h / ctab_h: host copies of a.Kbar / a.Ctab (null: the generic kernel)

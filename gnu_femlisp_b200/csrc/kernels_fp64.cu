@@ -303,6 +303,20 @@ __device__ __forceinline__ void q2_visit(const Q2Base<D>& b, long long M, F&& f)
   }
 }
 
+// ------------------------------------------------------------ batches
+// A batched level holds nb independent problems of the same geometry, each
+// at a fixed stride (vectors: the padded length Np; matrices: slots x Np).
+// The 1D-grid kernels take the problem from blockIdx.y, the transfer kernels
+// (1D/2D levels) from blockIdx.z; with one problem the offsets are zero.  A
+// reduction then runs per problem: its partials, counter and scalar slots
+// move with the problem.
+__device__ __forceinline__ Reduce batch_reduce(Reduce R, unsigned bq) {
+  R.part += (long long)bq * gridDim.x;
+  R.counter += bq;
+  R.scal += (long long)bq * S_COUNT;
+  return R;
+}
+
 // ----------------------------------------------------------------- matvec
 // y = A x (RES = false) or r = b - A x (RES = true, b may alias r); with DOT
 // the chunk reduction of (y, dv) is fused in (DR4096 order).
@@ -313,6 +327,15 @@ k_spmv(const double* __restrict__ A, long long N, long long Np, long long M,
        Reduce R) {
   constexpr int NS = St<D, P>::NS;
   __shared__ double smem[8];
+  const long long bq = blockIdx.y;  // problem of a batched level
+  A += bq * NS * Np;
+  x += bq * Np;
+  y += bq * Np;
+  if (RES) b += bq * Np;
+  if (DOT) {
+    dv += bq * Np;
+    R = batch_reduce(R, (unsigned)bq);
+  }
   const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
   double acc = 0.0;
 #pragma unroll 1
@@ -407,9 +430,14 @@ k_jacobi_q2(const double* __restrict__ A, long long N, long long Np, long long M
 // <jacobi> step with an up-to-date residual: t = r/d, x += w t, r := t
 __global__ void __launch_bounds__(kBlock)
 k_jacobi(const double* __restrict__ Dg, long long N, double damp, const double* __restrict__ omega,
-         double* x, double* r, int write_r) {
+         double* x, double* r, int write_r, long long vs = 0, long long as = 0) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  const long long bq = blockIdx.y;  // problem of a batched level: vector stride vs, matrix stride as
+  Dg += bq * as;
+  x += bq * vs;
+  r += bq * vs;
+  if (omega) omega += bq * vs;
   const double t = r[i] / Dg[i];
   if (write_r) r[i] = t;
   const double w = omega ? omega[i] : damp;
@@ -427,6 +455,17 @@ k_jacobi_res(const double* __restrict__ A, long long N, long long Np, long long 
   constexpr int NS = St<D, P>::NS;
   constexpr int C = St<D, P>::CENTER;
   __shared__ double smem[8];
+  const long long bq = blockIdx.y;  // problem of a batched level
+  A += bq * NS * Np;
+  x += bq * Np;
+  b += bq * Np;
+  xout += bq * Np;
+  r += bq * Np;
+  if (omega) omega += bq * Np;
+  if (DOT) {
+    dv += bq * Np;
+    R = batch_reduce(R, (unsigned)bq);
+  }
   const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
   double acc = 0.0;
 #pragma unroll 1
@@ -926,8 +965,15 @@ __device__ __forceinline__ bool face_dir(int c, int M, int k, int dmask) {
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
 k_restrict(int MC, int MF, int dmask, const double* __restrict__ rf, double* __restrict__ rc,
-           double* __restrict__ rhsc, double* __restrict__ solc) {
+           double* __restrict__ rhsc, double* __restrict__ solc, long long fs = 0, long long cs = 0) {
   if (D == 1 && threadIdx.y != 0) return;
+  if (D < 3) {  // problem of a batched level: fine stride fs, coarse stride cs
+    const long long bq = blockIdx.z;
+    rf += bq * fs;
+    rc += bq * cs;
+    rhsc += bq * cs;
+    solc += bq * cs;
+  }
   const int cJ[3] = {(int)(blockIdx.x * 32 + threadIdx.x), D > 1 ? (int)(blockIdx.y * 8 + threadIdx.y) : 0,
                      D > 2 ? (int)blockIdx.z : 0};
   if (cJ[0] >= MC || cJ[1] >= MC) return;
@@ -961,8 +1007,14 @@ k_restrict(int MC, int MF, int dmask, const double* __restrict__ rf, double* __r
 // xf := xf + I xc (constrained) (prolongate, multigrid.lisp:237-239)
 template <int D, int P>
 __global__ void __launch_bounds__(kBlock)
-k_prolong(int MF, int MC, int dmask, const double* __restrict__ xc, double* __restrict__ xf) {
+k_prolong(int MF, int MC, int dmask, const double* __restrict__ xc, double* __restrict__ xf, long long fs = 0,
+          long long cs = 0) {
   if (D == 1 && threadIdx.y != 0) return;
+  if (D < 3) {  // problem of a batched level
+    const long long bq = blockIdx.z;
+    xc += bq * cs;
+    xf += bq * fs;
+  }
   const int fi[3] = {(int)(blockIdx.x * 32 + threadIdx.x), D > 1 ? (int)(blockIdx.y * 8 + threadIdx.y) : 0,
                      D > 2 ? (int)blockIdx.z : 0};
   if (fi[0] >= MF || fi[1] >= MF) return;
@@ -1235,8 +1287,12 @@ __global__ void k_transpose(const double* __restrict__ X, int n, double* __restr
 
 // <lu> coarse-grid iterator: r := A^-1 r, x := x + damp r (one block, n <= 1024)
 __global__ void __launch_bounds__(1024)
-k_coarse_solve(const double* __restrict__ AinvT, int n, double damp, double* x, double* r) {
+k_coarse_solve(const double* __restrict__ AinvT, int n, double damp, double* x, double* r, long long vs = 0) {
   __shared__ double rs[1024];
+  const long long bq = blockIdx.x;  // one CTA per problem of a batched base level
+  AinvT += bq * n * n;
+  x += bq * vs;
+  r += bq * vs;
   const int i = threadIdx.x;
   if (i < n) rs[i] = r[i];
   __syncthreads();
@@ -1284,8 +1340,12 @@ __global__ void k_axpy(double alpha, const double* __restrict__ sc, int aslot, c
 
 // DR4096 dot product (x, y)
 __global__ void __launch_bounds__(kBlock)
-k_dot(const double* __restrict__ x, const double* __restrict__ y, long long n, Reduce R) {
+k_dot(const double* __restrict__ x, const double* __restrict__ y, long long n, Reduce R, long long vs = 0) {
   __shared__ double smem[8];
+  const long long bq = blockIdx.y;  // problem of a batched vector (stride vs)
+  x += bq * vs;
+  y += bq * vs;
+  R = batch_reduce(R, (unsigned)bq);
   const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
   double acc = 0.0;
 #pragma unroll
@@ -1302,8 +1362,20 @@ k_dot(const double* __restrict__ x, const double* __restrict__ y, long long n, R
 __global__ void __launch_bounds__(kBlock)
 k_cg_update(const double* __restrict__ sc, double* __restrict__ x, const double* __restrict__ p,
             double* __restrict__ r, const double* __restrict__ a, double* __restrict__ w,
-            double* __restrict__ w2, double* __restrict__ q, long long n, Reduce R) {
+            double* __restrict__ w2, double* __restrict__ q, long long n, Reduce R, long long vs = 0,
+            const double* __restrict__ frozen = nullptr) {
   __shared__ double smem[8];
+  const long long bq = blockIdx.y;  // problem of a batched vector (stride vs); frozen: it has converged
+  sc += bq * S_COUNT;
+  x += bq * vs;
+  p += bq * vs;
+  r += bq * vs;
+  a += bq * vs;
+  if (w) w += bq * vs;
+  if (w2) w2 += bq * vs;
+  if (q) q += bq * vs;
+  R = batch_reduce(R, (unsigned)bq);
+  const bool fz = frozen && frozen[bq] != 0.0;
   const double lam = sc[S_LAM], nlam = sc[S_NEGLAM];
   const long long base = (long long)blockIdx.x * kChunk + 2 * threadIdx.x;
   double acc = 0.0;
@@ -1313,9 +1385,11 @@ k_cg_update(const double* __restrict__ sc, double* __restrict__ x, const double*
     for (int u = 0; u < 2; ++u) {
       const long long i = base + 512LL * m + u;
       if (i < n) {
-        x[i] = fma(lam, p[i], x[i]);
-        const double rn = fma(nlam, a[i], r[i]);
-        r[i] = rn;
+        const double rn = fz ? r[i] : fma(nlam, a[i], r[i]);
+        if (!fz) {
+          x[i] = fma(lam, p[i], x[i]);
+          r[i] = rn;
+        }
         acc = fma(rn, rn, acc);
         if (w) w[i] = rn;
         if (w2) w2[i] = rn;
@@ -1328,9 +1402,14 @@ k_cg_update(const double* __restrict__ sc, double* __restrict__ x, const double*
 
 // p := (new_alpha/alpha) p (scal!), then p := p + q (m+!)
 __global__ void k_p_update(const double* __restrict__ sc, double* __restrict__ p, const double* __restrict__ q,
-                           long long n) {
+                           long long n, long long vs = 0, const double* __restrict__ frozen = nullptr) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const long long bq = blockIdx.y;  // problem of a batched vector; frozen problems keep p
+  if (frozen && frozen[bq] != 0.0) return;
+  sc += bq * S_COUNT;
+  p += bq * vs;
+  q += bq * vs;
   const double t = sc[S_RATIO] * p[i];
   p[i] = t + q[i];
 }
@@ -2153,7 +2232,7 @@ void launch_spmv(const LevelView& L, const double* x, const double* b, double* y
     if (dv) launch_dot(y, dv, L.N, *R, st);
     return;
   }
-  const unsigned g = nchunks(L.N);
+  const dim3 g(nchunks(L.N), (unsigned)L.nb);
   Reduce r0 = R ? *R : Reduce{};
   Q1_DISPATCH(L.dim, {
     if (b && dv) k_spmv<D, 1, true, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, dv, r0);
@@ -2181,7 +2260,10 @@ void launch_jacobi(const LevelView& L, double damp, double* x, double* r, bool w
     return;
   }
   const double* Dg = L.A + (long long)L.center * L.Np;
-  k_jacobi<<<grid1(L.N), kBlock, 0, st>>>(Dg, L.N, damp, L.omega, x, r, write_r ? 1 : 0);
+  long long ns = 1;
+  for (int k = 0; k < L.dim; ++k) ns *= 3;
+  k_jacobi<<<dim3(grid1(L.N), (unsigned)L.nb), kBlock, 0, st>>>(Dg, L.N, damp, L.omega, x, r, write_r ? 1 : 0,
+                                                                L.Np, ns * L.Np);
 }
 
 void launch_jacobi_res(const LevelView& L, double damp, const double* x, const double* b, double* xout,
@@ -2212,7 +2294,7 @@ void launch_jacobi_res(const LevelView& L, double damp, const double* x, const d
     if (dv) launch_dot(xout, dv, L.N, *R, st);
     return;
   }
-  const unsigned g = nchunks(L.N);
+  const dim3 g(nchunks(L.N), (unsigned)L.nb);
   Reduce r0 = R ? *R : Reduce{};
   Q1_DISPATCH(L.dim, {
     if (dv) k_jacobi_res<D, 1, true><<<g, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
@@ -2319,7 +2401,9 @@ void launch_restrict(const LevelView& F, const LevelView& Cl, const double* rf, 
     return;
   }
   FMG_DISPATCH(F.dim, F.order, {
-    k_restrict<D, P><<<xfer_grid(Cl.M, D), dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc);
+    dim3 gr = xfer_grid(Cl.M, D);
+    if (D < 3) gr.z = (unsigned)F.nb;  // the problems of a batched level
+    k_restrict<D, P><<<gr, dim3(32, 8), 0, st>>>((int)Cl.M, (int)F.M, F.dmask, rf, rc, rhsc, solc, F.Np, Cl.Np);
   });
 }
 
@@ -2337,14 +2421,17 @@ void launch_prolong(const LevelView& Cl, const LevelView& F, const double* xc, d
     return;
   }
   FMG_DISPATCH(F.dim, F.order, {
-    k_prolong<D, P><<<xfer_grid(F.M, D), dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf);
+    dim3 gr = xfer_grid(F.M, D);
+    if (D < 3) gr.z = (unsigned)F.nb;
+    k_prolong<D, P><<<gr, dim3(32, 8), 0, st>>>((int)F.M, (int)Cl.M, F.dmask, xc, xf, F.Np, Cl.Np);
   });
 }
 
-void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st) {
+void launch_coarse_solve(const double* AinvT, int n, double damp, double* x, double* r, cudaStream_t st, int nb,
+                         long long vs) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   if (n <= 1024) {
-    k_coarse_solve<<<1, 1024, 0, st>>>(AinvT, n, damp, x, r);
+    k_coarse_solve<<<(unsigned)nb, 1024, 0, st>>>(AinvT, n, damp, x, r, vs);
   } else {
     static bool init = false;
     if (!init) {
@@ -2406,6 +2493,11 @@ void launch_dot(const double* x, const double* y, long long n, const Reduce& R, 
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_dot<<<nchunks(n), kBlock, 0, st>>>(x, y, n, R);
 }
+void launch_dot_b(const double* x, const double* y, long long n, long long vs, int nb, const Reduce& R,
+                  cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_dot<<<dim3(nchunks(n), (unsigned)nb), kBlock, 0, st>>>(x, y, n, R, vs);
+}
 void launch_cg_update(const double* sc, double* x, const double* p, double* r, const double* a, double* w,
                       double* w2, double* q, long long n, const Reduce& R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -2414,6 +2506,17 @@ void launch_cg_update(const double* sc, double* x, const double* p, double* r, c
 void launch_p_update(const double* sc, double* p, const double* q, long long n, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   k_p_update<<<grid1(n), kBlock, 0, st>>>(sc, p, q, n);
+}
+void launch_cg_update_b(const double* sc, double* x, const double* p, double* r, const double* a, double* w,
+                        double* w2, double* q, long long n, long long vs, int nb, const double* frozen,
+                        const Reduce& R, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_cg_update<<<dim3(nchunks(n), (unsigned)nb), kBlock, 0, st>>>(sc, x, p, r, a, w, w2, q, n, R, vs, frozen);
+}
+void launch_p_update_b(const double* sc, double* p, const double* q, long long n, long long vs, int nb,
+                       const double* frozen, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_p_update<<<dim3(grid1(n), (unsigned)nb), kBlock, 0, st>>>(sc, p, q, n, vs, frozen);
 }
 
 void launch_sample_kq(int dim, long long ncells_l, long long n_l, long long n_top, double ratio, int np,

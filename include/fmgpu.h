@@ -401,6 +401,34 @@ int fmg_learned_judge_mixed(fmg_grid* grid, const fmg_solve_cfg* cfg, const fmg_
    runtime judge fell back to the plain cycle */
 int fmg_learned_status(const fmg_grid* grid, int* active, double* rho_plain, double* rho_learned, int* reverts);
 
+/* ---------------------------------------------------------------- batches */
+/* No counterpart in the reference, which solves one system per solve call:
+   a batch of nbatch independent problems with the geometry of `like` (a 1D
+   or 2D scalar Q1 hierarchy, base level <= 1024 unknowns), kept in shared
+   buffers and solved together -- every kernel launch covers all problems,
+   every reduction and CG scalar is per problem.  The result is a grid
+   handle; fmg_vec_create on it makes batched vectors of nbatch x N values
+   (problem k's values at k*N on the host side), fmg_grid_destroy releases
+   it.  Entry points that work on a single problem refuse a batch. */
+int fmg_batch_create(fmg_grid* like, int nbatch, fmg_grid** batch);
+/* Problem `index` from an assembled grid of the batch's geometry: its level
+   matrices, top-level rhs, coarse-level inverse and node damping (assembled
+   and damped as for fmg_solve on that grid: fmg_assemble, fmg_net_apply,
+   fmg_set_node_damping).  Node damping must be present on a level for every
+   problem of the batch or for none.  The batch is solvable once every
+   problem is loaded. */
+int fmg_batch_load(fmg_grid* batch, int index, fmg_grid* src);
+/* fmg_solve (solve.lisp:139-164 with <cg> krylow.lisp:72-132 or the MG
+   iteration) of every problem at once, from x: CG + MG, MG or CG with the
+   Jacobi smoother, multiplicative cycles, no f-cycle, compat_alias 0.  Each
+   problem stops at its own tolerance (or after maxsteps) and keeps its
+   iterate; steps[k], status[k] and hist[k*hist_len ..] (hist may be NULL)
+   are those fmg_solve reports for problem k on its own grid, and so are the
+   iterates, bit for bit.  The runtime judge of learned damping is not run:
+   each problem uses the damping it was loaded with. */
+int fmg_batch_solve(fmg_grid* batch, const fmg_solve_cfg* cfg, fmg_vec* x, double* hist, int hist_len, int* steps,
+                    int* status);
+
 /* No counterpart in the reference: a measurement hook for the mixed solve's
    top-level kernels.  Runs `reps` back-to-back launches of one of them on the
    grid's own mixed-solve buffers, as an earlier fmg_solve_mixed on this grid
