@@ -62,6 +62,7 @@ def parse_args():
                           "48^3 cells, FP64 CG + block-Jacobi V(2,2); each its own JSON line"))
     ap.add_argument("--c5-level", type=int, default=4, help="c5: 3 x 2^level cells per direction")
     ap.add_argument("--c4-fields", type=int, default=256)
+    ap.add_argument("--c4-batch", type=int, default=1024, help="c4: fields solved together in one batch")
     ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv", "ssc", "mfs"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
                          "the launch count, one more solve; net: the damping network on every level, 8 times; "
@@ -635,6 +636,7 @@ def run_c4(args):
             "judge_accepted": float(np.mean([r["accepted"] for r in rows])),
             "fields_learned_fewer_cycles": int(np.sum(ls < ps)), "fields_learned_more_cycles": int(np.sum(ls > ps)),
         }
+    out["batch"] = run_c4_batch(args, G, net, ctx)
     line = {"metric": "C4 learned smoother: cycles and time to 1e-10, learned damping vs plain w=0.6 GMG",
             "value": out["cg_gmg"]["plain"]["cycles_mean"] / out["cg_gmg"]["learned"]["cycles_mean"],
             "unit": "plain / learned mean CG+GMG cycles", "higher_is_better": True, "n_gpus": 1,
@@ -642,11 +644,87 @@ def run_c4(args):
             "config": {"workload": "2D Q1 128^2 cells, 8x8 blocks, log10 k ~ U[-3,3]",
                        "fields": f"held-out seeds 1000000..{1000000 + args.c4_fields - 1}",
                        "weights": os.path.relpath(WEIGHTS2D, ROOT),
-                       "solve": "one field at a time (fmg_solve), base level 2"},
+                       "solve": "one field at a time (fmg_solve), base level 2; batch: "
+                                f"{args.c4_batch} fields in one fmg_batch_solve"},
             "results": out}
     print(json.dumps(line), flush=True)
     net.close()
     ctx.close()
+
+
+def run_c4_batch(args, G, net, ctx):
+    """The C4 fields solved as one batch (fmg_batch_solve: every kernel launch
+    covers all fields): seeds 1,000,000 .. + c4_batch - 1, CG + V(1,1) Jacobi
+    to 1e-10, with the plain damping 0.6 and with the network's damping on
+    every level (no judge); the time of the batched solve (CUDA events on the
+    library's stream) against the same fields solved one at a time."""
+    import torch
+
+    from gnu_femlisp_b200 import learn
+    C = G._capi
+    B = args.c4_batch
+    seeds = list(range(1000000, 1000000 + B))
+    cfg = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_JACOBI, 0.6, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 200, C.FMG_MULTIPLICATIVE)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    g = G.Grid(ctx, 2, 1, 7, 2)
+    res = {"fields": B, "unknowns_per_field": g.nnodes(), "unknowns_total": B * g.nnodes()}
+    for name, learned in (("plain", False), ("learned", True)):
+        batch = G.Grid.batch(g, B)
+        t0 = time.perf_counter()
+        for k, sd in enumerate(seeds):
+            g.set_coefficient(C.FMG_K_CELL, learn.block_field(sd))
+            g.assemble()
+            if learned:
+                net.apply(g)
+            else:
+                for lev in range(g.base + 1, g.top + 1):
+                    g.set_node_damping(lev, None)
+            batch.batch_load(k, g)
+        ctx.synchronize()
+        t_setup = time.perf_counter() - t0
+        x = batch.vector()
+        ts = []
+        for rep in range(3):
+            x.fill(0.0)
+            ctx.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            _, steps, status = batch.batch_solve(cfg, x)
+            ev1.record(stream)
+            ev1.synchronize()
+            ts.append(ev0.elapsed_time(ev1) / 1e3)
+        t = min(ts)
+        # the first 32 fields one at a time (fmg_solve on their own grid), for the per-field time
+        xs = g.vector()
+        t_one = []
+        for k, sd in enumerate(seeds[:32]):
+            g.set_coefficient(C.FMG_K_CELL, learn.block_field(sd))
+            g.assemble()
+            if learned:
+                net.apply(g)
+            else:
+                for lev in range(g.base + 1, g.top + 1):
+                    g.set_node_damping(lev, None)
+            xs.fill(0.0)
+            ctx.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            _, st1, _ = g.solve(cfg, xs)
+            ev1.record(stream)
+            ev1.synchronize()
+            t_one.append(ev0.elapsed_time(ev1) / 1e3)
+            assert st1 == steps[k], (k, st1, steps[k])
+        xs.close()
+        per_one = float(np.mean(t_one))
+        res[name] = {"batch_solve_s": t, "per_field_ms": 1e3 * t / B, "cg_steps_mean": float(np.mean(steps)),
+                     "cg_steps_max": int(np.max(steps)), "failed": int(np.sum(status != 0)),
+                     "mdof_per_s": B * g.nnodes() / t / 1e6, "setup_s": t_setup,
+                     "one_at_a_time_ms_per_field": 1e3 * per_one,
+                     "batch_speedup_per_field": per_one / (t / B)}
+        x.close()
+        batch.close()
+    g.close()
+    return res
 
 
 def run_profile_c5(args):
