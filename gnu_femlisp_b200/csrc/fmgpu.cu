@@ -58,6 +58,10 @@ struct Lvl {
     double* value = nullptr;
   } ca, cp, cpt;
   double* diag = nullptr;
+  // the colouring of an algebraic level's matrix graph (SOR/SSC sweeps):
+  // rows grouped by colour, ascending inside a colour, and colour offsets
+  std::vector<long long> coff;
+  int* crow = nullptr;
 };
 
 }  // namespace
@@ -392,6 +396,9 @@ LevelView view(const fmg_grid* g, int l) {
     v.p = CsrView{L.cp.start, L.cp.index, L.cp.value};
     v.pt = CsrView{L.cpt.start, L.cpt.index, L.cpt.value};
     v.diag = L.diag;
+    v.crow = L.crow;
+    v.coff = L.coff.data();
+    v.ncol = L.coff.empty() ? 0 : (int)L.coff.size() - 1;
   }
   return v;
 }
@@ -571,8 +578,8 @@ int ssc_prepare(fmg_grid* g, int l) {
 
 int check_cfg(fmg_grid* g, const fmg_solve_cfg* c) {
   if (!c) return set_err(g->ctx, FMG_ERR_ARG, "null configuration");
-  if (g->algebraic && c->smoother != FMG_JACOBI)
-    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "algebraic grids: the Jacobi smoother");
+  if (g->algebraic && c->smoother == FMG_PSC)
+    return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "algebraic grids: Jacobi, SOR and one-unknown SSC");
   if (g->nc != 1 && c->smoother != FMG_JACOBI)
     return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "3-component grids: the (block) Jacobi smoother only");
   if (c->smoother != FMG_JACOBI && c->smoother != FMG_SOR && c->smoother != FMG_SSC && c->smoother != FMG_PSC)
@@ -1135,8 +1142,48 @@ static bool hierarchy_complete(const fmg_grid* g) {
   return true;
 }
 
-// fmg_set_matrix on an algebraic grid: the level matrix as compressed rows
-// and its diagonal
+// Greedy colouring of the graph of a level matrix (i ~ j when a_ij or a_ji is
+// stored, i != j): rows in ascending order take the smallest colour none of
+// their coloured neighbours has.  Rows of one colour then couple to none of
+// each other, so an SOR sweep over the colours in order, the rows of a
+// colour in any order, is Femlisp's <sor> with the rows ordered by colour
+// (the :compare ordering of linit.lisp:288-323).  Returns the rows grouped
+// by colour and the colour offsets.
+static void greedy_colouring(long n, const std::vector<long long>& rs, const std::vector<int>& ci,
+                             std::vector<int>& rows, std::vector<long long>& off) {
+  std::vector<long long> ts((size_t)n + 1, 0);  // the transpose's structure
+  for (long i = 0; i < n; ++i)
+    for (long long e = rs[(size_t)i]; e < rs[(size_t)i + 1]; ++e) ts[(size_t)ci[(size_t)e] + 1] += 1;
+  for (long i = 0; i < n; ++i) ts[(size_t)i + 1] += ts[(size_t)i];
+  std::vector<int> ti((size_t)ts[(size_t)n]);
+  std::vector<long long> fill(ts.begin(), ts.end() - 1);
+  for (long i = 0; i < n; ++i)
+    for (long long e = rs[(size_t)i]; e < rs[(size_t)i + 1]; ++e) ti[(size_t)fill[(size_t)ci[(size_t)e]]++] = (int)i;
+  std::vector<int> col((size_t)n, -1), mark;
+  int ncol = 0;
+  for (long i = 0; i < n; ++i) {
+    auto see = [&](int j) {
+      if (j == i || col[(size_t)j] < 0) return;
+      if ((size_t)col[(size_t)j] >= mark.size()) mark.resize((size_t)col[(size_t)j] + 1, -1);
+      mark[(size_t)col[(size_t)j]] = (int)i;
+    };
+    for (long long e = rs[(size_t)i]; e < rs[(size_t)i + 1]; ++e) see(ci[(size_t)e]);
+    for (long long e = ts[(size_t)i]; e < ts[(size_t)i + 1]; ++e) see(ti[(size_t)e]);
+    int c = 0;
+    while ((size_t)c < mark.size() && mark[(size_t)c] == i) ++c;
+    col[(size_t)i] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  off.assign((size_t)ncol + 1, 0);
+  for (long i = 0; i < n; ++i) off[(size_t)col[(size_t)i] + 1] += 1;
+  for (int c = 0; c < ncol; ++c) off[(size_t)c + 1] += off[(size_t)c];
+  rows.assign((size_t)n, 0);
+  std::vector<long long> pos(off.begin(), off.end() - 1);
+  for (long i = 0; i < n; ++i) rows[(size_t)pos[(size_t)col[(size_t)i]]++] = (int)i;
+}
+
+// fmg_set_matrix on an algebraic grid: the level matrix as compressed rows,
+// its diagonal and the colouring of its graph
 static int set_matrix_alg(fmg_grid* g, int level, int layout, const int* start, const int* index,
                           const double* values, long n) {
   Lvl& L = g->lev[level];
@@ -1156,6 +1203,12 @@ static int set_matrix_alg(fmg_grid* g, int level, int layout, const int* start, 
   dfree(g, L.diag);
   L.diag = nullptr;
   if ((rc = upload(g, &L.diag, dg))) return rc;
+  std::vector<int> crow;
+  greedy_colouring(n, rs, ci, crow, L.coff);
+  dfree(g, L.crow);
+  L.crow = nullptr;
+  if ((rc = dalloc(g, (double**)&L.crow, ((long long)n + 1) / 2))) return rc;
+  FMG_CK(g->ctx, cudaMemcpyAsync(L.crow, crow.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, g->ctx->stream));
   FMG_CK(g->ctx, cudaStreamSynchronize(g->ctx->stream));
   g->assembled = false;
   if ((int)g->have.size() != g->top + 1) g->have.assign(g->top + 1, 0);
@@ -1436,7 +1489,6 @@ int fmg_jacobi(fmg_grid* g, int level, double damp, fmg_vec* x, fmg_vec* r) {
 
 int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
   if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
-  if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (g && g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "SOR: scalar grids");
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level)) return FMG_ERR_ARG;
@@ -1447,7 +1499,6 @@ int fmg_sor(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, 
 
 int fmg_ssc(fmg_grid* g, int level, double omega, fmg_vec* x, const fmg_vec* b, fmg_vec* r) {
   if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
-  if (g && g->algebraic) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on an algebraic grid", __func__);
   if (!g || !g->assembled) return g ? set_err(g->ctx, FMG_ERR_STATE, "not assembled") : FMG_ERR_ARG;
   if (g->nc != 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "geometric SSC: scalar grids");
   if (vec_check(x, g, level) || vec_check(b, g, level) || vec_check(r, g, level) || x == b || x == r)

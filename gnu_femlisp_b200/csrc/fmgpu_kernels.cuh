@@ -26,6 +26,12 @@ struct LevelView {
   bool csr = false;
   CsrView a, p, pt;
   const double* diag = nullptr;
+  // algebraic levels: a colouring of the matrix graph for the SOR/SSC sweeps
+  // (rows of one colour couple to none of each other): the rows grouped by
+  // colour (device) and the colour offsets (host), ncol + 1 of them
+  const int* crow = nullptr;
+  const long long* coff = nullptr;
+  int ncol = 0;
 };
 
 // arguments of the assembly kernel of one level

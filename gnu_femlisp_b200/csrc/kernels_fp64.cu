@@ -898,6 +898,25 @@ k_csr_jacobi_res(long long N, CsrView a, const double* __restrict__ diag, double
   xout[i] = fma(omega ? omega[i] : damp, t, x[i]);
 }
 
+// one colour of the SOR (SSC = false: r := the scaled correction, the
+// <sor> of linit.lisp:288-323) or point-block SSC sweep (r := the residual,
+// blockit.lisp:131-138) of an algebraic level: rows of the colour in any
+// order (they couple to none of each other), the row sum over the stored
+// entries, columns ascending
+__global__ void __launch_bounds__(kBlock)
+k_csr_sor(const int* __restrict__ rows, long long cnt, CsrView a, const double* __restrict__ diag, double omega_s,
+          const double* __restrict__ omega, double* x, const double* b, double* r, int ssc) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const long long i = rows[t];
+  double s = 0.0;
+  for (long long e = a.start[i]; e < a.start[i + 1]; ++e) s = fma(a.value[e], x[a.index[e]], s);
+  const double rr = b[i] - s;
+  const double tt = rr / diag[i];
+  r[i] = ssc ? rr : tt;
+  x[i] = fma(omega ? omega[i] : omega_s, tt, x[i]);
+}
+
 // rc = I^T rf row by row of I^T (fine entries ascending); the coarse rhs
 // takes rc, the coarse solution 0 (the :after methods of restrict)
 __global__ void __launch_bounds__(kBlock)
@@ -2304,7 +2323,21 @@ void launch_jacobi_res(const LevelView& L, double damp, const double* x, const d
   });
 }
 
+static void launch_csr_sor(const LevelView& L, double omega, const double* om, double* x, const double* b, double* r,
+                           bool ssc, cudaStream_t st) {
+  g_launches.fetch_add(L.ncol, std::memory_order_relaxed);
+  for (int c = 0; c < L.ncol; ++c) {
+    const long long cnt = L.coff[c + 1] - L.coff[c];
+    if (cnt > 0)
+      k_csr_sor<<<grid1(cnt), kBlock, 0, st>>>(L.crow + L.coff[c], cnt, L.a, L.diag, omega, om, x, b, r, ssc ? 1 : 0);
+  }
+}
+
 void launch_sor(const LevelView& L, double omega, double* x, const double* b, double* r, cudaStream_t st) {
+  if (L.csr) {
+    launch_csr_sor(L, omega, L.omega, x, b, r, false, st);
+    return;
+  }
   const Q2Layout lay = q2_layout(L.dim, L.M);
   int Q = L.order + 1, ncol = 1;
   for (int k = 0; k < L.dim; ++k) ncol *= Q;
@@ -2339,6 +2372,10 @@ void launch_ssc_factor(const LevelView& L, double* F, unsigned char* P, cudaStre
 
 void launch_ssc(const LevelView& L, double omega, double* x, const double* b, double* r, const double* F,
                 const unsigned char* P, cudaStream_t st) {
+  if (L.csr) {  // an algebraic level: one-unknown blocks over its colouring
+    launch_csr_sor(L, omega, nullptr, x, b, r, true, st);
+    return;
+  }
   const int ncol = 1 << L.dim;
   g_launches.fetch_add(ncol, std::memory_order_relaxed);
   if (L.order == 1) {  // one-node blocks: the colour sweep of the SOR with the SSC residual

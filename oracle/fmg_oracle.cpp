@@ -233,6 +233,8 @@ struct Level {
   // level below (rows of this level) and its transpose (rows of the level below)
   Csr a, p, pt;
   std::vector<double> dg;
+  std::vector<int> colour;      // algebraic levels: the greedy colouring of the matrix graph
+  int ncol = 0;
 };
 
 struct Hier {
@@ -672,7 +674,32 @@ int colour_of(const Hier& H, const long c[3]) {
 // <sor> on a sparse matrix (linit.lisp:288-323), rows ordered by colour
 // class (the :compare slot, linit.lisp:260-263,293-295).  Rows of one colour
 // do not couple, so the order inside a colour does not matter.
+// SOR (ssc = false: r := the scaled correction, linit.lisp:288-323) or the
+// one-unknown-block SSC sweep (r := the residual, blockit.lisp:131-138) of
+// an algebraic level: colours in order, the row sum over the stored entries
+// in their (column-ascending) order
+void sor_alg(const Hier& H, int l, double omega, double* x, const double* b, double* r, bool ssc) {
+  const Level& L = H.lev[l];
+  const double* w = (L.omega.empty() || ssc) ? nullptr : L.omega.data();
+  for (int col = 0; col < L.ncol; ++col) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < L.N; ++i) {
+      if (L.colour[i] != col) continue;
+      double s = 0.0;
+      for (long e = L.a.start[i]; e < L.a.start[i + 1]; ++e) s = std::fma(L.a.value[e], x[L.a.index[e]], s);
+      const double rr = b[i] - s;
+      const double t = rr / L.dg[i];
+      r[i] = ssc ? rr : t;
+      x[i] = std::fma(w ? w[i] : omega, t, x[i]);
+    }
+  }
+}
+
 void sor(const Hier& H, int l, double omega, double* x, const double* b, double* r) {
+  if (H.algebraic) {
+    sor_alg(H, l, omega, x, b, r, false);
+    return;
+  }
   const Level& L = H.lev[l];
   int ncol = 1;
   for (int k = 0; k < H.dim; ++k) ncol *= H.order + 1;
@@ -823,6 +850,10 @@ void ssc_block(const Hier& H, const Level& L, const long v[3], double omega, dou
 }
 
 void ssc(const Hier& H, int l, double omega, double* x, const double* b, double* r) {
+  if (H.algebraic) {
+    sor_alg(H, l, omega, x, b, r, true);
+    return;
+  }
   const Level& L = H.lev[l];
   const int D = H.dim;
   const long nv = H.order == 2 ? (L.M + 1) / 2 : L.M;  // vertices per direction
@@ -1276,9 +1307,32 @@ int ora_set_csr_matrix(void* h, int level, const long* start, const int* index, 
   for (long i = 0; i < L.N; ++i)
     for (long e = start[i]; e < start[i + 1]; ++e)
       if (index[e] == i) L.dg[i] = value[e];
+  // the colouring of the SOR/SSC sweeps: rows in ascending order take the
+  // smallest colour none of their coloured neighbours (a_ij or a_ji stored,
+  // j != i) has -- Femlisp's <sor> with the rows ordered by colour
+  // (linit.lisp:288-323, the :compare ordering)
+  std::vector<std::vector<int>> nbr(L.N);
+  for (long i = 0; i < L.N; ++i)
+    for (long e = start[i]; e < start[i + 1]; ++e)
+      if (index[e] != i) {
+        nbr[i].push_back(index[e]);
+        nbr[index[e]].push_back((int)i);
+      }
+  L.colour.assign(L.N, -1);
+  L.ncol = 0;
+  for (long i = 0; i < L.N; ++i) {
+    std::vector<char> used(nbr[i].size() + 1, 0);
+    for (int j : nbr[i])
+      if (L.colour[j] >= 0 && (size_t)L.colour[j] < used.size()) used[L.colour[j]] = 1;
+    int c = 0;
+    while (used[c]) ++c;
+    L.colour[i] = c;
+    L.ncol = std::max(L.ncol, c + 1);
+  }
   H.assembled = false;
   return 0;
 }
+
 
 int ora_set_interpolation(void* h, int fine_level, const long* start, const int* index, const double* value) {
   Hier& H = *(Hier*)h;
@@ -1489,7 +1543,8 @@ int ora_vcycle(void* h, const ora_solve_cfg* cfg, double* x, double* b, double* 
 int ora_solve(void* h, const ora_solve_cfg* cfg, double* x, double* hist, int hist_len, int* nsteps) {
   Hier& H = *(Hier*)h;
   if (!H.assembled) return -1;
-  if ((H.nc != 1 || H.algebraic) && cfg->smoother != ORA_JACOBI) return -2;
+  if (H.nc != 1 && cfg->smoother != ORA_JACOBI) return -2;
+  if (H.algebraic && cfg->smoother == ORA_PSC) return -2;
   const ora_solve_cfg& c = *cfg;
   const int top = H.top;
   const long n = vec_len(H, top);

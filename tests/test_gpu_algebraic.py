@@ -2,8 +2,9 @@
 interpolations handed over as compressed rows, the path for unstructured and
 adaptively refined meshes): a structured hierarchy given this way iterates
 bit for bit like the structured oracle, an irregular problem bit for bit like
-the oracle's algebraic hierarchy, the level operators match, and
-geometry-bound calls are refused."""
+the oracle's algebraic hierarchy, the level operators match, the
+multicolour SOR and one-unknown SSC sweeps over the greedy colouring of the
+matrix graph match the oracle's, and geometry-bound calls are refused."""
 import numpy as np
 import pytest
 
@@ -120,8 +121,8 @@ def test_refusals_and_incomplete_hierarchy(G, ctx):
     assert e.value.code == -1
     g.set_interpolation(1, s_, i_, v_, sizes[0])
     g.set_rhs(rhs)
-    sor = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_SOR, 1.0, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 60, C.FMG_MULTIPLICATIVE, 0)
-    for call in (lambda: g.solve(sor, x), lambda: g.assemble(), lambda: g.set_coefficient(C.FMG_K_CONST, 1.0),
+    psc = G.SolveCfg(C.FMG_METHOD_CG_MG, C.FMG_PSC, 0.5, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 60, C.FMG_MULTIPLICATIVE, 0)
+    for call in (lambda: g.solve(psc, x), lambda: g.assemble(), lambda: g.set_coefficient(C.FMG_K_CONST, 1.0),
                  lambda: g.matrix(1)):
         with pytest.raises(G.FmgError) as e:
             call()
@@ -146,4 +147,44 @@ def test_algebraic_cycles(oracle_mod, G, ctx, gamma, fmg, comb):
     x = g.vector()
     hist, steps, st = g.solve(cfg, x)
     assert st == r.status == 0
+    assert np.array_equal(hist, r.history) and np.array_equal(x.get(), r.x)
+
+
+@pytest.mark.parametrize("smoother", ["sor", "ssc"])
+@pytest.mark.parametrize("case", ["structured", "irregular"])
+def test_algebraic_sor_and_ssc(oracle_mod, G, ctx, smoother, case):
+    """<sor> with the rows ordered by colour (linit.lisp:288-323) and the
+    one-unknown-block SSC sweep (blockit.lisp:118-204) on algebraic levels:
+    one sweep, then the MG iteration with V(1,1), against the oracle's
+    algebraic hierarchy (the same greedy colouring), bit for bit."""
+    O = oracle_mod
+    C = G._capi
+    if case == "structured":
+        o = O.Oracle(2, 1, 5, base_level=1)
+        o.set_coefficient(O.K_CELL, np.exp(np.random.default_rng(21).standard_normal(32 ** 2)))
+        o.assemble()
+        h = from_structured(o, 2, 1)
+    else:
+        h = irregular(n=2000, levels=4, seed=3)
+    a = oracle_of(O, *h)
+    g = gpu_of(G, ctx, *h)
+    sizes = h[0]
+    top = len(sizes) - 1
+    rng = np.random.default_rng(2)
+    xv, bv = rng.standard_normal(sizes[top]), rng.standard_normal(sizes[top])
+    X, B, R = g.vector(values=xv), g.vector(values=bv), g.vector()
+    if smoother == "sor":
+        g.sor(X, B, R, 1.1)
+        xo, ro = a.sor(xv, bv, np.zeros(sizes[top]), 1.1)
+    else:
+        g.ssc(X, B, R, 1.0)
+        xo, ro = a.ssc(xv, bv, np.zeros(sizes[top]), 1.0)
+    assert np.array_equal(X.get(), xo) and np.array_equal(R.get(), ro)
+    sm_o, sm_g = (O.SOR, C.FMG_SOR) if smoother == "sor" else (O.SSC, C.FMG_SSC)
+    r = a.solve(O.solve_cfg(method=O.METHOD_MG, smoother=sm_o, damp=1.0, pre=1, post=1, compat=False, rtol=1e-10,
+                            maxsteps=150))
+    x = g.vector()
+    cfg = G.SolveCfg(C.FMG_METHOD_MG, sm_g, 1.0, 1, 1, 1, 0, 1.0, 1e-10, 0.0, 150, C.FMG_MULTIPLICATIVE, 0)
+    hist, steps, st = g.solve(cfg, x)
+    assert st == r.status and steps == r.steps, (st, r.status, steps, r.steps)
     assert np.array_equal(hist, r.history) and np.array_equal(x.get(), r.x)
