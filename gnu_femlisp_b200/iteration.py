@@ -11,6 +11,8 @@ Femlisp reads the same here:
   Jacobi, SOR, GaussSeidel, LU      src/iteration/linit.lisp:132-385
   geometric_cs / GeometricCS        src/iteration/geomg.lisp:148-155,
                                     multigrid.lisp:55-70
+  local_mg / LocalMG                src/iteration/geomg.lisp:161-168 (on an
+                                    AlgebraicSystem of a locally refined mesh)
   CG                                src/iteration/krylow.lisp:67-132
   LinearSolver, solve               src/iteration/linsolve.lisp:40-73,
                                     solve.lisp:113-164, iterate.lisp:105-250
@@ -209,7 +211,12 @@ class AlgebraicSystem:
 
     fe = None
 
-    def __init__(self, matrices, interpolations, rhs, ctx: Context | None = None):
+    def __init__(self, matrices, interpolations, rhs, ctx: Context | None = None, order: int | None = None):
+        """order: the discretisation order of a scalar Lagrange space behind
+        the matrices (select-smoother then picks Gauss-Seidel for order 1 and
+        SSC above, geomg.lisp:48-60); None: <jacobi>."""
+        if order is not None:
+            self.fe = lagrange_fe(order)
         if len(interpolations) != len(matrices) - 1:
             raise ValueError("one interpolation per level above the coarsest")
         self.matrices = [_csr_triple(m) for m in matrices]
@@ -306,6 +313,20 @@ class GeometricCS:
 
 def geometric_cs(**kw) -> GeometricCS:
     return GeometricCS(**kw)
+
+
+@dataclass
+class LocalMG(GeometricCS):
+    """<local-mg> (geomg.lisp:161-168): the correction scheme on the levels of
+    a locally refined mesh.  Its systems come as an AlgebraicSystem (the
+    level matrices and constrained interpolations with the hanging-node and
+    essential constraints eliminated); smoothers <jacobi>, <sor> /
+    Gauss-Seidel (multicolour order) and geometric SSC (one-unknown
+    blocks)."""
+
+
+def local_mg(**kw) -> LocalMG:
+    return LocalMG(**kw)
 
 
 @dataclass

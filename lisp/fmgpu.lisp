@@ -338,12 +338,14 @@ discretization order, for the default smoother)."
                                    +fmg-additive+ +fmg-multiplicative+)
                   :fmg (if (fl.multigrid:fmg mgit) 1 0)))))
 
-(defun gpu-hierarchy (mgit matrix)
-  "The device hierarchy of MATRIX for the <gpu-geometric-cs> MGIT, made once
-per matrix (kept in its property list): a structured grid of the same
-levels, every level matrix from Femlisp's multilevel decomposition, and
-three top-level device vectors.  The hierarchy lives as long as the matrix
-(a weak table on SBCL)."
+(defgeneric gpu-hierarchy (mgit matrix)
+  (:documentation "The device hierarchy of MATRIX for the GPU multigrid
+iteration MGIT and three top-level device vectors, made once per matrix.
+The hierarchy lives as long as the matrix (a weak table on SBCL)."))
+
+(defmethod gpu-hierarchy ((mgit <gpu-geometric-cs>) matrix)
+  "A structured grid of the same levels, every level matrix from Femlisp's
+multilevel decomposition in the library's lexicographic node order."
   (or (gethash matrix *hierarchies*)
       (let* ((as (fl.discretization:ansatz-space matrix))
              (h-mesh (fl.discretization:hierarchical-mesh as))
@@ -393,6 +395,64 @@ preconditioner call."
                   (unless alias (%from-device h (gh-r h) r))
                   x))
      :residual-after nil)))
+
+;;;; <gpu-local-mg>
+
+(defclass <gpu-local-mg> (<gpu-geometric-cs> fl.geomg::<local-mg>)
+  ()
+  (:documentation "A <local-mg> (geomg.lisp:161-168) whose cycles run on the
+GPU over an algebraic device hierarchy, so that the mesh may be refined
+locally: the level matrices and the constrained interpolations of Femlisp's
+multilevel decomposition (geomg.lisp:109-142; hanging-node and essential
+constraints eliminated on the host, constraints.lisp:58-151,323-411) handed
+over as compressed columns in each level's own key order.  Scalar problems;
+smoothers <jacobi>, <sor> and <gauss-seidel> (the rows ordered by a greedy
+colouring of each level's matrix graph) and geometric-ssc (one-unknown
+blocks).  make-iterator, <gpu-cg> and <gpu-linear-solver> take it like a
+<gpu-geometric-cs>."))
+
+(defun %upload-interpolation (grid level imat row-keys col-keys)
+  "fmg_set_interpolation with the compressed columns of IMAT (rows: the keys
+of LEVEL, columns: the keys of the level below)."
+  (let* ((ccs (fl.matlisp:sparse-matrix->ccs imat :row-keys row-keys :col-keys col-keys))
+         (pattern (fl.matlisp:pattern ccs)))
+    (check (fl.port:foreign-call #'fmg-set-interpolation grid level +fmg-ccs+
+                                 (slot-value pattern 'fl.matlisp::starts)
+                                 (slot-value pattern 'fl.matlisp::indices)
+                                 (fl.matlisp:store ccs) (length row-keys) (length col-keys))
+           "fmg_set_interpolation")))
+
+(defmethod gpu-hierarchy ((mgit <gpu-local-mg>) matrix)
+  "An algebraic grid of the levels base .. top of the multilevel
+decomposition renumbered from 0: the a-vec matrices, and the i-vec
+interpolation from each level to the next (constrained-interpolation-matrix,
+constraints.lisp:58-72)."
+  (or (gethash matrix *hierarchies*)
+      (let* ((as (fl.discretization:ansatz-space matrix))
+             (top (fl.mesh:top-level (fl.discretization:hierarchical-mesh as)))
+             (base (fl.multigrid:base-level mgit))
+             (mg-data (fl.multigrid:multilevel-decomposition mgit matrix))
+             (a-vec (fl.utilities:getbb mg-data :a-vec))
+             (i-vec (fl.utilities:getbb mg-data :i-vec))
+             (keys (loop for level from base upto top
+                         collect (coerce (fl.matlisp:row-keys (aref a-vec level)) 'vector)))
+             (sizes (map '(vector (signed-byte 64)) #'length keys))
+             (ltop (- top base))
+             (cell (%u64-cell)))
+        (unless (= 1 (%block-size matrix (aref (nth ltop keys) 0)))
+          (error "fl.fmgpu: <gpu-local-mg> takes scalar problems"))
+        (check (fl.port:foreign-call #'fmg-grid-create-algebraic (gpu-context) (length sizes) sizes cell)
+               "fmg_grid_create_algebraic")
+        (let ((grid (aref cell 0)))
+          (loop for k in keys for level from 0 do
+            (%upload-level grid level (aref a-vec (+ base level)) k))
+          (loop for level from 1 upto ltop do
+            (%upload-interpolation grid level (aref i-vec (+ base level -1)) (nth level keys)
+                                   (nth (1- level) keys)))
+          (setf (gethash matrix *hierarchies*)
+                (make-gpu-hierarchy :grid grid :keys (nth ltop keys) :nc 1 :n (length (nth ltop keys))
+                                    :order (fl.discretization:discretization-order as)
+                                    :x (%vec grid ltop) :b (%vec grid ltop) :r (%vec grid ltop)))))))
 
 ;;;; <gpu-cg>
 
@@ -522,15 +582,7 @@ a double vector in the top level's key order.  Returns the grid handle."
                                        (fl.matlisp:store ccs) (length k))
                  "fmg_set_matrix")))
       (loop for i in interpolations for level from 1 do
-        (let* ((ccs (fl.matlisp:sparse-matrix->ccs i :row-keys (nth level keys)
-                                                     :col-keys (nth (1- level) keys)))
-               (pattern (fl.matlisp:pattern ccs)))
-          (check (fl.port:foreign-call #'fmg-set-interpolation grid level +fmg-ccs+
-                                       (slot-value pattern 'fl.matlisp::starts)
-                                       (slot-value pattern 'fl.matlisp::indices)
-                                       (fl.matlisp:store ccs) (length (nth level keys))
-                                       (length (nth (1- level) keys)))
-                 "fmg_set_interpolation")))
+        (%upload-interpolation grid level i (nth level keys) (nth (1- level) keys)))
       (check (fl.port:foreign-call #'fmg-set-rhs grid rhs (length rhs)) "fmg_set_rhs")
       grid)))
 

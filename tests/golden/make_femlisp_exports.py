@@ -1,6 +1,6 @@
 """Writes femlisp_exports.json: for every package the reference's sources
 define (defpackage), its names and nicknames, the symbol names it exports
-and the slot names of the classes defined in it (defclass).  The Lisp binding's test checks every package-qualified symbol in
+and the names and slot names of the classes defined in it (defclass).  The Lisp binding's test checks every package-qualified symbol in
 lisp/fmgpu.lisp against this table (no Lisp implementation runs here).
 
 Run from the repository root with the reference checked out:
@@ -87,6 +87,7 @@ def main(root):
                     cur = name(form[1])
                 elif head == "defclass" and cur and len(form) > 3 and isinstance(form[3], list):
                     entry = pkgs.setdefault(cur, {"nicknames": [], "exports": []})
+                    entry.setdefault("classes", []).append(name(form[1]))
                     slots = entry.setdefault("slots", [])
                     for slot in form[3]:
                         slots.append(name(slot[0] if isinstance(slot, list) and slot else slot))
@@ -115,6 +116,7 @@ def main(root):
         v["exports"] = sorted(set(v["exports"]))
         v["nicknames"] = sorted(set(v["nicknames"]))
         v["slots"] = sorted(set(v.get("slots", [])))
+        v["classes"] = sorted(set(v.get("classes", [])))
     with open(os.path.join(HERE, "femlisp_exports.json"), "w") as f:
         json.dump(pkgs, f, indent=0, sort_keys=True)
     print(f"{len(pkgs)} packages")

@@ -10,12 +10,14 @@ checked by reading it:
   (handles as integers, T** handles as (* sb-alien:unsigned-long), struct
   pointers and C strings as octet vectors);
 * every package-qualified symbol exists: fl.* symbols with one colon are
-  exported by the reference's defpackage forms, with two colons exported or
-  a slot name of a class of that package (tests/golden/femlisp_exports.json,
+  exported by the reference's defpackage forms, with two colons exported,
+  a class of that package or a slot name of one (tests/golden/femlisp_exports.json,
   made by tests/golden/make_femlisp_exports.py); sb-alien / sb-sys symbols
   are SBCL exports the binding needs;
 * the drop-in classes carry their methods: make-iterator for
-  <gpu-geometric-cs> and <gpu-cg>, solve for <gpu-linear-solver>.
+  <gpu-geometric-cs> and <gpu-cg>, solve for <gpu-linear-solver>, the device
+  hierarchy for <gpu-geometric-cs> (structured) and <gpu-local-mg>
+  (algebraic, for locally refined meshes).
 """
 import json
 import os
@@ -172,8 +174,9 @@ def test_package_qualified_symbols_exist():
         pkg, sym = re.split(r"::?", s, maxsplit=1)
         pkg, sym = pkg.upper(), sym.upper()
         assert pkg in names, f"{s}: package {pkg} is not defined by the reference"
-        ok = sym in names[pkg]["exports"] or (internal and sym in names[pkg].get("slots", []))
-        assert ok, f"{s}: not {'exported or a slot' if internal else 'exported'} in {pkg}"
+        ok = sym in names[pkg]["exports"] or (internal and (sym in names[pkg].get("slots", [])
+                                                            or sym in names[pkg].get("classes", [])))
+        assert ok, f"{s}: not {'exported, a slot or a class' if internal else 'exported'} in {pkg}"
     assert not any(s.lower().startswith("fl.port:sap-ref") for s in syms)
 
 
@@ -183,10 +186,13 @@ def test_drop_in_classes_have_their_methods():
     assert classes.get("<gpu-geometric-cs>") == ["fl.geomg:<geometric-cs>"]
     assert classes.get("<gpu-cg>") == ["fl.iteration:<cg>"]
     assert classes.get("<gpu-linear-solver>") == ["fl.iteration:<linear-solver>"]
+    assert classes.get("<gpu-local-mg>") == ["<gpu-geometric-cs>", "fl.geomg::<local-mg>"]
     methods = {(f[1], f[2][0][1]) for f in forms if isinstance(f, list) and f and f[0] == "defmethod"}
     assert ("fl.iteration:make-iterator", "<gpu-geometric-cs>") in methods
     assert ("fl.iteration:make-iterator", "<gpu-cg>") in methods
     assert ("fl.iteration:solve", "<gpu-linear-solver>") in methods
+    assert ("gpu-hierarchy", "<gpu-geometric-cs>") in methods
+    assert ("gpu-hierarchy", "<gpu-local-mg>") in methods
 
 
 def _struct_offsets(forms, defun_name):
