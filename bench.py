@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--c5-level", type=int, default=4, help="c5: 3 x 2^level cells per direction")
     ap.add_argument("--c4-fields", type=int, default=256)
     ap.add_argument("--c4-batch", type=int, default=1024, help="c4: fields solved together in one batch")
-    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv", "ssc", "mfs"], default=None,
+    ap.add_argument("--profile", choices=["solve", "net", "c5", "c5mv", "ssc", "mfs", "c2"], default=None,
                     help="no timing: a workload for an ncu capture (solve: setup, two mixed+learned solves, "
                          "the launch count, one more solve; net: the damping network on every level, 8 times; "
                          "c5: the elasticity setup, two mixed+learned solves, the launch count, one more; "
@@ -788,6 +788,49 @@ def run_profile_ssc(args):
     ctx.close()
 
 
+def run_profile_c2(args):
+    """The C2 V-cycles for ncu captures: the 3D Q2 hierarchy of the C2
+    problem at `--level` (6: the configuration), two V(2,2) SOR(1.2) cycles
+    and a matvec to warm up, then (after the printed launch count) one
+    V(2,2) SOR cycle, one V(1,1) SSC cycle and one top-level matvec inside
+    the NVTX range 'c2' (ncu --nvtx --nvtx-include c2/)."""
+    import torch
+
+    import gnu_femlisp_b200 as G
+    from gnu_femlisp_b200 import problems
+    from gnu_femlisp_b200.iteration import sample_at_gauss_points
+    C = G._capi
+    wl = problems.c2()
+    level = min(args.level, wl.level)
+    ctx = G.Context(0)
+    g = G.Grid(ctx, 3, 2, level, base_level=wl.base_level)
+    g.set_coefficient(C.FMG_F_IP, sample_at_gauss_points(wl.source, 3, 2, 1 << level))
+    g.assemble()
+    sor = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_SOR, wl.damp, wl.pre, wl.post, 1, 0, 1.0, 0.0, 0.0, 1,
+                     C.FMG_MULTIPLICATIVE)
+    ssc = G.SolveCfg(C.FMG_METHOD_MG, C.FMG_SSC, 1.0, 1, 1, 1, 0, 1.0, 0.0, 0.0, 1, C.FMG_MULTIPLICATIVE)
+    n = g.nnodes()
+    B = g.vector(values=g.rhs())
+    R, X, Y = g.vector(), g.vector(), g.vector()
+    for _ in range(2):
+        g.vcycle(sor, X, B, R)
+    g.vcycle(ssc, X, B, R)
+    g.matvec(X, Y)
+    ctx.synchronize()
+    print("launches_before", ctypes_count(C), "nodes", n, flush=True)
+    torch.cuda.nvtx.range_push("c2")
+    g.vcycle(sor, X, B, R)
+    ctx.synchronize()
+    print("launches_after_sor_cycle", ctypes_count(C), flush=True)
+    g.vcycle(ssc, X, B, R)
+    g.matvec(X, Y)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print("launches_after", ctypes_count(C), flush=True)
+    g.close()
+    ctx.close()
+
+
 def run_profile_mfs(args):
     """The matrix-free top-level kernels of the mixed solve at `--level`: one
     plain mixed solve (no damping network) leaves their buffers, then one
@@ -828,6 +871,8 @@ def run_profile(args):
         return run_profile_ssc(args)
     if args.profile == "mfs":
         return run_profile_mfs(args)
+    if args.profile == "c2":
+        return run_profile_c2(args)
     wl = problems.c3(seed=0, level=args.level)
     ctx = G.Context(0)
     g = G.Grid(ctx, 3, 1, wl.level, base_level=wl.base_level)

@@ -8,7 +8,9 @@
 // thread, coalesced across the warp.  Entries outside the grid, in eliminated
 // Dirichlet columns and structurally absent Q2 couplings are stored as zeros,
 // which lets neighbour indices be clamped to the vector instead of tested.
+#include <algorithm>
 #include <cstring>
+#include <type_traits>
 #include "fmgpu_kernels.cuh"
 
 namespace fmg {
@@ -368,49 +370,6 @@ k_spmv(const double* __restrict__ A, long long N, long long Np, long long M,
   if (DOT) dr_finish(acc, R, smem);
 }
 
-// y = A x or r = b - A x on a Q2 level in sliced storage, one row per thread
-// (the fused reduction of k_spmv runs as a separate DR4096 pass)
-template <int D, bool RES>
-__global__ void __launch_bounds__(kBlock)
-k_spmv_q2(const double* __restrict__ A, long long N, long long Np, long long M, const double* __restrict__ x,
-          const double* b, double* y, const __grid_constant__ Q2Layout lay) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  long long c[3];
-  node_coords32(i, M, D, c);
-  double acc = 0.0;
-  Q2Base<D> qb;
-  q2_base<D, true>(lay, c, M, qb);
-  q2_visit<D, false>(qb, M, [&](int s, long long o, long long p, bool) {
-    acc = fma(__ldg(A + (long long)s * Np + p), __ldg(x + clampi(i + o, N)), acc);
-  });
-  y[i] = RES ? b[i] - acc : acc;
-}
-
-// k_jacobi_res on a Q2 level in sliced storage, one row per thread
-template <int D>
-__global__ void __launch_bounds__(kBlock)
-k_jacobi_res_q2(const double* __restrict__ A, long long N, long long Np, long long M, double damp,
-                const double* __restrict__ omega, const double* __restrict__ x, const double* b,
-                double* __restrict__ xout, double* r, int write_r, const __grid_constant__ Q2Layout lay) {
-  constexpr int C = St<D, 2>::CENTER;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  long long c[3];
-  node_coords32(i, M, D, c);
-  double acc = 0.0, d = 1.0;
-  Q2Base<D> qb;
-  q2_base<D, true>(lay, c, M, qb);
-  q2_visit<D, false>(qb, M, [&](int s, long long o, long long p, bool) {
-    const double a = __ldg(A + (long long)s * Np + p);
-    if (s == C) d = a;
-    acc = fma(a, __ldg(x + clampi(i + o, N)), acc);
-  });
-  const double t = (b[i] - acc) / d;
-  if (write_r) r[i] = t;
-  xout[i] = fma(omega ? omega[i] : damp, t, x[i]);
-}
-
 // k_jacobi on a scalar Q2 level (the diagonal sits at the node's colour-major place)
 template <int D>
 __global__ void __launch_bounds__(kBlock)
@@ -424,6 +383,235 @@ k_jacobi_q2(const double* __restrict__ A, long long N, long long Np, long long M
   const double t = r[i] / A[(long long)C * Np + q2c_pos<D>(lay, c, M, 0)];
   if (write_r) r[i] = t;
   x[i] = fma(omega ? omega[i] : damp, t, x[i]);
+}
+
+// ------------------------------------- Q2 rows by colour class and parity
+// The row kernels of scalar Q2 levels give each block rows of one colour
+// class and one parity pattern (bit k: coordinate k odd).  All rows of a
+// warp then admit the same slots, so a row is a compile-time list of its
+// stored slots -- no per-slot test, no divergence -- and a thread issues a
+// whole z-plane of the stencil (up to 25 coefficient and 25 neighbour loads)
+// before the plane's first multiply-add; the row sum still runs in slot
+// order, skipping only structural zeros.  Along direction k the class (digit
+// d = c mod 3) holds c = d + 3 j, j = 0 .. n-1; its rows of parity p are
+// j = j0, j0 + 2, .. with j0 = (p + d) & 1.  Inside a class the coefficient
+// arrays are contiguous, so a warp's loads of one slot stay within a few
+// sectors.
+constexpr int kQ2T = 128;  // threads per block
+
+struct Q2Sub {
+  int d[3], j0[3], n[3];  // class digit, first place and row count along each direction
+  long long cnt;          // rows of the (class, parity) subgrid
+};
+
+template <int D>
+__host__ __device__ __forceinline__ void q2_sub(int M, int colour, int pat, Q2Sub& s) {
+  s.cnt = 1;
+  int t = colour;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (k < D) {
+      const int d = t % 3, nk = (M - d + 2) / 3, j0 = (((pat >> k) & 1) + d) & 1;
+      t /= 3;
+      s.d[k] = d;
+      s.j0[k] = j0;
+      s.n[k] = nk > j0 ? (nk - j0 + 1) / 2 : 0;
+    } else {
+      s.d[k] = 0;
+      s.j0[k] = 0;
+      s.n[k] = 1;
+    }
+    s.cnt *= s.n[k];
+  }
+}
+
+// blocks a class takes: its parity subgrids one after another
+template <int D>
+__host__ __device__ __forceinline__ long long q2_class_blocks(int M, int colour) {
+  long long nb = 0;
+  for (int pat = 0; pat < (1 << D); ++pat) {
+    Q2Sub s;
+    q2_sub<D>(M, colour, pat, s);
+    nb += (s.cnt + kQ2T - 1) / kQ2T;
+  }
+  return nb;
+}
+
+// block blk of a class: its parity pattern, subgrid and this thread's row u
+// in it; false when the thread has no row
+template <int D>
+__device__ __forceinline__ bool q2_block(int M, int colour, long long blk, int& pat, Q2Sub& s, long long& u) {
+  for (pat = 0; pat < (1 << D); ++pat) {
+    q2_sub<D>(M, colour, pat, s);
+    const long long nb = (s.cnt + kQ2T - 1) / kQ2T;
+    if (blk < nb) {
+      u = blk * kQ2T + threadIdx.x;
+      return u < s.cnt;
+    }
+    blk -= nb;
+  }
+  return false;
+}
+
+// a row's coordinates, node index and its positions in the arrays of every
+// slot pattern (colour-major layout; patterns it does not admit are never read)
+template <int D>
+__device__ __forceinline__ long long q2_place(const Q2Layout& lay, int M, int colour, const Q2Sub& s, long long u,
+                                              int c[3], int (&p)[1 << D]) {
+  const unsigned uu = (unsigned)u;
+  const unsigned q = D > 1 ? uu / (unsigned)s.n[0] : 0u;
+  const int uk[3] = {(int)(D > 1 ? uu - q * (unsigned)s.n[0] : uu), D > 2 ? (int)(q % (unsigned)s.n[1]) : (int)q,
+                     D > 2 ? (int)(q / (unsigned)s.n[1]) : 0};
+  int j[3][2], e[3][2];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (k < D) {
+      const int jj = s.j0[k] + 2 * uk[k], d = s.d[k], x0 = q2c_x0(d);
+      c[k] = d + 3 * jj;
+      j[k][0] = jj;
+      e[k][0] = (M - d + 2) / 3;
+      j[k][1] = (c[k] - x0) / 6;
+      e[k][1] = x0 < M ? (M - x0 + 5) / 6 : 0;
+    } else {
+      c[k] = 0;
+      j[k][0] = j[k][1] = 0;
+      e[k][0] = e[k][1] = 1;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < (1 << D); ++r) {
+    const int rx = r & 1, ry = (r >> 1) & 1, rz = (r >> 2) & 1;
+    p[r] = (int)lay.off[r][colour] + j[0][rx] + e[0][rx] * (j[1][ry] + e[1][ry] * j[2][rz]);
+  }
+  return (long long)c[0] + (long long)M * (c[1] + (long long)M * c[2]);
+}
+
+// sum over the row's stored slots, in slot order, of A(i, s) x(i + off_s).
+// PAT: the row's parity pattern.  Neighbour coordinates are clamped into the
+// grid per direction (a slot reaching outside holds a zero).  XL: how x is
+// read -- 0 plain loads (x is written by the kernel), 1 the read-only path
+template <int D, int PAT, int XL>
+__device__ __forceinline__ double q2_row_sum(const double* __restrict__ A, long long Np, const double* x, int M,
+                                             const int c[3], const int (&p)[1 << D]) {
+  int cl[3][5];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 0; o < 5; ++o) cl[k][o] = k < D ? min(max(c[k] + o - 2, 0), M - 1) : 0;
+  constexpr int NZ = D > 2 ? 5 : 1, NY = D > 1 ? 5 : 1;
+  double s = 0.0;
+#pragma unroll
+  for (int sz = 0; sz < NZ; ++sz) {
+    const bool rz = D > 2 && (sz == 0 || sz == 4);
+    if (rz && (PAT & 4)) continue;
+    double av[25], xv[25];
+    int q = 0;
+#pragma unroll
+    for (int sy = 0; sy < NY; ++sy) {
+      const bool ry = D > 1 && (sy == 0 || sy == 4);
+      if (ry && (PAT & 2)) continue;
+      const double* xl = x + (long long)M * (cl[1][sy] + (long long)M * cl[2][sz]);
+#pragma unroll
+      for (int sx = 0; sx < 5; ++sx) {
+        const bool rx = sx == 0 || sx == 4;
+        if (rx && (PAT & 1)) continue;
+        const int slot = sx + 5 * (sy + 5 * sz);
+        const int r = (rx ? 1 : 0) | (ry ? 2 : 0) | (rz ? 4 : 0);
+        av[q] = __ldg(A + (long long)slot * Np + p[r]);
+        xv[q] = XL == 1 ? __ldg(xl + cl[0][sx]) : xl[cl[0][sx]];
+        ++q;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < q; ++k) s = fma(av[k], xv[k], s);
+  }
+  return s;
+}
+
+// calls f(integral_constant<int, pat>) for the runtime pattern pat
+template <int D, typename F>
+__device__ __forceinline__ void q2_pat_dispatch(int pat, F&& f) {
+  switch (pat) {
+    case 0: f(std::integral_constant<int, 0>{}); break;
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: if constexpr (D > 1) f(std::integral_constant<int, 2>{}); break;
+    case 3: if constexpr (D > 1) f(std::integral_constant<int, 3>{}); break;
+    case 4: if constexpr (D > 2) f(std::integral_constant<int, 4>{}); break;
+    case 5: if constexpr (D > 2) f(std::integral_constant<int, 5>{}); break;
+    case 6: if constexpr (D > 2) f(std::integral_constant<int, 6>{}); break;
+    default: if constexpr (D > 2) f(std::integral_constant<int, 7>{}); break;
+  }
+}
+
+// the rows of block blk of colour class `colour` in the multicolour <sor>
+// sweep of a scalar Q2 level (linit.lisp:288-323): r = (b - A x)/d, x += w r
+template <int D, int XL>
+__device__ __forceinline__ void sor_q2_block(const double* __restrict__ A, long long Np, int M, int colour,
+                                             long long blk, double omega_s, const double* __restrict__ omega,
+                                             double* x, const double* b, double* r, const Q2Layout& lay) {
+  int pat;
+  Q2Sub sub;
+  long long u;
+  if (!q2_block<D>(M, colour, blk, pat, sub, u)) return;
+  int c[3], p[1 << D];
+  const long long i = q2_place<D>(lay, M, colour, sub, u, c, p);
+  constexpr int C = St<D, 2>::CENTER;
+  // the row's own operands first, so that their loads overlap the stencil's
+  const double d = __ldg(A + (long long)C * Np + p[0]);
+  const double bi = b[i], xi = x[i], wi = omega ? __ldg(omega + i) : omega_s;
+  double s = 0.0;
+  q2_pat_dispatch<D>(pat, [&](auto P) { s = q2_row_sum<D, decltype(P)::value, XL>(A, Np, x, M, c, p); });
+  const double tt = (bi - s) / d;
+  r[i] = tt;
+  x[i] = fma(wi, tt, xi);
+}
+
+// one colour of the sweep per launch
+template <int D>
+__global__ void __launch_bounds__(kQ2T)
+k_sor_q2(const double* __restrict__ A, long long Np, int M, int colour, double omega_s,
+         const double* __restrict__ omega, double* x, const double* b, double* r,
+         const __grid_constant__ Q2Layout lay) {
+  sor_q2_block<D, 0>(A, Np, M, colour, blockIdx.x, omega_s, omega, x, b, r, lay);
+}
+
+// y = A x or r = b - A x on a scalar Q2 level, rows by class (blockIdx.y) and parity
+template <int D, bool RES>
+__global__ void __launch_bounds__(kQ2T)
+k_spmv_q2c(const double* __restrict__ A, long long Np, int M, const double* __restrict__ x, const double* b,
+           double* y, const __grid_constant__ Q2Layout lay) {
+  int pat;
+  Q2Sub sub;
+  long long u;
+  const int colour = (int)blockIdx.y;
+  if (!q2_block<D>(M, colour, blockIdx.x, pat, sub, u)) return;
+  int c[3], p[1 << D];
+  const long long i = q2_place<D>(lay, M, colour, sub, u, c, p);
+  double s = 0.0;
+  q2_pat_dispatch<D>(pat, [&](auto P) { s = q2_row_sum<D, decltype(P)::value, 1>(A, Np, x, M, c, p); });
+  y[i] = RES ? b[i] - s : s;
+}
+
+// k_jacobi_res on a scalar Q2 level, rows by class and parity
+template <int D>
+__global__ void __launch_bounds__(kQ2T)
+k_jacobi_res_q2c(const double* __restrict__ A, long long Np, int M, double damp, const double* __restrict__ omega,
+                 const double* __restrict__ x, const double* b, double* __restrict__ xout, double* r, int write_r,
+                 const __grid_constant__ Q2Layout lay) {
+  int pat;
+  Q2Sub sub;
+  long long u;
+  const int colour = (int)blockIdx.y;
+  if (!q2_block<D>(M, colour, blockIdx.x, pat, sub, u)) return;
+  int c[3], p[1 << D];
+  const long long i = q2_place<D>(lay, M, colour, sub, u, c, p);
+  constexpr int C = St<D, 2>::CENTER;
+  const double d = __ldg(A + (long long)C * Np + p[0]);
+  double s = 0.0;
+  q2_pat_dispatch<D>(pat, [&](auto P) { s = q2_row_sum<D, decltype(P)::value, 1>(A, Np, x, M, c, p); });
+  const double t = (b[i] - s) / d;
+  if (write_r) r[i] = t;
+  xout[i] = fma(omega ? omega[i] : damp, t, x[i]);
 }
 
 // ------------------------------------------------------------- smoothers
@@ -502,15 +690,15 @@ k_jacobi_res(const double* __restrict__ A, long long N, long long Np, long long 
   if (DOT) dr_finish(acc, R, smem);
 }
 
-// one colour of the multicolour <sor> sweep: rows with (i_k mod (P+1)) = col_k.
+// one colour of the multicolour <sor> sweep on a Q1 level (P = 1): rows with
+// (i_k mod (P+1)) = col_k (scalar Q2 levels: k_sor_q2).
 // SSC: the <geometric-ssc> sweep of a Q1 level, whose vertex blocks hold one
 // node -- the same update, with r keeping the unscaled residual
 // (blockit.lisp:131-138) instead of the <sor> correction (linit.lisp:312-322)
 template <int D, int P, bool SSC = false>
 __global__ void __launch_bounds__(kBlock)
 k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long M, int colour,
-             double omega_s, const double* __restrict__ omega, double* x, const double* b, double* r,
-             const __grid_constant__ Q2Layout lay) {
+             double omega_s, const double* __restrict__ omega, double* x, const double* b, double* r) {
   constexpr int NS = St<D, P>::NS;
   constexpr int C = St<D, P>::CENTER;
   constexpr int Q = P + 1;
@@ -525,24 +713,12 @@ k_sor_colour(const double* __restrict__ A, long long N, long long Np, long long 
   const long long jx = tu - tq * nxu, jy = tq % nyu, jz = tq / nyu;
   const long long i = (cx + Q * jx) + M * ((D > 1 ? cy + Q * jy : 0) + M * (D > 2 ? cz + Q * jz : 0));
   double s = 0.0, d = 1.0;
-  if constexpr (P == 2) {  // colour-major sliced storage: the class's rows are contiguous
-    const long long c[3] = {cx + Q * jx, D > 1 ? cy + Q * jy : 0, D > 2 ? cz + Q * jz : 0};
-    Q2Base<D> qb;
-    q2_base<D, true, true>(lay, c, M, qb);
-    q2_visit<D, true>(qb, M, [&](int k, long long o, long long p, bool st) {
-      double a = A[(long long)k * Np + p];
-      a = st ? a : 0.0;
-      if (k == C) d = a;
-      s = fma(a, x[clampi(i + o, N)], s);
-    });
-  } else {
 #pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      const long long o = slot_off<D, P>(k, M);
-      const double a = A[(long long)k * Np + i];
-      if (k == C) d = a;
-      s = fma(a, x[clampi(i + o, N)], s);
-    }
+  for (int k = 0; k < NS; ++k) {
+    const long long o = slot_off<D, P>(k, M);
+    const double a = A[(long long)k * Np + i];
+    if (k == C) d = a;
+    s = fma(a, x[clampi(i + o, N)], s);
   }
   const double rr = b[i] - s;
   const double tt = rr / d;
@@ -1304,6 +1480,23 @@ __global__ void k_transpose(const double* __restrict__ X, int n, double* __restr
   XT[j * n + i] = X[i * n + j];
 }
 
+// row i of A^-1 r: sum_j (A^-1)^T[j][i] rs[j] in ascending j, sixteen
+// coefficients loaded before their multiply-adds (one memory wait per
+// sixteen terms instead of one per term)
+__device__ __forceinline__ double coarse_row(const double* __restrict__ AinvT, int n, int i, const double* rs) {
+  double acc = 0.0;
+  int j = 0;
+  for (; j + 16 <= n; j += 16) {
+    double a[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) a[q] = __ldg(AinvT + (long long)(j + q) * n + i);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc = fma(a[q], rs[j + q], acc);
+  }
+  for (; j < n; ++j) acc = fma(__ldg(AinvT + (long long)j * n + i), rs[j], acc);
+  return acc;
+}
+
 // <lu> coarse-grid iterator: r := A^-1 r, x := x + damp r (one block, n <= 1024)
 __global__ void __launch_bounds__(1024)
 k_coarse_solve(const double* __restrict__ AinvT, int n, double damp, double* x, double* r, long long vs = 0) {
@@ -1316,8 +1509,7 @@ k_coarse_solve(const double* __restrict__ AinvT, int n, double damp, double* x, 
   if (i < n) rs[i] = r[i];
   __syncthreads();
   if (i >= n) return;
-  double acc = 0.0;
-  for (int j = 0; j < n; ++j) acc = fma(AinvT[(long long)j * n + i], rs[j], acc);
+  const double acc = coarse_row(AinvT, n, i, rs);
   r[i] = acc;
   x[i] = fma(damp, acc, x[i]);
 }
@@ -1330,8 +1522,7 @@ k_coarse_solve_big(const double* __restrict__ AinvT, int n, double damp, double*
   for (int i = threadIdx.x; i < n; i += blockDim.x) rsb[i] = r[i];
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double acc = 0.0;
-    for (int j = 0; j < n; ++j) acc = fma(AinvT[(long long)j * n + i], rsb[j], acc);
+    const double acc = coarse_row(AinvT, n, i, rsb);
     r[i] = acc;
     x[i] = fma(damp, acc, x[i]);
   }
@@ -2221,6 +2412,17 @@ __global__ void k_fcg_beta(double* sc, int first) {
 
 static inline unsigned grid1(long long n, int bs = kBlock) { return (unsigned)((n + bs - 1) / bs); }
 
+// the row kernels of scalar Q2 levels over every class: blockIdx.y the class,
+// blockIdx.x the blocks of its parity subgrids (the largest class's count)
+template <int D>
+static dim3 q2_grid(int M) {
+  int ncol = 1;
+  for (int k = 0; k < D; ++k) ncol *= 3;
+  long long nb = 1;
+  for (int col = 0; col < ncol; ++col) nb = std::max(nb, q2_class_blocks<D>(M, col));
+  return dim3((unsigned)nb, (unsigned)ncol);
+}
+
 void launch_spmv(const LevelView& L, const double* x, const double* b, double* y, const double* dv,
                  const Reduce* R, cudaStream_t st) {
   if (L.csr) {  // the reduction as a separate DR4096 pass
@@ -2242,11 +2444,12 @@ void launch_spmv(const LevelView& L, const double* x, const double* b, double* y
     return;
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  if (L.order == 2) {  // sliced storage: one row per thread, the reduction as a separate DR4096 pass
+  if (L.order == 2) {  // rows by colour class and parity, the reduction as a separate DR4096 pass
     const Q2Layout lay = q2_layout(L.dim, L.M);
     Q2_DISPATCH(L.dim, {
-      if (b) k_spmv_q2<D, true><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, lay);
-      else k_spmv_q2<D, false><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, x, b, y, lay);
+      const dim3 g = q2_grid<D>((int)L.M);
+      if (b) k_spmv_q2c<D, true><<<g, kQ2T, 0, st>>>(L.A, L.Np, (int)L.M, x, b, y, lay);
+      else k_spmv_q2c<D, false><<<g, kQ2T, 0, st>>>(L.A, L.Np, (int)L.M, x, b, y, lay);
     });
     if (dv) launch_dot(y, dv, L.N, *R, st);
     return;
@@ -2304,11 +2507,11 @@ void launch_jacobi_res(const LevelView& L, double damp, const double* x, const d
     if (dv) launch_dot(xout, dv, 3 * L.N, *R, st);
     return;
   }
-  if (L.order == 2) {  // sliced storage
+  if (L.order == 2) {  // rows by colour class and parity
     const Q2Layout lay = q2_layout(L.dim, L.M);
     Q2_DISPATCH(L.dim, {
-      k_jacobi_res_q2<D><<<grid1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, damp, L.omega, x, b, xout, r,
-                                                        write_r ? 1 : 0, lay);
+      k_jacobi_res_q2c<D><<<q2_grid<D>((int)L.M), kQ2T, 0, st>>>(L.A, L.Np, (int)L.M, damp, L.omega, x, b, xout, r,
+                                                                 write_r ? 1 : 0, lay);
     });
     if (dv) launch_dot(xout, dv, L.N, *R, st);
     return;
@@ -2347,9 +2550,16 @@ void launch_sor(const LevelView& L, double omega, double* x, const double* b, do
     long long cnt = (L.M - cx + Q - 1) / Q;
     if (L.dim > 1) cnt *= (L.M - cy + Q - 1) / Q;
     if (L.dim > 2) cnt *= (L.M - cz + Q - 1) / Q;
-    FMG_DISPATCH(L.dim, L.order, {
-      k_sor_colour<D, P><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, L.omega, x, b, r, lay);
-    });
+    if (L.order == 2) {
+      Q2_DISPATCH(L.dim, {
+        const unsigned nb = (unsigned)q2_class_blocks<D>((int)L.M, col);
+        if (nb) k_sor_q2<D><<<nb, kQ2T, 0, st>>>(L.A, L.Np, (int)L.M, col, omega, L.omega, x, b, r, lay);
+      });
+    } else {
+      Q1_DISPATCH(L.dim, {
+        k_sor_colour<D, 1><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, L.omega, x, b, r);
+      });
+    }
   }
 }
 
@@ -2385,8 +2595,7 @@ void launch_ssc(const LevelView& L, double omega, double* x, const double* b, do
       if (L.dim > 1) cnt *= (L.M - cy + 1) / 2;
       if (L.dim > 2) cnt *= (L.M - cz + 1) / 2;
       Q1_DISPATCH(L.dim, {
-        k_sor_colour<D, 1, true><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, nullptr, x, b, r,
-                                                                  Q2Layout{});
+        k_sor_colour<D, 1, true><<<grid1(cnt), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, col, omega, nullptr, x, b, r);
       });
     }
     return;
