@@ -21,6 +21,7 @@ FMG_CSR, FMG_CCS = 0, 1
 FMG_METHOD_MG, FMG_METHOD_CG_MG, FMG_METHOD_CG = 0, 1, 2
 FMG_MULTIPLICATIVE, FMG_ADDITIVE = 0, 1
 FMG_MXK_RESIDUAL, FMG_MXK_SMOOTH, FMG_MXK_MATVEC64 = 1, 2, 3
+FMG_MXK_RESTRICT, FMG_MXK_PROLONG, FMG_MXK_PRESMOOTH = 4, 5, 6
 
 _ERRNAMES = {-1: "FMG_ERR_ARG", -2: "FMG_ERR_CUDA", -3: "FMG_ERR_STATE", -4: "FMG_ERR_NOMEM",
              -5: "FMG_ERR_NUMERIC", -6: "FMG_ERR_UNSUPPORTED", -7: "FMG_ERR_IO"}

@@ -153,6 +153,10 @@ struct MixedState {
   float *rtop = nullptr, *r = nullptr, *q = nullptr, *qs = nullptr;  // FP32 top-level vectors
   float *zp = nullptr, *zs = nullptr;  // the in-solve judge: the plain cycle's result and its spare
   float* p32 = nullptr;             // FP32 search direction of the flexible CG
+  double *r64 = nullptr, *a64 = nullptr;  // FP64 residual and A p of the mixed solve (layout lay)
+  VLay lay;                         // layout of the top-level vectors above (rtop excepted):
+                                    // padded with the matrix-free top level, natural otherwise
+  long long cap = 0;                // elements each top-level vector holds
   float* wd = nullptr;              // top level: damping / diagonal per node (matrix-free smoothing)
   const float* wd_om = nullptr;     // the node damping and scalar damping wd was formed with
   float wd_w = 0.f;
@@ -956,7 +960,10 @@ static int ensure_buffers(fmg_grid* g) {
       return rc;
   }
   if ((rc = dalloc(g, &g->scal, S_COUNT))) return rc;
-  if ((rc = dalloc(g, &g->part, nchunks(T.Np * nc) + 1))) return rc;
+  // reduction partials: the longest top-level vector (the mixed solve's padded ones in 3D)
+  long long nred = T.Np * nc;
+  if (g->dim == 3) nred = std::max(nred, padded_lay((int)T.M, g->dmask).total);
+  if ((rc = dalloc(g, &g->part, nchunks(nred) + 1))) return rc;
   if ((rc = dalloc(g, (double**)&g->counter, 1))) return rc;
   double** tv[] = {&g->p, &g->a, &g->w, &g->w2, &g->q, &g->r, &g->xs, &g->xs2};
   for (double** v : tv)
@@ -2022,6 +2029,7 @@ MFArgs64 mf64_args(const fmg_grid* g, double damp) {
   m.k = g->kcell_d; m.omega = nullptr; m.N = L.N; m.M = (int)L.M; m.n = (int)L.n; m.dmask = g->dmask;
   m.hs = L.h / 12.0; m.w = damp;
   m.err = g->scal + S_MFERR;
+  m.xl = m.ol = m.yl = natural_lay((int)L.M, 3);
   return m;
 }
 
@@ -2050,11 +2058,16 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     const Lvl& T = g->lev[g->top];
     long long ncell = 1;
     for (int k = 0; k < g->dim; ++k) ncell *= T.n;
+    // top-level vectors: room for the padded layout where the grid has one
+    X.cap = T.Np;
+    if (g->dim == 3) X.cap = std::max(X.cap, (padded_lay((int)T.M, g->dmask).total + 63) / 64 * 64);
     float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32, &X.wd, &X.zp, &X.zs};
     for (float** v : tv)
-      if ((rc = mx_alloc_f(g, v, T.Np))) return rc;
+      if ((rc = mx_alloc_f(g, v, X.cap))) return rc;
+    if ((rc = dalloc(g, &X.r64, X.cap)) || (rc = dalloc(g, &X.a64, X.cap))) return rc;
     if ((rc = mx_alloc_f(g, &X.k32, ncell))) return rc;
-    const long long nparts = std::max({(long long)nchunks(T.Np), mx_top_blocks((int)T.M), T.Np / kBlock + 1}) + 1;
+    const long long nparts =
+        std::max({(long long)nchunks(X.cap), mx_top_blocks((int)T.M), X.cap / kBlock + 1}) + 1;
     if ((rc = dalloc(g, &X.sc, M_COUNT)) || (rc = dalloc(g, &X.part, 2 * nparts)) ||
         (rc = dalloc(g, (double**)&X.counter, 1)))
       return rc;
@@ -2087,6 +2100,17 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     V.A = X.A32[l]; V.om = L.omega ? X.om32[l] : nullptr;
     V.N = L.N; V.Np = L.Np; V.M = L.M; V.dim = g->dim; V.order = g->order; V.dmask = g->dmask;
   }
+  const VLay lay = mf ? padded_lay((int)g->lev[g->top].M, g->dmask)
+                     : natural_lay((int)g->lev[g->top].M, g->dim);
+  if (lay.front != X.lay.front || lay.py != X.lay.py || lay.pz != X.lay.pz || lay.total != X.lay.total) {
+    // a new layout: the padding of every top-level vector starts (and stays) zero
+    float* fv[] = {X.r, X.q, X.qs, X.p32, X.wd, X.zp, X.zs};
+    for (float* v : fv) FMG_CK(c, cudaMemsetAsync(v, 0, X.cap * sizeof(float), st));
+    FMG_CK(c, cudaMemsetAsync(X.r64, 0, X.cap * sizeof(double), st));
+    FMG_CK(c, cudaMemsetAsync(X.a64, 0, X.cap * sizeof(double), st));
+    X.lay = lay;
+    X.wd_ok = false;
+  }
   X.mf = mf;
   return launched(c, "mixed prepare");
 }
@@ -2109,6 +2133,7 @@ struct MixedMG {
     const bool wd = X.wd_ok && X.wd_om == a.omega && X.wd_w == a.w;
     a.wd = wd ? X.wd : nullptr;
     a.err = g->scal + S_MFERR;
+    a.xl = a.ol = a.yl = X.lay;
     return a;
   }
   // damping / diagonal of the top level for the damping now in use (once per
@@ -2127,10 +2152,17 @@ struct MixedMG {
              const double* v2, const Reduce2* R) {
     Lev32 L = X.lv[l];
     L.w = (float)c.damp;
-    if (l == g->top && top_mf() && !b_bf16 && !y_bf16)
-      mx_top_apply(mode, mf_args(), x, (const float*)b, (float*)y, v, v2, R, st);
-    else
+    if (l == g->top && top_mf() && !b_bf16 && !y_bf16) {
+      MFArgs a = mf_args();
+      if (a.omega && (mode == 2 || mode == 3) && !a.wd) {  // the padded smoothing takes its damping over d formed
+        prepare_wd();
+        a = mf_args();
+      }
+      if (mode <= 1) a.yl = natural_lay(a.M, 3);  // A x and residuals come out in the natural layout (rtop)
+      mx_top_apply(mode, a, x, (const float*)b, (float*)y, v, v2, R, st);
+    } else {
       mx_level_apply(mode, L, x, b, b_bf16, y, y_bf16, v, v2, R, st);
+    }
   }
   // V-cycle on level l from x = 0 for rhs b (FP32 on the top level, BF16
   // below); the result is left in X.x0[l] (top: *xq); with R the last top-level
@@ -2151,13 +2183,13 @@ struct MixedMG {
         std::swap(x, xn);
       }
     } else {
-      launch_fill((double*)x, (X.lv[l].Np + 1) / 2, 0.0, st);
+      launch_fill((double*)x, ((top ? X.lay.total : X.lv[l].Np) + 1) / 2, 0.0, st);
     }
     void* r = top ? (void*)X.rtop : (void*)X.rc[l];  // residual and restriction
     apply(l, 1, x, b, bbf, r, !top, nullptr, nullptr, nullptr);
     mx_restrict(X.lv[l], X.lv[l - 1], r, !top, X.bc[l - 1], X.x0[l - 1], st);
     vcycle(l - 1, X.bc[l - 1], nullptr, nullptr, nullptr, nullptr, nullptr);
-    mx_prolong(X.lv[l - 1], X.lv[l], X.x0[l - 1], x, st);
+    mx_prolong(X.lv[l - 1], X.lv[l], X.x0[l - 1], x, st, top ? &X.lay : nullptr);
     for (int s = 0; s < c.post_steps; ++s) {
       const bool last = top && R && s == c.post_steps - 1;
       apply(l, 2, x, b, bbf, xn, false, last ? v : nullptr, last ? v2 : nullptr, last ? R : nullptr);
@@ -2168,7 +2200,10 @@ struct MixedMG {
   void matvec64(const float* p, double* a, const Reduce2& Rl) {
     const LevelView T = view(g, g->top);
     if (top_mf()) {
-      mx_top_apply64(mf64_args(g, c.damp), p, a, p, &Rl, st);
+      MFArgs64 m = mf64_args(g, c.damp);
+      m.xl = X.lay;                    // p: a top-level FP32 vector
+      if (a == X.a64) m.yl = X.lay;    // the CG's A p; elsewhere (the judge's scratch) natural
+      mx_top_apply64(m, p, a, p, &Rl, st);
     } else {  // stored FP64 matrix: widen p first
       mx_f32_to_f64(p, g->xs2, T.N, st);
       launch_spmv(T, g->xs2, nullptr, a, nullptr, nullptr, st);
@@ -2469,7 +2504,10 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   const long long n = T.N;
   double* x = xv->d;
   const double* b = g->rhs;
-  double *r = g->r, *a = g->a;
+  // the CG's vectors: padded with the matrix-free top level (its kernels take
+  // them by tensor copy), the solvers' natural ones otherwise
+  double *r = X.mf ? X.r64 : g->r, *a = X.mf ? X.a64 : g->a;
+  const long long nv = X.mf ? X.lay.total : n;  // elements of the top-level vectors, padding included
   float* p = X.p32;
   *status = 1;
   *nouter = 0;
@@ -2486,10 +2524,17 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   for (int restart = 0; restart <= max_restart; ++restart) {
     // true FP64 residual (x = 0: r = b exactly), from the cell coefficients
     // where the top level is matrix-free, else with the assembled matrix
-    if (restart == 0 && g->x_zero) launch_copy(b, r, n, st);
-    else if (mg.top_mf()) mx_top_residual64(mf64_args(g, cfg->damp), x, b, r, st);
-    else launch_spmv(T, x, b, r, nullptr, nullptr, st);
-    launch_dot(r, r, n, reducer(g, EPI_STORE, S_RR), st);
+    if (restart == 0 && g->x_zero) {
+      if (X.mf) mx_f64_copy_lay(b, r, X.lay, (int)T.M, st);
+      else launch_copy(b, r, n, st);
+    } else if (mg.top_mf()) {
+      MFArgs64 m = mf64_args(g, cfg->damp);
+      m.yl = X.lay;
+      mx_top_residual64(m, x, b, r, st);
+    } else {
+      launch_spmv(T, x, b, r, nullptr, nullptr, st);
+    }
+    launch_dot(r, r, nv, reducer(g, EPI_STORE, S_RR), st);
     if ((rc = read_scalars(g))) return rc;
     const double dn = std::sqrt(c->host_scal[S_RR]);
     if (!std::isfinite(dn)) return set_err(c, FMG_ERR_NUMERIC, "defnorm is %g", dn);
@@ -2506,11 +2551,11 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     if ((rc = mx_set_scalar(g, M_SCALE, dn > 0 ? 1.0 / dn : 1.0))) return rc;
     if ((rc = mx_set_scalar(g, M_SUSED, dn > 0 ? 1.0 / dn : 1.0))) return rc;
     if ((rc = mx_set_scalar(g, M_SINV, dn > 0 ? dn : 1.0))) return rc;
-    mx_scale_to32(r, X.sc, M_SCALE, X.r, T.Np, st);
+    mx_scale_to32(r, X.sc, M_SCALE, X.r, X.mf ? nv : T.Np, st);
     {
       const Reduce2 Rr = red2(X, EPI2_RHO, 0, 0);
       mg.vcycle(g->top, X.r, &X.q, &X.qs, r, nullptr, &Rr);
-      mx_fcg64_p(X.sc, p, X.q, n, true, st);
+      mx_fcg64_p(X.sc, p, X.q, nv, true, st);
     }
     bool converged = false;
     const int it0 = iters;
@@ -2520,15 +2565,15 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     auto step_body = [&]() {
       const Reduce2 Rf = red2(X, EPI2_FCG, 0, 0);
       mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
-      mx_fcg64_p(X.sc, p, X.q, n, false, st);
+      mx_fcg64_p(X.sc, p, X.q, nv, false, st);
       mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
-      mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
+      mx_fcg64_update(X.sc, x, p, r, a, X.r, X.lay, (int)T.M, g->dim, red2(X, EPI2_UPDATE, 0, 0), st);
       cudaMemcpyAsync(X.host, X.sc, M_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st);
     };
     while (iters <= cfg->maxsteps) {
       if (iters == it0) {
         mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
-        mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
+        mx_fcg64_update(X.sc, x, p, r, a, X.r, X.lay, (int)T.M, g->dim, red2(X, EPI2_UPDATE, 0, 0), st);
         if ((rc = launched(c, "mixed step"))) return rc;
         if ((rc = mx_read(g))) return rc;
       } else if (shadow && iters - it0 <= mcfg->judge) {
@@ -2562,9 +2607,9 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
           revert_restart = true;
           break;
         }
-        mx_fcg64_p(X.sc, p, X.q, n, false, st);
+        mx_fcg64_p(X.sc, p, X.q, nv, false, st);
         mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
-        mx_fcg64_update(X.sc, x, p, r, a, X.r, T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
+        mx_fcg64_update(X.sc, x, p, r, a, X.r, X.lay, (int)T.M, g->dim, red2(X, EPI2_UPDATE, 0, 0), st);
         if ((rc = launched(c, "mixed step"))) return rc;
         if ((rc = mx_read(g))) return rc;
       } else {
@@ -2624,8 +2669,10 @@ extern "C" int fmg_matvec_mf(fmg_grid* g, int fp32, const fmg_vec* x, const fmg_
     int rc = mixed_prepare(g, true);
     if (rc) return rc;
     MixedState& X = *g->mx;
-    mx_f64_to_f32(x->d, X.q, g->lev[g->top].N, st);
-    mx_top_apply64(mf64_args(g, 0.0), X.q, y->d, X.q, nullptr, st);
+    mx_f64_to_f32_lay(x->d, X.q, X.lay, (int)g->lev[g->top].M, st);
+    MFArgs64 m = mf64_args(g, 0.0);
+    m.xl = X.lay;
+    mx_top_apply64(m, X.q, y->d, X.q, nullptr, st);
   } else {
     int rc = mixed_prepare(g, true);
     if (rc) return rc;
@@ -2634,9 +2681,12 @@ extern "C" int fmg_matvec_mf(fmg_grid* g, int fp32, const fmg_vec* x, const fmg_
     fmg_solve_cfg c{};
     c.damp = 1.0;
     MixedMG mg{g, X, c, st};
-    mx_f64_to_f32(x->d, X.q, n, st);
-    if (b) mx_f64_to_f32(b->d, X.r, n, st);
-    mx_top_apply(b ? 1 : 0, mg.mf_args(), X.q, b ? X.r : nullptr, X.qs, nullptr, nullptr, nullptr, st);
+    const int M = (int)g->lev[g->top].M;
+    mx_f64_to_f32_lay(x->d, X.q, X.lay, M, st);
+    if (b) mx_f64_to_f32_lay(b->d, X.r, X.lay, M, st);
+    MFArgs a = mg.mf_args();
+    a.yl = natural_lay(M, 3);
+    mx_top_apply(b ? 1 : 0, a, X.q, b ? X.r : nullptr, X.qs, nullptr, nullptr, nullptr, st);
     mx_f32_to_f64(X.qs, y->d, n, st);
   }
   FMG_RC(launched(g->ctx, "matvec_mf"));
@@ -2646,9 +2696,9 @@ extern "C" int fmg_matvec_mf(fmg_grid* g, int fp32, const fmg_vec* x, const fmg_
 extern "C" int fmg_mixed_top_kernel(fmg_grid* g, int kind, int reps) {
   if (g && g->nb > 1) return set_err(g->ctx, FMG_ERR_UNSUPPORTED, "%s: not on a batch", __func__);
   if (!g) return FMG_ERR_ARG;
-  if (!g->mx || !g->mx->mf || !g->mx->wd_ok || !g->r || !g->a)
+  if (!g->mx || !g->mx->mf || !g->mx->wd_ok || !g->mx->r64 || !g->mx->a64)
     return set_err(g->ctx, FMG_ERR_STATE, "fmg_mixed_top_kernel: no matrix-free mixed solve has run on this grid");
-  if (reps < 1 || kind < FMG_MXK_RESIDUAL || kind > FMG_MXK_MATVEC64)
+  if (reps < 1 || kind < FMG_MXK_RESIDUAL || kind > FMG_MXK_PRESMOOTH)
     return set_err(g->ctx, FMG_ERR_ARG, "fmg_mixed_top_kernel: kind %d, reps %d", kind, reps);
   MixedState& X = *g->mx;
   fmg_solve_cfg c{};
@@ -2658,8 +2708,13 @@ extern "C" int fmg_mixed_top_kernel(fmg_grid* g, int kind, int reps) {
   const Reduce2 R = red2(X, EPI2_STORE, M_TMP, M_TMP);
   for (int k = 0; k < reps; ++k) {
     if (kind == FMG_MXK_RESIDUAL) mg.apply(g->top, 1, X.q, X.r, false, X.rtop, false, nullptr, nullptr, nullptr);
-    else if (kind == FMG_MXK_SMOOTH) mg.apply(g->top, 2, X.q, X.r, false, X.qs, false, g->r, g->a, &R);
-    else mg.matvec64(X.p32, g->a, R);
+    else if (kind == FMG_MXK_SMOOTH) mg.apply(g->top, 2, X.q, X.r, false, X.qs, false, X.r64, X.a64, &R);
+    else if (kind == FMG_MXK_MATVEC64) mg.matvec64(X.p32, X.a64, R);
+    else if (kind == FMG_MXK_RESTRICT)
+      mx_restrict(X.lv[g->top], X.lv[g->top - 1], X.rtop, false, X.bc[g->top - 1], X.x0[g->top - 1], g->ctx->stream);
+    else if (kind == FMG_MXK_PROLONG)
+      mx_prolong(X.lv[g->top - 1], X.lv[g->top], X.x0[g->top - 1], X.q, g->ctx->stream, &X.lay);
+    else mg.apply(g->top, 3, nullptr, X.r, false, X.q, false, nullptr, nullptr, nullptr);
   }
   return launched(g->ctx, "mixed_top_kernel");
 }

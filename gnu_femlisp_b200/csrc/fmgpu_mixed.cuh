@@ -20,17 +20,38 @@ struct Reduce2 {
   int epi, slot0, slot1;
 };
 
+// Where a top-level vector keeps node (ix, iy, iz): at front + ix + py iy +
+// pz iz.  Natural: front 0, py = M, pz = M^2.  Padded (the FP32 vectors and
+// the FP64 residual and A p of the matrix-free mixed solve): rows of py = 4k
+// elements and front = (4 - l) % 4, l = 1 when the face x = 0 is Dirichlet,
+// so that the row start of the first node off that face sits on a 16-byte
+// boundary -- a plane's tile of such a vector is one tensor copy.  The
+// padding stays zero.
+struct VLay {
+  int front = 0, py = 0;
+  long long pz = 0, total = 0;  // total: elements of the array (pads included)
+  __host__ __device__ __forceinline__ long long at(int ix, int iy, int iz) const {
+    return front + ix + (long long)py * iy + pz * iz;
+  }
+};
+VLay natural_lay(int M, int dim);
+VLay padded_lay(int M, int dmask);
+
 // matrix-free 3D Q1 top level
 template <typename T>
 struct MFArgsT {
   const T* k;          // coefficient per cell (n^3)
-  const T* omega;      // per-node damping or nullptr
+  const T* omega;      // per-node damping or nullptr (natural layout)
   long long N;
   int M, n, dmask;
   T hs;                // h / 12
   T w;                 // scalar damping
   const T* wd = nullptr;  // per-node damping / diagonal (mx_top_wd), or nullptr: formed in the kernel
   double* err = nullptr;  // set to 1 by a CTA whose bounded wait for a copy ran out
+  // layouts of x, of the per-node operands (b, wd, the reduction vectors) and
+  // of the output y.  An FP32 x comes by tensor copy and must be padded, so
+  // must the operands of the FP32 modes; FP64 x and operands are natural.
+  VLay xl, ol, yl;
 };
 typedef MFArgsT<float> MFArgs;
 typedef MFArgsT<double> MFArgs64;
@@ -57,17 +78,22 @@ void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, doub
 long long mx_top_blocks(int M);  // blocks of the matrix-free kernel (reduction partials)
 // wd = damping / diagonal per top-level node (Dirichlet nodes: the damping)
 // for the smoothing modes of mx_top_apply
-void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st);
+void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st);  // wd in g.ol
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
                     const double* v, const double* v2, const Reduce2* R, cudaStream_t st);
 void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, __nv_bfloat16* bc, float* xc,
                  cudaStream_t st);
-void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cudaStream_t st);
+void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cudaStream_t st,
+                const VLay* xfl = nullptr);  // xfl: the layout of xf (natural if null)
 void mx_coarse(const double* AinvT, int n, const __nv_bfloat16* b, float* x, cudaStream_t st);
 void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st);
-// FP64 flexible CG: x += lam p, r -= lam a, (r,r), r32 = r * scale (np = padded length)
-void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
-                     const Reduce2& R, cudaStream_t st);
+// b (layout bl) = a (natural, M nodes a side, 3D)
+void mx_f64_to_f32_lay(const double* a, float* b, const VLay& bl, int M, cudaStream_t st);
+void mx_f64_copy_lay(const double* a, double* b, const VLay& bl, int M, cudaStream_t st);
+// FP64 flexible CG: x += lam p, r -= lam a, (r,r), r32 = r * scale; p, r, a
+// and r32 in layout pl, x natural (M nodes a side, dim directions)
+void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, const VLay& pl,
+                     int M, int dim, const Reduce2& R, cudaStream_t st);
 // p = q / s + beta p (FP32 search direction)
 void mx_fcg64_p(const double* sc, float* p, const float* q, long long n, bool first, cudaStream_t st);
 void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st);

@@ -153,6 +153,8 @@ constexpr int kFX = 32, kFY = 16, kFZ = 32;   // tile: nodes along x, y; planes 
 constexpr int kFRows = kFY + 2;               // x rows of a plane (y0-1 .. y0+16)
 constexpr int kFCRows = kFY + 1;              // cell rows of a plane (y0-1 .. y0+15)
 constexpr int kFPW = kFX + 2;                 // packed row: x0-1 .. x0+32
+constexpr int kXW = 40;                       // tensor-copy halo row: 40 FP32 from the 16-byte boundary at or below x0-1
+constexpr int kOW = 36;                       // operand box row: 36 elements from tensor x0 (node x0 - front)
 constexpr int kFThreads = 256;
 constexpr int kFaceNodes = 1024;              // nodes per face CTA
 
@@ -226,10 +228,11 @@ __device__ __forceinline__ void mf_face_cta(const MFArgsT<T>& g, const MftGeo& g
     if (f >= geo.F) break;
     int ix, iy, iz;
     face_node(f, geo, M, ix, iy, iz);
-    const long long i = (long long)iz * MM + (long long)iy * M + ix;
+    const long long in = (long long)iz * MM + (long long)iy * M + ix;  // natural (omega)
+    const long long io = g.ol.at(ix, iy, iz);                          // operands
     T ax, d, xc;
     if (dirf(ix, 1, 2) || dirf(iy, 4, 8) || dirf(iz, 16, 32)) {
-      xc = HX ? (T)x[i] : T(0);
+      xc = HX ? (T)x[g.xl.at(ix, iy, iz)] : T(0);
       ax = xc;
       d = T(1);
     } else {
@@ -248,17 +251,18 @@ __device__ __forceinline__ void mf_face_cta(const MFArgsT<T>& g, const MftGeo& g
         const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
         const bool in = jx >= 0 && jx < M && jy >= 0 && jy < M && jz >= 0 && jz < M && !dirf(jx, 1, 2) &&
                         !dirf(jy, 4, 8) && !dirf(jz, 16, 32);
-        return in ? (T)x[(long long)jz * MM + (long long)jy * M + jx] : T(0);
+        return in ? (T)x[g.xl.at(jx, jy, jz)] : T(0);
       };
       mf_row<T, HX, DIFF>(k, X, g.hs, ax, d, xc);
     }
-    const T bb = HB ? __ldg(b + i) : T(0);
-    const T o = (HO && uwd) ? __ldg(g.wd + i) : ((HO && g.omega) ? __ldg(g.omega + i) : g.w);
+    const T bb = HB ? __ldg(b + io) : T(0);
+    const T o = (HO && uwd) ? __ldg(g.wd + io) : ((HO && g.omega) ? __ldg(g.omega + in) : g.w);
     const T out = mf_out<MODE>(ax, d, xc, bb, o, uwd);
-    y[i] = out;
+    y[g.yl.at(ix, iy, iz)] = out;
     if (RED) {
-      acc0 = fma((double)out, (double)v[i], acc0);
-      if (v2) acc1 = fma((double)out, (double)v2[i], acc1);
+      constexpr bool VX = sizeof(T) == 8;  // the FP64 operator reduces (A p, p): the vector is x itself
+      acc0 = fma((double)out, VX ? (double)xc : (double)v[io], acc0);
+      if (v2) acc1 = fma((double)out, (double)v2[io], acc1);
     }
   }
 }
@@ -271,34 +275,49 @@ __device__ __forceinline__ void mf_face_cta(const MFArgsT<T>& g, const MftGeo& g
 // cells a side -- and the Dirichlet faces x, y, z = 0 inside it (identity
 // rows), 1024 nodes each.  FP32 arithmetic, or FP64 in difference form with
 // each x value widened once as it enters the registers.
-// A stage of a tiled CTA's 6-slot shared-memory ring holds what one step
-// reads: the 18 x 34 x halo of the plane above (cp.async per element,
-// eliminated and outside entries zero-filled at the copy), the 17 x 36 cell
-// tile (one TMA box) and the per-node operands of the step's own plane (b, the
-// damping, the FP64 reduction vectors: each thread copies its own two
-// nodes').  All copies of a stage complete on its full mbarrier (256 cp.async
-// arrivals + the TMA's expect-tx arrival); each warp releases a stage on its
-// empty mbarrier once it has read it, and a slot is refilled only after all 8
-// warps have released it, so warps drift apart by a few steps and no block
-// barrier is needed.  Stages are requested three steps before they are read.
+// A stage of a tiled CTA's shared-memory ring (6 slots, 5 for the smoothing
+// mode) holds what one step reads: the x halo of the plane above, the 17 x 36
+// cell tile (one TMA box) and the per-node operands of the step's own plane
+// (b, the damping, the FP64 reduction vectors).  An FP32 x and the FP32
+// modes' operands are kept padded, so each comes as one TMA box per stage:
+// the 18 x 40 halo from the 16-byte boundary at or below node x0 - 1 of a map
+// that leaves out the Dirichlet faces (they and the outside read as zero),
+// and 16 x 36 operand boxes from node x0 - front.  An FP64 x (the true
+// residual of FP64 vectors) comes by cp.async per element (18 x 34, the
+// eliminated and outside entries zero-filled at the copy), its operands by a
+// cp.async per node and thread.  All copies of a stage complete on its full
+// mbarrier (the TMA's expect-tx arrival, plus 256 cp.async arrivals where
+// there are any); each warp releases a stage on its empty mbarrier once it has
+// read it, and a slot is refilled only after all 8 warps have released it, so
+// warps drift apart by a few steps and no block barrier is needed.  Stages are
+// requested two or three steps before they are read.
 // A thread keeps the x values and cells its two nodes read in registers as it
 // marches z, reading each plane once (the loop runs three steps per turn so
 // register roles rotate at compile time).
-constexpr int kCRing = 6;   // ring slots
-constexpr int kCLook = 5;   // stage j is requested at step j-5 and read at step j-2
+constexpr int kCRing = 6;   // ring slots (5 where six stages would not leave room for two CTAs per SM)
 constexpr int kPX = kFPW;   // packed x row: x0-1 .. x0+32
 
 template <typename T, typename TV, typename TX, int MODE, bool RED>
 struct MfcLayout {
   static constexpr bool HB = MODE != 0, HO = MODE == 2 || MODE == 3, HX = MODE != 3;
+  static constexpr bool XT = sizeof(TX) == 4;        // an FP32 x halo comes by tensor copy (padded x)
+  static constexpr bool OT = sizeof(T) == 4;         // so do the FP32 modes' operands (padded)
+  static constexpr bool VX = RED && sizeof(T) == 8;  // the FP64 operator reduces (A p, p): v is x
+  static constexpr bool HV = RED && !VX;             // reduction vectors to load
   static constexpr int up(int b) { return (b + 127) / 128 * 128; }
-  static constexpr int XS = HX ? up(kFRows * kPX * (int)sizeof(TX)) : 0;  // packed x halo
+  static constexpr int XR = XT ? kXW : kPX;          // halo row
+  static constexpr int XS = HX ? up(kFRows * XR * (int)sizeof(TX)) : 0;  // x halo
   static constexpr int CS = up(kFCRows * CellBox<T>::CW * (int)sizeof(T));  // cell box (TMA)
-  static constexpr int OB = HB ? up(2 * kFThreads * (int)sizeof(T)) : 0;  // b of the step's plane
-  static constexpr int OO = HO ? up(2 * kFThreads * (int)sizeof(T)) : 0;  // damping
-  static constexpr int OV = RED ? up(2 * kFThreads * (int)sizeof(TV)) : 0;  // reduction vectors
+  static constexpr int OPN = OT ? kFY * kOW : 2 * kFThreads;  // operand elements of a stage
+  static constexpr int OB = HB ? up(OPN * (int)sizeof(T)) : 0;  // b of the step's plane
+  static constexpr int OO = HO ? up(OPN * (int)sizeof(T)) : 0;  // damping
+  static constexpr int OV = HV ? up(OPN * (int)sizeof(TV)) : 0;  // reduction vectors
   static constexpr int SB = XS + CS + OB + OO + 2 * OV;
-  static constexpr int SMEM = kCRing * SB + 2 * kCRing * 8 + 128;
+  static constexpr int NR = SB * kCRing > 100 * 1024 ? kCRing - 1 : kCRing;  // ring slots: two CTAs per SM
+  static constexpr int LOOK = NR - 1;  // stage j is requested at step j - LOOK and read at step j - 2
+  static constexpr int SMEM = NR * SB + 2 * NR * 8 + 128;
+  // every copy of a stage is a tensor copy: its full barrier takes one arrival
+  static constexpr bool ALLT = (!HX || XT) && (OT || !(HB || HO || HV));
 };
 
 __device__ __forceinline__ void cpa(void* dst, const void* src, bool ok, int bytes) {
@@ -317,9 +336,11 @@ __device__ __forceinline__ void cpa_arrive(uint64_t* bar) {
 // vector, 4 the damping already divided by the diagonal (g.wd)
 template <typename T, typename TV, typename TX, int MODE, bool RED, int OPT>
 __global__ void __launch_bounds__(kFThreads, (sizeof(T) == 4 && MODE != 2) ? 3 : 2)
-k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, const TX* __restrict__ x,
-      const T* __restrict__ b, T* __restrict__ y, const TV* __restrict__ v, const TV* __restrict__ v2,
-      Reduce2 R) {
+k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, const __grid_constant__ CUtensorMap tm_x,
+      const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_o,
+      const __grid_constant__ CUtensorMap tm_v, const __grid_constant__ CUtensorMap tm_v2, MftGeo geo,
+      const TX* __restrict__ x, const T* __restrict__ b, T* __restrict__ y, const TV* __restrict__ v,
+      const TV* __restrict__ v2, Reduce2 R) {
   typedef MfcLayout<T, TV, TX, MODE, RED> L;
   typedef CellBox<T> LC;
   constexpr bool DIFF = sizeof(T) == 8;  // the FP64 operator in difference form
@@ -340,14 +361,21 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     const int bx = bid % geo.nbx, by = (bid / geo.nbx) % geo.nby, bz = bid / (geo.nbx * geo.nby);
     const int x0 = bx * kFX, y0 = by * kFY, z0 = bz * kFZ;
     const int lx = tid & 31, ly = tid >> 5;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sm + kCRing * L::SB);
-    uint64_t* empty = full + kCRing;
+    constexpr int NR = L::NR, LOOK = L::LOOK;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + NR * L::SB);
+    uint64_t* empty = full + NR;
     if (tid == 0)
-      for (int s = 0; s < kCRing; ++s) {
-        umma::mbar_init_count(&full[s], kFThreads + 1);
+      for (int s = 0; s < NR; ++s) {
+        umma::mbar_init_count(&full[s], L::ALLT ? 1 : kFThreads + 1);
         umma::mbar_init_count(&empty[s], kFThreads / 32);
       }
     __syncthreads();
+    // tensor-copy halo: its box starts on the 16-byte boundary at or below
+    // node x0 - 1 of the map, which leaves out the Dirichlet faces (so that
+    // they, like the outside, read as zero); node x0 - 1 sits at column xoff
+    const int lox = dm & 1, loy = (dm >> 2) & 1, loz = (dm >> 4) & 1;
+    const int xoff = (3 - lox) & 3;
+    const int fr = g.ol.front;  // operand boxes start at tensor x0: node x0 + c at column c + front
     const int last = kFZ + 1;
     // this thread's share of the x halo: elements tid, tid+256, tid+512 of 18 x 34
     int hoff[3];
@@ -361,7 +389,6 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
       hoff[q] = hok[q] ? yy * M + xx : 0;
     }
     const int ix = x0 + lx, iy0 = y0 + 2 * ly;
-    const long long ibase = (long long)iy0 * M + ix;
     bool ok = true;  // every wait of this warp so far completed; after one gives up, the rest wait 1 ms at most
     auto wait = [&](uint64_t* bar, uint32_t parity) {
       bool w = umma::mbar_test(bar, parity);
@@ -369,19 +396,34 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
       ok = __all_sync(0xffffffffu, w) && ok;
     };
     // stage j: x plane z0-1+j, cell plane z0-2+j, operands of plane z0-2+j, in
-    // ring slot j % kCRing; the issue and read streams count slots and phases
+    // ring slot j % NR; the issue and read streams count slots and phases
     int is = 0, rs = 0;          // slot of the next stage to request / to read
     uint32_t ip = 0u, rp = 0u;   // its phase parity
     auto issue = [&](int j) {
       const int s = is;
-      if (j >= kCRing) wait(&empty[s], ip ^ 1u);  // all warps released the slot's previous stage
+      if (j >= NR) wait(&empty[s], ip ^ 1u);  // all warps released the slot's previous stage
       unsigned char* st = sm + s * L::SB;
+      const int zo = z0 - 2 + j;  // the operands' plane
+      const bool ops = zo >= z0 && (HB || HO || L::HV);
       if (tid == 0) {
+        uint32_t tx = LC::CTX;
+        if (HX && L::XT) tx += kFRows * kXW * (uint32_t)sizeof(TX);
+        if (L::OT && ops)
+          tx += (uint32_t)L::OPN * ((HB ? (uint32_t)sizeof(T) : 0u) + (OM ? (uint32_t)sizeof(T) : 0u) +
+                                    (L::HV ? (uint32_t)sizeof(TV) : 0u) + (V2 ? (uint32_t)sizeof(TV) : 0u));
         umma::fence_async_smem();
-        umma::mbar_arrive_expect_tx(&full[s], LC::CTX);
+        umma::mbar_arrive_expect_tx(&full[s], tx);
         umma::tma_load_3d(st + L::XS, &tk_cells, &full[s], x0 - 1 - LC::COFF, y0 - 1, z0 - 2 + j);
+        if (HX && L::XT) umma::tma_load_3d(st, &tm_x, &full[s], x0 - 1 - xoff - lox, y0 - 1 - loy, z0 - 1 + j - loz);
+        if (L::OT && ops) {
+          unsigned char* op = st + L::XS + L::CS;
+          if (HB) umma::tma_load_3d(op, &tm_b, &full[s], x0, y0, zo);
+          if (OM) umma::tma_load_3d(op + L::OB, &tm_o, &full[s], x0, y0, zo);
+          if (L::HV) umma::tma_load_3d(op + L::OB + L::OO, &tm_v, &full[s], x0, y0, zo);
+          if (V2) umma::tma_load_3d(op + L::OB + L::OO + L::OV, &tm_v2, &full[s], x0, y0, zo);
+        }
       }
-      if (HX) {
+      if (HX && !L::XT) {
         const int z = z0 - 1 + j;
         const bool zok = z >= 0 && z < M && !dirf(z, 16, 32);
         const TX* pl = x + (zok ? (long long)z * MM : 0ll);
@@ -392,21 +434,20 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
           if (q < 2 || e < kFRows * kPX) cpa(xs + e, pl + hoff[q], zok && hok[q], (int)sizeof(TX));
         }
       }
-      const int zo = z0 - 2 + j;  // the operands' plane
-      if (zo >= z0 && (HB || HO || RED)) {
+      if (!L::OT && ops) {
         unsigned char* op = st + L::XS + L::CS;
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-          const long long i = (long long)zo * MM + ibase + r * M;
+          const long long i = g.ol.at(ix, iy0 + r, zo);
           const int k = r * kFThreads + tid;
           if (HB) cpa(reinterpret_cast<T*>(op) + k, b + i, true, (int)sizeof(T));
           if (OM) cpa(reinterpret_cast<T*>(op + L::OB) + k, om_src + i, true, (int)sizeof(T));
-          if (RED) cpa(reinterpret_cast<TV*>(op + L::OB + L::OO) + k, v + i, true, (int)sizeof(TV));
+          if (L::HV) cpa(reinterpret_cast<TV*>(op + L::OB + L::OO) + k, v + i, true, (int)sizeof(TV));
           if (V2) cpa(reinterpret_cast<TV*>(op + L::OB + L::OO + L::OV) + k, v2 + i, true, (int)sizeof(TV));
         }
       }
-      cpa_arrive(&full[s]);
-      if (++is == kCRing) {
+      if (!L::ALLT) cpa_arrive(&full[s]);
+      if (++is == NR) {
         is = 0;
         ip ^= 1u;
       }
@@ -415,11 +456,11 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
       wait(&full[rs], rp);
       const unsigned char* st = sm + rs * L::SB;
       if (HX) {
-        const TX* xs = reinterpret_cast<const TX*>(st);
+        const TX* xs = reinterpret_cast<const TX*>(st) + (L::XT ? xoff : 0);
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) xv[k][c] = (T)xs[(2 * ly + k) * kPX + lx + c];
+          for (int c = 0; c < 3; ++c) xv[k][c] = (T)xs[(2 * ly + k) * L::XR + lx + c];
       }
       if (want_k) {
         const T* cs = reinterpret_cast<const T*>(st + L::XS);
@@ -432,13 +473,13 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     auto release = [&]() {  // the stage just read; the read stream moves on
       __syncwarp();
       if (lx == 0) umma::mbar_arrive(&empty[rs]);
-      if (++rs == kCRing) {
+      if (++rs == NR) {
         rs = 0;
         rp ^= 1u;
       }
     };
     T xr[3][4][3], kr[3][3][2];
-    for (int j = 0; j < kCLook && j <= last; ++j) issue(j);
+    for (int j = 0; j < LOOK && j <= last; ++j) issue(j);
     consume(xr[0], kr[1], false);  // stage 0: x plane z0-1 (its cell plane is not read)
     release();
     consume(xr[1], kr[0], true);   // stage 1: x plane z0, cell plane z0-1
@@ -451,23 +492,22 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
     auto step = [&](auto Qc, int t) {
       constexpr int Q = decltype(Qc)::value;
       constexpr int PM = Q % 3, P0 = (Q + 1) % 3, PP = (Q + 2) % 3, CM = Q % 3, C0 = (Q + 1) % 3;
-      if (t + kCLook <= last) issue(t + kCLook);
+      if (t + LOOK <= last) issue(t + LOOK);
       consume(xr[PP], kr[C0], true);  // stage t+2
       const unsigned char* op = sm + rs * L::SB + L::XS + L::CS;
       T bb[2], oo[2];
       TV vv[2], vv2[2];
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
-        const int k = r * kFThreads + tid;
+        const int k = L::OT ? (2 * ly + r) * kOW + lx + fr : r * kFThreads + tid;
         bb[r] = HB ? reinterpret_cast<const T*>(op)[k] : T(0);
         oo[r] = OM ? reinterpret_cast<const T*>(op + L::OB)[k] : g.w;
-        vv[r] = RED ? reinterpret_cast<const TV*>(op + L::OB + L::OO)[k] : TV(0);
+        vv[r] = L::HV ? reinterpret_cast<const TV*>(op + L::OB + L::OO)[k] : TV(0);
         vv2[r] = V2 ? reinterpret_cast<const TV*>(op + L::OB + L::OO + L::OV)[k] : TV(0);
       }
       release();
       const int iz = z0 + t;
       const bool dirz = dirf(iz, 16, 32);
-      const long long i0 = (long long)iz * MM + ibase;
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         T k[2][2][2];
@@ -485,9 +525,9 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, MftGeo geo, co
         mf_row<T, HX, DIFF>(k, X, hs, ax, d, xc);
         const T out = mf_out<MODE>(ax, d, xc, bb[r], oo[r], UWD);
         if (!(dirz || dirx || (r ? diry1 : diry0))) {  // identity rows: the face CTAs
-          y[i0 + r * M] = out;
+          y[g.yl.at(ix, iy0 + r, iz)] = out;
           if (RED) {
-            acc0 = fma((double)out, (double)vv[r], acc0);
+            acc0 = fma((double)out, L::VX ? (double)xc : (double)vv[r], acc0);
             if (V2) acc1 = fma((double)out, (double)vv2[r], acc1);
           }
         }
@@ -621,6 +661,50 @@ k_restrict_q1(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat1
   xc[J] = 0.f;
 }
 
+// 3D Q1 restriction through shared memory: a block (32, 8) of coarse nodes
+// in plane K first stages the fine nodes its sums read -- planes 2K-1 .. 2K+1,
+// rows 2J0-1 .. 2J0+15, columns 2I0-1 .. 2I0+63, converted to FP32, zero
+// outside the grid and on Dirichlet faces -- with coalesced row loads, then
+// sums each coarse node's 27 terms with the weights and in the order of
+// k_restrict_q1 (a zero weight there is a zero value here).
+constexpr int kRsX = 65, kRsY = 17;
+template <typename TR>
+__global__ void __launch_bounds__(kBlock)
+k_restrict_q1s(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat16* __restrict__ bc,
+               float* __restrict__ xc) {
+  __shared__ float t[3][kRsY][kRsX];
+  const int I0 = blockIdx.x * 32, J0 = blockIdx.y * 8, K = blockIdx.z;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const long long MF2 = (long long)MF * MF;
+  for (int e = tid; e < 3 * kRsY * kRsX; e += 32 * 8) {
+    const int z = e / (kRsY * kRsX), rem = e - z * (kRsY * kRsX), y = rem / kRsX, x = rem - y * kRsX;
+    const int fx = 2 * I0 - 1 + x, fy = 2 * J0 - 1 + y, fz = 2 * K - 1 + z;
+    const bool ok = fx >= 0 && fx < MF && fy >= 0 && fy < MF && fz >= 0 && fz < MF && !fdir(fx, MF, 0, dmask) &&
+                    !fdir(fy, MF, 1, dmask) && !fdir(fz, MF, 2, dmask);
+    t[z][y][x] = ok ? ldv(rf, fz * MF2 + (long long)fy * MF + fx) : 0.f;
+  }
+  __syncthreads();
+  const int cx = I0 + threadIdx.x, cy = J0 + threadIdx.y;
+  if (cx >= MC || cy >= MC) return;
+  const long long J = cx + (long long)MC * (cy + (long long)MC * K);
+  const bool dj = fdir(cx, MC, 0, dmask) || fdir(cy, MC, 1, dmask) || fdir(K, MC, 2, dmask);
+  float acc = 0.f;
+  if (!dj) {
+    const float w[3] = {.5f, 1.f, .5f};
+#pragma unroll
+    for (int z = 0; z < 3; ++z)
+#pragma unroll
+      for (int y = 0; y < 3; ++y) {
+        const float wyz = w[y] * w[z];
+        const float* row = &t[z][2 * threadIdx.y + y][2 * threadIdx.x];
+#pragma unroll
+        for (int xx = 0; xx < 3; ++xx) acc = fmaf(w[xx] * wyz, row[xx], acc);
+      }
+  }
+  bc[J] = __float2bfloat16_rn(acc);
+  xc[J] = 0.f;
+}
+
 // restriction of a residual (FP32 or BF16) into the coarse rhs (BF16), coarse
 // solution zeroed; blocks (32, 8) over x, y and one z plane per blockIdx.z
 template <int D, int P, typename TR>
@@ -706,16 +790,16 @@ k_prolong_q1(int MF, int MC, int dmask, const float* __restrict__ xc, float* __r
   xf[i] += acc;
 }
 
-// 3D Q1 prolongation by coarse node: thread (I, J, K) updates the fine nodes
+// 3D Q1 prolongation by coarse node (xf in layout fl): thread (I, J, K) updates the fine nodes
 // (2I+a, 2J+b, 2K+c), a, b, c in {0, 1}, from the 8 coarse values at
 // I..I+1, J..J+1, K..K+1, loaded once; each fine node is summed with the
 // weights and in the order of k_prolong_q1 (coarse Dirichlet values read as
 // zero, which is what a zero weight gives there).
 __global__ void __launch_bounds__(kBlock)
-k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __restrict__ xf) {
+k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __restrict__ xf, VLay fl) {
   const int I = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, K = blockIdx.z;
   if (I >= MC || J >= MC) return;
-  const long long MC2 = (long long)MC * MC, MF2 = (long long)MF * MF;
+  const long long MC2 = (long long)MC * MC;
   float v[2][2][2];
 #pragma unroll
   for (int dz = 0; dz < 2; ++dz)
@@ -751,7 +835,7 @@ k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __
           // even fine index: the second coarse node is the first one, weight 0
           acc = fmaf(ww, v[c ? bz : 0][b ? by : 0][a ? bx : 0], acc);
         }
-        float* o = xf + fz * MF2 + (long long)fy * MF + fx;
+        float* o = xf + fl.at(fx, fy, fz);
         *o += acc;
       }
     }
@@ -806,7 +890,15 @@ k_coarse_mx(const double* __restrict__ AinvT, int n, const __nv_bfloat16* __rest
   __syncthreads();
   if (i >= n) return;
   double acc = 0.0;
-  for (int j = 0; j < n; ++j) acc = fma(AinvT[(long long)j * n + i], rs[j], acc);
+  int j = 0;
+  for (; j + 16 <= n; j += 16) {  // sixteen coefficients loaded before their multiply-adds
+    double a[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) a[q] = __ldg(AinvT + (long long)(j + q) * n + i);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc = fma(a[q], rs[j + q], acc);
+  }
+  for (; j < n; ++j) acc = fma(__ldg(AinvT + (long long)j * n + i), rs[j], acc);
   x[i] = (float)acc;
 }
 
@@ -835,7 +927,10 @@ __global__ void k_scale_out(const float* __restrict__ e32, const double* __restr
 }
 
 // FP64 flexible-CG update: x += lam p; r -= lam a; (r, r); and the FP32
-// copy of the new residual scaled by the current scale slot
+// copy of the new residual scaled by the current scale slot.  p, r, a and r32
+// share a layout (here natural: two entries per thread, 16-byte accesses; x
+// too).  k_fcg64_update_pad takes them padded, one entry per thread, skips
+// the padding (zero in r) and finds the node's place in the natural x.
 __global__ void __launch_bounds__(kBlock)
 k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, double* __restrict__ r,
                const double* __restrict__ a, float* __restrict__ r32, long long n, Reduce2 R) {
@@ -856,6 +951,30 @@ k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, 
     *reinterpret_cast<float2*>(r32 + i0) = make_float2((float)(rv.x * s), (float)(rv.y * s));
     acc = fma(rv.x, rv.x, acc);
     acc = fma(rv.y, rv.y, acc);
+  }
+  dr_finish2(acc, 0.0, R, smem);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_fcg64_update_pad(double* sc, double* __restrict__ x, const float* __restrict__ p, double* __restrict__ r,
+                   const double* __restrict__ a, float* __restrict__ r32, VLay pl, int M, Reduce2 R) {
+  __shared__ double smem[8];
+  const double lam = sc[M_LAM], s = sc[M_SCALE];
+  double acc = 0.0;
+  const long long pi = (long long)blockIdx.x * kBlock + threadIdx.x;
+  if (pi < pl.total) {
+    const long long q = pi - pl.front;
+    const long long iz = q / pl.pz, rem = q - iz * pl.pz;
+    const long long iy = rem / pl.py, ix = rem - iy * pl.py;
+    if (q >= 0 && ix < M) {
+      const double pv = (double)p[pi];
+      double* xp = x + ix + (long long)M * (iy + (long long)M * iz);
+      *xp = fma(lam, pv, *xp);
+      const double rv = fma(-lam, a[pi], r[pi]);
+      r[pi] = rv;
+      r32[pi] = (float)(rv * s);
+      acc = rv * rv;
+    }
   }
   dr_finish2(acc, 0.0, R, smem);
 }
@@ -981,13 +1100,79 @@ static bool cell_map(const T* k, int n, CUtensorMap* tk) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+VLay natural_lay(int M, int dim) {
+  VLay L;
+  L.front = 0;
+  L.py = M;
+  L.pz = (long long)M * M;
+  L.total = dim == 3 ? L.pz * M : (dim == 2 ? L.pz : M);
+  return L;
+}
+
+VLay padded_lay(int M, int dmask) {
+  VLay L;
+  L.front = (4 - (dmask & 1)) & 3;
+  L.py = (L.front + M + 3) / 4 * 4;
+  L.pz = (long long)L.py * M;
+  L.total = L.pz * M;
+  return L;
+}
+
+// an FP32 x in layout L as the halo source: the nodes off the Dirichlet
+// faces, boxes of 40 x 18 from a 16-byte boundary (the map's origin, node
+// (l_x, l_y, l_z), sits on one by the choice of front)
+static bool halo_map(const float* x, const VLay& L, int M, int dmask, CUtensorMap* tm) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return false;
+  const int lo[3] = {dmask & 1, (dmask >> 2) & 1, (dmask >> 4) & 1};
+  const int hi[3] = {(dmask >> 1) & 1, (dmask >> 3) & 1, (dmask >> 5) & 1};
+  const float* base = x + L.at(lo[0], lo[1], lo[2]);
+  if (((uintptr_t)base & 15) || ((L.py * 4) & 15) || ((L.pz * 4) & 15)) return false;
+  const cuuint32_t one[3] = {1, 1, 1};
+  const cuuint64_t dims[3] = {(cuuint64_t)(M - lo[0] - hi[0]), (cuuint64_t)(M - lo[1] - hi[1]),
+                              (cuuint64_t)(M - lo[2] - hi[2])};
+  const cuuint64_t strides[2] = {(cuuint64_t)L.py * 4, (cuuint64_t)L.pz * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)kXW, (cuuint32_t)kFRows, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, one,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// a per-node operand in layout L: the whole padded array (py x M x M),
+// boxes of 36 x 16 from tensor x0 (node x0 - front)
+template <typename E>
+static bool op_map(const E* p, const VLay& L, int M, CUtensorMap* tm) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return false;
+  if (((uintptr_t)p & 15) || ((L.py * sizeof(E)) & 15) || ((L.pz * sizeof(E)) & 15)) return false;
+  const cuuint32_t one[3] = {1, 1, 1};
+  const cuuint64_t dims[3] = {(cuuint64_t)L.py, (cuuint64_t)M, (cuuint64_t)M};
+  const cuuint64_t strides[2] = {(cuuint64_t)L.py * sizeof(E), (cuuint64_t)L.pz * sizeof(E)};
+  const cuuint32_t box[3] = {(cuuint32_t)kOW, (cuuint32_t)kFY, 1};
+  return enc(tm, tm_type<E>(), 3, const_cast<E*>(p), dims, strides, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename T, typename TV, typename TX, int MODE, bool RED>
 static void mft_launch(const MFArgsT<T>& g, const TX* x, const T* b, T* y, const TV* v, const TV* v2,
                        const Reduce2& R, cudaStream_t st) {
+  typedef MfcLayout<T, TV, TX, MODE, RED> L;
   MftGeo q = mft_geo(g.M, g.dmask);
-  CUtensorMap tk{};
-  // the cell map needs a 16-byte aligned base; without it every node goes to the face CTAs
-  if (q.nmain > 0 && !cell_map<T>(g.k, g.n, &tk)) {
+  CUtensorMap tk{}, tx{}, tb{}, to{}, tv{}, tv2{};
+  // every map needs a 16-byte aligned base and pitch, the operand boxes the
+  // operand layout's front at most 4; without them every node goes to the
+  // face CTAs
+  const T* om = g.wd ? g.wd : g.omega;
+  constexpr bool HO = MODE == 2 || MODE == 3;
+  bool maps = q.nmain > 0 && cell_map<T>(g.k, g.n, &tk);
+  if (maps && L::HX && L::XT) maps = halo_map(reinterpret_cast<const float*>(x), g.xl, g.M, g.dmask, &tx);
+  if (maps && L::OT) {
+    maps = g.ol.front <= 4 && (!L::HB || op_map<T>(b, g.ol, g.M, &tb)) &&
+           (!(HO && om) || (g.wd && op_map<T>(g.wd, g.ol, g.M, &to))) && (!L::HV || op_map<TV>(v, g.ol, g.M, &tv)) &&
+           (!(L::HV && v2) || op_map<TV>(v2, g.ol, g.M, &tv2));
+  }
+  if (!maps) {
     q = MftGeo{};
     q.F = g.N;
     q.nface = (int)((q.F + kFaceNodes - 1) / kFaceNodes);
@@ -995,18 +1180,17 @@ static void mft_launch(const MFArgsT<T>& g, const TX* x, const T* b, T* y, const
   int dev = 0;
   cudaGetDevice(&dev);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  constexpr bool HO = MODE == 2 || MODE == 3;
   const int opt = (HO && (g.wd || g.omega) ? 1 : 0) | (RED && v2 ? 2 : 0) | (HO && g.wd ? 4 : 0);
   auto go = [&](auto oc) {
     constexpr int OPT = decltype(oc)::value;
     auto kern = k_mfc<T, TV, TX, MODE, RED, OPT>;
-    constexpr int smem = MfcLayout<T, TV, TX, MODE, RED>::SMEM;
+    constexpr int smem = L::SMEM;
     static unsigned attr = 0;  // devices the shared-memory size was raised on
     if (dev < 32 && !((attr >> dev) & 1u)) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       attr |= 1u << dev;
     }
-    kern<<<mft_blocks(q), kFThreads, smem, st>>>(g, tk, q, x, b, y, v, v2, R);
+    kern<<<mft_blocks(q), kFThreads, smem, st>>>(g, tk, tx, tb, to, tv, tv2, q, x, b, y, v, v2, R);
   };
   switch (opt) {
     case 1: if constexpr (HO) go(std::integral_constant<int, 1>{}); break;
@@ -1043,14 +1227,22 @@ static void mf_launch(int mode, const MFArgsT<T>& g, const TX* x, const T* b, T*
   }
 }
 
-// pre-smoothing from zero with the damping over the diagonal formed: y = wd b
+// pre-smoothing from zero with the damping over the diagonal formed: y = wd b,
+// four nodes per thread (16-byte accesses when all three vectors allow them)
 __global__ void __launch_bounds__(kBlock) k_wd_scale(const float* __restrict__ wd, const float* __restrict__ b,
                                                      float* __restrict__ y, long long n) {
-  const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
-  if (i < n) y[i] = __ldg(wd + i) * __ldg(b + i);
+  const long long i0 = ((long long)blockIdx.x * kBlock + threadIdx.x) * 4;
+  if (i0 >= n) return;
+  if (i0 + 4 <= n && (((uintptr_t)wd | (uintptr_t)b | (uintptr_t)y) & 15) == 0) {
+    const float4 w = __ldg(reinterpret_cast<const float4*>(wd + i0));
+    const float4 v = __ldg(reinterpret_cast<const float4*>(b + i0));
+    *reinterpret_cast<float4*>(y + i0) = make_float4(w.x * v.x, w.y * v.y, w.z * v.z, w.w * v.w);
+  } else {
+    for (long long i = i0; i < n && i < i0 + 4; ++i) y[i] = __ldg(wd + i) * __ldg(b + i);
+  }
 }
 
-// wd = damping / diagonal of the matrix-free top level, the diagonal formed
+// wd (layout g.ol) = damping / diagonal of the matrix-free top level, the diagonal formed
 // as in the matrix-free operator (4 hs times the sum of the node's 8 cell coefficients, summed
 // in the same order; cells outside the grid count zero); Dirichlet nodes
 // (identity rows) get the damping itself
@@ -1061,8 +1253,9 @@ __global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ 
   const int ix = (int)(i % M), iy = (int)((i / M) % M), iz = (int)(i / ((long long)M * M));
   auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
   const float om = g.omega ? __ldg(g.omega + i) : g.w;
+  const long long o = g.ol.at(ix, iy, iz);
   if (dirf(ix, 1, 2) || dirf(iy, 4, 8) || dirf(iz, 16, 32)) {
-    wd[i] = om;
+    wd[o] = om;
     return;
   }
   float k[2][2][2];
@@ -1079,7 +1272,7 @@ __global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ 
   const float wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
                           {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
   const float ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
-  wd[i] = om / (4.f * g.hs * ksum);
+  wd[o] = om / (4.f * g.hs * ksum);
 }
 
 void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st) {
@@ -1089,9 +1282,10 @@ void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st) {
 
 void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,
                   const double* v2, const Reduce2* R, cudaStream_t st) {
-  if (mode == 3 && g.wd && !R) {  // a stream of two reads and a write
+  if (mode == 3 && g.wd && !R) {  // a stream of two reads and a write over the arrays (padding included)
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    k_wd_scale<<<g1(g.N), kBlock, 0, st>>>(g.wd, b, y, g.N);
+    const long long n = g.ol.total;
+    k_wd_scale<<<g1((n + 3) / 4), kBlock, 0, st>>>(g.wd, b, y, n);
     return;
   }
   mf_launch<float, double, float>(mode, g, x, b, y, v, v2, R, st);
@@ -1151,8 +1345,8 @@ void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, _
   if (F.order == 1) {
     typedef __nv_bfloat16 bf;
     if (F.dim == 3) {
-      if (rf_bf16) k_restrict_q1<3, bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
-      else k_restrict_q1<3, float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
+      if (rf_bf16) k_restrict_q1s<bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
+      else k_restrict_q1s<float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
     } else if (F.dim == 2) {
       if (rf_bf16) k_restrict_q1<2, bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
       else k_restrict_q1<2, float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
@@ -1168,13 +1362,13 @@ void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, _
   });
 }
 
-void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cudaStream_t st) {
+void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cudaStream_t st, const VLay* xfl) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   const dim3 gr = xgrid(F.M, F.dim), bl(32, 8);
   if (F.order == 1) {
     if (F.dim == 3)
       k_prolong_q1c<<<dim3((unsigned)((C.M + 31) / 32), (unsigned)((C.M + 7) / 8), (unsigned)C.M), bl, 0, st>>>(
-          (int)F.M, (int)C.M, F.dmask, xc, xf);
+          (int)F.M, (int)C.M, F.dmask, xc, xf, xfl ? *xfl : natural_lay((int)F.M, 3));
     else if (F.dim == 2) k_prolong_q1<2><<<gr, bl, 0, st>>>((int)F.M, (int)C.M, F.dmask, xc, xf);
     else k_prolong_q1<1><<<gr, bl, 0, st>>>((int)F.M, (int)C.M, F.dmask, xc, xf);
     return;
@@ -1192,10 +1386,43 @@ void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st) {
   k_f64_to_f32<<<g1(n), kBlock, 0, st>>>(a, b, n);
 }
 
-void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
-                     const Reduce2& R, cudaStream_t st) {
+void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, const VLay& pl,
+                     int M, int dim, const Reduce2& R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_fcg64_update<<<g1(np / 2), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
+  const VLay nat = natural_lay(M, dim);
+  if (pl.front == nat.front && pl.py == nat.py && pl.pz == nat.pz) {
+    const long long np = (pl.total + 1) / 2 * 2;  // natural vectors are allocated to an even length
+    k_fcg64_update<<<g1(np / 2), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
+  } else {
+    k_fcg64_update_pad<<<g1(pl.total), kBlock, 0, st>>>(sc, x, p, r, a, r32, pl, M, R);
+  }
+}
+
+// b (layout bl) = a (natural), 3D, M nodes a side: FP64 to FP32, and FP64 copied
+__global__ void k_f64_to_f32_lay(const double* __restrict__ a, float* __restrict__ b, VLay bl, int M) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long MM = (long long)M * M;
+  if (i >= MM * M) return;
+  const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
+  b[bl.at((int)ix, (int)iy, (int)iz)] = (float)a[i];
+}
+
+__global__ void k_f64_copy_lay(const double* __restrict__ a, double* __restrict__ b, VLay bl, int M) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long MM = (long long)M * M;
+  if (i >= MM * M) return;
+  const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
+  b[bl.at((int)ix, (int)iy, (int)iz)] = a[i];
+}
+
+void mx_f64_to_f32_lay(const double* a, float* b, const VLay& bl, int M, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_f64_to_f32_lay<<<g1((long long)M * M * M), kBlock, 0, st>>>(a, b, bl, M);
+}
+
+void mx_f64_copy_lay(const double* a, double* b, const VLay& bl, int M, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_f64_copy_lay<<<g1((long long)M * M * M), kBlock, 0, st>>>(a, b, bl, M);
 }
 
 void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st) {

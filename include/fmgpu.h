@@ -439,6 +439,9 @@ int fmg_batch_solve(fmg_grid* batch, const fmg_solve_cfg* cfg, fmg_vec* x, doubl
 #define FMG_MXK_RESIDUAL 1   /* FP32 r = b - A x, matrix-free */
 #define FMG_MXK_SMOOTH 2     /* FP32 y = x + w (b - A x) / d with the flexible CG's two FP64 dot products */
 #define FMG_MXK_MATVEC64 3   /* FP64 a = A p of the FP32 search direction, with (a, p) */
+#define FMG_MXK_RESTRICT 4   /* the top-level residual restricted to the level below (BF16 rhs, x zeroed) */
+#define FMG_MXK_PROLONG 5    /* the level below's correction prolongated and added to the top level */
+#define FMG_MXK_PRESMOOTH 6  /* the top-level pre-smoothing from zero, y = w b / d */
 int fmg_mixed_top_kernel(fmg_grid* grid, int kind, int reps);
 
 /* No counterpart in the reference: a self-test of the device-side give-up
