@@ -154,6 +154,7 @@ struct MixedState {
   float *zp = nullptr, *zs = nullptr;  // the in-solve judge: the plain cycle's result and its spare
   float* p32 = nullptr;             // FP32 search direction of the flexible CG
   double *r64 = nullptr, *a64 = nullptr;  // FP64 residual and A p of the mixed solve (layout lay)
+  double* x64 = nullptr;            // the solve's iterate in layout lay (copied from and back to the caller's)
   VLay lay;                         // layout of the top-level vectors above (rtop excepted):
                                     // padded with the matrix-free top level, natural otherwise
   long long cap = 0;                // elements each top-level vector holds
@@ -2064,7 +2065,8 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     float** tv[] = {&X.rtop, &X.r, &X.q, &X.qs, &X.p32, &X.wd, &X.zp, &X.zs};
     for (float** v : tv)
       if ((rc = mx_alloc_f(g, v, X.cap))) return rc;
-    if ((rc = dalloc(g, &X.r64, X.cap)) || (rc = dalloc(g, &X.a64, X.cap))) return rc;
+    if ((rc = dalloc(g, &X.r64, X.cap)) || (rc = dalloc(g, &X.a64, X.cap)) || (rc = dalloc(g, &X.x64, X.cap)))
+      return rc;
     if ((rc = mx_alloc_f(g, &X.k32, ncell))) return rc;
     const long long nparts =
         std::max({(long long)nchunks(X.cap), mx_top_blocks((int)T.M), X.cap / kBlock + 1}) + 1;
@@ -2108,6 +2110,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     for (float* v : fv) FMG_CK(c, cudaMemsetAsync(v, 0, X.cap * sizeof(float), st));
     FMG_CK(c, cudaMemsetAsync(X.r64, 0, X.cap * sizeof(double), st));
     FMG_CK(c, cudaMemsetAsync(X.a64, 0, X.cap * sizeof(double), st));
+    FMG_CK(c, cudaMemsetAsync(X.x64, 0, X.cap * sizeof(double), st));
     X.lay = lay;
     X.wd_ok = false;
   }
@@ -2502,10 +2505,15 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
   mg.prepare_wd();
   const LevelView T = view(g, g->top);
   const long long n = T.N;
-  double* x = xv->d;
   const double* b = g->rhs;
   // the CG's vectors: padded with the matrix-free top level (its kernels take
-  // them by tensor copy), the solvers' natural ones otherwise
+  // them by tensor copy; the iterate is copied in here and back at the end),
+  // the solvers' natural ones otherwise
+  double* x = xv->d;
+  if (X.mf) {
+    mx_f64_copy_lay(xv->d, X.x64, X.lay, (int)T.M, st);
+    x = X.x64;
+  }
   double *r = X.mf ? X.r64 : g->r, *a = X.mf ? X.a64 : g->a;
   const long long nv = X.mf ? X.lay.total : n;  // elements of the top-level vectors, padding included
   float* p = X.p32;
@@ -2529,7 +2537,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       else launch_copy(b, r, n, st);
     } else if (mg.top_mf()) {
       MFArgs64 m = mf64_args(g, cfg->damp);
-      m.yl = X.lay;
+      m.xl = m.yl = X.lay;  // x and r padded, b the grid's natural rhs
       mx_top_residual64(m, x, b, r, st);
     } else {
       launch_spmv(T, x, b, r, nullptr, nullptr, st);
@@ -2567,13 +2575,13 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
       mg.vcycle(g->top, X.r, &X.q, &X.qs, r, a, &Rf);
       mx_fcg64_p(X.sc, p, X.q, nv, false, st);
       mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
-      mx_fcg64_update(X.sc, x, p, r, a, X.r, X.lay, (int)T.M, g->dim, red2(X, EPI2_UPDATE, 0, 0), st);
+      mx_fcg64_update(X.sc, x, p, r, a, X.r, X.mf ? nv : T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
       cudaMemcpyAsync(X.host, X.sc, M_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st);
     };
     while (iters <= cfg->maxsteps) {
       if (iters == it0) {
         mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
-        mx_fcg64_update(X.sc, x, p, r, a, X.r, X.lay, (int)T.M, g->dim, red2(X, EPI2_UPDATE, 0, 0), st);
+        mx_fcg64_update(X.sc, x, p, r, a, X.r, X.mf ? nv : T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
         if ((rc = launched(c, "mixed step"))) return rc;
         if ((rc = mx_read(g))) return rc;
       } else if (shadow && iters - it0 <= mcfg->judge) {
@@ -2609,7 +2617,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
         }
         mx_fcg64_p(X.sc, p, X.q, nv, false, st);
         mg.matvec64(p, a, red2(X, EPI2_LAMBDA, 0, 0));
-        mx_fcg64_update(X.sc, x, p, r, a, X.r, X.lay, (int)T.M, g->dim, red2(X, EPI2_UPDATE, 0, 0), st);
+        mx_fcg64_update(X.sc, x, p, r, a, X.r, X.mf ? nv : T.Np, red2(X, EPI2_UPDATE, 0, 0), st);
         if ((rc = launched(c, "mixed step"))) return rc;
         if ((rc = mx_read(g))) return rc;
       } else {
@@ -2641,6 +2649,7 @@ extern "C" int fmg_solve_mixed(fmg_grid* g, const fmg_solve_cfg* cfg, const fmg_
     }
     ++step;  // the true-residual check occupies one history slot
   }
+  if (X.mf) mx_f64_from_lay(X.x64, X.lay, xv->d, (int)T.M, st);
   FMG_CK(c, cudaStreamSynchronize(st));
   return launched(c, "solve_mixed");
 }
@@ -3343,7 +3352,9 @@ int cg_probe(fmg_grid* g, const fmg_solve_cfg& cf, const fmg_mixed_cfg* mc, int 
   g->x_zero = false;
   if (rc) return rc;
   // |e_k|_A^2 = e_k . A e_k with A e_k = b - A x_k, the solve's FP64 residual
+  // (the matrix-free mixed solve leaves it padded: brought to g->r first)
   launch_sub_wv(xs, nullptr, x.d, e, n, st);
+  if (mc && g->mx && g->mx->mf) mx_f64_from_lay(g->mx->r64, g->mx->lay, g->r, (int)T.M, st);
   launch_dot(e, g->r, n, reducer(g, EPI_STORE, S_E3), st);
   if ((rc = launched(ctx, "judge probe"))) return rc;
   if ((rc = read_scalars(g))) return rc;

@@ -90,10 +90,12 @@ void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st);
 // b (layout bl) = a (natural, M nodes a side, 3D)
 void mx_f64_to_f32_lay(const double* a, float* b, const VLay& bl, int M, cudaStream_t st);
 void mx_f64_copy_lay(const double* a, double* b, const VLay& bl, int M, cudaStream_t st);
-// FP64 flexible CG: x += lam p, r -= lam a, (r,r), r32 = r * scale; p, r, a
-// and r32 in layout pl, x natural (M nodes a side, dim directions)
-void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, const VLay& pl,
-                     int M, int dim, const Reduce2& R, cudaStream_t st);
+// b (natural) = a (layout al), FP64, 3D
+void mx_f64_from_lay(const double* a, const VLay& al, double* b, int M, cudaStream_t st);
+// FP64 flexible CG: x += lam p, r -= lam a, (r,r), r32 = r * scale, all five
+// in one layout of np elements (even; padding zero)
+void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
+                     const Reduce2& R, cudaStream_t st);
 // p = q / s + beta p (FP32 search direction)
 void mx_fcg64_p(const double* sc, float* p, const float* q, long long n, bool first, cudaStream_t st);
 void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st);

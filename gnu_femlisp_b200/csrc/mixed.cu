@@ -386,7 +386,7 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, const __grid_c
       const int r = e / kPX, jj = e - r * kPX;
       const int xx = x0 - 1 + jj, yy = y0 - 1 + r;
       hok[q] = e < kFRows * kPX && xx >= 0 && xx < M && yy >= 0 && yy < M && !dirf(xx, 1, 2) && !dirf(yy, 4, 8);
-      hoff[q] = hok[q] ? yy * M + xx : 0;
+      hoff[q] = hok[q] ? (int)(g.xl.front + xx + (long long)g.xl.py * yy) : 0;
     }
     const int ix = x0 + lx, iy0 = y0 + 2 * ly;
     bool ok = true;  // every wait of this warp so far completed; after one gives up, the rest wait 1 ms at most
@@ -426,7 +426,7 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, const __grid_c
       if (HX && !L::XT) {
         const int z = z0 - 1 + j;
         const bool zok = z >= 0 && z < M && !dirf(z, 16, 32);
-        const TX* pl = x + (zok ? (long long)z * MM : 0ll);
+        const TX* pl = x + (zok ? (long long)z * g.xl.pz : 0ll);
         TX* xs = reinterpret_cast<TX*>(st);
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -661,50 +661,6 @@ k_restrict_q1(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat1
   xc[J] = 0.f;
 }
 
-// 3D Q1 restriction through shared memory: a block (32, 8) of coarse nodes
-// in plane K first stages the fine nodes its sums read -- planes 2K-1 .. 2K+1,
-// rows 2J0-1 .. 2J0+15, columns 2I0-1 .. 2I0+63, converted to FP32, zero
-// outside the grid and on Dirichlet faces -- with coalesced row loads, then
-// sums each coarse node's 27 terms with the weights and in the order of
-// k_restrict_q1 (a zero weight there is a zero value here).
-constexpr int kRsX = 65, kRsY = 17;
-template <typename TR>
-__global__ void __launch_bounds__(kBlock)
-k_restrict_q1s(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat16* __restrict__ bc,
-               float* __restrict__ xc) {
-  __shared__ float t[3][kRsY][kRsX];
-  const int I0 = blockIdx.x * 32, J0 = blockIdx.y * 8, K = blockIdx.z;
-  const int tid = threadIdx.y * 32 + threadIdx.x;
-  const long long MF2 = (long long)MF * MF;
-  for (int e = tid; e < 3 * kRsY * kRsX; e += 32 * 8) {
-    const int z = e / (kRsY * kRsX), rem = e - z * (kRsY * kRsX), y = rem / kRsX, x = rem - y * kRsX;
-    const int fx = 2 * I0 - 1 + x, fy = 2 * J0 - 1 + y, fz = 2 * K - 1 + z;
-    const bool ok = fx >= 0 && fx < MF && fy >= 0 && fy < MF && fz >= 0 && fz < MF && !fdir(fx, MF, 0, dmask) &&
-                    !fdir(fy, MF, 1, dmask) && !fdir(fz, MF, 2, dmask);
-    t[z][y][x] = ok ? ldv(rf, fz * MF2 + (long long)fy * MF + fx) : 0.f;
-  }
-  __syncthreads();
-  const int cx = I0 + threadIdx.x, cy = J0 + threadIdx.y;
-  if (cx >= MC || cy >= MC) return;
-  const long long J = cx + (long long)MC * (cy + (long long)MC * K);
-  const bool dj = fdir(cx, MC, 0, dmask) || fdir(cy, MC, 1, dmask) || fdir(K, MC, 2, dmask);
-  float acc = 0.f;
-  if (!dj) {
-    const float w[3] = {.5f, 1.f, .5f};
-#pragma unroll
-    for (int z = 0; z < 3; ++z)
-#pragma unroll
-      for (int y = 0; y < 3; ++y) {
-        const float wyz = w[y] * w[z];
-        const float* row = &t[z][2 * threadIdx.y + y][2 * threadIdx.x];
-#pragma unroll
-        for (int xx = 0; xx < 3; ++xx) acc = fmaf(w[xx] * wyz, row[xx], acc);
-      }
-  }
-  bc[J] = __float2bfloat16_rn(acc);
-  xc[J] = 0.f;
-}
-
 // restriction of a residual (FP32 or BF16) into the coarse rhs (BF16), coarse
 // solution zeroed; blocks (32, 8) over x, y and one z plane per blockIdx.z
 template <int D, int P, typename TR>
@@ -927,10 +883,9 @@ __global__ void k_scale_out(const float* __restrict__ e32, const double* __restr
 }
 
 // FP64 flexible-CG update: x += lam p; r -= lam a; (r, r); and the FP32
-// copy of the new residual scaled by the current scale slot.  p, r, a and r32
-// share a layout (here natural: two entries per thread, 16-byte accesses; x
-// too).  k_fcg64_update_pad takes them padded, one entry per thread, skips
-// the padding (zero in r) and finds the node's place in the natural x.
+// copy of the new residual scaled by the current scale slot; all five in one
+// layout (natural or padded), two entries per thread, 16-byte accesses; the
+// padding is zero in p and a and stays zero in x and r
 __global__ void __launch_bounds__(kBlock)
 k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, double* __restrict__ r,
                const double* __restrict__ a, float* __restrict__ r32, long long n, Reduce2 R) {
@@ -951,30 +906,6 @@ k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, 
     *reinterpret_cast<float2*>(r32 + i0) = make_float2((float)(rv.x * s), (float)(rv.y * s));
     acc = fma(rv.x, rv.x, acc);
     acc = fma(rv.y, rv.y, acc);
-  }
-  dr_finish2(acc, 0.0, R, smem);
-}
-
-__global__ void __launch_bounds__(kBlock)
-k_fcg64_update_pad(double* sc, double* __restrict__ x, const float* __restrict__ p, double* __restrict__ r,
-                   const double* __restrict__ a, float* __restrict__ r32, VLay pl, int M, Reduce2 R) {
-  __shared__ double smem[8];
-  const double lam = sc[M_LAM], s = sc[M_SCALE];
-  double acc = 0.0;
-  const long long pi = (long long)blockIdx.x * kBlock + threadIdx.x;
-  if (pi < pl.total) {
-    const long long q = pi - pl.front;
-    const long long iz = q / pl.pz, rem = q - iz * pl.pz;
-    const long long iy = rem / pl.py, ix = rem - iy * pl.py;
-    if (q >= 0 && ix < M) {
-      const double pv = (double)p[pi];
-      double* xp = x + ix + (long long)M * (iy + (long long)M * iz);
-      *xp = fma(lam, pv, *xp);
-      const double rv = fma(-lam, a[pi], r[pi]);
-      r[pi] = rv;
-      r32[pi] = (float)(rv * s);
-      acc = rv * rv;
-    }
   }
   dr_finish2(acc, 0.0, R, smem);
 }
@@ -1345,8 +1276,8 @@ void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, _
   if (F.order == 1) {
     typedef __nv_bfloat16 bf;
     if (F.dim == 3) {
-      if (rf_bf16) k_restrict_q1s<bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
-      else k_restrict_q1s<float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
+      if (rf_bf16) k_restrict_q1<3, bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
+      else k_restrict_q1<3, float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
     } else if (F.dim == 2) {
       if (rf_bf16) k_restrict_q1<2, bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
       else k_restrict_q1<2, float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
@@ -1386,16 +1317,10 @@ void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st) {
   k_f64_to_f32<<<g1(n), kBlock, 0, st>>>(a, b, n);
 }
 
-void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, const VLay& pl,
-                     int M, int dim, const Reduce2& R, cudaStream_t st) {
+void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
+                     const Reduce2& R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  const VLay nat = natural_lay(M, dim);
-  if (pl.front == nat.front && pl.py == nat.py && pl.pz == nat.pz) {
-    const long long np = (pl.total + 1) / 2 * 2;  // natural vectors are allocated to an even length
-    k_fcg64_update<<<g1(np / 2), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
-  } else {
-    k_fcg64_update_pad<<<g1(pl.total), kBlock, 0, st>>>(sc, x, p, r, a, r32, pl, M, R);
-  }
+  k_fcg64_update<<<g1(np / 2), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
 }
 
 // b (layout bl) = a (natural), 3D, M nodes a side: FP64 to FP32, and FP64 copied
@@ -1413,6 +1338,20 @@ __global__ void k_f64_copy_lay(const double* __restrict__ a, double* __restrict_
   if (i >= MM * M) return;
   const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
   b[bl.at((int)ix, (int)iy, (int)iz)] = a[i];
+}
+
+// b (natural) = a (layout al), FP64, 3D
+__global__ void k_f64_from_lay(const double* __restrict__ a, VLay al, double* __restrict__ b, int M) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long MM = (long long)M * M;
+  if (i >= MM * M) return;
+  const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
+  b[i] = a[al.at((int)ix, (int)iy, (int)iz)];
+}
+
+void mx_f64_from_lay(const double* a, const VLay& al, double* b, int M, cudaStream_t st) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  k_f64_from_lay<<<g1((long long)M * M * M), kBlock, 0, st>>>(a, al, b, M);
 }
 
 void mx_f64_to_f32_lay(const double* a, float* b, const VLay& bl, int M, cudaStream_t st) {
