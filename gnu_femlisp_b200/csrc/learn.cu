@@ -311,10 +311,31 @@ struct Z3 {
 
 // weights [27 taps][COUT][CIN] (tap = dx + 3 dy + 9 dz) -> per xy tap t a
 // K-major (3 COUT) x CIN tile whose row dz COUT + co holds tap t + 9 dz
+// (defined after the thread count of the kernel that stages them)
+
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// Warp roles: warp 4's first lane is the producer -- it issues, per input
+// plane, CIN/8 tiled TMA copies of the (8 channels) x 10 x 18 box of the
+// activation tensor [z][y][x][C] (viewed as 5D: 8 channels, C/8 chunks, x, y,
+// z; nodes beyond the array read as zeros) into the plane's ring slot,
+// completing on that slot's mbarrier, waits for the plane (bounded) and
+// issues its MMAs, committing them to the plane's mbarrier mb[k] (k the
+// plane's index in the work item).  Warps 0-3 (one tensor-memory lane
+// quadrant each) only run the epilogue: output plane j of the item is
+// complete once the MMAs of input plane j + 2 are, so they wait mb[j + 2] and
+// read the plane's accumulators, while the producer's copies and MMAs for the
+// planes after it go on.  The producer refills a ring slot once the MMAs of
+// the plane that read it are done (mb[k - 2]).  One block barrier per work
+// item orders the epilogue's tensor-memory reads before the next item's MMAs
+// (which reuse the columns); before it the producer waits every commit of
+// the item, so each mbarrier's phases complete strictly in turn.
+constexpr int kZThreads = 160;
+
 template <int CIN, int COUT>
 __device__ __forceinline__ void stage_weights_z3(uint8_t* ws, const bf16* __restrict__ w) {
   constexpr int CH = CIN / 8, R = 3 * COUT;
-  for (int idx = threadIdx.x; idx < 9 * R * CH; idx += kThreads) {
+  for (int idx = threadIdx.x; idx < 9 * R * CH; idx += kZThreads) {
     const int c = idx % CH, row = (idx / CH) % R, t = idx / (CH * R);
     const int dz = row / COUT, co = row - dz * COUT;
     cp16(ws + t * Z3<CIN, COUT>::WTAP + umma::kmajor_offset(row, c * 8, CIN),
@@ -322,28 +343,20 @@ __device__ __forceinline__ void stage_weights_z3(uint8_t* ws, const bf16* __rest
   }
 }
 
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-
-// The halo planes arrive by TMA: thread 0 issues, per plane, CIN/8 tiled
-// copies of the (8 channels) x 10 x 18 box of the activation tensor
-// [z][y][x][C] (viewed as 5D: 8 channels, C/8 chunks, x, y, z; nodes beyond
-// the array read as zeros) into the plane's ring slot, completing on that
-// slot's mbarrier; it waits for the plane (bounded) before its MMAs.  The
-// other threads only wait for MMA completion before their epilogue, so no
-// block-wide barrier is taken per plane; one per work item orders the
-// epilogue's tensor-memory reads before the next item's MMAs.
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_constant__ CUtensorMap tin) {
+__global__ void __launch_bounds__(kZThreads) k_conv3z(ConvArgs a, const __grid_constant__ CUtensorMap tin) {
   using Z = Z3<CIN, COUT>;
   constexpr uint32_t kPlaneTx = (CIN / 8) * kPlaneB;  // bytes of one plane's copies
+  constexpr int NP = kSeg + 2;                        // input planes of a full work item
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* ws = smem;
   uint8_t* hs = smem + Z::WBYTES;
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t mb[NP];
   __shared__ __align__(8) uint64_t full[kRing];
   __shared__ uint32_t tslot;
   __shared__ int halo_timeout;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp == 4 && lane == 0;
   const TileGeo& t = a.t;
   const int nseg = (t.Mz + kSeg - 1) / kSeg;
   const long long items = (long long)t.ntx * t.nty * nseg;
@@ -354,8 +367,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_co
   umma::fence_async_smem();  // the staged weights -> the tensor core's proxy
   if (warp == 0) umma::tmem_alloc(&tslot, Z::TCOLS);
   if (tid == 0) {
-    umma::mbar_init(&bar[0]);
-    umma::mbar_init(&bar[1]);
+    for (int i = 0; i < NP; ++i) umma::mbar_init(&mb[i]);
     for (int i = 0; i < kRing; ++i) umma::mbar_init(&full[i]);
     halo_timeout = 0;
   }
@@ -364,33 +376,17 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_co
   umma::fence_after();
   const uint32_t tmem = tslot;
   const uint32_t hb = umma::smem_u32(hs), wb = umma::smem_u32(ws);
-  uint32_t phase = 0u;   // bit i: parity of bar[i]'s next phase
-  uint32_t pend = 0u;    // bit i: a commit on bar[i] not yet waited for
-  uint32_t fphase = 0u;  // thread 0, bit s: parity of full[s]'s next phase
-  uint32_t fpend = 0u;   // thread 0, bit s: a plane load on full[s] not yet waited for
+  uint32_t mphase = 0u;  // bit k: parity of the phase of mb[k] this item's commit completes (every thread)
+  uint32_t fphase = 0u;  // producer, bit s: parity of full[s]'s next phase
+  uint32_t fpend = 0u;   // producer, bit s: a plane load on full[s] not yet waited for
   bool failed = false;
   int tx = 0, ty = 0;
-  auto load_plane = [&](int P) {  // thread 0
+  auto load_plane = [&](int P) {  // the producer
     const int sl = P % kRing;
     umma::mbar_arrive_expect_tx(&full[sl], kPlaneTx);
     uint8_t* dst = hs + sl * kSlotB;
     for (int c = 0; c < CIN / 8; ++c) umma::tma_load_5d(dst + c * Z::CHB, &tin, &full[sl], 0, c, tx * TX, ty * TY, P);
     fpend |= 1u << sl;
-  };
-  auto wait_mma = [&](int i) {  // this thread: the MMAs committed to bar[i] are done
-    if (umma::mbar_wait(&bar[i], (phase >> i) & 1u)) {
-      phase ^= 1u << i;
-      pend &= ~(1u << i);
-      return true;
-    }
-    return false;
-  };
-  auto epilogue = [&](int z0, int z) {
-    umma::fence_after();
-    float v[COUT];
-    umma::tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(COUT * (kSeg - 1 - (z - z0))), v);
-    const int r = warp * 32 + lane;
-    conv_epilogue<3, COUT, EPI>(a, v, tx * TX + (r & 7), ty * TY + (r >> 3), z);
   };
   for (long long id = blockIdx.x; id < items; id += gridDim.x) {
     tx = (int)(id % t.ntx);
@@ -399,15 +395,17 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_co
     const int z0 = (int)(rest / t.nty) * kSeg;
     const int S = min(kSeg, t.Mz - z0);
     const int nplanes = S + 2;  // padded input planes z0 .. z0+S+1
-    if (tid == 0) {
+    if (producer) {
       load_plane(z0);
       load_plane(z0 + 1);
-    }
-    for (int k = 0; k < nplanes; ++k) {
-      const int P = z0 + k;
-      if (tid == 0) {
-        // the slot of plane P + 2 was last read by the MMAs of plane P - 2, waited for at step k - 1
-        if (k + 2 < nplanes) load_plane(P + 2);
+      for (int k = 0; k < nplanes; ++k) {
+        const int P = z0 + k;
+        if (k + 2 < nplanes) {
+          // the slot of plane P + 2 was last read by the MMAs of plane P - 2
+          // (of this item; those of the item before are all done by now)
+          if (k >= 2 && !umma::mbar_wait(&mb[k - 2], (mphase >> (k - 2)) & 1u)) failed = true;
+          load_plane(P + 2);
+        }
         const int sl = P % kRing;
         const bool landed = umma::mbar_wait(&full[sl], (fphase >> sl) & 1u);
         if (landed) {
@@ -417,7 +415,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_co
           halo_timeout = 1;
         }
         umma::fence_after();
-        if (landed) {
+        if (landed && !failed) {
           const int dlo = max(0, P - (z0 + S - 1)), dhi = min(2, P - z0);
           const uint32_t dcol = tmem + (uint32_t)(COUT * (kSeg - 1 - (P - dlo - z0)));
           const uint32_t aslot = hb + (uint32_t)(sl * kSlotB);
@@ -446,17 +444,25 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_co
             }
           }
         }
-        umma::mma_commit(&bar[k & 1]);  // also when nothing was issued: every commit has its wait
+        umma::mma_commit(&mb[k]);  // also when nothing was issued: every commit is waited for
       }
-      pend |= 1u << (k & 1);
-      if (k >= 1) {
-        if (!wait_mma((k - 1) & 1)) failed = true;
-        if (!failed && k >= 3) epilogue(z0, P - 3);
-        umma::fence_before();
+      // every commit of the item done before the block barrier: each mbarrier
+      // then completes its phases strictly in turn
+      for (int k = 0; k < nplanes; ++k)
+        if (!umma::mbar_wait(&mb[k], (mphase >> k) & 1u)) failed = true;
+    } else if (warp < 4) {
+      for (int j = 0; j < S; ++j) {
+        if (!umma::mbar_wait(&mb[j + 2], (mphase >> (j + 2)) & 1u)) failed = true;
+        umma::fence_after();
+        if (!failed) {
+          float v[COUT];
+          umma::tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(COUT * (kSeg - 1 - j)), v);
+          const int r = warp * 32 + lane;
+          conv_epilogue<3, COUT, EPI>(a, v, tx * TX + (r & 7), ty * TY + (r >> 3), z0 + j);
+        }
       }
     }
-    if (!wait_mma((nplanes - 1) & 1)) failed = true;
-    if (!failed) epilogue(z0, z0 + S - 1);
+    mphase ^= (1u << nplanes) - 1u;
     umma::fence_before();  // the tensor-memory reads above precede the next item's MMAs
     const bool stop = __syncthreads_or(failed || halo_timeout != 0);
     umma::fence_after();
@@ -467,12 +473,10 @@ __global__ void __launch_bounds__(kThreads) k_conv3z(ConvArgs a, const __grid_co
   }
   if (failed) {
     if (tid == 0) atomicOr(a.err, 1u);
-    for (int i = 0; i < 2; ++i)
-      if ((pend >> i) & 1u) umma::mbar_wait(&bar[i], (phase >> i) & 1u);  // bounded: let issued MMAs drain
+    if (producer)  // bounded: no copy may still be landing when the CTA exits
+      for (int sl = 0; sl < kRing; ++sl)
+        if ((fpend >> sl) & 1u) umma::mbar_wait(&full[sl], (fphase >> sl) & 1u);
   }
-  if (tid == 0)  // bounded: no copy may still be landing when the CTA exits
-    for (int sl = 0; sl < kRing; ++sl)
-      if ((fpend >> sl) & 1u) umma::mbar_wait(&full[sl], (fphase >> sl) & 1u);
   umma::fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -948,7 +952,7 @@ int conv(const ConvArgs& a, cudaStream_t st) {
     const long long items = (long long)a.t.ntx * a.t.nty * ((a.t.Mz + kSeg - 1) / kSeg);
     const long long grid = std::min<long long>(items, 2LL * sm_count());
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    k_conv3z<CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kThreads, smem, st>>>(a, tin);
+    k_conv3z<CIN, COUT, EPI><<<(unsigned)std::max<long long>(grid, 1), kZThreads, smem, st>>>(a, tin);
   } else {
     constexpr size_t smem = (size_t)Tp<D>::TAPS * COUT * CIN * 2 + (size_t)(CIN / 8) * Tp<D>::CHB;
     static bool init = false;
