@@ -2075,24 +2075,13 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
       return rc;
     if (!X.host) FMG_CK(c, cudaMallocHost((void**)&X.host, M_COUNT * sizeof(double)));
   }
-  // levels the library assembled itself (re-discretised or Galerkin) are
-  // symmetric: their FP32 copy keeps only the upper slots C .. NS-1, moved to
-  // the front, and the kernels take a lower slot from its mirror row
-  const bool sym = g->nc == 1 && !g->uploaded;
-  auto to32 = [&](int l) -> int {
+  auto to32 = [&](int l) {
     const Lvl& L = g->lev[l];
     if (g->order == 2) launch_level_to_f32(view(g, l), g->nslots, X.A32[l], st);  // sliced -> full slots
     else mx_f64_to_f32(L.A, X.A32[l], (long long)g->nslots * L.Np, st);
-    if (sym) {
-      const int C = (g->nslots - 1) / 2;
-      for (int k = 0; k <= C; ++k)  // slot C + k to slot k: the ranges are disjoint (C >= 1)
-        FMG_CK(c, cudaMemcpyAsync(X.A32[l] + (long long)k * L.Np, X.A32[l] + (long long)(C + k) * L.Np,
-                                  L.Np * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    }
-    return FMG_OK;
   };
   if (X.epoch != g->epoch) {  // convert the current assembly (the top level only where it is stored)
-    for (int l = g->base; l < g->top; ++l) FMG_RC(to32(l));
+    for (int l = g->base; l < g->top; ++l) to32(l);
     if (g->kkind == FMG_K_CELL) {
       long long ncell = 1;
       for (int k = 0; k < g->dim; ++k) ncell *= g->lev[g->top].n;
@@ -2103,7 +2092,7 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
   }
   if (!mf && !X.top32) {
     FMG_RC(ensure_top(g));
-    FMG_RC(to32(g->top));
+    to32(g->top);
     X.top32 = true;
   }
   for (int l = g->base; l <= g->top; ++l) {  // per-node damping may change between solves
@@ -2112,7 +2101,6 @@ int mixed_prepare(fmg_grid* g, bool want_mf) {
     Lev32& V = X.lv[l];
     V.A = X.A32[l]; V.om = L.omega ? X.om32[l] : nullptr;
     V.N = L.N; V.Np = L.Np; V.M = L.M; V.dim = g->dim; V.order = g->order; V.dmask = g->dmask;
-    V.sym = sym ? 1 : 0;
   }
   const VLay lay = mf ? padded_lay((int)g->lev[g->top].M, g->dmask)
                      : natural_lay((int)g->lev[g->top].M, g->dim);

@@ -58,12 +58,11 @@ typedef MFArgsT<double> MFArgs64;
 
 // one level with an FP32 copy of its assembled matrix
 struct Lev32 {
-  const float* A;      // [slot][Np]; sym: only slots C .. NS-1 (C the centre), at 0 .. C
+  const float* A;      // [slot][Np]
   const float* om;     // per-node damping or nullptr
   long long N, Np, M;
   int dim, order, dmask;
   float w;
-  int sym = 0;         // the matrix is symmetric and kept as its upper slots
 };
 
 void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,

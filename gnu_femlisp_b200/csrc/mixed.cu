@@ -576,16 +576,11 @@ __device__ __forceinline__ long long soff(int s, long long M) {
 
 // mode 0: y = A x; 1: y = b - A x; 2: y = x + w (b - Ax)/d; 3: y = w b/d
 // One row per thread (the 27 loads of a row are its only latency chain).
-// sym: the matrix is kept as its upper slots C .. NS-1 (at 0 .. C), and the
-// entry of lower slot k < C of row i is that of slot NS-1-k (the opposite
-// offset) of row i + off_k -- zero where that row is outside the array, as
-// it is, stored, where the row lies on the far side of the grid -- so a
-// symmetric level streams 14 of its 27 slot arrays (3D Q1)
 template <int D, int P, int MODE, typename TB, typename TY, bool RED>
 __global__ void __launch_bounds__(kBlock)
 k_st32(const float* __restrict__ A, long long N, long long Np, long long M, float w, const float* __restrict__ om,
        const float* __restrict__ x, const TB* __restrict__ b, TY* __restrict__ y, const double* __restrict__ v,
-       const double* __restrict__ v2, Reduce2 R, int sym) {
+       const double* __restrict__ v2, Reduce2 R) {
   constexpr int NS = St32<D, P>::NS;
   constexpr int C = St32<D, P>::CENTER;
   __shared__ double smem[8];
@@ -596,13 +591,11 @@ k_st32(const float* __restrict__ A, long long N, long long Np, long long M, floa
     if (MODE != 3) {
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        const long long j = i + soff<D, P>(k, M);
-        if (sym && k < C) a[k] = (j >= 0 && j < N) ? __ldg(A + (long long)(C - k) * Np + j) : 0.f;
-        else a[k] = __ldg(A + (long long)(sym ? k - C : k) * Np + i);
-        xv[k] = __ldg(x + clampi(j, N));
+        a[k] = __ldg(A + (long long)k * Np + i);
+        xv[k] = __ldg(x + clampi(i + soff<D, P>(k, M), N));
       }
     }
-    const float d = MODE != 3 ? a[C] : __ldg(A + (long long)(sym ? 0 : C) * Np + i);
+    const float d = MODE != 3 ? a[C] : __ldg(A + (long long)C * Np + i);
     float s = 0.f;
     if (MODE != 3) {
 #pragma unroll
@@ -754,7 +747,7 @@ k_prolong_q1(int MF, int MC, int dmask, const float* __restrict__ xc, float* __r
 }
 
 // 3D Q1 prolongation by coarse node (xf in layout fl): thread (I, J, K) updates the fine nodes
-// (2I+o+a, 2J+b, 2K+c), a, b, c in {0, 1}, from the 8 coarse values at
+// (2I+a, 2J+b, 2K+c), a, b, c in {0, 1}, from the 8 coarse values at
 // I..I+1, J..J+1, K..K+1, loaded once; each fine node is summed with the
 // weights and in the order of k_prolong_q1 (coarse Dirichlet values read as
 // zero, which is what a zero weight gives there).
@@ -763,12 +756,6 @@ k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __
   const int I = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, K = blockIdx.z;
   if (I >= MC || J >= MC) return;
   const long long MC2 = (long long)MC * MC;
-  // even row pitches (the padded layout): a thread's two fine x nodes form an
-  // 8-byte aligned pair when they start at an even element, so they start at
-  // 2I + (front mod 2); node 0 is then the Dirichlet face (front = 3 only
-  // then) and needs no update
-  const bool pair = !(fl.py & 1) && !(fl.pz & 1);
-  const int o = pair ? (fl.front & 1) : 0;
   float v[2][2][2];
 #pragma unroll
   for (int dz = 0; dz < 2; ++dz)
@@ -791,34 +778,21 @@ k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __
       const int fy = 2 * J + b;
       if (fy >= MF || fdir(fy, MF, 1, dmask)) continue;
       const float wy0 = b ? .5f : 1.f, wy1 = b ? .5f : 0.f;
-      // the x pair 2I + o, 2I + o + 1: rel = fx - 2I is 0 (parent I), 1
-      // (between I and I + 1) or 2 (parent I + 1); an even fine index takes its
-      // parent for both coarse slots, the second with weight 0
-      float acc2[2];
-      bool in2[2];
 #pragma unroll
-      for (int a2 = 0; a2 < 2; ++a2) {
-        const int rel = o + a2, fx = 2 * I + rel;
-        in2[a2] = fx < MF && !fdir(fx, MF, 0, dmask);
-        const float wx0 = rel == 1 ? .5f : 1.f, wx1 = rel == 1 ? .5f : 0.f;
+      for (int a = 0; a < 2; ++a) {
+        const int fx = 2 * I + a;
+        if (fx >= MF || fdir(fx, MF, 0, dmask)) continue;
+        const float wx0 = a ? .5f : 1.f, wx1 = a ? .5f : 0.f;
         float acc = 0.f;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const int bx = q & 1, by = (q >> 1) & 1, bz = q >> 2;
           const float ww = (bx ? wx1 : wx0) * (by ? wy1 : wy0) * (bz ? wz1 : wz0);
-          acc = fmaf(ww, v[c ? bz : 0][b ? by : 0][rel == 0 ? 0 : (rel == 1 ? bx : 1)], acc);
+          // even fine index: the second coarse node is the first one, weight 0
+          acc = fmaf(ww, v[c ? bz : 0][b ? by : 0][a ? bx : 0], acc);
         }
-        acc2[a2] = acc;
-      }
-      float* op = xf + fl.at(2 * I + o, fy, fz);
-      if (pair && in2[0] && in2[1]) {  // one 8-byte read-modify-write
-        float2 w2 = *reinterpret_cast<float2*>(op);
-        w2.x += acc2[0];
-        w2.y += acc2[1];
-        *reinterpret_cast<float2*>(op) = w2;
-      } else {
-        if (in2[0]) op[0] += acc2[0];
-        if (in2[1]) op[1] += acc2[1];
+        float* o = xf + fl.at(fx, fy, fz);
+        *o += acc;
       }
     }
   }
@@ -1271,22 +1245,22 @@ void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, boo
   typedef __nv_bfloat16 bf;
   MX_DISPATCH(L.dim, L.order, {
     if (R) {  // reductions only on FP32 vectors
-      if (mode == 0) k_st32<D, P, 0, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
-      else if (mode == 2) k_st32<D, P, 2, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
-      else k_st32<D, P, 1, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
+      if (mode == 0) k_st32<D, P, 0, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      else if (mode == 2) k_st32<D, P, 2, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      else k_st32<D, P, 1, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
     } else if (mode == 0) {
-      k_st32<D, P, 0, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
+      k_st32<D, P, 0, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
     } else if (mode == 1) {
-      if (b_bf16 && y_bf16) k_st32<D, P, 1, bf, bf, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (bf*)y, v, v2, r0, L.sym);
-      else if (b_bf16) k_st32<D, P, 1, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0, L.sym);
-      else if (y_bf16) k_st32<D, P, 1, float, bf, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (bf*)y, v, v2, r0, L.sym);
-      else k_st32<D, P, 1, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
+      if (b_bf16 && y_bf16) k_st32<D, P, 1, bf, bf, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (bf*)y, v, v2, r0);
+      else if (b_bf16) k_st32<D, P, 1, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0);
+      else if (y_bf16) k_st32<D, P, 1, float, bf, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (bf*)y, v, v2, r0);
+      else k_st32<D, P, 1, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
     } else if (mode == 2) {
-      if (b_bf16) k_st32<D, P, 2, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0, L.sym);
-      else k_st32<D, P, 2, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
+      if (b_bf16) k_st32<D, P, 2, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0);
+      else k_st32<D, P, 2, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
     } else {
-      if (b_bf16) k_st32<D, P, 3, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0, L.sym);
-      else k_st32<D, P, 3, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0, L.sym);
+      if (b_bf16) k_st32<D, P, 3, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0);
+      else k_st32<D, P, 3, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
     }
   });
 }
