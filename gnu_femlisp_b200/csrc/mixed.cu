@@ -353,7 +353,6 @@ k_mfc(MFArgsT<T> g, const __grid_constant__ CUtensorMap tk_cells, const __grid_c
   double acc0 = 0.0, acc1 = 0.0;
   if ((int)blockIdx.x >= geo.nface) {
     const int M = g.M, dm = g.dmask;
-    const long long MM = (long long)M * M;
     auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
     const T* om_src = UWD ? g.wd : g.omega;  // per-node damping source (OM)
     const T hs = g.hs;
@@ -575,41 +574,66 @@ __device__ __forceinline__ long long soff(int s, long long M) {
 }
 
 // mode 0: y = A x; 1: y = b - A x; 2: y = x + w (b - Ax)/d; 3: y = w b/d
-// One row per thread (the 27 loads of a row are its only latency chain).
-template <int D, int P, int MODE, typename TB, typename TY, bool RED>
+// RPT consecutive rows per thread: with four, a slot's four coefficients come
+// as one 16-byte load (the slot arrays are 256-byte aligned, Np a multiple of
+// 64) and the neighbour values through L1 -- for the large levels, which are
+// bandwidth-bound; one row per thread on the small, latency-bound ones (and
+// on the 125-slot 3D Q2 rows, whose four-row form would spill).  Each row
+// sums in slot order either way.
+template <int D, int P, int MODE, typename TB, typename TY, bool RED, int RPT>
 __global__ void __launch_bounds__(kBlock)
 k_st32(const float* __restrict__ A, long long N, long long Np, long long M, float w, const float* __restrict__ om,
        const float* __restrict__ x, const TB* __restrict__ b, TY* __restrict__ y, const double* __restrict__ v,
        const double* __restrict__ v2, Reduce2 R) {
   constexpr int NS = St32<D, P>::NS;
   constexpr int C = St32<D, P>::CENTER;
+  static_assert(RPT == 1 || RPT == 4, "one or four rows per thread");
   __shared__ double smem[8];
   double acc0 = 0.0, acc1 = 0.0;
-  const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
-  if (i < N) {
-    float a[NS], xv[NS];
-    if (MODE != 3) {
+  const long long i0 = ((long long)blockIdx.x * kBlock + threadIdx.x) * RPT;
+  if (i0 < N) {
+    float s[RPT], d[RPT], xc[RPT];
 #pragma unroll
-      for (int k = 0; k < NS; ++k) {
-        a[k] = __ldg(A + (long long)k * Np + i);
-        xv[k] = __ldg(x + clampi(i + soff<D, P>(k, M), N));
+    for (int r = 0; r < RPT; ++r) s[r] = xc[r] = 0.f;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      if (MODE == 3 && k != C) continue;
+      float a[RPT];
+      if constexpr (RPT == 4) {
+        const float4 a4 = __ldg(reinterpret_cast<const float4*>(A + (long long)k * Np + i0));
+        a[0] = a4.x; a[1] = a4.y; a[2] = a4.z; a[3] = a4.w;
+      } else {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) a[r] = __ldg(A + (long long)k * Np + i0 + r);
+      }
+      if (k == C) {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) d[r] = a[r];
+      }
+      if (MODE == 3) continue;
+      const long long o = soff<D, P>(k, M);
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        const float xv = __ldg(x + clampi(i0 + r + o, N));
+        s[r] = fmaf(a[r], xv, s[r]);
+        if (k == C) xc[r] = xv;
       }
     }
-    const float d = MODE != 3 ? a[C] : __ldg(A + (long long)C * Np + i);
-    float s = 0.f;
-    if (MODE != 3) {
 #pragma unroll
-      for (int k = 0; k < NS; ++k) s = fmaf(a[k], xv[k], s);
-    }
-    float out;
-    if (MODE == 0) out = s;
-    else if (MODE == 1) out = ldv(b, i) - s;
-    else if (MODE == 2) out = fmaf(om ? om[i] : w, (ldv(b, i) - s) / d, xv[C]);
-    else out = (om ? om[i] : w) * (ldv(b, i) / d);
-    stv(y, i, out);
-    if (RED) {
-      acc0 = fma((double)out, (double)v[i], acc0);
-      if (v2) acc1 = fma((double)out, (double)v2[i], acc1);
+    for (int r = 0; r < RPT; ++r) {
+      const long long i = i0 + r;
+      if (i < N) {
+        float out;
+        if (MODE == 0) out = s[r];
+        else if (MODE == 1) out = ldv(b, i) - s[r];
+        else if (MODE == 2) out = fmaf(om ? om[i] : w, (ldv(b, i) - s[r]) / d[r], xc[r]);
+        else out = (om ? om[i] : w) * (ldv(b, i) / d[r]);
+        stv(y, i, out);
+        if (RED) {
+          acc0 = fma((double)out, (double)v[i], acc0);
+          if (v2) acc1 = fma((double)out, (double)v2[i], acc1);
+        }
+      }
     }
   }
   if (RED) dr_finish2(acc0, acc1, R, smem);
@@ -1237,30 +1261,44 @@ void mx_top_residual64(const MFArgs64& g, const double* x, const double* b, doub
 
 long long mx_top_blocks(int M) { return mft_blocks(mft_geo(M, 63)); }  // the most face CTAs any mask gives
 
+// levels from this many rows on take four rows per thread
+constexpr long long kSt32Wide = 1ll << 20;
+
+template <int D, int P, int MODE, typename TB, typename TY, bool RED>
+void st32_launch(const Lev32& L, const float* x, const void* b, void* y, const double* v, const double* v2,
+                 const Reduce2& r0, cudaStream_t st) {
+  constexpr int W = (D == 3 && P == 2) ? 1 : 4;
+  if (W == 4 && L.N >= kSt32Wide)
+    k_st32<D, P, MODE, TB, TY, RED, W><<<g1((L.N + W - 1) / W), kBlock, 0, st>>>(
+        L.A, L.N, L.Np, L.M, L.w, L.om, x, (const TB*)b, (TY*)y, v, v2, r0);
+  else
+    k_st32<D, P, MODE, TB, TY, RED, 1><<<g1(L.N), kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x,
+                                                                    (const TB*)b, (TY*)y, v, v2, r0);
+}
+
 void mx_level_apply(int mode, const Lev32& L, const float* x, const void* b, bool b_bf16, void* y, bool y_bf16,
                     const double* v, const double* v2, const Reduce2* R, cudaStream_t st) {
-  const unsigned grid = g1(L.N);
   Reduce2 r0 = R ? *R : Reduce2{};
   g_launches.fetch_add(1, std::memory_order_relaxed);
   typedef __nv_bfloat16 bf;
   MX_DISPATCH(L.dim, L.order, {
     if (R) {  // reductions only on FP32 vectors
-      if (mode == 0) k_st32<D, P, 0, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
-      else if (mode == 2) k_st32<D, P, 2, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
-      else k_st32<D, P, 1, float, float, true><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      if (mode == 0) st32_launch<D, P, 0, float, float, true>(L, x, b, y, v, v2, r0, st);
+      else if (mode == 2) st32_launch<D, P, 2, float, float, true>(L, x, b, y, v, v2, r0, st);
+      else st32_launch<D, P, 1, float, float, true>(L, x, b, y, v, v2, r0, st);
     } else if (mode == 0) {
-      k_st32<D, P, 0, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      st32_launch<D, P, 0, float, float, false>(L, x, b, y, v, v2, r0, st);
     } else if (mode == 1) {
-      if (b_bf16 && y_bf16) k_st32<D, P, 1, bf, bf, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (bf*)y, v, v2, r0);
-      else if (b_bf16) k_st32<D, P, 1, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0);
-      else if (y_bf16) k_st32<D, P, 1, float, bf, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (bf*)y, v, v2, r0);
-      else k_st32<D, P, 1, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      if (b_bf16 && y_bf16) st32_launch<D, P, 1, bf, bf, false>(L, x, b, y, v, v2, r0, st);
+      else if (b_bf16) st32_launch<D, P, 1, bf, float, false>(L, x, b, y, v, v2, r0, st);
+      else if (y_bf16) st32_launch<D, P, 1, float, bf, false>(L, x, b, y, v, v2, r0, st);
+      else st32_launch<D, P, 1, float, float, false>(L, x, b, y, v, v2, r0, st);
     } else if (mode == 2) {
-      if (b_bf16) k_st32<D, P, 2, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0);
-      else k_st32<D, P, 2, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      if (b_bf16) st32_launch<D, P, 2, bf, float, false>(L, x, b, y, v, v2, r0, st);
+      else st32_launch<D, P, 2, float, float, false>(L, x, b, y, v, v2, r0, st);
     } else {
-      if (b_bf16) k_st32<D, P, 3, bf, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const bf*)b, (float*)y, v, v2, r0);
-      else k_st32<D, P, 3, float, float, false><<<grid, kBlock, 0, st>>>(L.A, L.N, L.Np, L.M, L.w, L.om, x, (const float*)b, (float*)y, v, v2, r0);
+      if (b_bf16) st32_launch<D, P, 3, bf, float, false>(L, x, b, y, v, v2, r0, st);
+      else st32_launch<D, P, 3, float, float, false>(L, x, b, y, v, v2, r0, st);
     }
   });
 }
