@@ -834,8 +834,9 @@ def run_profile_c2(args):
 def run_profile_mfs(args):
     """The matrix-free top-level kernels of the mixed solve at `--level`: one
     plain mixed solve (no damping network) leaves their buffers, then one
-    launch of each (FMG_MXK_SMOOTH, FMG_MXK_MATVEC64, FMG_MXK_RESIDUAL)
-    inside the NVTX range 'mfs' (ncu --nvtx --nvtx-include mfs/)."""
+    launch of each (FMG_MXK_SMOOTH, FMG_MXK_MATVEC64, FMG_MXK_RESIDUAL, and the
+    top-level transfers FMG_MXK_RESTRICT, FMG_MXK_PROLONG) inside the NVTX
+    range 'mfs' (ncu --nvtx --nvtx-include mfs/)."""
     import torch
 
     import gnu_femlisp_b200 as G
@@ -850,7 +851,8 @@ def run_profile_mfs(args):
     g.solve_mixed(plain_cfg(G), x, matrix_free=True)
     ctx.synchronize()
     torch.cuda.nvtx.range_push("mfs")
-    for kind in (C.FMG_MXK_SMOOTH, C.FMG_MXK_MATVEC64, C.FMG_MXK_RESIDUAL):
+    for kind in (C.FMG_MXK_SMOOTH, C.FMG_MXK_MATVEC64, C.FMG_MXK_RESIDUAL, C.FMG_MXK_RESTRICT,
+                 C.FMG_MXK_PROLONG):
         g.mixed_top_kernel(kind, 1)
     ctx.synchronize()
     torch.cuda.nvtx.range_pop()

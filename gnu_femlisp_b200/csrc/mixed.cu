@@ -654,6 +654,26 @@ k_restrict_q1(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat1
                      D > 2 ? (int)blockIdx.z : 0};
   if (cJ[0] >= MC || cJ[1] >= MC) return;
   const long long J = cJ[0] + (long long)MC * (cJ[1] + (long long)MC * cJ[2]);
+  if (D == 3 && cJ[0] >= 1 && cJ[0] <= MC - 2 && cJ[1] >= 1 && cJ[1] <= MC - 2 && cJ[2] >= 1 && cJ[2] <= MC - 2) {
+    // interior coarse node: its 27 fine neighbours lie inside and off every
+    // face; weights 1/2, 1, 1/2 applied one direction at a time
+    const long long MF2 = (long long)MF * MF;
+    const TR* p0 = rf + (2 * cJ[0] - 1) + (long long)MF * (2 * cJ[1] - 1) + MF2 * (2 * cJ[2] - 1);
+    float t[3];
+#pragma unroll
+    for (int z = 0; z < 3; ++z) {
+      float u[3];
+#pragma unroll
+      for (int y = 0; y < 3; ++y) {
+        const TR* q = p0 + (long long)MF * y + MF2 * z;
+        u[y] = fmaf(.5f, ldv(q, 0) + ldv(q, 2), ldv(q, 1));
+      }
+      t[z] = fmaf(.5f, u[0] + u[2], u[1]);
+    }
+    bc[J] = __float2bfloat16_rn(fmaf(.5f, t[0] + t[2], t[1]));
+    xc[J] = 0.f;
+    return;
+  }
   bool dj = false;
 #pragma unroll
   for (int k = 0; k < D; ++k) dj = dj || fdir(cJ[k], MC, k, dmask);
@@ -772,14 +792,59 @@ k_prolong_q1(int MF, int MC, int dmask, const float* __restrict__ xc, float* __r
 
 // 3D Q1 prolongation by coarse node (xf in layout fl): thread (I, J, K) updates the fine nodes
 // (2I+a, 2J+b, 2K+c), a, b, c in {0, 1}, from the 8 coarse values at
-// I..I+1, J..J+1, K..K+1, loaded once; each fine node is summed with the
-// weights and in the order of k_prolong_q1 (coarse Dirichlet values read as
-// zero, which is what a zero weight gives there).
+// I..I+1, J..J+1, K..K+1, loaded once (coarse Dirichlet values read as
+// zero, which is what a zero weight gives there).  Cells whose fine nodes are
+// all off the faces interpolate one direction at a time; the others sum each
+// fine node with the weights and in the order of k_prolong_q1.
 __global__ void __launch_bounds__(kBlock)
 k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __restrict__ xf, VLay fl) {
   const int I = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, K = blockIdx.z;
   if (I >= MC || J >= MC) return;
   const long long MC2 = (long long)MC * MC;
+  if (I >= 1 && I <= MC - 2 && J >= 1 && J <= MC - 2 && K >= 1 && K <= MC - 2) {
+    // the eight fine nodes lie inside and off every face (only the coarse
+    // neighbours I + 1, J + 1, K + 1 can sit on a face): interpolate one
+    // direction at a time (weights 1 and 1/2, 1/2), read all eight fine
+    // values, then write them
+    const float* c0 = xc + K * MC2 + (long long)J * MC + I;
+    const bool hx = I + 1 < MC - 1 || !(dmask & 2), hy = J + 1 < MC - 1 || !(dmask & 8),
+               hz = K + 1 < MC - 1 || !(dmask & 32);
+    float e[2][2][2];
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+        const bool ok = (dz == 0 || hz) && (dy == 0 || hy);
+        const float* q = c0 + MC2 * dz + (long long)MC * dy;
+        const float v0 = ok ? __ldg(q) : 0.f, v1 = ok && hx ? __ldg(q + 1) : 0.f;
+        e[dz][dy][0] = v0;
+        e[dz][dy][1] = .5f * (v0 + v1);
+      }
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int a = 0; a < 2; ++a) e[dz][1][a] = .5f * (e[dz][0][a] + e[dz][1][a]);
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int a = 0; a < 2; ++a) e[1][b][a] = .5f * (e[0][b][a] + e[1][b][a]);
+    float* o = xf + fl.at(2 * I, 2 * J, 2 * K);
+    const long long py = fl.py, pz = fl.pz;
+    float old[2][2][2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int a = 0; a < 2; ++a) old[c][b][a] = o[a + py * b + pz * c];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int a = 0; a < 2; ++a) o[a + py * b + pz * c] = old[c][b][a] + e[c][b][a];
+    return;
+  }
   float v[2][2][2];
 #pragma unroll
   for (int dz = 0; dz < 2; ++dz)
@@ -792,20 +857,32 @@ k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __
                         !fdir(ck, MC, 2, dmask);
         v[dz][dy][dx] = ok ? __ldg(xc + ck * MC2 + (long long)cj * MC + ci) : 0.f;
       }
+  // the eight fine values are read before any is written (the compiler
+  // cannot tell that the eight layout offsets differ), so their loads overlap
+  bool fok[2][2][2];
+  long long fo[2][2][2];
+  float old[2][2][2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int fx = 2 * I + a, fy = 2 * J + b, fz = 2 * K + c;
+        fok[c][b][a] = fx < MF && fy < MF && fz < MF && !fdir(fx, MF, 0, dmask) && !fdir(fy, MF, 1, dmask) &&
+                       !fdir(fz, MF, 2, dmask);
+        fo[c][b][a] = fl.at(fx, fy, fz);
+        old[c][b][a] = fok[c][b][a] ? xf[fo[c][b][a]] : 0.f;
+      }
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-    const int fz = 2 * K + c;
-    if (fz >= MF || fdir(fz, MF, 2, dmask)) continue;
     const float wz0 = c ? .5f : 1.f, wz1 = c ? .5f : 0.f;
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
-      const int fy = 2 * J + b;
-      if (fy >= MF || fdir(fy, MF, 1, dmask)) continue;
       const float wy0 = b ? .5f : 1.f, wy1 = b ? .5f : 0.f;
 #pragma unroll
       for (int a = 0; a < 2; ++a) {
-        const int fx = 2 * I + a;
-        if (fx >= MF || fdir(fx, MF, 0, dmask)) continue;
+        if (!fok[c][b][a]) continue;
         const float wx0 = a ? .5f : 1.f, wx1 = a ? .5f : 0.f;
         float acc = 0.f;
 #pragma unroll
@@ -815,11 +892,93 @@ k_prolong_q1c(int MF, int MC, int dmask, const float* __restrict__ xc, float* __
           // even fine index: the second coarse node is the first one, weight 0
           acc = fmaf(ww, v[c ? bz : 0][b ? by : 0][a ? bx : 0], acc);
         }
-        float* o = xf + fl.at(fx, fy, fz);
-        *o += acc;
+        xf[fo[c][b][a]] = old[c][b][a] + acc;
       }
     }
   }
+}
+
+// 3D Q1 prolongation into a padded layout (rows of py = 4k elements, planes
+// of pz = py M, the array 16-byte aligned): thread (m, J, K) updates the
+// entries at row offsets 4m .. 4m + 3 of the fine rows (2J + b, 2K + c),
+// b, c in {0, 1}, one 16-byte load and store per row, all loads before the
+// stores; pads, Dirichlet nodes and nodes outside the grid get a zero
+// correction.  The four coarse rows (J..J+1, K..K+1) are read on the three
+// columns the four fine x need and interpolated over y, z, then x (coarse
+// Dirichlet values read as zero).
+__global__ void __launch_bounds__(kBlock)
+k_prolong_q1v(int MF, int MC, int dmask, const float* __restrict__ xc, float* __restrict__ xf, VLay fl) {
+  const unsigned q = (unsigned)fl.py >> 2;
+  const unsigned idx = blockIdx.x * kBlock + threadIdx.x;
+  if (idx >= q * (unsigned)MC) return;
+  const int J = (int)(idx / q), m = (int)(idx - (unsigned)J * q), K = blockIdx.y;
+  const int x0 = 4 * m - fl.front;
+  const int c0 = x0 >> 1;  // floor(x0 / 2), x0 >= -3
+  bool okc[3], oky[2], okz[2];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) okc[t] = c0 + t >= 0 && c0 + t < MC && !fdir(c0 + t, MC, 0, dmask);
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    oky[d] = J + d < MC && !fdir(J + d, MC, 1, dmask);
+    okz[d] = K + d < MC && !fdir(K + d, MC, 2, dmask);
+  }
+  const long long MC2 = (long long)MC * MC;
+  float R[2][2][3];
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy) {
+      const float* row = xc + (K + dz) * MC2 + (long long)(J + dy) * MC + c0;
+#pragma unroll
+      for (int t = 0; t < 3; ++t) R[dz][dy][t] = okz[dz] && oky[dy] && okc[t] ? __ldg(row + t) : 0.f;
+    }
+  // over y, then z: R[c][b][t] becomes the value on fine row (2J + b, 2K + c)
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int t = 0; t < 3; ++t) R[dz][1][t] = .5f * (R[dz][0][t] + R[dz][1][t]);
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int t = 0; t < 3; ++t) R[1][b][t] = .5f * (R[0][b][t] + R[1][b][t]);
+  bool okx[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) okx[l] = x0 + l >= 0 && x0 + l < MF && !fdir(x0 + l, MF, 0, dmask);
+  bool okr[2][2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int fy = 2 * J + b, fz = 2 * K + c;
+      okr[c][b] = fy < MF && fz < MF && !fdir(fy, MF, 1, dmask) && !fdir(fz, MF, 2, dmask);
+    }
+  float4* o = reinterpret_cast<float4*>(xf + (long long)fl.py * (2 * J) + fl.pz * (2 * K) + 4 * m);
+  const long long qy = q, qz = fl.pz >> 2;  // row and plane strides in float4
+  float4 v[2][2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+      if (okr[c][b]) v[c][b] = o[qy * b + qz * c];
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      if (!okr[c][b]) continue;
+      const float* r = R[c][b];
+      float e[4];
+      if (x0 & 1) {  // x0 = 2 c0 + 1
+        e[0] = .5f * (r[0] + r[1]); e[1] = r[1]; e[2] = .5f * (r[1] + r[2]); e[3] = r[2];
+      } else {
+        e[0] = r[0]; e[1] = .5f * (r[0] + r[1]); e[2] = r[1]; e[3] = .5f * (r[1] + r[2]);
+      }
+      float4 w = v[c][b];
+      w.x += okx[0] ? e[0] : 0.f;
+      w.y += okx[1] ? e[1] : 0.f;
+      w.z += okx[2] ? e[2] : 0.f;
+      w.w += okx[3] ? e[3] : 0.f;
+      o[qy * b + qz * c] = w;
+    }
 }
 
 // Q2 (and any order): generic stencil with runtime lengths
@@ -1335,7 +1494,10 @@ void mx_prolong(const Lev32& C, const Lev32& F, const float* xc, float* xf, cuda
   g_launches.fetch_add(1, std::memory_order_relaxed);
   const dim3 gr = xgrid(F.M, F.dim), bl(32, 8);
   if (F.order == 1) {
-    if (F.dim == 3)
+    if (F.dim == 3 && xfl && xfl->py % 4 == 0 && xfl->pz % 4 == 0 && ((uintptr_t)xf & 15) == 0)
+      k_prolong_q1v<<<dim3((unsigned)((xfl->py / 4 * C.M + kBlock - 1) / kBlock), (unsigned)C.M), kBlock, 0, st>>>(
+          (int)F.M, (int)C.M, F.dmask, xc, xf, *xfl);
+    else if (F.dim == 3)
       k_prolong_q1c<<<dim3((unsigned)((C.M + 31) / 32), (unsigned)((C.M + 7) / 8), (unsigned)C.M), bl, 0, st>>>(
           (int)F.M, (int)C.M, F.dmask, xc, xf, xfl ? *xfl : natural_lay((int)F.M, 3));
     else if (F.dim == 2) k_prolong_q1<2><<<gr, bl, 0, st>>>((int)F.M, (int)C.M, F.dmask, xc, xf);

@@ -53,6 +53,29 @@ def test_mixed_reaches_tolerance_and_matches_fp64(G, ctx, matrix_free):
     assert ninner <= 30
 
 
+@pytest.mark.parametrize("dmask", [21, 42, 7, 56, 45])
+def test_mixed_matrix_free_boundary_masks(G, ctx, dmask):
+    # Dirichlet on some faces only: the padded layout's front, the face CTAs
+    # and the transfers at Neumann faces; the matrix-free solve takes the
+    # stored solve's steps and reaches the FP64 solution
+    from gnu_femlisp_b200 import problems
+    g = G.Grid(ctx, 3, 1, 5, base_level=2, dirichlet_mask=dmask)
+    g.set_coefficient(G._capi.FMG_K_CELL, np.exp(problems.fourier_log_field(32, 3, 5)))
+    g.assemble()
+    x64 = g.vector()
+    _, _, st64 = g.solve(_cfg(G, 1e-13), x64)
+    assert st64 == 0
+    steps = {}
+    for mf in (True, False):
+        xm = g.vector()
+        hist, nouter, ninner, st = g.solve_mixed(_cfg(G, 1e-10), xm, matrix_free=mf)
+        assert st == 0 and hist[-1] / hist[0] < 1e-10, (mf, hist)
+        rel = np.linalg.norm(xm.get() - x64.get()) / np.linalg.norm(x64.get())
+        assert rel <= 1e-10, (mf, rel)
+        steps[mf] = ninner
+    assert abs(steps[True] - steps[False]) <= 1, steps
+
+
 def test_mixed_tight_tolerance_error_vs_fp64(G, ctx):
     # both driven to 1e-13: the mixed result agrees with FP64 to 1e-10
     g = _grid(G, ctx, 3, 6, 2, seed=1)
