@@ -113,26 +113,30 @@ __device__ __forceinline__ void mf_row(const T (&k)[2][2][2], const XF& X, T hs,
   xc = T(0);
   if (HX) {
     xc = X(0, 0, 0);
-    auto term = [&](T w, T xj) { sacc = DIFF ? fma(w, xc - xj, sacc) : fma(w, xj, sacc); };
+    // three independent sums (the plane's own 4 terms, then 8 for each of the
+    // planes below and above) so that the multiply-add chains overlap
+    T sp[3] = {T(0), T(0), T(0)};
+    auto term = [&](int a, T w, T xj) { sp[a] = DIFF ? fma(w, xc - xj, sp[a]) : fma(w, xj, sp[a]); };
 #pragma unroll
     for (int sy = 0; sy < 2; ++sy)
 #pragma unroll
-      for (int sx = 0; sx < 2; ++sx) term(wc[sy][sx], X(2 * sx - 1, 2 * sy - 1, 0));
+      for (int sx = 0; sx < 2; ++sx) term(0, wc[sy][sx], X(2 * sx - 1, 2 * sy - 1, 0));
 #pragma unroll
     for (int cz = 0; cz < 2; ++cz) {
       const int dz = 2 * cz - 1;
 #pragma unroll
       for (int sx = 0; sx < 2; ++sx)  // face diagonals (sx, 0, sz): cells (sx, *, sz)
-        term(k[cz][0][sx] + k[cz][1][sx], X(2 * sx - 1, 0, dz));
+        term(1 + cz, k[cz][0][sx] + k[cz][1][sx], X(2 * sx - 1, 0, dz));
 #pragma unroll
       for (int sy = 0; sy < 2; ++sy)  // face diagonals (0, sy, sz): cells (*, sy, sz)
-        term(k[cz][sy][0] + k[cz][sy][1], X(0, 2 * sy - 1, dz));
+        term(1 + cz, k[cz][sy][0] + k[cz][sy][1], X(0, 2 * sy - 1, dz));
 #pragma unroll
       for (int sy = 0; sy < 2; ++sy)
 #pragma unroll
         for (int sx = 0; sx < 2; ++sx)  // body diagonals
-          term(k[cz][sy][sx], X(2 * sx - 1, 2 * sy - 1, dz));
+          term(1 + cz, k[cz][sy][sx], X(2 * sx - 1, 2 * sy - 1, dz));
     }
+    sacc = sp[0] + (sp[1] + sp[2]);
     if (!DIFF) sacc = fma(T(4) * ksum, xc, -sacc);
   }
   d = T(4) * hs * ksum;

@@ -1505,17 +1505,19 @@ void mf_apply(int M, int dm, const double* kc, const double* xd, const double* b
                           {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
       const T ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
       const T xc = X(0, 0, 0);
-      T s = T(0);
-      auto term = [&](T w, T xj) { s = DIFF ? std::fma(w, xc - xj, s) : std::fma(w, xj, s); };
+      // three partial sums: the node's own plane, the plane below, the plane above
+      T sp[3] = {T(0), T(0), T(0)};
+      auto term = [&](int a, T w, T xj) { sp[a] = DIFF ? std::fma(w, xc - xj, sp[a]) : std::fma(w, xj, sp[a]); };
       for (int sy = 0; sy < 2; ++sy)
-        for (int sx = 0; sx < 2; ++sx) term(wc[sy][sx], X(2 * sx - 1, 2 * sy - 1, 0));
+        for (int sx = 0; sx < 2; ++sx) term(0, wc[sy][sx], X(2 * sx - 1, 2 * sy - 1, 0));
       for (int cz = 0; cz < 2; ++cz) {
         const int dz = 2 * cz - 1;
-        for (int sx = 0; sx < 2; ++sx) term(k[cz][0][sx] + k[cz][1][sx], X(2 * sx - 1, 0, dz));
-        for (int sy = 0; sy < 2; ++sy) term(k[cz][sy][0] + k[cz][sy][1], X(0, 2 * sy - 1, dz));
+        for (int sx = 0; sx < 2; ++sx) term(1 + cz, k[cz][0][sx] + k[cz][1][sx], X(2 * sx - 1, 0, dz));
+        for (int sy = 0; sy < 2; ++sy) term(1 + cz, k[cz][sy][0] + k[cz][sy][1], X(0, 2 * sy - 1, dz));
         for (int sy = 0; sy < 2; ++sy)
-          for (int sx = 0; sx < 2; ++sx) term(k[cz][sy][sx], X(2 * sx - 1, 2 * sy - 1, dz));
+          for (int sx = 0; sx < 2; ++sx) term(1 + cz, k[cz][sy][sx], X(2 * sx - 1, 2 * sy - 1, dz));
       }
+      T s = sp[0] + (sp[1] + sp[2]);
       if (!DIFF) s = std::fma(T(4) * ksum, xc, -s);
       ax = hs * s;
     }
