@@ -38,10 +38,10 @@ HBM_FALLBACK_GBS = 6650.0
 JUDGE_STEPS = 1  # CG steps after each (re)start on which the plain cycle judges the learned one
 # DRAM bytes per top-level node of one launch (read + write), from the ncu
 # capture of the 257^3 case (profiles/k_mfc_q1_3d_mixed_257cube.md): mode 2
-# 668.6 MB, FP64 mode 0 324.8 MB, mode 1 274.0 MB over 16,974,593 nodes
-TOP_TRAFFIC_B_PER_NODE = {"k_mfc<float,double,float,2,1,7>": 668.6e6 / 16974593,
-                          "k_mfc<double,float,float,0,1,0>": 324.8e6 / 16974593,
-                          "k_mfc<float,double,float,1,0,0>": 274.0e6 / 16974593}
+# 668.7 MB, FP64 mode 0 322.2 MB, mode 1 273.0 MB over 16,974,593 nodes
+TOP_TRAFFIC_B_PER_NODE = {"k_mfc<float,double,float,2,1,7>": 668.7e6 / 16974593,
+                          "k_mfc<double,float,float,0,1,0>": 322.2e6 / 16974593,
+                          "k_mfc<float,double,float,1,0,0>": 273.0e6 / 16974593}
 
 
 def parse_args():
