@@ -2812,8 +2812,13 @@ int net_level_forward(fmg_net* net, fmg_grid* g, int l, bool with_mean) {
   for (int k = 0; k < g->dim; ++k) ncell_top *= T.n;
   const bool kc = g->kkind == FMG_K_CELL;
   if (with_mean) {
-    if (kc) launch_logmean(g->kcell_d, ncell_top, net->stat + 8, net->stat, st);
-    else launch_set_scalar(net->stat, std::log(g->kconst), st);
+    if (kc) {
+      if ((rc = launch_logmean(net, g->kcell_d, ncell_top, net->stat, st)))
+        return set_err(c, rc, "damping network: no memory");
+    } else {
+      net->lraw_n = 0;
+      launch_set_scalar(net->stat, std::log(g->kconst), st);
+    }
   }
   const ActGeom ag = act_geom(g->dim, (int)L.M, 1);
   if ((rc = launch_features(net, ag, (int)L.n, g->order, T.n, std::ldexp(1.0, g->top - l), g->np, g->xi_d,
@@ -3048,7 +3053,7 @@ int fmg_net_create(fmg_ctx* c, int dim, unsigned long long seed, fmg_net** out) 
       (rc = net_alloc(net, (void**)&net->wf3, T * kNetOut * kNetHid * nb)) ||
       (rc = net_alloc(net, (void**)&net->wb2, T * kNetHid * kNetHid * nb)) ||
       (rc = net_alloc(net, (void**)&net->wb3, T * kNetHid * kNetOut * nb)) ||
-      (rc = net_alloc(net, (void**)&net->stat, 512 * sizeof(double))) ||
+      (rc = net_alloc(net, (void**)&net->stat, (8 + kLogSumBlocks) * sizeof(double))) ||
       (rc = net_alloc(net, (void**)&net->err, sizeof(unsigned)))) {
     net_release(net);
     return set_err(c, rc, "damping network: device allocation failed");

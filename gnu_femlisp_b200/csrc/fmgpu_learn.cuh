@@ -23,6 +23,7 @@ namespace fmg {
 constexpr int kNetIn = 16;    // input channels (padded)
 constexpr int kNetHid = 32;   // hidden channels
 constexpr int kNetOut = 16;   // output channels of the last GEMM (channel 0 used)
+constexpr int kLogSumBlocks = 1184;  // blocks of the mean-log-k reduction (8 per SM of a B200)
 
 // offsets of the flat FP32 parameter vector
 struct NetLayout {
@@ -67,9 +68,11 @@ struct fmg_net {
   bool have_forward = false;
   float* part = nullptr;       // weight-gradient partials
   long long part_cap = 0;
-  double* stat = nullptr;      // [0] mean log k, scratch partials after it
+  double* stat = nullptr;      // [0] mean log k, from [8] the kLogSumBlocks partials of its sum
   double* lk = nullptr;        // cell log-coefficients of the level being featurised
   long long lk_cap = 0;
+  double* lraw = nullptr;      // log k of every top-level cell, taken with the mean
+  long long lraw_cap = 0, lraw_n = 0;  // capacity; cells it holds now (0: none)
   unsigned* err = nullptr;     // device error word (bounded waits that ran out)
   std::vector<void*> allocs;
 };
@@ -83,7 +86,7 @@ int net_reserve(fmg_net* net, const ActGeom& g);  // activation buffers for g
 void net_refresh_weights(fmg_net* net, cudaStream_t st);
 
 // mean of log k over n cells -> *out (device), deterministic
-void launch_logmean(const double* k, long long n, double* scratch, double* out, cudaStream_t st);
+int launch_logmean(fmg_net* net, const double* k, long long n, double* out, cudaStream_t st);
 // features of level nodes (Q1): cells of n_l per direction, coefficient of
 // the top level (n_top cells per direction) sampled at np Gauss points xi
 // per direction of each level cell (ratio = n_top / n_l); kconst used when

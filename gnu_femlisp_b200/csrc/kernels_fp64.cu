@@ -398,6 +398,11 @@ k_jacobi_q2(const double* __restrict__ A, long long N, long long Np, long long M
 // arrays are contiguous, so a warp's loads of one slot stay within a few
 // sectors.
 constexpr int kQ2T = 128;  // threads per block
+// matvec and Jacobi residual in 3D: four blocks per SM (at most 128
+// registers: the batched loads of a stencil plane fit without spills, 16
+// warps per SM instead of 12; the SOR sweep measured slower so)
+template <int D>
+constexpr int kQ2MinBlocks = D == 3 ? 4 : 1;
 
 struct Q2Sub {
   int d[3], j0[3], n[3];  // class digit, first place and row count along each direction
@@ -577,7 +582,7 @@ k_sor_q2(const double* __restrict__ A, long long Np, int M, int colour, double o
 
 // y = A x or r = b - A x on a scalar Q2 level, rows by class (blockIdx.y) and parity
 template <int D, bool RES>
-__global__ void __launch_bounds__(kQ2T)
+__global__ void __launch_bounds__(kQ2T, kQ2MinBlocks<D>)
 k_spmv_q2c(const double* __restrict__ A, long long Np, int M, const double* __restrict__ x, const double* b,
            double* y, const __grid_constant__ Q2Layout lay) {
   int pat;
@@ -594,7 +599,7 @@ k_spmv_q2c(const double* __restrict__ A, long long Np, int M, const double* __re
 
 // k_jacobi_res on a scalar Q2 level, rows by class and parity
 template <int D>
-__global__ void __launch_bounds__(kQ2T)
+__global__ void __launch_bounds__(kQ2T, kQ2MinBlocks<D>)
 k_jacobi_res_q2c(const double* __restrict__ A, long long Np, int M, double damp, const double* __restrict__ omega,
                  const double* __restrict__ x, const double* b, double* __restrict__ xout, double* r, int write_r,
                  const __grid_constant__ Q2Layout lay) {

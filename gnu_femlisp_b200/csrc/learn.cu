@@ -724,12 +724,18 @@ __global__ void k_adam(float* __restrict__ P, float* __restrict__ G, float* __re
   G[i] = 0.f;
 }
 
-// deterministic sum of log k over n values: per-block partials then one block
-__global__ void __launch_bounds__(kBlock) k_logsum(const double* __restrict__ k, long long n, double* __restrict__ part) {
+// raw[i] = log k[i] and a deterministic sum of them: per-block partials (a
+// fixed grid of eight blocks per SM of a B200, so the FP64 logarithms of all
+// SMs overlap) then one block
+__global__ void __launch_bounds__(kBlock) k_logsum(const double* __restrict__ k, long long n, double* __restrict__ raw,
+                                                   double* __restrict__ part) {
   __shared__ double sm[8];
   double acc = 0.0;
-  for (long long i = (long long)blockIdx.x * kBlock + threadIdx.x; i < n; i += (long long)gridDim.x * kBlock)
-    acc += log(k[i]);
+  for (long long i = (long long)blockIdx.x * kBlock + threadIdx.x; i < n; i += (long long)gridDim.x * kBlock) {
+    const double l = log(k[i]);
+    raw[i] = l;
+    acc += l;
+  }
   const double s = dr_fold256(acc, sm);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
@@ -754,10 +760,12 @@ __global__ void k_ratio_acc(double* scal, int dst, int num, int den, double fact
 // cell's np^D Gauss points xi, k being the top level's cell coefficient
 // (ratio = n_top / n_l fine cells per level cell and direction).  Consecutive
 // points in one fine cell reuse its logarithm (the same value the sum would
-// add again), so the top level costs one log per cell.
+// add again), so the top level costs one log per cell; with lraw (log k of
+// every top-level cell, taken with the mean) no level takes a logarithm.
 template <int D>
 __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, const double* __restrict__ xi,
-                            const double* __restrict__ kcell, double* __restrict__ lk) {
+                            const double* __restrict__ kcell, const double* __restrict__ lraw,
+                            double* __restrict__ lk) {
   long long nc = n_l;
   for (int k = 1; k < D; ++k) nc *= n_l;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -767,7 +775,7 @@ __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, cons
   int nq = 1;
   for (int k = 0; k < D; ++k) nq *= np;
   if (ratio == 1.0) {  // every Gauss point lies in the cell itself (0 < xi < 1)
-    const double l1 = log(kcell[c]);
+    const double l1 = lraw ? lraw[c] : log(kcell[c]);
     double s1 = 0.0;
     for (int q = 0; q < nq; ++q) s1 += l1;
     lk[c] = s1 / nq;
@@ -781,7 +789,7 @@ __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, cons
     for (int k = 0; k < D; ++k) fi[k] = (long long)floor(((double)cc[k] + xi[qi[k]]) * ratio);
     const long long idx = fi[0] + n_top * (fi[1] + n_top * fi[2]);
     if (idx != last) {
-      lv = log(kcell[idx]);
+      lv = lraw ? __ldg(lraw + idx) : log(kcell[idx]);
       last = idx;
     }
     s += lv;
@@ -811,7 +819,7 @@ __global__ void k_features(TileGeo t, int n_l, int sub, const double* __restrict
     for (int k = 0; k < D; ++k) {  // adjacent cell (sub = 2: half-cell of a Q2 node, then its cell)
       const int h = node[k] - 1 + ((c >> k) & 1);
       in = in && h >= 0 && h < n_l * sub;
-      cc[k] = h / sub;
+      cc[k] = sub == 1 ? h : (sub == 2 ? h >> 1 : h / sub);  // h >= 0 wherever cc is used
     }
     if (!in) continue;
     const double lk = lkc ? __ldg(lkc + cc[0] + (long long)n_l * (cc[1] + (long long)n_l * cc[2])) : log(kconst);
@@ -1112,11 +1120,25 @@ void net_refresh_weights(fmg_net* net, cudaStream_t st) {
   net->weights_stale = false;
 }
 
-void launch_logmean(const double* k, long long n, double* scratch, double* out, cudaStream_t st) {
-  const int nb = 256;
+// the mean log k over the n top-level cells into out (= net->stat, its
+// partials after it), the logs themselves kept in net->lraw for the levels'
+// cell means
+int launch_logmean(fmg_net* net, const double* k, long long n, double* out, cudaStream_t st) {
+  const int nb = kLogSumBlocks;  // fixed, so the sum's order does not depend on the GPU
+  net->lraw_n = 0;
+  if (n > net->lraw_cap) {
+    cudaStreamSynchronize(st);
+    net_free(net, net->lraw);
+    net->lraw = nullptr;
+    net->lraw_cap = 0;
+    if (int rc = net_alloc(net, (void**)&net->lraw, (size_t)n * sizeof(double))) return rc;
+    net->lraw_cap = n;
+  }
   g_launches.fetch_add(2, std::memory_order_relaxed);
-  k_logsum<<<nb, kBlock, 0, st>>>(k, n, scratch);
-  k_logmean_final<<<1, kBlock, 0, st>>>(scratch, nb, n, out);
+  k_logsum<<<nb, kBlock, 0, st>>>(k, n, net->lraw, out + 8);
+  k_logmean_final<<<1, kBlock, 0, st>>>(out + 8, nb, n, out);
+  net->lraw_n = n;
+  return FMG_OK;
 }
 
 int launch_features(fmg_net* net, const ActGeom& g, int n_l, int sub, long long n_top, double ratio, int np,
@@ -1133,13 +1155,16 @@ int launch_features(fmg_net* net, const ActGeom& g, int n_l, int sub, long long 
     net->lk_cap = ncell;
   }
   const double* lk = kcell ? net->lk : nullptr;
+  long long ntop = n_top;
+  for (int k = 1; k < g.D; ++k) ntop *= n_top;
+  const double* lraw = net->lraw_n == ntop ? net->lraw : nullptr;  // logs of this top level
   if (ncell >= (1LL << 32) || g.nodes() >= (1LL << 32)) return FMG_ERR_UNSUPPORTED;
   g_launches.fetch_add(kcell ? 2 : 1, std::memory_order_relaxed);
   if (g.D == 3) {
-    if (kcell) k_cell_logk<3><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, net->lk);
+    if (kcell) k_cell_logk<3><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, lraw, net->lk);
     k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, sub, lk, kconst, mean, net->X0);
   } else {
-    if (kcell) k_cell_logk<2><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, net->lk);
+    if (kcell) k_cell_logk<2><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, lraw, net->lk);
     k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, sub, lk, kconst, mean, net->X0);
   }
   return FMG_OK;
