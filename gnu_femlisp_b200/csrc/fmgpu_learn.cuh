@@ -69,8 +69,8 @@ struct fmg_net {
   float* part = nullptr;       // weight-gradient partials
   long long part_cap = 0;
   double* stat = nullptr;      // [0] mean log k, from [8] the kLogSumBlocks partials of its sum
-  double* lk = nullptr;        // cell log-coefficients of the level being featurised
-  long long lk_cap = 0;
+  float* fc = nullptr;         // cell feature values of the level being featurised
+  long long fc_cap = 0;
   double* lraw = nullptr;      // log k of every top-level cell, taken with the mean
   long long lraw_cap = 0, lraw_n = 0;  // capacity; cells it holds now (0: none)
   unsigned* err = nullptr;     // device error word (bounded waits that ran out)

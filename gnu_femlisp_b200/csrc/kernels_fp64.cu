@@ -509,26 +509,33 @@ __device__ __forceinline__ double q2_row_sum(const double* __restrict__ A, long 
   for (int sz = 0; sz < NZ; ++sz) {
     const bool rz = D > 2 && (sz == 0 || sz == 4);
     if (rz && (PAT & 4)) continue;
-    double av[25], xv[25];
+    // the loads of a plane's rows 0-2, their multiply-adds, then rows 3-4
+    // (at most 30 doubles in flight: the 3D kernels fit four or five blocks
+    // per SM without spills); the sum stays in slot order
+    double av[15], xv[15];
     int q = 0;
 #pragma unroll
     for (int sy = 0; sy < NY; ++sy) {
       const bool ry = D > 1 && (sy == 0 || sy == 4);
-      if (ry && (PAT & 2)) continue;
-      const double* xl = x + (long long)M * (cl[1][sy] + (long long)M * cl[2][sz]);
+      if (!(ry && (PAT & 2))) {
+        const double* xl = x + (long long)M * (cl[1][sy] + (long long)M * cl[2][sz]);
 #pragma unroll
-      for (int sx = 0; sx < 5; ++sx) {
-        const bool rx = sx == 0 || sx == 4;
-        if (rx && (PAT & 1)) continue;
-        const int slot = sx + 5 * (sy + 5 * sz);
-        const int r = (rx ? 1 : 0) | (ry ? 2 : 0) | (rz ? 4 : 0);
-        av[q] = __ldg(A + (long long)slot * Np + p[r]);
-        xv[q] = XL == 1 ? __ldg(xl + cl[0][sx]) : xl[cl[0][sx]];
-        ++q;
+        for (int sx = 0; sx < 5; ++sx) {
+          const bool rx = sx == 0 || sx == 4;
+          if (rx && (PAT & 1)) continue;
+          const int slot = sx + 5 * (sy + 5 * sz);
+          const int r = (rx ? 1 : 0) | (ry ? 2 : 0) | (rz ? 4 : 0);
+          av[q] = __ldg(A + (long long)slot * Np + p[r]);
+          xv[q] = XL == 1 ? __ldg(xl + cl[0][sx]) : xl[cl[0][sx]];
+          ++q;
+        }
+      }
+      if (sy == 2 || sy == NY - 1) {
+#pragma unroll
+        for (int k = 0; k < q; ++k) s = fma(av[k], xv[k], s);
+        q = 0;
       }
     }
-#pragma unroll
-    for (int k = 0; k < q; ++k) s = fma(av[k], xv[k], s);
   }
   return s;
 }

@@ -756,16 +756,24 @@ __global__ void k_ratio_acc(double* scal, int dst, int num, int den, double fact
   scal[dst] = first ? r : scal[dst] + r;
 }
 
+// a cell's input to the network: its mean log-coefficient lk, centred by the
+// top level's mean log k, halved and clamped to [-8, 8]
+__device__ __forceinline__ float cell_feature(double lk, double mu) {
+  return (float)fmin(fmax((lk - mu) * 0.5, -8.0), 8.0);
+}
+
 // log-coefficient of every cell of one Q1 level: the mean of log k over the
 // cell's np^D Gauss points xi, k being the top level's cell coefficient
 // (ratio = n_top / n_l fine cells per level cell and direction).  Consecutive
 // points in one fine cell reuse its logarithm (the same value the sum would
 // add again), so the top level costs one log per cell; with lraw (log k of
 // every top-level cell, taken with the mean) no level takes a logarithm.
+// Written: the cell's feature value (cell_feature), once per cell rather than
+// once per adjacent node.
 template <int D>
 __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, const double* __restrict__ xi,
                             const double* __restrict__ kcell, const double* __restrict__ lraw,
-                            double* __restrict__ lk) {
+                            const double* __restrict__ mean, float* __restrict__ fc) {
   long long nc = n_l;
   for (int k = 1; k < D; ++k) nc *= n_l;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -778,7 +786,7 @@ __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, cons
     const double l1 = lraw ? lraw[c] : log(kcell[c]);
     double s1 = 0.0;
     for (int q = 0; q < nq; ++q) s1 += l1;
-    lk[c] = s1 / nq;
+    fc[c] = cell_feature(s1 / nq, *mean);
     return;
   }
   double s = 0.0, lv = 0.0;
@@ -794,36 +802,36 @@ __global__ void k_cell_logk(int n_l, long long n_top, double ratio, int np, cons
     }
     s += lv;
   }
-  lk[c] = s / nq;
+  fc[c] = cell_feature(s / nq, *mean);
 }
 
-// node features of one Q1 level from the level's cell log-coefficients lk
-// (null: the constant log kconst)
+// node features of one Q1 level from the level's cell feature values fc
+// (null: every cell the value of the constant log kconst); blockIdx.y is the
+// node plane
 template <int D>
-__global__ void k_features(TileGeo t, int n_l, int sub, const double* __restrict__ lkc, double kconst,
+__global__ void k_features(TileGeo t, int n_l, int sub, const float* __restrict__ fc, double kconst,
                            const double* __restrict__ mean, bf16* __restrict__ X0) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)t.Mx * t.My * t.Mz) return;
-  const unsigned iu = (unsigned)i, mx = (unsigned)t.Mx, my = (unsigned)t.My;  // < 2^32 nodes (launcher)
-  const int ix = (int)(iu % mx), iy = (int)((iu / mx) % my), iz = (int)(iu / (mx * my));
+  const unsigned iu = blockIdx.x * blockDim.x + threadIdx.x, mx = (unsigned)t.Mx;
+  if (iu >= mx * (unsigned)t.My) return;
+  const int iy = (int)(iu / mx), ix = (int)(iu - (unsigned)iy * mx), iz = D == 3 ? (int)blockIdx.y : 0;
   const int node[3] = {ix, iy, iz};
   constexpr int NC = 1 << D;
+  const float fconst = fc ? 0.f : cell_feature(log(kconst), *mean);
   float f[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) f[c] = 0.f;
-  const double mu = *mean;
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     int cc[3] = {0, 0, 0};
     bool in = true;
+#pragma unroll
     for (int k = 0; k < D; ++k) {  // adjacent cell (sub = 2: half-cell of a Q2 node, then its cell)
       const int h = node[k] - 1 + ((c >> k) & 1);
       in = in && h >= 0 && h < n_l * sub;
       cc[k] = sub == 1 ? h : (sub == 2 ? h >> 1 : h / sub);  // h >= 0 wherever cc is used
     }
     if (!in) continue;
-    const double lk = lkc ? __ldg(lkc + cc[0] + (long long)n_l * (cc[1] + (long long)n_l * cc[2])) : log(kconst);
-    f[c] = (float)fmin(fmax((lk - mu) * 0.5, -8.0), 8.0);
+    f[c] = fc ? __ldg(fc + cc[0] + (long long)n_l * (cc[1] + (long long)n_l * cc[2])) : fconst;
     f[NC + c] = 1.f;
   }
   uint4* o = reinterpret_cast<uint4*>(X0 + pad_index<D>(t, ix, iy, iz) * kNetIn);
@@ -1146,26 +1154,27 @@ int launch_features(fmg_net* net, const ActGeom& g, int n_l, int sub, long long 
   const TileGeo t = tile_geo(g);
   long long ncell = n_l;
   for (int k = 1; k < g.D; ++k) ncell *= n_l;
-  if (kcell && ncell > net->lk_cap) {
+  if (kcell && ncell > net->fc_cap) {
     cudaStreamSynchronize(st);
-    net_free(net, net->lk);
-    net->lk = nullptr;
-    net->lk_cap = 0;
-    if (int rc = net_alloc(net, (void**)&net->lk, (size_t)ncell * sizeof(double))) return rc;
-    net->lk_cap = ncell;
+    net_free(net, net->fc);
+    net->fc = nullptr;
+    net->fc_cap = 0;
+    if (int rc = net_alloc(net, (void**)&net->fc, (size_t)ncell * sizeof(float))) return rc;
+    net->fc_cap = ncell;
   }
-  const double* lk = kcell ? net->lk : nullptr;
+  const float* fc = kcell ? net->fc : nullptr;
   long long ntop = n_top;
   for (int k = 1; k < g.D; ++k) ntop *= n_top;
   const double* lraw = net->lraw_n == ntop ? net->lraw : nullptr;  // logs of this top level
-  if (ncell >= (1LL << 32) || g.nodes() >= (1LL << 32)) return FMG_ERR_UNSUPPORTED;
+  if (ncell >= (1LL << 32) || g.nodes() >= (1LL << 32) || g.Mz > 65535) return FMG_ERR_UNSUPPORTED;
   g_launches.fetch_add(kcell ? 2 : 1, std::memory_order_relaxed);
+  const dim3 fg(blocks_for((long long)g.Mx * g.My), g.D == 3 ? (unsigned)g.Mz : 1u);  // node planes in y
   if (g.D == 3) {
-    if (kcell) k_cell_logk<3><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, lraw, net->lk);
-    k_features<3><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, sub, lk, kconst, mean, net->X0);
+    if (kcell) k_cell_logk<3><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, lraw, mean, net->fc);
+    k_features<3><<<fg, 256, 0, st>>>(t, n_l, sub, fc, kconst, mean, net->X0);
   } else {
-    if (kcell) k_cell_logk<2><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, lraw, net->lk);
-    k_features<2><<<blocks_for(g.nodes()), 256, 0, st>>>(t, n_l, sub, lk, kconst, mean, net->X0);
+    if (kcell) k_cell_logk<2><<<blocks_for(ncell), 256, 0, st>>>(n_l, n_top, ratio, np, xi, kcell, lraw, mean, net->fc);
+    k_features<2><<<fg, 256, 0, st>>>(t, n_l, sub, fc, kconst, mean, net->X0);
   }
   return FMG_OK;
 }
