@@ -650,13 +650,10 @@ __device__ __forceinline__ bool fdir(int c, int M, int k, int dmask) {
 // Q1 restriction: three fine nodes per direction with weights 1/2, 1, 1/2,
 // fixed-size loops in registers
 template <int D, typename TR>
-__global__ void __launch_bounds__(kBlock)
-k_restrict_q1(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat16* __restrict__ bc,
-              float* __restrict__ xc) {
-  if (D == 1 && threadIdx.y != 0) return;
-  const int cJ[3] = {(int)(blockIdx.x * 32 + threadIdx.x), D > 1 ? (int)(blockIdx.y * 8 + threadIdx.y) : 0,
-                     D > 2 ? (int)blockIdx.z : 0};
-  if (cJ[0] >= MC || cJ[1] >= MC) return;
+__device__ __forceinline__ void restrict_q1_node(int MC, int MF, int dmask, const TR* __restrict__ rf,
+                                                 __nv_bfloat16* __restrict__ bc, float* __restrict__ xc, int c0,
+                                                 int c1, int c2) {
+  const int cJ[3] = {c0, c1, c2};
   const long long J = cJ[0] + (long long)MC * (cJ[1] + (long long)MC * cJ[2]);
   if (D == 3 && cJ[0] >= 1 && cJ[0] <= MC - 2 && cJ[1] >= 1 && cJ[1] <= MC - 2 && cJ[2] >= 1 && cJ[2] <= MC - 2) {
     // interior coarse node: its 27 fine neighbours lie inside and off every
@@ -707,6 +704,62 @@ k_restrict_q1(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat1
   }
   bc[J] = __float2bfloat16_rn(acc);
   xc[J] = 0.f;
+}
+
+template <int D, typename TR>
+__global__ void __launch_bounds__(kBlock)
+k_restrict_q1(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat16* __restrict__ bc,
+              float* __restrict__ xc) {
+  if (D == 1 && threadIdx.y != 0) return;
+  const int c0 = (int)(blockIdx.x * 32 + threadIdx.x), c1 = D > 1 ? (int)(blockIdx.y * 8 + threadIdx.y) : 0;
+  if (c0 >= MC || c1 >= MC) return;
+  restrict_q1_node<D, TR>(MC, MF, dmask, rf, bc, xc, c0, c1, D > 2 ? (int)blockIdx.z : 0);
+}
+
+// 3D Q1 restriction by 2 x 2 coarse nodes (J0 .. J0+1, K0 .. K0+1 at one I)
+// per thread, blocks (32, 8) over I and J0 / 2, blockIdx.z = K0 / 2: when all
+// four are interior their 5 x 5 fine rows are summed over x once and shared
+// (75 loads for four nodes instead of 108), each node then combined over y
+// and z exactly as k_restrict_q1's interior form does; otherwise each node
+// takes k_restrict_q1's per-node form
+template <typename TR>
+__global__ void __launch_bounds__(kBlock)
+k_restrict_q1b(int MC, int MF, int dmask, const TR* __restrict__ rf, __nv_bfloat16* __restrict__ bc,
+               float* __restrict__ xc) {
+  const int I = blockIdx.x * 32 + threadIdx.x, J0 = 2 * (blockIdx.y * 8 + threadIdx.y), K0 = 2 * blockIdx.z;
+  if (I >= MC || J0 >= MC) return;
+  if (I >= 1 && I <= MC - 2 && J0 >= 1 && J0 + 1 <= MC - 2 && K0 >= 1 && K0 + 1 <= MC - 2) {
+    const long long MF2 = (long long)MF * MF;
+    const TR* p0 = rf + (2 * I - 1) + (long long)MF * (2 * J0 - 1) + MF2 * (2 * K0 - 1);
+    float u[5][5];
+#pragma unroll
+    for (int z = 0; z < 5; ++z)
+#pragma unroll
+      for (int y = 0; y < 5; ++y) {
+        const TR* q = p0 + (long long)MF * y + MF2 * z;
+        u[z][y] = fmaf(.5f, ldv(q, 0) + ldv(q, 2), ldv(q, 1));
+      }
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+        float t[3];
+#pragma unroll
+        for (int z = 0; z < 3; ++z) {
+          const float* w = u[2 * dz + z] + 2 * dy;
+          t[z] = fmaf(.5f, w[0] + w[2], w[1]);
+        }
+        const long long J = I + (long long)MC * ((J0 + dy) + (long long)MC * (K0 + dz));
+        bc[J] = __float2bfloat16_rn(fmaf(.5f, t[0] + t[2], t[1]));
+        xc[J] = 0.f;
+      }
+    return;
+  }
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+      if (J0 + dy < MC && K0 + dz < MC) restrict_q1_node<3, TR>(MC, MF, dmask, rf, bc, xc, I, J0 + dy, K0 + dz);
 }
 
 // restriction of a residual (FP32 or BF16) into the coarse rhs (BF16), coarse
@@ -1476,7 +1529,11 @@ void mx_restrict(const Lev32& F, const Lev32& C, const void* rf, bool rf_bf16, _
   const dim3 gr = xgrid(C.M, F.dim), bl(32, 8);
   if (F.order == 1) {
     typedef __nv_bfloat16 bf;
-    if (F.dim == 3) {
+    if (F.dim == 3 && C.N >= (1ll << 20)) {  // large levels: 2 x 2 coarse nodes per thread
+      const dim3 g2((unsigned)((C.M + 31) / 32), (unsigned)((C.M + 15) / 16), (unsigned)((C.M + 1) / 2));
+      if (rf_bf16) k_restrict_q1b<bf><<<g2, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
+      else k_restrict_q1b<float><<<g2, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
+    } else if (F.dim == 3) {  // small levels are latency-bound: one coarse node per thread
       if (rf_bf16) k_restrict_q1<3, bf><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const bf*)rf, bc, xc);
       else k_restrict_q1<3, float><<<gr, bl, 0, st>>>((int)C.M, (int)F.M, F.dmask, (const float*)rf, bc, xc);
     } else if (F.dim == 2) {

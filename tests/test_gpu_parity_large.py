@@ -75,3 +75,25 @@ def test_benchmark_recipe_mixed_error_vs_oracle(oracle_mod, G, ctx):
         assert st == 0 and hist[-1] / hist[0] < 1e-10
         err = np.linalg.norm(xm.get() - ref.x) / np.linalg.norm(ref.x)
         assert err <= 1e-10, (mf, err)
+
+
+def test_benchmark_size_mixed_matrix_free_vs_fp64(G, ctx):
+    # the benchmark's own size (257^3 nodes): the matrix-free mixed solve runs
+    # the large-level kernels (restriction by 2 x 2 coarse nodes into the
+    # 129^3 level, prolongation into the padded top level by 16-byte row
+    # segments) and must end within 1e-10 of an FP64 solve driven to 1e-13
+    from gnu_femlisp_b200 import problems
+    wl = problems.c3(seed=0, level=8)
+    g = G.Grid(ctx, 3, 1, 8, base_level=wl.base_level)
+    g.set_coefficient(G._capi.FMG_K_CELL, wl.kcell)
+    g.assemble()
+    x64 = g.vector()
+    _, _, st64 = g.solve(_cfg(G, 1e-13), x64)
+    assert st64 == 0
+    xm = g.vector()
+    hist, nouter, ninner, st = g.solve_mixed(_cfg(G), xm, matrix_free=True)
+    assert st == 0 and hist[-1] / hist[0] < 1e-10
+    ref = x64.get()
+    err = np.linalg.norm(xm.get() - ref) / np.linalg.norm(ref)
+    assert err <= 1e-10, err
+    assert ninner <= 20, ninner
