@@ -1124,16 +1124,21 @@ __global__ void k_scale_out(const float* __restrict__ e32, const double* __restr
 
 // FP64 flexible-CG update: x += lam p; r -= lam a; (r, r); and the FP32
 // copy of the new residual scaled by the current scale slot; all five in one
-// layout (natural or padded), two entries per thread, 16-byte accesses; the
-// padding is zero in p and a and stays zero in x and r
+// layout (natural or padded), two entries per thread and pass, 16-byte
+// accesses; the padding is zero in p and a and stays zero in x and r.  A
+// fixed grid of kUpdBlocks blocks strides over the vectors, so the last
+// block's sum of the per-block partials is short and the sum's order does
+// not depend on the GPU.
+constexpr int kUpdBlocks = 1184;  // eight per SM of a B200
 __global__ void __launch_bounds__(kBlock)
 k_fcg64_update(double* sc, double* __restrict__ x, const float* __restrict__ p, double* __restrict__ r,
                const double* __restrict__ a, float* __restrict__ r32, long long n, Reduce2 R) {
   __shared__ double smem[8];
   const double lam = sc[M_LAM], s = sc[M_SCALE];
   double acc = 0.0;
-  const long long i0 = ((long long)blockIdx.x * kBlock + threadIdx.x) * 2;
-  if (i0 < n) {  // n is the padded length (even); padding entries are zero
+  const long long stride = (long long)gridDim.x * kBlock * 2;
+  for (long long i0 = ((long long)blockIdx.x * kBlock + threadIdx.x) * 2; i0 < n; i0 += stride) {
+    // n is the padded length (even); padding entries are zero
     const float2 pf = *reinterpret_cast<const float2*>(p + i0);
     const double2 pv = make_double2((double)pf.x, (double)pf.y);
     const double2 av = *reinterpret_cast<const double2*>(a + i0);
@@ -1581,7 +1586,8 @@ void mx_f64_to_f32(const double* a, float* b, long long n, cudaStream_t st) {
 void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const double* a, float* r32, long long np,
                      const Reduce2& R, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_fcg64_update<<<g1(np / 2), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
+  const long long nb = std::min<long long>(g1(np / 2), kUpdBlocks);
+  k_fcg64_update<<<(unsigned)std::max<long long>(nb, 1), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
 }
 
 // b (layout bl) = a (natural), 3D, M nodes a side: FP64 to FP32, and FP64 copied
