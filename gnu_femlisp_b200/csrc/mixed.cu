@@ -1418,15 +1418,28 @@ __global__ void __launch_bounds__(kBlock) k_wd_scale(const float* __restrict__ w
   }
 }
 
+// kernels over every node of an M^3 grid launched as dim3(g1(M^2), M): node
+// (ix, iy) of plane blockIdx.y with one 32-bit division (M^2 < 2^32), i its
+// natural index
+__device__ __forceinline__ bool plane_node(int M, int& ix, int& iy, int& iz, long long& i) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x, mu = (unsigned)M;
+  if (q >= mu * mu) return false;
+  iy = (int)(q / mu);
+  ix = (int)(q - (unsigned)iy * mu);
+  iz = (int)blockIdx.y;
+  i = (long long)iz * ((long long)M * M) + q;
+  return true;
+}
+
 // wd (layout g.ol) = damping / diagonal of the matrix-free top level, the diagonal formed
 // as in the matrix-free operator (4 hs times the sum of the node's 8 cell coefficients, summed
 // in the same order; cells outside the grid count zero); Dirichlet nodes
 // (identity rows) get the damping itself
 __global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ wd) {
-  const long long i = (long long)blockIdx.x * kBlock + threadIdx.x;
-  if (i >= g.N) return;
   const int M = g.M, n = g.n, dm = g.dmask;
-  const int ix = (int)(i % M), iy = (int)((i / M) % M), iz = (int)(i / ((long long)M * M));
+  int ix, iy, iz;
+  long long i;
+  if (!plane_node(M, ix, iy, iz, i)) return;
   auto dirf = [&](int c, int lo, int hi) { return (c == 0 && (dm & lo)) || (c == M - 1 && (dm & hi)); };
   const float om = g.omega ? __ldg(g.omega + i) : g.w;
   const long long o = g.ol.at(ix, iy, iz);
@@ -1453,7 +1466,7 @@ __global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ 
 
 void mx_top_wd(const MFArgs& g, float* wd, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_mf_wd<<<g1(g.N), kBlock, 0, st>>>(g, wd);
+  k_mf_wd<<<dim3(g1((long long)g.M * g.M), (unsigned)g.M), kBlock, 0, st>>>(g, wd);
 }
 
 void mx_top_apply(int mode, const MFArgs& g, const float* x, const float* b, float* y, const double* v,
@@ -1590,45 +1603,44 @@ void mx_fcg64_update(double* sc, double* x, const float* p, double* r, const dou
   k_fcg64_update<<<(unsigned)std::max<long long>(nb, 1), kBlock, 0, st>>>(sc, x, p, r, a, r32, np, R);
 }
 
-// b (layout bl) = a (natural), 3D, M nodes a side: FP64 to FP32, and FP64 copied
+// b (layout bl) = a (natural), 3D, M nodes a side: FP64 to FP32, and FP64
+// copied (grids of plane_node)
+
 __global__ void k_f64_to_f32_lay(const double* __restrict__ a, float* __restrict__ b, VLay bl, int M) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long MM = (long long)M * M;
-  if (i >= MM * M) return;
-  const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
-  b[bl.at((int)ix, (int)iy, (int)iz)] = (float)a[i];
+  int ix, iy, iz;
+  long long i;
+  if (!plane_node(M, ix, iy, iz, i)) return;
+  b[bl.at(ix, iy, iz)] = (float)a[i];
 }
 
 __global__ void k_f64_copy_lay(const double* __restrict__ a, double* __restrict__ b, VLay bl, int M) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long MM = (long long)M * M;
-  if (i >= MM * M) return;
-  const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
-  b[bl.at((int)ix, (int)iy, (int)iz)] = a[i];
+  int ix, iy, iz;
+  long long i;
+  if (!plane_node(M, ix, iy, iz, i)) return;
+  b[bl.at(ix, iy, iz)] = a[i];
 }
 
 // b (natural) = a (layout al), FP64, 3D
 __global__ void k_f64_from_lay(const double* __restrict__ a, VLay al, double* __restrict__ b, int M) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long MM = (long long)M * M;
-  if (i >= MM * M) return;
-  const long long iz = i / MM, rem = i - iz * MM, iy = rem / M, ix = rem - iy * M;
-  b[i] = a[al.at((int)ix, (int)iy, (int)iz)];
+  int ix, iy, iz;
+  long long i;
+  if (!plane_node(M, ix, iy, iz, i)) return;
+  b[i] = a[al.at(ix, iy, iz)];
 }
 
 void mx_f64_from_lay(const double* a, const VLay& al, double* b, int M, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_f64_from_lay<<<g1((long long)M * M * M), kBlock, 0, st>>>(a, al, b, M);
+  k_f64_from_lay<<<dim3(g1((long long)M * M), (unsigned)M), kBlock, 0, st>>>(a, al, b, M);
 }
 
 void mx_f64_to_f32_lay(const double* a, float* b, const VLay& bl, int M, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_f64_to_f32_lay<<<g1((long long)M * M * M), kBlock, 0, st>>>(a, b, bl, M);
+  k_f64_to_f32_lay<<<dim3(g1((long long)M * M), (unsigned)M), kBlock, 0, st>>>(a, b, bl, M);
 }
 
 void mx_f64_copy_lay(const double* a, double* b, const VLay& bl, int M, cudaStream_t st) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  k_f64_copy_lay<<<g1((long long)M * M * M), kBlock, 0, st>>>(a, b, bl, M);
+  k_f64_copy_lay<<<dim3(g1((long long)M * M), (unsigned)M), kBlock, 0, st>>>(a, b, bl, M);
 }
 
 void mx_f32_to_f64(const float* a, double* b, long long n, cudaStream_t st) {
