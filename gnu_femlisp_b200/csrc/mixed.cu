@@ -1077,25 +1077,28 @@ k_prolong_mx(int MF, int MC, int dmask, const float* __restrict__ xc, float* __r
   xf[i] += acc;
 }
 
-// coarsest level in FP64: x = A^-1 b (b BF16 -> FP64, x FP32)
+// coarsest level in FP64: x = A^-1 b (b BF16 -> FP64, x FP32), n <= 1024;
+// eight threads per row (each a strided eighth of the columns, then a
+// shuffle sum), 128 rows at a time, so the coefficient loads of all rows
+// are in flight together
 __global__ void __launch_bounds__(1024)
 k_coarse_mx(const double* __restrict__ AinvT, int n, const __nv_bfloat16* __restrict__ b, float* __restrict__ x) {
   __shared__ double rs[1024];
-  const int i = threadIdx.x;
-  if (i < n) rs[i] = (double)__bfloat162float(b[i]);
+  for (int i = threadIdx.x; i < n; i += 1024) rs[i] = (double)__bfloat162float(b[i]);
   __syncthreads();
-  if (i >= n) return;
-  double acc = 0.0;
-  int j = 0;
-  for (; j + 16 <= n; j += 16) {  // sixteen coefficients loaded before their multiply-adds
-    double a[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) a[q] = __ldg(AinvT + (long long)(j + q) * n + i);
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc = fma(a[q], rs[j + q], acc);
+  const int l8 = threadIdx.x & 7;
+  for (int base = (threadIdx.x >> 5) * 4; base < n; base += 128) {  // warp-uniform: rows base .. base+3
+    const int i = base + ((threadIdx.x >> 3) & 3);
+    double acc = 0.0;
+    if (i < n) {
+#pragma unroll 4
+      for (int j = l8; j < n; j += 8) acc = fma(__ldg(AinvT + (long long)j * n + i), rs[j], acc);
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    if (i < n && l8 == 0) x[i] = (float)acc;
   }
-  for (; j < n; ++j) acc = fma(__ldg(AinvT + (long long)j * n + i), rs[j], acc);
-  x[i] = (float)acc;
 }
 
 // ------------------------------------------------------------ vector ops
