@@ -1451,16 +1451,28 @@ __global__ void __launch_bounds__(kBlock) k_mf_wd(MFArgs g, float* __restrict__ 
     return;
   }
   float k[2][2][2];
+  if (ix >= 1 && ix <= n - 1 && iy >= 1 && iy <= n - 1 && iz >= 1 && iz <= n - 1) {
+    // interior node: its 8 cells exist, one base address and fixed strides
+    const long long nn = (long long)n * n;
+    const float* c0 = g.k + (ix - 1) + (long long)n * (iy - 1) + nn * (iz - 1);
 #pragma unroll
-  for (int cz = 0; cz < 2; ++cz)
+    for (int cz = 0; cz < 2; ++cz)
 #pragma unroll
-    for (int cy = 0; cy < 2; ++cy)
+      for (int cy = 0; cy < 2; ++cy)
 #pragma unroll
-      for (int cx = 0; cx < 2; ++cx) {
-        const int x = ix - 1 + cx, y = iy - 1 + cy, z = iz - 1 + cz;
-        const bool in = x >= 0 && x < n && y >= 0 && y < n && z >= 0 && z < n;
-        k[cz][cy][cx] = in ? __ldg(g.k + x + (long long)n * (y + (long long)n * z)) : 0.f;
-      }
+        for (int cx = 0; cx < 2; ++cx) k[cz][cy][cx] = __ldg(c0 + cx + (long long)n * cy + nn * cz);
+  } else {
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+      for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+        for (int cx = 0; cx < 2; ++cx) {
+          const int x = ix - 1 + cx, y = iy - 1 + cy, z = iz - 1 + cz;
+          const bool in = x >= 0 && x < n && y >= 0 && y < n && z >= 0 && z < n;
+          k[cz][cy][cx] = in ? __ldg(g.k + x + (long long)n * (y + (long long)n * z)) : 0.f;
+        }
+  }
   const float wc[2][2] = {{k[0][0][0] + k[1][0][0], k[0][0][1] + k[1][0][1]},
                           {k[0][1][0] + k[1][1][0], k[0][1][1] + k[1][1][1]}};
   const float ksum = (wc[0][0] + wc[0][1]) + (wc[1][0] + wc[1][1]);
